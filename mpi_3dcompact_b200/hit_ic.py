@@ -1,0 +1,138 @@
+"""Seeded initial condition for decaying homogeneous isotropic turbulence.
+
+Restates the algorithm of the reference's generator
+tests/hit/generate_init_hit.f90 (emathew1/MPI_3DCompact):
+  * the combined-LCG shuffle generator randset/randvec (:16-81);
+  * random phases phi1..phi3 in (-pi, pi] (:223-229);
+  * spectrum E(k) = (k/k0)^4 exp(-2 (k/k0)^2) (:277);
+  * the solenoidal two-angle construction of u_hat (:301-329);
+  * Hermitian symmetry on the kx=0 plane, zeroed Nyquist planes and mean (:338-356);
+  * the unnormalised complex-to-real 3-D transform (FFTW c2r, :359).
+The reference writes an ASCII Tecplot box of N+1 points; the solver grid is
+the periodic N^3 part of it, which is what this returns. Velocities are then
+scaled to a target turbulent Mach number (rms |u| / c, c = 1 for p = 1/gamma,
+rho = 1) as BASELINE's HIT configurations ask.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+_M1, _IA1, _IC1 = 259200, 7141, 54773
+_M2, _IA2, _IC2 = 134456, 8121, 28441
+_M3, _IA3, _IC3 = 243000, 4561, 51349
+_RM1, _RM2 = 1.0 / _M1, 1.0 / _M2
+
+
+class _Gen:
+    """randset/randvec of generate_init_hit.f90:16-81."""
+
+    def __init__(self, idum: int):
+        ix1 = (_IC1 - idum) % _M1
+        ix1 = (_IA1 * ix1 + _IC1) % _M1
+        ix2 = ix1 % _M2
+        ix1 = (_IA1 * ix1 + _IC1) % _M1
+        ix3 = ix1 % _M3
+        r = [0.0] * 97
+        for j in range(97):
+            ix1 = (_IA1 * ix1 + _IC1) % _M1
+            ix2 = (_IA2 * ix2 + _IC2) % _M2
+            r[j] = min(1.0, max(0.0, (float(ix1) + float(ix2) * _RM2) * _RM1))
+        self.r, self.ix1, self.ix2, self.ix3 = r, ix1, ix2, ix3
+
+    def vec(self, n: int) -> np.ndarray:
+        try:
+            from . import _native
+            lib = _native.host_lib()
+        except Exception:  # the host library is optional for small fields
+            lib = None
+        if lib is not None and n > 200000:
+            return _native.hit_randvec(lib, self, n)
+        out = np.empty(n)
+        r, ix1, ix2, ix3 = self.r, self.ix1, self.ix2, self.ix3
+        for m in range(n):
+            ix1 = (_IA1 * ix1 + _IC1) % _M1
+            ix2 = (_IA2 * ix2 + _IC2) % _M2
+            ix3 = (_IA3 * ix3 + _IC3) % _M3
+            j = (97 * ix3) // _M3 % 97
+            out[m] = r[j]
+            r[j] = min(1.0, max(0.0, (float(ix1) + float(ix2) * _RM2) * _RM1))
+        self.ix1, self.ix2, self.ix3 = ix1, ix2, ix3
+        return out
+
+
+def hit_velocity(n: int, k0: float = 4.0, seed: int = 1):
+    """Random-phase solenoidal velocity on an n^3 periodic box of side 2*pi,
+    arrays shaped (n, n, n) = (z, y, x). `seed` plays the role of randset's idum."""
+    if n % 2:
+        raise ValueError("n must be even (generate_init_hit.f90:150-153)")
+    kx_max = n // 2 + 1
+    shape_f = (n, n, kx_max)        # Fortran (kx, ky, kz) column-major == C (kz, ky, kx)
+    g = _Gen(seed)
+    cnt = kx_max * n * n
+    # randvec fills phi(kx, ky, kz) in Fortran order: kx fastest
+    phis = [2.0 * math.pi * (g.vec(cnt).reshape(shape_f) - 0.5) for _ in range(3)]
+    tol = 1e-4
+    kmin = tol
+    i = np.arange(kx_max, dtype=np.float64)
+    j = np.arange(n)
+    kx = i[None, None, :]
+    ky = np.where(j + 1 > kx_max, -(n - j).astype(np.float64), j.astype(np.float64))[None, :, None]
+    kz = np.where(j + 1 > kx_max, -(n - j).astype(np.float64), j.astype(np.float64))[:, None, None]
+    kxyz = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    kxy = np.sqrt(kx ** 2 + ky ** 2) + 0.0 * kz
+    eq = (kxyz / k0) ** 4 * np.exp(-2.0 * (kxyz / k0) ** 2)
+    amp = np.where(kxyz > kmin, np.sqrt(eq / (2.0 * math.pi * np.maximum(kxyz, kmin) ** 2)), 0.0)
+    a = amp * np.exp(1j * phis[0]) * np.cos(phis[2])
+    b = amp * np.exp(1j * phis[1]) * np.sin(phis[2])
+    safe = np.maximum(kxyz * kxy, 1e-300)
+    out = []
+    for comp in range(3):
+        if comp == 0:
+            uk = np.where(kxy > kmin, (a * kxyz * ky + b * kx * kz) / safe, (a + b) / math.sqrt(2.0))
+        elif comp == 1:
+            uk = np.where(kxy > kmin, (b * ky * kz - a * kxyz * kx) / safe, (b - a) / math.sqrt(2.0))
+        else:
+            uk = -b * kxy / np.maximum(kxyz, kmin)
+        uk = np.where(kxyz > kmin, uk, 0.0).astype(np.complex128)
+        # Hermitian symmetry on the kx = 0 plane (:338-348), Fortran 1-based -> 0-based
+        for kk in range(1, n):
+            for jj in range(kx_max, n):
+                uk[kk, jj, 0] = np.conj(uk[n - kk, n - jj, 0])
+        for kk in range(kx_max, n):
+            uk[kk, 0, 0] = np.conj(uk[n - kk, 0, 0])
+        for jj in range(kx_max, n):
+            uk[0, jj, 0] = np.conj(uk[0, n - jj, 0])
+        # odd-ball (Nyquist) planes and the mean removed (:351-356)
+        uk[:, :, kx_max - 1] = 0.0
+        uk[:, kx_max - 1, :] = 0.0
+        uk[kx_max - 1, :, :] = 0.0
+        uk[0, 0, 0] = 0.0
+        u = np.fft.irfftn(uk, s=(n, n, n), axes=(0, 1, 2)) * float(n) ** 3
+        out.append(np.ascontiguousarray(u))
+    return out
+
+
+def hit_initial_condition(n: int, k0: float = 4.0, seed: int = 1, mt: float = 0.3, gamma: float = 1.4):
+    """Primitive ICs (rho, U, V, W, p) with rho = 1, p = 1/gamma (c = 1) and the
+    velocity scaled so that sqrt(<|u|^2>)/c = mt."""
+    u, v, w = hit_velocity(n, k0, seed)
+    urms = math.sqrt(float(np.mean(u * u + v * v + w * w)))
+    s = mt / urms if urms > 0 else 0.0
+    rho = np.ones((n, n, n))
+    p = np.full((n, n, n), 1.0 / gamma)
+    return [rho, u * s, v * s, w * s, p]
+
+
+def reynolds_lambda_mu(ic, L=2.0 * math.pi):
+    """mu_ref giving Re_lambda for a target (helper for the HIT configurations):
+    returns (u', lambda) where u' = rms of one component and lambda the Taylor
+    microscale sqrt(<u^2>/<(du/dx)^2>), spectral derivative on the periodic box."""
+    rho, u, v, w, p = ic
+    n = u.shape[0]
+    k = np.fft.fftfreq(n, d=L / n) * 2.0 * math.pi
+    du = np.real(np.fft.ifft(1j * k[None, None, :] * np.fft.fft(u, axis=2), axis=2))
+    up = math.sqrt(float(np.mean(u * u + v * v + w * w)) / 3.0)
+    lam = math.sqrt(float(np.mean(u * u)) / float(np.mean(du * du)))
+    return up, lam

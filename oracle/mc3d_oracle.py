@@ -1,0 +1,742 @@
+"""CPU oracle: a numpy restatement of the reference CurvilinearCSolver time step.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the product package imports this module;
+only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+may call it, and only as the checker. Every function cites the file:line of
+emathew1/MPI_3DCompact (paths relative to that project) whose arithmetic it
+restates. The restatement itself is pinned against the reference's own C++,
+compiled unchanged into ``oracle/_ref/mc3d_ref`` (see oracle/Makefile), through
+the fixtures in tests/golden/.
+
+Layout: every field is a float64 array shaped (Nz, Ny, Nx) (x fastest), the
+global order the reference uses for its dumps (CurvilinearCSolver_Core.cpp:1333).
+Direction d in {0,1,2} = xi1 (x, axis 2), xi2 (y, axis 1), xi3 (z, axis 0).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PERIODIC, DIRICHLET = 0, 1
+_AXIS = {0: 2, 1: 1, 2: 0}
+
+
+def _to_lines(f, d):
+    return np.moveaxis(f, _AXIS[d], -1)
+
+
+def _from_lines(f, d):
+    return np.moveaxis(f, -1, _AXIS[d])
+
+
+# --------------------------------------------------------------------------
+# Banded solvers (src/Utils.cpp:4-191), vectorised over leading axes.
+# --------------------------------------------------------------------------
+def solve_tri(a, b, c, d):
+    """Thomas algorithm, src/Utils.cpp:4-20 (a[0] and c[n-1] unused)."""
+    n = d.shape[-1]
+    work = np.array(b, dtype=np.float64, copy=True)
+    x = np.array(d, dtype=np.float64, copy=True)
+    for ip in range(1, n):
+        m = a[ip] / work[ip - 1]
+        work[ip] = work[ip] - m * c[ip - 1]
+        x[..., ip] = x[..., ip] - m * x[..., ip - 1]
+    x[..., n - 1] /= work[n - 1]
+    for ip in range(n - 2, -1, -1):
+        x[..., ip] = (x[..., ip] - c[ip] * x[..., ip + 1]) / work[ip]
+    return x
+
+
+def cyclic(a, b, c, alpha, beta, r):
+    """Sherman-Morrison cyclic tridiagonal, src/Utils.cpp:22-46."""
+    n = r.shape[-1]
+    gamma = -b[0]
+    bb = np.array(b, dtype=np.float64, copy=True)
+    bb[0] = b[0] - gamma
+    bb[n - 1] = b[n - 1] - alpha * beta / gamma
+    x = solve_tri(a, bb, c, r)
+    u = np.zeros(n)
+    u[0] = gamma
+    u[n - 1] = alpha
+    z = solve_tri(a, bb, c, u)
+    fact = (x[..., 0] + beta * x[..., n - 1] / gamma) / (1.0 + z[0] + beta * z[n - 1] / gamma)
+    return x - fact[..., None] * z
+
+
+def solve_penta(e, a, d, c, f, b):
+    """Pentadiagonal elimination, src/Utils.cpp:48-83 (band layout of :50-57)."""
+    size = b.shape[-1]
+    x = np.array(a, dtype=np.float64, copy=True)        # lower band, becomes multipliers
+    B = np.array(b, dtype=np.float64, copy=True)
+    C = np.array(c, dtype=np.float64, copy=True)
+    D = np.array(d, dtype=np.float64, copy=True)
+    xs = np.zeros(b.shape)
+    for ip in range(1, size - 1):
+        xmult = x[ip - 1] / D[ip - 1]
+        D[ip] = D[ip] - xmult * C[ip - 1]
+        C[ip] = C[ip] - xmult * f[ip - 1]
+        B[..., ip] = B[..., ip] - xmult * B[..., ip - 1]
+        xmult = e[ip - 1] / D[ip - 1]
+        x[ip] = x[ip] - xmult * C[ip - 1]
+        D[ip + 1] = D[ip + 1] - xmult * f[ip - 1]
+        B[..., ip + 1] = B[..., ip + 1] - xmult * B[..., ip - 1]
+    xmult = x[size - 2] / D[size - 2]
+    D[size - 1] = D[size - 1] - xmult * C[size - 2]
+    xs[..., size - 1] = (B[..., size - 1] - xmult * B[..., size - 2]) / D[size - 1]
+    xs[..., size - 2] = (B[..., size - 2] - C[size - 2] * xs[..., size - 1]) / D[size - 2]
+    for ip in range(size - 3, -1, -1):
+        xs[..., ip] = (B[..., ip] - f[ip] * xs[..., ip + 2] - C[ip] * xs[..., ip + 1]) / D[ip]
+    return xs
+
+
+def _inv4_adjugate(m):
+    """4x4 inverse by adjugate / determinant, src/Utils.cpp:193-224."""
+    def minor(r0, r1, r2, c0, c1, c2):
+        return (m[r0, c0] * (m[r1, c1] * m[r2, c2] - m[r2, c1] * m[r1, c2])
+                - m[r0, c1] * (m[r1, c0] * m[r2, c2] - m[r2, c0] * m[r1, c2])
+                + m[r0, c2] * (m[r1, c0] * m[r2, c1] - m[r2, c0] * m[r1, c1]))
+    adj = np.array([
+        [minor(1, 2, 3, 1, 2, 3), -minor(0, 2, 3, 1, 2, 3), minor(0, 1, 3, 1, 2, 3), -minor(0, 1, 2, 1, 2, 3)],
+        [-minor(1, 2, 3, 0, 2, 3), minor(0, 2, 3, 0, 2, 3), -minor(0, 1, 3, 0, 2, 3), minor(0, 1, 2, 0, 2, 3)],
+        [minor(1, 2, 3, 0, 1, 3), -minor(0, 2, 3, 0, 1, 3), minor(0, 1, 3, 0, 1, 3), -minor(0, 1, 2, 0, 1, 3)],
+        [-minor(1, 2, 3, 0, 1, 2), minor(0, 2, 3, 0, 1, 2), -minor(0, 1, 3, 0, 1, 2), minor(0, 1, 2, 0, 1, 2)]])
+    det = (m[0, 0] * minor(1, 2, 3, 1, 2, 3) - m[0, 1] * minor(1, 2, 3, 0, 2, 3)
+           + m[0, 2] * minor(1, 2, 3, 0, 1, 3) - m[0, 3] * minor(1, 2, 3, 0, 1, 2))
+    return adj * (1.0 / det)
+
+
+def cyclic_penta(e2, e1, d0, f1, f2, rhs, cp):
+    """Cyclic pentadiagonal via a rank-4 Woodbury correction, src/Utils.cpp:85-191.
+    Arguments follow the reference call cyclicPenta(offlower2, offlower, diag,
+    offupper, offupper2, RHS, cpvec) (src/Penta10.cpp:254-261)."""
+    n = rhs.shape[-1]
+    U = np.zeros((4, n))
+    V = np.zeros((4, n))
+    U[0, 0] = U[1, 1] = U[2, n - 2] = U[3, n - 1] = 1.0
+    V[0, n - 2], V[0, n - 1], V[1, n - 1] = cp[0], cp[1], cp[2]
+    V[2, 0], V[3, 0], V[3, 1] = cp[3], cp[4], cp[5]
+    Z = np.stack([solve_penta(e2, e1, d0, f1, f2, U[i]) for i in range(4)])
+    y = solve_penta(e2, e1, d0, f1, f2, rhs)
+    P = np.empty((4, 4))
+    for i in range(4):
+        for j in range(4):
+            s = 0.0
+            for k in range(n):
+                s += V[i, k] * Z[j, k]
+            P[i, j] = s
+    P += np.eye(4)
+    H = _inv4_adjugate(P)
+    # r[i] = sum_k V[i,k] y[k]; V rows have nonzeros only at k in {0,1,n-2,n-1}
+    r = [np.zeros(y.shape[:-1]) + 0.0 for _ in range(4)]
+    for i in range(4):
+        for k in (0, 1, n - 2, n - 1) if n > 3 else range(n):
+            if V[i, k] != 0.0:
+                r[i] = r[i] + V[i, k] * y[..., k]
+    s = [H[i, 0] * r[0] + H[i, 1] * r[1] + H[i, 2] * r[2] + H[i, 3] * r[3] for i in range(4)]
+    corr = Z[0] * s[0][..., None] + Z[1] * s[1][..., None] + Z[2] * s[2][..., None] + Z[3] * s[3][..., None]
+    return y - corr
+
+
+# --------------------------------------------------------------------------
+# Compact first derivatives (src/Pade6.*, src/Penta10.*, src/CD2.*)
+# --------------------------------------------------------------------------
+def _roll(phi, s):
+    """phi[(i + s) mod N] along the last axis."""
+    return np.roll(phi, -s, axis=-1)
+
+
+def pade6_lhs(n, bc):
+    """Band arrays of src/Pade6.hpp:183-215 (first derivative)."""
+    alpha = 1.0 / 3.0
+    lo = np.full(n, alpha)
+    up = np.full(n, alpha)
+    dg = np.ones(n)
+    if bc == DIRICHLET:
+        alpha11, alpha21, alpha22 = 2.0, 1.0 / 6.0, 1.0 / 2.0
+        up[0], up[1], lo[1] = alpha11, alpha22, alpha21
+        lo[n - 1], lo[n - 2], up[n - 2] = alpha11, alpha22, alpha21
+    return lo, dg, up
+
+
+def pade6_deriv_lines(phi, dh, bc):
+    """src/Pade6.cpp:187-218 (periodic RHS), :284-313 (Dirichlet RHS),
+    :351-384 (cyclic / solveTri)."""
+    n = phi.shape[-1]
+    a_1d, b_1d = 14.0 / 9.0, 1.0 / 9.0
+    cc2, cc3, cc4, cc5 = -b_1d / 4.0, -a_1d / 2.0, a_1d / 2.0, b_1d / 4.0
+    lo, dg, up = pade6_lhs(n, bc)
+    if bc == PERIODIC:
+        rhs = cc2 * _roll(phi, -2) + cc3 * _roll(phi, -1) + cc4 * _roll(phi, 1) + cc5 * _roll(phi, 2)
+        rhs = rhs / dh
+        return cyclic(lo, dg, up, 1.0 / 3.0, 1.0 / 3.0, rhs)
+    a1, b1, c1, d1, e1, f1 = -5.0 / 2.0, 2.0, 1.0 / 2.0, 0.0, 0.0, 0.0
+    a2, b2, c2, d2, e2 = -5.0 / 9.0, -1.0 / 2.0, 1.0, 1.0 / 18.0, 0.0
+    rhs = np.zeros(phi.shape)
+    p = phi
+    rhs[..., 0] = a1 * p[..., 0] + b1 * p[..., 1] + c1 * p[..., 2] + d1 * p[..., 3] + e1 * p[..., 4] + f1 * p[..., 5]
+    rhs[..., 1] = a2 * p[..., 0] + b2 * p[..., 1] + c2 * p[..., 2] + d2 * p[..., 3] + e2 * p[..., 4]
+    rhs[..., 2:n - 2] = (cc2 * p[..., 0:n - 4] + cc3 * p[..., 1:n - 3] + cc4 * p[..., 3:n - 1] + cc5 * p[..., 4:n])
+    rhs[..., n - 2] = (-e2 * p[..., n - 5] - d2 * p[..., n - 4] - c2 * p[..., n - 3] - b2 * p[..., n - 2] - a2 * p[..., n - 1])
+    rhs[..., n - 1] = (-f1 * p[..., n - 6] - e1 * p[..., n - 5] - d1 * p[..., n - 4] - c1 * p[..., n - 3]
+                       - b1 * p[..., n - 2] - a1 * p[..., n - 1])
+    rhs = rhs / dh
+    return solve_tri(lo, dg, up, rhs)
+
+
+def penta10_lhs(n, bc):
+    """Band arrays of src/Penta10.hpp:116-175 (penta layout: lower bands skip
+    the last index, src/Utils.cpp:50-57)."""
+    beta, alpha = 1.0 / 20.0, 1.0 / 2.0
+    dg = np.ones(n)
+    lo = np.full(n, alpha)
+    up = np.full(n, alpha)
+    lo2 = np.full(n, beta)
+    up2 = np.full(n, beta)
+    if bc == DIRICHLET:
+        beta1, alpha1 = 0.0, 5.0
+        beta2, alpha2_1, alpha2_2 = 0.0, 1.0 / 12.0, 5.0 / 4.0
+        beta3_1 = beta3_2 = 1.0 / 36.0
+        alpha3_1 = alpha3_2 = 4.0 / 9.0
+        up[0], up[1], up[2] = alpha1, alpha2_2, alpha3_2
+        lo[0], lo[1] = alpha2_1, alpha3_1
+        up2[0], up2[1], up2[2] = beta1, beta2, beta3_2
+        lo2[0] = beta3_1
+        up[n - 2], up[n - 3] = alpha2_1, alpha3_1
+        lo[n - 2], lo[n - 3], lo[n - 4] = alpha1, alpha2_2, alpha3_2
+        up2[n - 3] = beta3_1
+        lo2[n - 3], lo2[n - 4], lo2[n - 5] = beta1, beta2, beta3_2
+    return lo2, lo, dg, up, up2
+
+
+def penta10_deriv_lines(phi, dh, bc):
+    """src/Penta10.cpp:141-173 (periodic RHS), :211-252 (Dirichlet RHS),
+    :254-282 (cyclicPenta / solvePenta)."""
+    n = phi.shape[-1]
+    a, b, c = 17.0 / 12.0, 101.0 / 150.0, 1.0 / 100.0
+    cc1, cc2, cc3, cc4, cc5, cc6 = -c / 6.0, -b / 4.0, -a / 2.0, a / 2.0, b / 4.0, c / 6.0
+    lo2, lo, dg, up, up2 = penta10_lhs(n, bc)
+    p = phi
+    if bc == PERIODIC:
+        rhs = (cc1 * _roll(p, -3) + cc2 * _roll(p, -2) + cc3 * _roll(p, -1)
+               + cc4 * _roll(p, 1) + cc5 * _roll(p, 2) + cc6 * _roll(p, 3))
+        rhs = rhs / dh
+        beta, alpha = 1.0 / 20.0, 1.0 / 2.0
+        cp = [beta, alpha, beta, beta, alpha, beta]
+        return cyclic_penta(lo2, lo, dg, up, up2, rhs, cp)
+    a1, b1, c1, d1, e1, f1, g1, h1, i1 = (-197.0 / 60.0, -5.0 / 12.0, 5.0, -5.0 / 3.0, 5.0 / 12.0, -1.0 / 20.0,
+                                          0.0, 0.0, 0.0)
+    a2, b2, c2, d2, e2, f2, g2, h2 = (-79.0 / 240.0, -77.0 / 60.0, 55.0 / 48.0, 5.0 / 9.0, -5.0 / 48.0,
+                                      1.0 / 60.0, -1.0 / 720.0, 0.0)
+    a3, b3, c3, d3, e3, f3, g3 = (-25.0 / 54.0 / 4.0, -40.0 / 27.0 / 2.0, 0.0, 40.0 / 27.0 / 2.0,
+                                  25.0 / 54.0 / 4.0, 0.0, 0.0)
+    rhs = np.zeros(p.shape)
+    rhs[..., 0] = (a1 * p[..., 0] + b1 * p[..., 1] + c1 * p[..., 2] + d1 * p[..., 3] + e1 * p[..., 4]
+                   + f1 * p[..., 5] + g1 * p[..., 6] + h1 * p[..., 7] + i1 * p[..., 8])
+    rhs[..., 1] = (a2 * p[..., 0] + b2 * p[..., 1] + c2 * p[..., 2] + d2 * p[..., 3] + e2 * p[..., 4]
+                   + f2 * p[..., 5] + g2 * p[..., 6] + h2 * p[..., 7])
+    rhs[..., 2] = (a3 * p[..., 0] + b3 * p[..., 1] + c3 * p[..., 2] + d3 * p[..., 3] + e3 * p[..., 4]
+                   + f3 * p[..., 5] + g3 * p[..., 6])
+    rhs[..., 3:n - 3] = (cc1 * p[..., 0:n - 6] + cc2 * p[..., 1:n - 5] + cc3 * p[..., 2:n - 4]
+                         + cc4 * p[..., 4:n - 2] + cc5 * p[..., 5:n - 1] + cc6 * p[..., 6:n])
+    rhs[..., n - 3] = (-g3 * p[..., n - 7] - f3 * p[..., n - 6] - e3 * p[..., n - 5] - d3 * p[..., n - 4]
+                       - c3 * p[..., n - 3] - b3 * p[..., n - 2] - a3 * p[..., n - 1])
+    rhs[..., n - 2] = (-h2 * p[..., n - 8] - g2 * p[..., n - 7] - f2 * p[..., n - 6] - e2 * p[..., n - 5]
+                       - d2 * p[..., n - 4] - c2 * p[..., n - 3] - b2 * p[..., n - 2] - a2 * p[..., n - 1])
+    rhs[..., n - 1] = (-i1 * p[..., n - 9] - h1 * p[..., n - 8] - g1 * p[..., n - 7] - f1 * p[..., n - 6]
+                       - e1 * p[..., n - 5] - d1 * p[..., n - 4] - c1 * p[..., n - 3] - b1 * p[..., n - 2]
+                       - a1 * p[..., n - 1])
+    rhs = rhs / dh
+    return solve_penta(lo2, lo, dg, up, up2, rhs)
+
+
+def cd2_deriv_lines(phi, dh, bc):
+    """Explicit two-point difference exactly as src/CD2.cpp:129-183 computes it:
+    with a=-1/2, c=+1/2 (src/CD2.hpp:56-58) the interior and node N-1 rows are
+    (a*phi[i+1] + c*phi[i-1])/h, i.e. the NEGATIVE of the central difference,
+    while node 0 of a Dirichlet line is the positive one-sided (-3/2, 2, -1/2)/h.
+    The sign quirk is reproduced, not corrected."""
+    n = phi.shape[-1]
+    a, c = -0.5, 0.5
+    aa, bb, cc = -1.5, 2.0, -0.5
+    out = np.empty(phi.shape)
+    out[..., 1:n - 1] = (a * phi[..., 2:n] + c * phi[..., 0:n - 2]) / dh
+    if bc == PERIODIC:
+        out[..., 0] = (a * phi[..., n - 1] + c * phi[..., 1]) / dh
+        out[..., n - 1] = (a * phi[..., n - 2] + c * phi[..., 0]) / dh
+    else:
+        out[..., 0] = (aa * phi[..., 0] + bb * phi[..., 1] + cc * phi[..., 2]) / dh
+        out[..., n - 1] = (aa * phi[..., n - 1] + bb * phi[..., n - 2] + cc * phi[..., n - 3]) / dh
+    return out
+
+
+def deriv(f, d, scheme, bc, dh):
+    """calc1stDerivField for one direction (src/AbstractDerivatives.hpp:45)."""
+    lines = _to_lines(f, d)
+    if scheme == "PADE6":
+        out = pade6_deriv_lines(lines, dh, bc)
+    elif scheme == "PENTA10":
+        out = penta10_deriv_lines(lines, dh, bc)
+    elif scheme == "CD2":
+        out = cd2_deriv_lines(lines, dh, bc)
+    else:
+        raise ValueError(scheme)
+    return np.ascontiguousarray(_from_lines(out, d))
+
+
+# --------------------------------------------------------------------------
+# Compact filters (src/Compact8Filter.*, src/Compact10Filter.*)
+# --------------------------------------------------------------------------
+def compact10_coeffs(af):
+    """Interior and boundary (scheme 1) coefficients, src/Compact10Filter.hpp:58-134."""
+    a = [(193.0 + 126.0 * af) / 256.0, (105.0 + 302.0 * af) / 256.0, (-15.0 + 30.0 * af) / 64.0,
+         (45.0 - 90.0 * af) / 512.0, (-5.0 + 10.0 * af) / 256.0, (1.0 - 2.0 * af) / 512.0]
+    fb2 = [(1.0 + 1022.0 * af) / 1024.0, (507.0 + 10.0 * af) / 512.0, (45.0 + 934.0 * af) / 1024.0,
+           (-15.0 + 30.0 * af) / 128.0, (105.0 - 210.0 * af) / 512.0, (-63.0 + 126.0 * af) / 256.0,
+           (105.0 - 210.0 * af) / 512.0, (-15.0 + 30.0 * af) / 128.0, (45.0 - 90.0 * af) / 1024.0,
+           (-5.0 + 10.0 * af) / 512.0, (1.0 - 2.0 * af) / 1024.0]
+    fb3 = [(-1.0 + 2.0 * af) / 1024.0, (5.0 + 502.0 * af) / 512.0, (979.0 + 90.0 * af) / 1024.0,
+           (15.0 + 98.0 * af) / 128.0, (-105.0 + 210.0 * af) / 512.0, (63.0 - 126.0 * af) / 256.0,
+           (-105.0 + 210.0 * af) / 512.0, (15.0 - 30.0 * af) / 128.0, (-45.0 + 90.0 * af) / 1024.0,
+           (5.0 - 10.0 * af) / 512.0, (-1.0 + 2.0 * af) / 1024.0]
+    fb4 = [(1.0 - 2.0 * af) / 1024.0, (-5.0 + 10.0 * af) / 512.0, (45.0 + 934.0 * af) / 1024.0,
+           (113.0 + 30.0 * af) / 128.0, (105.0 + 302.0 * af) / 512.0, (-63.0 + 126.0 * af) / 256.0,
+           (105.0 - 210.0 * af) / 512.0, (-15.0 + 30.0 * af) / 128.0, (45.0 - 90.0 * af) / 1024.0,
+           (-5.0 + 10.0 * af) / 512.0, (1.0 - 2.0 * af) / 1024.0]
+    fb5 = [(-1.0 + 2.0 * af) / 1024.0, (5.0 - 10.0 * af) / 512.0, (-45.0 + 90.0 * af) / 1024.0,
+           (15.0 + 98.0 * af) / 128.0, (407.0 + 210.0 * af) / 512.0, (63.0 + 130.0 * af) / 256.0,
+           (-105.0 + 210.0 * af) / 512.0, (15.0 - 30.0 * af) / 128.0, (-45.0 + 90.0 * af) / 1024.0,
+           (5.0 - 10.0 * af) / 512.0, (-1.0 + 2.0 * af) / 1024.0]
+    return a, [fb2, fb3, fb4, fb5]
+
+
+def compact8_coeffs(af):
+    """Interior and boundary coefficients, src/Compact8Filter.hpp:55-94."""
+    a = [(93.0 + 70.0 * af) / 128.0, (7.0 + 18.0 * af) / 16.0, (-7.0 + 14.0 * af) / 32.0,
+         (1.0 - 2.0 * af) / 16.0, (-1.0 + 2.0 * af) / 128.0]
+    fb2 = [1.0 / 256.0 + 127.0 * af / 128.0, 31.0 / 32.0 + 1.0 * af / 16.0, 7.0 / 64.0 + 25.0 * af / 32.0,
+           -7.0 / 32.0 + 7.0 * af / 16.0, 7.0 * (5.0 - 10.0 * af) / 128.0, -7.0 / 32.0 + 7.0 * af / 16.0,
+           7.0 / 64.0 - 7.0 * af / 32.0, -1.0 / 32.0 + 1.0 * af / 16.0, 1.0 / 256.0 - 1.0 * af / 128.0]
+    fb3 = [-1.0 / 256.0 + 1.0 * af / 128.0, 1.0 / 32.0 + 15.0 * af / 16.0, 57.0 / 64.0 + 7.0 * af / 32.0,
+           7.0 / 32.0 + 9.0 * af / 16.0, 7.0 * (-5.0 + 10.0 * af) / 128.0, 7.0 / 32.0 - 7.0 * af / 16.0,
+           -7.0 / 64.0 + 7.0 * af / 32.0, 1.0 / 32.0 - 1.0 * af / 16.0, -1.0 / 256.0 + 1.0 * af / 128.0]
+    fb4 = [1.0 / 256.0 - 1.0 * af / 128.0, -1.0 / 32.0 + 1.0 * af / 16.0, 7.0 / 64.0 + 25.0 * af / 32.0,
+           25.0 / 32.0 + 7.0 * af / 16.0, 35.0 / 128.0 + 29.0 * af / 64.0, -7.0 / 32.0 + 7.0 * af / 16.0,
+           7.0 / 64.0 - 7.0 * af / 32.0, -1.0 / 32.0 + 1.0 * af / 16.0, 1.0 / 256.0 - 1.0 * af / 128.0]
+    return a, [fb2, fb3, fb4]
+
+
+def filter_lines(phi, ftype, af, bc):
+    """One-direction compact filter on lines: src/Compact10Filter.cpp:5-141 and
+    src/Compact8Filter.cpp:5-117 (periodic cyclic / Dirichlet solveTri)."""
+    n = phi.shape[-1]
+    if ftype == "COMPACT10":
+        a, fbs = compact10_coeffs(af)
+    elif ftype == "COMPACT8":
+        a, fbs = compact8_coeffs(af)
+    else:
+        raise ValueError(ftype)
+    H = len(a) - 1
+    cc = [a[0]] + [a[k] / 2.0 for k in range(1, H + 1)]
+    lo = np.full(n, af)
+    up = np.full(n, af)
+    dg = np.ones(n)
+    # the reference sums the symmetric stencil from the far-left point to the far-right point
+    rhs = np.zeros(phi.shape)
+    if bc == PERIODIC:
+        for s in range(-H, H + 1):
+            rhs = rhs + cc[abs(s)] * _roll(phi, s)
+        return cyclic(lo, dg, up, af, af, rhs)
+    lo[0] = up[0] = lo[n - 1] = up[n - 1] = 0.0
+    for s in range(-H, H + 1):
+        rhs[..., H:n - H] = rhs[..., H:n - H] + cc[abs(s)] * phi[..., H + s:n - H + s]
+    rhs[..., 0] = phi[..., 0]
+    rhs[..., n - 1] = phi[..., n - 1]
+    w = len(fbs[0])
+    for r, fb in enumerate(fbs, start=1):
+        acc = np.zeros(phi.shape[:-1])
+        acc2 = np.zeros(phi.shape[:-1])
+        for k in range(w):
+            acc = acc + fb[k] * phi[..., k]
+            acc2 = acc2 + fb[k] * phi[..., n - 1 - k]
+        rhs[..., r] = acc
+        rhs[..., n - 1 - r] = acc2
+    return solve_tri(lo, dg, up, rhs)
+
+
+def filt(f, d, ftype, af, bcs):
+    """filterField along direction d (src/Compact10Filter.cpp:166-252): lines on
+    a Dirichlet face of either other direction pass through unfiltered."""
+    lines = _to_lines(f, d)
+    out = filter_lines(lines, ftype, af, bcs[d])
+    others = [o for o in range(3) if o != d]
+    mask = np.zeros(f.shape, dtype=bool)
+    for o in others:
+        if bcs[o] == DIRICHLET:
+            ax = _AXIS[o]
+            sl0 = [slice(None)] * 3
+            sl1 = [slice(None)] * 3
+            sl0[ax] = 0
+            sl1[ax] = f.shape[ax] - 1
+            mask[tuple(sl0)] = True
+            mask[tuple(sl1)] = True
+    res = np.ascontiguousarray(_from_lines(out, d))
+    res[mask] = f[mask]
+    return res
+
+
+# --------------------------------------------------------------------------
+# Ideal gas (src/IdealGas.hpp:9-80)
+# --------------------------------------------------------------------------
+GAMMA, PR = 1.4, 0.7
+P_REF = 1.0 / GAMMA
+R_GAS = P_REF / 1.0 / 1.0
+CP = R_GAS * GAMMA / (GAMMA - 1.0)
+
+
+def primitives(q, mu_ref):
+    """updateNonConservedData, src/CurvilinearCSolver_Core.cpp:1158-1197."""
+    rho, ru, rv, rw, re = q
+    U, V, W = ru / rho, rv / rho, rw / rho
+    p = (GAMMA - 1) * (re - 0.5 * rho * (U * U + V * V + W * W))
+    T = p / (rho * R_GAS)
+    mu = mu_ref * np.power(T / 1.0, 0.76)
+    sos = np.sqrt(GAMMA * p / rho)
+    return U, V, W, p, T, mu, sos
+
+
+# --------------------------------------------------------------------------
+# Time-integration coefficients (src/RK4.hpp:27-34, src/TVDRK3.hpp,
+# src/KenRK4.hpp:30-40, src/LSLDDRK4.hpp:40-78)
+# --------------------------------------------------------------------------
+KENRK4_A = [0.0, -6234157559845.0 / 12983515589748.0, -6194124222391.0 / 4410992767914.0,
+            -31623096876824.0 / 15682348800105.0, -12251185447671.0 / 11596622555746.0]
+KENRK4_B = [494393426753.0 / 4806282396855.0, 4047970641027.0 / 5463924506627.0,
+            9795748752853.0 / 13190207949281.0, 4009051133189.0 / 8539092990294.0,
+            1348533437543.0 / 7166442652324.0]
+LSLDD_A1 = [0.0, -0.60512264332862261228, -2.04375640234761394333, -0.74069990637544192841,
+            -4.42317651302968168941]
+LSLDD_B1 = [0.26874543888713438496, 0.8014706973220802933, 0.50515704269422722538,
+            0.56235680379000296407, 0.05900655127758823335]
+LSLDD_A2 = [0.0, -0.44127377153877382565, -1.073982008079781868, -1.7063570791256758809,
+            -2.7979293162682443056, -4.0913537120919160454]
+LSLDD_B2 = [0.11584888181285561688, 0.37287699051652864918, 0.73795368921435295698,
+            0.57981109366311039538, 1.031284991300145194, 0.15]
+
+
+@dataclass
+class Config:
+    """The MPI_3DCompact.in options the time step reads (src/Options.hpp:133-206)."""
+    N: tuple = (16, 16, 16)                # (Nx, Ny, Nz)
+    bc: tuple = (PERIODIC, PERIODIC, PERIODIC)
+    fd: tuple = ("PADE6", "PADE6", "PADE6")
+    filter: str = "COMPACT10"
+    alphaF: float = 0.49
+    mu_ref: float = 0.001
+    rk: str = "RK4"
+    ts_type: str = "CONST_CFL"
+    cfl: float = 0.5
+    dt: float = -1.0
+    filter_step: int = 1
+    substep_filtering: bool = False
+    les: str = "NOMODEL"
+    les_avg: str = "NONE"
+
+
+@dataclass
+class State:
+    q1: list                                 # rho1, rhoU1, rhoV1, rhoW1, rhoE1
+    qk: list = None
+    k2: list = None
+    q2: list = None
+    time: float = 0.0
+    time_step: int = 0
+    filter_time_step: int = 0
+    dt: float = 0.0
+    history: list = field(default_factory=list)
+
+
+class Oracle:
+    """The CurvilinearCSolver time step on one block (src/CurvilinearCSolver.hpp:25-379)."""
+
+    def __init__(self, cfg: Config, metrics=None):
+        self.cfg = cfg
+        Nx, Ny, Nz = cfg.N
+        # Domain with Lx=Ly=Lz=1 (src/Domain.hpp:45-79)
+        self.dxi = [1.0 / n if b == PERIODIC else 1.0 / (n - 1.0) for n, b in zip(cfg.N, cfg.bc)]
+        if metrics is None:
+            raise ValueError("metrics (J, J11..J33) are required")
+        self.J = metrics[0]
+        self.Jm = [[metrics[1], metrics[2], metrics[3]],
+                   [metrics[4], metrics[5], metrics[6]],
+                   [metrics[7], metrics[8], metrics[9]]]
+        self.pr_t = 0.9
+
+    # -- operators --------------------------------------------------------
+    def d(self, f, direction):
+        c = self.cfg
+        return deriv(f, direction, c.fd[direction], c.bc[direction], self.dxi[direction])
+
+    def grad(self, f):
+        return [self.d(f, 0), self.d(f, 1), self.d(f, 2)]
+
+    def f3(self, f, order, ftype, af):
+        for d in order:
+            f = filt(f, d, ftype, af, self.cfg.bc)
+        return f
+
+    # -- SGS (src/VremanSGS.hpp:43-96, src/AbstractSGS.cpp:13-160) ---------
+    def vreman(self, gu, rho):
+        J = self.J
+        vol = self.dxi[0] * self.dxi[1] * self.dxi[2] / J
+        d1 = np.power(vol, 1.0 / 3.0) ** 2
+        d1v1, d2v1, d3v1 = gu[0][0], gu[0][1], gu[0][2]
+        d1v2, d2v2, d3v2 = gu[1][0], gu[1][1], gu[1][2]
+        d1v3, d2v3, d3v3 = gu[2][0], gu[2][1], gu[2][2]
+        b11 = d1 * d1v1 * d1v1 + d1 * d2v1 * d2v1 + d1 * d3v1 * d3v1
+        b12 = d1 * d1v1 * d1v2 + d1 * d2v1 * d2v2 + d1 * d3v1 * d3v2
+        b13 = d1 * d1v1 * d1v3 + d1 * d2v1 * d2v3 + d1 * d3v1 * d3v3
+        b22 = d1 * d1v2 * d1v2 + d1 * d2v2 * d2v2 + d1 * d3v2 * d3v2
+        b23 = d1 * d1v2 * d1v3 + d1 * d2v2 * d2v3 + d1 * d3v2 * d3v3
+        b33 = d1 * d1v3 * d1v3 + d1 * d2v3 * d2v3 + d1 * d3v3 * d3v3
+        # the reference sums d2v3^2 twice and omits d3v2^2 (VremanSGS.hpp:74-76)
+        abeta = (d1v1 * d1v1 + d1v2 * d1v2 + d1v3 * d1v3 + d2v1 * d2v1 + d2v2 * d2v2 + d2v3 * d2v3
+                 + d3v1 * d3v1 + d2v3 * d2v3 + d3v3 * d3v3)
+        bbeta = b11 * b22 - (b12 * b12) + b11 * b33 - (b13 * b13) + b22 * b33 - (b23 * b23)
+        eps = 1e-12
+        bbeta = np.where(bbeta < eps, eps, bbeta)
+        ss = np.sqrt(bbeta / (abeta + eps))
+        c = 2.5 * 0.17 * 0.17
+        mu_sgs = c * rho * ss
+        mu_sgs = np.minimum(mu_sgs, 0.05 * d1 * np.sqrt(2.0 * abeta))
+        if self.cfg.les_avg == "LOCAL":
+            # doAveraging LOCAL: Compact10 filter alpha=-0.49, order Y, Z, X (AbstractSGS.cpp:144-152)
+            mu_sgs = self.f3(mu_sgs, (1, 2, 0), "COMPACT10", -0.49)
+        elif self.cfg.les_avg != "NONE":
+            raise NotImplementedError("LESAVERAGING=" + self.cfg.les_avg)
+        return mu_sgs
+
+    # -- one stage: preStepDerivatives + solveEqnSet (Core.cpp:468-947) ----
+    def rhs(self, qP, k2):
+        c = self.cfg
+        J, Jm = self.J, self.Jm
+        rhoP, ruP, rvP, rwP, reP = qP
+        U, V, W, p, T, mu, sos = primitives(qP, c.mu_ref)
+        Ucurv = Jm[0][0] * U + Jm[0][1] * V + Jm[0][2] * W
+        Vcurv = Jm[1][0] * U + Jm[1][1] * V + Jm[1][2] * W
+        Wcurv = Jm[2][0] * U + Jm[2][1] * V + Jm[2][2] * W
+        dU, dV, dW = self.grad(U), self.grad(V), self.grad(W)
+
+        def phys(dq, j):   # Core.cpp:548-561: d/dx_j = sum_i J_ij d/dxi_i
+            return Jm[0][j] * dq[0] + Jm[1][j] * dq[1] + Jm[2][j] * dq[2]
+        gu = [[phys(dU, 0), phys(dU, 1), phys(dU, 2)],
+              [phys(dV, 0), phys(dV, 1), phys(dV, 2)],
+              [phys(dW, 0), phys(dW, 1), phys(dW, 2)]]
+        les = c.les != "NOMODEL"
+        mu_sgs = None
+        if c.les == "VREMAN":
+            mu_sgs = self.vreman(gu, rhoP)
+        elif les:
+            raise NotImplementedError(c.les)
+        dT = self.grad(T)
+        dUdx, dUdy, dUdz = gu[0]
+        dVdx, dVdy, dVdz = gu[1]
+        dWdx, dWdy, dWdz = gu[2]
+        t11 = (4.0 / 3.0) * dUdx - (2.0 / 3.0) * dVdy - (2.0 / 3.0) * dWdz
+        t22 = -(2.0 / 3.0) * dUdx + (4.0 / 3.0) * dVdy - (2.0 / 3.0) * dWdz
+        t33 = -(2.0 / 3.0) * dUdx - (2.0 / 3.0) * dVdy + (4.0 / 3.0) * dWdz
+        t12 = dUdy + dVdx
+        t13 = dUdz + dWdx
+        t23 = dVdz + dWdy
+        if les:
+            mu_eff = mu + mu_sgs
+            k_eff = CP * (mu / PR + mu_sgs / self.pr_t)
+            mu_eff = np.where(mu_eff < 0.0, 0.0, mu_eff)
+            k_eff = np.where(k_eff < 0.0, 0.0, k_eff)
+        else:
+            mu_eff = mu
+            k_eff = (CP / PR) * mu
+        t11, t22, t33, t12, t13, t23 = (t * mu_eff for t in (t11, t22, t33, t12, t13, t23))
+        t21, t31, t32 = t12, t13, t23
+        q1 = k_eff * (Jm[0][0] * dT[0] + Jm[1][0] * dT[1] + Jm[2][0] * dT[2])
+        q2 = k_eff * (Jm[0][1] * dT[0] + Jm[1][1] * dT[1] + Jm[2][1] * dT[2])
+        q3 = k_eff * (Jm[0][2] * dT[0] + Jm[1][2] * dT[1] + Jm[2][2] * dT[2])
+        b1 = U * t11 + V * t12 + W * t13 + q1
+        b2 = U * t21 + V * t22 + W * t23 + q2
+        b3 = U * t31 + V * t32 + W * t33 + q3
+        iJ = 1.0 / J
+        cont = [iJ * (rhoP * Ucurv), iJ * (rhoP * Vcurv), iJ * (rhoP * Wcurv)]
+
+        def mom(rq, tcol, row):
+            F1 = rq * Ucurv + Jm[0][row] * p
+            F2 = rq * Vcurv + Jm[1][row] * p
+            F3 = rq * Wcurv + Jm[2][row] * p
+            G1 = Jm[0][0] * tcol[0] + Jm[0][1] * tcol[1] + Jm[0][2] * tcol[2]
+            G2 = Jm[1][0] * tcol[0] + Jm[1][1] * tcol[1] + Jm[1][2] * tcol[2]
+            G3 = Jm[2][0] * tcol[0] + Jm[2][1] * tcol[1] + Jm[2][2] * tcol[2]
+            return [iJ * (F1 - G1), iJ * (F2 - G2), iJ * (F3 - G3)]
+        m1 = mom(ruP, (t11, t21, t31), 0)
+        m2 = mom(rvP, (t12, t22, t32), 1)
+        m3 = mom(rwP, (t13, t23, t33), 2)
+        F1, F2, F3 = (reP + p) * Ucurv, (reP + p) * Vcurv, (reP + p) * Wcurv
+        G1 = Jm[0][0] * b1 + Jm[0][1] * b2 + Jm[0][2] * b3
+        G2 = Jm[1][0] * b1 + Jm[1][1] * b2 + Jm[1][2] * b3
+        G3 = Jm[2][0] * b1 + Jm[2][1] * b2 + Jm[2][2] * b3
+        en = [iJ * (F1 - G1), iJ * (F2 - G2), iJ * (F3 - G3)]
+        comps = [cont, m1, m2, m3, en]
+        div = [[self.d(comp[0], 0), self.d(comp[1], 1), self.d(comp[2], 2)] for comp in comps]
+        dt = self.state.dt
+        # solveContinuity/X/Y/ZMomentum/Energy, Core.cpp:790-947 (no sponge, zero hooks)
+        new = [None] * 5
+        new[0] = dt * J * (-div[0][0] - div[0][1] - div[0][2] + (0.0 + 0.0) / J)
+        for e in (1, 2, 3):
+            # momentum accumulates into the previous k2 (Core.cpp:839,872,904)
+            t = k2[e] + (-div[e][0] - div[e][1] - div[e][2] + (0.0 + 0.0) / J)
+            new[e] = t * (dt * J)
+        t = -div[4][0] - div[4][1] - div[4][2] + (0.0 + 0.0) / J
+        new[4] = t * (dt * J)
+        return new
+
+    # -- time-step bookkeeping ---------------------------------------------
+    def cfl(self, q):
+        """calcDtFromCFL, Core.cpp:189-237 (diagonal metrics only)."""
+        c, st = self.cfg, self.state
+        U, V, W, p, T, mu, sos = self._prims
+        uc = (self.Jm[0][0] * (np.abs(U) + sos) / self.dxi[0] + self.Jm[1][1] * (np.abs(V) + sos) / self.dxi[1]
+              + self.Jm[2][2] * (np.abs(W) + sos) / self.dxi[2])
+        m = float(np.max(uc))
+        if c.ts_type == "CONST_CFL":
+            st.dt = c.cfl / m
+        else:
+            st.dt = c.dt
+        if st.time_step == self.start_step:
+            st.time_step += 1
+        else:
+            st.time_step += 1
+            st.time += st.dt
+
+    def filter_conserved(self, qin, last):
+        """filterConservedData, Core.cpp:949-1155: direction order rotates with
+        filterTimeStep % 3 (1: Y,Z,X; 2: Z,X,Y; 0: X,Y,Z); otherwise copy."""
+        c, st = self.cfg, self.state
+        if st.time_step % c.filter_step == 0:
+            st.filter_time_step += 1
+            r = st.filter_time_step % 3
+            order = (1, 2, 0) if r == 1 else ((2, 0, 1) if r == 2 else (0, 1, 2))
+            return [self.f3(f, order, c.filter, c.alphaF) for f in qin]
+        return [f.copy() for f in qin] if last else qin
+
+    def init(self, rho0, U0, V0, W0, p0, time=0.0, time_step=0):
+        """setInitialConditions, src/CurvilinearCSolver_BC.cpp:3-59 (periodic:
+        no walls, no sponge)."""
+        z = np.zeros_like(rho0)
+        rhoE = p0 / (GAMMA - 1.0) + 0.5 * rho0 * (U0 * U0 + V0 * V0 + W0 * W0)
+        q1 = [rho0.copy(), rho0 * U0, rho0 * V0, rho0 * W0, rhoE]
+        self.state = State(q1=q1, qk=[z.copy() for _ in range(5)], k2=[z.copy() for _ in range(5)],
+                           q2=[z.copy() for _ in range(5)], time=time, time_step=time_step)
+        self.start_step = time_step
+        T0 = p0 / (rho0 * R_GAS)
+        self._prims = (U0, V0, W0, p0, T0, self.cfg.mu_ref * np.power(T0, 0.76), np.sqrt(GAMMA * p0 / rho0))
+
+    def _stage(self, qP, rk_step, last, update):
+        st = self.state
+        st.k2 = self.rhs(qP, st.k2)
+        update(rk_step)
+        if last or self.cfg.substep_filtering:
+            if last:
+                st.q1 = self.filter_conserved(st.q2, True)
+            else:
+                st.qk = self.filter_conserved(st.qk, False)
+        src = st.q1 if last else st.qk
+        self._prims = primitives(src, self.cfg.mu_ref)
+
+    def step(self):
+        """One time step (or the LSLDDRK4 two-step pair's half): src/RK4.hpp:127-178,
+        src/TVDRK3.hpp, src/KenRK4.hpp:154-217, src/LSLDDRK4.hpp:324-459."""
+        c, st = self.cfg, self.state
+        self.cfl(st.q1)
+        if c.rk == "RK4":
+            a = [1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0]
+            b = [0.5, 0.5, 1.0]
+
+            def upd(s):   # RK4.hpp:47-125
+                k2 = st.k2
+                if s == 1:
+                    st.q2 = [st.q1[i] + a[0] * k2[i] for i in range(5)]
+                    st.qk = [st.q1[i] + b[0] * k2[i] for i in range(5)]
+                elif s in (2, 3):
+                    st.q2 = [st.q2[i] + a[s - 1] * k2[i] for i in range(5)]
+                    st.qk = [st.q1[i] + b[s - 1] * k2[i] for i in range(5)]
+                else:
+                    st.q2 = [st.q2[i] + a[3] * k2[i] for i in range(5)]
+            for s in range(1, 5):
+                self._stage(st.q1 if s == 1 else st.qk, s, s == 4, upd)
+        elif c.rk == "TVDRK3":
+            def upd(s):   # TVDRK3.hpp:50-133
+                k2 = st.k2
+                if s == 1:
+                    st.qk = [st.q1[i] + 1.0 * k2[i] for i in range(5)]
+                elif s == 2:
+                    st.qk = [(3.0 / 4.0) * st.q1[i] + (1.0 / 4.0) * st.qk[i] + (1.0 / 4.0) * k2[i] for i in range(5)]
+                else:
+                    st.q2 = [(1.0 / 3.0) * st.q1[i] + (2.0 / 3.0) * st.qk[i] + (2.0 / 3.0) * k2[i]
+                             for i in range(5)]
+            for s in range(1, 4):
+                self._stage(st.q1 if s == 1 else st.qk, s, s == 3, upd)
+        elif c.rk in ("KENRK4", "LSLDDRK4"):
+            if c.rk == "KENRK4":
+                A, B = KENRK4_A, KENRK4_B
+            else:
+                half = getattr(self, "_lsldd_half", 1)
+                A, B = (LSLDD_A1, LSLDD_B1) if half == 1 else (LSLDD_A2, LSLDD_B2)
+            ns = len(A)
+
+            def upd(s):   # 2N-storage form: KenRK4.hpp:53-152, LSLDDRK4.hpp:93-320
+                k2 = st.k2
+                if s == 1:
+                    st.qk = [st.q1[i] + B[0] * k2[i] for i in range(5)]
+                    st.q1 = [k2[i].copy() for i in range(5)]
+                else:
+                    st.q1 = [k2[i] + A[s - 1] * st.q1[i] for i in range(5)]
+                    if s < ns:
+                        st.qk = [st.qk[i] + B[s - 1] * st.q1[i] for i in range(5)]
+                    else:
+                        st.q2 = [st.qk[i] + B[s - 1] * st.q1[i] for i in range(5)]
+            for s in range(1, ns + 1):
+                self._stage(st.q1 if s == 1 else st.qk, s, s == ns, upd)
+            if c.rk == "LSLDDRK4":
+                self._lsldd_half = 2 if getattr(self, "_lsldd_half", 1) == 1 else 1
+        else:
+            raise ValueError(c.rk)
+
+    def stages_per_step(self):
+        c = self.cfg
+        if c.rk == "RK4":
+            return 4
+        if c.rk == "TVDRK3":
+            return 3
+        if c.rk == "KENRK4":
+            return 5
+        return 5 if getattr(self, "_lsldd_half", 1) == 1 else 6
+
+
+def cube_metrics(N, L=2.0 * math.pi):
+    """Analytic metrics of the periodic cube x = L*xi (the HIT box of
+    tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156): J_ii = 1/L,
+    J = 1/L^3, off-diagonals zero."""
+    Nx, Ny, Nz = N
+    shp = (Nz, Ny, Nx)
+    z = np.zeros(shp)
+    d = np.full(shp, 1.0 / L)
+    return [np.full(shp, 1.0 / L ** 3), d, z, z, z, d.copy(), z, z, z, d.copy()]
+
+
+def run(cfg: Config, ic, nsteps, metrics=None):
+    """Run `nsteps` time steps from primitive ICs (rho, U, V, W, p) and return
+    (conserved state rho1..rhoE1, state object)."""
+    o = Oracle(cfg, metrics if metrics is not None else cube_metrics(cfg.N))
+    o.init(*ic)
+    for _ in range(nsteps):
+        o.step()
+    return o.state.q1, o.state

@@ -1,0 +1,286 @@
+/*
+ * CPU oracle harness: drives the reference solver (emathew1/MPI_3DCompact,
+ * compiled unchanged from its own sources with the single-rank shims in
+ * oracle/ref_shims) so its outputs can pin the numpy restatement and the GPU
+ * path. Test infrastructure only: the product never links or runs this.
+ *
+ * It replaces the reference's driver (src/MPI_3DCompact.cpp:34-316) with a
+ * harness that supplies the mesh, the initial condition and the solver hooks
+ * (src/MPI_3DCompact.cpp:318-543 define them for the cylinder case; here they
+ * are empty, as in the HIT case tests/hit/Samtaney_D4/MPI_3DCompact.cpp).
+ *
+ * Run inside a directory holding MPI_3DCompact.in. Modes:
+ *   run  <mesh> <ic.bin> <out.bin>        N steps (TIMESTEPPING.MAXTIMESTEP),
+ *                                          then dump the conserved state.
+ *   ops  <scheme> <dir> <in.bin> <out.bin> one operator on one field:
+ *        scheme = PADE6|PENTA10|CD2 (derivative) or COMPACT8|COMPACT10 (filter,
+ *        SOLVER.ALPHAF); dir = 0,1,2.
+ *   metrics <mesh> <out.bin>               J, J11..J33 from solveForJacobians.
+ * <mesh> is "cube:<L>" (x = L*xi, the HIT box) or "file:<path>" (x,y,z FP64).
+ * All binary fields are FP64, x-fastest global order (i + Nx*(j + Ny*k)).
+ */
+#include <mpi.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+using namespace std;
+
+#include "C2Decomp.hpp"
+#include "Macros.hpp"
+#include "Options.hpp"
+#include "TimeStepping.hpp"
+#include "Domain.hpp"
+#include "BC.hpp"
+#include "AbstractCSolver.hpp"
+#include "CurvilinearCSolver.hpp"
+#include "AbstractSingleBlockMesh.hpp"
+#include "AbstractRK.hpp"
+#include "TVDRK3.hpp"
+#include "RK4.hpp"
+#include "KenRK4.hpp"
+#include "LSLDDRK4.hpp"
+
+// ---- solver hooks (the reference leaves their bodies to the driver) ----
+void CurvilinearCSolver::initialHook() {}
+void CurvilinearCSolver::fullStepTemporalHook() {}
+void CurvilinearCSolver::subStepTemporalHook() {}
+void CurvilinearCSolver::preStepBoundaryHook() {}
+void CurvilinearCSolver::postStepBoundaryHook() {}
+double CurvilinearCSolver::contRHSSource(int) { return 0.0; }
+double CurvilinearCSolver::xmomRHSSource(int) { return 0.0; }
+double CurvilinearCSolver::ymomRHSSource(int) { return 0.0; }
+double CurvilinearCSolver::zmomRHSSource(int) { return 0.0; }
+double CurvilinearCSolver::engyRHSSource(int) { return 0.0; }
+
+static void die(const string &m) {
+    fprintf(stderr, "mc3d_ref: %s\n", m.c_str());
+    exit(2);
+}
+
+static vector<double> read_bin(const string &path, size_t n) {
+    vector<double> v(n);
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) die("cannot open " + path);
+    if (fread(v.data(), sizeof(double), n, f) != n) die("short read " + path);
+    fclose(f);
+    return v;
+}
+
+// Mesh plugin: the harness's own getMesh (the reference's AlgebraicSingleBlockMesh
+// hard-codes its geometry, so each test supplies one here).
+class HarnessMesh : public AbstractSingleBlockMesh {
+  public:
+    string spec;
+    HarnessMesh(C2Decomp *c2d_, AbstractCSolver *cs_, Domain *dom, const string &spec_) : spec(spec_) {
+        mpiRank = 0;
+        cs = cs_;
+        c2d = c2d_;
+        d = dom;
+        derivX = cs->derivX;
+        derivY = cs->derivY;
+        derivZ = cs->derivZ;
+        d->getPencilDecompInfo(pxSize, pySize, pzSize, pxStart, pyStart, pzStart, pxEnd, pyEnd, pzEnd);
+        max_xi = d->gLx;
+        max_eta = d->gLy;
+        max_zta = d->gLz;
+        Nx = d->gNx;
+        Ny = d->gNy;
+        Nz = d->gNz;
+        allocateForMesh();
+        getMesh();
+        handlePeriodicStuff();
+        solveForJacobians();
+    }
+    void getMesh() {
+        vector<double> X, Y, Z;
+        double L = 0;
+        bool cube = spec.compare(0, 5, "cube:") == 0;
+        if (cube) {
+            L = atof(spec.c_str() + 5);
+        } else if (spec.compare(0, 5, "file:") == 0) {
+            size_t n = (size_t)Nx * Ny * Nz;
+            vector<double> all = read_bin(spec.substr(5), 3 * n);
+            X.assign(all.begin(), all.begin() + n);
+            Y.assign(all.begin() + n, all.begin() + 2 * n);
+            Z.assign(all.begin() + 2 * n, all.end());
+        } else {
+            die("bad mesh spec " + spec);
+        }
+        for (int i = 0; i < 3; i++) { x_min[i] = 1e300; x_max[i] = -1e300; }
+        FOR_Z_YPEN {
+            FOR_Y_YPEN {
+                FOR_X_YPEN {
+                    int ip = GETMAJIND_YPEN;
+                    int ii = GETGLOBALXIND_YPEN, jj = GETGLOBALYIND_YPEN, kk = GETGLOBALZIND_YPEN;
+                    size_t g = (size_t)ii + (size_t)Nx * (jj + (size_t)Ny * kk);
+                    if (cube) {
+                        x[ip] = L * d->x[ii];
+                        y[ip] = L * d->y[jj];
+                        z[ip] = L * d->z[kk];
+                    } else {
+                        x[ip] = X[g];
+                        y[ip] = Y[g];
+                        z[ip] = Z[g];
+                    }
+                    x_min[0] = fmin(x_min[0], x[ip]); x_max[0] = fmax(x_max[0], x[ip]);
+                    x_min[1] = fmin(x_min[1], y[ip]); x_max[1] = fmax(x_max[1], y[ip]);
+                    x_min[2] = fmin(x_min[2], z[ip]); x_max[2] = fmax(x_max[2], z[ip]);
+                }
+            }
+        }
+    }
+};
+
+struct Setup {
+    Options *opt;
+    TimeStepping *ts;
+    BC *bc;
+    Domain *d;
+    C2Decomp *c2d;
+};
+
+static Setup make_setup() {
+    Setup s;
+    s.opt = new Options(0);
+    s.ts = new TimeStepping(s.opt);
+    bool periodicBC[3];
+    s.bc = new BC(s.opt, periodicBC);
+    s.d = new Domain(s.opt, 1.0, 1.0, 1.0);
+    s.c2d = new C2Decomp(s.opt->Nx, s.opt->Ny, s.opt->Nz, s.opt->pRow, s.opt->pCol, periodicBC);
+    s.d->setPencilDecompInfo(s.c2d);
+    return s;
+}
+
+// global x-fastest <-> reference y-pencil "major" layout (i*Nz*Ny + k*Ny + j)
+static inline size_t ymaj(int i, int j, int k, int Ny, int Nz) { return (size_t)i * Nz * Ny + (size_t)k * Ny + j; }
+static inline size_t glob(int i, int j, int k, int Nx, int Ny) { return (size_t)i + (size_t)Nx * (j + (size_t)Ny * k); }
+
+static void write_fields(const string &path, const vector<double *> &fields, int Nx, int Ny, int Nz,
+                         const double *hdr, int nhdr) {
+    FILE *f = fopen(path.c_str(), "wb");
+    if (!f) die("cannot write " + path);
+    fwrite(hdr, sizeof(double), nhdr, f);
+    vector<double> buf((size_t)Nx * Ny * Nz);
+    for (double *fld : fields) {
+        for (int k = 0; k < Nz; k++)
+            for (int j = 0; j < Ny; j++)
+                for (int i = 0; i < Nx; i++) buf[glob(i, j, k, Nx, Ny)] = fld[ymaj(i, j, k, Ny, Nz)];
+        fwrite(buf.data(), sizeof(double), buf.size(), f);
+    }
+    fclose(f);
+}
+
+static int mode_run(const string &mesh, const string &icpath, const string &out) {
+    Setup s = make_setup();
+    int Nx = s.opt->Nx, Ny = s.opt->Ny, Nz = s.opt->Nz;
+    size_t n = (size_t)Nx * Ny * Nz;
+    CurvilinearCSolver *cs = new CurvilinearCSolver(s.c2d, s.d, s.bc, s.ts, s.opt);
+    // The reference allocates solver arrays with new[] and never clears them;
+    // the momentum update accumulates into rho{U,V,W}k2 (Core.cpp:839,872,904),
+    // so every array starts from zero here, as the GPU context does.
+    double *arrs[] = {cs->rhok, cs->rhok2, cs->rho2, cs->rhoUk, cs->rhoUk2, cs->rhoU2, cs->rhoVk, cs->rhoVk2,
+                      cs->rhoV2, cs->rhoWk, cs->rhoWk2, cs->rhoW2, cs->rhoEk, cs->rhoEk2, cs->rhoE2};
+    for (double *a : arrs) memset(a, 0, n * sizeof(double));
+    cs->msh = new HarnessMesh(s.c2d, cs, s.d, mesh);
+    AbstractRK *rk = nullptr;
+    if (s.opt->rkType == Options::TVDRK3) rk = new TVDRK3(cs);
+    else if (s.opt->rkType == Options::RK4) rk = new RK4(cs);
+    else if (s.opt->rkType == Options::KENRK4) rk = new KenRK4(cs);
+    else if (s.opt->rkType == Options::LSLDDRK4) rk = new LSLDDRK4(cs);
+    else die("unknown RK type");
+
+    vector<double> ic = read_bin(icpath, 5 * n);
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++) {
+                size_t g = glob(i, j, k, Nx, Ny), ip = ymaj(i, j, k, Ny, Nz);
+                cs->rho0[ip] = ic[g];
+                cs->U0[ip] = ic[n + g];
+                cs->V0[ip] = ic[2 * n + g];
+                cs->W0[ip] = ic[3 * n + g];
+                cs->p0[ip] = ic[4 * n + g];
+            }
+    cs->setInitialConditions();
+
+    double t0 = MPI_Wtime();
+    rk->executeSolverLoop();
+    double t1 = MPI_Wtime();
+    fprintf(stderr, "mc3d_ref: wall %.6f s for %d steps\n", t1 - t0, cs->timeStep);
+
+    double hdr[8] = {(double)cs->timeStep, cs->time, (double)Nx, (double)Ny, (double)Nz, s.ts->dt, t1 - t0, 0.0};
+    vector<double *> f = {cs->rho1, cs->rhoU1, cs->rhoV1, cs->rhoW1, cs->rhoE1};
+    write_fields(out, f, Nx, Ny, Nz, hdr, 8);
+    return 0;
+}
+
+static int mode_metrics(const string &mesh, const string &out) {
+    Setup s = make_setup();
+    int Nx = s.opt->Nx, Ny = s.opt->Ny, Nz = s.opt->Nz;
+    CurvilinearCSolver *cs = new CurvilinearCSolver(s.c2d, s.d, s.bc, s.ts, s.opt);
+    HarnessMesh *m = new HarnessMesh(s.c2d, cs, s.d, mesh);
+    double hdr[8] = {0, 0, (double)Nx, (double)Ny, (double)Nz, 0, 0, 0};
+    vector<double *> f = {m->J, m->J11, m->J12, m->J13, m->J21, m->J22, m->J23, m->J31, m->J32, m->J33};
+    write_fields(out, f, Nx, Ny, Nz, hdr, 8);
+    return 0;
+}
+
+// one operator on one field, in the pencil layout the reference uses for it
+static int mode_ops(const string &scheme, int dir, const string &in, const string &out) {
+    Setup s = make_setup();
+    int Nx = s.opt->Nx, Ny = s.opt->Ny, Nz = s.opt->Nz;
+    size_t n = (size_t)Nx * Ny * Nz;
+    vector<double> src = read_bin(in, n), pin(n), pout(n), dst(n);
+    AbstractDerivatives::Direct D = dir == 0 ? AbstractDerivatives::DIRX
+                                   : dir == 1 ? AbstractDerivatives::DIRY : AbstractDerivatives::DIRZ;
+    Options::BCType bct = dir == 0 ? s.bc->bcXType : dir == 1 ? s.bc->bcYType : s.bc->bcZType;
+    // pencil "major" index of (i,j,k) for the operator's direction
+    auto pidx = [&](int i, int j, int k) -> size_t {
+        if (dir == 0) return (size_t)k * Nx * Ny + (size_t)j * Nx + i;
+        if (dir == 1) return (size_t)i * Nz * Ny + (size_t)k * Ny + j;
+        return (size_t)j * Nx * Nz + (size_t)i * Nz + k;
+    };
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++) pin[pidx(i, j, k)] = src[glob(i, j, k, Nx, Ny)];
+    if (scheme == "PADE6" || scheme == "PENTA10" || scheme == "CD2") {
+        AbstractDerivatives *op;
+        if (scheme == "PADE6") op = new Pade6(s.d, bct, D);
+        else if (scheme == "PENTA10") op = new Penta10(s.d, bct, D);
+        else op = new CD2(s.d, bct, D);
+        op->calc1stDerivField(pin.data(), pout.data());
+    } else if (scheme == "COMPACT8" || scheme == "COMPACT10") {
+        AbstractFilter *op;
+        if (scheme == "COMPACT8") op = new Compact8Filter(s.opt->alphaF, s.d, s.bc, bct, D);
+        else op = new Compact10Filter(s.opt->alphaF, s.d, s.bc, bct, D);
+        op->filterField(pin.data(), pout.data());
+    } else {
+        die("unknown operator " + scheme);
+    }
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++) dst[glob(i, j, k, Nx, Ny)] = pout[pidx(i, j, k)];
+    FILE *f = fopen(out.c_str(), "wb");
+    if (!f) die("cannot write " + out);
+    fwrite(dst.data(), sizeof(double), n, f);
+    fclose(f);
+    return 0;
+}
+
+int main(int argc, char **argv) {
+    MPI_Init(&argc, &argv);
+    if (argc < 2) die("usage: mc3d_ref run|ops|metrics ...");
+    string mode = argv[1];
+    int rc = 2;
+    if (mode == "run" && argc == 5) rc = mode_run(argv[2], argv[3], argv[4]);
+    else if (mode == "ops" && argc == 6) rc = mode_ops(argv[2], atoi(argv[3]), argv[4], argv[5]);
+    else if (mode == "metrics" && argc == 4) rc = mode_metrics(argv[2], argv[3]);
+    else die("bad arguments");
+    MPI_Finalize();
+    return rc;
+}

@@ -1,0 +1,144 @@
+"""Runs the reference solver binary oracle/_ref/mc3d_ref (built by oracle/Makefile
+from the reference's own sources). TEST INFRASTRUCTURE ONLY: used by the golden
+fixture generator, the oracle's self-check tests and bench.py's reference arm.
+
+Fields cross the process boundary as FP64 arrays shaped (Nz, Ny, Nx).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(HERE, "_ref", "mc3d_ref")
+
+_BC = {0: "PERIODIC_SOLVE", 1: "DIRICHLET_SOLVE"}
+
+
+def available() -> bool:
+    return os.path.isfile(REF_BIN) and os.access(REF_BIN, os.X_OK)
+
+
+def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
+    """MPI_3DCompact.in for an oracle Config (keys of src/Options.hpp:133-206).
+    Periodic faces are translated by `box` along their own axis, as the HIT case
+    sets PERIODICDISPX_X = PERIODICDISPY_Y = PERIODICDISPZ_Z = 2*pi
+    (tests/hit/Samtaney_D4/MPI_3DCompact.in)."""
+    Nx, Ny, Nz = cfg.N
+    if kinds is None:
+        kinds = ["PERIODIC" if b == 0 else "ADIABATIC_WALL" for b in cfg.bc]
+    lines = [
+        "[TIMESTEPPING]",
+        f"TSTYPE = {cfg.ts_type}",
+        f"CFL = {cfg.cfl!r}",
+    ]
+    if cfg.ts_type == "CONST_DT":
+        lines.append(f"DT = {cfg.dt!r}")
+    lines += [
+        "MAXTIME = 1e30",
+        f"MAXTIMESTEP = {max_steps}",
+        f"FILTERSTEP = {cfg.filter_step}",
+        f"SUBSTEPFILTERING = {'true' if cfg.substep_filtering else 'false'}",
+        "CHECKSTEP = 1000000000",
+        "DUMPSTEP = 1000000000",
+        "[RESTART]",
+        "FROMRESTART = false",
+        "ONLYGRIDFROMRESTART = false",
+        "SPONGEAVGFROMRESTART = false",
+        "[STATS]",
+        "VELOCITYSTATS = false",
+        "THERMOSTATS = false",
+        "STATSAVGTYPE = NONE",
+        "[BC]",
+    ]
+    for ax, name in enumerate("XYZ"):
+        lines.append(f"BC{name}TYPE = {_BC[cfg.bc[ax]]}")
+        lines.append(f"BC{name}0 = {kinds[ax]}")
+        lines.append(f"BC{name}1 = {kinds[ax]}")
+        if kinds[ax] == "PERIODIC":
+            for c in "XYZ":
+                lines.append(f"PERIODICDISP{name}_{c} = {(box if c == name else 0.0)!r}")
+    lines += [
+        "[DOMAIN]",
+        f"NX = {Nx}",
+        f"NY = {Ny}",
+        f"NZ = {Nz}",
+        "[SOLVER]",
+        f"ALPHAF = {cfg.alphaF!r}",
+        f"MU_REF = {cfg.mu_ref!r}",
+        f"XFDTYPE = {cfg.fd[0]}",
+        f"YFDTYPE = {cfg.fd[1]}",
+        f"ZFDTYPE = {cfg.fd[2]}",
+        f"FILTERTYPE = {cfg.filter}",
+        f"RKTYPE = {cfg.rk}",
+        "[LES]",
+        f"LESMODEL = {cfg.les}",
+        f"LESAVERAGING = {cfg.les_avg}",
+    ]
+    return "\n".join(lines) + "\n"
+
+
+def _write(path, arrays):
+    with open(path, "wb") as f:
+        for a in arrays:
+            f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+
+
+def _read_fields(path, N, nf, header=8):
+    Nx, Ny, Nz = N
+    raw = np.fromfile(path, dtype=np.float64)
+    hdr = raw[:header]
+    n = Nx * Ny * Nz
+    fields = [raw[header + i * n: header + (i + 1) * n].reshape(Nz, Ny, Nx).copy() for i in range(nf)]
+    return hdr, fields
+
+
+def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600):
+    """Run the reference solver for `nsteps` time steps from primitive ICs
+    (rho, U, V, W, p). Returns (conserved fields, header dict)."""
+    if not available():
+        raise RuntimeError("oracle/_ref/mc3d_ref is not built (make -C oracle)")
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
+            f.write(ini_text(cfg, nsteps))
+        _write(os.path.join(d, "ic.bin"), ic)
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "run", mesh, "ic.bin", "out.bin"], cwd=d,
+                           capture_output=True, text=True, timeout=timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError("mc3d_ref failed: " + r.stderr[-2000:] + r.stdout[-2000:])
+        hdr, fields = _read_fields(os.path.join(d, "out.bin"), cfg.N, 5)
+    info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall}
+    return fields, info
+
+
+def run_metrics(cfg, mesh="cube:6.283185307179586"):
+    """J, J11..J33 as the reference's solveForJacobians computes them."""
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
+            f.write(ini_text(cfg, 1))
+        r = subprocess.run([REF_BIN, "metrics", mesh, "m.bin"], cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("mc3d_ref metrics failed: " + r.stderr[-2000:])
+        _, fields = _read_fields(os.path.join(d, "m.bin"), cfg.N, 10)
+    return fields
+
+
+def run_op(cfg, scheme, direction, field):
+    """One derivative (PADE6|PENTA10|CD2) or filter (COMPACT8|COMPACT10, alpha
+    = cfg.alphaF) along `direction` with the reference's own operator class."""
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
+            f.write(ini_text(cfg, 1))
+        _write(os.path.join(d, "in.bin"), [field])
+        r = subprocess.run([REF_BIN, "ops", scheme, str(direction), "in.bin", "out.bin"], cwd=d,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("mc3d_ref ops failed: " + r.stderr[-2000:])
+        Nx, Ny, Nz = cfg.N
+        return np.fromfile(os.path.join(d, "out.bin"), dtype=np.float64).reshape(Nz, Ny, Nx)
