@@ -1,0 +1,185 @@
+/*
+ * mc3d: B200-native CurvilinearCSolver time step (compact derivatives, compact
+ * filtering, SGS model and RK stage update) behind a plain C ABI.
+ *
+ * Conventions
+ *   - Every function returns an int status (MC3D_OK = 0) and never aborts the
+ *     process; mc3d_last_error() returns the calling thread's last message.
+ *   - Fields are 3-D arrays of Nx*Ny*Nz values in x-fastest order
+ *     (index i + Nx*(j + Ny*k)), the global order of the reference's dumps
+ *     (src/CurvilinearCSolver_Core.cpp:1333-1436).
+ *   - "device" pointers live on the solver's / operator's CUDA device; "host"
+ *     pointers are ordinary CPU memory.
+ *   - Directions: 0 = xi1 (x), 1 = xi2 (y), 2 = xi3 (z), as
+ *     AbstractDerivatives::Direct {DIRX, DIRY, DIRZ} (src/AbstractDerivatives.hpp:32).
+ *
+ * Reference interfaces each group replaces (paths within emathew1/MPI_3DCompact):
+ *   mc3d_deriv_*   AbstractDerivatives (src/AbstractDerivatives.hpp:13-54):
+ *                  calc1stDerivField(in, out) and calcNeumann(f); concrete
+ *                  Pade6 (src/Pade6.hpp:11), Penta10 (src/Penta10.hpp:7),
+ *                  CD2 (src/CD2.hpp).
+ *   mc3d_filter_*  AbstractFilter (src/AbstractFilter.hpp:13-35): filterField(in,
+ *                  out); Compact8Filter (src/Compact8Filter.hpp:9),
+ *                  Compact10Filter (src/Compact10Filter.hpp:9).
+ *   mc3d_solver_*  AbstractCSolver + CurvilinearCSolver (src/AbstractCSolver.hpp:14,
+ *                  src/CurvilinearCSolver.hpp:25) driven by an AbstractRK
+ *                  (src/AbstractRK.hpp:6): RK4, TVDRK3, KenRK4, LSLDDRK4, with
+ *                  the AbstractSGS models (src/AbstractSGS.hpp:10) NOMODEL and
+ *                  VREMAN.
+ *   mc3d_config_*  Options (src/Options.hpp:13-598): the MPI_3DCompact.in keys.
+ */
+#ifndef MC3D_H
+#define MC3D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MC3D_OK 0
+#define MC3D_ERR_CONFIG 1    /* invalid option or unsupported combination        */
+#define MC3D_ERR_CUDA 2      /* a CUDA runtime call failed                        */
+#define MC3D_ERR_NONFINITE 3 /* the state became NaN/Inf                          */
+#define MC3D_ERR_OOM 4       /* device allocation failed                          */
+#define MC3D_ERR_TIMEOUT 5   /* a bounded device wait gave up                     */
+#define MC3D_ERR_ARG 6       /* null handle / bad argument                        */
+
+/* ---- enumerations (values follow src/Options.hpp:19-37 where it has them) ---- */
+enum { MC3D_CONST_DT = 0, MC3D_CONST_CFL = 1 };                 /* TimeSteppingType */
+enum { MC3D_PERIODIC_SOLVE = 0, MC3D_DIRICHLET_SOLVE = 1 };     /* BCType           */
+enum { MC3D_CD2 = 0, MC3D_PADE6 = 1, MC3D_PENTA10 = 2 };        /* FDType           */
+enum { MC3D_COMPACT8 = 0, MC3D_COMPACT10 = 1 };                 /* FilterType       */
+enum { MC3D_NOMODEL = 0, MC3D_VREMAN = 1, MC3D_DSM = 2 };       /* LESModel         */
+enum { MC3D_AVG_NONE = 0, MC3D_AVG_XI1 = 1, MC3D_AVG_XI2 = 2, MC3D_AVG_XI3 = 3,
+       MC3D_AVG_LOCAL = 4, MC3D_AVG_GLOBAL = 5 };               /* StatsAvgType     */
+enum { MC3D_TVDRK3 = 0, MC3D_RK4 = 1, MC3D_KENRK4 = 2, MC3D_LSLDDRK4 = 3 }; /* RKType */
+/* BCKind (src/Options.hpp:21-27) */
+enum { MC3D_BC_PERIODIC = 0, MC3D_BC_INTERNALLY_PERIODIC = 1, MC3D_BC_SPONGE = 2,
+       MC3D_BC_ADIABATIC_WALL = 3, MC3D_BC_CONST_T_WALL = 4, MC3D_BC_MOVING_ADIABATIC_WALL = 5,
+       MC3D_BC_INLET = 6 };
+/* precision of the bulk arithmetic; metrics, LU factors, the conserved state,
+ * the RK registers and the time accumulators are FP64 in both */
+enum { MC3D_FP64 = 0, MC3D_FP32BULK = 1 };
+
+/* The options of the time step (src/Options.hpp:46-118 members). */
+typedef struct mc3d_config {
+    int Nx, Ny, Nz;
+    int bc_type[3];          /* BCType per direction                         */
+    int bc_kind[6];          /* BCKind for X0, X1, Y0, Y1, Z0, Z1             */
+    int fd_type[3];          /* FDType per direction                         */
+    int filter_type;         /* FilterType                                   */
+    double alphaF;           /* SOLVER.ALPHAF                                */
+    double mu_ref;           /* SOLVER.MU_REF                                */
+    int rk_type;             /* SOLVER.RKTYPE                                */
+    int ts_type;             /* TIMESTEPPING.TSTYPE                          */
+    double cfl;              /* TIMESTEPPING.CFL                             */
+    double dt;               /* TIMESTEPPING.DT                              */
+    int filter_step;         /* TIMESTEPPING.FILTERSTEP                      */
+    int substep_filtering;   /* TIMESTEPPING.SUBSTEPFILTERING                */
+    int max_time_step;       /* TIMESTEPPING.MAXTIMESTEP                     */
+    double max_time;         /* TIMESTEPPING.MAXTIME                         */
+    int les_model;           /* LES.LESMODEL                                 */
+    int les_averaging;       /* LES.LESAVERAGING                             */
+    int time_step0;          /* starting time step (restart)                 */
+    double time0;            /* starting time                                */
+    /* [GPU] section: keys the reference does not have */
+    int precision;           /* GPU.PRECISION = FP64 | FP32BULK              */
+    int reference_quirks;    /* GPU.REFERENCEQUIRKS (default 1): keep the
+                                reference's momentum k2 carry-over
+                                (src/CurvilinearCSolver_Core.cpp:839,872,904) */
+} mc3d_config;
+
+/* ---- configuration ---- */
+int mc3d_config_default(mc3d_config *cfg);
+/* Parse an MPI_3DCompact.in file: same sections, keys, enum strings, defaults
+ * and required keys as Options (src/Options.hpp:128-428, src/Options.cpp:3-312);
+ * LESMODEL also accepts NONE for NOMODEL. Unsupported but valid settings are
+ * reported as MC3D_ERR_CONFIG. */
+int mc3d_config_from_ini(const char *path, mc3d_config *cfg);
+
+/* ---- last error of the calling thread ---- */
+const char *mc3d_last_error(void);
+
+/* ---- compact-derivative and filter operators ---- */
+typedef struct mc3d_op_s *mc3d_op;
+
+/* Replaces `new Pade6/Penta10/CD2(Domain*, BCType, Direct)` (src/Pade6.hpp:39,
+ * src/Penta10.hpp:38, src/CD2.hpp:30). `dh` is the computational spacing
+ * (Domain::dx/dy/dz, src/Domain.hpp:45-79). precision: MC3D_FP64 -> fields are
+ * double, MC3D_FP32BULK -> fields are float. */
+int mc3d_deriv_create(int fd_type, int bc_type, int dir, int Nx, int Ny, int Nz, double dh,
+                      int precision, int device, mc3d_op *out);
+
+/* Replaces `new Compact8Filter/Compact10Filter(alphaF, Domain*, BC*, BCType,
+ * Direct)` (src/Compact8Filter.hpp:28, src/Compact10Filter.hpp:30).
+ * bc_types[3] are the BC types of all three directions: lines lying on a
+ * Dirichlet face of another direction pass through (src/Compact10Filter.cpp:166-252). */
+int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_types[3], int Nx, int Ny,
+                       int Nz, int precision, int device, mc3d_op *out);
+
+/* calc1stDerivField / filterField on `nfields` device fields at once:
+ * out[f] = op(in[f]). `stream` is a cudaStream_t (NULL = legacy default).
+ * in[f] and out[f] may not alias. */
+int mc3d_op_apply(mc3d_op op, const void *const *in, void *const *out, int nfields, void *stream);
+int mc3d_op_destroy(mc3d_op op);
+
+/* AbstractDerivatives::calcNeumann (src/Pade6.cpp:395-397, src/CD2.cpp:183):
+ * the wall value giving a zero normal derivative from f[1..5]. Host-side. */
+double mc3d_calc_neumann(int fd_type, const double *f);
+
+/* ---- solver: CurvilinearCSolver + AbstractRK on one GPU ---- */
+typedef struct mc3d_solver_s *mc3d_solver;
+
+int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out);
+int mc3d_solver_destroy(mc3d_solver s);
+
+/* Metrics J, J11, J12, J13, J21, J22, J23, J31, J32, J33 (host, FP64), as
+ * AbstractSingleBlockMesh::solveForJacobians produces them
+ * (src/AbstractSingleBlockMesh.cpp:23-1439). */
+int mc3d_solver_set_metrics(mc3d_solver s, const double *const metrics[10]);
+/* The uniform periodic box x = L*xi (the HIT mesh,
+ * tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156). */
+int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz);
+
+/* setInitialConditions from primitive fields (host, FP64): rho, U, V, W, p
+ * (src/CurvilinearCSolver_BC.cpp:3-59). */
+int mc3d_solver_set_initial(mc3d_solver s, const double *rho, const double *U, const double *V,
+                            const double *W, const double *p);
+/* Same from device FP64 primitive fields (no host copy). */
+int mc3d_solver_set_initial_device(mc3d_solver s, const double *rho, const double *U, const double *V,
+                                   const double *W, const double *p);
+
+/* Advance `nsteps` time steps (preStep .. postStep of AbstractRK::executeSolverLoop,
+ * e.g. src/RK4.hpp:127-178). For LSLDDRK4 the 5- and 6-stage halves alternate,
+ * one half per step. Asynchronous on the solver's stream. */
+int mc3d_solver_step(mc3d_solver s, int nsteps);
+
+/* Copy the conserved state rho1, rhoU1, rhoV1, rhoW1, rhoE1 (FP64) to host. */
+int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *rhoV, double *rhoW,
+                              double *rhoE);
+/* Device pointers (FP64) of the five conserved fields. */
+int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]);
+
+/* Time-step counter, time, last dt and total RK stages run (synchronises). */
+int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, long long *stages);
+
+/* Kinetic-energy and mass integrals sum(rho|u|^2/2), sum(rho) over the grid
+ * (FP64 device reduction, synchronises). */
+int mc3d_solver_integrals(mc3d_solver s, double *kinetic, double *mass);
+
+/* The cudaStream_t the solver launches on (for event timing). */
+int mc3d_solver_stream(mc3d_solver s, void **stream);
+/* Total number of kernels this solver has launched so far (launch accounting). */
+int mc3d_solver_launch_count(mc3d_solver s, long long *count);
+int mc3d_solver_sync(mc3d_solver s);
+
+/* ---- host utilities ---- */
+/* The combined-LCG shuffle generator of the reference's HIT IC generator
+ * (tests/hit/generate_init_hit.f90:16-81). state[0..2] = ix1..ix3 and
+ * table[0..96] = r(1..97) are updated in place; n values go to out. */
+int mc3d_hit_randvec(int *state, double *table, long long n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,262 @@
+"""mpi_3dcompact_b200: the CurvilinearCSolver time step of emathew1/MPI_3DCompact
+on one NVIDIA B200, behind the reference's operator interfaces.
+
+Host-side mirror of the reference classes over the C ABI (include/mc3d.h):
+
+  reference (emathew1/MPI_3DCompact)          here
+  ------------------------------------------  ------------------------------------
+  AbstractDerivatives / Pade6 / Penta10 / CD2  Pade6, Penta10, CD2 (.calc1stDerivField)
+  AbstractFilter / Compact8Filter / ...10      Compact8Filter, Compact10Filter (.filterField)
+  Options (MPI_3DCompact.in)                   Options.from_ini / Options(...)
+  CurvilinearCSolver + AbstractRK              CurvilinearCSolver (.step)
+  AbstractCSolver::calcNeumann                 calc_neumann
+
+Fields are CUDA torch tensors (or any object with .data_ptr()) shaped
+(Nz, Ny, Nx) = x-fastest, float64 for FP64 and float32 for FP32BULK operators.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import (AVG_LOCAL, AVG_NONE, CD2 as _CD2, COMPACT8, COMPACT10, CONST_CFL, CONST_DT, DIRICHLET_SOLVE,
+                      FP32BULK, FP64, KENRK4, LSLDDRK4, Mc3dError, NOMODEL, PADE6 as _PADE6, PENTA10 as _PENTA10,
+                      PERIODIC_SOLVE, RK4, TVDRK3, VREMAN)
+
+DIRX, DIRY, DIRZ = 0, 1, 2
+
+__all__ = ["Pade6", "Penta10", "CD2", "Compact8Filter", "Compact10Filter", "Options", "CurvilinearCSolver",
+           "calc_neumann", "Mc3dError", "DIRX", "DIRY", "DIRZ", "FP64", "FP32BULK", "PERIODIC_SOLVE",
+           "DIRICHLET_SOLVE"]
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class _Operator:
+    """Shared apply() of the derivative and filter operators."""
+
+    _h = None
+
+    def _apply(self, ins, outs, stream=None):
+        if len(ins) != len(outs):
+            raise ValueError("in/out field counts differ")
+        n = len(ins)
+        for t in list(ins) + list(outs):
+            if tuple(t.shape) != self.shape:
+                raise ValueError(f"field shape {tuple(t.shape)} != {self.shape}")
+            if not t.is_contiguous():
+                raise ValueError("fields must be contiguous")
+        a = (C.c_void_p * n)(*[t.data_ptr() for t in ins])
+        b = (C.c_void_p * n)(*[t.data_ptr() for t in outs])
+        st = C.c_void_p(stream) if stream is not None else None
+        N.check(N.host_lib().mc3d_op_apply(self._h, a, b, n, st))
+
+    def __del__(self):
+        if self._h:
+            try:
+                N.host_lib().mc3d_op_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class _Derivative(_Operator):
+    _fd = None
+
+    def __init__(self, shape, bc_type, direction, dh=None, precision=FP64, device=0):
+        """`shape` = (Nz, Ny, Nx). `dh` defaults to the unit-domain spacing of
+        Domain (1/N periodic, 1/(N-1) Dirichlet; src/Domain.hpp:45-79)."""
+        self.shape = tuple(shape)
+        nz, ny, nx = self.shape
+        n = (nx, ny, nz)[direction]
+        if dh is None:
+            dh = 1.0 / n if bc_type == PERIODIC_SOLVE else 1.0 / (n - 1.0)
+        self.direction, self.bc_type, self.dh, self.precision = direction, bc_type, dh, precision
+        h = C.c_void_p()
+        N.check(N.host_lib().mc3d_deriv_create(self._fd, bc_type, direction, nx, ny, nz, dh, precision, device,
+                                               C.byref(h)))
+        self._h = h
+
+    def calc1stDerivField(self, dataIn, dataOut, stream=None):
+        """AbstractDerivatives::calc1stDerivField (src/AbstractDerivatives.hpp:45)."""
+        self._apply([dataIn], [dataOut], stream)
+
+    def calc1stDerivFields(self, ins, outs, stream=None):
+        """Batched form: one launch for several fields."""
+        self._apply(ins, outs, stream)
+
+    def calcNeumann(self, f):
+        return calc_neumann(self._fd, f)
+
+
+class Pade6(_Derivative):
+    """Sixth-order tridiagonal compact first derivative (src/Pade6.hpp)."""
+    _fd = _PADE6
+
+
+class Penta10(_Derivative):
+    """Tenth-order pentadiagonal compact first derivative (src/Penta10.hpp)."""
+    _fd = _PENTA10
+
+
+class CD2(_Derivative):
+    """Explicit two-point difference exactly as src/CD2.cpp computes it."""
+    _fd = _CD2
+
+
+class _Filter(_Operator):
+    _ft = None
+
+    def __init__(self, alphaF, shape, bc_types, direction, precision=FP64, device=0):
+        self.shape = tuple(shape)
+        nz, ny, nx = self.shape
+        self.alphaF, self.direction, self.precision = alphaF, direction, precision
+        bcs = (C.c_int * 3)(*bc_types)
+        h = C.c_void_p()
+        N.check(N.host_lib().mc3d_filter_create(self._ft, alphaF, direction, bcs, nx, ny, nz, precision, device,
+                                                C.byref(h)))
+        self._h = h
+
+    def filterField(self, dataIn, dataOut, stream=None):
+        """AbstractFilter::filterField (src/AbstractFilter.hpp:33)."""
+        self._apply([dataIn], [dataOut], stream)
+
+    def filterFields(self, ins, outs, stream=None):
+        self._apply(ins, outs, stream)
+
+
+class Compact8Filter(_Filter):
+    """Eighth-order tridiagonal compact filter (src/Compact8Filter.hpp)."""
+    _ft = COMPACT8
+
+
+class Compact10Filter(_Filter):
+    """Tenth-order tridiagonal compact filter (src/Compact10Filter.hpp)."""
+    _ft = COMPACT10
+
+
+def calc_neumann(fd_type, f):
+    a = np.ascontiguousarray(np.asarray(f, dtype=np.float64))
+    return N.host_lib().mc3d_calc_neumann(fd_type, N.dptr(a))
+
+
+_FD = {"CD2": _CD2, "PADE6": _PADE6, "PENTA10": _PENTA10}
+_FILT = {"COMPACT8": COMPACT8, "COMPACT10": COMPACT10}
+_RK = {"TVDRK3": TVDRK3, "RK4": RK4, "KENRK4": KENRK4, "LSLDDRK4": LSLDDRK4}
+_LES = {"NOMODEL": NOMODEL, "NONE": NOMODEL, "VREMAN": VREMAN, "DSM": 2}
+_AVG = {"NONE": 0, "XI1_AVG": 1, "XI2_AVG": 2, "XI3_AVG": 3, "LOCAL": 4, "GLOBAL": 5}
+
+
+class Options:
+    """The MPI_3DCompact.in options of the time step (src/Options.hpp)."""
+
+    def __init__(self, grid=(64, 64, 64), fd="PADE6", filter="COMPACT10", alphaF=0.45, mu_ref=1e-3, rk="RK4",
+                 ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
+                 les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3):
+        c = N.Config()
+        N.check(N.host_lib().mc3d_config_default(C.byref(c)))
+        c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
+        fds = fd if isinstance(fd, (tuple, list)) else (fd, fd, fd)
+        for d in range(3):
+            c.fd_type[d] = _FD[fds[d]]
+            c.bc_type[d] = bc[d]
+        c.filter_type = _FILT[filter]
+        c.alphaF, c.mu_ref = alphaF, mu_ref
+        c.rk_type = _RK[rk]
+        c.ts_type = CONST_CFL if ts_type == "CONST_CFL" else CONST_DT
+        c.cfl, c.dt = cfl, dt
+        c.filter_step = filter_step
+        c.substep_filtering = int(bool(substep_filtering))
+        c.les_model = _LES[les]
+        c.les_averaging = _AVG[les_avg]
+        c.precision = precision
+        c.reference_quirks = int(bool(reference_quirks))
+        self.c = c
+
+    @classmethod
+    def from_ini(cls, path):
+        """Options(mpiRank) reading MPI_3DCompact.in (src/Options.hpp:121-428)."""
+        o = cls.__new__(cls)
+        o.c = N.Config()
+        N.check(N.host_lib().mc3d_config_from_ini(str(path).encode(), C.byref(o.c)))
+        return o
+
+    @property
+    def shape(self):
+        return (self.c.Nz, self.c.Ny, self.c.Nx)
+
+
+class CurvilinearCSolver:
+    """CurvilinearCSolver + its AbstractRK driver on one GPU
+    (src/CurvilinearCSolver.hpp:25-379, src/AbstractRK.hpp:6-17)."""
+
+    def __init__(self, opt: Options, device=0):
+        self.opt = opt
+        h = C.c_void_p()
+        N.check(N.host_lib().mc3d_solver_create(C.byref(opt.c), device, C.byref(h)))
+        self._h = h
+        self.shape = opt.shape
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                N.host_lib().mc3d_solver_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_box_metrics(self, L=2.0 * np.pi, Ly=None, Lz=None):
+        N.check(N.host_lib().mc3d_solver_set_box_metrics(self._h, L, Ly or L, Lz or L))
+
+    def set_metrics(self, metrics):
+        """J, J11..J33 (10 float64 arrays shaped (Nz, Ny, Nx))."""
+        arrs = [np.ascontiguousarray(m, dtype=np.float64) for m in metrics]
+        self._met_keep = arrs
+        p = (C.POINTER(C.c_double) * 10)(*[N.dptr(a) for a in arrs])
+        N.check(N.host_lib().mc3d_solver_set_metrics(self._h, p))
+
+    def set_initial_conditions(self, rho, U, V, W, p):
+        """setInitialConditions from primitive host arrays (src/CurvilinearCSolver_BC.cpp:3-59)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, U, V, W, p)]
+        N.check(N.host_lib().mc3d_solver_set_initial(self._h, *[N.dptr(a) for a in arrs]))
+
+    def step(self, n=1):
+        N.check(N.host_lib().mc3d_solver_step(self._h, int(n)))
+
+    def conserved(self):
+        """Host copies of rho1, rhoU1, rhoV1, rhoW1, rhoE1."""
+        out = [np.empty(self.shape) for _ in range(5)]
+        N.check(N.host_lib().mc3d_solver_get_conserved(self._h, *[N.dptr(a) for a in out]))
+        return out
+
+    def conserved_device_ptrs(self):
+        p = (C.c_void_p * 5)()
+        N.check(N.host_lib().mc3d_solver_conserved_device(self._h, p))
+        return [p[i] for i in range(5)]
+
+    def info(self):
+        ts, t, dt, st = C.c_int(), C.c_double(), C.c_double(), C.c_longlong()
+        N.check(N.host_lib().mc3d_solver_info(self._h, C.byref(ts), C.byref(t), C.byref(dt), C.byref(st)))
+        return {"time_step": ts.value, "time": t.value, "dt": dt.value, "stages": st.value}
+
+    def integrals(self):
+        ke, m = C.c_double(), C.c_double()
+        N.check(N.host_lib().mc3d_solver_integrals(self._h, C.byref(ke), C.byref(m)))
+        return ke.value, m.value
+
+    def stream(self):
+        s = C.c_void_p()
+        N.check(N.host_lib().mc3d_solver_stream(self._h, C.byref(s)))
+        return s.value
+
+    def launch_count(self):
+        c = C.c_longlong()
+        N.check(N.host_lib().mc3d_solver_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def sync(self):
+        N.check(N.host_lib().mc3d_solver_sync(self._h))

@@ -1,0 +1,428 @@
+// Host-side set-up of the compact operators: RHS stencils, boundary closures
+// and the LU factors of the (cyclic) banded left-hand sides, all in FP64.
+//
+// The factors are produced by the same elimination sequence the reference
+// runs on every call (src/Utils.cpp:4-191), once per operator instead of once
+// per line: the GPU line solve then only replays the RHS-dependent half.
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "mc3d_internal.h"
+
+namespace mc3d {
+
+namespace {
+
+// Thomas factorisation of src/Utils.cpp:4-20: work[] and the multipliers m[].
+void tri_factor(const std::vector<double> &a, const std::vector<double> &b, const std::vector<double> &c,
+                std::vector<double> &m, std::vector<double> &work) {
+    int n = (int)b.size();
+    work = b;
+    m.assign(n, 0.0);
+    for (int ip = 1; ip < n; ip++) {
+        m[ip] = a[ip] / work[ip - 1];
+        work[ip] = work[ip] - m[ip] * c[ip - 1];
+    }
+}
+
+// Full solveTri (src/Utils.cpp:4-20) for set-up vectors.
+std::vector<double> tri_solve(const std::vector<double> &a, const std::vector<double> &b,
+                              const std::vector<double> &c, const std::vector<double> &d) {
+    int n = (int)b.size();
+    std::vector<double> work = b, x = d;
+    for (int ip = 1; ip < n; ip++) {
+        double m = a[ip] / work[ip - 1];
+        work[ip] = work[ip] - m * c[ip - 1];
+        x[ip] = x[ip] - m * x[ip - 1];
+    }
+    x[n - 1] /= work[n - 1];
+    for (int ip = n - 2; ip >= 0; ip--) x[ip] = (x[ip] - c[ip] * x[ip + 1]) / work[ip];
+    return x;
+}
+
+// Matrix half of solvePenta (src/Utils.cpp:48-83): multipliers m1 (row ip,
+// column ip-1), m2 (row ip+1, column ip-1), mL, and the final C and D.
+struct PentaFactor {
+    std::vector<double> m1, m2, C, D;
+    double mL;
+};
+PentaFactor penta_factor(const std::vector<double> &e, const std::vector<double> &a, const std::vector<double> &d,
+                         const std::vector<double> &c, const std::vector<double> &f) {
+    int size = (int)d.size();
+    PentaFactor P;
+    std::vector<double> x = a, C = c, D = d;
+    P.m1.assign(size, 0.0);
+    P.m2.assign(size, 0.0);
+    for (int ip = 1; ip < size - 1; ip++) {
+        double xm = x[ip - 1] / D[ip - 1];
+        P.m1[ip] = xm;
+        D[ip] = D[ip] - xm * C[ip - 1];
+        C[ip] = C[ip] - xm * f[ip - 1];
+        xm = e[ip - 1] / D[ip - 1];
+        P.m2[ip] = xm;
+        x[ip] = x[ip] - xm * C[ip - 1];
+        D[ip + 1] = D[ip + 1] - xm * f[ip - 1];
+    }
+    P.mL = x[size - 2] / D[size - 2];
+    D[size - 1] = D[size - 1] - P.mL * C[size - 2];
+    P.C = C;
+    P.D = D;
+    return P;
+}
+
+// Full solvePenta for set-up vectors (same arithmetic order as the reference).
+std::vector<double> penta_solve(const std::vector<double> &e, const std::vector<double> &a,
+                                const std::vector<double> &d, const std::vector<double> &c,
+                                const std::vector<double> &f, const std::vector<double> &b) {
+    int size = (int)d.size();
+    std::vector<double> x = a, B = b, C = c, D = d;
+    for (int ip = 1; ip < size - 1; ip++) {
+        double xm = x[ip - 1] / D[ip - 1];
+        D[ip] = D[ip] - xm * C[ip - 1];
+        C[ip] = C[ip] - xm * f[ip - 1];
+        B[ip] = B[ip] - xm * B[ip - 1];
+        xm = e[ip - 1] / D[ip - 1];
+        x[ip] = x[ip] - xm * C[ip - 1];
+        D[ip + 1] = D[ip + 1] - xm * f[ip - 1];
+        B[ip + 1] = B[ip + 1] - xm * B[ip - 1];
+    }
+    double xm = x[size - 2] / D[size - 2];
+    D[size - 1] = D[size - 1] - xm * C[size - 2];
+    std::vector<double> out(size);
+    out[size - 1] = (B[size - 1] - xm * B[size - 2]) / D[size - 1];
+    out[size - 2] = (B[size - 2] - C[size - 2] * out[size - 1]) / D[size - 2];
+    for (int ip = size - 3; ip >= 0; ip--)
+        out[ip] = (B[ip] - f[ip] * out[ip + 2] - C[ip] * out[ip + 1]) / D[ip];
+    return out;
+}
+
+double minor3(const double m[16], int r0, int r1, int r2, int c0, int c1, int c2) {
+    return m[4 * r0 + c0] * (m[4 * r1 + c1] * m[4 * r2 + c2] - m[4 * r2 + c1] * m[4 * r1 + c2]) -
+           m[4 * r0 + c1] * (m[4 * r1 + c0] * m[4 * r2 + c2] - m[4 * r2 + c0] * m[4 * r1 + c2]) +
+           m[4 * r0 + c2] * (m[4 * r1 + c0] * m[4 * r2 + c1] - m[4 * r2 + c0] * m[4 * r1 + c1]);
+}
+
+// 4x4 inverse by adjugate over determinant (the method of src/Utils.cpp:193-224).
+void inverse4(const double m[16], double inv[16]) {
+    const int R[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            // cofactor of element (j, i), transposed into inv[i][j]
+            double mn = minor3(m, R[j][0], R[j][1], R[j][2], R[i][0], R[i][1], R[i][2]);
+            inv[4 * i + j] = ((i + j) % 2 ? -mn : mn);
+        }
+    double det = m[0] * minor3(m, 1, 2, 3, 1, 2, 3) - m[1] * minor3(m, 1, 2, 3, 0, 2, 3) +
+                 m[2] * minor3(m, 1, 2, 3, 0, 1, 3) - m[3] * minor3(m, 1, 2, 3, 0, 1, 2);
+    double id = 1.0 / det;
+    for (int i = 0; i < 16; i++) inv[i] *= id;
+}
+
+// Packed factor layout (LineOpHost::arr), N values per array:
+//   tri:   [m | rw | c | z]          (z only for the cyclic kind)
+//   penta: [m1 | m2 | rD | C | f | z0 | z1 | z2 | z3]  (z* only cyclic)
+void pack_tri(LineOpHost &op, const std::vector<double> &a, const std::vector<double> &b,
+              const std::vector<double> &c, bool cyclic, double alpha, double beta) {
+    int n = op.N;
+    std::vector<double> bb = b;
+    double gamma = 0;
+    if (cyclic) {   // src/Utils.cpp:22-46
+        gamma = -b[0];
+        bb[0] = b[0] - gamma;
+        bb[n - 1] = b[n - 1] - alpha * beta / gamma;
+    }
+    std::vector<double> m, work;
+    tri_factor(a, bb, c, m, work);
+    op.arr.assign(4 * n, 0.0);
+    for (int i = 0; i < n; i++) {
+        op.arr[i] = m[i];
+        op.arr[n + i] = 1.0 / work[i];
+        op.arr[2 * n + i] = c[i];
+    }
+    if (cyclic) {
+        std::vector<double> u(n, 0.0);
+        u[0] = gamma;
+        u[n - 1] = alpha;
+        std::vector<double> z = tri_solve(a, bb, c, u);
+        for (int i = 0; i < n; i++) op.arr[3 * n + i] = z[i];
+        op.sc[0] = beta;
+        op.sc[1] = 1.0 / gamma;
+        op.sc[2] = 1.0 / (1.0 + z[0] + beta * z[n - 1] / gamma);
+    }
+}
+
+void pack_penta(LineOpHost &op, const std::vector<double> &lo2, const std::vector<double> &lo,
+                const std::vector<double> &dg, const std::vector<double> &up, const std::vector<double> &up2,
+                bool cyclic, const double cp[6]) {
+    int n = op.N;
+    PentaFactor P = penta_factor(lo2, lo, dg, up, up2);
+    op.arr.assign(9 * n, 0.0);
+    for (int i = 0; i < n; i++) {
+        op.arr[i] = P.m1[i];
+        op.arr[n + i] = P.m2[i];
+        op.arr[2 * n + i] = 1.0 / P.D[i];
+        op.arr[3 * n + i] = P.C[i];
+        op.arr[4 * n + i] = up2[i];
+    }
+    op.arr[n - 1] = P.mL;   // row N-1 uses mL in place of m1
+    if (cyclic) {           // Woodbury set-up of src/Utils.cpp:85-157
+        std::vector<std::vector<double> > Z(4), V(4, std::vector<double>(n, 0.0));
+        int upos[4] = {0, 1, n - 2, n - 1};
+        for (int j = 0; j < 4; j++) {
+            std::vector<double> u(n, 0.0);
+            u[upos[j]] = 1.0;
+            Z[j] = penta_solve(lo2, lo, dg, up, up2, u);
+        }
+        V[0][n - 2] = cp[0];
+        V[0][n - 1] = cp[1];
+        V[1][n - 1] = cp[2];
+        V[2][0] = cp[3];
+        V[3][0] = cp[4];
+        V[3][1] = cp[5];
+        double Pm[16];
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+                double s = 0.0;
+                for (int k = 0; k < n; k++) s += V[i][k] * Z[j][k];
+                Pm[4 * i + j] = s + (i == j ? 1.0 : 0.0);
+            }
+        inverse4(Pm, op.Hm);
+        for (int j = 0; j < 4; j++)
+            for (int i = 0; i < n; i++) op.arr[(5 + j) * n + i] = Z[j][i];
+        for (int i = 0; i < 6; i++) op.cp[i] = cp[i];
+    }
+}
+
+}  // namespace
+
+LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh) {
+    if (N <= 10) throw std::runtime_error("line length must be greater than 10 (src/Options.cpp:241-244)");
+    LineOpHost op;
+    op.N = N;
+    op.deriv = true;
+    op.inv_dh = 1.0 / dh;
+    bool per = bc_type == MC3D_PERIODIC_SOLVE;
+    if (fd_type == MC3D_PADE6) {
+        // src/Pade6.hpp:70-75 interior, :78-137 boundary scheme 1, :183-215 bands
+        double alpha = 1.0 / 3.0, a = 14.0 / 9.0, b = 1.0 / 9.0;
+        op.H = 2;
+        op.st[0] = -b / 4.0;
+        op.st[1] = -a / 2.0;
+        op.st[3] = a / 2.0;
+        op.st[4] = b / 4.0;
+        std::vector<double> lo(N, alpha), up(N, alpha), dg(N, 1.0);
+        if (per) {
+            op.kind = K_TRI_PER;
+            pack_tri(op, lo, dg, up, true, alpha, alpha);
+        } else {
+            op.kind = K_TRI_DIR;
+            double alpha11 = 2.0, alpha21 = 1.0 / 6.0, alpha22 = 1.0 / 2.0;
+            up[0] = alpha11; up[1] = alpha22; lo[1] = alpha21;
+            lo[N - 1] = alpha11; lo[N - 2] = alpha22; up[N - 2] = alpha21;
+            double a1 = -5.0 / 2.0, b1 = 2.0, c1 = 1.0 / 2.0;
+            double a2 = -5.0 / 9.0, b2 = -1.0 / 2.0, c2 = 1.0, d2 = 1.0 / 18.0;
+            op.bw = 6;
+            op.head = {a1, b1, c1, 0.0, 0.0, 0.0, a2, b2, c2, d2, 0.0, 0.0};
+            // rows N-1 and N-2 are the mirrored, negated closures (src/Pade6.cpp:306-310)
+            op.tail = {0.0, 0.0, 0.0, -c1, -b1, -a1,    // row N-1 on phi[N-6..N-1]
+                       0.0, 0.0, -d2, -c2, -b2, -a2};  // row N-2
+            pack_tri(op, lo, dg, up, false, 0, 0);
+        }
+    } else if (fd_type == MC3D_PENTA10) {
+        // src/Penta10.hpp:68-175
+        double beta = 1.0 / 20.0, alpha = 1.0 / 2.0, a = 17.0 / 12.0, b = 101.0 / 150.0, c = 1.0 / 100.0;
+        op.H = 3;
+        op.st[0] = -c / 6.0; op.st[1] = -b / 4.0; op.st[2] = -a / 2.0;
+        op.st[4] = a / 2.0;  op.st[5] = b / 4.0;  op.st[6] = c / 6.0;
+        std::vector<double> dg(N, 1.0), lo(N, alpha), up(N, alpha), lo2(N, beta), up2(N, beta);
+        if (per) {
+            op.kind = K_PEN_PER;
+            double cp[6] = {beta, alpha, beta, beta, alpha, beta};
+            pack_penta(op, lo2, lo, dg, up, up2, true, cp);
+        } else {
+            op.kind = K_PEN_DIR;
+            double beta1 = 0.0, alpha1 = 5.0;
+            double beta2 = 0.0, alpha2_1 = 1.0 / 12.0, alpha2_2 = 5.0 / 4.0;
+            double beta3_1 = 1.0 / 36.0, beta3_2 = 1.0 / 36.0, alpha3_1 = 4.0 / 9.0, alpha3_2 = 4.0 / 9.0;
+            up[0] = alpha1; up[1] = alpha2_2; up[2] = alpha3_2;
+            lo[0] = alpha2_1; lo[1] = alpha3_1;
+            up2[0] = beta1; up2[1] = beta2; up2[2] = beta3_2;
+            lo2[0] = beta3_1;
+            up[N - 2] = alpha2_1; up[N - 3] = alpha3_1;
+            lo[N - 2] = alpha1; lo[N - 3] = alpha2_2; lo[N - 4] = alpha3_2;
+            up2[N - 3] = beta3_1;
+            lo2[N - 3] = beta1; lo2[N - 4] = beta2; lo2[N - 5] = beta3_2;
+            double r1[9] = {-197.0 / 60.0, -5.0 / 12.0, 5.0, -5.0 / 3.0, 5.0 / 12.0, -1.0 / 20.0, 0, 0, 0};
+            double r2[9] = {-79.0 / 240.0, -77.0 / 60.0, 55.0 / 48.0, 5.0 / 9.0, -5.0 / 48.0, 1.0 / 60.0,
+                            -1.0 / 720.0, 0.0, 0.0};
+            double r3[9] = {-25.0 / 54.0 / 4.0, -40.0 / 27.0 / 2.0, 0.0, 40.0 / 27.0 / 2.0, 25.0 / 54.0 / 4.0,
+                            0.0, 0.0, 0.0, 0.0};
+            op.bw = 9;
+            op.head.assign(3 * 9, 0.0);
+            op.tail.assign(3 * 9, 0.0);
+            const double *rows[3] = {r1, r2, r3};
+            for (int r = 0; r < 3; r++)
+                for (int k = 0; k < 9; k++) {
+                    op.head[r * 9 + k] = rows[r][k];
+                    // row N-1-r on phi[N-9..N-1]: coefficient of phi[N-1-k] is -rows[r][k]
+                    op.tail[r * 9 + (8 - k)] = -rows[r][k];
+                }
+            double cp[6] = {0, 0, 0, 0, 0, 0};
+            pack_penta(op, lo2, lo, dg, up, up2, false, cp);
+        }
+    } else if (fd_type == MC3D_CD2) {
+        // src/CD2.hpp:56-63 and src/CD2.cpp:129-183: interior row is
+        // (a*phi[i+1] + c*phi[i-1])/h with a = -1/2, c = 1/2 (sign as the reference)
+        op.H = 1;
+        op.st[0] = 0.5;
+        op.st[2] = -0.5;
+        if (per) {
+            op.kind = K_EXPL_PER;
+        } else {
+            op.kind = K_EXPL_DIR;
+            op.bw = 3;
+            op.head = {-1.5, 2.0, -0.5};
+            op.tail = {-0.5, 2.0, -1.5};   // (aa*phi[N-1] + bb*phi[N-2] + cc*phi[N-3])
+        }
+    } else {
+        throw std::runtime_error("unknown derivative type");
+    }
+    return op;
+}
+
+LineOpHost build_filter_op(int filter_type, double af, int bc_type, int N) {
+    if (N <= 10) throw std::runtime_error("line length must be greater than 10 (src/Options.cpp:241-244)");
+    LineOpHost op;
+    op.N = N;
+    op.deriv = false;
+    op.inv_dh = 1.0;
+    bool per = bc_type == MC3D_PERIODIC_SOLVE;
+    std::vector<double> a;
+    std::vector<std::vector<double> > fb;
+    if (filter_type == MC3D_COMPACT10) {
+        // src/Compact10Filter.hpp:58-134 (boundary scheme 1)
+        a = {(193.0 + 126.0 * af) / 256.0, (105.0 + 302.0 * af) / 256.0, (-15.0 + 30.0 * af) / 64.0,
+             (45.0 - 90.0 * af) / 512.0, (-5.0 + 10.0 * af) / 256.0, (1.0 - 2.0 * af) / 512.0};
+        fb = {{(1.0 + 1022.0 * af) / 1024.0, (507.0 + 10.0 * af) / 512.0, (45.0 + 934.0 * af) / 1024.0,
+               (-15.0 + 30.0 * af) / 128.0, (105.0 - 210.0 * af) / 512.0, (-63.0 + 126.0 * af) / 256.0,
+               (105.0 - 210.0 * af) / 512.0, (-15.0 + 30.0 * af) / 128.0, (45.0 - 90.0 * af) / 1024.0,
+               (-5.0 + 10.0 * af) / 512.0, (1.0 - 2.0 * af) / 1024.0},
+              {(-1.0 + 2.0 * af) / 1024.0, (5.0 + 502.0 * af) / 512.0, (979.0 + 90.0 * af) / 1024.0,
+               (15.0 + 98.0 * af) / 128.0, (-105.0 + 210.0 * af) / 512.0, (63.0 - 126.0 * af) / 256.0,
+               (-105.0 + 210.0 * af) / 512.0, (15.0 - 30.0 * af) / 128.0, (-45.0 + 90.0 * af) / 1024.0,
+               (5.0 - 10.0 * af) / 512.0, (-1.0 + 2.0 * af) / 1024.0},
+              {(1.0 - 2.0 * af) / 1024.0, (-5.0 + 10.0 * af) / 512.0, (45.0 + 934.0 * af) / 1024.0,
+               (113.0 + 30.0 * af) / 128.0, (105.0 + 302.0 * af) / 512.0, (-63.0 + 126.0 * af) / 256.0,
+               (105.0 - 210.0 * af) / 512.0, (-15.0 + 30.0 * af) / 128.0, (45.0 - 90.0 * af) / 1024.0,
+               (-5.0 + 10.0 * af) / 512.0, (1.0 - 2.0 * af) / 1024.0},
+              {(-1.0 + 2.0 * af) / 1024.0, (5.0 - 10.0 * af) / 512.0, (-45.0 + 90.0 * af) / 1024.0,
+               (15.0 + 98.0 * af) / 128.0, (407.0 + 210.0 * af) / 512.0, (63.0 + 130.0 * af) / 256.0,
+               (-105.0 + 210.0 * af) / 512.0, (15.0 - 30.0 * af) / 128.0, (-45.0 + 90.0 * af) / 1024.0,
+               (5.0 - 10.0 * af) / 512.0, (-1.0 + 2.0 * af) / 1024.0}};
+    } else if (filter_type == MC3D_COMPACT8) {
+        // src/Compact8Filter.hpp:55-94
+        a = {(93.0 + 70.0 * af) / 128.0, (7.0 + 18.0 * af) / 16.0, (-7.0 + 14.0 * af) / 32.0,
+             (1.0 - 2.0 * af) / 16.0, (-1.0 + 2.0 * af) / 128.0};
+        fb = {{1.0 / 256.0 + 127.0 * af / 128.0, 31.0 / 32.0 + 1.0 * af / 16.0, 7.0 / 64.0 + 25.0 * af / 32.0,
+               -7.0 / 32.0 + 7.0 * af / 16.0, 7.0 * (5.0 - 10.0 * af) / 128.0, -7.0 / 32.0 + 7.0 * af / 16.0,
+               7.0 / 64.0 - 7.0 * af / 32.0, -1.0 / 32.0 + 1.0 * af / 16.0, 1.0 / 256.0 - 1.0 * af / 128.0},
+              {-1.0 / 256.0 + 1.0 * af / 128.0, 1.0 / 32.0 + 15.0 * af / 16.0, 57.0 / 64.0 + 7.0 * af / 32.0,
+               7.0 / 32.0 + 9.0 * af / 16.0, 7.0 * (-5.0 + 10.0 * af) / 128.0, 7.0 / 32.0 - 7.0 * af / 16.0,
+               -7.0 / 64.0 + 7.0 * af / 32.0, 1.0 / 32.0 - 1.0 * af / 16.0, -1.0 / 256.0 + 1.0 * af / 128.0},
+              {1.0 / 256.0 - 1.0 * af / 128.0, -1.0 / 32.0 + 1.0 * af / 16.0, 7.0 / 64.0 + 25.0 * af / 32.0,
+               25.0 / 32.0 + 7.0 * af / 16.0, 35.0 / 128.0 + 29.0 * af / 64.0, -7.0 / 32.0 + 7.0 * af / 16.0,
+               7.0 / 64.0 - 7.0 * af / 32.0, -1.0 / 32.0 + 1.0 * af / 16.0, 1.0 / 256.0 - 1.0 * af / 128.0}};
+    } else {
+        throw std::runtime_error("unknown filter type");
+    }
+    int H = (int)a.size() - 1;
+    op.H = H;
+    // symmetric interior stencil (src/Compact10Filter.cpp:5-75): cc0 = a0, cck = ak/2
+    for (int k = -H; k <= H; k++) op.st[k + H] = (k == 0) ? a[0] : a[k < 0 ? -k : k] / 2.0;
+    std::vector<double> lo(N, af), up(N, af), dg(N, 1.0);
+    if (per) {
+        op.kind = K_TRI_PER;
+        pack_tri(op, lo, dg, up, true, af, af);
+    } else {
+        op.kind = K_TRI_DIR;
+        lo[0] = up[0] = lo[N - 1] = up[N - 1] = 0.0;
+        int bw = (int)fb[0].size();
+        op.bw = bw;
+        op.head.assign(H * bw, 0.0);
+        op.tail.assign(H * bw, 0.0);
+        op.head[0] = 1.0;                  // RHSvec[0] = phi[0]
+        op.tail[bw - 1] = 1.0;             // RHSvec[N-1] = phi[N-1]
+        for (int r = 1; r < H; r++)
+            for (int k = 0; k < bw; k++) {
+                op.head[r * bw + k] = fb[r - 1][k];
+                op.tail[r * bw + (bw - 1 - k)] = fb[r - 1][k];   // mirrored on phi[N-1-k]
+            }
+        pack_tri(op, lo, dg, up, false, 0, 0);
+    }
+    return op;
+}
+
+namespace {
+template <typename R>
+void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
+    d.N = h.N;
+    d.kind = h.kind;
+    d.H = h.H;
+    d.bw = h.bw;
+    d.inv_dh = (R)h.inv_dh;
+    for (int i = 0; i < 11; i++) d.st[i] = (R)h.st[i];
+    for (int i = 0; i < 4; i++) d.sc[i] = (R)h.sc[i];
+    for (int i = 0; i < 16; i++) d.Hm[i] = (R)h.Hm[i];
+    for (int i = 0; i < 6; i++) d.cp[i] = (R)h.cp[i];
+    const R *p = (const R *)base;
+    size_t n = h.N;
+    size_t na = h.arr.size() / n;
+    d.a0 = na > 0 ? p : nullptr;
+    d.a1 = na > 1 ? p + n : nullptr;
+    d.a2 = na > 2 ? p + 2 * n : nullptr;
+    d.a3 = na > 3 ? p + 3 * n : nullptr;
+    d.a4 = na > 4 ? p + 4 * n : nullptr;
+    d.z0 = na > 5 ? p + 5 * n : nullptr;
+    d.z1 = na > 6 ? p + 6 * n : nullptr;
+    d.z2 = na > 7 ? p + 7 * n : nullptr;
+    d.z3 = na > 8 ? p + 8 * n : nullptr;
+    const R *q = p + h.arr.size();
+    d.head = h.head.empty() ? nullptr : q;
+    d.tail = h.tail.empty() ? nullptr : q + h.head.size();
+}
+
+template <typename R>
+std::vector<R> flatten(const LineOpHost &h) {
+    std::vector<R> v;
+    v.reserve(h.arr.size() + h.head.size() + h.tail.size());
+    for (double x : h.arr) v.push_back((R)x);
+    for (double x : h.head) v.push_back((R)x);
+    for (double x : h.tail) v.push_back((R)x);
+    if (v.empty()) v.push_back((R)0);
+    return v;
+}
+}  // namespace
+
+int upload_line_op(const LineOpHost &h, int precision, LineOpBuf &out) {
+    out.precision = precision;
+    MC3D_CUDA_TRY(cudaGetDevice(&out.device));
+    if (precision == MC3D_FP64) {
+        std::vector<double> v = flatten<double>(h);
+        MC3D_CUDA_TRY(cudaMalloc(&out.dev, v.size() * sizeof(double)));
+        MC3D_CUDA_TRY(cudaMemcpy(out.dev, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        fill_dev<double>(h, (const char *)out.dev, out.f64);
+    } else {
+        std::vector<float> v = flatten<float>(h);
+        MC3D_CUDA_TRY(cudaMalloc(&out.dev, v.size() * sizeof(float)));
+        MC3D_CUDA_TRY(cudaMemcpy(out.dev, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+        fill_dev<float>(h, (const char *)out.dev, out.f32);
+    }
+    return MC3D_OK;
+}
+
+void free_line_op(LineOpBuf &b) {
+    if (b.dev) cudaFree(b.dev);
+    b.dev = nullptr;
+}
+
+}  // namespace mc3d

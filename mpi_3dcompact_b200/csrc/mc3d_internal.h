@@ -1,0 +1,177 @@
+// Internal declarations shared by the host and device translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mc3d.h"
+
+namespace mc3d {
+
+// ---- error plumbing ----------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+#define MC3D_CUDA_TRY(expr)                                                                      \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return ::mc3d::fail(_e == cudaErrorMemoryAllocation ? MC3D_ERR_OOM : MC3D_ERR_CUDA,  \
+                                std::string(#expr) + ": " + cudaGetErrorString(_e));            \
+    } while (0)
+
+// ---- one compact operator along one direction ---------------------------
+// Line kinds: periodic kinds are even.
+enum LineKind { K_EXPL_PER = 0, K_EXPL_DIR = 1, K_TRI_PER = 2, K_TRI_DIR = 3, K_PEN_PER = 4, K_PEN_DIR = 5 };
+
+// Host-side description, all factors in FP64 (computed with the reference's
+// own elimination order so the GPU reproduces its factors exactly).
+struct LineOpHost {
+    int N = 0;
+    int kind = 0;
+    int H = 0;            // interior stencil half-width == boundary rows per end
+    int bw = 0;           // boundary row width (Dirichlet)
+    bool deriv = false;   // multiply the RHS by 1/dh
+    double inv_dh = 1.0;
+    double st[11] = {0};  // interior stencil, st[k] multiplies phi[n + k - H]
+    std::vector<double> head, tail;   // [H][bw]: rows 0..H-1 on phi[0..bw-1];
+                                      // row N-1-r on phi[N-bw..N-1] (ascending)
+    // packed factor arrays (see pack layout in coeffs.cpp)
+    std::vector<double> arr;
+    double sc[4] = {0};   // kind-specific scalars
+    double Hm[16] = {0};  // penta cyclic capacitance inverse
+    double cp[6] = {0};   // penta cyclic corner values
+};
+
+LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh);
+LineOpHost build_filter_op(int filter_type, double alphaF, int bc_type, int N);
+
+// Device-side view (trivially copyable, passed by value to kernels).
+template <typename R>
+struct LineOpDev {
+    int N, kind, H, bw;
+    R inv_dh;
+    R st[11];
+    R sc[4];
+    R Hm[16];
+    R cp[6];
+    const R *head;   // [H][bw]
+    const R *tail;   // [H][bw]
+    const R *a0;     // tri: m | penta: m1 (m1[N-1] = mL)
+    const R *a1;     // tri: rw | penta: m2
+    const R *a2;     // tri: c  | penta: rD
+    const R *a3;     // tri: z  | penta: C
+    const R *a4;     // penta: f
+    const R *z0, *z1, *z2, *z3;   // penta cyclic Woodbury columns
+};
+
+// Device copy of an operator in one precision.
+struct LineOpBuf {
+    void *dev = nullptr;          // single allocation holding every array
+    LineOpDev<float> f32{};
+    LineOpDev<double> f64{};
+    int precision = MC3D_FP64;
+    int device = 0;
+};
+int upload_line_op(const LineOpHost &h, int precision, LineOpBuf &out);
+void free_line_op(LineOpBuf &b);
+
+// ---- sweep launch ---------------------------------------------------------
+enum EpiMode {
+    EPI_STORE = 0,      // out[f] = v
+    EPI_STORE_NEG = 1,  // out[f] = -v
+    EPI_SUB = 2,        // out[f] -= v
+    EPI_RHS_FINAL = 3,  // k2 assembly of solveContinuity..solveEnergy
+    EPI_STORE_F64 = 4,  // out64[f] = (double)v
+};
+
+struct Grid3 {
+    int Nx, Ny, Nz;
+    __host__ __device__ long long n() const { return (long long)Nx * Ny * Nz; }
+};
+
+// Extra inputs of the k2 assembly epilogue (RHS_FINAL).
+template <typename R>
+struct RhsFinalArgs {
+    const double *dt;        // device scalar (FP64 time accumulator)
+    const R *J;              // metric Jacobian field or nullptr (constant)
+    R Jc;                    // constant J when J == nullptr
+    int quirk;               // momentum k2 carry-over
+};
+
+template <typename R>
+struct SweepBatch {
+    int nf;
+    const R *in[16];
+    R *out[16];            // EPI_STORE/NEG/SUB target, or the k2 arrays for RHS_FINAL
+    const R *aux[16];      // RHS_FINAL: partial RHS arrays
+    double *out64[16];     // EPI_STORE_F64 targets
+    int eq[16];            // RHS_FINAL: equation index 0..4 of field f
+};
+
+template <typename R>
+int launch_sweep(int dir, const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
+                 const RhsFinalArgs<R> &rf, const int bc_types[3], bool filter_passthrough,
+                 cudaStream_t st);
+
+// ---- pointwise kernels ----------------------------------------------------
+template <typename R>
+struct Metrics {
+    const R *m[10];          // J, J11..J33 (nullptr when constant)
+    R c[10];                 // constants
+    bool constant;
+};
+
+struct FluxParams {
+    double mu_ref;
+    double dxi[3];
+    int les;                 // 0 none, 1 Vreman inline, 2 mu_sgs field
+    double pr_t;
+};
+
+template <typename R>
+int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[4], cudaStream_t st);
+
+template <typename R>
+int launch_flux(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+                const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st);
+
+template <typename R>
+int launch_vreman(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+                  const FluxParams &p, R *mu_sgs, cudaStream_t st);
+
+// RK register update for one stage: see rk.cu for the per-scheme formulas.
+struct RkStage {
+    int scheme;        // MC3D_* RK type
+    int stage;         // 1-based
+    int nstages;
+    double a, b;       // scheme coefficients of this stage
+};
+template <typename R>
+int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
+                     double *const qk[5], double *const q2[5], cudaStream_t st);
+
+template <typename R>
+int launch_to_real(const Grid3 &g, const double *const src[5], R *const dst[5], cudaStream_t st);
+
+// CFL: max over points of J11(|U|+c)/dxi + J22(|V|+c)/deta + J33(|W|+c)/dzeta into *umax
+// (FP64, non-negative values compared as integers with atomicMax).
+template <typename R>
+int launch_cfl(const Grid3 &g, const double *const q[5], const Metrics<R> &m, const double dxi[3],
+               unsigned long long *umax, cudaStream_t st);
+
+// dt/time/timeStep bookkeeping of calcDtFromCFL (Core.cpp:189-237) on device.
+struct TimeState {
+    double dt, time, cfl_max;
+    long long time_step;
+    unsigned long long umax_bits;
+    int nonfinite;
+};
+int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, int first_step,
+                       cudaStream_t st);
+
+int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cudaStream_t st);
+int launch_nonfinite_check(const Grid3 &g, const double *const q[5], int *flag, cudaStream_t st);
+
+}  // namespace mc3d

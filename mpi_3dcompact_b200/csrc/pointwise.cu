@@ -1,0 +1,432 @@
+// Pointwise kernels of the time step: primitives, the fused velocity-gradient /
+// stress / heat-flux / contravariant-flux evaluation (with the Vreman closure
+// inline), the RK register updates, the CFL reduction and the dt bookkeeping.
+// Grid-stride loops over x-fastest fields; one thread per point per iteration.
+#include <cmath>
+
+#include "mc3d_internal.h"
+
+namespace mc3d {
+
+constexpr double GAMMA = 1.4;        // src/IdealGas.hpp:38-46
+constexpr double PR = 0.7;
+constexpr double R_GAS = (1.0 / 1.4) / 1.0 / 1.0;
+constexpr double CP = R_GAS * GAMMA / (GAMMA - 1.0);
+
+static int grid_for(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    int sms = 148;
+    long long cap = (long long)sms * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <typename R>
+__device__ __forceinline__ R met(const Metrics<R> &m, int c, long long i) {
+    return m.constant ? m.c[c] : m.m[c][i];
+}
+
+__device__ __forceinline__ float mu_of_T(float T, double mu_ref) { return (float)mu_ref * powf(T, 0.76f); }
+__device__ __forceinline__ double mu_of_T(double T, double mu_ref) { return mu_ref * pow(T, 0.76); }
+
+// ---- primitives U, V, W, T (updateNonConservedData, Core.cpp:1158-1197) ----
+template <typename R>
+__global__ void primitives_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
+                                  const double *__restrict__ r2, const double *__restrict__ r3,
+                                  const double *__restrict__ r4, R *U, R *V, R *W, R *T) {
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double rho = r0[i];
+        double u = r1[i] / rho, v = r2[i] / rho, w = r3[i] / rho;
+        double p = (GAMMA - 1) * (r4[i] - 0.5 * rho * (u * u + v * v + w * w));
+        U[i] = (R)u;
+        V[i] = (R)v;
+        W[i] = (R)w;
+        T[i] = (R)(p / (rho * R_GAS));
+    }
+}
+
+template <typename R>
+int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[4], cudaStream_t st) {
+    primitives_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], prim[0], prim[1],
+                                                               prim[2], prim[3]);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+// ---- Vreman eddy viscosity (src/VremanSGS.hpp:43-96) ----
+template <typename R>
+__device__ __forceinline__ R vreman_mu(const R gu[3][3], R rho, R d1) {
+    R d1v1 = gu[0][0], d2v1 = gu[0][1], d3v1 = gu[0][2];
+    R d1v2 = gu[1][0], d2v2 = gu[1][1], d3v2 = gu[1][2];
+    R d1v3 = gu[2][0], d2v3 = gu[2][1], d3v3 = gu[2][2];
+    R b11 = d1 * d1v1 * d1v1 + d1 * d2v1 * d2v1 + d1 * d3v1 * d3v1;
+    R b12 = d1 * d1v1 * d1v2 + d1 * d2v1 * d2v2 + d1 * d3v1 * d3v2;
+    R b13 = d1 * d1v1 * d1v3 + d1 * d2v1 * d2v3 + d1 * d3v1 * d3v3;
+    R b22 = d1 * d1v2 * d1v2 + d1 * d2v2 * d2v2 + d1 * d3v2 * d3v2;
+    R b23 = d1 * d1v2 * d1v3 + d1 * d2v2 * d2v3 + d1 * d3v2 * d3v3;
+    R b33 = d1 * d1v3 * d1v3 + d1 * d2v3 * d2v3 + d1 * d3v3 * d3v3;
+    // the reference sums d2v3^2 twice and omits d3v2^2 (VremanSGS.hpp:74-76)
+    R abeta = d1v1 * d1v1 + d1v2 * d1v2 + d1v3 * d1v3 + d2v1 * d2v1 + d2v2 * d2v2 + d2v3 * d2v3 + d3v1 * d3v1 +
+              d2v3 * d2v3 + d3v3 * d3v3;
+    R bbeta = b11 * b22 - (b12 * b12) + b11 * b33 - (b13 * b13) + b22 * b33 - (b23 * b23);
+    const R eps = (R)1e-12;
+    if (bbeta < eps) bbeta = eps;
+    R ss = sqrt(bbeta / (abeta + eps));
+    const R c = (R)(2.5 * 0.17 * 0.17);
+    R mu = c * rho * ss;
+    R cap = (R)0.05 * d1 * sqrt((R)2.0 * abeta);
+    return mu < cap ? mu : cap;
+}
+
+// Filter width squared d1 = (dxi deta dzeta / J)^(2/3) of VremanSGS.hpp:49-52.
+template <typename R>
+__device__ __forceinline__ R vreman_d1(double dvol, R J) {
+    double del = pow(dvol / (double)J, 1.0 / 3.0);
+    return (R)(del * del);
+}
+
+template <typename R>
+__device__ __forceinline__ void velocity_gradient(const Metrics<R> &m, long long i, const R *const *d, R gu[3][3]) {
+    // gradU[a][b] = J1b dUa1 + J2b dUa2 + J3b dUa3  (Core.cpp:548-561)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        R d1 = d[3 * a][i], d2 = d[3 * a + 1][i], d3 = d[3 * a + 2][i];
+#pragma unroll
+        for (int b = 0; b < 3; b++) gu[a][b] = met(m, 1 + b, i) * d1 + met(m, 4 + b, i) * d2 + met(m, 7 + b, i) * d3;
+    }
+}
+
+struct DerivPtrs12 {
+    const void *p[12];
+};
+struct OutPtrs15 {
+    void *p[15];
+};
+
+// ---- fluxes: preStepDerivatives, Core.cpp:615-752 ----
+template <typename R>
+__global__ void __launch_bounds__(256) flux_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
+                                                   const double *__restrict__ r2, const double *__restrict__ r3,
+                                                   const double *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
+                                                   FluxParams fp, const R *__restrict__ mu_sgs_f, OutPtrs15 op) {
+    const R *const *d = reinterpret_cast<const R *const *>(dp.p);
+    R *const *F = reinterpret_cast<R *const *>(op.p);
+    const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double rho_d = r0[i];
+        double Ud = r1[i] / rho_d, Vd = r2[i] / rho_d, Wd = r3[i] / rho_d;
+        double pd = (GAMMA - 1) * (r4[i] - 0.5 * rho_d * (Ud * Ud + Vd * Vd + Wd * Wd));
+        double Td = pd / (rho_d * R_GAS);
+        R rho = (R)rho_d, U = (R)Ud, V = (R)Vd, W = (R)Wd, p = (R)pd, T = (R)Td;
+        R rhoU = (R)r1[i], rhoV = (R)r2[i], rhoW = (R)r3[i], rhoE = (R)r4[i];
+        R mu = mu_of_T(T, fp.mu_ref);
+        R J = met(m, 0, i);
+        R J11 = met(m, 1, i), J12 = met(m, 2, i), J13 = met(m, 3, i);
+        R J21 = met(m, 4, i), J22 = met(m, 5, i), J23 = met(m, 6, i);
+        R J31 = met(m, 7, i), J32 = met(m, 8, i), J33 = met(m, 9, i);
+        R Ucurv = J11 * U + J12 * V + J13 * W;
+        R Vcurv = J21 * U + J22 * V + J23 * W;
+        R Wcurv = J31 * U + J32 * V + J33 * W;
+
+        R gu[3][3];
+        velocity_gradient<R>(m, i, d, gu);
+
+        R mu_eff, k_eff;
+        if (fp.les) {
+            R mu_sgs;
+            if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, vreman_d1<R>(dvol, J));
+            else mu_sgs = mu_sgs_f[i];
+            mu_eff = mu + mu_sgs;
+            k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
+            if (mu_eff < (R)0) mu_eff = 0;
+            if (k_eff < (R)0) k_eff = 0;
+        } else {
+            mu_eff = mu;
+            k_eff = (R)(CP / PR) * mu;
+        }
+        R dUdx = gu[0][0], dUdy = gu[0][1], dUdz = gu[0][2];
+        R dVdx = gu[1][0], dVdy = gu[1][1], dVdz = gu[1][2];
+        R dWdx = gu[2][0], dWdy = gu[2][1], dWdz = gu[2][2];
+        const R c43 = (R)(4.0 / 3.0), c23 = (R)(2.0 / 3.0);
+        R t11 = (c43 * dUdx - c23 * dVdy - c23 * dWdz) * mu_eff;
+        R t22 = (-c23 * dUdx + c43 * dVdy - c23 * dWdz) * mu_eff;
+        R t33 = (-c23 * dUdx - c23 * dVdy + c43 * dWdz) * mu_eff;
+        R t12 = (dUdy + dVdx) * mu_eff;
+        R t13 = (dUdz + dWdx) * mu_eff;
+        R t23 = (dVdz + dWdy) * mu_eff;
+        const R t21 = t12, t31 = t13, t32 = t23;
+
+        R dT1 = d[9][i], dT2 = d[10][i], dT3 = d[11][i];
+        R q1 = k_eff * (J11 * dT1 + J21 * dT2 + J31 * dT3);
+        R q2 = k_eff * (J12 * dT1 + J22 * dT2 + J32 * dT3);
+        R q3 = k_eff * (J13 * dT1 + J23 * dT2 + J33 * dT3);
+        R b1 = U * t11 + V * t12 + W * t13 + q1;
+        R b2 = U * t21 + V * t22 + W * t23 + q2;
+        R b3 = U * t31 + V * t32 + W * t33 + q3;
+
+        R iJ = (R)1 / J;
+        F[0][i] = iJ * (rho * Ucurv);
+        F[5][i] = iJ * (rho * Vcurv);
+        F[10][i] = iJ * (rho * Wcurv);
+
+        R f1, f2, f3, g1, g2, g3;
+        f1 = rhoU * Ucurv + J11 * p; f2 = rhoU * Vcurv + J21 * p; f3 = rhoU * Wcurv + J31 * p;
+        g1 = J11 * t11 + J12 * t21 + J13 * t31;
+        g2 = J21 * t11 + J22 * t21 + J23 * t31;
+        g3 = J31 * t11 + J32 * t21 + J33 * t31;
+        F[1][i] = iJ * (f1 - g1); F[6][i] = iJ * (f2 - g2); F[11][i] = iJ * (f3 - g3);
+
+        f1 = rhoV * Ucurv + J12 * p; f2 = rhoV * Vcurv + J22 * p; f3 = rhoV * Wcurv + J32 * p;
+        g1 = J11 * t12 + J12 * t22 + J13 * t32;
+        g2 = J21 * t12 + J22 * t22 + J23 * t32;
+        g3 = J31 * t12 + J32 * t22 + J33 * t32;
+        F[2][i] = iJ * (f1 - g1); F[7][i] = iJ * (f2 - g2); F[12][i] = iJ * (f3 - g3);
+
+        f1 = rhoW * Ucurv + J13 * p; f2 = rhoW * Vcurv + J23 * p; f3 = rhoW * Wcurv + J33 * p;
+        g1 = J11 * t13 + J12 * t23 + J13 * t33;
+        g2 = J21 * t13 + J22 * t23 + J23 * t33;
+        g3 = J31 * t13 + J32 * t23 + J33 * t33;
+        F[3][i] = iJ * (f1 - g1); F[8][i] = iJ * (f2 - g2); F[13][i] = iJ * (f3 - g3);
+
+        R ep = rhoE + p;
+        f1 = ep * Ucurv; f2 = ep * Vcurv; f3 = ep * Wcurv;
+        g1 = J11 * b1 + J12 * b2 + J13 * b3;
+        g2 = J21 * b1 + J22 * b2 + J23 * b3;
+        g3 = J31 * b1 + J32 * b2 + J33 * b3;
+        F[4][i] = iJ * (f1 - g1); F[9][i] = iJ * (f2 - g2); F[14][i] = iJ * (f3 - g3);
+    }
+}
+
+template <typename R>
+int launch_flux(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+                const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st) {
+    DerivPtrs12 dp;
+    for (int i = 0; i < 12; i++) dp.p[i] = d[i];
+    OutPtrs15 op;
+    for (int i = 0; i < 15; i++) op.p[i] = F[i];
+    flux_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+template <typename R>
+__global__ void vreman_kernel(Grid3 g, const double *__restrict__ r0, DerivPtrs12 dp, Metrics<R> m, FluxParams fp,
+                              R *mu_sgs) {
+    const R *const *d = reinterpret_cast<const R *const *>(dp.p);
+    const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        R gu[3][3];
+        velocity_gradient<R>(m, i, d, gu);
+        mu_sgs[i] = vreman_mu<R>(gu, (R)r0[i], vreman_d1<R>(dvol, met(m, 0, i)));
+    }
+}
+
+template <typename R>
+int launch_vreman(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+                  const FluxParams &p, R *mu_sgs, cudaStream_t st) {
+    DerivPtrs12 dp;
+    for (int i = 0; i < 12; i++) dp.p[i] = d[i];
+    vreman_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], dp, m, p, mu_sgs);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+// ---- RK register updates ----
+// RK4 (src/RK4.hpp:47-125), TVDRK3 (src/TVDRK3.hpp:50-133) and the 2N-storage
+// KenRK4 / LSLDDRK4 (src/KenRK4.hpp:53-152, src/LSLDDRK4.hpp:93-320).
+struct Q5 {
+    double *p[5];
+};
+template <typename R>
+struct K5 {
+    const R *p[5];
+};
+
+template <typename R>
+__global__ void rk_kernel(Grid3 g, RkStage rs, K5<R> k2, Q5 q1, Q5 qk, Q5 q2) {
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            double k = (double)k2.p[v][i];
+            if (rs.scheme == MC3D_RK4) {
+                if (rs.stage == 1) {
+                    double b1 = q1.p[v][i];
+                    q2.p[v][i] = b1 + rs.a * k;
+                    qk.p[v][i] = b1 + rs.b * k;
+                } else if (rs.stage < 4) {
+                    q2.p[v][i] += rs.a * k;
+                    qk.p[v][i] = q1.p[v][i] + rs.b * k;
+                } else {
+                    q2.p[v][i] += rs.a * k;
+                }
+            } else if (rs.scheme == MC3D_TVDRK3) {
+                if (rs.stage == 1) qk.p[v][i] = q1.p[v][i] + 1.0 * k;
+                else if (rs.stage == 2) qk.p[v][i] = 0.75 * q1.p[v][i] + 0.25 * qk.p[v][i] + 0.25 * k;
+                else q2.p[v][i] = (1.0 / 3.0) * q1.p[v][i] + (2.0 / 3.0) * qk.p[v][i] + (2.0 / 3.0) * k;
+            } else {
+                if (rs.stage == 1) {
+                    qk.p[v][i] = q1.p[v][i] + rs.b * k;
+                    q1.p[v][i] = k;
+                } else {
+                    double r = k + rs.a * q1.p[v][i];
+                    q1.p[v][i] = r;
+                    if (rs.stage < rs.nstages) qk.p[v][i] += rs.b * r;
+                    else q2.p[v][i] = qk.p[v][i] + rs.b * r;
+                }
+            }
+        }
+    }
+}
+
+template <typename R>
+int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
+                     double *const qk[5], double *const q2[5], cudaStream_t st) {
+    K5<R> k;
+    Q5 a, b, c;
+    for (int v = 0; v < 5; v++) {
+        k.p[v] = k2[v];
+        a.p[v] = q1[v];
+        b.p[v] = qk[v];
+        c.p[v] = q2[v];
+    }
+    rk_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rs, k, a, b, c);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+template <typename R>
+__global__ void to_real_kernel(Grid3 g, Q5 src, K5<R> dst) {
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) const_cast<R *>(dst.p[v])[i] = (R)src.p[v][i];
+    }
+}
+
+template <typename R>
+int launch_to_real(const Grid3 &g, const double *const src[5], R *const dst[5], cudaStream_t st) {
+    Q5 s;
+    K5<R> d;
+    for (int v = 0; v < 5; v++) {
+        s.p[v] = const_cast<double *>(src[v]);
+        d.p[v] = dst[v];
+    }
+    to_real_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, s, d);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+// ---- CFL (calcDtFromCFL, Core.cpp:189-237) ----
+template <typename R>
+__global__ void cfl_kernel(Grid3 g, Q5 q, Metrics<R> m, double i0, double i1, double i2, unsigned long long *umax) {
+    __shared__ double red[32];
+    double best = 0.0;
+    bool bad = false;
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double rho = q.p[0][i];
+        double u = q.p[1][i] / rho, v = q.p[2][i] / rho, w = q.p[3][i] / rho;
+        double p = (GAMMA - 1) * (q.p[4][i] - 0.5 * rho * (u * u + v * v + w * w));
+        double c = sqrt(GAMMA * p / rho);
+        double uc = (double)met(m, 1, i) * (fabs(u) + c) * i0 + (double)met(m, 5, i) * (fabs(v) + c) * i1 +
+                    (double)met(m, 9, i) * (fabs(w) + c) * i2;
+        if (!isfinite(uc)) bad = true;
+        else if (uc > best) best = uc;
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double b = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+        if (threadIdx.x == 0) atomicMax(umax, (unsigned long long)__double_as_longlong(b));
+    }
+    // a non-finite state poisons the maximum: dt becomes NaN and the host check reports it
+    if (bad) atomicMax(umax, 0x7ff8000000000000ull);
+}
+
+template <typename R>
+int launch_cfl(const Grid3 &g, const double *const q[5], const Metrics<R> &m, const double dxi[3],
+               unsigned long long *umax, cudaStream_t st) {
+    Q5 s;
+    for (int v = 0; v < 5; v++) s.p[v] = const_cast<double *>(q[v]);
+    cfl_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, s, m, 1.0 / dxi[0], 1.0 / dxi[1], 1.0 / dxi[2], umax);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+__global__ void finalize_dt_kernel(TimeState *ts, int ts_type, double cfl, double dt_const, int first) {
+    double m = __longlong_as_double((long long)ts->umax_bits);
+    ts->cfl_max = m;
+    if (!isfinite(m)) ts->nonfinite = 1;
+    ts->dt = (ts_type == MC3D_CONST_CFL) ? cfl / m : dt_const;
+    ts->time_step += 1;
+    if (!first) ts->time += ts->dt;
+    ts->umax_bits = 0ull;
+}
+
+int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, int first_step, cudaStream_t st) {
+    finalize_dt_kernel<<<1, 1, 0, st>>>(ts, ts_type, cfl, dt_const, first_step);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+__global__ void integrals_kernel(Grid3 g, Q5 q, double *acc) {
+    __shared__ double r1[32], r2[32];
+    double ke = 0, ms = 0;
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double rho = q.p[0][i];
+        double a = q.p[1][i], b = q.p[2][i], c = q.p[3][i];
+        ke += 0.5 * (a * a + b * b + c * c) / rho;
+        ms += rho;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ke += __shfl_xor_sync(0xffffffffu, ke, o);
+        ms += __shfl_xor_sync(0xffffffffu, ms, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        r1[threadIdx.x >> 5] = ke;
+        r2[threadIdx.x >> 5] = ms;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            a += r1[w];
+            b += r2[w];
+        }
+        atomicAdd(acc, a);
+        atomicAdd(acc + 1, b);
+    }
+}
+
+int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cudaStream_t st) {
+    Q5 s;
+    for (int v = 0; v < 5; v++) s.p[v] = const_cast<double *>(q[v]);
+    integrals_kernel<<<grid_for(g.n(), 256), 256, 0, st>>>(g, s, acc2);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+#define MC3D_INST(R)                                                                                              \
+    template int launch_primitives<R>(const Grid3 &, const double *const[5], R *const[4], cudaStream_t);          \
+    template int launch_flux<R>(const Grid3 &, const double *const[5], const R *const[12], const Metrics<R> &,    \
+                                const FluxParams &, const R *, R *const[15], cudaStream_t);                       \
+    template int launch_vreman<R>(const Grid3 &, const double *const[5], const R *const[12], const Metrics<R> &,  \
+                                  const FluxParams &, R *, cudaStream_t);                                         \
+    template int launch_rk_update<R>(const Grid3 &, const RkStage &, const R *const[5], double *const[5],         \
+                                     double *const[5], double *const[5], cudaStream_t);                           \
+    template int launch_to_real<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);             \
+    template int launch_cfl<R>(const Grid3 &, const double *const[5], const Metrics<R> &, const double[3],        \
+                               unsigned long long *, cudaStream_t);
+MC3D_INST(float)
+MC3D_INST(double)
+#undef MC3D_INST
+
+}  // namespace mc3d

@@ -1,0 +1,530 @@
+// GPU CurvilinearCSolver: one block resident on one device, driven by the RK
+// schemes of the reference. Host code only sequences kernels on one stream;
+// dt, time and the time-step counter live on the device (FP64) so a step
+// needs no host synchronisation.
+//
+// Stage data flow (per RK stage; every array is a full Nx*Ny*Nz field):
+//   primitives(qP) -> U,V,W,T                           (Core.cpp:1158-1197)
+//   3 sweeps: d/dxi_d of U,V,W,T -> 12 derivatives        (Core.cpp:239-348)
+//   flux: gradU, Vreman, tau, q, 15 flux components       (Core.cpp:548-752)
+//   3 sweeps: -dF/dxi1, -dG/dxi2, -dH/dxi3 -> k2          (Core.cpp:350-466, 790-947)
+//   RK register update                                    (RK4.hpp, LSLDDRK4.hpp, ...)
+//   filter (last stage or every stage)                   (Core.cpp:949-1155)
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mc3d_internal.h"
+
+struct mc3d_solver_s {
+    mc3d_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    mc3d::Grid3 g{};
+    int prec = MC3D_FP64;
+    double dxi[3] = {0, 0, 0};
+    mc3d::LineOpBuf dop[3], fop[3], vop[3];
+    double *q1[5] = {}, *qk[5] = {}, *q2[5] = {};
+    void *k2[5] = {}, *rhs[5] = {}, *prim[4] = {}, *der[12] = {}, *flux[15] = {};
+    void *tA[5] = {}, *tB[5] = {}, *tC[5] = {}, *mu_sgs = nullptr;
+    double *met64[10] = {};
+    void *metR[10] = {};
+    bool const_met = true;
+    double met_c[10] = {0};
+    bool have_metrics = false;
+    mc3d::TimeState *ts = nullptr;
+    double *acc = nullptr;
+    int host_time_step = 0;
+    int filter_time_step = 0;
+    int lsldd_half = 1;
+    long long stages = 0;
+    long long launches = 0;
+    bool initialized = false;
+    std::vector<void *> allocs;
+};
+
+namespace mc3d {
+
+static const double RK4_A[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+static const double RK4_B[3] = {1.0 / 2.0, 1.0 / 2.0, 1.0};
+// src/KenRK4.hpp:30-40
+static const double KEN_A[5] = {0.0, -6234157559845.0 / 12983515589748.0, -6194124222391.0 / 4410992767914.0,
+                                -31623096876824.0 / 15682348800105.0, -12251185447671.0 / 11596622555746.0};
+static const double KEN_B[5] = {494393426753.0 / 4806282396855.0, 4047970641027.0 / 5463924506627.0,
+                                9795748752853.0 / 13190207949281.0, 4009051133189.0 / 8539092990294.0,
+                                1348533437543.0 / 7166442652324.0};
+// src/LSLDDRK4.hpp:40-78
+static const double LS_A1[5] = {0.0, -0.60512264332862261228, -2.04375640234761394333, -0.74069990637544192841,
+                                -4.42317651302968168941};
+static const double LS_B1[5] = {0.26874543888713438496, 0.8014706973220802933, 0.50515704269422722538,
+                                0.56235680379000296407, 0.05900655127758823335};
+static const double LS_A2[6] = {0.0, -0.44127377153877382565, -1.073982008079781868, -1.7063570791256758809,
+                                -2.7979293162682443056, -4.0913537120919160454};
+static const double LS_B2[6] = {0.11584888181285561688, 0.37287699051652864918, 0.73795368921435295698,
+                                0.57981109366311039538, 1.031284991300145194, 0.15};
+
+static int salloc(mc3d_solver s, void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(MC3D_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    s->allocs.push_back(*p);
+    MC3D_CUDA_TRY(cudaMemsetAsync(*p, 0, bytes, s->stream));
+    return MC3D_OK;
+}
+
+template <typename R>
+static Metrics<R> metrics_of(mc3d_solver s) {
+    Metrics<R> m;
+    m.constant = s->const_met;
+    for (int i = 0; i < 10; i++) {
+        m.c[i] = (R)s->met_c[i];
+        m.m[i] = s->const_met ? nullptr : (const R *)s->metR[i];
+    }
+    return m;
+}
+
+template <typename R>
+static const LineOpDev<R> &opdev(const LineOpBuf &b);
+template <>
+const LineOpDev<float> &opdev<float>(const LineOpBuf &b) { return b.f32; }
+template <>
+const LineOpDev<double> &opdev<double>(const LineOpBuf &b) { return b.f64; }
+
+template <typename R>
+static int sweep(mc3d_solver s, int dir, const LineOpBuf &op, int nf, const void *const *in, void *const *out,
+                 int epi, const void *const *aux, double *const *out64, bool filter) {
+    SweepBatch<R> b{};
+    b.nf = nf;
+    for (int f = 0; f < nf; f++) {
+        b.in[f] = (const R *)in[f];
+        b.out[f] = out ? (R *)out[f] : nullptr;
+        b.aux[f] = aux ? (const R *)aux[f] : nullptr;
+        b.out64[f] = out64 ? out64[f] : nullptr;
+        b.eq[f] = f;
+    }
+    RhsFinalArgs<R> rf{};
+    rf.dt = &s->ts->dt;
+    rf.J = s->const_met ? nullptr : (const R *)s->metR[0];
+    rf.Jc = (R)s->met_c[0];
+    rf.quirk = s->cfg.reference_quirks;
+    s->launches++;
+    return launch_sweep<R>(dir, s->g, opdev<R>(op), b, epi, rf, s->cfg.bc_type, filter, s->stream);
+}
+
+// Three directional filter sweeps in the rotating order of
+// filterConservedData (Core.cpp:996-1134): filterTimeStep%3 == 1: Y,Z,X;
+// == 2: Z,X,Y; == 0: X,Y,Z. in -> out (both FP64 state arrays).
+template <typename R>
+static int filter_state(mc3d_solver s, double *const in[5], double *const out[5], const LineOpBuf *ops,
+                        const int order[3]) {
+    int rc;
+    void *src0[5];
+    if (s->prec == MC3D_FP64) {
+        for (int v = 0; v < 5; v++) src0[v] = in[v];
+    } else {
+        R *dst[5];
+        for (int v = 0; v < 5; v++) dst[v] = (R *)s->tC[v];
+        s->launches++;
+        if ((rc = launch_to_real<R>(s->g, in, dst, s->stream))) return rc;
+        for (int v = 0; v < 5; v++) src0[v] = s->tC[v];
+    }
+    if ((rc = sweep<R>(s, order[0], ops[order[0]], 5, src0, s->tA, EPI_STORE, nullptr, nullptr, true))) return rc;
+    if ((rc = sweep<R>(s, order[1], ops[order[1]], 5, s->tA, s->tB, EPI_STORE, nullptr, nullptr, true))) return rc;
+    if (s->prec == MC3D_FP64) {
+        void *o[5];
+        for (int v = 0; v < 5; v++) o[v] = out[v];
+        return sweep<R>(s, order[2], ops[order[2]], 5, s->tB, o, EPI_STORE, nullptr, nullptr, true);
+    }
+    return sweep<R>(s, order[2], ops[order[2]], 5, s->tB, nullptr, EPI_STORE_F64, nullptr, out, true);
+}
+
+template <typename R>
+static int filter_conserved(mc3d_solver s, bool last) {
+    double **in = last ? s->q2 : s->qk;
+    double **out = last ? s->q1 : s->qk;
+    if (s->host_time_step % s->cfg.filter_step == 0) {
+        s->filter_time_step++;
+        int r = s->filter_time_step % 3;
+        int order[3];
+        if (r == 1) { order[0] = 1; order[1] = 2; order[2] = 0; }
+        else if (r == 2) { order[0] = 2; order[1] = 0; order[2] = 1; }
+        else { order[0] = 0; order[1] = 1; order[2] = 2; }
+        return filter_state<R>(s, in, out, s->fop, order);
+    }
+    if (last) {
+        size_t bytes = (size_t)s->g.n() * sizeof(double);
+        for (int v = 0; v < 5; v++)
+            MC3D_CUDA_TRY(cudaMemcpyAsync(s->q1[v], s->q2[v], bytes, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    return MC3D_OK;
+}
+
+template <typename R>
+static int stage_rhs(mc3d_solver s, double *const qP[5]) {
+    int rc;
+    R *prim[4];
+    for (int v = 0; v < 4; v++) prim[v] = (R *)s->prim[v];
+    s->launches++;
+    if ((rc = launch_primitives<R>(s->g, qP, prim, s->stream))) return rc;
+    // gradients of U, V, W, T in each direction: der[3*var + dir]
+    for (int d = 0; d < 3; d++) {
+        void *out[4] = {s->der[0 + d], s->der[3 + d], s->der[6 + d], s->der[9 + d]};
+        if ((rc = sweep<R>(s, d, s->dop[d], 4, s->prim, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+    }
+    Metrics<R> m = metrics_of<R>(s);
+    FluxParams fp{};
+    fp.mu_ref = s->cfg.mu_ref;
+    for (int i = 0; i < 3; i++) fp.dxi[i] = s->dxi[i];
+    fp.pr_t = 0.9;   // src/CurvilinearCSolver.hpp:232
+    fp.les = 0;
+    const R *dd[12];
+    for (int i = 0; i < 12; i++) dd[i] = (const R *)s->der[i];
+    if (s->cfg.les_model == MC3D_VREMAN) {
+        if (s->cfg.les_averaging == MC3D_AVG_NONE) {
+            fp.les = 1;
+        } else {
+            // mu_sgs, then doAveraging LOCAL: Compact10(-0.49) along Y, Z, X (AbstractSGS.cpp:144-152)
+            s->launches++;
+            if ((rc = launch_vreman<R>(s->g, qP, dd, m, fp, (R *)s->mu_sgs, s->stream))) return rc;
+            void *a[1] = {s->mu_sgs}, *t1[1] = {s->tA[0]}, *t2[1] = {s->tB[0]};
+            if ((rc = sweep<R>(s, 1, s->vop[1], 1, a, t1, EPI_STORE, nullptr, nullptr, true))) return rc;
+            if ((rc = sweep<R>(s, 2, s->vop[2], 1, t1, t2, EPI_STORE, nullptr, nullptr, true))) return rc;
+            if ((rc = sweep<R>(s, 0, s->vop[0], 1, t2, a, EPI_STORE, nullptr, nullptr, true))) return rc;
+            fp.les = 2;
+        }
+    }
+    R *F[15];
+    for (int i = 0; i < 15; i++) F[i] = (R *)s->flux[i];
+    s->launches++;
+    if ((rc = launch_flux<R>(s->g, qP, dd, m, fp, (const R *)s->mu_sgs, F, s->stream))) return rc;
+    // divergence of the contravariant fluxes, accumulated into the RHS, then k2
+    if ((rc = sweep<R>(s, 0, s->dop[0], 5, s->flux + 0, s->rhs, EPI_STORE_NEG, nullptr, nullptr, false))) return rc;
+    if ((rc = sweep<R>(s, 1, s->dop[1], 5, s->flux + 5, s->rhs, EPI_SUB, nullptr, nullptr, false))) return rc;
+    if ((rc = sweep<R>(s, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->rhs, nullptr, false))) return rc;
+    return MC3D_OK;
+}
+
+template <typename R>
+static int one_step(mc3d_solver s) {
+    int rc;
+    // preStep: calcDtFromCFL on the current state (Core.cpp:189-237)
+    Metrics<R> m = metrics_of<R>(s);
+    s->launches += 2;
+    if ((rc = launch_cfl<R>(s->g, s->q1, m, s->dxi, &s->ts->umax_bits, s->stream))) return rc;
+    int first = s->host_time_step == s->cfg.time_step0;
+    if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
+    s->host_time_step++;
+
+    int scheme = s->cfg.rk_type;
+    int ns = scheme == MC3D_RK4 ? 4 : scheme == MC3D_TVDRK3 ? 3 : scheme == MC3D_KENRK4 ? 5 : (s->lsldd_half == 1 ? 5 : 6);
+    for (int st = 1; st <= ns; st++) {
+        double *const *qP = st == 1 ? s->q1 : s->qk;
+        if ((rc = stage_rhs<R>(s, qP))) return rc;
+        RkStage rs{};
+        rs.scheme = scheme;
+        rs.stage = st;
+        rs.nstages = ns;
+        if (scheme == MC3D_RK4) {
+            rs.a = RK4_A[st - 1];
+            rs.b = st < 4 ? RK4_B[st - 1] : 0.0;
+        } else if (scheme == MC3D_KENRK4) {
+            rs.a = KEN_A[st - 1];
+            rs.b = KEN_B[st - 1];
+        } else if (scheme == MC3D_LSLDDRK4) {
+            rs.a = s->lsldd_half == 1 ? LS_A1[st - 1] : LS_A2[st - 1];
+            rs.b = s->lsldd_half == 1 ? LS_B1[st - 1] : LS_B2[st - 1];
+        }
+        const R *k2[5];
+        for (int v = 0; v < 5; v++) k2[v] = (const R *)s->k2[v];
+        s->launches++;
+        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, s->stream))) return rc;
+        bool last = st == ns;
+        if (last || s->cfg.substep_filtering)
+            if ((rc = filter_conserved<R>(s, last))) return rc;
+        s->stages++;
+    }
+    if (scheme == MC3D_LSLDDRK4) s->lsldd_half = s->lsldd_half == 1 ? 2 : 1;
+    return MC3D_OK;
+}
+
+}  // namespace mc3d
+
+using namespace mc3d;
+
+extern "C" {
+
+int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
+    if (!cfg || !out) return fail(MC3D_ERR_ARG, "null argument");
+    *out = nullptr;
+    const mc3d_config &c = *cfg;
+    if (c.Nx <= 10 || c.Ny <= 10 || c.Nz <= 10)
+        return fail(MC3D_ERR_CONFIG, "Number of grid points in any direction must be greater than 10");
+    if (c.precision != MC3D_FP64 && c.precision != MC3D_FP32BULK) return fail(MC3D_ERR_CONFIG, "bad precision");
+    if (c.les_model == MC3D_DSM) return fail(MC3D_ERR_CONFIG, "LESMODEL=DSM is not available in this build");
+    if (c.les_model == MC3D_VREMAN && c.les_averaging != MC3D_AVG_NONE && c.les_averaging != MC3D_AVG_LOCAL)
+        return fail(MC3D_ERR_CONFIG, "LESAVERAGING other than NONE/LOCAL is not available in this build");
+    for (int d = 0; d < 3; d++)
+        if (c.bc_type[d] != MC3D_PERIODIC_SOLVE)
+            return fail(MC3D_ERR_CONFIG, "DIRICHLET_SOLVE boundaries (walls, sponge) are not available in the solver yet");
+    if (c.filter_step < 1) return fail(MC3D_ERR_CONFIG, "FILTERSTEP must be >= 1");
+    MC3D_CUDA_TRY(cudaSetDevice(device));
+    mc3d_solver s = new mc3d_solver_s();
+    s->cfg = c;
+    s->device = device;
+    s->prec = c.precision;
+    s->g = Grid3{c.Nx, c.Ny, c.Nz};
+    s->host_time_step = c.time_step0;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(MC3D_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    int N[3] = {c.Nx, c.Ny, c.Nz};
+    int rc = MC3D_OK;
+    try {
+        for (int d = 0; d < 3; d++) {
+            // Domain with unit extents (src/Domain.hpp:45-79)
+            s->dxi[d] = c.bc_type[d] == MC3D_PERIODIC_SOLVE ? 1.0 / N[d] : 1.0 / (N[d] - 1.0);
+            LineOpHost dh = build_deriv_op(c.fd_type[d], c.bc_type[d], N[d], s->dxi[d]);
+            LineOpHost fh = build_filter_op(c.filter_type, c.alphaF, c.bc_type[d], N[d]);
+            LineOpHost vh = build_filter_op(MC3D_COMPACT10, -0.49, c.bc_type[d], N[d]);
+            if ((rc = upload_line_op(dh, c.precision, s->dop[d]))) break;
+            if ((rc = upload_line_op(fh, c.precision, s->fop[d]))) break;
+            if ((rc = upload_line_op(vh, c.precision, s->vop[d]))) break;
+        }
+    } catch (const std::exception &ex) {
+        rc = fail(MC3D_ERR_CONFIG, ex.what());
+    }
+    size_t n = (size_t)s->g.n();
+    size_t rb = c.precision == MC3D_FP64 ? sizeof(double) : sizeof(float);
+    for (int v = 0; v < 5 && !rc; v++) {
+        rc = rc ? rc : salloc(s, (void **)&s->q1[v], n * sizeof(double));
+        rc = rc ? rc : salloc(s, (void **)&s->qk[v], n * sizeof(double));
+        rc = rc ? rc : salloc(s, (void **)&s->q2[v], n * sizeof(double));
+        rc = rc ? rc : salloc(s, &s->k2[v], n * rb);
+        rc = rc ? rc : salloc(s, &s->rhs[v], n * rb);
+        rc = rc ? rc : salloc(s, &s->tA[v], n * rb);
+        rc = rc ? rc : salloc(s, &s->tB[v], n * rb);
+        if (!rc && c.precision != MC3D_FP64) rc = salloc(s, &s->tC[v], n * rb);
+    }
+    for (int v = 0; v < 4 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
+    for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
+    for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
+    if (!rc && c.les_model == MC3D_VREMAN) rc = salloc(s, &s->mu_sgs, n * rb);
+    if (!rc) rc = salloc(s, (void **)&s->ts, sizeof(TimeState));
+    if (!rc) rc = salloc(s, (void **)&s->acc, 2 * sizeof(double));
+    if (!rc) {
+        TimeState t{};
+        t.time = c.time0;
+        t.time_step = c.time_step0;
+        t.dt = c.ts_type == MC3D_CONST_DT ? c.dt : 0.0;
+        e = cudaMemcpyAsync(s->ts, &t, sizeof(t), cudaMemcpyHostToDevice, s->stream);
+        if (e != cudaSuccess) rc = fail(MC3D_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (!rc) {
+        e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) rc = fail(MC3D_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc) {
+        mc3d_solver_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return MC3D_OK;
+}
+
+int mc3d_solver_destroy(mc3d_solver s) {
+    if (!s) return MC3D_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void *p : s->allocs) cudaFree(p);
+    for (int d = 0; d < 3; d++) {
+        free_line_op(s->dop[d]);
+        free_line_op(s->fop[d]);
+        free_line_op(s->vop[d]);
+    }
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return MC3D_OK;
+}
+
+static int upload_metrics(mc3d_solver s, const double *const h[10], const double *cvals) {
+    size_t n = (size_t)s->g.n();
+    int rc;
+    if (h) {
+        // constant metrics (uniform Cartesian blocks such as the HIT box) are
+        // carried as 10 scalars instead of 10 resident fields
+        bool cst = true;
+        for (int c = 0; c < 10 && cst; c++) {
+            double v0 = h[c][0], scale = std::fabs(v0) > 0 ? std::fabs(v0) : 1.0;
+            for (size_t i = 1; i < n; i++)
+                if (std::fabs(h[c][i] - v0) > 1e-13 * scale) { cst = false; break; }
+        }
+        s->const_met = cst;
+        for (int c = 0; c < 10; c++) s->met_c[c] = h[c][0];
+        if (!cst) {
+            size_t rb = s->prec == MC3D_FP64 ? sizeof(double) : sizeof(float);
+            for (int c = 0; c < 10; c++) {
+                if (!s->met64[c] && (rc = salloc(s, (void **)&s->met64[c], n * sizeof(double)))) return rc;
+                MC3D_CUDA_TRY(cudaMemcpyAsync(s->met64[c], h[c], n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+                if (s->prec == MC3D_FP64) {
+                    s->metR[c] = s->met64[c];
+                } else {
+                    if (!s->metR[c] && (rc = salloc(s, &s->metR[c], n * rb))) return rc;
+                    std::vector<float> tmp(n);
+                    for (size_t i = 0; i < n; i++) tmp[i] = (float)h[c][i];
+                    MC3D_CUDA_TRY(cudaMemcpyAsync(s->metR[c], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+                    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+                }
+            }
+        }
+    } else {
+        s->const_met = true;
+        for (int c = 0; c < 10; c++) s->met_c[c] = cvals[c];
+    }
+    s->have_metrics = true;
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
+}
+
+int mc3d_solver_set_metrics(mc3d_solver s, const double *const metrics[10]) {
+    if (!s || !metrics) return fail(MC3D_ERR_ARG, "null argument");
+    for (int c = 0; c < 10; c++)
+        if (!metrics[c]) return fail(MC3D_ERR_ARG, "null metric field");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    return upload_metrics(s, metrics, nullptr);
+}
+
+int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    if (!(Lx > 0 && Ly > 0 && Lz > 0)) return fail(MC3D_ERR_ARG, "box lengths must be positive");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    double c[10] = {1.0 / (Lx * Ly * Lz), 1.0 / Lx, 0, 0, 0, 1.0 / Ly, 0, 0, 0, 1.0 / Lz};
+    return upload_metrics(s, nullptr, c);
+}
+
+static int set_initial_impl(mc3d_solver s, const double *rho, const double *U, const double *V, const double *W,
+                            const double *p, bool device) {
+    if (!s || !rho || !U || !V || !W || !p) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->have_metrics) return fail(MC3D_ERR_CONFIG, "set the metrics before the initial condition");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    size_t n = (size_t)s->g.n();
+    // conserved state of setInitialConditions (src/CurvilinearCSolver_BC.cpp:31-59)
+    std::vector<double> h[5];
+    std::vector<double> hr(n), hu(n), hv(n), hw(n), hp(n);
+    if (device) {
+        MC3D_CUDA_TRY(cudaMemcpy(hr.data(), rho, n * 8, cudaMemcpyDeviceToHost));
+        MC3D_CUDA_TRY(cudaMemcpy(hu.data(), U, n * 8, cudaMemcpyDeviceToHost));
+        MC3D_CUDA_TRY(cudaMemcpy(hv.data(), V, n * 8, cudaMemcpyDeviceToHost));
+        MC3D_CUDA_TRY(cudaMemcpy(hw.data(), W, n * 8, cudaMemcpyDeviceToHost));
+        MC3D_CUDA_TRY(cudaMemcpy(hp.data(), p, n * 8, cudaMemcpyDeviceToHost));
+        rho = hr.data(); U = hu.data(); V = hv.data(); W = hw.data(); p = hp.data();
+    }
+    const double gamma = 1.4;
+    for (int v = 0; v < 5; v++) h[v].resize(n);
+    for (size_t i = 0; i < n; i++) {
+        double r = rho[i];
+        h[0][i] = r;
+        h[1][i] = r * U[i];
+        h[2][i] = r * V[i];
+        h[3][i] = r * W[i];
+        h[4][i] = p[i] / (gamma - 1.0) + 0.5 * r * (U[i] * U[i] + V[i] * V[i] + W[i] * W[i]);
+        if (!std::isfinite(h[4][i]) || !(r > 0)) return fail(MC3D_ERR_NONFINITE, "non-finite or non-positive initial state");
+    }
+    for (int v = 0; v < 5; v++) {
+        MC3D_CUDA_TRY(cudaMemcpyAsync(s->q1[v], h[v].data(), n * 8, cudaMemcpyHostToDevice, s->stream));
+        MC3D_CUDA_TRY(cudaMemsetAsync(s->k2[v], 0, n * (s->prec == MC3D_FP64 ? 8 : 4), s->stream));
+    }
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->initialized = true;
+    return MC3D_OK;
+}
+
+int mc3d_solver_set_initial(mc3d_solver s, const double *rho, const double *U, const double *V, const double *W,
+                            const double *p) {
+    return set_initial_impl(s, rho, U, V, W, p, false);
+}
+int mc3d_solver_set_initial_device(mc3d_solver s, const double *rho, const double *U, const double *V,
+                                   const double *W, const double *p) {
+    return set_initial_impl(s, rho, U, V, W, p, true);
+}
+
+int mc3d_solver_step(mc3d_solver s, int nsteps) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no initial condition");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    for (int i = 0; i < nsteps; i++) {
+        int rc = s->prec == MC3D_FP64 ? one_step<double>(s) : one_step<float>(s);
+        if (rc) return rc;
+    }
+    return MC3D_OK;
+}
+
+int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *rhoV, double *rhoW, double *rhoE) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    double *dst[5] = {rho, rhoU, rhoV, rhoW, rhoE};
+    size_t n = (size_t)s->g.n();
+    for (int v = 0; v < 5; v++)
+        if (dst[v]) MC3D_CUDA_TRY(cudaMemcpyAsync(dst[v], s->q1[v], n * 8, cudaMemcpyDeviceToHost, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    TimeState t;
+    MC3D_CUDA_TRY(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+    if (t.nonfinite) return fail(MC3D_ERR_NONFINITE, "the state became non-finite");
+    return MC3D_OK;
+}
+
+int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]) {
+    if (!s || !ptrs) return fail(MC3D_ERR_ARG, "null argument");
+    for (int v = 0; v < 5; v++) ptrs[v] = s->q1[v];
+    return MC3D_OK;
+}
+
+int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, long long *stages) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    TimeState t;
+    MC3D_CUDA_TRY(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+    if (time_step) *time_step = (int)t.time_step;
+    if (time) *time = t.time;
+    if (dt) *dt = t.dt;
+    if (stages) *stages = s->stages;
+    if (t.nonfinite) return fail(MC3D_ERR_NONFINITE, "the state became non-finite");
+    return MC3D_OK;
+}
+
+int mc3d_solver_integrals(mc3d_solver s, double *kinetic, double *mass) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaMemsetAsync(s->acc, 0, 2 * sizeof(double), s->stream));
+    int rc = launch_integrals(s->g, s->q1, s->acc, s->stream);
+    if (rc) return rc;
+    double h[2];
+    MC3D_CUDA_TRY(cudaMemcpyAsync(h, s->acc, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (kinetic) *kinetic = h[0];
+    if (mass) *mass = h[1];
+    return MC3D_OK;
+}
+
+int mc3d_solver_stream(mc3d_solver s, void **stream) {
+    if (!s || !stream) return fail(MC3D_ERR_ARG, "null argument");
+    *stream = (void *)s->stream;
+    return MC3D_OK;
+}
+
+int mc3d_solver_launch_count(mc3d_solver s, long long *count) {
+    if (!s || !count) return fail(MC3D_ERR_ARG, "null argument");
+    *count = s->launches;
+    return MC3D_OK;
+}
+
+int mc3d_solver_sync(mc3d_solver s) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
+}
+
+}  // extern "C"

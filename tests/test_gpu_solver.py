@@ -1,0 +1,120 @@
+"""GPU parity of the full time step (C ABI mc3d_solver_* through the
+CurvilinearCSolver mirror).
+
+  * FP64 path vs the reference solver's own output (golden fixtures, 3-5 steps
+    of every RK scheme, both compact schemes, both filters, Vreman with and
+    without LOCAL averaging, sub-step filtering, non-cubic grids):
+    max error <= 1e-12 relative per conserved field.
+  * FP64 path vs the oracle after 10 steps of the 64^3-class HIT set-up
+    (PADE6 / RK4 / COMPACT10 alpha_f = 0.49) on 16^3: <= 1e-12 relative.
+  * General (non-constant) metric fields vs the oracle: <= 1e-12.
+  * FP32-bulk vs FP64 on 32^3 HIT after 20 LSLDDRK4 steps: relative L2 per
+    field <= 1e-5 (the error target stated for the FP32 path).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import mpi_3dcompact_b200 as m
+from oracle import mc3d_oracle as O
+from tests import helpers as H
+from tests.golden import gen_golden as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _opts(cfg: O.Config, precision=m.FP64):
+    return m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                     ts_type=cfg.ts_type, cfl=cfg.cfl, dt=cfg.dt, filter_step=cfg.filter_step,
+                     substep_filtering=cfg.substep_filtering, les=cfg.les, les_avg=cfg.les_avg,
+                     precision=precision)
+
+
+def _run(cfg, ic, n, precision=m.FP64, metrics=None):
+    s = m.CurvilinearCSolver(_opts(cfg, precision))
+    if metrics is None:
+        s.set_box_metrics(2.0 * math.pi)
+    else:
+        s.set_metrics(metrics)
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    q = s.conserved()
+    return q, s.info(), s
+
+
+@pytest.mark.parametrize("name", list(G.STEP_CASES))
+def test_fp64_matches_reference_solver(name):
+    cfg, ic, n = H.oracle_config(name)
+    q, info, _ = _run(cfg, ic, n)
+    gold = H.golden_steps()
+    for i in range(5):
+        err = H.rel_max(q[i], gold[f"{name}_q{i}"])
+        assert err <= 1e-12, (name, i, err)
+    ts, t, dt = gold[f"{name}_info"]
+    assert info["time_step"] == int(ts)
+    assert abs(info["time"] - t) <= 1e-12 * abs(t)
+    assert abs(info["dt"] - dt) <= 1e-12 * abs(dt)
+
+
+def test_fp64_hit_10_steps_vs_oracle():
+    cfg = O.Config(N=(16, 16, 16), fd=("PADE6",) * 3, filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=0.002)
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    ic = hit_initial_condition(16, k0=4.0, seed=1, mt=0.3)
+    q, info, _ = _run(cfg, ic, 10)
+    qo, st = O.run(cfg, ic, 10)
+    for i in range(5):
+        assert H.rel_max(q[i], qo[i]) <= 1e-12, i
+        assert H.rel_l2(q[i], qo[i]) <= 1e-12, i
+    assert info["time_step"] == st.time_step == 10
+    assert info["stages"] == 40
+
+
+def test_general_metrics_vs_oracle():
+    """Non-constant metric fields exercise the per-point metric path."""
+    cfg = O.Config(N=(16, 14, 12), fd=("PENTA10", "PADE6", "PADE6"), filter="COMPACT8", alphaF=0.45, rk="KENRK4",
+                   les="VREMAN", mu_ref=0.003)
+    met = O.cube_metrics(cfg.N)
+    Nx, Ny, Nz = cfg.N
+    z, y, x = np.meshgrid(np.arange(Nz) / Nz, np.arange(Ny) / Ny, np.arange(Nx) / Nx, indexing="ij")
+    bump = 1.0 + 0.05 * np.sin(2 * math.pi * x) * np.cos(2 * math.pi * y) * np.sin(2 * math.pi * z + 0.3)
+    met = [met[0] * bump] + [mm + 0.01 * np.sin(2 * math.pi * (x + 2 * y)) * (c % 4 == 0) for c, mm in
+                             enumerate(met[1:], start=1)]
+    ic = G.step_ic(cfg.N, 11)
+    q, info, _ = _run(cfg, ic, 3, metrics=met)
+    qo, st = O.run(cfg, ic, 3, metrics=met)
+    for i in range(5):
+        assert H.rel_max(q[i], qo[i]) <= 1e-12, i
+
+
+def test_fp32bulk_vs_fp64():
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    cfg = O.Config(N=(32, 32, 32), fd=("PENTA10",) * 3, filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4",
+                   les="VREMAN", mu_ref=0.001)
+    ic = hit_initial_condition(32, k0=4.0, seed=2, mt=0.3)
+    q64, _, _ = _run(cfg, ic, 20, precision=m.FP64)
+    q32, _, _ = _run(cfg, ic, 20, precision=m.FP32BULK)
+    for i in range(5):
+        # momenta have zero mean: compare against the field's own scale
+        assert H.rel_l2(q32[i], q64[i]) <= 1e-5, (i, H.rel_l2(q32[i], q64[i]))
+
+
+def test_mass_is_conserved():
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    cfg = O.Config(N=(24, 24, 24), fd=("PADE6",) * 3, filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=0.002)
+    ic = hit_initial_condition(24, k0=4.0, seed=3, mt=0.3)
+    s = m.CurvilinearCSolver(_opts(cfg))
+    s.set_box_metrics(2 * math.pi)
+    s.set_initial_conditions(*ic)
+    ke0, m0 = s.integrals()
+    s.step(5)
+    ke1, m1 = s.integrals()
+    assert abs(m1 - m0) <= 1e-12 * m0
+    assert 0 < ke1 < ke0          # decaying turbulence
+
+
+def test_solver_rejects_unsupported_configs():
+    with pytest.raises(m.Mc3dError):
+        m.CurvilinearCSolver(m.Options(grid=16, les="DSM"))
+    with pytest.raises(m.Mc3dError):
+        m.CurvilinearCSolver(m.Options(grid=(16, 16, 8)))

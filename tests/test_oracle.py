@@ -1,0 +1,115 @@
+"""CPU tests of the oracle: the numpy restatement against golden fixtures made
+by the reference solver itself (tests/golden/gen_golden.py), operator
+known-answer tests, and a live comparison with oracle/_ref when it is built."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import mc3d_oracle as O
+from oracle import ref_runner as R
+from tests import helpers as H
+from tests.golden import gen_golden as G
+
+
+@pytest.mark.parametrize("bname", list(G.OPS_BCS))
+@pytest.mark.parametrize("op", G.OPS)
+def test_oracle_ops_match_reference_fixtures(op, bname):
+    gold = H.golden_ops()
+    f = G.ops_input()
+    bcs = G.OPS_BCS[bname]
+    for d in range(3):
+        ref = gold[f"{op}_{bname}_{d}"]
+        if op in ("COMPACT8", "COMPACT10"):
+            out = O.filt(f, d, op, G.OPS_ALPHA, bcs)
+        else:
+            n = G.OPS_GRID[d]
+            dh = 1.0 / n if bcs[d] == 0 else 1.0 / (n - 1.0)
+            out = O.deriv(f, d, op, bcs[d], dh)
+        # the restatement follows the reference's arithmetic order: bit-identical
+        assert np.array_equal(out, ref), (op, bname, d, H.rel_max(out, ref))
+
+
+@pytest.mark.parametrize("name", list(G.STEP_CASES))
+def test_oracle_steps_match_reference_fixtures(name):
+    cfg, ic, n = H.oracle_config(name)
+    q, st = O.run(cfg, ic, n)
+    gold = H.golden_steps()
+    for i in range(5):
+        assert H.rel_max(q[i], gold[f"{name}_q{i}"]) < 1e-13, (name, i)
+    ts, t, dt = gold[f"{name}_info"]
+    assert st.time_step == int(ts)
+    assert abs(st.time - t) <= 1e-13 * abs(t)
+    assert abs(st.dt - dt) <= 1e-13 * abs(dt)
+
+
+def test_pade6_modified_wavenumber():
+    """Known answer: d/dx sin(kx) for the periodic Pade6 scheme equals
+    k'(k) cos(kx) with Lele's modified wavenumber (interior alpha=1/3,
+    a=14/9, b=1/9; src/Pade6.hpp:70-75)."""
+    n, k = 32, 3
+    x = np.arange(n) / n
+    f = np.sin(2 * math.pi * k * x)[None, None, :] * np.ones((2, 2, 1))
+    out = O.deriv(f, 0, "PADE6", O.PERIODIC, 1.0 / n)
+    w = 2 * math.pi * k / n
+    kp = (14 / 9 * math.sin(w) + 1 / 9 / 2 * math.sin(2 * w)) / (1 + 2 / 3 * math.cos(w)) * n
+    assert np.allclose(out[0, 0], kp * np.cos(2 * math.pi * k * x), atol=1e-12)
+
+
+def test_filter_transfer_function():
+    """Known answer: the periodic compact filter scales sin(kx) by its transfer
+    function T(w) = sum_k a_k cos(kw) / (1 + 2 alpha cos w) and removes the
+    Nyquist mode (src/Compact10Filter.hpp:58-63)."""
+    n, af = 32, 0.45
+    x = np.arange(n) / n
+    for ftype in ("COMPACT8", "COMPACT10"):
+        a, _ = O.compact10_coeffs(af) if ftype == "COMPACT10" else O.compact8_coeffs(af)
+        for k in (2, 5, 9):
+            f = np.sin(2 * math.pi * k * x)[None, None, :] * np.ones((1, 1, 1))
+            out = O.filt(f, 0, ftype, af, (0, 0, 0))
+            w = 2 * math.pi * k / n
+            T = sum(a[m] * math.cos(m * w) for m in range(len(a))) / (1 + 2 * af * math.cos(w))
+            assert np.allclose(out[0, 0], T * f[0, 0], atol=1e-13)
+        nyq = np.cos(math.pi * np.arange(n))[None, None, :]
+        assert np.max(np.abs(O.filt(nyq, 0, ftype, af, (0, 0, 0)))) < 1e-12
+
+
+def test_cube_metrics_match_reference_metrics():
+    if not R.available():
+        pytest.skip("oracle/_ref not built")
+    cfg = O.Config(N=(12, 12, 12))
+    ref = R.run_metrics(cfg)
+    for a, b in zip(ref, O.cube_metrics(cfg.N)):
+        assert np.max(np.abs(a - b)) < 1e-13
+
+
+def test_oracle_live_reference_run():
+    """Live check against the reference binary on a fresh configuration."""
+    if not R.available():
+        pytest.skip("oracle/_ref not built")
+    cfg = O.Config(N=(12, 12, 12), fd=("PENTA10",) * 3, filter="COMPACT10", alphaF=0.4, rk="KENRK4",
+                   mu_ref=0.002, cfl=0.4)
+    ic = G.step_ic((12, 12, 12), 9)
+    ref, info = R.run_solver(cfg, ic, 4)
+    q, st = O.run(cfg, ic, 4)
+    for i in range(5):
+        assert H.rel_max(q[i], ref[i]) < 1e-13
+    assert st.time_step == info["time_step"]
+
+
+def test_hit_ic_is_seeded_and_solenoidal():
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    a = hit_initial_condition(16, k0=4.0, seed=3, mt=0.3)
+    b = hit_initial_condition(16, k0=4.0, seed=3, mt=0.3)
+    c = hit_initial_condition(16, k0=4.0, seed=4, mt=0.3)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert not np.array_equal(a[1], c[1])
+    u, v, w = a[1], a[2], a[3]
+    assert abs(math.sqrt(np.mean(u * u + v * v + w * w)) - 0.3) < 1e-12
+    # spectral divergence of the generated field is at round-off level
+    n = 16
+    k = np.fft.fftfreq(n, d=1.0 / n)
+    div = (1j * k[None, None, :] * np.fft.fftn(u) + 1j * k[None, :, None] * np.fft.fftn(v)
+           + 1j * k[:, None, None] * np.fft.fftn(w))
+    assert np.max(np.abs(div)) / np.max(np.abs(np.fft.fftn(u))) < 1e-10
