@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Throughput of the CurvilinearCSolver time step on B200: grid-point RK stages
+per second for decaying HIT on a 256^3 periodic box (Penta10 derivatives,
+Compact8 filter alpha_f = 0.45, LSLDDRK4, Vreman SGS), FP32-bulk arithmetic
+with FP64 state/accumulators, next to the FP64 GPU path on the same input.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one time step of the solver (LSLDDRK4 alternates 5- and
+6-stage halves; the metric counts the stages actually run). N > 1 runs
+independent replicas (one per rank, different seeds): the path has no
+exchange between GPUs. Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt RK stages/s, 256^3: FP32 vs FP64 GPU; learned SGS vs DSM at stated error"
+UNIT = "grid-pt RK stages/s"
+GRID = 256
+K0, MT, RE_LAMBDA = 4.0, 0.3, 100.0
+SCHEME = dict(fd="PENTA10", filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4", les="VREMAN", les_avg="NONE", cfl=0.5)
+WORKLOAD = ("decaying HIT 256^3 periodic box 2*pi, PENTA10 derivatives, COMPACT8 filter alpha_f=0.45 every step, "
+            "LSLDDRK4, VREMAN SGS, CFL 0.5, Mt=0.3, Re_lambda~100, FP32-bulk (FP64 state, RK registers, dt/time)")
+CPU_SAMPLE_GRID = 64
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def lsldd_stages(first_step: int, nsteps: int) -> int:
+    """Stages of LSLDDRK4 steps first_step..first_step+nsteps-1 (1-based): odd
+    steps run the 5-stage half, even steps the 6-stage half."""
+    return sum(5 if (s % 2) == 1 else 6 for s in range(first_step, first_step + nsteps))
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the line-solve kernel from the committed ncu
+    summary (a line `traffic_bytes_per_launch: <float>`), else None."""
+    p = os.path.join(ROOT, "profiles", "sweep_linesolve_hit256_fp32.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+-]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_id), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def mu_for(ic):
+    from mpi_3dcompact_b200.hit_ic import reynolds_lambda_mu
+    up, lam = reynolds_lambda_mu(ic)
+    return up * lam / RE_LAMBDA
+
+
+def cpu_reference_rate(grid, steps, warmup):
+    """The reference's own C++ time step (oracle/_ref/mc3d_ref, one core) on a
+    `grid`^3 sample of the same scheme; returns (pt-stages/s, sample text, kind)."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    from oracle import mc3d_oracle as O
+    from oracle import ref_runner as R
+    ic = hit_initial_condition(grid, k0=K0, seed=1, mt=MT)
+    cfg = O.Config(N=(grid,) * 3, fd=(SCHEME["fd"],) * 3, filter=SCHEME["filter"], alphaF=SCHEME["alphaF"],
+                   rk=SCHEME["rk"], les=SCHEME["les"], les_avg=SCHEME["les_avg"], cfl=SCHEME["cfl"],
+                   mu_ref=mu_for(ic))
+    total = warmup + steps
+    if R.available():
+        _, info = R.run_solver(cfg, ic, total)
+        st = info["step_s"][warmup:total]
+        kind = "reference"
+    else:   # the numpy restatement when the reference binary is not built
+        o = O.Oracle(cfg, O.cube_metrics(cfg.N))
+        o.init(*ic)
+        st = []
+        for i in range(total):
+            t0 = time.perf_counter()
+            o.step()
+            if i >= warmup:
+                st.append(time.perf_counter() - t0)
+        kind = "port"
+    stages = lsldd_stages(warmup + 1, steps)
+    rate = grid ** 3 * stages / sum(st)
+    sample = (f"{grid}^3 box, same scheme, {steps} timed time steps ({stages} RK stages) after {warmup} warm-up, "
+              f"1 core")
+    return rate, sample, kind, sum(st)
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = max(args.warmup, 1)
+    rate, sample, kind, secs = cpu_reference_rate(CPU_SAMPLE_GRID, args.steps, w)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": w, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded HIT IC)",
+        "config": {"workload": WORKLOAD.replace("FP32-bulk (FP64 state, RK registers, dt/time)", "FP64"),
+                   "sample_grid": CPU_SAMPLE_GRID, "parallelism": "single rank"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import mpi_3dcompact_b200 as m
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    n = args.grid
+    ic = hit_initial_condition(n, k0=K0, seed=1 + rank, mt=MT)
+    mu = mu_for(ic)
+
+    def make(precision):
+        s = m.CurvilinearCSolver(m.Options(grid=n, mu_ref=mu, precision=precision, **SCHEME), device=local)
+        s.set_box_metrics(2 * math.pi)
+        s.set_initial_conditions(*ic)
+        return s
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(s, steps, warmup, with_timing):
+        s.step(warmup)
+        s.sync()
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st0 = s.info()["stages"]
+        l0 = s.launch_count()
+        if with_timing:
+            s.set_timing(True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        rep = s.timing_report() if with_timing else None
+        if with_timing:
+            s.set_timing(False)
+        return ms, s.info()["stages"] - st0, s.launch_count() - l0, rep
+
+    gpu_id = local
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        gpu_id = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+    except Exception:
+        pass
+    clocks = ClockSampler(gpu_id)
+
+    # ---- FP32-bulk, device-resident (the headline value) ----
+    s32 = make(m.FP32BULK)
+    clocks.start()
+    ms, stages, launches, rep = timed(s32, args.steps, args.warmup, True)
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = float(n) ** 3
+    value = ws * pts * stages / (ms * 1e-3)
+    q32 = s32.conserved()
+    del s32
+
+    # ---- FP64 GPU path on the same input ----
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        s64 = make(m.FP64)
+        ms64, st64, _, _ = timed(s64, args.steps, args.warmup, False)
+        q64 = s64.conserved()
+        del s64
+        fp64 = pts * st64 / (ms64 * 1e-3)
+        names = ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]
+        err = {nm: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for nm, a, b in zip(names, q32, q64)}
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        se = m.CurvilinearCSolver(m.Options(grid=n, mu_ref=mu, precision=m.FP32BULK, **SCHEME), device=local)
+        se.set_box_metrics(2 * math.pi)
+        host_ic = [np.ascontiguousarray(a) for a in ic]
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        se.set_initial_conditions(*host_ic)          # host -> device (FP64 primitives)
+        for _ in range(args.steps):
+            se.step(1)
+            se.info()                                # per-step device -> host read of time step / dt
+        out = se.conserved()                         # device -> host (FP64 conserved state)
+        wall = time.perf_counter() - t0
+        barrier()
+        st_e = se.info()["stages"]
+        del se
+        if dist is not None:
+            t = torch.tensor([wall], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": ws * pts * st_e / wall, "unit": UNIT,
+               "h2d_bytes_per_step": int(5 * 8 * pts / args.steps),
+               "d2h_bytes_per_step": int(5 * 8 * pts / args.steps + 32)}
+        del out
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        rate, sample, kind, _ = cpu_reference_rate(CPU_SAMPLE_GRID, 2, 0)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample}
+
+    peak, peak_kind = hbm_peak()
+    sw = rep.get("sweep_linesolve", {}) if rep else {}
+    roof = None
+    if sw:
+        per_launch_bytes = sw["bytes"] / sw["launches"]
+        per_launch_s = sw["ms"] * 1e-3 / sw["launches"]
+        achieved = per_launch_bytes / per_launch_s / 1e9
+        tr = profile_traffic()
+        roof = {"bound": "hbm", "kernel": "sweep_linesolve (compact line solve, all directions/epilogues)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": tr, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "kernel_share": sw["ms"] / sum(v["ms"] for v in rep.values())}
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded HIT initial condition, k0=4, Mt=0.3)",
+        "config": {"workload": WORKLOAD, "grid": n, "stages_timed": stages,
+                   "l2": "inputs larger than L2: 40 resident fields of 64-128 MB", "parallelism":
+                   "replicas" if ws > 1 else "single GPU"},
+        "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
+        "fp32_vs_fp64_rel_l2": err,
+        "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

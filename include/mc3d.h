@@ -173,6 +173,14 @@ int mc3d_solver_stream(mc3d_solver s, void **stream);
 int mc3d_solver_launch_count(mc3d_solver s, long long *count);
 int mc3d_solver_sync(mc3d_solver s);
 
+/* Optional CUDA-event timing of every kernel the solver launches, grouped by
+ * kernel class. Enabling clears earlier records. The report is a JSON object
+ * {"class": {"launches": L, "ms": T, "bytes": B}, ...} with B the algorithmic
+ * bytes those launches must move; the string is owned by the solver and valid
+ * until the next call (synchronises). */
+int mc3d_solver_set_timing(mc3d_solver s, int enable);
+const char *mc3d_solver_timing_report(mc3d_solver s);
+
 /* ---- host utilities ---- */
 /* The combined-LCG shuffle generator of the reference's HIT IC generator
  * (tests/hit/generate_init_hit.f90:16-81). state[0..2] = ix1..ix3 and

@@ -260,3 +260,13 @@ class CurvilinearCSolver:
 
     def sync(self):
         N.check(N.host_lib().mc3d_solver_sync(self._h))
+
+    def set_timing(self, enable=True):
+        N.check(N.host_lib().mc3d_solver_set_timing(self._h, int(bool(enable))))
+
+    def timing_report(self):
+        import json
+        r = N.host_lib().mc3d_solver_timing_report(self._h)
+        if r is None:
+            N.check(2)
+        return json.loads(r.decode())

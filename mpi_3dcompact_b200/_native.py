@@ -80,6 +80,8 @@ def host_lib():
             "mc3d_solver_stream": (ip, [vp, C.POINTER(vp)]),
             "mc3d_solver_launch_count": (ip, [vp, C.POINTER(C.c_longlong)]),
             "mc3d_solver_sync": (ip, [vp]),
+            "mc3d_solver_set_timing": (ip, [vp, ip]),
+            "mc3d_solver_timing_report": (C.c_char_p, [vp]),
             "mc3d_hit_randvec": (ip, [C.POINTER(C.c_int), C.POINTER(dp), C.c_longlong, C.POINTER(dp)]),
         }
         for name, (res, args) in sigs.items():

@@ -11,6 +11,7 @@
 //   RK register update                                    (RK4.hpp, LSLDDRK4.hpp, ...)
 //   filter (last stage or every stage)                   (Core.cpp:949-1155)
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -42,9 +43,39 @@ struct mc3d_solver_s {
     long long launches = 0;
     bool initialized = false;
     std::vector<void *> allocs;
+    // optional per-kernel-class CUDA-event timing (mc3d_solver_set_timing)
+    bool timing = false;
+    struct Rec { int cls; size_t ev; double bytes; };
+    std::vector<cudaEvent_t> events;
+    std::vector<Rec> recs;
+    size_t ev_used = 0;
+    std::string report;
 };
 
 namespace mc3d {
+
+// kernel classes for the optional event timing
+enum KClass { KC_SWEEP = 0, KC_FLUX, KC_PRIM, KC_RK, KC_CFL, KC_TOREAL, KC_VREMAN, KC_COUNT };
+static const char *KC_NAME[KC_COUNT] = {"sweep_linesolve", "flux", "primitives", "rk_update", "cfl_dt", "to_fp32",
+                                        "vreman"};
+
+static int tic(mc3d_solver s, int cls, double bytes) {
+    if (!s->timing) return MC3D_OK;
+    while (s->events.size() < s->ev_used + 2) {
+        cudaEvent_t e;
+        MC3D_CUDA_TRY(cudaEventCreate(&e));
+        s->events.push_back(e);
+    }
+    MC3D_CUDA_TRY(cudaEventRecord(s->events[s->ev_used], s->stream));
+    s->recs.push_back({cls, s->ev_used, bytes});
+    s->ev_used += 2;
+    return MC3D_OK;
+}
+static int toc(mc3d_solver s) {
+    if (!s->timing) return MC3D_OK;
+    MC3D_CUDA_TRY(cudaEventRecord(s->events[s->recs.back().ev + 1], s->stream));
+    return MC3D_OK;
+}
 
 static const double RK4_A[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 static const double RK4_B[3] = {1.0 / 2.0, 1.0 / 2.0, 1.0};
@@ -108,7 +139,18 @@ static int sweep(mc3d_solver s, int dir, const LineOpBuf &op, int nf, const void
     rf.Jc = (R)s->met_c[0];
     rf.quirk = s->cfg.reference_quirks;
     s->launches++;
-    return launch_sweep<R>(dir, s->g, opdev<R>(op), b, epi, rf, s->cfg.bc_type, filter, s->stream);
+    // algorithmic bytes: every field read once and written once, plus the
+    // epilogue's extra operands (partial RHS, previous k2, FP64 store)
+    double per = 2.0 * sizeof(R);
+    if (epi == EPI_SUB) per = 3.0 * sizeof(R);
+    if (epi == EPI_STORE_F64) per = sizeof(R) + 8.0;
+    double bytes = per * nf * (double)s->g.n();
+    if (epi == EPI_RHS_FINAL) bytes = (3.0 * nf + (s->cfg.reference_quirks ? 3.0 : 0.0)) * sizeof(R) * (double)s->g.n();
+    int rc = tic(s, KC_SWEEP, bytes);
+    if (rc) return rc;
+    rc = launch_sweep<R>(dir, s->g, opdev<R>(op), b, epi, rf, s->cfg.bc_type, filter, s->stream);
+    if (rc) return rc;
+    return toc(s);
 }
 
 // Three directional filter sweeps in the rotating order of
@@ -125,7 +167,9 @@ static int filter_state(mc3d_solver s, double *const in[5], double *const out[5]
         R *dst[5];
         for (int v = 0; v < 5; v++) dst[v] = (R *)s->tC[v];
         s->launches++;
+        if ((rc = tic(s, KC_TOREAL, (8.0 + sizeof(R)) * 5 * (double)s->g.n()))) return rc;
         if ((rc = launch_to_real<R>(s->g, in, dst, s->stream))) return rc;
+        if ((rc = toc(s))) return rc;
         for (int v = 0; v < 5; v++) src0[v] = s->tC[v];
     }
     if ((rc = sweep<R>(s, order[0], ops[order[0]], 5, src0, s->tA, EPI_STORE, nullptr, nullptr, true))) return rc;
@@ -165,7 +209,9 @@ static int stage_rhs(mc3d_solver s, double *const qP[5]) {
     R *prim[4];
     for (int v = 0; v < 4; v++) prim[v] = (R *)s->prim[v];
     s->launches++;
+    if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 4.0 * sizeof(R)) * (double)s->g.n()))) return rc;
     if ((rc = launch_primitives<R>(s->g, qP, prim, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
     // gradients of U, V, W, T in each direction: der[3*var + dir]
     for (int d = 0; d < 3; d++) {
         void *out[4] = {s->der[0 + d], s->der[3 + d], s->der[6 + d], s->der[9 + d]};
@@ -185,7 +231,9 @@ static int stage_rhs(mc3d_solver s, double *const qP[5]) {
         } else {
             // mu_sgs, then doAveraging LOCAL: Compact10(-0.49) along Y, Z, X (AbstractSGS.cpp:144-152)
             s->launches++;
+            if ((rc = tic(s, KC_VREMAN, (8.0 + 10.0 * sizeof(R)) * (double)s->g.n()))) return rc;
             if ((rc = launch_vreman<R>(s->g, qP, dd, m, fp, (R *)s->mu_sgs, s->stream))) return rc;
+            if ((rc = toc(s))) return rc;
             void *a[1] = {s->mu_sgs}, *t1[1] = {s->tA[0]}, *t2[1] = {s->tB[0]};
             if ((rc = sweep<R>(s, 1, s->vop[1], 1, a, t1, EPI_STORE, nullptr, nullptr, true))) return rc;
             if ((rc = sweep<R>(s, 2, s->vop[2], 1, t1, t2, EPI_STORE, nullptr, nullptr, true))) return rc;
@@ -196,7 +244,12 @@ static int stage_rhs(mc3d_solver s, double *const qP[5]) {
     R *F[15];
     for (int i = 0; i < 15; i++) F[i] = (R *)s->flux[i];
     s->launches++;
+    {
+        double b = 5.0 * 8 + (12.0 + 15.0) * sizeof(R) + (fp.les == 2 ? sizeof(R) : 0) + (s->const_met ? 0 : 10.0 * sizeof(R));
+        if ((rc = tic(s, KC_FLUX, b * (double)s->g.n()))) return rc;
+    }
     if ((rc = launch_flux<R>(s->g, qP, dd, m, fp, (const R *)s->mu_sgs, F, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
     // divergence of the contravariant fluxes, accumulated into the RHS, then k2
     if ((rc = sweep<R>(s, 0, s->dop[0], 5, s->flux + 0, s->rhs, EPI_STORE_NEG, nullptr, nullptr, false))) return rc;
     if ((rc = sweep<R>(s, 1, s->dop[1], 5, s->flux + 5, s->rhs, EPI_SUB, nullptr, nullptr, false))) return rc;
@@ -210,9 +263,11 @@ static int one_step(mc3d_solver s) {
     // preStep: calcDtFromCFL on the current state (Core.cpp:189-237)
     Metrics<R> m = metrics_of<R>(s);
     s->launches += 2;
+    if ((rc = tic(s, KC_CFL, 5.0 * 8 * (double)s->g.n()))) return rc;
     if ((rc = launch_cfl<R>(s->g, s->q1, m, s->dxi, &s->ts->umax_bits, s->stream))) return rc;
     int first = s->host_time_step == s->cfg.time_step0;
     if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
     s->host_time_step++;
 
     int scheme = s->cfg.rk_type;
@@ -237,7 +292,16 @@ static int one_step(mc3d_solver s) {
         const R *k2[5];
         for (int v = 0; v < 5; v++) k2[v] = (const R *)s->k2[v];
         s->launches++;
+        {
+            // reads k2 and the FP64 registers the scheme touches, writes the updated ones
+            double b = 5.0 * sizeof(R);
+            if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
+            else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
+            else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
+            if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
+        }
         if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, s->stream))) return rc;
+        if ((rc = toc(s))) return rc;
         bool last = st == ns;
         if (last || s->cfg.substep_filtering)
             if ((rc = filter_conserved<R>(s, last))) return rc;
@@ -337,6 +401,7 @@ int mc3d_solver_destroy(mc3d_solver s) {
     if (!s) return MC3D_OK;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->events) cudaEventDestroy(e);
     for (void *p : s->allocs) cudaFree(p);
     for (int d = 0; d < 3; d++) {
         free_line_op(s->dop[d]);
@@ -518,6 +583,50 @@ int mc3d_solver_launch_count(mc3d_solver s, long long *count) {
     if (!s || !count) return fail(MC3D_ERR_ARG, "null argument");
     *count = s->launches;
     return MC3D_OK;
+}
+
+int mc3d_solver_set_timing(mc3d_solver s, int enable) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->timing = enable != 0;
+    s->recs.clear();
+    s->ev_used = 0;
+    return MC3D_OK;
+}
+
+const char *mc3d_solver_timing_report(mc3d_solver s) {
+    if (!s) {
+        fail(MC3D_ERR_ARG, "null solver");
+        return nullptr;
+    }
+    cudaSetDevice(s->device);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        fail(MC3D_ERR_CUDA, "stream synchronisation failed");
+        return nullptr;
+    }
+    double ms[KC_COUNT] = {0}, by[KC_COUNT] = {0};
+    long long cnt[KC_COUNT] = {0};
+    for (const auto &r : s->recs) {
+        float t = 0;
+        if (cudaEventElapsedTime(&t, s->events[r.ev], s->events[r.ev + 1]) != cudaSuccess) continue;
+        ms[r.cls] += t;
+        by[r.cls] += r.bytes;
+        cnt[r.cls]++;
+    }
+    std::string o = "{";
+    char buf[256];
+    bool firstk = true;
+    for (int c = 0; c < KC_COUNT; c++) {
+        if (!cnt[c]) continue;
+        snprintf(buf, sizeof(buf), "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"bytes\": %.6e}", firstk ? "" : ", ",
+                 KC_NAME[c], cnt[c], ms[c], by[c]);
+        o += buf;
+        firstk = false;
+    }
+    o += "}";
+    s->report = o;
+    return s->report.c_str();
 }
 
 int mc3d_solver_sync(mc3d_solver s) {

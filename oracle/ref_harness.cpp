@@ -46,9 +46,12 @@ using namespace std;
 #include "KenRK4.hpp"
 #include "LSLDDRK4.hpp"
 
+// wall-clock stamp at the end of every time step (postStep -> fullStepTemporalHook)
+static std::vector<double> g_step_stamps;
+
 // ---- solver hooks (the reference leaves their bodies to the driver) ----
 void CurvilinearCSolver::initialHook() {}
-void CurvilinearCSolver::fullStepTemporalHook() {}
+void CurvilinearCSolver::fullStepTemporalHook() { g_step_stamps.push_back(MPI_Wtime()); }
 void CurvilinearCSolver::subStepTemporalHook() {}
 void CurvilinearCSolver::preStepBoundaryHook() {}
 void CurvilinearCSolver::postStepBoundaryHook() {}
@@ -212,6 +215,17 @@ static int mode_run(const string &mesh, const string &icpath, const string &out)
     rk->executeSolverLoop();
     double t1 = MPI_Wtime();
     fprintf(stderr, "mc3d_ref: wall %.6f s for %d steps\n", t1 - t0, cs->timeStep);
+    {
+        FILE *st = fopen("step_times.txt", "w");
+        if (st) {
+            double prev = t0;
+            for (double s : g_step_stamps) {
+                fprintf(st, "%.9f\n", s - prev);
+                prev = s;
+            }
+            fclose(st);
+        }
+    }
 
     double hdr[8] = {(double)cs->timeStep, cs->time, (double)Nx, (double)Ny, (double)Nz, s.ts->dt, t1 - t0, 0.0};
     vector<double *> f = {cs->rho1, cs->rhoU1, cs->rhoV1, cs->rhoW1, cs->rhoE1};

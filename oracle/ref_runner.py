@@ -113,7 +113,10 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600):
         if r.returncode != 0:
             raise RuntimeError("mc3d_ref failed: " + r.stderr[-2000:] + r.stdout[-2000:])
         hdr, fields = _read_fields(os.path.join(d, "out.bin"), cfg.N, 5)
-    info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall}
+        st = os.path.join(d, "step_times.txt")
+        step_s = [float(x) for x in open(st).read().split()] if os.path.exists(st) else []
+    info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall,
+            "step_s": step_s}
     return fields, info
 
 
