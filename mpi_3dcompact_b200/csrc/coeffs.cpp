@@ -4,6 +4,7 @@
 // The factors are produced by the same elimination sequence the reference
 // runs on every call (src/Utils.cpp:4-191), once per operator instead of once
 // per line: the GPU line solve then only replays the RHS-dependent half.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -363,8 +364,110 @@ LineOpHost build_filter_op(int filter_type, double af, int bc_type, int N) {
 }
 
 namespace {
+// Stationary interior of the factor arrays and the correction window.
+void analyse(LineOpHost &h) {
+    int n = h.N;
+    size_t na = h.arr.size() / (n ? n : 1);
+    int nfac = h.kind == K_TRI_PER || h.kind == K_TRI_DIR ? 3 : (h.kind == K_PEN_PER || h.kind == K_PEN_DIR ? 5 : 0);
+    h.stat_lo = h.stat_hi = 0;
+    if (nfac && na >= (size_t)nfac) {
+        // largest run [lo, hi) with all factor arrays (and a1[n-1]) constant
+        auto at = [&](int a, int i) { return h.arr[(size_t)a * n + i]; };
+        int best_lo = 0, best_hi = 0, lo = 1;
+        for (int i = 1; i < n; i++) {
+            bool same = true;
+            for (int a = 0; a < nfac && same; a++) same = at(a, i) == at(a, lo);
+            same = same && at(1, i - 1) == at(1, lo);
+            if (!same) lo = i;
+            if (i + 1 - lo > best_hi - best_lo) { best_lo = lo; best_hi = i + 1; }
+        }
+        if (best_hi - best_lo >= 16 && best_lo >= 2) {
+            h.stat_lo = best_lo;
+            h.stat_hi = best_hi;
+            for (int a = 0; a < nfac; a++) h.stat_c[a] = at(a, best_lo);
+        }
+    }
+    h.corr_lo = h.corr_hi = 0;
+    int first = -1, ncol = h.kind == K_TRI_PER ? 1 : (h.kind == K_PEN_PER ? 4 : 0);
+    if (ncol) {
+        int base = h.kind == K_TRI_PER ? 3 : 5;
+        double peak = 0;
+        for (int c = 0; c < ncol; c++)
+            for (int i = 0; i < n; i++) peak = std::max(peak, std::fabs(h.arr[(size_t)(base + c) * n + i]));
+        const double thr = peak * std::ldexp(1.0, -64);
+        auto small = [&](int i) {
+            for (int c = 0; c < ncol; c++)
+                if (std::fabs(h.arr[(size_t)(base + c) * n + i]) > thr) return false;
+            return true;
+        };
+        for (int i = 0; i < n; i++)
+            if (small(i)) { first = i; break; }
+        if (first >= 0) {
+            int last = first;
+            while (last < n && small(last)) last++;
+            h.corr_lo = first;
+            h.corr_hi = last;
+        }
+    }
+}
+
+// Segment count and homogeneous responses for the segmented line solve.
+// tri:   forward  x_n = -m_n x_{n-1}                        from x_{a-1} = 1
+//        backward x_n = -c_n x_{n+1} rw_n                    from x_b = 1
+// penta: forward  B_n = -m2_{n-1} B_{n-2} - m1_n B_{n-1}     from (B_{a-1}, B_{a-2}) = (1,0) | (0,1)
+//        backward x_n = (-f_n x_{n+2} - C_n x_{n+1}) rD_n    from (x_b, x_{b+1}) = (1,0) | (0,1)
+void segment(LineOpHost &h) {
+    int n = h.N;
+    bool tri = h.kind == K_TRI_PER || h.kind == K_TRI_DIR;
+    bool pen = h.kind == K_PEN_PER || h.kind == K_PEN_DIR;
+    h.S = 1;
+    if (!(tri || pen)) return;
+    const int UB = 8;
+    int S = 0;
+    for (int cand : {4, 2})
+        if (n % cand == 0 && (n / cand) % UB == 0 && n / cand >= 32 && n / cand >= h.bw) { S = cand; break; }
+    if (!S) return;
+    h.S = S;
+    int L = n / S;
+    auto A = [&](int a, int i) { return h.arr[(size_t)a * n + i]; };
+    h.sfa.assign(n, 0.0);
+    h.sfb.assign(n, 0.0);
+    h.sba.assign(n, 0.0);
+    h.sbb.assign(n, 0.0);
+    for (int w = 0; w < S; w++) {
+        int a = w * L, b = a + L;
+        for (int which = 0; which < (pen ? 2 : 1); which++) {
+            // forward
+            double p1 = which == 0 ? 1.0 : 0.0, p2 = which == 0 ? 0.0 : 1.0;   // B_{n-1}, B_{n-2}
+            for (int i = a; i < b; i++) {
+                double x;
+                if (tri) x = -A(0, i) * p1;
+                else x = -(i >= 1 ? A(1, i - 1) : 0.0) * p2 - A(0, i) * p1;
+                (which == 0 ? h.sfa : h.sfb)[i] = x;
+                p2 = p1;
+                p1 = x;
+            }
+            // backward
+            double q1 = which == 0 ? 1.0 : 0.0, q2 = which == 0 ? 0.0 : 1.0;   // x_{n+1}, x_{n+2}
+            for (int i = b - 1; i >= a; i--) {
+                double x;
+                if (tri) x = (0.0 - A(2, i) * q1) * A(1, i);
+                else x = (0.0 - A(4, i) * q2 - A(3, i) * q1) * A(2, i);
+                (which == 0 ? h.sba : h.sbb)[i] = x;
+                q2 = q1;
+                q1 = x;
+            }
+        }
+    }
+}
+
 template <typename R>
 void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
+    d.stat_lo = h.stat_lo;
+    d.stat_hi = h.stat_hi;
+    d.corr_lo = h.corr_lo;
+    d.corr_hi = h.corr_hi;
+    for (int i = 0; i < 5; i++) d.stat_c[i] = (R)h.stat_c[i];
     d.N = h.N;
     d.kind = h.kind;
     d.H = h.H;
@@ -389,6 +492,12 @@ void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
     const R *q = p + h.arr.size();
     d.head = h.head.empty() ? nullptr : q;
     d.tail = h.tail.empty() ? nullptr : q + h.head.size();
+    const R *sg = q + h.head.size() + h.tail.size();
+    d.S = h.S;
+    d.sfa = h.S > 1 ? sg : nullptr;
+    d.sfb = h.S > 1 ? sg + n : nullptr;
+    d.sba = h.S > 1 ? sg + 2 * n : nullptr;
+    d.sbb = h.S > 1 ? sg + 3 * n : nullptr;
 }
 
 template <typename R>
@@ -398,12 +507,18 @@ std::vector<R> flatten(const LineOpHost &h) {
     for (double x : h.arr) v.push_back((R)x);
     for (double x : h.head) v.push_back((R)x);
     for (double x : h.tail) v.push_back((R)x);
+    if (h.S > 1)
+        for (const std::vector<double> *a : {&h.sfa, &h.sfb, &h.sba, &h.sbb})
+            for (double x : *a) v.push_back((R)x);
     if (v.empty()) v.push_back((R)0);
     return v;
 }
 }  // namespace
 
-int upload_line_op(const LineOpHost &h, int precision, LineOpBuf &out) {
+int upload_line_op(const LineOpHost &hin, int precision, LineOpBuf &out) {
+    LineOpHost h = hin;
+    analyse(h);
+    segment(h);
     out.precision = precision;
     MC3D_CUDA_TRY(cudaGetDevice(&out.device));
     if (precision == MC3D_FP64) {

@@ -42,6 +42,19 @@ struct LineOpHost {
     double sc[4] = {0};   // kind-specific scalars
     double Hm[16] = {0};  // penta cyclic capacitance inverse
     double cp[6] = {0};   // penta cyclic corner values
+    // Rows [stat_lo, stat_hi) where every elimination factor is exactly
+    // constant (Toeplitz interior: the factors reach their fixed point a few
+    // dozen rows from the ends); stat_c holds those constants.
+    int stat_lo = 0, stat_hi = 0;
+    double stat_c[5] = {0};
+    // Rows [corr_lo, corr_hi) where the cyclic correction columns are below
+    // 2^-64 of their peak, so the correction is skipped there.
+    int corr_lo = 0, corr_hi = 0;
+    // Segmented solve: S segments of L = N/S rows per line; homogeneous
+    // responses of the local forward (to the two incoming eliminated values)
+    // and backward (to the two outgoing solution values) recurrences, per row.
+    int S = 1;
+    std::vector<double> sfa, sfb, sba, sbb;
 };
 
 LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh);
@@ -64,6 +77,10 @@ struct LineOpDev {
     const R *a3;     // tri: z  | penta: C
     const R *a4;     // penta: f
     const R *z0, *z1, *z2, *z3;   // penta cyclic Woodbury columns
+    int stat_lo, stat_hi, corr_lo, corr_hi;
+    R stat_c[5];
+    int S;                         // segments per line (1 = whole-line kernel)
+    const R *sfa, *sfb, *sba, *sbb;
 };
 
 // Device copy of an operator in one precision.

@@ -88,3 +88,36 @@ def test_operator_errors_are_reported():
     x = torch.zeros((12, 12, 12), dtype=torch.float64, device="cuda")
     with pytest.raises(m.Mc3dError):
         o.calc1stDerivField(x, x)                         # in and out alias
+
+
+@pytest.mark.parametrize("prec", [m.FP64, m.FP32BULK])
+@pytest.mark.parametrize("bc", [m.PERIODIC_SOLVE, m.DIRICHLET_SOLVE])
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_segmented_lines_vs_oracle(n, bc, prec):
+    """Lines long enough for the segmented solve (2 or 4 segments per line),
+    every operator kind, every direction, against the oracle."""
+    torch = _torch()
+    from oracle import mc3d_oracle as O
+    rng = np.random.default_rng(n + 7 * bc)
+    dt = torch.float64 if prec == m.FP64 else torch.float32
+    for d in range(3):
+        shape = [12, 20, 36]
+        shape[2 - d] = n                       # (Nz, Ny, Nx): direction d has n points
+        shape = tuple(shape)
+        f = rng.standard_normal(shape)
+        x = torch.tensor(f, dtype=dt, device="cuda")
+        bcs = [m.PERIODIC_SOLVE] * 3
+        bcs[d] = bc
+        for op in ("PADE6", "PENTA10", "COMPACT8", "COMPACT10"):
+            o = _make(op, d, bcs, shape, prec)
+            y = torch.empty_like(x)
+            if op.startswith("COMPACT"):
+                o.filterField(x, y)
+                ref = O.filt(f, d, op, G.OPS_ALPHA, tuple(bcs))
+            else:
+                o.calc1stDerivField(x, y)
+                dh = 1.0 / n if bc == m.PERIODIC_SOLVE else 1.0 / (n - 1.0)
+                ref = O.deriv(f, d, op, bc, dh)
+            torch.cuda.synchronize()
+            err = H.rel_max(y.double().cpu().numpy(), ref)
+            assert err <= TOL[prec], (op, n, d, bc, err)

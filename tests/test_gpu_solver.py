@@ -118,3 +118,17 @@ def test_solver_rejects_unsupported_configs():
         m.CurvilinearCSolver(m.Options(grid=16, les="DSM"))
     with pytest.raises(m.Mc3dError):
         m.CurvilinearCSolver(m.Options(grid=(16, 16, 8)))
+
+
+@pytest.mark.parametrize("prec,tol", [(m.FP64, 1e-12), (m.FP32BULK, 1e-5)])
+def test_64cube_two_steps_vs_oracle(prec, tol):
+    """64^3 lines take the segmented line-solve kernels in every sweep
+    (gradients, flux divergence with all epilogues, filter)."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    cfg = O.Config(N=(64, 64, 64), fd=("PENTA10",) * 3, filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4",
+                   les="VREMAN", mu_ref=0.001)
+    ic = hit_initial_condition(64, k0=4.0, seed=6, mt=0.3)
+    q, info, _ = _run(cfg, ic, 2, precision=prec)
+    qo, st = O.run(cfg, ic, 2)
+    for i in range(5):
+        assert H.rel_l2(q[i], qo[i]) <= tol, (i, H.rel_l2(q[i], qo[i]))
