@@ -148,14 +148,15 @@ struct FluxParams {
 };
 
 template <typename R>
-int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[4], cudaStream_t st);
+int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st);
 
+// prim = rho, U, V, W, T of the stage state
 template <typename R>
-int launch_flux(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+int launch_flux(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
                 const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st);
 
 template <typename R>
-int launch_vreman(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+int launch_vreman(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
                   const FluxParams &p, R *mu_sgs, cudaStream_t st);
 
 // RK register update for one stage: see rk.cu for the per-scheme formulas.
@@ -165,9 +166,10 @@ struct RkStage {
     int nstages;
     double a, b;       // scheme coefficients of this stage
 };
+// prim (optional, may be null): also write rho, U, V, W, T of the new stage state
 template <typename R>
 int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
-                     double *const qk[5], double *const q2[5], cudaStream_t st);
+                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st);
 
 template <typename R>
 int launch_to_real(const Grid3 &g, const double *const src[5], R *const dst[5], cudaStream_t st);

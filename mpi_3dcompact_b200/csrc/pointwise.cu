@@ -31,26 +31,39 @@ __device__ __forceinline__ float mu_of_T(float T, double mu_ref) { return (float
 __device__ __forceinline__ double mu_of_T(double T, double mu_ref) { return mu_ref * pow(T, 0.76); }
 
 // ---- primitives U, V, W, T (updateNonConservedData, Core.cpp:1158-1197) ----
+// rho, U, V, W, T of one point from the FP64 conserved state (solveU, solvep,
+// solveT of src/IdealGas.hpp:56-70)
 template <typename R>
-__global__ void primitives_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
-                                  const double *__restrict__ r2, const double *__restrict__ r3,
-                                  const double *__restrict__ r4, R *U, R *V, R *W, R *T) {
-    long long n = g.n();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double rho = r0[i];
-        double u = r1[i] / rho, v = r2[i] / rho, w = r3[i] / rho;
-        double p = (GAMMA - 1) * (r4[i] - 0.5 * rho * (u * u + v * v + w * w));
-        U[i] = (R)u;
-        V[i] = (R)v;
-        W[i] = (R)w;
-        T[i] = (R)(p / (rho * R_GAS));
-    }
+__device__ __forceinline__ void prims_of(double rho, double ru, double rv, double rw, double re, R *const *P,
+                                         long long i) {
+    double u = ru / rho, v = rv / rho, w = rw / rho;
+    double p = (GAMMA - 1) * (re - 0.5 * rho * (u * u + v * v + w * w));
+    P[0][i] = (R)rho;
+    P[1][i] = (R)u;
+    P[2][i] = (R)v;
+    P[3][i] = (R)w;
+    P[4][i] = (R)(p / (rho * R_GAS));
 }
 
 template <typename R>
-int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[4], cudaStream_t st) {
-    primitives_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], prim[0], prim[1],
-                                                               prim[2], prim[3]);
+struct P5 {
+    R *p[5];
+};
+
+template <typename R>
+__global__ void primitives_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
+                                  const double *__restrict__ r2, const double *__restrict__ r3,
+                                  const double *__restrict__ r4, P5<R> P) {
+    long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        prims_of<R>(r0[i], r1[i], r2[i], r3[i], r4[i], P.p, i);
+}
+
+template <typename R>
+int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st) {
+    P5<R> P;
+    for (int v = 0; v < 5; v++) P.p[v] = prim[v];
+    primitives_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], P);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -107,21 +120,22 @@ struct OutPtrs15 {
 
 // ---- fluxes: preStepDerivatives, Core.cpp:615-752 ----
 template <typename R>
-__global__ void __launch_bounds__(256) flux_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
-                                                   const double *__restrict__ r2, const double *__restrict__ r3,
-                                                   const double *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
-                                                   FluxParams fp, const R *__restrict__ mu_sgs_f, OutPtrs15 op) {
+__global__ void __launch_bounds__(256, 3) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
+                                                      const R *__restrict__ r2, const R *__restrict__ r3,
+                                                      const R *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
+                                                      FluxParams fp, const R *__restrict__ mu_sgs_f, OutPtrs15 op) {
     const R *const *d = reinterpret_cast<const R *const *>(dp.p);
     R *const *F = reinterpret_cast<R *const *>(op.p);
     const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
+    const R d1c = m.constant ? vreman_d1<R>(dvol, m.c[0]) : R(0);   // filter width of a uniform block
     long long n = g.n();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double rho_d = r0[i];
-        double Ud = r1[i] / rho_d, Vd = r2[i] / rho_d, Wd = r3[i] / rho_d;
-        double pd = (GAMMA - 1) * (r4[i] - 0.5 * rho_d * (Ud * Ud + Vd * Vd + Wd * Wd));
-        double Td = pd / (rho_d * R_GAS);
-        R rho = (R)rho_d, U = (R)Ud, V = (R)Vd, W = (R)Wd, p = (R)pd, T = (R)Td;
-        R rhoU = (R)r1[i], rhoV = (R)r2[i], rhoW = (R)r3[i], rhoE = (R)r4[i];
+        // primitives rho, U, V, W, T of the stage state; p and rhoE follow
+        // from the ideal-gas relations (src/IdealGas.hpp:64-78)
+        R rho = r0[i], U = r1[i], V = r2[i], W = r3[i], T = r4[i];
+        R p = rho * (R)R_GAS * T;
+        R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
+        R rhoE = p / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
         R mu = mu_of_T(T, fp.mu_ref);
         R J = met(m, 0, i);
         R J11 = met(m, 1, i), J12 = met(m, 2, i), J13 = met(m, 3, i);
@@ -137,7 +151,7 @@ __global__ void __launch_bounds__(256) flux_kernel(Grid3 g, const double *__rest
         R mu_eff, k_eff;
         if (fp.les) {
             R mu_sgs;
-            if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, vreman_d1<R>(dvol, J));
+            if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, m.constant ? d1c : vreman_d1<R>(dvol, J));
             else mu_sgs = mu_sgs_f[i];
             mu_eff = mu + mu_sgs;
             k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
@@ -201,7 +215,7 @@ __global__ void __launch_bounds__(256) flux_kernel(Grid3 g, const double *__rest
 }
 
 template <typename R>
-int launch_flux(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const Metrics<R> &m,
                 const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st) {
     DerivPtrs12 dp;
     for (int i = 0; i < 12; i++) dp.p[i] = d[i];
@@ -213,7 +227,7 @@ int launch_flux(const Grid3 &g, const double *const q[5], const R *const d[12], 
 }
 
 template <typename R>
-__global__ void vreman_kernel(Grid3 g, const double *__restrict__ r0, DerivPtrs12 dp, Metrics<R> m, FluxParams fp,
+__global__ void vreman_kernel(Grid3 g, const R *__restrict__ r0, DerivPtrs12 dp, Metrics<R> m, FluxParams fp,
                               R *mu_sgs) {
     const R *const *d = reinterpret_cast<const R *const *>(dp.p);
     const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
@@ -226,7 +240,7 @@ __global__ void vreman_kernel(Grid3 g, const double *__restrict__ r0, DerivPtrs1
 }
 
 template <typename R>
-int launch_vreman(const Grid3 &g, const double *const q[5], const R *const d[12], const Metrics<R> &m,
+int launch_vreman(const Grid3 &g, const R *const q[5], const R *const d[12], const Metrics<R> &m,
                   const FluxParams &p, R *mu_sgs, cudaStream_t st) {
     DerivPtrs12 dp;
     for (int i = 0; i < 12; i++) dp.p[i] = d[i];
@@ -247,54 +261,60 @@ struct K5 {
 };
 
 template <typename R>
-__global__ void rk_kernel(Grid3 g, RkStage rs, K5<R> k2, Q5 q1, Q5 qk, Q5 q2) {
+__global__ void rk_kernel(Grid3 g, RkStage rs, K5<R> k2, Q5 q1, Q5 qk, Q5 q2, P5<R> prim, int want_prims) {
     long long n = g.n();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double nk[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             double k = (double)k2.p[v][i];
+            nk[v] = 0.0;
             if (rs.scheme == MC3D_RK4) {
                 if (rs.stage == 1) {
                     double b1 = q1.p[v][i];
                     q2.p[v][i] = b1 + rs.a * k;
-                    qk.p[v][i] = b1 + rs.b * k;
+                    qk.p[v][i] = nk[v] = b1 + rs.b * k;
                 } else if (rs.stage < 4) {
                     q2.p[v][i] += rs.a * k;
-                    qk.p[v][i] = q1.p[v][i] + rs.b * k;
+                    qk.p[v][i] = nk[v] = q1.p[v][i] + rs.b * k;
                 } else {
                     q2.p[v][i] += rs.a * k;
                 }
             } else if (rs.scheme == MC3D_TVDRK3) {
-                if (rs.stage == 1) qk.p[v][i] = q1.p[v][i] + 1.0 * k;
-                else if (rs.stage == 2) qk.p[v][i] = 0.75 * q1.p[v][i] + 0.25 * qk.p[v][i] + 0.25 * k;
+                if (rs.stage == 1) qk.p[v][i] = nk[v] = q1.p[v][i] + 1.0 * k;
+                else if (rs.stage == 2) qk.p[v][i] = nk[v] = 0.75 * q1.p[v][i] + 0.25 * qk.p[v][i] + 0.25 * k;
                 else q2.p[v][i] = (1.0 / 3.0) * q1.p[v][i] + (2.0 / 3.0) * qk.p[v][i] + (2.0 / 3.0) * k;
             } else {
                 if (rs.stage == 1) {
-                    qk.p[v][i] = q1.p[v][i] + rs.b * k;
+                    qk.p[v][i] = nk[v] = q1.p[v][i] + rs.b * k;
                     q1.p[v][i] = k;
                 } else {
                     double r = k + rs.a * q1.p[v][i];
                     q1.p[v][i] = r;
-                    if (rs.stage < rs.nstages) qk.p[v][i] += rs.b * r;
+                    if (rs.stage < rs.nstages) qk.p[v][i] = nk[v] = qk.p[v][i] + rs.b * r;
                     else q2.p[v][i] = qk.p[v][i] + rs.b * r;
                 }
             }
         }
+        // primitives of the next stage state (updateNonConservedData, Core.cpp:1165-1177)
+        if (want_prims) prims_of<R>(nk[0], nk[1], nk[2], nk[3], nk[4], prim.p, i);
     }
 }
 
 template <typename R>
 int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
-                     double *const qk[5], double *const q2[5], cudaStream_t st) {
+                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st) {
     K5<R> k;
     Q5 a, b, c;
+    P5<R> P;
     for (int v = 0; v < 5; v++) {
         k.p[v] = k2[v];
         a.p[v] = q1[v];
         b.p[v] = qk[v];
         c.p[v] = q2[v];
+        P.p[v] = prim ? prim[v] : nullptr;
     }
-    rk_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rs, k, a, b, c);
+    rk_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rs, k, a, b, c, P, prim != nullptr);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -415,13 +435,13 @@ int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cud
 }
 
 #define MC3D_INST(R)                                                                                              \
-    template int launch_primitives<R>(const Grid3 &, const double *const[5], R *const[4], cudaStream_t);          \
-    template int launch_flux<R>(const Grid3 &, const double *const[5], const R *const[12], const Metrics<R> &,    \
+    template int launch_primitives<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);          \
+    template int launch_flux<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,         \
                                 const FluxParams &, const R *, R *const[15], cudaStream_t);                       \
-    template int launch_vreman<R>(const Grid3 &, const double *const[5], const R *const[12], const Metrics<R> &,  \
+    template int launch_vreman<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,       \
                                   const FluxParams &, R *, cudaStream_t);                                         \
     template int launch_rk_update<R>(const Grid3 &, const RkStage &, const R *const[5], double *const[5],         \
-                                     double *const[5], double *const[5], cudaStream_t);                           \
+                                     double *const[5], double *const[5], R *const[5], cudaStream_t);              \
     template int launch_to_real<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);             \
     template int launch_cfl<R>(const Grid3 &, const double *const[5], const Metrics<R> &, const double[3],        \
                                unsigned long long *, cudaStream_t);

@@ -27,7 +27,7 @@ struct mc3d_solver_s {
     double dxi[3] = {0, 0, 0};
     mc3d::LineOpBuf dop[3], fop[3], vop[3];
     double *q1[5] = {}, *qk[5] = {}, *q2[5] = {};
-    void *k2[5] = {}, *rhs[5] = {}, *prim[4] = {}, *der[12] = {}, *flux[15] = {};
+    void *k2[5] = {}, *rhs[5] = {}, *prim[5] = {}, *der[12] = {}, *flux[15] = {};
     void *tA[5] = {}, *tB[5] = {}, *tC[5] = {}, *mu_sgs = nullptr;
     double *met64[10] = {};
     void *metR[10] = {};
@@ -203,20 +203,29 @@ static int filter_conserved(mc3d_solver s, bool last) {
     return MC3D_OK;
 }
 
+// rho, U, V, W, T of `q` into s->prim (updateNonConservedData, Core.cpp:1158-1197)
 template <typename R>
-static int stage_rhs(mc3d_solver s, double *const qP[5]) {
+static int primitives(mc3d_solver s, double *const q[5]) {
     int rc;
-    R *prim[4];
-    for (int v = 0; v < 4; v++) prim[v] = (R *)s->prim[v];
+    R *prim[5];
+    for (int v = 0; v < 5; v++) prim[v] = (R *)s->prim[v];
     s->launches++;
-    if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 4.0 * sizeof(R)) * (double)s->g.n()))) return rc;
-    if ((rc = launch_primitives<R>(s->g, qP, prim, s->stream))) return rc;
-    if ((rc = toc(s))) return rc;
+    if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 5.0 * sizeof(R)) * (double)s->g.n()))) return rc;
+    if ((rc = launch_primitives<R>(s->g, q, prim, s->stream))) return rc;
+    return toc(s);
+}
+
+// RHS of one stage; s->prim holds rho, U, V, W, T of the stage state.
+template <typename R>
+static int stage_rhs(mc3d_solver s) {
+    int rc;
     // gradients of U, V, W, T in each direction: der[3*var + dir]
     for (int d = 0; d < 3; d++) {
         void *out[4] = {s->der[0 + d], s->der[3 + d], s->der[6 + d], s->der[9 + d]};
-        if ((rc = sweep<R>(s, d, s->dop[d], 4, s->prim, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+        if ((rc = sweep<R>(s, d, s->dop[d], 4, s->prim + 1, out, EPI_STORE, nullptr, nullptr, false))) return rc;
     }
+    const R *pr[5];
+    for (int v = 0; v < 5; v++) pr[v] = (const R *)s->prim[v];
     Metrics<R> m = metrics_of<R>(s);
     FluxParams fp{};
     fp.mu_ref = s->cfg.mu_ref;
@@ -231,8 +240,8 @@ static int stage_rhs(mc3d_solver s, double *const qP[5]) {
         } else {
             // mu_sgs, then doAveraging LOCAL: Compact10(-0.49) along Y, Z, X (AbstractSGS.cpp:144-152)
             s->launches++;
-            if ((rc = tic(s, KC_VREMAN, (8.0 + 10.0 * sizeof(R)) * (double)s->g.n()))) return rc;
-            if ((rc = launch_vreman<R>(s->g, qP, dd, m, fp, (R *)s->mu_sgs, s->stream))) return rc;
+            if ((rc = tic(s, KC_VREMAN, 11.0 * sizeof(R) * (double)s->g.n()))) return rc;
+            if ((rc = launch_vreman<R>(s->g, pr, dd, m, fp, (R *)s->mu_sgs, s->stream))) return rc;
             if ((rc = toc(s))) return rc;
             void *a[1] = {s->mu_sgs}, *t1[1] = {s->tA[0]}, *t2[1] = {s->tB[0]};
             if ((rc = sweep<R>(s, 1, s->vop[1], 1, a, t1, EPI_STORE, nullptr, nullptr, true))) return rc;
@@ -245,10 +254,10 @@ static int stage_rhs(mc3d_solver s, double *const qP[5]) {
     for (int i = 0; i < 15; i++) F[i] = (R *)s->flux[i];
     s->launches++;
     {
-        double b = 5.0 * 8 + (12.0 + 15.0) * sizeof(R) + (fp.les == 2 ? sizeof(R) : 0) + (s->const_met ? 0 : 10.0 * sizeof(R));
+        double b = (5.0 + 12.0 + 15.0) * sizeof(R) + (fp.les == 2 ? sizeof(R) : 0) + (s->const_met ? 0 : 10.0 * sizeof(R));
         if ((rc = tic(s, KC_FLUX, b * (double)s->g.n()))) return rc;
     }
-    if ((rc = launch_flux<R>(s->g, qP, dd, m, fp, (const R *)s->mu_sgs, F, s->stream))) return rc;
+    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, (const R *)s->mu_sgs, F, s->stream))) return rc;
     if ((rc = toc(s))) return rc;
     // divergence of the contravariant fluxes, accumulated into the RHS, then k2
     if ((rc = sweep<R>(s, 0, s->dop[0], 5, s->flux + 0, s->rhs, EPI_STORE_NEG, nullptr, nullptr, false))) return rc;
@@ -273,8 +282,12 @@ static int one_step(mc3d_solver s) {
     int scheme = s->cfg.rk_type;
     int ns = scheme == MC3D_RK4 ? 4 : scheme == MC3D_TVDRK3 ? 3 : scheme == MC3D_KENRK4 ? 5 : (s->lsldd_half == 1 ? 5 : 6);
     for (int st = 1; st <= ns; st++) {
-        double *const *qP = st == 1 ? s->q1 : s->qk;
-        if ((rc = stage_rhs<R>(s, qP))) return rc;
+        // stage 1 works on q1 (filtered at the end of the previous step); later
+        // stages on qk, whose primitives the RK update of the previous stage
+        // already wrote unless a sub-step filter changed qk since
+        if (st == 1 || s->cfg.substep_filtering)
+            if ((rc = primitives<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
+        if ((rc = stage_rhs<R>(s))) return rc;
         RkStage rs{};
         rs.scheme = scheme;
         rs.stage = st;
@@ -290,7 +303,12 @@ static int one_step(mc3d_solver s) {
             rs.b = s->lsldd_half == 1 ? LS_B1[st - 1] : LS_B2[st - 1];
         }
         const R *k2[5];
-        for (int v = 0; v < 5; v++) k2[v] = (const R *)s->k2[v];
+        R *pw[5];
+        for (int v = 0; v < 5; v++) {
+            k2[v] = (const R *)s->k2[v];
+            pw[v] = (R *)s->prim[v];
+        }
+        bool fuse_prims = st < ns && !s->cfg.substep_filtering;
         s->launches++;
         {
             // reads k2 and the FP64 registers the scheme touches, writes the updated ones
@@ -298,9 +316,10 @@ static int one_step(mc3d_solver s) {
             if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
             else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
             else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
+            if (fuse_prims) b += 5.0 * sizeof(R);
             if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
         }
-        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, s->stream))) return rc;
+        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, fuse_prims ? pw : nullptr, s->stream))) return rc;
         if ((rc = toc(s))) return rc;
         bool last = st == ns;
         if (last || s->cfg.substep_filtering)
@@ -371,7 +390,7 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         rc = rc ? rc : salloc(s, &s->tB[v], n * rb);
         if (!rc && c.precision != MC3D_FP64) rc = salloc(s, &s->tC[v], n * rb);
     }
-    for (int v = 0; v < 4 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
+    for (int v = 0; v < 5 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
     for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
     for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
     if (!rc && c.les_model == MC3D_VREMAN) rc = salloc(s, &s->mu_sgs, n * rb);
