@@ -494,6 +494,8 @@ void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
     d.tail = h.tail.empty() ? nullptr : q + h.head.size();
     const R *sg = q + h.head.size() + h.tail.size();
     d.S = h.S;
+    d.seg_kf = h.seg_kf;
+    d.seg_kb = h.seg_kb;
     d.sfa = h.S > 1 ? sg : nullptr;
     d.sfb = h.S > 1 ? sg + n : nullptr;
     d.sba = h.S > 1 ? sg + 2 * n : nullptr;
@@ -519,6 +521,18 @@ int upload_line_op(const LineOpHost &hin, int precision, LineOpBuf &out) {
     LineOpHost h = hin;
     analyse(h);
     segment(h);
+    if (h.S > 1) {
+        // responses below 2^-64 (FP64) / 2^-40 (FP32) of their unit start are dropped
+        const double thr = std::ldexp(1.0, precision == MC3D_FP64 ? -64 : -40);
+        int n = h.N, L = n / h.S;
+        h.seg_kf = h.seg_kb = 0;
+        for (int w = 0; w < h.S; w++)
+            for (int r = 0; r < L; r++) {
+                int i = w * L + r;
+                if (std::fabs(h.sfa[i]) > thr || std::fabs(h.sfb[i]) > thr) h.seg_kf = std::max(h.seg_kf, r + 1);
+                if (std::fabs(h.sba[i]) > thr || std::fabs(h.sbb[i]) > thr) h.seg_kb = std::max(h.seg_kb, L - r);
+            }
+    }
     out.precision = precision;
     MC3D_CUDA_TRY(cudaGetDevice(&out.device));
     if (precision == MC3D_FP64) {

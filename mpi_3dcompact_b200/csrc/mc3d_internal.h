@@ -55,6 +55,9 @@ struct LineOpHost {
     // and backward (to the two outgoing solution values) recurrences, per row.
     int S = 1;
     std::vector<double> sfa, sfb, sba, sbb;
+    // rows from a segment's start (kf) / end (kb) over which the forward /
+    // backward responses are above the precision's cut-off (set at upload)
+    int seg_kf = 0, seg_kb = 0;
 };
 
 LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh);
@@ -81,6 +84,7 @@ struct LineOpDev {
     R stat_c[5];
     int S;                         // segments per line (1 = whole-line kernel)
     const R *sfa, *sfb, *sba, *sbb;
+    int seg_kf, seg_kb;
 };
 
 // Device copy of an operator in one precision.

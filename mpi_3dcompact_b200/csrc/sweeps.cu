@@ -16,6 +16,7 @@
 // Reference loops this replaces: Pade6/Penta10/CD2::calc1stDerivField
 // (src/Pade6.cpp:3-46), Compact8/10Filter::filterField
 // (src/Compact10Filter.cpp:166-252) with src/Utils.cpp:4-191 per line.
+#include <cstdint>
 #include <cstdio>
 
 #include "mc3d_internal.h"
@@ -441,56 +442,122 @@ static int launch_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R
 // backward states are chained the same way, and the epilogue folds in the
 // backward superposition and the cyclic correction. Dependency chains are S
 // times shorter and S times more warps share each tile than in sweep_kernel.
+//
+// Row pitch: x-lines (DIR 0) are transposed on load into rows of W+1 words
+// (bank-conflict-free scatter); strided lines (DIR 1, 2) are 128-byte rows of
+// W words filled with 16-byte asynchronous copies when the field is aligned.
 // ---------------------------------------------------------------------------
-template <typename R, int KIND, int E>
+template <int DIR>
+constexpr int seg_pitch() { return DIR == 0 ? W + 1 : W; }
+
+template <typename R>
+__device__ __forceinline__ void cp_async_16(R *dst, const R *src) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// strided-direction epilogue of one warp's segment rows, in blocks of UB rows
+template <typename R, int KIND, int E, int P>
 __device__ __forceinline__ void seg_epi_rows(const SweepBatch<R> &b, const RhsFinalArgs<R> &rf, int f, long long base,
-                                             long long stride, const R *col, int a, int L, const LineOpDev<R> &op,
-                                             const R corr[4], R Y1, R Y2, bool fold) {
-    R *__restrict__ o = (E == EPI_STORE_F64) ? nullptr : b.out[f] + base;
-    double *__restrict__ o64 = (E == EPI_STORE_F64) ? b.out64[f] + base : nullptr;
-    const R *__restrict__ ax = (E == EPI_RHS_FINAL) ? b.aux[f] + base : nullptr;
-    const R *__restrict__ Jp = (E == EPI_RHS_FINAL && rf.J) ? rf.J + base : nullptr;
+                                             long long stride, const R *col, int a, int L, int kb,
+                                             const LineOpDev<R> &op, const R corr[4], R Y1, R Y2, bool fold) {
+    R *__restrict__ o = (E == EPI_STORE_F64) ? nullptr : b.out[f] + base + (long long)a * stride;
+    double *__restrict__ o64 = (E == EPI_STORE_F64) ? b.out64[f] + base + (long long)a * stride : nullptr;
+    const R *__restrict__ ax = (E == EPI_RHS_FINAL) ? b.aux[f] + base + (long long)a * stride : nullptr;
+    const R *__restrict__ Jp = (E == EPI_RHS_FINAL && rf.J) ? rf.J + base + (long long)a * stride : nullptr;
     R dt = (E == EPI_RHS_FINAL) ? (R)(*rf.dt) : R(0);
     const bool mom = (E == EPI_RHS_FINAL) && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
-#pragma unroll 4
-    for (int r = 0; r < L; r++) {
-        int n = a + r;
-        long long off = (long long)n * stride;
-        R v = col[r * SP];
-        if (fold) v += ldc(op.sba + n) * Y1 + ldc(op.sbb + n) * Y2;
-        v = corrected<R, KIND>(v, n, op, corr);
-        if (E == EPI_STORE) o[off] = v;
-        if (E == EPI_STORE_NEG) o[off] = -v;
-        if (E == EPI_SUB) o[off] = o[off] - v;
-        if (E == EPI_STORE_F64) o64[off] = (double)v;
-        if (E == EPI_RHS_FINAL) {
-            R t = ax[off] - v;
-            R dtJ = dt * (Jp ? Jp[off] : rf.Jc);
-            o[off] = mom ? (o[off] + t) * dtJ : t * dtJ;
+    const int fold_from = fold ? L - kb : L;   // rows of the segment carrying the backward superposition
+    for (int r0 = 0; r0 < L; r0 += UB) {
+        const bool fb = r0 + UB > fold_from;
+        const bool cw = a + r0 >= op.corr_lo && a + r0 + UB <= op.corr_hi;   // inside the no-correction window
+        R v[UB], t[UB], jj[UB], old[UB];
+#pragma unroll
+        for (int u = 0; u < UB; u++) {
+            int r = r0 + u, n = a + r;
+            v[u] = col[r * P];
+            if (fb && r >= fold_from) v[u] += ldc(op.sba + n) * Y1 + ldc(op.sbb + n) * Y2;
+            if (!cw) v[u] = corrected<R, KIND>(v[u], n, op, corr);
+            long long off = (long long)r * stride;
+            if (E == EPI_RHS_FINAL) {
+                t[u] = ax[off];
+                jj[u] = Jp ? Jp[off] : rf.Jc;
+                old[u] = mom ? o[off] : R(0);
+            } else if (E == EPI_SUB) {
+                old[u] = o[off];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UB; u++) {
+            long long off = (long long)(r0 + u) * stride;
+            if (E == EPI_STORE) o[off] = v[u];
+            if (E == EPI_STORE_NEG) o[off] = -v[u];
+            if (E == EPI_SUB) o[off] = old[u] - v[u];
+            if (E == EPI_STORE_F64) o64[off] = (double)v[u];
+            if (E == EPI_RHS_FINAL) {
+                // solveContinuity .. solveEnergy (src/CurvilinearCSolver_Core.cpp:790-947)
+                R tt = t[u] - v[u];
+                R dtJ = dt * jj[u];
+                o[off] = mom ? (old[u] + tt) * dtJ : tt * dtJ;
+            }
+        }
+    }
+}
+
+// x-direction epilogue: warp `seg` streams its rows of every line, lanes along x
+template <typename R, int KIND, int E, int P, int H_OF_REG>
+__device__ __forceinline__ void seg_epi_x(const SweepBatch<R> &b, const RhsFinalArgs<R> &rf, int f, long long off0,
+                                          int N, const R *reg, int a, int L, int kb, int nl, const R *scorr,
+                                          const R *Yb, const LineOpDev<R> &op, bool fold, int lane) {
+    R dt = (E == EPI_RHS_FINAL) ? (R)(*rf.dt) : R(0);
+    const bool mom = (E == EPI_RHS_FINAL) && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
+    const int fold_from = fold ? L - kb : L;
+    for (int l = 0; l < nl; l++) {
+        R cl[4] = {scorr[l * 4 + 0], scorr[l * 4 + 1], scorr[l * 4 + 2], scorr[l * 4 + 3]};
+        R Y1 = Yb[l], Y2 = Yb[W + l];
+        long long lo = off0 + (long long)l * N + a;
+        for (int r = lane; r < L; r += 32) {
+            int n = a + r;
+            R v = reg[(H_OF_REG + r) * P + l];
+            if (r >= fold_from) v += ldc(op.sba + n) * Y1 + ldc(op.sbb + n) * Y2;
+            v = corrected<R, KIND>(v, n, op, cl);
+            long long idx = lo + r;
+            if (E == EPI_STORE) b.out[f][idx] = v;
+            if (E == EPI_STORE_NEG) b.out[f][idx] = -v;
+            if (E == EPI_SUB) b.out[f][idx] -= v;
+            if (E == EPI_STORE_F64) b.out64[f][idx] = (double)v;
+            if (E == EPI_RHS_FINAL) {
+                R tt = b.aux[f][idx] - v;
+                R dtJ = dt * (rf.J ? rf.J[idx] : rf.Jc);
+                b.out[f][idx] = mom ? (b.out[f][idx] + tt) * dtJ : tt * dtJ;
+            }
         }
     }
 }
 
 template <int DIR, typename R, int KIND, int H, int S>
 __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R> op, SweepBatch<R> b, int epi,
-                                                           RhsFinalArgs<R> rf, int pass_y, int pass_z, int pass_x) {
+                                                           RhsFinalArgs<R> rf, int pass_y, int pass_z, int pass_x,
+                                                           int vec16) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
+    constexpr int P = seg_pitch<DIR>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N = op.N, L = N / S;
-    const int RG = L + 2 * H + UB;   // rows per segment region
+    const int RG = L + 2 * H + UB;   // rows per segment region (UB keeps regions 16-byte aligned)
     R *s = reinterpret_cast<R *>(smem_raw);
-    R *fwdEnd = s + (size_t)S * RG * SP;   // [S][2][W]
+    R *fwdEnd = s + (size_t)S * RG * P;   // [S][2][W]
     R *fwdIn = fwdEnd + S * 2 * W;
     R *bwdStart = fwdIn + S * 2 * W;
     R *bwdNext = bwdStart + S * 2 * W;
-    R *scorr = bwdNext + S * 2 * W;        // [W][4]
+    R *scorr = bwdNext + S * 2 * W;       // [W][4]
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int tile = blockIdx.x, f = blockIdx.y;
     const int a = seg * L, bEnd = a + L;
     const R *in = b.in[f];
     TileGeom t = tile_geom<DIR>(g, tile, lane);
-    R *col = s + (size_t)seg * RG * SP + lane;   // region of this warp's segment, line `lane`
+    R *reg = s + (size_t)seg * RG * P;    // this warp's segment region
+    R *col = reg + lane;                  // ... line `lane`
 
     // ---- load: warp `seg` brings its own rows of every line ----
     int nl = W;
@@ -498,23 +565,30 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
         long long rem = (long long)g.Ny * g.Nz - (long long)tile * W;
         nl = rem < W ? (int)rem : W;
         const R *src = in + (long long)tile * W * N;
-        R *reg = s + (size_t)seg * RG * SP;
         for (int l = 0; l < nl; l++)
-            for (int i = a + lane; i < bEnd; i += 32)
-                cp_async_elem(&reg[(H + i - a) * SP + l], src + (long long)l * N + i);
+            for (int i = a + lane; i < bEnd; i += 32) cp_async_elem(&reg[(H + i - a) * P + l], src + (long long)l * N + i);
+    } else if (vec16) {
+        // 16-byte chunks of 128-byte rows: CPR chunks per row, 32/CPR rows per pass
+        constexpr int EPC = 16 / sizeof(R), CPR = W / EPC, RPP = 32 / CPR;
+        TileGeom t0 = tile_geom<DIR>(g, tile, 0);
+        long long nvalid = DIR == 1 ? (long long)g.Nx - t0.i : (long long)g.Nx * g.Ny - (long long)tile * W;
+        const int c = lane % CPR;
+        if (c * EPC < nvalid)
+            for (int r = lane / CPR; r < L; r += RPP)
+                cp_async_16(&reg[(H + r) * P + c * EPC], in + t0.base + (long long)(a + r) * t0.stride + c * EPC);
     } else if (t.active) {
-        for (int n = a; n < bEnd; n++) cp_async_elem(&col[(H + n - a) * SP], in + t.base + (long long)n * t.stride);
+        for (int n = a; n < bEnd; n++) cp_async_elem(&col[(H + n - a) * P], in + t.base + (long long)n * t.stride);
     }
     cp_async_wait_all();
     __syncthreads();
     // halos: rows a-H..a-1 and b..b+H-1 (periodic wrap, zero beyond a Dirichlet end)
     if (t.active) {
         const int prev = (seg + S - 1) % S, next = (seg + 1) % S;
-        const R *pr = s + (size_t)prev * RG * SP + lane, *nx = s + (size_t)next * RG * SP + lane;
+        const R *pr = s + (size_t)prev * RG * P + lane, *nx = s + (size_t)next * RG * P + lane;
 #pragma unroll
         for (int h = 0; h < H; h++) {
-            col[h * SP] = (PER || seg > 0) ? pr[(L + h) * SP] : R(0);
-            col[(H + L + h) * SP] = (PER || seg < S - 1) ? nx[(H + h) * SP] : R(0);
+            col[h * P] = (PER || seg > 0) ? pr[(L + h) * P] : R(0);
+            col[(H + L + h) * P] = (PER || seg < S - 1) ? nx[(H + h) * P] : R(0);
         }
     }
     bool pass = false;
@@ -522,17 +596,16 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
     if (DIR == 1) pass = (pass_x && (t.i == 0 || t.i == g.Nx - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
     if (DIR == 2) pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_x && (t.i == 0 || t.i == g.Nx - 1));
     const bool work = t.active && !pass;
-    // Dirichlet boundary rows (only in the first / last segment) read inputs
-    // the in-place sweep overwrites: evaluate before the barrier
+    // Dirichlet boundary rows (first / last segment) read inputs the in-place sweep overwrites
     R headr[H], tailr[H];
     if (!PER && work) {
 #pragma unroll
         for (int r = 0; r < H; r++) {
             R hsum = 0, tsum = 0;
             if (seg == 0)
-                for (int k = 0; k < op.bw; k++) hsum += ldc(op.head + r * op.bw + k) * col[(H + k) * SP];
+                for (int k = 0; k < op.bw; k++) hsum += ldc(op.head + r * op.bw + k) * col[(H + k) * P];
             if (seg == S - 1)
-                for (int k = 0; k < op.bw; k++) tsum += ldc(op.tail + r * op.bw + k) * col[(H + L - op.bw + k) * SP];
+                for (int k = 0; k < op.bw; k++) tsum += ldc(op.tail + r * op.bw + k) * col[(H + L - op.bw + k) * P];
             headr[r] = hsum * op.inv_dh;
             tailr[r] = tsum * op.inv_dh;
         }
@@ -544,55 +617,54 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
     if (work) {
         R w[2 * H];
 #pragma unroll
-        for (int k = 0; k < 2 * H; k++) w[k] = col[k * SP];
+        for (int k = 0; k < 2 * H; k++) w[k] = col[k * P];
         for (int n0 = a; n0 < bEnd; n0 += UB) {
-            R inb[UB], ca[UB], cb[UB], rhs[UB];
+            R inb[UB], rhs[UB];
 #pragma unroll
-            for (int u = 0; u < UB; u++) inb[u] = col[(n0 - a + 2 * H + u) * SP];
-            const bool stat = n0 >= op.stat_lo && n0 + UB <= op.stat_hi;
-            if (stat) {
-#pragma unroll
-                for (int u = 0; u < UB; u++) {
-                    ca[u] = op.stat_c[0];
-                    cb[u] = op.stat_c[1];
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < UB; u++) {
-                    int n = n0 + u;
-                    ca[u] = ldc(op.a0 + n);
-                    cb[u] = (!TRI && n >= 2) ? ldc(op.a1 + (n - 1)) : R(0);
-                }
-            }
+            for (int u = 0; u < UB; u++) inb[u] = col[(n0 - a + 2 * H + u) * P];
 #pragma unroll
             for (int u = 0; u < UB; u++) {
                 R acc = op.st[0] * win_at<H>(w, inb, u);
 #pragma unroll
                 for (int k = 1; k < 2 * H + 1; k++) acc += op.st[k] * win_at<H>(w, inb, u + k);
                 rhs[u] = acc * op.inv_dh;
-                if (!PER) {
-                    int n = n0 + u;
-#pragma unroll
-                    for (int r = 0; r < H; r++) {
-                        if (n == r) rhs[u] = headr[r];
-                        if (n == N - 1 - r) rhs[u] = tailr[r];
-                    }
-                }
             }
+            const bool clean = n0 >= 2 && n0 >= op.stat_lo && n0 + UB <= op.stat_hi && (PER || n0 >= H) &&
+                               (PER || n0 + UB <= N - H);
+            if (clean) {
+                // stationary interior: constant factors, no boundary rows
+                const R ca = op.stat_c[0], cb = op.stat_c[1];
 #pragma unroll
-            for (int u = 0; u < UB; u++) {
-                int n = n0 + u;
-                R x;
-                if (TRI) {
-                    x = (n == 0) ? rhs[u] : rhs[u] - ca[u] * xp;
-                } else {
-                    x = rhs[u];
-                    if (n >= 2) x -= cb[u] * xpp;
-                    if (n >= 1) x -= ca[u] * xp;
+                for (int u = 0; u < UB; u++) {
+                    R x = TRI ? rhs[u] - ca * xp : rhs[u] - cb * xpp - ca * xp;
+                    xpp = xp;
+                    xp = x;
+                    col[(H + n0 - a + u) * P] = x;
                 }
-                xpp = xp;
-                xp = x;
-                col[(H + n - a) * SP] = x;
+            } else {
+#pragma unroll
+                for (int u = 0; u < UB; u++) {
+                    int n = n0 + u;
+                    if (!PER) {
+#pragma unroll
+                        for (int r = 0; r < H; r++) {
+                            if (n == r) rhs[u] = headr[r];
+                            if (n == N - 1 - r) rhs[u] = tailr[r];
+                        }
+                    }
+                    R ca = ldc(op.a0 + n);
+                    R x;
+                    if (TRI) {
+                        x = (n == 0) ? rhs[u] : rhs[u] - ca * xp;
+                    } else {
+                        x = rhs[u];
+                        if (n >= 2) x -= ldc(op.a1 + (n - 1)) * xpp;
+                        if (n >= 1) x -= ca * xp;
+                    }
+                    xpp = xp;
+                    xp = x;
+                    col[(H + n - a) * P] = x;
+                }
             }
 #pragma unroll
             for (int k = 0; k < 2 * H; k++) w[k] = win_at<H>(w, inb, UB + k);
@@ -623,15 +695,16 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
     R xa = 0, xb = 0;
     if (work) {
         const R X1 = fwdIn[(seg * 2 + 0) * W + lane], X2 = fwdIn[(seg * 2 + 1) * W + lane];
-        const bool fold = seg > 0;
+        const int fold_to = seg > 0 ? a + op.seg_kf : a;   // rows [a, fold_to) carry the forward superposition
         for (int n1 = bEnd - 1; n1 >= a; n1 -= UB) {
             R bb[UB], c1[UB], c2[UB], rr[UB];
             const bool stat = n1 - UB + 1 >= op.stat_lo && n1 < op.stat_hi;
+            const bool ff = n1 - UB + 1 < fold_to;
 #pragma unroll
             for (int u = 0; u < UB; u++) {
                 int n = n1 - u;
-                bb[u] = col[(H + n - a) * SP];
-                if (fold) bb[u] += ldc(op.sfa + n) * X1 + ldc(op.sfb + n) * X2;
+                bb[u] = col[(H + n - a) * P];
+                if (ff && n < fold_to) bb[u] += ldc(op.sfa + n) * X1 + (TRI ? R(0) : ldc(op.sfb + n) * X2);
                 if (stat) {
                     c1[u] = TRI ? op.stat_c[2] : op.stat_c[3];
                     c2[u] = TRI ? R(0) : op.stat_c[4];
@@ -650,7 +723,7 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
             for (int u = 0; u < UB; u++) {
                 int n = n1 - u;
                 R x = TRI ? (bb[u] - c1[u] * xa) * rr[u] : (bb[u] - c2[u] * xb - c1[u] * xa) * rr[u];
-                col[(H + n - a) * SP] = x;
+                col[(H + n - a) * P] = x;
                 xb = xa;
                 xa = x;
             }
@@ -679,8 +752,8 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
             // final x_0, x_1 (first segment, folded) and x_{N-1}, x_{N-2} (last segment)
             R x0 = bwdStart[0 * W + lane] + ldc(op.sba + 0) * Y1 + ldc(op.sbb + 0) * Y2;
             R x1 = bwdStart[1 * W + lane] + ldc(op.sba + 1) * Y1 + ldc(op.sbb + 1) * Y2;
-            const R *last = s + (size_t)(S - 1) * RG * SP + lane;
-            R xN1 = last[(H + L - 1) * SP], xN2 = last[(H + L - 2) * SP];
+            const R *last = s + (size_t)(S - 1) * RG * P + lane;
+            R xN1 = last[(H + L - 1) * P], xN2 = last[(H + L - 2) * P];
             if (KIND == K_TRI_PER) {
                 c[0] = (x0 + op.sc[0] * xN1 * op.sc[1]) * op.sc[2];
             } else {
@@ -701,41 +774,44 @@ __global__ void __launch_bounds__(32 * S) sweep_seg_kernel(Grid3 g, LineOpDev<R>
 
     // ---- epilogue: backward superposition, cyclic correction, output ----
     const bool fold = seg < S - 1;
+    const int kb = op.seg_kb;
     if (DIR == 0) {
-        R *reg = s + (size_t)seg * RG * SP;
-        long long off = (long long)tile * W * N;
-        for (int l = 0; l < nl; l++) {
-            R cl[4] = {scorr[l * 4 + 0], scorr[l * 4 + 1], scorr[l * 4 + 2], scorr[l * 4 + 3]};
-            R Y1 = bwdNext[(seg * 2 + 0) * W + l], Y2 = bwdNext[(seg * 2 + 1) * W + l];
-            for (int i = a + lane; i < bEnd; i += 32) {
-                R v = reg[(H + i - a) * SP + l];
-                if (fold) v += ldc(op.sba + i) * Y1 + ldc(op.sbb + i) * Y2;
-                epi_apply<R>(epi, b, rf, f, off + (long long)l * N + i, corrected<R, KIND>(v, i, op, cl));
-            }
+        long long off0 = (long long)tile * W * N;
+        const R *Yb = bwdNext + seg * 2 * W;
+#define MC3D_EPX(E) seg_epi_x<R, KIND, E, P, H>(b, rf, f, off0, N, reg, a, L, kb, nl, scorr, Yb, op, fold, lane)
+        switch (epi) {
+            case EPI_STORE: MC3D_EPX(EPI_STORE); break;
+            case EPI_STORE_NEG: MC3D_EPX(EPI_STORE_NEG); break;
+            case EPI_SUB: MC3D_EPX(EPI_SUB); break;
+            case EPI_STORE_F64: MC3D_EPX(EPI_STORE_F64); break;
+            case EPI_RHS_FINAL: MC3D_EPX(EPI_RHS_FINAL); break;
         }
+#undef MC3D_EPX
     } else if (t.active) {
         R cl[4] = {scorr[lane * 4 + 0], scorr[lane * 4 + 1], scorr[lane * 4 + 2], scorr[lane * 4 + 3]};
         R Y1 = bwdNext[(seg * 2 + 0) * W + lane], Y2 = bwdNext[(seg * 2 + 1) * W + lane];
-        const R *c0 = col + H * SP;
+        const R *c0 = col + H * P;
+#define MC3D_EPR(E) seg_epi_rows<R, KIND, E, P>(b, rf, f, t.base, t.stride, c0, a, L, kb, op, cl, Y1, Y2, fold)
         switch (epi) {
-            case EPI_STORE: seg_epi_rows<R, KIND, EPI_STORE>(b, rf, f, t.base, t.stride, c0, a, L, op, cl, Y1, Y2, fold); break;
-            case EPI_STORE_NEG: seg_epi_rows<R, KIND, EPI_STORE_NEG>(b, rf, f, t.base, t.stride, c0, a, L, op, cl, Y1, Y2, fold); break;
-            case EPI_SUB: seg_epi_rows<R, KIND, EPI_SUB>(b, rf, f, t.base, t.stride, c0, a, L, op, cl, Y1, Y2, fold); break;
-            case EPI_STORE_F64: seg_epi_rows<R, KIND, EPI_STORE_F64>(b, rf, f, t.base, t.stride, c0, a, L, op, cl, Y1, Y2, fold); break;
-            case EPI_RHS_FINAL: seg_epi_rows<R, KIND, EPI_RHS_FINAL>(b, rf, f, t.base, t.stride, c0, a, L, op, cl, Y1, Y2, fold); break;
+            case EPI_STORE: MC3D_EPR(EPI_STORE); break;
+            case EPI_STORE_NEG: MC3D_EPR(EPI_STORE_NEG); break;
+            case EPI_SUB: MC3D_EPR(EPI_SUB); break;
+            case EPI_STORE_F64: MC3D_EPR(EPI_STORE_F64); break;
+            case EPI_RHS_FINAL: MC3D_EPR(EPI_RHS_FINAL); break;
         }
+#undef MC3D_EPR
     }
 }
 
 template <int S>
-constexpr size_t seg_smem_elems(int N, int H) {
-    return (size_t)S * (N / S + 2 * H + UB) * SP + 4 * S * 2 * W + 4 * W;
+constexpr size_t seg_smem_elems(int N, int H, int P) {
+    return (size_t)S * (N / S + 2 * H + UB) * P + 4 * S * 2 * W + 4 * W;
 }
 
 template <int DIR, typename R, int KIND, int H, int S>
 static int launch_seg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
                       const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
-    size_t smem = seg_smem_elems<S>(op.N, H) * sizeof(R);
+    size_t smem = seg_smem_elems<S>(op.N, H, seg_pitch<DIR>()) * sizeof(R);
     auto kern = sweep_seg_kernel<DIR, R, KIND, H, S>;
     static thread_local int configured_smem = -1;
     if ((int)smem > configured_smem) {
@@ -746,8 +822,16 @@ static int launch_seg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R
     if (DIR == 0) tiles = (int)(((long long)g.Ny * g.Nz + W - 1) / W);
     else if (DIR == 1) tiles = ((g.Nx + W - 1) / W) * g.Nz;
     else tiles = (int)(((long long)g.Nx * g.Ny + W - 1) / W);
+    // 16-byte copies need 16-byte aligned rows: field bases and the line stride
+    int vec16 = 0;
+    if (DIR != 0) {
+        const int epc = 16 / sizeof(R);
+        long long inner = DIR == 1 ? g.Nx : (long long)g.Nx * g.Ny;
+        vec16 = (inner % epc == 0);
+        for (int f = 0; f < b.nf && vec16; f++) vec16 = ((uintptr_t)b.in[f] % 16) == 0;
+    }
     dim3 grid(tiles, b.nf);
-    kern<<<grid, 32 * S, smem, st>>>(g, op, b, epi, rf, py, pz, px);
+    kern<<<grid, 32 * S, smem, st>>>(g, op, b, epi, rf, py, pz, px, vec16);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -783,7 +867,8 @@ int launch_sweep(int dir, const Grid3 &g, const LineOpDev<R> &op, const SweepBat
     if (b.nf <= 0) return MC3D_OK;
     if (b.nf > 16) return fail(MC3D_ERR_ARG, "at most 16 fields per sweep");
     size_t smem = ((size_t)(op.N + op.H + UB) * SP + 4 * W) * sizeof(R);
-    if (op.S > 1) smem = (op.S == 4 ? seg_smem_elems<4>(op.N, op.H) : seg_smem_elems<2>(op.N, op.H)) * sizeof(R);
+    if (op.S > 1)
+        smem = (op.S == 4 ? seg_smem_elems<4>(op.N, op.H, W + 1) : seg_smem_elems<2>(op.N, op.H, W + 1)) * sizeof(R);
     if (smem > 227 * 1024) return fail(MC3D_ERR_CONFIG, "line too long for the shared-memory tile");
     int px = filter_passthrough && bc_types[0] == MC3D_DIRICHLET_SOLVE;
     int py = filter_passthrough && bc_types[1] == MC3D_DIRICHLET_SOLVE;
