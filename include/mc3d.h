@@ -181,6 +181,28 @@ int mc3d_solver_sync(mc3d_solver s);
 int mc3d_solver_set_timing(mc3d_solver s, int enable);
 const char *mc3d_solver_timing_report(mc3d_solver s);
 
+/* ---- allocation-free CFL reduction ----
+ * No counterpart in the reference: an extra entry point for callers that must
+ * not have the library allocate device memory (a host code that hands all GPU
+ * memory to its own pool at start-up, where a cudaMalloc in the time loop
+ * could fail or would synchronise the device). Computes the CFL wave-speed
+ * maximum max(J11(|U|+c)/dxi + J22(|V|+c)/deta + J33(|W|+c)/dzeta) over the
+ * FP64 conserved fields (device pointers, x-fastest) into *out_max (device
+ * pointer to one double). J11/J22/J33 may be NULL, then J11c/J22c/J33c are
+ * used. It allocates nothing: the per-block partial maxima sit in a fixed
+ * 512 KiB device array inside the library, which every GPU that loads the
+ * library holds until the process exits; fields larger than 16,777,216
+ * points (256^3) are rejected with MC3D_ERR_ARG. The first call on a device
+ * looks up that array's address (cudaGetSymbolAddress), so make the first
+ * call on each device before any stream capture. All calls share the array:
+ * calls that overlap on the GPU (different streams, no ordering) race; no
+ * scratch value needs to start at zero, every slot a call reads is written by
+ * the same call. Asynchronous on `stream`. */
+int mc3d_cfl_max_noalloc(const double *rho, const double *rhoU, const double *rhoV, const double *rhoW,
+                         const double *rhoE, const double *J11, const double *J22, const double *J33,
+                         double J11c, double J22c, double J33c, int Nx, int Ny, int Nz, double dxi, double deta,
+                         double dzeta, double *out_max, void *stream);
+
 /* ---- host utilities ---- */
 /* The combined-LCG shuffle generator of the reference's HIT IC generator
  * (tests/hit/generate_init_hit.f90:16-81). state[0..2] = ix1..ix3 and

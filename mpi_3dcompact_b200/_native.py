@@ -83,6 +83,7 @@ def host_lib():
             "mc3d_solver_set_timing": (ip, [vp, ip]),
             "mc3d_solver_timing_report": (C.c_char_p, [vp]),
             "mc3d_hit_randvec": (ip, [C.POINTER(C.c_int), C.POINTER(dp), C.c_longlong, C.POINTER(dp)]),
+            "mc3d_cfl_max_noalloc": (ip, [vp] * 8 + [dp] * 3 + [ip] * 3 + [dp] * 3 + [vp, vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)
