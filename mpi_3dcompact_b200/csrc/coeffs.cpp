@@ -364,15 +364,20 @@ LineOpHost build_filter_op(int filter_type, double af, int bc_type, int N) {
 }
 
 namespace {
-// Stationary interior of the factor arrays and the correction window.
-void analyse(LineOpHost &h) {
+// Stationary interior of the factor arrays (equality after rounding to the
+// working precision) and the correction window.
+void analyse(LineOpHost &h, int precision) {
     int n = h.N;
     size_t na = h.arr.size() / (n ? n : 1);
     int nfac = h.kind == K_TRI_PER || h.kind == K_TRI_DIR ? 3 : (h.kind == K_PEN_PER || h.kind == K_PEN_DIR ? 5 : 0);
+    const bool f32 = precision != MC3D_FP64;
     h.stat_lo = h.stat_hi = 0;
     if (nfac && na >= (size_t)nfac) {
         // largest run [lo, hi) with all factor arrays (and a1[n-1]) constant
-        auto at = [&](int a, int i) { return h.arr[(size_t)a * n + i]; };
+        auto at = [&](int a, int i) {
+            double v = h.arr[(size_t)a * n + i];
+            return f32 ? (double)(float)v : v;
+        };
         int best_lo = 0, best_hi = 0, lo = 1;
         for (int i = 1; i < n; i++) {
             bool same = true;
@@ -394,7 +399,7 @@ void analyse(LineOpHost &h) {
         double peak = 0;
         for (int c = 0; c < ncol; c++)
             for (int i = 0; i < n; i++) peak = std::max(peak, std::fabs(h.arr[(size_t)(base + c) * n + i]));
-        const double thr = peak * std::ldexp(1.0, -64);
+        const double thr = peak * std::ldexp(1.0, f32 ? -32 : -64);
         auto small = [&](int i) {
             for (int c = 0; c < ncol; c++)
                 if (std::fabs(h.arr[(size_t)(base + c) * n + i]) > thr) return false;
@@ -416,16 +421,23 @@ void analyse(LineOpHost &h) {
 //        backward x_n = -c_n x_{n+1} rw_n                    from x_b = 1
 // penta: forward  B_n = -m2_{n-1} B_{n-2} - m1_n B_{n-1}     from (B_{a-1}, B_{a-2}) = (1,0) | (0,1)
 //        backward x_n = (-f_n x_{n+2} - C_n x_{n+1}) rD_n    from (x_b, x_{b+1}) = (1,0) | (0,1)
-void segment(LineOpHost &h) {
+void segment(LineOpHost &h, int precision) {
     int n = h.N;
     bool tri = h.kind == K_TRI_PER || h.kind == K_TRI_DIR;
     bool pen = h.kind == K_PEN_PER || h.kind == K_PEN_DIR;
     h.S = 1;
+    h.L = 0;
     if (!(tri || pen)) return;
     const int UB = 8;
     int S = 0;
-    for (int cand : {4, 2})
-        if (n % cand == 0 && (n / cand) % UB == 0 && n / cand >= 32 && n / cand >= h.bw) { S = cand; break; }
+    int Lr = reg_segment_len(n, h.kind, precision);
+    if (Lr) {
+        S = n / Lr;
+        h.L = Lr;
+    } else {
+        for (int cand : {4, 2})
+            if (n % cand == 0 && (n / cand) % UB == 0 && n / cand >= 32 && n / cand >= h.bw) { S = cand; break; }
+    }
     if (!S) return;
     h.S = S;
     int L = n / S;
@@ -461,8 +473,14 @@ void segment(LineOpHost &h) {
     }
 }
 
+// Offsets (in elements) of the arrays inside one operator's device buffer.
+struct Layout {
+    size_t arr = 0, head = 0, tail = 0, seg = 0;
+    size_t pf = 0, pb = 0, pz = 0, sf2 = 0, sb2 = 0, hp = 0, tp = 0;
+};
+
 template <typename R>
-void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
+void fill_dev(const LineOpHost &h, const char *base, const Layout &lo, LineOpDev<R> &d) {
     d.stat_lo = h.stat_lo;
     d.stat_hi = h.stat_hi;
     d.corr_lo = h.corr_lo;
@@ -480,19 +498,19 @@ void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
     const R *p = (const R *)base;
     size_t n = h.N;
     size_t na = h.arr.size() / n;
-    d.a0 = na > 0 ? p : nullptr;
-    d.a1 = na > 1 ? p + n : nullptr;
-    d.a2 = na > 2 ? p + 2 * n : nullptr;
-    d.a3 = na > 3 ? p + 3 * n : nullptr;
-    d.a4 = na > 4 ? p + 4 * n : nullptr;
-    d.z0 = na > 5 ? p + 5 * n : nullptr;
-    d.z1 = na > 6 ? p + 6 * n : nullptr;
-    d.z2 = na > 7 ? p + 7 * n : nullptr;
-    d.z3 = na > 8 ? p + 8 * n : nullptr;
-    const R *q = p + h.arr.size();
-    d.head = h.head.empty() ? nullptr : q;
-    d.tail = h.tail.empty() ? nullptr : q + h.head.size();
-    const R *sg = q + h.head.size() + h.tail.size();
+    const R *a = p + lo.arr;
+    d.a0 = na > 0 ? a : nullptr;
+    d.a1 = na > 1 ? a + n : nullptr;
+    d.a2 = na > 2 ? a + 2 * n : nullptr;
+    d.a3 = na > 3 ? a + 3 * n : nullptr;
+    d.a4 = na > 4 ? a + 4 * n : nullptr;
+    d.z0 = na > 5 ? a + 5 * n : nullptr;
+    d.z1 = na > 6 ? a + 6 * n : nullptr;
+    d.z2 = na > 7 ? a + 7 * n : nullptr;
+    d.z3 = na > 8 ? a + 8 * n : nullptr;
+    d.head = h.head.empty() ? nullptr : p + lo.head;
+    d.tail = h.tail.empty() ? nullptr : p + lo.tail;
+    const R *sg = p + lo.seg;
     d.S = h.S;
     d.seg_kf = h.seg_kf;
     d.seg_kb = h.seg_kb;
@@ -500,30 +518,109 @@ void fill_dev(const LineOpHost &h, const char *base, LineOpDev<R> &d) {
     d.sfb = h.S > 1 ? sg + n : nullptr;
     d.sba = h.S > 1 ? sg + 2 * n : nullptr;
     d.sbb = h.S > 1 ? sg + 3 * n : nullptr;
+    d.L = h.L;
+    d.pf = h.L ? p + lo.pf : nullptr;
+    d.pb = h.L ? p + lo.pb : nullptr;
+    d.pz = h.L && h.kind == K_PEN_PER ? p + lo.pz : nullptr;
+    d.sf2 = h.L ? p + lo.sf2 : nullptr;
+    d.sb2 = h.L ? p + lo.sb2 : nullptr;
+    const bool dir = h.kind == K_TRI_DIR || h.kind == K_PEN_DIR;
+    d.hp = h.L && dir ? p + lo.hp : nullptr;
+    d.tp = h.L && dir ? p + lo.tp : nullptr;
 }
 
 template <typename R>
-std::vector<R> flatten(const LineOpHost &h) {
+std::vector<R> flatten(const LineOpHost &h, Layout &lo) {
     std::vector<R> v;
-    v.reserve(h.arr.size() + h.head.size() + h.tail.size());
-    for (double x : h.arr) v.push_back((R)x);
-    for (double x : h.head) v.push_back((R)x);
-    for (double x : h.tail) v.push_back((R)x);
+    auto put = [&](double x) { v.push_back((R)x); };
+    auto align4 = [&]() {   // vector loads of 2 or 4 values need 16-byte aligned rows
+        while (v.size() % 4) v.push_back((R)0);
+    };
+    lo.arr = v.size();
+    for (double x : h.arr) put(x);
+    lo.head = v.size();
+    for (double x : h.head) put(x);
+    lo.tail = v.size();
+    for (double x : h.tail) put(x);
+    lo.seg = v.size();
     if (h.S > 1)
         for (const std::vector<double> *a : {&h.sfa, &h.sfb, &h.sba, &h.sbb})
-            for (double x : *a) v.push_back((R)x);
+            for (double x : *a) put(x);
+    if (h.L) {
+        const int n = h.N;
+        const bool tri = h.kind == K_TRI_PER || h.kind == K_TRI_DIR;
+        auto A = [&](int a, int i) { return h.arr[(size_t)a * n + i]; };
+        align4();
+        lo.pf = v.size();
+        for (int i = 0; i < n; i++) {
+            put(i >= 1 ? A(0, i) : 0.0);
+            put(!tri && i >= 2 ? A(1, i - 1) : 0.0);
+        }
+        align4();
+        lo.pb = v.size();
+        for (int i = 0; i < n; i++) {
+            if (tri) {
+                put(A(2, i));
+                put(0.0);
+                put(A(1, i));
+            } else {
+                put(A(3, i));
+                put(A(4, i));
+                put(A(2, i));
+            }
+            put(0.0);
+        }
+        if (h.kind == K_PEN_PER) {
+            align4();
+            lo.pz = v.size();
+            for (int i = 0; i < n; i++)
+                for (int c = 0; c < 4; c++) put(A(5 + c, i));
+        }
+        align4();
+        lo.sf2 = v.size();
+        for (int i = 0; i < n; i++) {
+            put(h.sfa[i]);
+            put(h.sfb[i]);
+        }
+        align4();
+        lo.sb2 = v.size();
+        for (int i = 0; i < n; i++) {
+            put(h.sba[i]);
+            put(h.sbb[i]);
+        }
+        if (h.kind == K_TRI_DIR || h.kind == K_PEN_DIR) {
+            const int bw = h.bw, B = MC3D_BWMAX;
+            lo.hp = v.size();
+            for (int r = 0; r < h.H; r++)
+                for (int k = 0; k < B; k++) put(k < bw ? h.head[(size_t)r * bw + k] : 0.0);
+            lo.tp = v.size();
+            for (int r = 0; r < h.H; r++)
+                for (int k = 0; k < B; k++) {
+                    int kk = k - (B - bw);
+                    put(kk >= 0 ? h.tail[(size_t)r * bw + kk] : 0.0);
+                }
+        }
+    }
     if (v.empty()) v.push_back((R)0);
     return v;
 }
 }  // namespace
 
+int reg_segment_len(int N, int kind, int precision) {
+    if (!(kind == K_TRI_PER || kind == K_TRI_DIR || kind == K_PEN_PER || kind == K_PEN_DIR)) return 0;
+    if (precision != MC3D_FP64 && N % 64 == 0 && N / 64 >= 2 && N / 64 <= 16) return 64;
+    if (N % 32 == 0 && N / 32 >= 2 && N / 32 <= 16) return 32;
+    return 0;
+}
+
 int upload_line_op(const LineOpHost &hin, int precision, LineOpBuf &out) {
     LineOpHost h = hin;
-    analyse(h);
-    segment(h);
+    if (h.bw > MC3D_BWMAX) return fail(MC3D_ERR_CONFIG, "boundary row wider than the kernels support");
+    analyse(h, precision);
+    segment(h, precision);
     if (h.S > 1) {
-        // responses below 2^-64 (FP64) / 2^-40 (FP32) of their unit start are dropped
-        const double thr = std::ldexp(1.0, precision == MC3D_FP64 ? -64 : -40);
+        // responses below 2^-64 (FP64) / 2^-32 (FP32) of their unit start are dropped
+        const double thr = std::ldexp(1.0, precision == MC3D_FP64 ? -64 : -32);
         int n = h.N, L = n / h.S;
         h.seg_kf = h.seg_kb = 0;
         for (int w = 0; w < h.S; w++)
@@ -535,16 +632,17 @@ int upload_line_op(const LineOpHost &hin, int precision, LineOpBuf &out) {
     }
     out.precision = precision;
     MC3D_CUDA_TRY(cudaGetDevice(&out.device));
+    Layout lo;
     if (precision == MC3D_FP64) {
-        std::vector<double> v = flatten<double>(h);
+        std::vector<double> v = flatten<double>(h, lo);
         MC3D_CUDA_TRY(cudaMalloc(&out.dev, v.size() * sizeof(double)));
         MC3D_CUDA_TRY(cudaMemcpy(out.dev, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
-        fill_dev<double>(h, (const char *)out.dev, out.f64);
+        fill_dev<double>(h, (const char *)out.dev, lo, out.f64);
     } else {
-        std::vector<float> v = flatten<float>(h);
+        std::vector<float> v = flatten<float>(h, lo);
         MC3D_CUDA_TRY(cudaMalloc(&out.dev, v.size() * sizeof(float)));
         MC3D_CUDA_TRY(cudaMemcpy(out.dev, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
-        fill_dev<float>(h, (const char *)out.dev, out.f32);
+        fill_dev<float>(h, (const char *)out.dev, lo, out.f32);
     }
     return MC3D_OK;
 }

@@ -42,13 +42,14 @@ struct LineOpHost {
     double sc[4] = {0};   // kind-specific scalars
     double Hm[16] = {0};  // penta cyclic capacitance inverse
     double cp[6] = {0};   // penta cyclic corner values
-    // Rows [stat_lo, stat_hi) where every elimination factor is exactly
-    // constant (Toeplitz interior: the factors reach their fixed point a few
-    // dozen rows from the ends); stat_c holds those constants.
+    // Rows [stat_lo, stat_hi) where every elimination factor, rounded to the
+    // working precision, is exactly constant (Toeplitz interior: the factors
+    // reach their fixed point a few dozen rows from the ends); stat_c holds
+    // those constants.
     int stat_lo = 0, stat_hi = 0;
     double stat_c[5] = {0};
     // Rows [corr_lo, corr_hi) where the cyclic correction columns are below
-    // 2^-64 of their peak, so the correction is skipped there.
+    // 2^-64 (FP64) / 2^-32 (FP32) of their peak, so the correction is skipped.
     int corr_lo = 0, corr_hi = 0;
     // Segmented solve: S segments of L = N/S rows per line; homogeneous
     // responses of the local forward (to the two incoming eliminated values)
@@ -58,7 +59,12 @@ struct LineOpHost {
     // rows from a segment's start (kf) / end (kb) over which the forward /
     // backward responses are above the precision's cut-off (set at upload)
     int seg_kf = 0, seg_kb = 0;
+    int L = 0;   // segment length of the register-resident kernel (0: not used)
 };
+
+// Segment length of the register-resident line solve for a line of N points
+// in a precision (0 when the line goes to the shared-memory kernels).
+int reg_segment_len(int N, int kind, int precision);
 
 LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh);
 LineOpHost build_filter_op(int filter_type, double alphaF, int bc_type, int N);
@@ -85,7 +91,19 @@ struct LineOpDev {
     int S;                         // segments per line (1 = whole-line kernel)
     const R *sfa, *sfb, *sba, *sbb;
     int seg_kf, seg_kb;
+    // Register-resident segmented solve (segment length L = N/S rows, 0 when
+    // the line length does not suit it). Row-interleaved copies of the
+    // factors so one vector load fetches a row's coefficients:
+    //   pf  [N][2]  forward  (m1_n, m2_{n-1}) | tri (m_n, 0); zero where unused
+    //   pb  [N][4]  backward (C_n, f_n, rD_n, 0) | tri (c_n, 0, rw_n, 0)
+    //   pz  [N][4]  penta cyclic columns (z0..z3)_n
+    //   sf2 [N][2]  (sfa, sfb)_n,  sb2 [N][2]  (sba, sbb)_n
+    //   hp, tp [H][MC3D_BWMAX]  Dirichlet boundary rows, zero padded (head on
+    //   phi[0..BWMAX-1], tail right-aligned on phi[N-BWMAX..N-1])
+    int L;
+    const R *pf, *pb, *pz, *sf2, *sb2, *hp, *tp;
 };
+constexpr int MC3D_BWMAX = 11;   // widest boundary row (11-point filter closures)
 
 // Device copy of an operator in one precision.
 struct LineOpBuf {

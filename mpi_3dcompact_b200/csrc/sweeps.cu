@@ -19,82 +19,9 @@
 #include <cstdint>
 #include <cstdio>
 
-#include "mc3d_internal.h"
+#include "sweep_common.cuh"
 
 namespace mc3d {
-
-constexpr int W = 32;       // lines per tile
-constexpr int SP = W + 1;   // shared-memory row pitch (elements)
-
-template <typename R>
-__device__ __forceinline__ R ldc(const R *p) {
-    return __ldg(p);
-}
-
-// Asynchronous global->shared element copy (cp.async, L1-allocating), so a
-// whole tile is in flight at once without staging through registers.
-template <typename R>
-__device__ __forceinline__ void cp_async_elem(R *dst, const R *src) {
-    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    if (sizeof(R) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-}
-
-// Tile geometry: line `lane` of tile `tile` starts at base(lane) and advances by
-// `stride`; for DIR 0 the tile's lines are one contiguous block of len*N values.
-struct TileGeom {
-    long long base;   // element 0 of this lane's line
-    long long stride;
-    bool active;
-    int j, k, i;      // grid coordinates of the line (the running one is unused)
-};
-
-template <int DIR>
-__device__ __forceinline__ TileGeom tile_geom(const Grid3 &g, int tile, int lane) {
-    TileGeom t;
-    if (DIR == 0) {
-        long long L = (long long)tile * W + lane;
-        long long nl = (long long)g.Ny * g.Nz;
-        t.active = L < nl;
-        t.base = L * g.Nx;
-        t.stride = 1;
-        t.j = (int)(L % g.Ny);
-        t.k = (int)(L / g.Ny);
-        t.i = 0;
-    } else if (DIR == 1) {
-        int tx = (g.Nx + W - 1) / W;
-        int k = tile / tx;
-        int i = (tile % tx) * W + lane;
-        t.active = i < g.Nx;
-        t.base = (long long)i + (long long)g.Nx * g.Ny * k;
-        t.stride = g.Nx;
-        t.i = i;
-        t.k = k;
-        t.j = 0;
-    } else {
-        long long L = (long long)tile * W + lane;
-        long long nl = (long long)g.Nx * g.Ny;
-        t.active = L < nl;
-        t.base = L;
-        t.stride = (long long)g.Nx * g.Ny;
-        t.i = (int)(L % g.Nx);
-        t.j = (int)(L / g.Nx);
-        t.k = 0;
-    }
-    return t;
-}
-
-template <int DIR>
-__device__ __forceinline__ int tile_count(const Grid3 &g) {
-    if (DIR == 0) return (int)(((long long)g.Ny * g.Nz + W - 1) / W);
-    if (DIR == 1) return ((g.Nx + W - 1) / W) * g.Nz;
-    return (int)(((long long)g.Nx * g.Ny + W - 1) / W);
-}
 
 // ---------------------------------------------------------------------------
 // per-line solve, in place on col[n * SP]. Rows N .. N+H-1 hold the periodic
@@ -107,7 +34,6 @@ __device__ __forceinline__ int tile_count(const Grid3 &g) {
 // The periodic (Sherman-Morrison / Woodbury) correction is returned as up to
 // four per-line scalars and applied in the epilogue.
 // ---------------------------------------------------------------------------
-constexpr int UB = 8;
 
 template <int H, typename R>
 __device__ __forceinline__ R win_at(const R (&w)[2 * H], const R (&in)[UB], int j) {
@@ -866,13 +792,20 @@ int launch_sweep(int dir, const Grid3 &g, const LineOpDev<R> &op, const SweepBat
                  const RhsFinalArgs<R> &rf, const int bc_types[3], bool filter_passthrough, cudaStream_t st) {
     if (b.nf <= 0) return MC3D_OK;
     if (b.nf > 16) return fail(MC3D_ERR_ARG, "at most 16 fields per sweep");
-    size_t smem = ((size_t)(op.N + op.H + UB) * SP + 4 * W) * sizeof(R);
-    if (op.S > 1)
-        smem = (op.S == 4 ? seg_smem_elems<4>(op.N, op.H, W + 1) : seg_smem_elems<2>(op.N, op.H, W + 1)) * sizeof(R);
-    if (smem > 227 * 1024) return fail(MC3D_ERR_CONFIG, "line too long for the shared-memory tile");
     int px = filter_passthrough && bc_types[0] == MC3D_DIRICHLET_SOLVE;
     int py = filter_passthrough && bc_types[1] == MC3D_DIRICHLET_SOLVE;
     int pz = filter_passthrough && bc_types[2] == MC3D_DIRICHLET_SOLVE;
+    if (op.L > 0 && g.n() < (1LL << 31) &&   // register-resident kernels index fields with 32-bit offsets
+        reg_smem_bytes(dir, op.N, op.N / op.L, sizeof(R)) <= 227 * 1024) {
+        int rc = dir == 0 ? launch_sweep_reg<0, R>(g, op, b, epi, rf, px, py, pz, st)
+                 : dir == 1 ? launch_sweep_reg<1, R>(g, op, b, epi, rf, px, py, pz, st)
+                            : launch_sweep_reg<2, R>(g, op, b, epi, rf, px, py, pz, st);
+        if (rc != MC3D_ERR_CONFIG) return rc;
+    }
+    size_t smem = ((size_t)(op.N + op.H + UB) * SP + 4 * W) * sizeof(R);
+    if (op.S == 4) smem = seg_smem_elems<4>(op.N, op.H, W + 1) * sizeof(R);
+    if (op.S == 2) smem = seg_smem_elems<2>(op.N, op.H, W + 1) * sizeof(R);
+    if (smem > 227 * 1024) return fail(MC3D_ERR_CONFIG, "line too long for the shared-memory tile");
     if (dir == 0) return dispatch_kind<0, R>(g, op, b, epi, rf, px, py, pz, st);
     if (dir == 1) return dispatch_kind<1, R>(g, op, b, epi, rf, px, py, pz, st);
     return dispatch_kind<2, R>(g, op, b, epi, rf, px, py, pz, st);
