@@ -65,56 +65,122 @@ struct RegVec<double> {
     }
 };
 
-// The caller's operation on element `off` of field f's output
-template <typename R, int E>
-__device__ __forceinline__ void reg_out(R *o, double *o64, const R *ax, const R *jp, R jc, R dt, bool mom, int off,
-                                        R v) {
-    if (E == EPI_STORE) o[off] = v;
-    if (E == EPI_STORE_NEG) o[off] = -v;
-    if (E == EPI_SUB) o[off] = o[off] - v;
-    if (E == EPI_STORE_F64) o64[off] = (double)v;
-    if (E == EPI_RHS_FINAL) {
-        // solveContinuity .. solveEnergy (src/CurvilinearCSolver_Core.cpp:790-947)
-        // with zero sponge and zero hook sources
-        R tt = ax[off] - v;
-        R dtJ = dt * (jp ? jp[off] : jc);
-        o[off] = mom ? (o[off] + tt) * dtJ : tt * dtJ;
-    }
-}
-
-// strided lines: write this lane's L rows (row a + r at off0 + r * stride)
+// strided lines: write this lane's L rows (row a + r at off0 + r * stride).
+// Operands the operation reads (previous output, partial RHS, J) are loaded a
+// block of UB rows ahead of the block being stored, in program order before
+// those stores, so each block costs one memory round trip at most and the
+// loads overlap the previous block's stores.
 template <typename R, int E, int L>
 __device__ __forceinline__ void reg_store_rows(const SweepBatch<R> &b, const RhsFinalArgs<R> &rf, int f, int off0,
                                                int stride, const R (&y)[L]) {
+    constexpr int NB = L / UB;
+    constexpr bool RD_OLD = E == EPI_SUB || E == EPI_RHS_FINAL;   // RHS_FINAL: only momentum with the quirk
+    constexpr bool RD_AUX = E == EPI_RHS_FINAL;
     const R dt = (E == EPI_RHS_FINAL) ? (R)(*rf.dt) : R(0);
     const bool mom = (E == EPI_RHS_FINAL) && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
+    const bool rd_old = E == EPI_SUB || mom;
     R *o = b.out[f];
     double *o64 = b.out64[f];
     const R *ax = b.aux[f];
-    int off = off0;
+    const R *jp = rf.J;
+    // FP32: the next block's operands are fetched while this block is stored;
+    // FP64 (twice the registers per value): each block fetches its own.
+    constexpr bool AHEAD = sizeof(R) == 4;
+    R old[2][UB], aux[2][UB], jj[2][UB];
+    auto fetch = [&](int blk, int slot) {
 #pragma unroll
-    for (int r = 0; r < L; r++) {
-        reg_out<R, E>(o, o64, ax, rf.J, rf.Jc, dt, mom, off, y[r]);
-        off += stride;
+        for (int u = 0; u < UB; u++) {
+            const int off = off0 + (blk * UB + u) * stride;
+            if (RD_OLD) old[slot][u] = rd_old ? o[off] : R(0);
+            if (RD_AUX) {
+                aux[slot][u] = ax[off];
+                jj[slot][u] = jp ? jp[off] : rf.Jc;
+            }
+        }
+    };
+    if (AHEAD && (RD_OLD || RD_AUX)) fetch(0, 0);
+#pragma unroll
+    for (int blk = 0; blk < NB; blk++) {
+        const int cur = AHEAD ? (blk & 1) : 0;
+        if (AHEAD && (RD_OLD || RD_AUX) && blk + 1 < NB) fetch(blk + 1, cur ^ 1);
+        if (!AHEAD && (RD_OLD || RD_AUX)) fetch(blk, 0);
+#pragma unroll
+        for (int u = 0; u < UB; u++) {
+            const int r = blk * UB + u;
+            const int off = off0 + r * stride;
+            const R v = y[r];
+            if (E == EPI_STORE) o[off] = v;
+            if (E == EPI_STORE_NEG) o[off] = -v;
+            if (E == EPI_SUB) o[off] = old[cur][u] - v;
+            if (E == EPI_STORE_F64) o64[off] = (double)v;
+            if (E == EPI_RHS_FINAL) {
+                // solveContinuity .. solveEnergy (src/CurvilinearCSolver_Core.cpp:790-947)
+                // with zero sponge and zero hook sources
+                R tt = aux[cur][u] - v;
+                R dtJ = dt * jj[cur][u];
+                o[off] = mom ? (old[cur][u] + tt) * dtJ : tt * dtJ;
+            }
+        }
     }
 }
 
-// x lines: warp `seg` writes rows [a, a+L) of the tile's nl lines, lanes along x
+// x lines: warp `seg` writes rows [a, a+L) of the tile's nl lines, lanes
+// along x. The read operands of a group of lines are loaded before any of the
+// group's stores.
 template <typename R, int E, int L>
 __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFinalArgs<R> &rf, int f, int tile0,
                                              int N, int nl, int a, int lane, const R *tile) {
     constexpr int P = W + 1;
+    constexpr int Q = L / 32;    // elements per lane and line
+    constexpr int G = 8 / Q;     // lines per group: 8 elements per lane in flight
+    constexpr bool RD_OLD = E == EPI_SUB || E == EPI_RHS_FINAL;
+    constexpr bool RD_AUX = E == EPI_RHS_FINAL;
     const R dt = (E == EPI_RHS_FINAL) ? (R)(*rf.dt) : R(0);
     const bool mom = (E == EPI_RHS_FINAL) && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
+    const bool rd_old = E == EPI_SUB || mom;
     R *o = b.out[f];
     double *o64 = b.out64[f];
     const R *ax = b.aux[f];
-    for (int l = 0; l < nl; l++) {
-        const int line0 = (tile0 + l) * N + a;
+    const R *jp = rf.J;
+    for (int l0 = 0; l0 < nl; l0 += G) {
+        R old[G][Q], aux[G][Q], jj[G][Q];
+        if (RD_OLD || RD_AUX) {
 #pragma unroll
-        for (int i0 = 0; i0 < L; i0 += 32) {
-            const int i = i0 + lane;
-            reg_out<R, E>(o, o64, ax, rf.J, rf.Jc, dt, mom, line0 + i, tile[(a + i) * P + l]);
+            for (int gl = 0; gl < G; gl++) {
+                if (l0 + gl < nl) {
+                    const int line0 = (tile0 + l0 + gl) * N + a + lane;
+#pragma unroll
+                    for (int q = 0; q < Q; q++) {
+                        const int off = line0 + 32 * q;
+                        if (RD_OLD) old[gl][q] = rd_old ? o[off] : R(0);
+                        if (RD_AUX) {
+                            aux[gl][q] = ax[off];
+                            jj[gl][q] = jp ? jp[off] : rf.Jc;
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int gl = 0; gl < G; gl++) {
+            if (l0 + gl < nl) {
+                const int l = l0 + gl;
+                const int line0 = (tile0 + l) * N + a + lane;
+#pragma unroll
+                for (int q = 0; q < Q; q++) {
+                    const int off = line0 + 32 * q;
+                    const R v = tile[(a + lane + 32 * q) * P + l];
+                    if (E == EPI_STORE) o[off] = v;
+                    if (E == EPI_STORE_NEG) o[off] = -v;
+                    if (E == EPI_SUB) o[off] = old[gl][q] - v;
+                    if (E == EPI_STORE_F64) o64[off] = (double)v;
+                    if (E == EPI_RHS_FINAL) {
+                        R tt = aux[gl][q] - v;
+                        R dtJ = dt * jj[gl][q];
+                        o[off] = mom ? (old[gl][q] + tt) * dtJ : tt * dtJ;
+                    }
+                }
+            }
         }
     }
 }
