@@ -260,44 +260,135 @@ struct K5 {
     const R *p[5];
 };
 
-template <typename R>
-__global__ void rk_kernel(Grid3 g, RkStage rs, K5<R> k2, Q5 q1, Q5 qk, Q5 q2, P5<R> prim, int want_prims) {
-    long long n = g.n();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double nk[5];
+// Two consecutive points per thread: one 8/16-byte access per array, and every
+// array the stage reads is loaded before any store of the iteration (the
+// register arrays are written in place, so stores would otherwise order the
+// following loads behind them).
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using V = float2;
+};
+template <>
+struct Pair<double> {
+    using V = double2;
+};
+template <typename T>
+__device__ __forceinline__ void ld_pair(const T *p, long long i, bool two, double (&o)[2]) {
+    if (two) {
+        typename Pair<T>::V v = *reinterpret_cast<const typename Pair<T>::V *>(p + i);
+        o[0] = (double)v.x;
+        o[1] = (double)v.y;
+    } else {
+        o[0] = (double)p[i];
+        o[1] = 0.0;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *p, long long i, bool two, double x0, double x1) {
+    if (two) {
+        typename Pair<T>::V v;
+        v.x = (T)x0;
+        v.y = (T)x1;
+        *reinterpret_cast<typename Pair<T>::V *>(p + i) = v;
+    } else {
+        p[i] = (T)x0;
+    }
+}
+
+// Stage kinds: the scheme and where the stage sits in it (first, middle,
+// last), which fixes the registers it reads and writes.
+enum RkMode { RKM_RK4_1, RKM_RK4_MID, RKM_RK4_LAST, RKM_TVD_1, RKM_TVD_2, RKM_TVD_3, RKM_2N_1, RKM_2N_MID, RKM_2N_LAST };
+
+template <typename R, int M>
+__global__ void __launch_bounds__(256) rk_kernel(Grid3 g, RkStage rs, K5<R> k2, Q5 q1, Q5 qk, Q5 q2, P5<R> prim,
+                                                 int want_prims) {
+    const long long n = g.n();
+    constexpr bool rk4 = M <= RKM_RK4_LAST, tvd = M >= RKM_TVD_1 && M <= RKM_TVD_3, two_n = M >= RKM_2N_1;
+    constexpr bool last = M == RKM_RK4_LAST || M == RKM_TVD_3 || M == RKM_2N_LAST;
+    // registers read / written by this stage
+    constexpr bool rd_q1 = M != RKM_RK4_LAST;
+    constexpr bool rd_qk = M == RKM_TVD_2 || M == RKM_TVD_3 || M == RKM_2N_MID || M == RKM_2N_LAST;
+    constexpr bool rd_q2 = M == RKM_RK4_MID || M == RKM_RK4_LAST;
+    constexpr bool wr_q1 = two_n;
+    constexpr bool wr_qk = !last;
+    constexpr bool wr_q2 = rk4 || last;
+    constexpr bool first = M == RKM_RK4_1 || M == RKM_TVD_1 || M == RKM_2N_1;
+    const long long npairs = (n + 1) / 2;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < npairs;
+         j += (long long)gridDim.x * blockDim.x) {
+        const long long i = 2 * j;
+        const bool two = i + 1 < n;
+        double K[5][2], A[5][2], B[5][2], C[5][2];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            double k = (double)k2.p[v][i];
-            nk[v] = 0.0;
-            if (rs.scheme == MC3D_RK4) {
-                if (rs.stage == 1) {
-                    double b1 = q1.p[v][i];
-                    q2.p[v][i] = b1 + rs.a * k;
-                    qk.p[v][i] = nk[v] = b1 + rs.b * k;
-                } else if (rs.stage < 4) {
-                    q2.p[v][i] += rs.a * k;
-                    qk.p[v][i] = nk[v] = q1.p[v][i] + rs.b * k;
+            ld_pair<R>(k2.p[v], i, two, K[v]);
+            if (rd_q1) ld_pair<double>(q1.p[v], i, two, A[v]);
+            if (rd_qk) ld_pair<double>(qk.p[v], i, two, B[v]);
+            if (rd_q2) ld_pair<double>(q2.p[v], i, two, C[v]);
+        }
+        double nk[5][2], o1[5][2], ok[5][2], o2[5][2];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                const double k = K[v][p];
+                nk[v][p] = o1[v][p] = ok[v][p] = o2[v][p] = 0.0;
+                if (rk4) {
+                    // src/RK4.hpp:47-125
+                    if (first) {
+                        double b1 = A[v][p];
+                        o2[v][p] = b1 + rs.a * k;
+                        ok[v][p] = nk[v][p] = b1 + rs.b * k;
+                    } else if (!last) {
+                        o2[v][p] = C[v][p] + rs.a * k;
+                        ok[v][p] = nk[v][p] = A[v][p] + rs.b * k;
+                    } else {
+                        o2[v][p] = C[v][p] + rs.a * k;
+                    }
+                } else if (tvd) {
+                    // src/TVDRK3.hpp:50-133
+                    if (first) ok[v][p] = nk[v][p] = A[v][p] + 1.0 * k;
+                    else if (M == RKM_TVD_2) ok[v][p] = nk[v][p] = 0.75 * A[v][p] + 0.25 * B[v][p] + 0.25 * k;
+                    else o2[v][p] = (1.0 / 3.0) * A[v][p] + (2.0 / 3.0) * B[v][p] + (2.0 / 3.0) * k;
                 } else {
-                    q2.p[v][i] += rs.a * k;
-                }
-            } else if (rs.scheme == MC3D_TVDRK3) {
-                if (rs.stage == 1) qk.p[v][i] = nk[v] = q1.p[v][i] + 1.0 * k;
-                else if (rs.stage == 2) qk.p[v][i] = nk[v] = 0.75 * q1.p[v][i] + 0.25 * qk.p[v][i] + 0.25 * k;
-                else q2.p[v][i] = (1.0 / 3.0) * q1.p[v][i] + (2.0 / 3.0) * qk.p[v][i] + (2.0 / 3.0) * k;
-            } else {
-                if (rs.stage == 1) {
-                    qk.p[v][i] = nk[v] = q1.p[v][i] + rs.b * k;
-                    q1.p[v][i] = k;
-                } else {
-                    double r = k + rs.a * q1.p[v][i];
-                    q1.p[v][i] = r;
-                    if (rs.stage < rs.nstages) qk.p[v][i] = nk[v] = qk.p[v][i] + rs.b * r;
-                    else q2.p[v][i] = qk.p[v][i] + rs.b * r;
+                    // 2N low-storage schemes (src/KenRK4.hpp:53-152, src/LSLDDRK4.hpp:93-320)
+                    if (first) {
+                        ok[v][p] = nk[v][p] = A[v][p] + rs.b * k;
+                        o1[v][p] = k;
+                    } else {
+                        double r = k + rs.a * A[v][p];
+                        o1[v][p] = r;
+                        if (!last) ok[v][p] = nk[v][p] = B[v][p] + rs.b * r;
+                        else o2[v][p] = B[v][p] + rs.b * r;
+                    }
                 }
             }
         }
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            if (wr_q1) st_pair<double>(q1.p[v], i, two, o1[v][0], o1[v][1]);
+            if (wr_qk) st_pair<double>(qk.p[v], i, two, ok[v][0], ok[v][1]);
+            if (wr_q2) st_pair<double>(q2.p[v], i, two, o2[v][0], o2[v][1]);
+        }
         // primitives of the next stage state (updateNonConservedData, Core.cpp:1165-1177)
-        if (want_prims) prims_of<R>(nk[0], nk[1], nk[2], nk[3], nk[4], prim.p, i);
+        if (want_prims) {
+            double pr[5][2];
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                double rho = nk[0][p];
+                double u = nk[1][p] / rho, vv = nk[2][p] / rho, w = nk[3][p] / rho;
+                double pp = (GAMMA - 1) * (nk[4][p] - 0.5 * rho * (u * u + vv * vv + w * w));
+                pr[0][p] = rho;
+                pr[1][p] = u;
+                pr[2][p] = vv;
+                pr[3][p] = w;
+                pr[4][p] = pp / (rho * R_GAS);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; v++) st_pair<R>(prim.p[v], i, two, pr[v][0], pr[v][1]);
+        }
     }
 }
 
@@ -314,7 +405,23 @@ int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], do
         c.p[v] = q2[v];
         P.p[v] = prim ? prim[v] : nullptr;
     }
-    rk_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rs, k, a, b, c, P, prim != nullptr);
+    const bool first = rs.stage == 1, last = rs.stage >= rs.nstages;
+    int mode;
+    if (rs.scheme == MC3D_RK4) mode = first ? RKM_RK4_1 : (last ? RKM_RK4_LAST : RKM_RK4_MID);
+    else if (rs.scheme == MC3D_TVDRK3) mode = first ? RKM_TVD_1 : (last ? RKM_TVD_3 : RKM_TVD_2);
+    else mode = first ? RKM_2N_1 : (last ? RKM_2N_LAST : RKM_2N_MID);
+    const int grid = grid_for((g.n() + 1) / 2, 256), wp = prim != nullptr;
+    switch (mode) {
+        case RKM_RK4_1: rk_kernel<R, RKM_RK4_1><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_RK4_MID: rk_kernel<R, RKM_RK4_MID><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_RK4_LAST: rk_kernel<R, RKM_RK4_LAST><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_TVD_1: rk_kernel<R, RKM_TVD_1><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_TVD_2: rk_kernel<R, RKM_TVD_2><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_TVD_3: rk_kernel<R, RKM_TVD_3><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_2N_1: rk_kernel<R, RKM_2N_1><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        case RKM_2N_MID: rk_kernel<R, RKM_2N_MID><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+        default: rk_kernel<R, RKM_2N_LAST><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
+    }
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
