@@ -118,99 +118,225 @@ struct OutPtrs15 {
     void *p[15];
 };
 
+// Paired access to two consecutive points: one 8/16-byte load or store.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using V = float2;
+};
+template <>
+struct Pair<double> {
+    using V = double2;
+};
+template <typename T>
+__device__ __forceinline__ void ld_pair(const T *p, long long i, bool two, double (&o)[2]) {
+    if (two) {
+        typename Pair<T>::V v = *reinterpret_cast<const typename Pair<T>::V *>(p + i);
+        o[0] = (double)v.x;
+        o[1] = (double)v.y;
+    } else {
+        o[0] = (double)p[i];
+        o[1] = 0.0;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *p, long long i, bool two, double x0, double x1) {
+    if (two) {
+        typename Pair<T>::V v;
+        v.x = (T)x0;
+        v.y = (T)x1;
+        *reinterpret_cast<typename Pair<T>::V *>(p + i) = v;
+    } else {
+        p[i] = (T)x0;
+    }
+}
+
+template <typename T, int NP>
+__device__ __forceinline__ void ld_np(const T *p, long long i, bool two, T (&o)[NP]) {
+    if (NP == 2 && two) {
+        typename Pair<T>::V v = *reinterpret_cast<const typename Pair<T>::V *>(p + i);
+        o[0] = v.x;
+        o[NP - 1] = v.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < NP; k++) o[k] = k == 0 ? p[i] : T(0);
+    }
+}
+template <typename T, int NP>
+__device__ __forceinline__ void st_np(T *p, long long i, bool two, const T (&x)[NP]) {
+    if (NP == 2 && two) {
+        typename Pair<T>::V v;
+        v.x = x[0];
+        v.y = x[NP - 1];
+        *reinterpret_cast<typename Pair<T>::V *>(p + i) = v;
+    } else {
+        p[i] = x[0];
+    }
+}
+
 // ---- fluxes: preStepDerivatives, Core.cpp:615-752 ----
-template <typename R>
-__global__ void __launch_bounds__(256, 3) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
+// Metric forms: per-point fields, ten constants, or constants with zero
+// off-diagonal J_ab (rectilinear box). The diagonal form leaves out the terms
+// that multiply a zero metric, which changes no finite result.
+enum MetForm { MET_FIELD = 0, MET_CONST = 1, MET_DIAG = 2 };
+
+template <typename R, int MET>
+__device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&dd)[12], const R (&mj)[10], R msgs,
+                                           const Metrics<R> &m, const FluxParams &fp, R d1c, R iJc, double dvol,
+                                           R (&o)[15]) {
+    constexpr bool DIAG = MET == MET_DIAG;
+    const R J = MET == MET_FIELD ? mj[0] : m.c[0];
+    const R J11 = MET == MET_FIELD ? mj[1] : m.c[1], J12 = MET == MET_FIELD ? mj[2] : m.c[2],
+            J13 = MET == MET_FIELD ? mj[3] : m.c[3];
+    const R J21 = MET == MET_FIELD ? mj[4] : m.c[4], J22 = MET == MET_FIELD ? mj[5] : m.c[5],
+            J23 = MET == MET_FIELD ? mj[6] : m.c[6];
+    const R J31 = MET == MET_FIELD ? mj[7] : m.c[7], J32 = MET == MET_FIELD ? mj[8] : m.c[8],
+            J33 = MET == MET_FIELD ? mj[9] : m.c[9];
+    // p and rhoE from the ideal-gas relations (src/IdealGas.hpp:64-78)
+    R p = rho * (R)R_GAS * T;
+    R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
+    R rhoE = p / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
+    R mu = mu_of_T(T, fp.mu_ref);
+    R Ucurv = DIAG ? J11 * U : J11 * U + J12 * V + J13 * W;
+    R Vcurv = DIAG ? J22 * V : J21 * U + J22 * V + J23 * W;
+    R Wcurv = DIAG ? J33 * W : J31 * U + J32 * V + J33 * W;
+
+    // gradU[a][b] = J1b dUa1 + J2b dUa2 + J3b dUa3  (Core.cpp:548-561)
+    R gu[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        R d1 = dd[3 * a], d2 = dd[3 * a + 1], d3 = dd[3 * a + 2];
+        gu[a][0] = DIAG ? J11 * d1 : J11 * d1 + J21 * d2 + J31 * d3;
+        gu[a][1] = DIAG ? J22 * d2 : J12 * d1 + J22 * d2 + J32 * d3;
+        gu[a][2] = DIAG ? J33 * d3 : J13 * d1 + J23 * d2 + J33 * d3;
+    }
+
+    R mu_eff, k_eff;
+    if (fp.les) {
+        R mu_sgs;
+        if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, MET != MET_FIELD ? d1c : vreman_d1<R>(dvol, J));
+        else mu_sgs = msgs;
+        mu_eff = mu + mu_sgs;
+        k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
+        if (mu_eff < (R)0) mu_eff = 0;
+        if (k_eff < (R)0) k_eff = 0;
+    } else {
+        mu_eff = mu;
+        k_eff = (R)(CP / PR) * mu;
+    }
+    R dUdx = gu[0][0], dUdy = gu[0][1], dUdz = gu[0][2];
+    R dVdx = gu[1][0], dVdy = gu[1][1], dVdz = gu[1][2];
+    R dWdx = gu[2][0], dWdy = gu[2][1], dWdz = gu[2][2];
+    const R c43 = (R)(4.0 / 3.0), c23 = (R)(2.0 / 3.0);
+    R t11 = (c43 * dUdx - c23 * dVdy - c23 * dWdz) * mu_eff;
+    R t22 = (-c23 * dUdx + c43 * dVdy - c23 * dWdz) * mu_eff;
+    R t33 = (-c23 * dUdx - c23 * dVdy + c43 * dWdz) * mu_eff;
+    R t12 = (dUdy + dVdx) * mu_eff;
+    R t13 = (dUdz + dWdx) * mu_eff;
+    R t23 = (dVdz + dWdy) * mu_eff;
+    const R t21 = t12, t31 = t13, t32 = t23;
+
+    R dT1 = dd[9], dT2 = dd[10], dT3 = dd[11];
+    R q1 = k_eff * (DIAG ? J11 * dT1 : J11 * dT1 + J21 * dT2 + J31 * dT3);
+    R q2 = k_eff * (DIAG ? J22 * dT2 : J12 * dT1 + J22 * dT2 + J32 * dT3);
+    R q3 = k_eff * (DIAG ? J33 * dT3 : J13 * dT1 + J23 * dT2 + J33 * dT3);
+    R b1 = U * t11 + V * t12 + W * t13 + q1;
+    R b2 = U * t21 + V * t22 + W * t23 + q2;
+    R b3 = U * t31 + V * t32 + W * t33 + q3;
+
+    R iJ = MET != MET_FIELD ? iJc : (R)1 / J;
+    o[0] = iJ * (rho * Ucurv);
+    o[5] = iJ * (rho * Vcurv);
+    o[10] = iJ * (rho * Wcurv);
+
+    R f1, f2, f3, g1, g2, g3;
+    f1 = rhoU * Ucurv + J11 * p;
+    f2 = DIAG ? rhoU * Vcurv : rhoU * Vcurv + J21 * p;
+    f3 = DIAG ? rhoU * Wcurv : rhoU * Wcurv + J31 * p;
+    g1 = DIAG ? J11 * t11 : J11 * t11 + J12 * t21 + J13 * t31;
+    g2 = DIAG ? J22 * t21 : J21 * t11 + J22 * t21 + J23 * t31;
+    g3 = DIAG ? J33 * t31 : J31 * t11 + J32 * t21 + J33 * t31;
+    o[1] = iJ * (f1 - g1);
+    o[6] = iJ * (f2 - g2);
+    o[11] = iJ * (f3 - g3);
+
+    f1 = DIAG ? rhoV * Ucurv : rhoV * Ucurv + J12 * p;
+    f2 = rhoV * Vcurv + J22 * p;
+    f3 = DIAG ? rhoV * Wcurv : rhoV * Wcurv + J32 * p;
+    g1 = DIAG ? J11 * t12 : J11 * t12 + J12 * t22 + J13 * t32;
+    g2 = DIAG ? J22 * t22 : J21 * t12 + J22 * t22 + J23 * t32;
+    g3 = DIAG ? J33 * t32 : J31 * t12 + J32 * t22 + J33 * t32;
+    o[2] = iJ * (f1 - g1);
+    o[7] = iJ * (f2 - g2);
+    o[12] = iJ * (f3 - g3);
+
+    f1 = DIAG ? rhoW * Ucurv : rhoW * Ucurv + J13 * p;
+    f2 = DIAG ? rhoW * Vcurv : rhoW * Vcurv + J23 * p;
+    f3 = rhoW * Wcurv + J33 * p;
+    g1 = DIAG ? J11 * t13 : J11 * t13 + J12 * t23 + J13 * t33;
+    g2 = DIAG ? J22 * t23 : J21 * t13 + J22 * t23 + J23 * t33;
+    g3 = DIAG ? J33 * t33 : J31 * t13 + J32 * t23 + J33 * t33;
+    o[3] = iJ * (f1 - g1);
+    o[8] = iJ * (f2 - g2);
+    o[13] = iJ * (f3 - g3);
+
+    R ep = rhoE + p;
+    f1 = ep * Ucurv;
+    f2 = ep * Vcurv;
+    f3 = ep * Wcurv;
+    g1 = DIAG ? J11 * b1 : J11 * b1 + J12 * b2 + J13 * b3;
+    g2 = DIAG ? J22 * b2 : J21 * b1 + J22 * b2 + J23 * b3;
+    g3 = DIAG ? J33 * b3 : J31 * b1 + J32 * b2 + J33 * b3;
+    o[4] = iJ * (f1 - g1);
+    o[9] = iJ * (f2 - g2);
+    o[14] = iJ * (f3 - g3);
+}
+
+// NP consecutive points per thread (2 in FP32: paired 8-byte accesses), all
+// inputs of the iteration loaded before its 15 stores.
+template <typename R, int MET, int NP>
+__global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
                                                       const R *__restrict__ r2, const R *__restrict__ r3,
                                                       const R *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
                                                       FluxParams fp, const R *__restrict__ mu_sgs_f, OutPtrs15 op) {
     const R *const *d = reinterpret_cast<const R *const *>(dp.p);
     R *const *F = reinterpret_cast<R *const *>(op.p);
     const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
-    const R d1c = m.constant ? vreman_d1<R>(dvol, m.c[0]) : R(0);   // filter width of a uniform block
-    long long n = g.n();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        // primitives rho, U, V, W, T of the stage state; p and rhoE follow
-        // from the ideal-gas relations (src/IdealGas.hpp:64-78)
-        R rho = r0[i], U = r1[i], V = r2[i], W = r3[i], T = r4[i];
-        R p = rho * (R)R_GAS * T;
-        R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
-        R rhoE = p / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
-        R mu = mu_of_T(T, fp.mu_ref);
-        R J = met(m, 0, i);
-        R J11 = met(m, 1, i), J12 = met(m, 2, i), J13 = met(m, 3, i);
-        R J21 = met(m, 4, i), J22 = met(m, 5, i), J23 = met(m, 6, i);
-        R J31 = met(m, 7, i), J32 = met(m, 8, i), J33 = met(m, 9, i);
-        R Ucurv = J11 * U + J12 * V + J13 * W;
-        R Vcurv = J21 * U + J22 * V + J23 * W;
-        R Wcurv = J31 * U + J32 * V + J33 * W;
-
-        R gu[3][3];
-        velocity_gradient<R>(m, i, d, gu);
-
-        R mu_eff, k_eff;
-        if (fp.les) {
-            R mu_sgs;
-            if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, m.constant ? d1c : vreman_d1<R>(dvol, J));
-            else mu_sgs = mu_sgs_f[i];
-            mu_eff = mu + mu_sgs;
-            k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
-            if (mu_eff < (R)0) mu_eff = 0;
-            if (k_eff < (R)0) k_eff = 0;
-        } else {
-            mu_eff = mu;
-            k_eff = (R)(CP / PR) * mu;
+    const R d1c = MET != MET_FIELD ? vreman_d1<R>(dvol, m.c[0]) : R(0);   // filter width of a uniform block
+    const R iJc = MET != MET_FIELD ? (R)1 / m.c[0] : R(0);
+    const long long n = g.n(), nit = (n + NP - 1) / NP;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nit; j += (long long)gridDim.x * blockDim.x) {
+        const long long i = NP * j;
+        const bool two = i + 1 < n;
+        R rho[NP], U[NP], V[NP], Wv[NP], T[NP], dd[12][NP], mj[10][NP], ms[NP];
+        ld_np<R, NP>(r0, i, two, rho);
+        ld_np<R, NP>(r1, i, two, U);
+        ld_np<R, NP>(r2, i, two, V);
+        ld_np<R, NP>(r3, i, two, Wv);
+        ld_np<R, NP>(r4, i, two, T);
+#pragma unroll
+        for (int k = 0; k < 12; k++) ld_np<R, NP>(d[k], i, two, dd[k]);
+        if (MET == MET_FIELD) {
+#pragma unroll
+            for (int c = 0; c < 10; c++) ld_np<R, NP>(m.m[c], i, two, mj[c]);
         }
-        R dUdx = gu[0][0], dUdy = gu[0][1], dUdz = gu[0][2];
-        R dVdx = gu[1][0], dVdy = gu[1][1], dVdz = gu[1][2];
-        R dWdx = gu[2][0], dWdy = gu[2][1], dWdz = gu[2][2];
-        const R c43 = (R)(4.0 / 3.0), c23 = (R)(2.0 / 3.0);
-        R t11 = (c43 * dUdx - c23 * dVdy - c23 * dWdz) * mu_eff;
-        R t22 = (-c23 * dUdx + c43 * dVdy - c23 * dWdz) * mu_eff;
-        R t33 = (-c23 * dUdx - c23 * dVdy + c43 * dWdz) * mu_eff;
-        R t12 = (dUdy + dVdx) * mu_eff;
-        R t13 = (dUdz + dWdx) * mu_eff;
-        R t23 = (dVdz + dWdy) * mu_eff;
-        const R t21 = t12, t31 = t13, t32 = t23;
-
-        R dT1 = d[9][i], dT2 = d[10][i], dT3 = d[11][i];
-        R q1 = k_eff * (J11 * dT1 + J21 * dT2 + J31 * dT3);
-        R q2 = k_eff * (J12 * dT1 + J22 * dT2 + J32 * dT3);
-        R q3 = k_eff * (J13 * dT1 + J23 * dT2 + J33 * dT3);
-        R b1 = U * t11 + V * t12 + W * t13 + q1;
-        R b2 = U * t21 + V * t22 + W * t23 + q2;
-        R b3 = U * t31 + V * t32 + W * t33 + q3;
-
-        R iJ = (R)1 / J;
-        F[0][i] = iJ * (rho * Ucurv);
-        F[5][i] = iJ * (rho * Vcurv);
-        F[10][i] = iJ * (rho * Wcurv);
-
-        R f1, f2, f3, g1, g2, g3;
-        f1 = rhoU * Ucurv + J11 * p; f2 = rhoU * Vcurv + J21 * p; f3 = rhoU * Wcurv + J31 * p;
-        g1 = J11 * t11 + J12 * t21 + J13 * t31;
-        g2 = J21 * t11 + J22 * t21 + J23 * t31;
-        g3 = J31 * t11 + J32 * t21 + J33 * t31;
-        F[1][i] = iJ * (f1 - g1); F[6][i] = iJ * (f2 - g2); F[11][i] = iJ * (f3 - g3);
-
-        f1 = rhoV * Ucurv + J12 * p; f2 = rhoV * Vcurv + J22 * p; f3 = rhoV * Wcurv + J32 * p;
-        g1 = J11 * t12 + J12 * t22 + J13 * t32;
-        g2 = J21 * t12 + J22 * t22 + J23 * t32;
-        g3 = J31 * t12 + J32 * t22 + J33 * t32;
-        F[2][i] = iJ * (f1 - g1); F[7][i] = iJ * (f2 - g2); F[12][i] = iJ * (f3 - g3);
-
-        f1 = rhoW * Ucurv + J13 * p; f2 = rhoW * Vcurv + J23 * p; f3 = rhoW * Wcurv + J33 * p;
-        g1 = J11 * t13 + J12 * t23 + J13 * t33;
-        g2 = J21 * t13 + J22 * t23 + J23 * t33;
-        g3 = J31 * t13 + J32 * t23 + J33 * t33;
-        F[3][i] = iJ * (f1 - g1); F[8][i] = iJ * (f2 - g2); F[13][i] = iJ * (f3 - g3);
-
-        R ep = rhoE + p;
-        f1 = ep * Ucurv; f2 = ep * Vcurv; f3 = ep * Wcurv;
-        g1 = J11 * b1 + J12 * b2 + J13 * b3;
-        g2 = J21 * b1 + J22 * b2 + J23 * b3;
-        g3 = J31 * b1 + J32 * b2 + J33 * b3;
-        F[4][i] = iJ * (f1 - g1); F[9][i] = iJ * (f2 - g2); F[14][i] = iJ * (f3 - g3);
+        if (fp.les == 2) ld_np<R, NP>(mu_sgs_f, i, two, ms);
+        R out[15][NP];
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            R dq[12], mq[10], oq[15];
+#pragma unroll
+            for (int k = 0; k < 12; k++) dq[k] = dd[k][q];
+#pragma unroll
+            for (int c = 0; c < 10; c++) mq[c] = MET == MET_FIELD ? mj[c][q] : R(0);
+            flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], dq, mq, fp.les == 2 ? ms[q] : R(0), m, fp, d1c, iJc,
+                               dvol, oq);
+#pragma unroll
+            for (int k = 0; k < 15; k++) out[k][q] = oq[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 15; k++) st_np<R, NP>(F[k], i, two, out[k]);
     }
 }
 
@@ -221,7 +347,16 @@ int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const
     for (int i = 0; i < 12; i++) dp.p[i] = d[i];
     OutPtrs15 op;
     for (int i = 0; i < 15; i++) op.p[i] = F[i];
-    flux_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+    constexpr int NP = sizeof(R) == 4 ? 2 : 1;
+    const int grid = grid_for((g.n() + NP - 1) / NP, 256);
+    bool diag = m.constant;
+    for (int c : {2, 3, 4, 6, 7, 8}) diag = diag && m.c[c] == R(0);
+    if (!m.constant)
+        flux_kernel<R, MET_FIELD, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+    else if (!diag)
+        flux_kernel<R, MET_CONST, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+    else
+        flux_kernel<R, MET_DIAG, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -264,39 +399,6 @@ struct K5 {
 // array the stage reads is loaded before any store of the iteration (the
 // register arrays are written in place, so stores would otherwise order the
 // following loads behind them).
-template <typename T>
-struct Pair;
-template <>
-struct Pair<float> {
-    using V = float2;
-};
-template <>
-struct Pair<double> {
-    using V = double2;
-};
-template <typename T>
-__device__ __forceinline__ void ld_pair(const T *p, long long i, bool two, double (&o)[2]) {
-    if (two) {
-        typename Pair<T>::V v = *reinterpret_cast<const typename Pair<T>::V *>(p + i);
-        o[0] = (double)v.x;
-        o[1] = (double)v.y;
-    } else {
-        o[0] = (double)p[i];
-        o[1] = 0.0;
-    }
-}
-template <typename T>
-__device__ __forceinline__ void st_pair(T *p, long long i, bool two, double x0, double x1) {
-    if (two) {
-        typename Pair<T>::V v;
-        v.x = (T)x0;
-        v.y = (T)x1;
-        *reinterpret_cast<typename Pair<T>::V *>(p + i) = v;
-    } else {
-        p[i] = (T)x0;
-    }
-}
-
 // Stage kinds: the scheme and where the stage sits in it (first, middle,
 // last), which fixes the registers it reads and writes.
 enum RkMode { RKM_RK4_1, RKM_RK4_MID, RKM_RK4_LAST, RKM_TVD_1, RKM_TVD_2, RKM_TVD_3, RKM_2N_1, RKM_2N_MID, RKM_2N_LAST };
