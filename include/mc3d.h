@@ -48,7 +48,8 @@ extern "C" {
 enum { MC3D_CONST_DT = 0, MC3D_CONST_CFL = 1 };                 /* TimeSteppingType */
 enum { MC3D_PERIODIC_SOLVE = 0, MC3D_DIRICHLET_SOLVE = 1 };     /* BCType           */
 enum { MC3D_CD2 = 0, MC3D_PADE6 = 1, MC3D_PENTA10 = 2 };        /* FDType           */
-enum { MC3D_COMPACT8 = 0, MC3D_COMPACT10 = 1 };                 /* FilterType       */
+enum { MC3D_COMPACT8 = 0, MC3D_COMPACT10 = 1,                  /* FilterType       */
+       MC3D_TESTFILTER_PADE = 2, MC3D_TESTFILTER_EXP = 3 };      /* DSM test filters */
 enum { MC3D_NOMODEL = 0, MC3D_VREMAN = 1, MC3D_DSM = 2 };       /* LESModel         */
 enum { MC3D_AVG_NONE = 0, MC3D_AVG_XI1 = 1, MC3D_AVG_XI2 = 2, MC3D_AVG_XI3 = 3,
        MC3D_AVG_LOCAL = 4, MC3D_AVG_GLOBAL = 5 };               /* StatsAvgType     */
@@ -87,6 +88,9 @@ typedef struct mc3d_config {
     int reference_quirks;    /* GPU.REFERENCEQUIRKS (default 1): keep the
                                 reference's momentum k2 carry-over
                                 (src/CurvilinearCSolver_Core.cpp:839,872,904) */
+    int dsm_test_filter;     /* LES.DSMTESTFILTER (default 1): 1 = Pade test
+                                filter, 2 = explicit (src/DSMSGS.hpp:57-67)   */
+    int dsm_use_taukk;       /* LES.DSMUSETAUKK (default 1)                  */
 } mc3d_config;
 
 /* ---- configuration ---- */
@@ -111,7 +115,10 @@ int mc3d_deriv_create(int fd_type, int bc_type, int dir, int Nx, int Ny, int Nz,
                       int precision, int device, mc3d_op *out);
 
 /* Replaces `new Compact8Filter/Compact10Filter(alphaF, Domain*, BC*, BCType,
- * Direct)` (src/Compact8Filter.hpp:28, src/Compact10Filter.hpp:30).
+ * Direct)` (src/Compact8Filter.hpp:28, src/Compact10Filter.hpp:30), and with
+ * filter_type MC3D_TESTFILTER_PADE / MC3D_TESTFILTER_EXP (alphaF unused) the
+ * DSM test filters `new CommN5PadeTestFilter/CommN5ExpTestFilter(Domain*, BC*,
+ * BCType, Direct)` (src/CommN5PadeTestFilter.hpp:32, src/CommN5ExpTestFilter.hpp:16).
  * bc_types[3] are the BC types of all three directions: lines lying on a
  * Dirichlet face of another direction pass through (src/Compact10Filter.cpp:166-252). */
 int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_types[3], int Nx, int Ny,

@@ -139,6 +139,23 @@ class Compact10Filter(_Filter):
     _ft = COMPACT10
 
 
+class CommN5PadeTestFilter(_Filter):
+    """DSM Pade test filter (src/CommN5PadeTestFilter.hpp): 11-point RHS,
+    pentadiagonal LHS. Constructed as (shape, bc_types, direction)."""
+    _ft = 2
+
+    def __init__(self, shape, bc_types, direction, precision=FP64, device=0):
+        super().__init__(0.0, shape, bc_types, direction, precision, device)
+
+
+class CommN5ExpTestFilter(_Filter):
+    """DSM explicit 7-point test filter (src/CommN5ExpTestFilter.hpp)."""
+    _ft = 3
+
+    def __init__(self, shape, bc_types, direction, precision=FP64, device=0):
+        super().__init__(0.0, shape, bc_types, direction, precision, device)
+
+
 def calc_neumann(fd_type, f):
     a = np.ascontiguousarray(np.asarray(f, dtype=np.float64))
     return N.host_lib().mc3d_calc_neumann(fd_type, N.dptr(a))
@@ -156,7 +173,8 @@ class Options:
 
     def __init__(self, grid=(64, 64, 64), fd="PADE6", filter="COMPACT10", alphaF=0.45, mu_ref=1e-3, rk="RK4",
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
-                 les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3):
+                 les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
+                 dsm_test_filter=1, dsm_use_taukk=True):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -175,6 +193,8 @@ class Options:
         c.les_averaging = _AVG[les_avg]
         c.precision = precision
         c.reference_quirks = int(bool(reference_quirks))
+        c.dsm_test_filter = int(dsm_test_filter)
+        c.dsm_use_taukk = int(bool(dsm_use_taukk))
         self.c = c
 
     @classmethod

@@ -43,7 +43,7 @@ class Config(C.Structure):
                 ("filter_step", C.c_int), ("substep_filtering", C.c_int), ("max_time_step", C.c_int),
                 ("max_time", C.c_double), ("les_model", C.c_int), ("les_averaging", C.c_int),
                 ("time_step0", C.c_int), ("time0", C.c_double), ("precision", C.c_int),
-                ("reference_quirks", C.c_int)]
+                ("reference_quirks", C.c_int), ("dsm_test_filter", C.c_int), ("dsm_use_taukk", C.c_int)]
 
 
 _lib = None

@@ -65,6 +65,8 @@ int mc3d_config_default(mc3d_config *c) {
     c->time0 = 0.0;
     c->precision = MC3D_FP64;
     c->reference_quirks = 1;
+    c->dsm_test_filter = 1;   // src/Options.hpp:424-425 defaults
+    c->dsm_use_taukk = 1;
     return MC3D_OK;
 }
 
@@ -249,6 +251,12 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
         c->les_averaging = parse_enum(ini, "LES.LESAVERAGING",
                                       {{"NONE", MC3D_AVG_NONE}, {"XI1_AVG", MC3D_AVG_XI1}, {"XI2_AVG", MC3D_AVG_XI2},
                                        {"XI3_AVG", MC3D_AVG_XI3}, {"LOCAL", MC3D_AVG_LOCAL}, {"GLOBAL", MC3D_AVG_GLOBAL}});
+        if (ini.has("LES.DSMTESTFILTER")) {
+            c->dsm_test_filter = parse_int("DSMTESTFILTER", ini.get("LES.DSMTESTFILTER"));
+            // DSMSGS aborts on any other value (src/DSMSGS.hpp:57-67)
+            if (c->dsm_test_filter != 1 && c->dsm_test_filter != 2) throw CfgError{"DSMTESTFILTER must be 1 or 2"};
+        }
+        if (ini.has("LES.DSMUSETAUKK")) c->dsm_use_taukk = parse_bool("DSMUSETAUKK", ini.get("LES.DSMUSETAUKK"));
         // [GPU]
         if (ini.has("GPU.PRECISION"))
             c->precision = parse_enum(ini, "GPU.PRECISION", {{"FP64", MC3D_FP64}, {"FP32BULK", MC3D_FP32BULK}});
@@ -314,7 +322,10 @@ extern "C" int mc3d_filter_create(int filter_type, double alphaF, int dir, const
     o->device = device;
     int N[3] = {Nx, Ny, Nz};
     try {
-        o->host = build_filter_op(filter_type, alphaF, bc_types[dir], N[dir]);
+        if (filter_type == MC3D_TESTFILTER_PADE || filter_type == MC3D_TESTFILTER_EXP)
+            o->host = build_testfilter_op(filter_type, bc_types[dir], N[dir]);
+        else
+            o->host = build_filter_op(filter_type, alphaF, bc_types[dir], N[dir]);
     } catch (const std::exception &e) {
         delete o;
         return fail(MC3D_ERR_CONFIG, e.what());

@@ -363,6 +363,80 @@ LineOpHost build_filter_op(int filter_type, double af, int bc_type, int N) {
     return op;
 }
 
+// DSM test filters (src/CommN5PadeTestFilter.{hpp,cpp}, src/CommN5ExpTestFilter.{hpp,cpp}).
+// MC3D_TESTFILTER_PADE: 11-point RHS, pentadiagonal LHS (v2, 0, v0, 0, v2),
+// cyclic or with nodes 0..4 / N-5..N-1 explicitly filtered; MC3D_TESTFILTER_EXP:
+// explicit 7-point filter. Both share the one-sided closures of nodes 0..2.
+LineOpHost build_testfilter_op(int type, int bc_type, int N) {
+    if (N <= 10) throw std::runtime_error("line length must be greater than 10 (src/Options.cpp:241-244)");
+    static const double B[3][6] = {{31.0 / 32.0, 5.0 / 32.0, -5.0 / 16.0, 5.0 / 16.0, -5.0 / 32.0, 1.0 / 32.0},
+                                   {1.0 / 32.0, 27.0 / 32.0, 5.0 / 16.0, -5.0 / 16.0, 5.0 / 32.0, -1.0 / 32.0},
+                                   {-1.0 / 32.0, 5.0 / 32.0, 11.0 / 16.0, 5.0 / 16.0, -5.0 / 32.0, 1.0 / 32.0}};
+    static const double w[4] = {11.0 / 16.0, 15.0 / 64.0, -3.0 / 32.0, 1.0 / 64.0};
+    static const double wi[6] = {7.0 / 24.0, 175.0 / 768.0, 5.0 / 48.0, 35.0 / 1536.0, 0.0, -1.0 / 1536.0};
+    const double v0 = 7.0 / 12.0, v1 = 0.0, v2 = 5.0 / 24.0;
+    LineOpHost op;
+    op.N = N;
+    op.deriv = false;
+    op.inv_dh = 1.0;
+    const bool per = bc_type == MC3D_PERIODIC_SOLVE;
+    // head row r on phi[0..bw-1]; tail row r (node N-1-r) mirrored onto phi[N-bw..N-1]
+    auto closures = [&](int H, int bw) {
+        op.bw = bw;
+        op.head.assign(H * bw, 0.0);
+        op.tail.assign(H * bw, 0.0);
+        for (int r = 0; r < 3; r++)
+            for (int k = 0; k < 6; k++) {
+                op.head[r * bw + k] = B[r][k];
+                op.tail[r * bw + (bw - 1 - k)] = B[r][k];
+            }
+    };
+    if (type == MC3D_TESTFILTER_EXP) {
+        op.H = 3;
+        for (int k = -3; k <= 3; k++) op.st[k + 3] = w[k < 0 ? -k : k];
+        if (per) {
+            op.kind = K_EXPL_PER;
+        } else {
+            op.kind = K_EXPL_DIR;
+            closures(3, 6);
+        }
+        return op;
+    }
+    if (type != MC3D_TESTFILTER_PADE) throw std::runtime_error("unknown test filter type");
+    op.H = 5;
+    for (int k = -5; k <= 5; k++) op.st[k + 5] = wi[k < 0 ? -k : k];
+    std::vector<double> dg(N, v0), lo(N, v1), up(N, v1), lo2(N, v2), up2(N, v2);
+    if (per) {
+        op.kind = K_PEN_PER;
+        const double cp[6] = {v2, v1, v2, v2, v1, v2};
+        pack_penta(op, lo2, lo, dg, up, up2, true, cp);
+        return op;
+    }
+    op.kind = K_PEN_DIR;
+    // nodes 0..4 and N-5..N-1: identity rows (CommN5PadeTestFilter.hpp:83-177)
+    for (int r = 0; r < 5; r++) {
+        dg[r] = dg[N - 1 - r] = 1.0;
+        up[r] = up2[r] = 0.0;
+    }
+    for (int i = 0; i < 4; i++) lo[i] = 0.0;
+    for (int i = 0; i < 3; i++) lo2[i] = 0.0;
+    for (int i = N - 7; i < N - 2; i++) lo2[i] = 0.0;
+    for (int i = N - 6; i < N - 1; i++) lo[i] = 0.0;
+    for (int i = N - 5; i < N - 1; i++) up[i] = 0.0;
+    for (int i = N - 5; i < N - 2; i++) up2[i] = 0.0;
+    closures(5, 8);
+    // nodes 3, 4: 7-point rows on phi[r-3..r+3] (CommN5PadeTestFilter.cpp:106-111, :125-130)
+    for (int r = 3; r < 5; r++)
+        for (int s = -3; s <= 3; s++) {
+            const double c = w[s < 0 ? -s : s];
+            op.head[r * 8 + (r + s)] = c;
+            op.tail[r * 8 + (7 - (r + s))] = c;
+        }
+    const double cp0[6] = {0, 0, 0, 0, 0, 0};
+    pack_penta(op, lo2, lo, dg, up, up2, false, cp0);
+    return op;
+}
+
 namespace {
 // Stationary interior of the factor arrays (equality after rounding to the
 // working precision) and the correction window.

@@ -68,6 +68,7 @@ int reg_segment_len(int N, int kind, int precision);
 
 LineOpHost build_deriv_op(int fd_type, int bc_type, int N, double dh);
 LineOpHost build_filter_op(int filter_type, double alphaF, int bc_type, int N);
+LineOpHost build_testfilter_op(int type, int bc_type, int N);
 
 // Device-side view (trivially copyable, passed by value to kernels).
 template <typename R>
@@ -165,7 +166,7 @@ struct Metrics {
 struct FluxParams {
     double mu_ref;
     double dxi[3];
-    int les;                 // 0 none, 1 Vreman inline, 2 mu_sgs field
+    int les;                 // 0 none, 1 Vreman inline, 2 mu_sgs field, 3 DSM fields
     double pr_t;
 };
 
@@ -173,9 +174,12 @@ template <typename R>
 int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st);
 
 // prim = rho, U, V, W, T of the stage state
+// les 3 (DSM): mu_sgs, k_sgs and tau_kk fields; T in prim[4] is the
+// temperature of p - tau_kk / 2, rhoE that of p
 template <typename R>
 int launch_flux(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
-                const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st);
+                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, R *const F[15],
+                cudaStream_t st);
 
 template <typename R>
 int launch_vreman(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
@@ -211,6 +215,68 @@ struct TimeState {
 };
 int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, int first_step,
                        cudaStream_t st);
+
+// ---- dynamic Smagorinsky model and SGS averaging (dsm.cu) ---------------
+template <typename R>
+struct DsmPrepMu {
+    const R *d[9];        // dU/dxi_d, dV/dxi_d, dW/dxi_d: d[3 * var + dir]
+    const double *q[4];   // stage state rho, rhoU, rhoV, rhoW
+    R *out[24];           // M_ij(2) x6, S_ij x6, |S|, rho, L_ij(t) x6, 2 rho |S|^2, rhoU, rhoV, rhoW
+    R *smag;              // |S| kept for the later kernels
+};
+template <typename R>
+struct DsmFinishMu {
+    const R *hat[24];     // the test-filtered out[] of DsmPrepMu
+    R *out[4];            // Lkk, C_I denominator, L_ij M_ij, M_ij M_ij
+    int use_taukk;
+};
+template <typename R>
+struct DsmMuTaukk {
+    const double *q[5];
+    const R *smag;
+    const R *avg[4];      // averaged Lkk, C_I denominator, L_ij M_ij, M_ij M_ij
+    R *mu_sgs, *taukk;
+    R *T;                 // temperature of p - tau_kk / 2 (written in place)
+    int use_taukk;
+};
+template <typename R>
+struct DsmPrepK {
+    const R *dT[3];
+    const double *q[4];
+    const R *T, *smag;
+    R *out[10];           // N_i(RHS) x3, rhoU_i T x3, rho T, gradT x3
+};
+template <typename R>
+struct DsmFinishK {
+    const R *hat[10];     // the test-filtered out[] of DsmPrepK
+    const R *rho_hat, *smag_hat, *ru_hat[3];
+    const double *q[4];
+    R *out[2];            // N_i N_i, N_i K_i
+};
+template <typename R>
+struct AvgBatch {
+    int nf;
+    const R *in[8];
+    R *out[8];
+};
+template <typename R>
+int launch_dsm_prep_mu(const Grid3 &g, const DsmPrepMu<R> &a, const Metrics<R> &m, cudaStream_t st);
+template <typename R>
+int launch_dsm_finish_mu(const Grid3 &g, const DsmFinishMu<R> &a, cudaStream_t st);
+template <typename R>
+int launch_dsm_mu_taukk(const Grid3 &g, const DsmMuTaukk<R> &a, cudaStream_t st);
+template <typename R>
+int launch_dsm_prep_k(const Grid3 &g, const DsmPrepK<R> &a, const Metrics<R> &m, cudaStream_t st);
+template <typename R>
+int launch_dsm_finish_k(const Grid3 &g, const DsmFinishK<R> &a, cudaStream_t st);
+template <typename R>
+int launch_dsm_ksgs(const Grid3 &g, const double *rho, const R *smag, const R *nini, const R *niki, R *ksgs,
+                    cudaStream_t st);
+// XI1/XI2/XI3 line means or the GLOBAL block mean of up to 8 fields (in may equal out);
+// scratch holds the FP64 partial sums of GLOBAL
+template <typename R>
+int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scratch, size_t scratch_doubles,
+                   cudaStream_t st);
 
 int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cudaStream_t st);
 int launch_nonfinite_check(const Grid3 &g, const double *const q[5], int *flag, cudaStream_t st);

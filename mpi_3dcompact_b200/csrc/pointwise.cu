@@ -4,28 +4,9 @@
 // Grid-stride loops over x-fastest fields; one thread per point per iteration.
 #include <cmath>
 
-#include "mc3d_internal.h"
+#include "pointwise_common.cuh"
 
 namespace mc3d {
-
-constexpr double GAMMA = 1.4;        // src/IdealGas.hpp:38-46
-constexpr double PR = 0.7;
-constexpr double R_GAS = (1.0 / 1.4) / 1.0 / 1.0;
-constexpr double CP = R_GAS * GAMMA / (GAMMA - 1.0);
-
-static int grid_for(long long n, int block) {
-    long long g = (n + block - 1) / block;
-    int sms = 148;
-    long long cap = (long long)sms * 16;
-    if (g > cap) g = cap;
-    if (g < 1) g = 1;
-    return (int)g;
-}
-
-template <typename R>
-__device__ __forceinline__ R met(const Metrics<R> &m, int c, long long i) {
-    return m.constant ? m.c[c] : m.m[c][i];
-}
 
 __device__ __forceinline__ float mu_of_T(float T, double mu_ref) { return (float)mu_ref * powf(T, 0.76f); }
 __device__ __forceinline__ double mu_of_T(double T, double mu_ref) { return mu_ref * pow(T, 0.76); }
@@ -183,8 +164,8 @@ enum MetForm { MET_FIELD = 0, MET_CONST = 1, MET_DIAG = 2 };
 
 template <typename R, int MET>
 __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&dd)[12], const R (&mj)[10], R msgs,
-                                           const Metrics<R> &m, const FluxParams &fp, R d1c, R iJc, double dvol,
-                                           R (&o)[15]) {
+                                           R ksgs, R tk, const Metrics<R> &m, const FluxParams &fp, R d1c, R iJc,
+                                           double dvol, R (&o)[15]) {
     constexpr bool DIAG = MET == MET_DIAG;
     const R J = MET == MET_FIELD ? mj[0] : m.c[0];
     const R J11 = MET == MET_FIELD ? mj[1] : m.c[1], J12 = MET == MET_FIELD ? mj[2] : m.c[2],
@@ -196,7 +177,8 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&
     // p and rhoE from the ideal-gas relations (src/IdealGas.hpp:64-78)
     R p = rho * (R)R_GAS * T;
     R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
-    R rhoE = p / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
+    // with DSM, p (and T, mu) carry -tau_kk / 2 but rhoE is the state's (Core.cpp:573-584)
+    R rhoE = (fp.les == 3 ? p + (R)0.5 * tk : p) / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
     R mu = mu_of_T(T, fp.mu_ref);
     R Ucurv = DIAG ? J11 * U : J11 * U + J12 * V + J13 * W;
     R Vcurv = DIAG ? J22 * V : J21 * U + J22 * V + J23 * W;
@@ -218,7 +200,8 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&
         if (fp.les == 1) mu_sgs = vreman_mu<R>(gu, rho, MET != MET_FIELD ? d1c : vreman_d1<R>(dvol, J));
         else mu_sgs = msgs;
         mu_eff = mu + mu_sgs;
-        k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
+        if (fp.les == 3) k_eff = (R)CP * mu / (R)PR + ksgs;   // Core.cpp:636-639
+        else k_eff = (R)CP * (mu / (R)PR + mu_sgs / (R)fp.pr_t);
         if (mu_eff < (R)0) mu_eff = 0;
         if (k_eff < (R)0) k_eff = 0;
     } else {
@@ -299,7 +282,9 @@ template <typename R, int MET, int NP>
 __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
                                                       const R *__restrict__ r2, const R *__restrict__ r3,
                                                       const R *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
-                                                      FluxParams fp, const R *__restrict__ mu_sgs_f, OutPtrs15 op) {
+                                                      FluxParams fp, const R *__restrict__ mu_sgs_f,
+                                                      const R *__restrict__ ksgs_f, const R *__restrict__ taukk_f,
+                                                      OutPtrs15 op) {
     const R *const *d = reinterpret_cast<const R *const *>(dp.p);
     R *const *F = reinterpret_cast<R *const *>(op.p);
     const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
@@ -309,7 +294,7 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nit; j += (long long)gridDim.x * blockDim.x) {
         const long long i = NP * j;
         const bool two = i + 1 < n;
-        R rho[NP], U[NP], V[NP], Wv[NP], T[NP], dd[12][NP], mj[10][NP], ms[NP];
+        R rho[NP], U[NP], V[NP], Wv[NP], T[NP], dd[12][NP], mj[10][NP], ms[NP], ks[NP], tk[NP];
         ld_np<R, NP>(r0, i, two, rho);
         ld_np<R, NP>(r1, i, two, U);
         ld_np<R, NP>(r2, i, two, V);
@@ -321,7 +306,11 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
 #pragma unroll
             for (int c = 0; c < 10; c++) ld_np<R, NP>(m.m[c], i, two, mj[c]);
         }
-        if (fp.les == 2) ld_np<R, NP>(mu_sgs_f, i, two, ms);
+        if (fp.les >= 2) ld_np<R, NP>(mu_sgs_f, i, two, ms);
+        if (fp.les == 3) {
+            ld_np<R, NP>(ksgs_f, i, two, ks);
+            ld_np<R, NP>(taukk_f, i, two, tk);
+        }
         R out[15][NP];
 #pragma unroll
         for (int q = 0; q < NP; q++) {
@@ -330,8 +319,8 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
             for (int k = 0; k < 12; k++) dq[k] = dd[k][q];
 #pragma unroll
             for (int c = 0; c < 10; c++) mq[c] = MET == MET_FIELD ? mj[c][q] : R(0);
-            flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], dq, mq, fp.les == 2 ? ms[q] : R(0), m, fp, d1c, iJc,
-                               dvol, oq);
+            flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], dq, mq, fp.les >= 2 ? ms[q] : R(0),
+                               fp.les == 3 ? ks[q] : R(0), fp.les == 3 ? tk[q] : R(0), m, fp, d1c, iJc, dvol, oq);
 #pragma unroll
             for (int k = 0; k < 15; k++) out[k][q] = oq[k];
         }
@@ -342,7 +331,8 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
 
 template <typename R>
 int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const Metrics<R> &m,
-                const FluxParams &p, const R *mu_sgs, R *const F[15], cudaStream_t st) {
+                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, R *const F[15],
+                cudaStream_t st) {
     DerivPtrs12 dp;
     for (int i = 0; i < 12; i++) dp.p[i] = d[i];
     OutPtrs15 op;
@@ -352,11 +342,11 @@ int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const
     bool diag = m.constant;
     for (int c : {2, 3, 4, 6, 7, 8}) diag = diag && m.c[c] == R(0);
     if (!m.constant)
-        flux_kernel<R, MET_FIELD, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+        flux_kernel<R, MET_FIELD, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
     else if (!diag)
-        flux_kernel<R, MET_CONST, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+        flux_kernel<R, MET_CONST, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
     else
-        flux_kernel<R, MET_DIAG, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, op);
+        flux_kernel<R, MET_DIAG, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -646,7 +636,7 @@ int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cud
 #define MC3D_INST(R)                                                                                              \
     template int launch_primitives<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);          \
     template int launch_flux<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,         \
-                                const FluxParams &, const R *, R *const[15], cudaStream_t);                       \
+                                const FluxParams &, const R *, const R *, const R *, R *const[15], cudaStream_t); \
     template int launch_vreman<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,       \
                                   const FluxParams &, R *, cudaStream_t);                                         \
     template int launch_rk_update<R>(const Grid3 &, const RkStage &, const R *const[5], double *const[5],         \

@@ -7,9 +7,12 @@
 //   primitives(qP) -> U,V,W,T                           (Core.cpp:1158-1197)
 //   3 sweeps: d/dxi_d of U,V,W,T -> 12 derivatives        (Core.cpp:239-348)
 //   flux: gradU, Vreman, tau, q, 15 flux components       (Core.cpp:548-752)
+//   (DSM: gradients of U,V,W; DSM mu_sgs/tau_kk with two test-filtered
+//    batches; gradient of the tau_kk-corrected T; k_sgs; then the flux)
 //   3 sweeps: -dF/dxi1, -dG/dxi2, -dH/dxi3 -> k2          (Core.cpp:350-466, 790-947)
 //   RK register update                                    (RK4.hpp, LSLDDRK4.hpp, ...)
 //   filter (last stage or every stage)                   (Core.cpp:949-1155)
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -25,10 +28,13 @@ struct mc3d_solver_s {
     mc3d::Grid3 g{};
     int prec = MC3D_FP64;
     double dxi[3] = {0, 0, 0};
-    mc3d::LineOpBuf dop[3], fop[3], vop[3];
+    mc3d::LineOpBuf dop[3], fop[3], vop[3], top[3];   // derivative, filter, Vreman averaging, DSM test filter
     double *q1[5] = {}, *qk[5] = {}, *q2[5] = {};
     void *k2[5] = {}, *rhs[5] = {}, *prim[5] = {}, *der[12] = {}, *flux[15] = {};
     void *tA[5] = {}, *tB[5] = {}, *tC[5] = {}, *mu_sgs = nullptr;
+    // DSM work fields: two banks of 24, |S|, tau_kk, k_sgs; FP64 partial sums of GLOBAL averaging
+    void *dA[24] = {}, *dB[24] = {}, *smag = nullptr, *taukk = nullptr, *ksgs = nullptr;
+    double *avg_scratch = nullptr;
     double *met64[10] = {};
     void *metR[10] = {};
     bool const_met = true;
@@ -54,10 +60,13 @@ struct mc3d_solver_s {
 
 namespace mc3d {
 
+// FP64 partial sums of GLOBAL averaging: up to 148 x 4 blocks for up to 8 fields
+constexpr size_t AVG_SCRATCH = 148 * 4 * 8;
+
 // kernel classes for the optional event timing
-enum KClass { KC_SWEEP = 0, KC_FLUX, KC_PRIM, KC_RK, KC_CFL, KC_TOREAL, KC_VREMAN, KC_COUNT };
+enum KClass { KC_SWEEP = 0, KC_FLUX, KC_PRIM, KC_RK, KC_CFL, KC_TOREAL, KC_VREMAN, KC_SGS, KC_COUNT };
 static const char *KC_NAME[KC_COUNT] = {"sweep_linesolve", "flux", "primitives", "rk_update", "cfl_dt", "to_fp32",
-                                        "vreman"};
+                                        "vreman", "sgs_pointwise"};
 
 static int tic(mc3d_solver s, int cls, double bytes) {
     if (!s->timing) return MC3D_OK;
@@ -215,14 +224,139 @@ static int primitives(mc3d_solver s, double *const q[5]) {
     return toc(s);
 }
 
-// RHS of one stage; s->prim holds rho, U, V, W, T of the stage state.
+// Test-filter sweeps of nf fields along Y, Z, X (DSMSGS::filterQuantity,
+// src/DSMSGS.hpp:120-128) in batches of at most 16: in -> tmp -> in -> tmp, so
+// the filtered fields end in tmp and in is overwritten.
 template <typename R>
-static int stage_rhs(mc3d_solver s) {
+static int test_filter3(mc3d_solver s, int nf, void *const *in, void *const *tmp) {
     int rc;
-    // gradients of U, V, W, T in each direction: der[3*var + dir]
+    for (int b0 = 0; b0 < nf; b0 += 16) {
+        const int nb = std::min(16, nf - b0);
+        if ((rc = sweep<R>(s, 1, s->top[1], nb, in + b0, tmp + b0, EPI_STORE, nullptr, nullptr, true))) return rc;
+        if ((rc = sweep<R>(s, 2, s->top[2], nb, tmp + b0, in + b0, EPI_STORE, nullptr, nullptr, true))) return rc;
+        if ((rc = sweep<R>(s, 0, s->top[0], nb, in + b0, tmp + b0, EPI_STORE, nullptr, nullptr, true))) return rc;
+    }
+    return MC3D_OK;
+}
+
+// AbstractSGS::doAveraging (src/AbstractSGS.cpp:13-160) of nf fields f[]:
+// LOCAL filters them along Y, Z, X with `ops` (f -> t -> f -> t: the result is
+// in t); XI1/XI2/XI3/GLOBAL average in place; NONE leaves them. Returns the
+// arrays that hold the result in res[].
+template <typename R>
+static int sgs_average(mc3d_solver s, int nf, void *const *f, void *const *t, const LineOpBuf *ops, void **res) {
+    int rc;
+    const int mode = s->cfg.les_averaging;
+    for (int i = 0; i < nf; i++) res[i] = f[i];
+    if (mode == MC3D_AVG_NONE) return MC3D_OK;
+    if (mode == MC3D_AVG_LOCAL) {
+        if ((rc = sweep<R>(s, 1, ops[1], nf, f, t, EPI_STORE, nullptr, nullptr, true))) return rc;
+        if ((rc = sweep<R>(s, 2, ops[2], nf, t, f, EPI_STORE, nullptr, nullptr, true))) return rc;
+        if ((rc = sweep<R>(s, 0, ops[0], nf, f, t, EPI_STORE, nullptr, nullptr, true))) return rc;
+        for (int i = 0; i < nf; i++) res[i] = t[i];
+        return MC3D_OK;
+    }
+    AvgBatch<R> b{};
+    b.nf = nf;
+    for (int i = 0; i < nf; i++) {
+        b.in[i] = (const R *)f[i];
+        b.out[i] = (R *)f[i];
+    }
+    s->launches += mode == MC3D_AVG_GLOBAL ? 2 : 1;
+    if ((rc = tic(s, KC_SGS, 2.0 * nf * sizeof(R) * (double)s->g.n()))) return rc;
+    if ((rc = launch_average<R>(s->g, mode, b, s->avg_scratch, AVG_SCRATCH, s->stream))) return rc;
+    return toc(s);
+}
+
+// DSMSGS::calcMuSGSTaukk (src/DSMSGS.hpp:130-331) on the stage state qP, then
+// p -= tau_kk / 2 and T of that pressure into prim[4] (Core.cpp:567-585).
+template <typename R>
+static int dsm_mu_taukk(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
+    int rc;
+    const double n = (double)s->g.n();
+    DsmPrepMu<R> a{};
+    for (int i = 0; i < 9; i++) a.d[i] = (const R *)s->der[i];
+    for (int v = 0; v < 4; v++) a.q[v] = qP[v];
+    for (int i = 0; i < 24; i++) a.out[i] = (R *)s->dA[i];
+    a.smag = (R *)s->smag;
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, (9.0 * sizeof(R) + 4.0 * 8 + 25.0 * sizeof(R)) * n))) return rc;
+    if ((rc = launch_dsm_prep_mu<R>(s->g, a, m, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
+    if ((rc = test_filter3<R>(s, 24, s->dA, s->dB))) return rc;   // filtered fields in dB
+    DsmFinishMu<R> fm{};
+    for (int i = 0; i < 24; i++) fm.hat[i] = (const R *)s->dB[i];
+    for (int i = 0; i < 4; i++) fm.out[i] = (R *)s->dA[i];
+    fm.use_taukk = s->cfg.dsm_use_taukk;
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, 28.0 * sizeof(R) * n))) return rc;
+    if ((rc = launch_dsm_finish_mu<R>(s->g, fm, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
+    void *avg[4];
+    if ((rc = sgs_average<R>(s, 4, s->dA, s->dA + 4, s->top, avg))) return rc;
+    DsmMuTaukk<R> mt{};
+    for (int v = 0; v < 5; v++) mt.q[v] = qP[v];
+    mt.smag = (const R *)s->smag;
+    for (int i = 0; i < 4; i++) mt.avg[i] = (const R *)avg[i];
+    mt.mu_sgs = (R *)s->mu_sgs;
+    mt.taukk = (R *)s->taukk;
+    mt.T = (R *)s->prim[4];
+    mt.use_taukk = s->cfg.dsm_use_taukk;
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, (5.0 * 8 + 8.0 * sizeof(R)) * n))) return rc;
+    if ((rc = launch_dsm_mu_taukk<R>(s->g, mt, s->stream))) return rc;
+    return toc(s);
+}
+
+// DSMSGS::calcKSGS (src/DSMSGS.hpp:333-443) with gradT of the corrected T.
+template <typename R>
+static int dsm_ksgs(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
+    int rc;
+    const double n = (double)s->g.n();
+    DsmPrepK<R> a{};
+    for (int i = 0; i < 3; i++) a.dT[i] = (const R *)s->der[9 + i];
+    for (int v = 0; v < 4; v++) a.q[v] = qP[v];
+    a.T = (const R *)s->prim[4];
+    a.smag = (const R *)s->smag;
+    for (int i = 0; i < 10; i++) a.out[i] = (R *)s->dA[i];
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, (5.0 * sizeof(R) + 4.0 * 8 + 10.0 * sizeof(R)) * n))) return rc;
+    if ((rc = launch_dsm_prep_k<R>(s->g, a, m, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
+    if ((rc = test_filter3<R>(s, 10, s->dA, s->dA + 10))) return rc;   // filtered fields in dA[10..19]
+    DsmFinishK<R> fk{};
+    for (int i = 0; i < 10; i++) fk.hat[i] = (const R *)s->dA[10 + i];
+    fk.smag_hat = (const R *)s->dB[12];
+    fk.rho_hat = (const R *)s->dB[13];
+    for (int i = 0; i < 3; i++) fk.ru_hat[i] = (const R *)s->dB[21 + i];
+    for (int v = 0; v < 4; v++) fk.q[v] = qP[v];
+    fk.out[0] = (R *)s->dA[0];
+    fk.out[1] = (R *)s->dA[1];
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, (15.0 * sizeof(R) + 8.0 + 2.0 * sizeof(R)) * n))) return rc;
+    if ((rc = launch_dsm_finish_k<R>(s->g, fk, s->stream))) return rc;
+    if ((rc = toc(s))) return rc;
+    void *avg[2];
+    if ((rc = sgs_average<R>(s, 2, s->dA, s->dA + 2, s->top, avg))) return rc;
+    s->launches++;
+    if ((rc = tic(s, KC_SGS, (8.0 + 4.0 * sizeof(R)) * n))) return rc;
+    if ((rc = launch_dsm_ksgs<R>(s->g, qP[0], (const R *)s->smag, (const R *)avg[0], (const R *)avg[1],
+                                 (R *)s->ksgs, s->stream)))
+        return rc;
+    return toc(s);
+}
+
+// RHS of one stage; s->prim holds rho, U, V, W, T of the stage state qP.
+template <typename R>
+static int stage_rhs(mc3d_solver s, double *const *qP) {
+    int rc;
+    const bool dsm = s->cfg.les_model == MC3D_DSM;
+    // gradients of U, V, W, T in each direction: der[3*var + dir]; with DSM
+    // the T gradient waits for the tau_kk correction of T
     for (int d = 0; d < 3; d++) {
         void *out[4] = {s->der[0 + d], s->der[3 + d], s->der[6 + d], s->der[9 + d]};
-        if ((rc = sweep<R>(s, d, s->dop[d], 4, s->prim + 1, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+        if ((rc = sweep<R>(s, d, s->dop[d], dsm ? 3 : 4, s->prim + 1, out, EPI_STORE, nullptr, nullptr, false)))
+            return rc;
     }
     const R *pr[5];
     for (int v = 0; v < 5; v++) pr[v] = (const R *)s->prim[v];
@@ -234,30 +368,41 @@ static int stage_rhs(mc3d_solver s) {
     fp.les = 0;
     const R *dd[12];
     for (int i = 0; i < 12; i++) dd[i] = (const R *)s->der[i];
+    const R *mu_sgs = (const R *)s->mu_sgs;
     if (s->cfg.les_model == MC3D_VREMAN) {
         if (s->cfg.les_averaging == MC3D_AVG_NONE) {
             fp.les = 1;
         } else {
-            // mu_sgs, then doAveraging LOCAL: Compact10(-0.49) along Y, Z, X (AbstractSGS.cpp:144-152)
+            // mu_sgs, then doAveraging with Compact10(-0.49) filters (VremanSGS.hpp:38-40)
             s->launches++;
             if ((rc = tic(s, KC_VREMAN, 11.0 * sizeof(R) * (double)s->g.n()))) return rc;
             if ((rc = launch_vreman<R>(s->g, pr, dd, m, fp, (R *)s->mu_sgs, s->stream))) return rc;
             if ((rc = toc(s))) return rc;
-            void *a[1] = {s->mu_sgs}, *t1[1] = {s->tA[0]}, *t2[1] = {s->tB[0]};
-            if ((rc = sweep<R>(s, 1, s->vop[1], 1, a, t1, EPI_STORE, nullptr, nullptr, true))) return rc;
-            if ((rc = sweep<R>(s, 2, s->vop[2], 1, t1, t2, EPI_STORE, nullptr, nullptr, true))) return rc;
-            if ((rc = sweep<R>(s, 0, s->vop[0], 1, t2, a, EPI_STORE, nullptr, nullptr, true))) return rc;
+            void *a[1] = {s->mu_sgs}, *t1[1] = {s->tA[0]}, *res[1];
+            if ((rc = sgs_average<R>(s, 1, a, t1, s->vop, res))) return rc;
+            mu_sgs = (const R *)res[0];
             fp.les = 2;
         }
+    } else if (dsm) {
+        if ((rc = dsm_mu_taukk<R>(s, qP, m))) return rc;
+        for (int d = 0; d < 3; d++) {
+            void *in[1] = {s->prim[4]}, *out[1] = {s->der[9 + d]};
+            if ((rc = sweep<R>(s, d, s->dop[d], 1, in, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+        }
+        if ((rc = dsm_ksgs<R>(s, qP, m))) return rc;
+        fp.les = 3;
     }
     R *F[15];
     for (int i = 0; i < 15; i++) F[i] = (R *)s->flux[i];
     s->launches++;
     {
-        double b = (5.0 + 12.0 + 15.0) * sizeof(R) + (fp.les == 2 ? sizeof(R) : 0) + (s->const_met ? 0 : 10.0 * sizeof(R));
+        double b = (5.0 + 12.0 + 15.0) * sizeof(R) + (fp.les >= 2 ? sizeof(R) : 0) + (fp.les == 3 ? 2.0 * sizeof(R) : 0) +
+                   (s->const_met ? 0 : 10.0 * sizeof(R));
         if ((rc = tic(s, KC_FLUX, b * (double)s->g.n()))) return rc;
     }
-    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, (const R *)s->mu_sgs, F, s->stream))) return rc;
+    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, mu_sgs, (const R *)s->ksgs, (const R *)s->taukk, F,
+                             s->stream)))
+        return rc;
     if ((rc = toc(s))) return rc;
     // divergence of the contravariant fluxes, accumulated into the RHS, then k2
     if ((rc = sweep<R>(s, 0, s->dop[0], 5, s->flux + 0, s->rhs, EPI_STORE_NEG, nullptr, nullptr, false))) return rc;
@@ -287,7 +432,7 @@ static int one_step(mc3d_solver s) {
         // already wrote unless a sub-step filter changed qk since
         if (st == 1 || s->cfg.substep_filtering)
             if ((rc = primitives<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
-        if ((rc = stage_rhs<R>(s))) return rc;
+        if ((rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
         RkStage rs{};
         rs.scheme = scheme;
         rs.stage = st;
@@ -343,9 +488,10 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     if (c.Nx <= 10 || c.Ny <= 10 || c.Nz <= 10)
         return fail(MC3D_ERR_CONFIG, "Number of grid points in any direction must be greater than 10");
     if (c.precision != MC3D_FP64 && c.precision != MC3D_FP32BULK) return fail(MC3D_ERR_CONFIG, "bad precision");
-    if (c.les_model == MC3D_DSM) return fail(MC3D_ERR_CONFIG, "LESMODEL=DSM is not available in this build");
-    if (c.les_model == MC3D_VREMAN && c.les_averaging != MC3D_AVG_NONE && c.les_averaging != MC3D_AVG_LOCAL)
-        return fail(MC3D_ERR_CONFIG, "LESAVERAGING other than NONE/LOCAL is not available in this build");
+    if (c.les_model == MC3D_DSM && c.dsm_test_filter != 1 && c.dsm_test_filter != 2)
+        return fail(MC3D_ERR_CONFIG, "DSMTESTFILTER must be 1 or 2");
+    if (c.les_averaging < MC3D_AVG_NONE || c.les_averaging > MC3D_AVG_GLOBAL)
+        return fail(MC3D_ERR_CONFIG, "unknown LESAVERAGING");
     for (int d = 0; d < 3; d++)
         if (c.bc_type[d] != MC3D_PERIODIC_SOLVE)
             return fail(MC3D_ERR_CONFIG, "DIRICHLET_SOLVE boundaries (walls, sponge) are not available in the solver yet");
@@ -374,6 +520,12 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
             if ((rc = upload_line_op(dh, c.precision, s->dop[d]))) break;
             if ((rc = upload_line_op(fh, c.precision, s->fop[d]))) break;
             if ((rc = upload_line_op(vh, c.precision, s->vop[d]))) break;
+            if (c.les_model == MC3D_DSM) {
+                // DSMTESTFILTER 1 -> Pade, 2 -> explicit (src/DSMSGS.hpp:57-67)
+                LineOpHost th = build_testfilter_op(c.dsm_test_filter == 1 ? MC3D_TESTFILTER_PADE : MC3D_TESTFILTER_EXP,
+                                                    c.bc_type[d], N[d]);
+                if ((rc = upload_line_op(th, c.precision, s->top[d]))) break;
+            }
         }
     } catch (const std::exception &ex) {
         rc = fail(MC3D_ERR_CONFIG, ex.what());
@@ -393,7 +545,15 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     for (int v = 0; v < 5 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
     for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
     for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
-    if (!rc && c.les_model == MC3D_VREMAN) rc = salloc(s, &s->mu_sgs, n * rb);
+    if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, &s->mu_sgs, n * rb);
+    if (c.les_model == MC3D_DSM) {
+        for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dA[i], n * rb);
+        for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dB[i], n * rb);
+        if (!rc) rc = salloc(s, &s->smag, n * rb);
+        if (!rc) rc = salloc(s, &s->taukk, n * rb);
+        if (!rc) rc = salloc(s, &s->ksgs, n * rb);
+    }
+    if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, (void **)&s->avg_scratch, AVG_SCRATCH * sizeof(double));
     if (!rc) rc = salloc(s, (void **)&s->ts, sizeof(TimeState));
     if (!rc) rc = salloc(s, (void **)&s->acc, 2 * sizeof(double));
     if (!rc) {
@@ -426,6 +586,7 @@ int mc3d_solver_destroy(mc3d_solver s) {
         free_line_op(s->dop[d]);
         free_line_op(s->fop[d]);
         free_line_op(s->vop[d]);
+        free_line_op(s->top[d]);
     }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;

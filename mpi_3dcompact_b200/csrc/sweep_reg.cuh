@@ -598,7 +598,9 @@ int launch_sweep_reg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R>
     MC3D_RCASE(K_TRI_PER, 4, LL)   \
     MC3D_RCASE(K_TRI_DIR, 4, LL)   \
     MC3D_RCASE(K_TRI_PER, 5, LL)   \
-    MC3D_RCASE(K_TRI_DIR, 5, LL)
+    MC3D_RCASE(K_TRI_DIR, 5, LL)   \
+    MC3D_RCASE(K_PEN_PER, 5, LL)   \
+    MC3D_RCASE(K_PEN_DIR, 5, LL)
     MC3D_RKINDS(32)
     if constexpr (sizeof(R) == 4) {
         MC3D_RKINDS(64)

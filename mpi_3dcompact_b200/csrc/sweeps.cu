@@ -783,6 +783,10 @@ static int dispatch_kind(const Grid3 &g, const LineOpDev<R> &op, const SweepBatc
     MC3D_CASE(K_TRI_DIR, 4)   // Compact8 Dirichlet
     MC3D_CASE(K_TRI_PER, 5)   // Compact10 periodic
     MC3D_CASE(K_TRI_DIR, 5)   // Compact10 Dirichlet
+    MC3D_CASE(K_PEN_PER, 5)   // DSM Pade test filter periodic
+    MC3D_CASE(K_PEN_DIR, 5)   // DSM Pade test filter Dirichlet
+    MC3D_CASE(K_EXPL_PER, 3)  // DSM explicit test filter periodic
+    MC3D_CASE(K_EXPL_DIR, 3)  // DSM explicit test filter Dirichlet
 #undef MC3D_CASE
     return fail(MC3D_ERR_CONFIG, "no line-solve kernel for this operator");
 }

@@ -387,6 +387,118 @@ def filt(f, d, ftype, af, bcs):
 
 
 # --------------------------------------------------------------------------
+# DSM test filters (src/CommN5PadeTestFilter.{hpp,cpp},
+# src/CommN5ExpTestFilter.{hpp,cpp}): commutative filters of filter-width
+# ratio 2, with the same one-sided closures at Dirichlet ends.
+# --------------------------------------------------------------------------
+TF_B = [[31.0 / 32.0, 5.0 / 32.0, -5.0 / 16.0, 5.0 / 16.0, -5.0 / 32.0, 1.0 / 32.0],    # node 0 (w*_n1)
+        [1.0 / 32.0, 27.0 / 32.0, 5.0 / 16.0, -5.0 / 16.0, 5.0 / 32.0, -1.0 / 32.0],    # node 1 (w*_n2)
+        [-1.0 / 32.0, 5.0 / 32.0, 11.0 / 16.0, 5.0 / 16.0, -5.0 / 32.0, 1.0 / 32.0]]    # node 2 (w*_n3)
+TF_W = [11.0 / 16.0, 15.0 / 64.0, -3.0 / 32.0, 1.0 / 64.0]                             # w0..w3
+TF_WI = [7.0 / 24.0, 175.0 / 768.0, 5.0 / 48.0, 35.0 / 1536.0, 0.0, -1.0 / 1536.0]     # wi0..wi5
+TF_V = (7.0 / 12.0, 0.0, 5.0 / 24.0)                                                    # v0, v1, v2
+
+
+def _closure_rows(phi, rhs, rows):
+    """Boundary rows of the test filters: node r on phi[0..5] and its mirror
+    node N-1-r on phi[N-1], phi[N-2], ... (CommN5ExpTestFilter.cpp:22-48)."""
+    n = phi.shape[-1]
+    for r in rows:
+        b = TF_B[r]
+        acc = b[0] * phi[..., 0]
+        acc2 = b[0] * phi[..., n - 1]
+        for k in range(1, 6):
+            acc = acc + b[k] * phi[..., k]
+            acc2 = acc2 + b[k] * phi[..., n - 1 - k]
+        rhs[..., r] = acc
+        rhs[..., n - 1 - r] = acc2
+
+
+def exp_test_filter_lines(phi, bc):
+    """CommN5ExpTestFilter::FilterPeriodic / FilterDirichlet
+    (src/CommN5ExpTestFilter.cpp:3-50): explicit 7-point filter."""
+    n = phi.shape[-1]
+    w = TF_W
+    out = np.zeros(phi.shape)
+    if bc == PERIODIC:
+        acc = w[3] * _roll(phi, -3)
+        for s in (-2, -1, 0, 1, 2, 3):
+            acc = acc + w[abs(s)] * _roll(phi, s)
+        return acc
+    acc = w[3] * phi[..., 0:n - 6]
+    for s in (-2, -1, 0, 1, 2, 3):
+        acc = acc + w[abs(s)] * phi[..., 3 + s:n - 3 + s]
+    out[..., 3:n - 3] = acc
+    _closure_rows(phi, out, (0, 1, 2))
+    return out
+
+
+def pade_test_filter_lines(phi, bc):
+    """CommN5PadeTestFilter::FilterPeriodic / FilterDirichlet
+    (src/CommN5PadeTestFilter.cpp:3-130, LHS of CommN5PadeTestFilter.hpp:56-178):
+    11-point RHS, pentadiagonal LHS (v2, v1, v0, v1, v2) with v1 = 0."""
+    n = phi.shape[-1]
+    v0, v1, v2 = TF_V
+    wi = TF_WI
+    dg = np.full(n, v0)
+    lo, up = np.full(n, v1), np.full(n, v1)
+    lo2, up2 = np.full(n, v2), np.full(n, v2)
+    if bc == PERIODIC:
+        rhs = wi[5] * _roll(phi, -5)
+        for s in range(-4, 6):
+            rhs = rhs + wi[abs(s)] * _roll(phi, s)
+        return cyclic_penta(lo2, lo, dg, up, up2, rhs, [v2, v1, v2, v2, v1, v2])
+    # nodes 0..4 and N-5..N-1 are explicitly filtered (identity LHS rows)
+    for r in range(5):
+        dg[r] = dg[n - 1 - r] = 1.0
+        up[r] = up2[r] = 0.0
+    lo[0:4] = 0.0
+    lo2[0:3] = 0.0
+    lo2[n - 7:n - 2] = 0.0
+    lo[n - 6:n - 1] = 0.0
+    up[n - 5:n - 1] = 0.0
+    up2[n - 5:n - 2] = 0.0
+    rhs = np.zeros(phi.shape)
+    acc = wi[5] * phi[..., 0:n - 10]
+    for s in range(-4, 6):
+        acc = acc + wi[abs(s)] * phi[..., 5 + s:n - 5 + s]
+    rhs[..., 5:n - 5] = acc
+    _closure_rows(phi, rhs, (0, 1, 2))
+    w = TF_W
+    for r in (3, 4):   # 7-point rows (CommN5PadeTestFilter.cpp:106-111, :125-130)
+        a = w[3] * phi[..., r - 3]
+        a2 = w[3] * phi[..., n - 1 - r + 3]
+        for s in (-2, -1, 0, 1, 2, 3):
+            a = a + w[abs(s)] * phi[..., r + s]
+            a2 = a2 + w[abs(s)] * phi[..., n - 1 - r - s]
+        rhs[..., r] = a
+        rhs[..., n - 1 - r] = a2
+    return solve_penta(lo2, lo, dg, up, up2, rhs)
+
+
+def test_filter(f, d, ftype, bcs):
+    """filterField of the DSM test filter along d, with the Dirichlet-face
+    pass-through of src/CommN5PadeTestFilter.cpp:134-241. ftype is the
+    LES.DSMTESTFILTER value: 1 = Pade, 2 = explicit (src/DSMSGS.hpp:57-67)."""
+    lines = _to_lines(f, d)
+    out = pade_test_filter_lines(lines, bcs[d]) if ftype == 1 else exp_test_filter_lines(lines, bcs[d])
+    others = [o for o in range(3) if o != d]
+    mask = np.zeros(f.shape, dtype=bool)
+    for o in others:
+        if bcs[o] == DIRICHLET:
+            ax = _AXIS[o]
+            sl0 = [slice(None)] * 3
+            sl1 = [slice(None)] * 3
+            sl0[ax] = 0
+            sl1[ax] = f.shape[ax] - 1
+            mask[tuple(sl0)] = True
+            mask[tuple(sl1)] = True
+    res = np.ascontiguousarray(_from_lines(out, d))
+    res[mask] = f[mask]
+    return res
+
+
+# --------------------------------------------------------------------------
 # Ideal gas (src/IdealGas.hpp:9-80)
 # --------------------------------------------------------------------------
 GAMMA, PR = 1.4, 0.7
@@ -442,6 +554,8 @@ class Config:
     substep_filtering: bool = False
     les: str = "NOMODEL"
     les_avg: str = "NONE"
+    dsm_test_filter: int = 1               # LES.DSMTESTFILTER (1 Pade, 2 explicit)
+    dsm_use_taukk: bool = True             # LES.DSMUSETAUKK
 
 
 @dataclass
@@ -510,12 +624,100 @@ class Oracle:
         c = 2.5 * 0.17 * 0.17
         mu_sgs = c * rho * ss
         mu_sgs = np.minimum(mu_sgs, 0.05 * d1 * np.sqrt(2.0 * abeta))
-        if self.cfg.les_avg == "LOCAL":
-            # doAveraging LOCAL: Compact10 filter alpha=-0.49, order Y, Z, X (AbstractSGS.cpp:144-152)
-            mu_sgs = self.f3(mu_sgs, (1, 2, 0), "COMPACT10", -0.49)
-        elif self.cfg.les_avg != "NONE":
-            raise NotImplementedError("LESAVERAGING=" + self.cfg.les_avg)
-        return mu_sgs
+        # VremanSGS averages with a Compact10 filter of alpha = -0.49 (VremanSGS.hpp:38-40)
+        return self.average(mu_sgs, lambda f, d: filt(f, d, "COMPACT10", -0.49, self.cfg.bc))
+
+    def average(self, phi, filt1):
+        """AbstractSGS::doAveraging (src/AbstractSGS.cpp:13-160) for LESAVERAGING:
+        XI1/XI2/XI3 replace phi by its mean along xi1/xi2/xi3, GLOBAL by its
+        mean over the block, LOCAL applies the SGS model's filter along Y, Z, X
+        (filt1(f, d) filters f along d); NONE leaves it."""
+        a = self.cfg.les_avg
+        if a == "NONE":
+            return phi
+        if a == "LOCAL":
+            for d in (1, 2, 0):
+                phi = filt1(phi, d)
+            return phi
+        if a == "GLOBAL":
+            return np.full(phi.shape, np.sum(phi) / phi.size)
+        ax = {"XI1_AVG": 2, "XI2_AVG": 1, "XI3_AVG": 0}[a]
+        m = np.sum(phi / phi.shape[ax], axis=ax, keepdims=True)
+        return np.broadcast_to(m, phi.shape).copy()
+
+    # -- dynamic Smagorinsky (src/DSMSGS.hpp:130-447) -------------------------
+    def _fq(self, phi):
+        """DSMSGS::filterQuantity: test filter along Y, Z, X (DSMSGS.hpp:120-128)."""
+        for d in (1, 2, 0):
+            phi = test_filter(phi, d, self.cfg.dsm_test_filter, self.cfg.bc)
+        return phi
+
+    def dsm_mu_taukk(self, gu, rho, ru, rv, rw):
+        """DSMSGS::calcMuSGSTaukk (DSMSGS.hpp:130-331): returns mu_sgs, taukk and
+        the filtered quantities calcKSGS reuses."""
+        tfr2 = 2.0 * 2.0
+        avg = lambda f: self.average(f, lambda g, d: test_filter(g, d, self.cfg.dsm_test_filter, self.cfg.bc))
+        S00, S11, S22 = gu[0][0], gu[1][1], gu[2][2]
+        S01 = 0.5 * (gu[0][1] + gu[1][0])
+        S02 = 0.5 * (gu[0][2] + gu[2][0])
+        S12 = 0.5 * (gu[1][2] + gu[2][1])
+        Smag = np.sqrt(2.0 * (S00 * S00 + S11 * S11 + S22 * S22) + 4.0 * (S01 * S01 + S02 * S02 + S12 * S12))
+        tr = S00 + S11 + S22
+        M2 = [2.0 * rho * Smag * (S00 - (1.0 / 3.0) * tr), 2.0 * rho * Smag * S01, 2.0 * rho * Smag * S02,
+              2.0 * rho * Smag * (S11 - (1.0 / 3.0) * tr), 2.0 * rho * Smag * S12,
+              2.0 * rho * Smag * (S22 - (1.0 / 3.0) * tr)]
+        M = [self._fq(m) for m in M2]              # M00, M01, M02, M11, M12, M22
+        rho_hat = self._fq(rho)
+        Sh = [self._fq(x) for x in (S00, S01, S02, S11, S12, S22)]
+        Smag_hat = self._fq(Smag)
+        trh = Sh[0] + Sh[3] + Sh[5]
+        c = 2.0 * tfr2 * rho_hat * Smag_hat
+        M = [M[0] - c * (Sh[0] - (1.0 / 3.0) * trh), M[1] - c * Sh[1], M[2] - c * Sh[2],
+             M[3] - c * (Sh[3] - (1.0 / 3.0) * trh), M[4] - c * Sh[4], M[5] - c * (Sh[5] - (1.0 / 3.0) * trh)]
+        Lt = [ru * ru / rho, ru * rv / rho, ru * rw / rho, rv * rv / rho, rv * rw / rho, rw * rw / rho]
+        L = [self._fq(x) for x in Lt]
+        ruh, rvh, rwh = self._fq(ru), self._fq(rv), self._fq(rw)
+        L = [L[0] - ruh * ruh / rho_hat, L[1] - ruh * rvh / rho_hat, L[2] - ruh * rwh / rho_hat,
+             L[3] - rvh * rvh / rho_hat, L[4] - rvh * rwh / rho_hat, L[5] - rwh * rwh / rho_hat]
+        if self.cfg.dsm_use_taukk:
+            alpha_hat = self._fq(2.0 * rho * Smag * Smag)
+            CIdenom = 2.0 * tfr2 * rho_hat * Smag_hat * Smag_hat - alpha_hat
+        Lkk = L[0] + L[3] + L[5]
+        LijMij = ((L[0] - (1.0 / 3.0) * Lkk) * M[0] + (L[3] - (1.0 / 3.0) * Lkk) * M[3]
+                  + (L[5] - (1.0 / 3.0) * Lkk) * M[5] + 2.0 * L[1] * M[1] + 2.0 * L[2] * M[2] + 2.0 * L[4] * M[4])
+        MijMij = (M[0] * M[0] + M[3] * M[3] + M[5] * M[5] + 2.0 * M[1] * M[1] + 2.0 * M[2] * M[2]
+                  + 2.0 * M[4] * M[4])
+        if self.cfg.dsm_use_taukk:
+            Lkk_avg = avg(Lkk)
+            CIdenom_avg = avg(CIdenom)
+        LijMij_avg = avg(LijMij)
+        MijMij_avg = avg(MijMij)
+        mu_sgs = rho * Smag * LijMij_avg / MijMij_avg
+        if self.cfg.dsm_use_taukk:
+            taukk = 2.0 * rho * Smag * Smag * Lkk_avg / CIdenom_avg
+        else:
+            taukk = np.zeros(rho.shape)
+        ctx = dict(Smag=Smag, rho_hat=rho_hat, Smag_hat=Smag_hat, ruh=ruh, rvh=rvh, rwh=rwh)
+        return mu_sgs, taukk, ctx
+
+    def dsm_ksgs(self, gradT, rho, ru, rv, rw, T, ctx):
+        """DSMSGS::calcKSGS (DSMSGS.hpp:333-443); K_i divides by rho, not
+        rho_hat (DSMSGS.hpp:406-408)."""
+        tfr2 = 2.0 * 2.0
+        avg = lambda f: self.average(f, lambda g, d: test_filter(g, d, self.cfg.dsm_test_filter, self.cfg.bc))
+        Smag, rho_hat, Smag_hat = ctx["Smag"], ctx["rho_hat"], ctx["Smag_hat"]
+        NR = [self._fq(rho * Smag * g) for g in gradT]
+        KR = [self._fq(x * T) for x in (ru, rv, rw)]
+        rhoT_hat = self._fq(rho * T)
+        gh = [self._fq(g) for g in gradT]
+        N = [tfr2 * rho_hat * Smag_hat * gh[i] - NR[i] for i in range(3)]
+        uh = (ctx["ruh"], ctx["rvh"], ctx["rwh"])
+        K = [-uh[i] * rhoT_hat / rho + KR[i] for i in range(3)]
+        NiNi = N[0] * N[0] + N[1] * N[1] + N[2] * N[2]
+        NiKi = K[0] * N[0] + K[1] * N[1] + K[2] * N[2]
+        NiNi_avg = avg(NiNi)
+        NiKi_avg = avg(NiKi)
+        return -CP * (NiKi_avg / NiNi_avg) * rho * Smag
 
     # -- one stage: preStepDerivatives + solveEqnSet (Core.cpp:468-947) ----
     def rhs(self, qP, k2):
@@ -534,12 +736,21 @@ class Oracle:
               [phys(dV, 0), phys(dV, 1), phys(dV, 2)],
               [phys(dW, 0), phys(dW, 1), phys(dW, 2)]]
         les = c.les != "NOMODEL"
-        mu_sgs = None
+        mu_sgs = k_sgs = None
         if c.les == "VREMAN":
             mu_sgs = self.vreman(gu, rhoP)
+        elif c.les == "DSM":
+            mu_sgs, taukk, ctx = self.dsm_mu_taukk(gu, rhoP, ruP, rvP, rwP)
+            # pressure with the SGS normal stresses; T, mu follow (Core.cpp:573-584)
+            p = p - 0.5 * taukk
+            T = p / (rhoP * R_GAS)
+            mu = c.mu_ref * np.power(T / 1.0, 0.76)
         elif les:
             raise NotImplementedError(c.les)
         dT = self.grad(T)
+        if c.les == "DSM":
+            gradT = [phys(dT, 0), phys(dT, 1), phys(dT, 2)]   # Core.cpp:596-600
+            k_sgs = self.dsm_ksgs(gradT, rhoP, ruP, rvP, rwP, T, ctx)
         dUdx, dUdy, dUdz = gu[0]
         dVdx, dVdy, dVdz = gu[1]
         dWdx, dWdy, dWdz = gu[2]
@@ -551,7 +762,10 @@ class Oracle:
         t23 = dVdz + dWdy
         if les:
             mu_eff = mu + mu_sgs
-            k_eff = CP * (mu / PR + mu_sgs / self.pr_t)
+            if c.les == "DSM":
+                k_eff = CP * mu / PR + k_sgs               # Core.cpp:637-639
+            else:
+                k_eff = CP * (mu / PR + mu_sgs / self.pr_t)
             mu_eff = np.where(mu_eff < 0.0, 0.0, mu_eff)
             k_eff = np.where(k_eff < 0.0, 0.0, k_eff)
         else:

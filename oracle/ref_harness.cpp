@@ -13,8 +13,9 @@
  *   run  <mesh> <ic.bin> <out.bin>        N steps (TIMESTEPPING.MAXTIMESTEP),
  *                                          then dump the conserved state.
  *   ops  <scheme> <dir> <in.bin> <out.bin> one operator on one field:
- *        scheme = PADE6|PENTA10|CD2 (derivative) or COMPACT8|COMPACT10 (filter,
- *        SOLVER.ALPHAF); dir = 0,1,2.
+ *        scheme = PADE6|PENTA10|CD2 (derivative), COMPACT8|COMPACT10 (filter,
+ *        SOLVER.ALPHAF) or TESTPADE|TESTEXP (the DSM test filters
+ *        CommN5PadeTestFilter / CommN5ExpTestFilter); dir = 0,1,2.
  *   metrics <mesh> <out.bin>               J, J11..J33 from solveForJacobians.
  * <mesh> is "cube:<L>" (x = L*xi, the HIT box) or "file:<path>" (x,y,z FP64).
  * All binary fields are FP64, x-fastest global order (i + Nx*(j + Ny*k)).
@@ -45,6 +46,8 @@ using namespace std;
 #include "RK4.hpp"
 #include "KenRK4.hpp"
 #include "LSLDDRK4.hpp"
+#include "CommN5PadeTestFilter.hpp"
+#include "CommN5ExpTestFilter.hpp"
 
 // wall-clock stamp at the end of every time step (postStep -> fullStepTemporalHook)
 static std::vector<double> g_step_stamps;
@@ -268,10 +271,12 @@ static int mode_ops(const string &scheme, int dir, const string &in, const strin
         else if (scheme == "PENTA10") op = new Penta10(s.d, bct, D);
         else op = new CD2(s.d, bct, D);
         op->calc1stDerivField(pin.data(), pout.data());
-    } else if (scheme == "COMPACT8" || scheme == "COMPACT10") {
+    } else if (scheme == "COMPACT8" || scheme == "COMPACT10" || scheme == "TESTPADE" || scheme == "TESTEXP") {
         AbstractFilter *op;
         if (scheme == "COMPACT8") op = new Compact8Filter(s.opt->alphaF, s.d, s.bc, bct, D);
-        else op = new Compact10Filter(s.opt->alphaF, s.d, s.bc, bct, D);
+        else if (scheme == "COMPACT10") op = new Compact10Filter(s.opt->alphaF, s.d, s.bc, bct, D);
+        else if (scheme == "TESTPADE") op = new CommN5PadeTestFilter(s.d, s.bc, bct, D);
+        else op = new CommN5ExpTestFilter(s.d, s.bc, bct, D);
         op->filterField(pin.data(), pout.data());
     } else {
         die("unknown operator " + scheme);

@@ -78,6 +78,8 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
         "[LES]",
         f"LESMODEL = {cfg.les}",
         f"LESAVERAGING = {cfg.les_avg}",
+        f"DSMTESTFILTER = {getattr(cfg, 'dsm_test_filter', 1)}",
+        f"DSMUSETAUKK = {'true' if getattr(cfg, 'dsm_use_taukk', True) else 'false'}",
     ]
     return "\n".join(lines) + "\n"
 

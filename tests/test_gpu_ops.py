@@ -1,6 +1,7 @@
 """GPU parity of the compact operators (C ABI mc3d_op_apply through the
-Pade6/Penta10/CD2/Compact8Filter/Compact10Filter mirrors) against fixtures made
-by the reference's own operator classes.
+Pade6/Penta10/CD2/Compact8Filter/Compact10Filter and DSM test-filter
+CommN5PadeTestFilter/CommN5ExpTestFilter mirrors) against fixtures made by the
+reference's own operator classes.
 
 Tolerances: FP64 max error <= 1e-13 relative to max|out| (the GPU replays the
 reference elimination with precomputed factors and reciprocal pivots, so only
@@ -33,7 +34,15 @@ def _make(op, d, bcs, shape, prec):
         return m.CD2(shape, bcs[d], d, precision=prec)
     if op == "COMPACT8":
         return m.Compact8Filter(G.OPS_ALPHA, shape, bcs, d, precision=prec)
+    if op == "TESTPADE":
+        return m.CommN5PadeTestFilter(shape, bcs, d, precision=prec)
+    if op == "TESTEXP":
+        return m.CommN5ExpTestFilter(shape, bcs, d, precision=prec)
     return m.Compact10Filter(G.OPS_ALPHA, shape, bcs, d, precision=prec)
+
+
+def _is_filter(op):
+    return op.startswith("COMPACT") or op.startswith("TEST")
 
 
 @pytest.mark.parametrize("prec", [m.FP64, m.FP32BULK])
@@ -49,7 +58,7 @@ def test_operator_matches_reference(op, bname, prec):
     for d in range(3):
         o = _make(op, d, bcs, f.shape, prec)
         y = torch.empty_like(x)
-        if op.startswith("COMPACT"):
+        if _is_filter(op):
             o.filterField(x, y)
         else:
             o.calc1stDerivField(x, y)
@@ -108,12 +117,15 @@ def test_segmented_lines_vs_oracle(n, bc, prec):
         x = torch.tensor(f, dtype=dt, device="cuda")
         bcs = [m.PERIODIC_SOLVE] * 3
         bcs[d] = bc
-        for op in ("PADE6", "PENTA10", "COMPACT8", "COMPACT10"):
+        for op in ("PADE6", "PENTA10", "COMPACT8", "COMPACT10", "TESTPADE", "TESTEXP"):
             o = _make(op, d, bcs, shape, prec)
             y = torch.empty_like(x)
             if op.startswith("COMPACT"):
                 o.filterField(x, y)
                 ref = O.filt(f, d, op, G.OPS_ALPHA, tuple(bcs))
+            elif op.startswith("TEST"):
+                o.filterField(x, y)
+                ref = O.test_filter(f, d, 1 if op == "TESTPADE" else 2, tuple(bcs))
             else:
                 o.calc1stDerivField(x, y)
                 dh = 1.0 / n if bc == m.PERIODIC_SOLVE else 1.0 / (n - 1.0)

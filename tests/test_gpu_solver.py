@@ -10,6 +10,8 @@ CurvilinearCSolver mirror).
   * General (non-constant) metric fields vs the oracle: <= 1e-12.
   * FP32-bulk vs FP64 on 32^3 HIT after 20 LSLDDRK4 steps: relative L2 per
     field <= 1e-5 (the error target stated for the FP32 path).
+  * Dynamic Smagorinsky (both test filters, XI2/GLOBAL averaging) on 64^3 vs
+    the oracle after two steps: 1e-12 (FP64), 1e-5 (FP32-bulk).
 """
 import math
 
@@ -28,7 +30,7 @@ def _opts(cfg: O.Config, precision=m.FP64):
     return m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
                      ts_type=cfg.ts_type, cfl=cfg.cfl, dt=cfg.dt, filter_step=cfg.filter_step,
                      substep_filtering=cfg.substep_filtering, les=cfg.les, les_avg=cfg.les_avg,
-                     precision=precision)
+                     precision=precision, dsm_test_filter=cfg.dsm_test_filter, dsm_use_taukk=cfg.dsm_use_taukk)
 
 
 def _run(cfg, ic, n, precision=m.FP64, metrics=None):
@@ -115,9 +117,24 @@ def test_mass_is_conserved():
 
 def test_solver_rejects_unsupported_configs():
     with pytest.raises(m.Mc3dError):
-        m.CurvilinearCSolver(m.Options(grid=16, les="DSM"))
+        m.CurvilinearCSolver(m.Options(grid=16, les="DSM", dsm_test_filter=3))
     with pytest.raises(m.Mc3dError):
         m.CurvilinearCSolver(m.Options(grid=(16, 16, 8)))
+
+
+@pytest.mark.parametrize("prec,tol", [(m.FP64, 1e-12), (m.FP32BULK, 1e-5)])
+@pytest.mark.parametrize("ft,avg", [(1, "XI2_AVG"), (2, "GLOBAL")])
+def test_dsm_64cube_vs_oracle(ft, avg, prec, tol):
+    """Dynamic Smagorinsky on 64^3 (segmented test-filter sweeps of 24 and 10
+    fields, averaging reductions) against the oracle after two steps."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    cfg = O.Config(N=(64, 64, 64), fd=("PADE6",) * 3, filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=0.001,
+                   les="DSM", les_avg=avg, dsm_test_filter=ft)
+    ic = hit_initial_condition(64, k0=4.0, seed=11, mt=0.3)
+    q, info, _ = _run(cfg, ic, 2, precision=prec)
+    qo, st = O.run(cfg, ic, 2)
+    for i in range(5):
+        assert H.rel_l2(q[i], qo[i]) <= tol, (i, H.rel_l2(q[i], qo[i]))
 
 
 @pytest.mark.parametrize("prec,tol", [(m.FP64, 1e-12), (m.FP32BULK, 1e-5)])

@@ -22,6 +22,8 @@ def test_oracle_ops_match_reference_fixtures(op, bname):
         ref = gold[f"{op}_{bname}_{d}"]
         if op in ("COMPACT8", "COMPACT10"):
             out = O.filt(f, d, op, G.OPS_ALPHA, bcs)
+        elif op in ("TESTPADE", "TESTEXP"):
+            out = O.test_filter(f, d, 1 if op == "TESTPADE" else 2, bcs)
         else:
             n = G.OPS_GRID[d]
             dh = 1.0 / n if bcs[d] == 0 else 1.0 / (n - 1.0)
