@@ -58,6 +58,7 @@ enum { MC3D_TVDRK3 = 0, MC3D_RK4 = 1, MC3D_KENRK4 = 2, MC3D_LSLDDRK4 = 3 }; /* R
 enum { MC3D_BC_PERIODIC = 0, MC3D_BC_INTERNALLY_PERIODIC = 1, MC3D_BC_SPONGE = 2,
        MC3D_BC_ADIABATIC_WALL = 3, MC3D_BC_CONST_T_WALL = 4, MC3D_BC_MOVING_ADIABATIC_WALL = 5,
        MC3D_BC_INLET = 6 };
+enum { MC3D_SPONGE_RECTILINEAR = 0, MC3D_SPONGE_CYLINDRICAL = 1 };   /* SpongeKind */
 /* precision of the bulk arithmetic; metrics, LU factors, the conserved state,
  * the RK registers and the time accumulators are FP64 in both */
 enum { MC3D_FP64 = 0, MC3D_FP32BULK = 1 };
@@ -91,6 +92,17 @@ typedef struct mc3d_config {
     int dsm_test_filter;     /* LES.DSMTESTFILTER (default 1): 1 = Pade test
                                 filter, 2 = explicit (src/DSMSGS.hpp:57-67)   */
     int dsm_use_taukk;       /* LES.DSMUSETAUKK (default 1)                  */
+    /* [SPONGE] (src/Options.hpp:161-175, read when a face is SPONGE) */
+    int sponge_kind;         /* SPONGE.KIND: MC3D_SPONGE_*                   */
+    double sponge_strength;  /* SPONGE.STRENGTH (default 1)                  */
+    double sponge_rect_perc[6];  /* SPONGE.RECT{X,Y,Z}{0,1}PERC, X0 X1 Y0 Y1 Z0 Z1 */
+    int sponge_cyl_orient;   /* SPONGE.CYLAXIS_ORIENT                        */
+    double sponge_cyl_axis[3];   /* SPONGE.CYLAXIS_X, _Y, _Z                 */
+    double sponge_rmin;      /* SPONGE.RMIN                                  */
+    /* tangential velocity of MOVING_ADIABATIC_WALL faces X0 X1 Y0 Y1 Z0 Z1:
+     * (V, W) on X faces, (U, W) on Y faces, (U, V) on Z faces; the reference
+     * sets them to zero in its constructor (src/CurvilinearCSolver.hpp:219-221) */
+    double wall_velocity[6][2];
 } mc3d_config;
 
 /* ---- configuration ---- */
@@ -100,6 +112,11 @@ int mc3d_config_default(mc3d_config *cfg);
  * LESMODEL also accepts NONE for NOMODEL. Unsupported but valid settings are
  * reported as MC3D_ERR_CONFIG. */
 int mc3d_config_from_ini(const char *path, mc3d_config *cfg);
+
+/* SpongeBC::initRectSpongeBC / initCylSpongeBC (src/SpongeBC.cpp:65-360):
+ * the sponge strength sigma of every point from the mesh coordinates (host
+ * arrays, x-fastest, Nx*Ny*Nz each) and the [SPONGE] options of cfg. */
+int mc3d_sponge_sigma(const mc3d_config *cfg, const double *x, const double *y, const double *z, double *sigma);
 
 /* ---- last error of the calling thread ---- */
 const char *mc3d_last_error(void);
@@ -148,8 +165,19 @@ int mc3d_solver_set_metrics(mc3d_solver s, const double *const metrics[10]);
  * tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156). */
 int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz);
 
-/* setInitialConditions from primitive fields (host, FP64): rho, U, V, W, p
- * (src/CurvilinearCSolver_BC.cpp:3-59). */
+/* Sponge strength sigma (host, FP64, x-fastest; e.g. from mc3d_sponge_sigma),
+ * required before set_initial when a face is SPONGE (SpongeBC::sigma,
+ * src/SpongeBC.cpp:42-61). */
+int mc3d_solver_set_sponge(mc3d_solver s, const double *sigma);
+/* Sponge target state rho, rhoU, rhoV, rhoW, rhoE (host, FP64), in place of
+ * the initial conserved state (SpongeBC::readSpongeAvgFromRestart,
+ * src/SpongeBC.cpp:426-487); call after set_initial. */
+int mc3d_solver_set_sponge_avg(mc3d_solver s, const double *const avg[5]);
+
+/* setInitialConditions from primitive fields (host, FP64): rho, U, V, W, p,
+ * with the wall conditions of the BC kinds (no-slip / moving velocity, the
+ * Neumann wall temperature, p and rhoE from rho and T) and the sponge target
+ * state (src/CurvilinearCSolver_BC.cpp:3-369). */
 int mc3d_solver_set_initial(mc3d_solver s, const double *rho, const double *U, const double *V,
                             const double *W, const double *p);
 /* Same from device FP64 primitive fields (no host copy). */

@@ -166,6 +166,16 @@ _FILT = {"COMPACT8": COMPACT8, "COMPACT10": COMPACT10}
 _RK = {"TVDRK3": TVDRK3, "RK4": RK4, "KENRK4": KENRK4, "LSLDDRK4": LSLDDRK4}
 _LES = {"NOMODEL": NOMODEL, "NONE": NOMODEL, "VREMAN": VREMAN, "DSM": 2}
 _AVG = {"NONE": 0, "XI1_AVG": 1, "XI2_AVG": 2, "XI3_AVG": 3, "LOCAL": 4, "GLOBAL": 5}
+_BCKIND = {"PERIODIC": 0, "INTERNALLY_PERIODIC": 1, "SPONGE": 2, "ADIABATIC_WALL": 3, "CONST_T_WALL": 4,
+           "MOVING_ADIABATIC_WALL": 5, "INLET": 6}
+
+
+def sponge_sigma(opt, x, y, z):
+    """SpongeBC sigma (src/SpongeBC.cpp:65-360) from mesh coordinates (host arrays)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+    out = np.empty(arrs[0].shape)
+    N.check(N.host_lib().mc3d_sponge_sigma(C.byref(opt.c), *[N.dptr(a) for a in arrs], N.dptr(out)))
+    return out
 
 
 class Options:
@@ -174,7 +184,7 @@ class Options:
     def __init__(self, grid=(64, 64, 64), fd="PADE6", filter="COMPACT10", alphaF=0.45, mu_ref=1e-3, rk="RK4",
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
-                 dsm_test_filter=1, dsm_use_taukk=True):
+                 dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -195,6 +205,20 @@ class Options:
         c.reference_quirks = int(bool(reference_quirks))
         c.dsm_test_filter = int(dsm_test_filter)
         c.dsm_use_taukk = int(bool(dsm_use_taukk))
+        # BC kinds of the faces X0, X1, Y0, Y1, Z0, Z1 (names of src/Options.hpp:21-27);
+        # default: PERIODIC on periodic directions, ADIABATIC_WALL otherwise
+        kinds = bc_kind or [("PERIODIC" if bc[f // 2] == PERIODIC_SOLVE else "ADIABATIC_WALL") for f in range(6)]
+        for f in range(6):
+            c.bc_kind[f] = _BCKIND[kinds[f]]
+        if sponge:   # {"kind": "RECTILINEAR"|"CYLINDRICAL", "strength", "rect_perc"[6], "cyl_axis"[3], "rmin", "orient"}
+            c.sponge_kind = 0 if sponge.get("kind", "RECTILINEAR") == "RECTILINEAR" else 1
+            c.sponge_strength = sponge.get("strength", 1.0)
+            for f, v in enumerate(sponge.get("rect_perc", [0.0] * 6)):
+                c.sponge_rect_perc[f] = v
+            c.sponge_cyl_orient = sponge.get("orient", 2)
+            for d, v in enumerate(sponge.get("cyl_axis", [0.0] * 3)):
+                c.sponge_cyl_axis[d] = v
+            c.sponge_rmin = sponge.get("rmin", 0.0)
         self.c = c
 
     @classmethod
@@ -239,8 +263,20 @@ class CurvilinearCSolver:
         p = (C.POINTER(C.c_double) * 10)(*[N.dptr(a) for a in arrs])
         N.check(N.host_lib().mc3d_solver_set_metrics(self._h, p))
 
+    def set_sponge(self, sigma):
+        """Sponge strength field (SpongeBC::sigma); needed before the initial condition."""
+        a = np.ascontiguousarray(sigma, dtype=np.float64)
+        N.check(N.host_lib().mc3d_solver_set_sponge(self._h, N.dptr(a)))
+
+    def set_sponge_avg(self, avg):
+        """Sponge target state rho, rhoU, rhoV, rhoW, rhoE (readSpongeAvgFromRestart)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in avg]
+        p = (C.POINTER(C.c_double) * 5)(*[N.dptr(a) for a in arrs])
+        N.check(N.host_lib().mc3d_solver_set_sponge_avg(self._h, p))
+
     def set_initial_conditions(self, rho, U, V, W, p):
-        """setInitialConditions from primitive host arrays (src/CurvilinearCSolver_BC.cpp:3-59)."""
+        """setInitialConditions from primitive host arrays, with the wall
+        conditions and sponge target (src/CurvilinearCSolver_BC.cpp:3-369)."""
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, U, V, W, p)]
         N.check(N.host_lib().mc3d_solver_set_initial(self._h, *[N.dptr(a) for a in arrs]))
 

@@ -43,7 +43,10 @@ class Config(C.Structure):
                 ("filter_step", C.c_int), ("substep_filtering", C.c_int), ("max_time_step", C.c_int),
                 ("max_time", C.c_double), ("les_model", C.c_int), ("les_averaging", C.c_int),
                 ("time_step0", C.c_int), ("time0", C.c_double), ("precision", C.c_int),
-                ("reference_quirks", C.c_int), ("dsm_test_filter", C.c_int), ("dsm_use_taukk", C.c_int)]
+                ("reference_quirks", C.c_int), ("dsm_test_filter", C.c_int), ("dsm_use_taukk", C.c_int),
+                ("sponge_kind", C.c_int), ("sponge_strength", C.c_double), ("sponge_rect_perc", C.c_double * 6),
+                ("sponge_cyl_orient", C.c_int), ("sponge_cyl_axis", C.c_double * 3), ("sponge_rmin", C.c_double),
+                ("wall_velocity", (C.c_double * 2) * 6)]
 
 
 _lib = None
@@ -84,6 +87,9 @@ def host_lib():
             "mc3d_solver_timing_report": (C.c_char_p, [vp]),
             "mc3d_hit_randvec": (ip, [C.POINTER(C.c_int), C.POINTER(dp), C.c_longlong, C.POINTER(dp)]),
             "mc3d_cfl_max_noalloc": (ip, [vp] * 8 + [dp] * 3 + [ip] * 3 + [dp] * 3 + [vp, vp]),
+            "mc3d_sponge_sigma": (ip, [C.POINTER(Config)] + [C.POINTER(dp)] * 4),
+            "mc3d_solver_set_sponge": (ip, [vp, C.POINTER(dp)]),
+            "mc3d_solver_set_sponge_avg": (ip, [vp, C.POINTER(C.POINTER(dp))]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)

@@ -67,6 +67,13 @@ int mc3d_config_default(mc3d_config *c) {
     c->reference_quirks = 1;
     c->dsm_test_filter = 1;   // src/Options.hpp:424-425 defaults
     c->dsm_use_taukk = 1;
+    c->sponge_kind = MC3D_SPONGE_RECTILINEAR;
+    c->sponge_strength = 1.0;   // src/Options.hpp:323
+    for (int f = 0; f < 6; f++) c->sponge_rect_perc[f] = 0.0;
+    c->sponge_cyl_orient = 2;
+    for (int d = 0; d < 3; d++) c->sponge_cyl_axis[d] = 0.0;
+    c->sponge_rmin = 0.0;
+    for (int f = 0; f < 6; f++) c->wall_velocity[f][0] = c->wall_velocity[f][1] = 0.0;
     return MC3D_OK;
 }
 
@@ -257,6 +264,35 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
             if (c->dsm_test_filter != 1 && c->dsm_test_filter != 2) throw CfgError{"DSMTESTFILTER must be 1 or 2"};
         }
         if (ini.has("LES.DSMUSETAUKK")) c->dsm_use_taukk = parse_bool("DSMUSETAUKK", ini.get("LES.DSMUSETAUKK"));
+        // [SPONGE]: read when a face is a sponge (src/Options.hpp:314-358)
+        bool sponge = false;
+        for (int f = 0; f < 6; f++) sponge = sponge || c->bc_kind[f] == MC3D_BC_SPONGE;
+        if (sponge) {
+            c->sponge_kind = parse_enum(ini, "SPONGE.KIND", {{"RECTILINEAR", MC3D_SPONGE_RECTILINEAR},
+                                                             {"CYLINDRICAL", MC3D_SPONGE_CYLINDRICAL}});
+            if (ini.has("SPONGE.STRENGTH")) c->sponge_strength = parse_double("STRENGTH", ini.get("SPONGE.STRENGTH"));
+            const char *pk[6] = {"SPONGE.RECTX0PERC", "SPONGE.RECTX1PERC", "SPONGE.RECTY0PERC",
+                                 "SPONGE.RECTY1PERC", "SPONGE.RECTZ0PERC", "SPONGE.RECTZ1PERC"};
+            if (c->sponge_kind == MC3D_SPONGE_RECTILINEAR) {
+                for (int f = 0; f < 6; f++)
+                    if (c->bc_kind[f] == MC3D_BC_SPONGE) {
+                        if (!ini.has(pk[f])) throw CfgError{std::string(pk[f]) + " is required"};
+                        c->sponge_rect_perc[f] = parse_double(pk[f], ini.get(pk[f]));
+                    }
+            } else {
+                const char *ck[4] = {"SPONGE.CYLAXIS_X", "SPONGE.CYLAXIS_Y", "SPONGE.CYLAXIS_Z", "SPONGE.RMIN"};
+                if (!ini.has("SPONGE.CYLAXIS_ORIENT")) throw CfgError{"SPONGE.CYLAXIS_ORIENT is required"};
+                c->sponge_cyl_orient = parse_int("CYLAXIS_ORIENT", ini.get("SPONGE.CYLAXIS_ORIENT"));
+                if (c->sponge_cyl_orient < 0 || c->sponge_cyl_orient > 2)
+                    throw CfgError{"SPONGE.CYLAXIS_ORIENT must be 0, 1 or 2"};
+                for (int k = 0; k < 4; k++) {
+                    if (!ini.has(ck[k])) throw CfgError{std::string(ck[k]) + " is required"};
+                    double v = parse_double(ck[k], ini.get(ck[k]));
+                    if (k < 3) c->sponge_cyl_axis[k] = v;
+                    else c->sponge_rmin = v;
+                }
+            }
+        }
         // [GPU]
         if (ini.has("GPU.PRECISION"))
             c->precision = parse_enum(ini, "GPU.PRECISION", {{"FP64", MC3D_FP64}, {"FP32BULK", MC3D_FP32BULK}});

@@ -168,6 +168,7 @@ struct FluxParams {
     double dxi[3];
     int les;                 // 0 none, 1 Vreman inline, 2 mu_sgs field, 3 DSM fields
     double pr_t;
+    int wall_mask;           // bit f: face f is a wall (mu there from the saved temperature)
 };
 
 template <typename R>
@@ -176,10 +177,12 @@ int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5]
 // prim = rho, U, V, W, T of the stage state
 // les 3 (DSM): mu_sgs, k_sgs and tau_kk fields; T in prim[4] is the
 // temperature of p - tau_kk / 2, rhoE that of p
+// with walls (p.wall_mask), mu on wall points comes from Tmu: the temperature
+// before the wall treatment, which preStepBCHandling leaves mu at
 template <typename R>
 int launch_flux(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
-                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, R *const F[15],
-                cudaStream_t st);
+                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, const R *Tmu,
+                R *const F[15], cudaStream_t st);
 
 template <typename R>
 int launch_vreman(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
@@ -215,6 +218,21 @@ struct TimeState {
 };
 int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, int first_step,
                        cudaStream_t st);
+
+// ---- boundary conditions (bc.cu) -------------------------------------------
+// face: 0 X0, 1 X1, 2 Y0, 3 Y1, 4 Z0, 5 Z1
+template <typename R>
+int launch_wall_prestep(const Grid3 &g, int face, int neumann, int fd_type, double vt1, double vt2,
+                        double *const q[5], R *const prim[5], cudaStream_t st);
+// Tmu = T on the points of the faces in wall_mask
+template <typename R>
+int launch_wall_save_T(const Grid3 &g, int wall_mask, const R *T, R *Tmu, cudaStream_t st);
+template <typename R>
+int launch_face_k2(const Grid3 &g, int face, int wall, const R *cont, const R *J, R Jc, const double *dt,
+                   R *const k2[5], cudaStream_t st);
+template <typename R>
+int launch_sponge_source(const Grid3 &g, const double *sigma, const double *const avg[5], const double *const q[5],
+                         const R *J, R Jc, R *const rhs[5], cudaStream_t st);
 
 // ---- dynamic Smagorinsky model and SGS averaging (dsm.cu) ---------------
 template <typename R>

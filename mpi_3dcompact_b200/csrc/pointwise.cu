@@ -163,9 +163,9 @@ __device__ __forceinline__ void st_np(T *p, long long i, bool two, const T (&x)[
 enum MetForm { MET_FIELD = 0, MET_CONST = 1, MET_DIAG = 2 };
 
 template <typename R, int MET>
-__device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&dd)[12], const R (&mj)[10], R msgs,
-                                           R ksgs, R tk, const Metrics<R> &m, const FluxParams &fp, R d1c, R iJc,
-                                           double dvol, R (&o)[15]) {
+__device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, R Tm, const R (&dd)[12], const R (&mj)[10],
+                                           R msgs, R ksgs, R tk, const Metrics<R> &m, const FluxParams &fp, R d1c,
+                                           R iJc, double dvol, R (&o)[15]) {
     constexpr bool DIAG = MET == MET_DIAG;
     const R J = MET == MET_FIELD ? mj[0] : m.c[0];
     const R J11 = MET == MET_FIELD ? mj[1] : m.c[1], J12 = MET == MET_FIELD ? mj[2] : m.c[2],
@@ -179,7 +179,7 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&
     R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
     // with DSM, p (and T, mu) carry -tau_kk / 2 but rhoE is the state's (Core.cpp:573-584)
     R rhoE = (fp.les == 3 ? p + (R)0.5 * tk : p) / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
-    R mu = mu_of_T(T, fp.mu_ref);
+    R mu = mu_of_T(Tm, fp.mu_ref);
     R Ucurv = DIAG ? J11 * U : J11 * U + J12 * V + J13 * W;
     R Vcurv = DIAG ? J22 * V : J21 * U + J22 * V + J23 * W;
     R Wcurv = DIAG ? J33 * W : J31 * U + J32 * V + J33 * W;
@@ -276,15 +276,23 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, const R (&
     o[14] = iJ * (f3 - g3);
 }
 
+// is linear index i on one of the faces in mask (bit f: 0 X0, 1 X1, 2 Y0, 3 Y1, 4 Z0, 5 Z1)
+__device__ __forceinline__ bool on_faces(const Grid3 &g, long long i, int mask) {
+    const long long ix = i % g.Nx, r = i / g.Nx, iy = r % g.Ny, iz = r / g.Ny;
+    return ((mask & 1) && ix == 0) || ((mask & 2) && ix == g.Nx - 1) || ((mask & 4) && iy == 0) ||
+           ((mask & 8) && iy == g.Ny - 1) || ((mask & 16) && iz == 0) || ((mask & 32) && iz == g.Nz - 1);
+}
+
 // NP consecutive points per thread (2 in FP32: paired 8-byte accesses), all
-// inputs of the iteration loaded before its 15 stores.
-template <typename R, int MET, int NP>
+// inputs of the iteration loaded before its 15 stores. WALL: mu on wall points
+// from Tmu.
+template <typename R, int MET, int NP, bool WALL>
 __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
                                                       const R *__restrict__ r2, const R *__restrict__ r3,
                                                       const R *__restrict__ r4, DerivPtrs12 dp, Metrics<R> m,
                                                       FluxParams fp, const R *__restrict__ mu_sgs_f,
                                                       const R *__restrict__ ksgs_f, const R *__restrict__ taukk_f,
-                                                      OutPtrs15 op) {
+                                                      const R *__restrict__ Tmu, OutPtrs15 op) {
     const R *const *d = reinterpret_cast<const R *const *>(dp.p);
     R *const *F = reinterpret_cast<R *const *>(op.p);
     const double dvol = fp.dxi[0] * fp.dxi[1] * fp.dxi[2];
@@ -319,7 +327,9 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
             for (int k = 0; k < 12; k++) dq[k] = dd[k][q];
 #pragma unroll
             for (int c = 0; c < 10; c++) mq[c] = MET == MET_FIELD ? mj[c][q] : R(0);
-            flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], dq, mq, fp.les >= 2 ? ms[q] : R(0),
+            R Tm = T[q];
+            if (WALL && fp.les != 3 && on_faces(g, i + q, fp.wall_mask)) Tm = Tmu[i + q];
+            flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], Tm, dq, mq, fp.les >= 2 ? ms[q] : R(0),
                                fp.les == 3 ? ks[q] : R(0), fp.les == 3 ? tk[q] : R(0), m, fp, d1c, iJc, dvol, oq);
 #pragma unroll
             for (int k = 0; k < 15; k++) out[k][q] = oq[k];
@@ -331,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
 
 template <typename R>
 int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const Metrics<R> &m,
-                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, R *const F[15],
+                const FluxParams &p, const R *mu_sgs, const R *k_sgs, const R *taukk, const R *Tmu, R *const F[15],
                 cudaStream_t st) {
     DerivPtrs12 dp;
     for (int i = 0; i < 12; i++) dp.p[i] = d[i];
@@ -341,12 +351,20 @@ int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const
     const int grid = grid_for((g.n() + NP - 1) / NP, 256);
     bool diag = m.constant;
     for (int c : {2, 3, 4, 6, 7, 8}) diag = diag && m.c[c] == R(0);
-    if (!m.constant)
-        flux_kernel<R, MET_FIELD, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
-    else if (!diag)
-        flux_kernel<R, MET_CONST, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
-    else
-        flux_kernel<R, MET_DIAG, NP><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, op);
+#define MC3D_FLUX(MF, WL) \
+    flux_kernel<R, MF, NP, WL><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, Tmu, op)
+    const bool wall = p.wall_mask != 0;
+    if (!m.constant) {
+        if (wall) MC3D_FLUX(MET_FIELD, true);
+        else MC3D_FLUX(MET_FIELD, false);
+    } else if (!diag) {
+        if (wall) MC3D_FLUX(MET_CONST, true);
+        else MC3D_FLUX(MET_CONST, false);
+    } else {
+        if (wall) MC3D_FLUX(MET_DIAG, true);
+        else MC3D_FLUX(MET_DIAG, false);
+    }
+#undef MC3D_FLUX
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -636,7 +654,8 @@ int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cud
 #define MC3D_INST(R)                                                                                              \
     template int launch_primitives<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);          \
     template int launch_flux<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,         \
-                                const FluxParams &, const R *, const R *, const R *, R *const[15], cudaStream_t); \
+                                const FluxParams &, const R *, const R *, const R *, const R *, R *const[15],    \
+                                cudaStream_t);                                                                   \
     template int launch_vreman<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,       \
                                   const FluxParams &, R *, cudaStream_t);                                         \
     template int launch_rk_update<R>(const Grid3 &, const RkStage &, const R *const[5], double *const[5],         \

@@ -18,6 +18,18 @@ inline int grid_for(long long n, int block) {
     return (int)g;
 }
 
+// kernel-argument bundles of five field pointers
+struct Q5d {
+    double *p[5];
+};
+struct Q5c {
+    const double *p[5];
+};
+template <typename R>
+struct P5w {
+    R *p[5];
+};
+
 template <typename R>
 __device__ __forceinline__ R met(const Metrics<R> &m, int c, long long i) {
     return m.constant ? m.c[c] : m.m[c][i];

@@ -35,6 +35,15 @@ struct mc3d_solver_s {
     // DSM work fields: two banks of 24, |S|, tau_kk, k_sgs; FP64 partial sums of GLOBAL averaging
     void *dA[24] = {}, *dB[24] = {}, *smag = nullptr, *taukk = nullptr, *ksgs = nullptr;
     double *avg_scratch = nullptr;
+    // sponge: strength and target state (FP64); walls present
+    double *sigma = nullptr, *spg_avg[5] = {};
+    bool have_sponge = false, have_walls = false, sigma_set = false;
+    // walls: temperature that mu at wall points follows (set_initial fills it
+    // with the initial temperature for the first stage; later stages save it
+    // before the wall treatment)
+    void *Tmu = nullptr;
+    int wall_mask = 0;
+    bool tmu_from_init = false;
     double *met64[10] = {};
     void *metR[10] = {};
     bool const_met = true;
@@ -64,9 +73,9 @@ namespace mc3d {
 constexpr size_t AVG_SCRATCH = 148 * 4 * 8;
 
 // kernel classes for the optional event timing
-enum KClass { KC_SWEEP = 0, KC_FLUX, KC_PRIM, KC_RK, KC_CFL, KC_TOREAL, KC_VREMAN, KC_SGS, KC_COUNT };
+enum KClass { KC_SWEEP = 0, KC_FLUX, KC_PRIM, KC_RK, KC_CFL, KC_TOREAL, KC_VREMAN, KC_SGS, KC_BC, KC_COUNT };
 static const char *KC_NAME[KC_COUNT] = {"sweep_linesolve", "flux", "primitives", "rk_update", "cfl_dt", "to_fp32",
-                                        "vreman", "sgs_pointwise"};
+                                        "vreman", "sgs_pointwise", "boundary"};
 
 static int tic(mc3d_solver s, int cls, double bytes) {
     if (!s->timing) return MC3D_OK;
@@ -224,6 +233,64 @@ static int primitives(mc3d_solver s, double *const q[5]) {
     return toc(s);
 }
 
+static bool is_wall_kind(int k) {
+    return k == MC3D_BC_ADIABATIC_WALL || k == MC3D_BC_CONST_T_WALL || k == MC3D_BC_MOVING_ADIABATIC_WALL;
+}
+
+// preStepBCHandling (src/CurvilinearCSolver_BC.cpp:372-700) on the stage
+// state qP and its primitives: no-slip walls of all faces X0..Z1 first, then
+// the moving walls.
+template <typename R>
+static int wall_prestep(mc3d_solver s, double *const *qP) {
+    if (!s->have_walls) return MC3D_OK;
+    int rc;
+    R *pr[5];
+    for (int v = 0; v < 5; v++) pr[v] = (R *)s->prim[v];
+    // mu keeps updateNonConservedData's value on the walls: keep that temperature
+    if (!s->tmu_from_init) {
+        s->launches += 6;
+        if ((rc = launch_wall_save_T<R>(s->g, s->wall_mask, pr[4], (R *)s->Tmu, s->stream))) return rc;
+    }
+    s->tmu_from_init = false;
+    for (int pass = 0; pass < 2; pass++)
+        for (int f = 0; f < 6; f++) {
+            const int k = s->cfg.bc_kind[f];
+            const bool noslip = k == MC3D_BC_ADIABATIC_WALL || k == MC3D_BC_CONST_T_WALL;
+            if (pass == 0 ? !noslip : k != MC3D_BC_MOVING_ADIABATIC_WALL) continue;
+            const int neumann = k != MC3D_BC_CONST_T_WALL;
+            const double *vt = s->cfg.wall_velocity[f];
+            s->launches++;
+            if ((rc = tic(s, KC_BC, 0.0))) return rc;
+            if ((rc = launch_wall_prestep<R>(s->g, f, neumann, s->cfg.fd_type[f >> 1], pass ? vt[0] : 0.0,
+                                             pass ? vt[1] : 0.0, qP, pr, s->stream)))
+                return rc;
+            if ((rc = toc(s))) return rc;
+        }
+    return MC3D_OK;
+}
+
+// postStepBCHandling (src/CurvilinearCSolver_BC.cpp:702-842): wall faces keep
+// -dt J dF_mass/dxi_d in the continuity k2, sponge faces zero the k2 entirely.
+template <typename R>
+static int face_poststep(mc3d_solver s) {
+    int rc;
+    R *k2[5];
+    for (int v = 0; v < 5; v++) k2[v] = (R *)s->k2[v];
+    const R *J = s->const_met ? nullptr : (const R *)s->metR[0];
+    for (int pass = 0; pass < 2; pass++)
+        for (int f = 0; f < 6; f++) {
+            const int k = s->cfg.bc_kind[f];
+            if (pass == 0 ? !is_wall_kind(k) : k != MC3D_BC_SPONGE) continue;
+            s->launches++;
+            if ((rc = tic(s, KC_BC, 0.0))) return rc;
+            if ((rc = launch_face_k2<R>(s->g, f, pass == 0, (const R *)s->tB[f >> 1], J, (R)s->met_c[0], &s->ts->dt,
+                                        k2, s->stream)))
+                return rc;
+            if ((rc = toc(s))) return rc;
+        }
+    return MC3D_OK;
+}
+
 // Test-filter sweeps of nf fields along Y, Z, X (DSMSGS::filterQuantity,
 // src/DSMSGS.hpp:120-128) in batches of at most 16: in -> tmp -> in -> tmp, so
 // the filtered fields end in tmp and in is overwritten.
@@ -366,6 +433,7 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
     for (int i = 0; i < 3; i++) fp.dxi[i] = s->dxi[i];
     fp.pr_t = 0.9;   // src/CurvilinearCSolver.hpp:232
     fp.les = 0;
+    fp.wall_mask = s->wall_mask;
     const R *dd[12];
     for (int i = 0; i < 12; i++) dd[i] = (const R *)s->der[i];
     const R *mu_sgs = (const R *)s->mu_sgs;
@@ -400,14 +468,38 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
                    (s->const_met ? 0 : 10.0 * sizeof(R));
         if ((rc = tic(s, KC_FLUX, b * (double)s->g.n()))) return rc;
     }
-    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, mu_sgs, (const R *)s->ksgs, (const R *)s->taukk, F,
-                             s->stream)))
+    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, mu_sgs, (const R *)s->ksgs, (const R *)s->taukk,
+                             (const R *)s->Tmu, F, s->stream)))
         return rc;
     if ((rc = toc(s))) return rc;
     // divergence of the contravariant fluxes, accumulated into the RHS, then k2
     if ((rc = sweep<R>(s, 0, s->dop[0], 5, s->flux + 0, s->rhs, EPI_STORE_NEG, nullptr, nullptr, false))) return rc;
     if ((rc = sweep<R>(s, 1, s->dop[1], 5, s->flux + 5, s->rhs, EPI_SUB, nullptr, nullptr, false))) return rc;
+    if (s->have_sponge) {
+        R *rh[5];
+        const double *qc[5], *ac[5];
+        for (int v = 0; v < 5; v++) {
+            rh[v] = (R *)s->rhs[v];
+            qc[v] = qP[v];
+            ac[v] = s->spg_avg[v];
+        }
+        s->launches++;
+        if ((rc = tic(s, KC_BC, (8.0 + 10.0 * 8 + 10.0 * sizeof(R)) * (double)s->g.n()))) return rc;
+        if ((rc = launch_sponge_source<R>(s->g, s->sigma, ac, qc, s->const_met ? nullptr : (const R *)s->metR[0],
+                                          (R)s->met_c[0], rh, s->stream)))
+            return rc;
+        if ((rc = toc(s))) return rc;
+    }
     if ((rc = sweep<R>(s, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->rhs, nullptr, false))) return rc;
+    if (s->have_walls || s->have_sponge) {
+        // wall faces need the wall-normal derivative of the mass flux alone
+        for (int d = 0; d < 3; d++) {
+            if (!is_wall_kind(s->cfg.bc_kind[2 * d]) && !is_wall_kind(s->cfg.bc_kind[2 * d + 1])) continue;
+            void *in[1] = {s->flux[5 * d]}, *out[1] = {s->tB[d]};
+            if ((rc = sweep<R>(s, d, s->dop[d], 1, in, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+        }
+        if ((rc = face_poststep<R>(s))) return rc;
+    }
     return MC3D_OK;
 }
 
@@ -432,6 +524,7 @@ static int one_step(mc3d_solver s) {
         // already wrote unless a sub-step filter changed qk since
         if (st == 1 || s->cfg.substep_filtering)
             if ((rc = primitives<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
+        if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
         if ((rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
         RkStage rs{};
         rs.scheme = scheme;
@@ -492,9 +585,9 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         return fail(MC3D_ERR_CONFIG, "DSMTESTFILTER must be 1 or 2");
     if (c.les_averaging < MC3D_AVG_NONE || c.les_averaging > MC3D_AVG_GLOBAL)
         return fail(MC3D_ERR_CONFIG, "unknown LESAVERAGING");
-    for (int d = 0; d < 3; d++)
-        if (c.bc_type[d] != MC3D_PERIODIC_SOLVE)
-            return fail(MC3D_ERR_CONFIG, "DIRICHLET_SOLVE boundaries (walls, sponge) are not available in the solver yet");
+    for (int f = 0; f < 6; f++)
+        if (c.bc_kind[f] == MC3D_BC_INLET)
+            return fail(MC3D_ERR_CONFIG, "INLET faces have no boundary treatment in the reference solver");
     if (c.filter_step < 1) return fail(MC3D_ERR_CONFIG, "FILTERSTEP must be >= 1");
     MC3D_CUDA_TRY(cudaSetDevice(device));
     mc3d_solver s = new mc3d_solver_s();
@@ -503,6 +596,11 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     s->prec = c.precision;
     s->g = Grid3{c.Nx, c.Ny, c.Nz};
     s->host_time_step = c.time_step0;
+    for (int f = 0; f < 6; f++) {
+        s->have_walls = s->have_walls || is_wall_kind(c.bc_kind[f]);
+        s->have_sponge = s->have_sponge || c.bc_kind[f] == MC3D_BC_SPONGE;
+        if (is_wall_kind(c.bc_kind[f])) s->wall_mask |= 1 << f;
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete s;
@@ -554,6 +652,11 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         if (!rc) rc = salloc(s, &s->ksgs, n * rb);
     }
     if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, (void **)&s->avg_scratch, AVG_SCRATCH * sizeof(double));
+    if (s->have_walls && !rc) rc = salloc(s, &s->Tmu, n * rb);
+    if (s->have_sponge) {
+        if (!rc) rc = salloc(s, (void **)&s->sigma, n * sizeof(double));
+        for (int v = 0; v < 5 && !rc; v++) rc = salloc(s, (void **)&s->spg_avg[v], n * sizeof(double));
+    }
     if (!rc) rc = salloc(s, (void **)&s->ts, sizeof(TimeState));
     if (!rc) rc = salloc(s, (void **)&s->acc, 2 * sizeof(double));
     if (!rc) {
@@ -665,20 +768,73 @@ static int set_initial_impl(mc3d_solver s, const double *rho, const double *U, c
         MC3D_CUDA_TRY(cudaMemcpy(hp.data(), p, n * 8, cudaMemcpyDeviceToHost));
         rho = hr.data(); U = hu.data(); V = hv.data(); W = hw.data(); p = hp.data();
     }
-    const double gamma = 1.4;
+    const double gamma = 1.4, Rg = 1.0 / 1.4;
+    if (s->have_sponge && !s->sigma_set) return fail(MC3D_ERR_CONFIG, "set the sponge strength before the initial condition");
+    std::vector<double> uu(U, U + n), vv(V, V + n), ww(W, W + n), T;
+    if (s->have_walls) {
+        // wall conditions of setInitialConditions (src/CurvilinearCSolver_BC.cpp:60-313): no-slip
+        // faces X0..Z1, then moving walls; the Neumann wall temperature uses the
+        // scheme of the wall-normal direction. On X1 the reference takes it for
+        // CONST_T_WALL rather than ADIABATIC_WALL (:98).
+        T.resize(n);
+        for (size_t i = 0; i < n; i++) T[i] = p[i] / (rho[i] * Rg);
+        // mu of the first stage stays that of this temperature on the walls
+        if (s->prec == MC3D_FP64) {
+            MC3D_CUDA_TRY(cudaMemcpy(s->Tmu, T.data(), n * 8, cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> tf(T.begin(), T.end());
+            MC3D_CUDA_TRY(cudaMemcpy(s->Tmu, tf.data(), n * 4, cudaMemcpyHostToDevice));
+        }
+        s->tmu_from_init = true;
+        const long long Nx = s->g.Nx, Ny = s->g.Ny, Nz = s->g.Nz;
+        const long long dimn[3] = {Nx, Ny, Nz}, strd[3] = {1, Nx, Nx * Ny};
+        for (int pass = 0; pass < 2; pass++)
+            for (int f = 0; f < 6; f++) {
+                const int k = s->cfg.bc_kind[f], d = f >> 1, side = f & 1;
+                const bool noslip = k == MC3D_BC_ADIABATIC_WALL || k == MC3D_BC_CONST_T_WALL;
+                if (pass == 0 ? !noslip : k != MC3D_BC_MOVING_ADIABATIC_WALL) continue;
+                bool neumann = pass == 1 || (f == 1 ? k == MC3D_BC_CONST_T_WALL : k == MC3D_BC_ADIABATIC_WALL);
+                const double v1 = pass ? s->cfg.wall_velocity[f][0] : 0.0, v2 = pass ? s->cfg.wall_velocity[f][1] : 0.0;
+                const long long step = side ? -strd[d] : strd[d];
+                for (long long kk = 0; kk < Nz; kk++)
+                    for (long long jj = 0; jj < Ny; jj++)
+                        for (long long ii = 0; ii < Nx; ii++) {
+                            const long long c3[3] = {ii, jj, kk};
+                            if (c3[d] != (side ? dimn[d] - 1 : 0)) continue;
+                            const long long i = ii + Nx * (jj + Ny * kk);
+                            double uw[3];
+                            uw[d] = 0.0;
+                            uw[d == 0 ? 1 : 0] = v1;
+                            uw[d == 2 ? 1 : 2] = v2;
+                            uu[i] = uw[0];
+                            vv[i] = uw[1];
+                            ww[i] = uw[2];
+                            if (neumann) {
+                                double f6[6];
+                                for (int m = 0; m < 6; m++) f6[m] = (m < dimn[d] - 1) ? T[i + (m + 1) * step] : 0.0;
+                                T[i] = mc3d_calc_neumann(s->cfg.fd_type[d], f6);
+                            }
+                        }
+            }
+    }
     for (int v = 0; v < 5; v++) h[v].resize(n);
     for (size_t i = 0; i < n; i++) {
         double r = rho[i];
         h[0][i] = r;
-        h[1][i] = r * U[i];
-        h[2][i] = r * V[i];
-        h[3][i] = r * W[i];
-        h[4][i] = p[i] / (gamma - 1.0) + 0.5 * r * (U[i] * U[i] + V[i] * V[i] + W[i] * W[i]);
+        h[1][i] = r * uu[i];
+        h[2][i] = r * vv[i];
+        h[3][i] = r * ww[i];
+        // with walls p and rhoE follow from rho and T everywhere (src/CurvilinearCSolver_BC.cpp:314-323)
+        const double pp = s->have_walls ? r * Rg * T[i] : p[i];
+        h[4][i] = pp / (gamma - 1.0) + 0.5 * r * (uu[i] * uu[i] + vv[i] * vv[i] + ww[i] * ww[i]);
         if (!std::isfinite(h[4][i]) || !(r > 0)) return fail(MC3D_ERR_NONFINITE, "non-finite or non-positive initial state");
     }
     for (int v = 0; v < 5; v++) {
         MC3D_CUDA_TRY(cudaMemcpyAsync(s->q1[v], h[v].data(), n * 8, cudaMemcpyHostToDevice, s->stream));
         MC3D_CUDA_TRY(cudaMemsetAsync(s->k2[v], 0, n * (s->prec == MC3D_FP64 ? 8 : 4), s->stream));
+        // the sponge target starts as the initial state (src/CurvilinearCSolver_BC.cpp:325-341)
+        if (s->have_sponge)
+            MC3D_CUDA_TRY(cudaMemcpyAsync(s->spg_avg[v], h[v].data(), n * 8, cudaMemcpyHostToDevice, s->stream));
     }
     MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->initialized = true;
@@ -692,6 +848,28 @@ int mc3d_solver_set_initial(mc3d_solver s, const double *rho, const double *U, c
 int mc3d_solver_set_initial_device(mc3d_solver s, const double *rho, const double *U, const double *V,
                                    const double *W, const double *p) {
     return set_initial_impl(s, rho, U, V, W, p, true);
+}
+
+int mc3d_solver_set_sponge(mc3d_solver s, const double *sigma) {
+    if (!s || !sigma) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->have_sponge) return fail(MC3D_ERR_CONFIG, "no face is a SPONGE");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaMemcpyAsync(s->sigma, sigma, (size_t)s->g.n() * 8, cudaMemcpyHostToDevice, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->sigma_set = true;
+    return MC3D_OK;
+}
+
+int mc3d_solver_set_sponge_avg(mc3d_solver s, const double *const avg[5]) {
+    if (!s || !avg) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->have_sponge) return fail(MC3D_ERR_CONFIG, "no face is a SPONGE");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    for (int v = 0; v < 5; v++) {
+        if (!avg[v]) return fail(MC3D_ERR_ARG, "null argument");
+        MC3D_CUDA_TRY(cudaMemcpyAsync(s->spg_avg[v], avg[v], (size_t)s->g.n() * 8, cudaMemcpyHostToDevice, s->stream));
+    }
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
 }
 
 int mc3d_solver_step(mc3d_solver s, int nsteps) {

@@ -556,6 +556,83 @@ class Config:
     les_avg: str = "NONE"
     dsm_test_filter: int = 1               # LES.DSMTESTFILTER (1 Pade, 2 explicit)
     dsm_use_taukk: bool = True             # LES.DSMUSETAUKK
+    # face kinds X0, X1, Y0, Y1, Z0, Z1 (src/Options.hpp:21-27); None: PERIODIC on
+    # periodic directions, ADIABATIC_WALL on the others
+    bc_kind: tuple = None
+    # [SPONGE]: dict(kind="RECTILINEAR"|"CYLINDRICAL", strength, rect_perc[6], orient, cyl_axis[3], rmin)
+    sponge: dict = None
+    # periodic translation of each periodic direction's faces along its own axis
+    # (BC.PERIODICDISP*), for the reference runs; None: the 2*pi HIT box
+    periodic_box: tuple = None
+
+    def kinds(self):
+        if self.bc_kind is not None:
+            return tuple(self.bc_kind)
+        return tuple("PERIODIC" if self.bc[f // 2] == PERIODIC else "ADIABATIC_WALL" for f in range(6))
+
+
+def _ramp(strength, s):
+    return strength * (0.068 * np.power(s, 2.0) + 0.845 * np.power(s, 8.0))
+
+
+def sponge_sigma(cfg, x, y, z):
+    """SpongeBC::initRectSpongeBC / initCylSpongeBC (src/SpongeBC.cpp:65-262):
+    sponge strength from the mesh coordinates (fields shaped (Nz, Ny, Nx))."""
+    sp, k = cfg.sponge, cfg.kinds()
+    X = (x, y, z)
+    mn = [float(np.min(a)) for a in X]
+    mx = [float(np.max(a)) for a in X]
+    sigma = np.zeros(x.shape)
+    st = sp.get("strength", 1.0)
+    if sp.get("kind", "RECTILINEAR") == "RECTILINEAR":
+        perc = sp.get("rect_perc", [0.0] * 6)
+        for d in range(3):
+            L0 = perc[2 * d] * (mx[d] - mn[d])
+            L1 = perc[2 * d + 1] * (mx[d] - mn[d])
+            if k[2 * d] == "SPONGE":
+                dd = X[d] - mn[d]
+                m = dd < L0
+                sigma = np.where(m, np.fmax(_ramp(st, (L0 - dd) / L0), sigma), sigma)
+            if k[2 * d + 1] == "SPONGE":
+                dd = mx[d] - X[d]
+                m = dd < L1
+                sigma = np.where(m, np.fmax(_ramp(st, (X[d] - (mx[d] - L1)) / L1), sigma), sigma)
+        return sigma
+    if sp.get("orient", 2) != 2:
+        raise NotImplementedError("cylindrical sponge orientation")
+    ax = sp["cyl_axis"]
+    rmax = max(max(abs(mn[0] - ax[0]), abs(mx[0] - ax[0])), max(abs(mn[1] - ax[1]), abs(mx[1] - ax[1])))
+    rmin = sp["rmin"]
+    if k[3] == "SPONGE":
+        r = np.sqrt(np.power(x - ax[0], 2.0) + np.power(y - ax[1], 2.0))
+        m = r > rmin
+        sigma = np.where(m, np.fmax(_ramp(st, (r - rmin) / (rmax - rmin)), sigma), sigma)
+    return sigma
+
+
+_WALLS = ("ADIABATIC_WALL", "CONST_T_WALL", "MOVING_ADIABATIC_WALL")
+
+
+def _face_slices(f, shape):
+    """(face slice, slices of the points 1..6 inward) of face f on (Nz, Ny, Nx) arrays."""
+    ax = _AXIS[f // 2]
+    n = shape[ax]
+    side = f % 2
+    sl = [slice(None)] * 3
+    sl[ax] = n - 1 if side else 0
+    inward = []
+    for m in range(1, 7):
+        t = [slice(None)] * 3
+        t[ax] = n - 1 - m if side else m
+        inward.append(tuple(t))
+    return tuple(sl), inward
+
+
+def calc_neumann(scheme, f):
+    """calcNeumann (src/Pade6.cpp:395-397, src/Penta10.cpp:284-286, src/CD2.cpp:183)."""
+    if scheme == "CD2":
+        return (f[0] * 4.0 - f[1] * 1.0) / 3.0
+    return (f[0] * 360.0 - f[1] * 450.0 + f[2] * 400.0 - f[3] * 225.0 + f[4] * 72.0 - f[5] * 10.0) / 147.0
 
 
 @dataclass
@@ -574,8 +651,14 @@ class State:
 class Oracle:
     """The CurvilinearCSolver time step on one block (src/CurvilinearCSolver.hpp:25-379)."""
 
-    def __init__(self, cfg: Config, metrics=None):
+    def __init__(self, cfg: Config, metrics=None, sigma=None):
         self.cfg = cfg
+        self.sigma = sigma
+        self.kinds = cfg.kinds()
+        self.walls = any(k in _WALLS for k in self.kinds)
+        self.sponge_on = any(k == "SPONGE" for k in self.kinds)
+        if self.sponge_on and sigma is None:
+            raise ValueError("sponge faces need sigma")
         Nx, Ny, Nz = cfg.N
         # Domain with Lx=Ly=Lz=1 (src/Domain.hpp:45-79)
         self.dxi = [1.0 / n if b == PERIODIC else 1.0 / (n - 1.0) for n, b in zip(cfg.N, cfg.bc)]
@@ -720,11 +803,14 @@ class Oracle:
         return -CP * (NiKi_avg / NiNi_avg) * rho * Smag
 
     # -- one stage: preStepDerivatives + solveEqnSet (Core.cpp:468-947) ----
-    def rhs(self, qP, k2):
+    def rhs(self, qP, k2, prims=None):
+        """preStepDerivatives + solveEqnSet + postStepBCHandling on the stage
+        state qP with the primitives `prims` (U, V, W, p, T, mu, sos) of
+        updateNonConservedData as preStepBCHandling left them."""
         c = self.cfg
         J, Jm = self.J, self.Jm
         rhoP, ruP, rvP, rwP, reP = qP
-        U, V, W, p, T, mu, sos = primitives(qP, c.mu_ref)
+        U, V, W, p, T, mu, sos = prims if prims is not None else primitives(qP, c.mu_ref)
         Ucurv = Jm[0][0] * U + Jm[0][1] * V + Jm[0][2] * W
         Vcurv = Jm[1][0] * U + Jm[1][1] * V + Jm[1][2] * W
         Wcurv = Jm[2][0] * U + Jm[2][1] * V + Jm[2][2] * W
@@ -801,16 +887,62 @@ class Oracle:
         comps = [cont, m1, m2, m3, en]
         div = [[self.d(comp[0], 0), self.d(comp[1], 1), self.d(comp[2], 2)] for comp in comps]
         dt = self.state.dt
-        # solveContinuity/X/Y/ZMomentum/Energy, Core.cpp:790-947 (no sponge, zero hooks)
+        # sponge source sigma (avg - phi) (src/CurvilinearCSolver.hpp:293-295)
+        if self.sponge_on:
+            spg = [self.sigma * (self.spg_avg[e] - qP[e]) for e in range(5)]
+        else:
+            spg = [0.0] * 5
+        # solveContinuity/X/Y/ZMomentum/Energy, Core.cpp:790-947 (zero hooks)
         new = [None] * 5
-        new[0] = dt * J * (-div[0][0] - div[0][1] - div[0][2] + (0.0 + 0.0) / J)
+        new[0] = dt * J * (-div[0][0] - div[0][1] - div[0][2] + (spg[0] + 0.0) / J)
         for e in (1, 2, 3):
             # momentum accumulates into the previous k2 (Core.cpp:839,872,904)
-            t = k2[e] + (-div[e][0] - div[e][1] - div[e][2] + (0.0 + 0.0) / J)
+            t = k2[e] + (-div[e][0] - div[e][1] - div[e][2] + (spg[e] + 0.0) / J)
             new[e] = t * (dt * J)
-        t = -div[4][0] - div[4][1] - div[4][2] + (0.0 + 0.0) / J
+        t = -div[4][0] - div[4][1] - div[4][2] + (spg[4] + 0.0) / J
         new[4] = t * (dt * J)
+        # postStepBCHandling (src/CurvilinearCSolver_BC.cpp:702-842): walls keep the
+        # wall-normal mass-flux derivative in the continuity k2, sponge faces zero all
+        if self.walls or self.sponge_on:
+            for f in range(6):
+                if self.kinds[f] in _WALLS:
+                    sl, _ = _face_slices(f, rhoP.shape)
+                    new[0][sl] = -dt * J[sl] * div[0][f // 2][sl]
+                    for e in (1, 2, 3, 4):
+                        new[e][sl] = 0.0
+            for f in range(6):
+                if self.kinds[f] == "SPONGE":
+                    sl, _ = _face_slices(f, rhoP.shape)
+                    for e in range(5):
+                        new[e][sl] = 0.0
         return new
+
+    def wall_prestep(self, qP, prims):
+        """preStepBCHandling (src/CurvilinearCSolver_BC.cpp:372-700): no-slip walls
+        of faces X0..Z1, then moving walls; modifies the stage state qP in place
+        and returns the primitives with U, V, W, T, p replaced on the walls (mu
+        and sos keep their values)."""
+        U, V, W, p, T, mu, sos = [a.copy() if isinstance(a, np.ndarray) else a for a in prims]
+        rho, ru, rv, rw, re = qP
+        for pass_ in (0, 1):
+            for f in range(6):
+                k = self.kinds[f]
+                if pass_ == 0 and k not in ("ADIABATIC_WALL", "CONST_T_WALL"):
+                    continue
+                if pass_ == 1 and k != "MOVING_ADIABATIC_WALL":
+                    continue
+                sl, inward = _face_slices(f, rho.shape)
+                if k != "CONST_T_WALL":
+                    T[sl] = calc_neumann(self.cfg.fd[f // 2], [T[t] for t in inward])
+                U[sl] = 0.0
+                V[sl] = 0.0
+                W[sl] = 0.0
+                ru[sl] = 0.0
+                rv[sl] = 0.0
+                rw[sl] = 0.0
+                p[sl] = rho[sl] * R_GAS * T[sl]
+                re[sl] = p[sl] / (GAMMA - 1.0) + 0.5 * rho[sl] * (U[sl] * U[sl] + V[sl] * V[sl] + W[sl] * W[sl])
+        return U, V, W, p, T, mu, sos
 
     # -- time-step bookkeeping ---------------------------------------------
     def cfl(self, q):
@@ -845,17 +977,45 @@ class Oracle:
         """setInitialConditions, src/CurvilinearCSolver_BC.cpp:3-59 (periodic:
         no walls, no sponge)."""
         z = np.zeros_like(rho0)
+        if self.walls:
+            # wall conditions of setInitialConditions (src/CurvilinearCSolver_BC.cpp:60-323):
+            # on X1 the Neumann temperature is taken for CONST_T_WALL (:98)
+            U0, V0, W0 = U0.copy(), V0.copy(), W0.copy()
+            T = p0 / (rho0 * R_GAS)
+            mu_init = self.cfg.mu_ref * np.power(T / 1.0, 0.76)   # mu is not updated after the walls
+            for pass_ in (0, 1):
+                for f in range(6):
+                    k = self.kinds[f]
+                    if pass_ == 0 and k not in ("ADIABATIC_WALL", "CONST_T_WALL"):
+                        continue
+                    if pass_ == 1 and k != "MOVING_ADIABATIC_WALL":
+                        continue
+                    sl, inward = _face_slices(f, rho0.shape)
+                    U0[sl] = 0.0
+                    V0[sl] = 0.0
+                    W0[sl] = 0.0
+                    neumann = pass_ == 1 or (k == "CONST_T_WALL" if f == 1 else k == "ADIABATIC_WALL")
+                    if neumann:
+                        T[sl] = calc_neumann(self.cfg.fd[f // 2], [T[t] for t in inward])
+            p0 = rho0 * R_GAS * T
         rhoE = p0 / (GAMMA - 1.0) + 0.5 * rho0 * (U0 * U0 + V0 * V0 + W0 * W0)
         q1 = [rho0.copy(), rho0 * U0, rho0 * V0, rho0 * W0, rhoE]
+        if self.sponge_on:
+            self.spg_avg = [a.copy() for a in q1]
         self.state = State(q1=q1, qk=[z.copy() for _ in range(5)], k2=[z.copy() for _ in range(5)],
                            q2=[z.copy() for _ in range(5)], time=time, time_step=time_step)
         self.start_step = time_step
         T0 = p0 / (rho0 * R_GAS)
         self._prims = (U0, V0, W0, p0, T0, self.cfg.mu_ref * np.power(T0, 0.76), np.sqrt(GAMMA * p0 / rho0))
+        if self.walls:
+            # arrays as setInitialConditions leaves them: wall U, V, W, T; p and sos
+            # from rho and T; mu still that of the initial temperature
+            self._prims = (U0, V0, W0, p0, T, mu_init, np.sqrt(GAMMA * p0 / rho0))
 
     def _stage(self, qP, rk_step, last, update):
         st = self.state
-        st.k2 = self.rhs(qP, st.k2)
+        prims = self.wall_prestep(qP, self._prims) if self.walls else self._prims
+        st.k2 = self.rhs(qP, st.k2, prims)
         update(rk_step)
         if last or self.cfg.substep_filtering:
             if last:
@@ -935,6 +1095,18 @@ class Oracle:
         return 5 if getattr(self, "_lsldd_half", 1) == 1 else 6
 
 
+def ogrid_mesh(N, r0=0.5, ratio=1.08, span=2.0):
+    """O-grid around a cylinder of radius r0: xi1 = theta (periodic, internally),
+    xi2 = r (geometric spacing, wall at r0), xi3 = z (periodic, `span` long);
+    coordinates shaped (Nz, Ny, Nx)."""
+    Nx, Ny, Nz = N
+    th = 2.0 * math.pi * np.arange(Nx) / Nx
+    r = r0 * np.cumprod(np.concatenate([[1.0], np.full(Ny - 1, ratio)]))
+    zz = span * np.arange(Nz) / Nz
+    Z, Rr, TH = np.meshgrid(zz, r, th, indexing="ij")
+    return Rr * np.cos(TH), Rr * np.sin(TH), Z
+
+
 def cube_metrics(N, L=2.0 * math.pi):
     """Analytic metrics of the periodic cube x = L*xi (the HIT box of
     tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156): J_ii = 1/L,
@@ -946,10 +1118,10 @@ def cube_metrics(N, L=2.0 * math.pi):
     return [np.full(shp, 1.0 / L ** 3), d, z, z, z, d.copy(), z, z, z, d.copy()]
 
 
-def run(cfg: Config, ic, nsteps, metrics=None):
+def run(cfg: Config, ic, nsteps, metrics=None, sigma=None):
     """Run `nsteps` time steps from primitive ICs (rho, U, V, W, p) and return
     (conserved state rho1..rhoE1, state object)."""
-    o = Oracle(cfg, metrics if metrics is not None else cube_metrics(cfg.N))
+    o = Oracle(cfg, metrics if metrics is not None else cube_metrics(cfg.N), sigma=sigma)
     o.init(*ic)
     for _ in range(nsteps):
         o.step()

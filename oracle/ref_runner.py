@@ -30,7 +30,10 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
     (tests/hit/Samtaney_D4/MPI_3DCompact.in)."""
     Nx, Ny, Nz = cfg.N
     if kinds is None:
-        kinds = ["PERIODIC" if b == 0 else "ADIABATIC_WALL" for b in cfg.bc]
+        kinds = cfg.kinds() if hasattr(cfg, "kinds") else \
+            [k for b in cfg.bc for k in (("PERIODIC",) * 2 if b == 0 else ("ADIABATIC_WALL",) * 2)]
+    elif len(kinds) == 3:
+        kinds = [k for k in kinds for _ in range(2)]
     lines = [
         "[TIMESTEPPING]",
         f"TSTYPE = {cfg.ts_type}",
@@ -57,11 +60,24 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
     ]
     for ax, name in enumerate("XYZ"):
         lines.append(f"BC{name}TYPE = {_BC[cfg.bc[ax]]}")
-        lines.append(f"BC{name}0 = {kinds[ax]}")
-        lines.append(f"BC{name}1 = {kinds[ax]}")
-        if kinds[ax] == "PERIODIC":
+        lines.append(f"BC{name}0 = {kinds[2 * ax]}")
+        lines.append(f"BC{name}1 = {kinds[2 * ax + 1]}")
+        if kinds[2 * ax] == "PERIODIC":
+            L = getattr(cfg, "periodic_box", None)
+            b = L[ax] if L is not None else box
             for c in "XYZ":
-                lines.append(f"PERIODICDISP{name}_{c} = {(box if c == name else 0.0)!r}")
+                lines.append(f"PERIODICDISP{name}_{c} = {(b if c == name else 0.0)!r}")
+    sp = getattr(cfg, "sponge", None)
+    if "SPONGE" in kinds and sp:
+        lines += ["[SPONGE]", f"KIND = {sp.get('kind', 'RECTILINEAR')}", f"STRENGTH = {sp.get('strength', 1.0)!r}"]
+        if sp.get("kind", "RECTILINEAR") == "RECTILINEAR":
+            for f, key in enumerate(("X0", "X1", "Y0", "Y1", "Z0", "Z1")):
+                if kinds[f] == "SPONGE":
+                    lines.append(f"RECT{key}PERC = {sp['rect_perc'][f]!r}")
+        else:
+            lines += [f"CYLAXIS_ORIENT = {sp.get('orient', 2)}", f"CYLAXIS_X = {sp['cyl_axis'][0]!r}",
+                      f"CYLAXIS_Y = {sp['cyl_axis'][1]!r}", f"CYLAXIS_Z = {sp['cyl_axis'][2]!r}",
+                      f"RMIN = {sp['rmin']!r}"]
     lines += [
         "[DOMAIN]",
         f"NX = {Nx}",
@@ -99,15 +115,19 @@ def _read_fields(path, N, nf, header=8):
     return hdr, fields
 
 
-def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600):
+def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coords=None):
     """Run the reference solver for `nsteps` time steps from primitive ICs
-    (rho, U, V, W, p). Returns (conserved fields, header dict)."""
+    (rho, U, V, W, p). `coords` = (x, y, z) selects a mesh from file. Returns
+    (conserved fields, header dict)."""
     if not available():
         raise RuntimeError("oracle/_ref/mc3d_ref is not built (make -C oracle)")
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
             f.write(ini_text(cfg, nsteps))
         _write(os.path.join(d, "ic.bin"), ic)
+        if coords is not None:
+            _write(os.path.join(d, "mesh.bin"), coords)
+            mesh = "file:mesh.bin"
         t0 = time.perf_counter()
         r = subprocess.run([REF_BIN, "run", mesh, "ic.bin", "out.bin"], cwd=d,
                            capture_output=True, text=True, timeout=timeout)
@@ -122,11 +142,14 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600):
     return fields, info
 
 
-def run_metrics(cfg, mesh="cube:6.283185307179586"):
+def run_metrics(cfg, mesh="cube:6.283185307179586", coords=None):
     """J, J11..J33 as the reference's solveForJacobians computes them."""
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
             f.write(ini_text(cfg, 1))
+        if coords is not None:
+            _write(os.path.join(d, "mesh.bin"), coords)
+            mesh = "file:mesh.bin"
         r = subprocess.run([REF_BIN, "metrics", mesh, "m.bin"], cwd=d, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("mc3d_ref metrics failed: " + r.stderr[-2000:])

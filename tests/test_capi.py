@@ -165,3 +165,17 @@ def test_null_arguments_are_errors_not_crashes():
     assert lib.mc3d_op_apply(None, None, None, 1, None) == 6
     assert lib.mc3d_config_from_ini(None, None) == 6
     assert b"null" in lib.mc3d_last_error()
+
+
+@pytest.mark.parametrize("name", ["channel_sponge_rect_lsldd", "ogrid_cyl_sponge_kenrk4"])
+def test_sponge_sigma_matches_oracle(name):
+    """mc3d_sponge_sigma (host code) restates SpongeBC's sigma exactly."""
+    import mpi_3dcompact_b200 as m
+    from oracle import mc3d_oracle as O
+    from tests.golden import gen_golden as G
+    cfg, ic, n, coords = G.wall_case(name)
+    opt = m.Options(grid=cfg.N, bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge)
+    got = m.sponge_sigma(opt, *coords)
+    ref = O.sponge_sigma(cfg, *coords)
+    assert np.array_equal(got, ref)
+    assert ref.max() > 0.1

@@ -149,3 +149,54 @@ def test_64cube_two_steps_vs_oracle(prec, tol):
     qo, st = O.run(cfg, ic, 2)
     for i in range(5):
         assert H.rel_l2(q[i], qo[i]) <= tol, (i, H.rel_l2(q[i], qo[i]))
+
+
+def _wall_opts(cfg, precision=m.FP64):
+    return m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                     ts_type=cfg.ts_type, cfl=cfg.cfl, dt=cfg.dt, filter_step=cfg.filter_step,
+                     substep_filtering=cfg.substep_filtering, les=cfg.les, les_avg=cfg.les_avg, precision=precision,
+                     bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge)
+
+
+@pytest.mark.parametrize("name", list(G.WALL_CASES))
+def test_boundary_cases_match_reference_solver(name):
+    """Walls, sponges and the O-grid cylinder (curvilinear metrics of the
+    reference) against the reference solver's output: <= 1e-12 relative."""
+    cfg, ic, n, coords = G.wall_case(name)
+    gold = H.golden_steps()
+    opt = _wall_opts(cfg)
+    s = m.CurvilinearCSolver(opt)
+    s.set_metrics([gold[f"{name}_met{c}"] for c in range(10)])
+    if cfg.sponge:
+        s.set_sponge(m.sponge_sigma(opt, *coords))
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    q = s.conserved()
+    for i in range(5):
+        err = H.rel_max(q[i], gold[f"{name}_q{i}"])
+        assert err <= 1e-12, (name, i, err)
+    ts, t, dt = gold[f"{name}_info"]
+    assert s.info()["time_step"] == int(ts)
+
+
+def test_boundary_case_fp32bulk():
+    """FP32-bulk on the O-grid cylinder stays within 1e-5 of the FP64 path."""
+    name = "ogrid_cyl_sponge_kenrk4"
+    cfg, ic, n, coords = G.wall_case(name)
+    gold = H.golden_steps()
+    outs = []
+    for prec in (m.FP64, m.FP32BULK):
+        opt = _wall_opts(cfg, prec)
+        s = m.CurvilinearCSolver(opt)
+        s.set_metrics([gold[f"{name}_met{c}"] for c in range(10)])
+        s.set_sponge(m.sponge_sigma(opt, *coords))
+        s.set_initial_conditions(*ic)
+        s.step(n)
+        outs.append(s.conserved())
+    # momentum errors against the momentum-vector norm: the cross-stream
+    # components are a 0.2% disturbance of a Mach 0.2 stream along x
+    mom = np.sqrt(sum(np.sum(outs[0][i] ** 2) for i in (1, 2, 3)))
+    for i in range(5):
+        scale = mom if i in (1, 2, 3) else np.sqrt(np.sum(outs[0][i] ** 2))
+        err = np.sqrt(np.sum((outs[1][i] - outs[0][i]) ** 2)) / scale
+        assert err <= 1e-5, (i, err)

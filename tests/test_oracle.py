@@ -115,3 +115,19 @@ def test_hit_ic_is_seeded_and_solenoidal():
     div = (1j * k[None, None, :] * np.fft.fftn(u) + 1j * k[None, :, None] * np.fft.fftn(v)
            + 1j * k[:, None, None] * np.fft.fftn(w))
     assert np.max(np.abs(div)) / np.max(np.abs(np.fft.fftn(u))) < 1e-10
+
+
+@pytest.mark.parametrize("name", list(G.WALL_CASES))
+def test_oracle_boundary_cases_match_reference_fixtures(name):
+    """Walls (adiabatic, the X1 constant-temperature quirk), rectilinear and
+    cylindrical sponges, an O-grid cylinder: the reference's own metrics."""
+    cfg, ic, n, coords = G.wall_case(name)
+    gold = H.golden_steps()
+    met = [gold[f"{name}_met{c}"] for c in range(10)]
+    sigma = O.sponge_sigma(cfg, *coords) if cfg.sponge else None
+    q, st = O.run(cfg, ic, n, metrics=met, sigma=sigma)
+    for i in range(5):
+        assert H.rel_max(q[i], gold[f"{name}_q{i}"]) < 1e-12, (name, i, H.rel_max(q[i], gold[f"{name}_q{i}"]))
+    ts, t, dt = gold[f"{name}_info"]
+    assert st.time_step == int(ts)
+    assert abs(st.dt - dt) <= 1e-13 * abs(dt)
