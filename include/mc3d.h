@@ -50,7 +50,8 @@ enum { MC3D_PERIODIC_SOLVE = 0, MC3D_DIRICHLET_SOLVE = 1 };     /* BCType       
 enum { MC3D_CD2 = 0, MC3D_PADE6 = 1, MC3D_PENTA10 = 2 };        /* FDType           */
 enum { MC3D_COMPACT8 = 0, MC3D_COMPACT10 = 1,                  /* FilterType       */
        MC3D_TESTFILTER_PADE = 2, MC3D_TESTFILTER_EXP = 3 };      /* DSM test filters */
-enum { MC3D_NOMODEL = 0, MC3D_VREMAN = 1, MC3D_DSM = 2 };       /* LESModel         */
+enum { MC3D_NOMODEL = 0, MC3D_VREMAN = 1, MC3D_DSM = 2,        /* LESModel         */
+       MC3D_MLPSGS = 3 };   /* learned closure (LESMODEL = MLP), an addition with DSM as its fallback */
 enum { MC3D_AVG_NONE = 0, MC3D_AVG_XI1 = 1, MC3D_AVG_XI2 = 2, MC3D_AVG_XI3 = 3,
        MC3D_AVG_LOCAL = 4, MC3D_AVG_GLOBAL = 5 };               /* StatsAvgType     */
 enum { MC3D_TVDRK3 = 0, MC3D_RK4 = 1, MC3D_KENRK4 = 2, MC3D_LSLDDRK4 = 3 }; /* RKType */
@@ -151,6 +152,37 @@ int mc3d_op_destroy(mc3d_op op);
  * the wall value giving a zero normal derivative from f[1..5]. Host-side. */
 double mc3d_calc_neumann(int fd_type, const double *f);
 
+/* ---- learned SGS closure: no counterpart in the reference, where VremanSGS /
+ * DSMSGS (src/VremanSGS.hpp, src/DSMSGS.hpp) are the models. A 9-64-64-64-2
+ * GELU MLP from invariants of the resolved velocity gradient and the grid
+ * scale to C (mu_t = rho C Delta^2 |S|) and Pr_t. Arrays are device FP32:
+ * x [n][9] raw features, y [n][2]. ---- */
+typedef struct mc3d_mlp_s *mc3d_mlp;
+int mc3d_mlp_create(unsigned long long seed, int device, mc3d_mlp *out);
+int mc3d_mlp_destroy(mc3d_mlp m);
+/* feature mean/std (normalisation), training range lo/hi (outside it the
+ * solver falls back to DSM), target mean/std (outputs are normalised targets) */
+int mc3d_mlp_set_normalization(mc3d_mlp m, const float *mean, const float *std, const float *lo, const float *hi,
+                               const float *ymean, const float *ystd);
+int mc3d_mlp_get_normalization(mc3d_mlp m, float *out);
+/* one Adam step (lr) on MSE against normalised targets y; loss (host, may be NULL) */
+int mc3d_mlp_train_step(mc3d_mlp m, const float *x, const float *y, int n, float lr, double *loss, void *stream);
+/* FP32 forward on CUDA cores, and the BF16 tensor-core inference */
+int mc3d_mlp_forward(mc3d_mlp m, const float *x, float *y, int n, void *stream);
+int mc3d_mlp_infer_bf16(mc3d_mlp m, const float *x, float *y, int n, void *stream);
+int mc3d_mlp_get_params(mc3d_mlp m, float *P);          /* host, 9090 floats */
+int mc3d_mlp_set_params(mc3d_mlp m, const float *P);
+int mc3d_mlp_save(mc3d_mlp m, const char *path);
+int mc3d_mlp_load(mc3d_mlp m, const char *path);
+/* training data from DNS fields (device FP64): box filter of factor f of the
+ * conserved state into 14 coarse fields (rho, rhoU_i, rhoU_iU_j, rhoT, rhoU_iT),
+ * and features + least-squares targets from them and the xi-derivatives
+ * grads[3*var + dir] of the Favre-filtered u, v, w, T (box metrics jd[3]) */
+int mc3d_sgs_box_filter(const double *const q[5], int Nx, int Ny, int Nz, int f, double *const out[14],
+                        void *stream);
+int mc3d_sgs_training_pairs(const double *const coarse[14], const double *const grads[12], int Nx, int Ny, int Nz,
+                            const double jd[3], double delta, double mu_ref, float *x, float *y, void *stream);
+
 /* ---- solver: CurvilinearCSolver + AbstractRK on one GPU ---- */
 typedef struct mc3d_solver_s *mc3d_solver;
 
@@ -164,6 +196,12 @@ int mc3d_solver_set_metrics(mc3d_solver s, const double *const metrics[10]);
 /* The uniform periodic box x = L*xi (the HIT mesh,
  * tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156). */
 int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz);
+
+/* The learned closure a LESMODEL = MLP solver evaluates (kept by reference;
+ * it must outlive the solver). */
+int mc3d_solver_set_mlp(mc3d_solver s, mc3d_mlp m);
+/* RK stages that fell back to DSM because a feature left the training range */
+int mc3d_solver_mlp_fallbacks(mc3d_solver s, long long *stages);
 
 /* Sponge strength sigma (host, FP64, x-fastest; e.g. from mc3d_sponge_sigma),
  * required before set_initial when a face is SPONGE (SpongeBC::sigma,
@@ -192,6 +230,8 @@ int mc3d_solver_step(mc3d_solver s, int nsteps);
 /* Copy the conserved state rho1, rhoU1, rhoV1, rhoW1, rhoE1 (FP64) to host. */
 int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *rhoV, double *rhoW,
                               double *rhoE);
+/* Device-to-device copy of the conserved state into caller buffers (FP64). */
+int mc3d_solver_copy_conserved_device(mc3d_solver s, double *const dst[5]);
 /* Device pointers (FP64) of the five conserved fields. */
 int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]);
 

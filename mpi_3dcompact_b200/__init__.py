@@ -164,7 +164,7 @@ def calc_neumann(fd_type, f):
 _FD = {"CD2": _CD2, "PADE6": _PADE6, "PENTA10": _PENTA10}
 _FILT = {"COMPACT8": COMPACT8, "COMPACT10": COMPACT10}
 _RK = {"TVDRK3": TVDRK3, "RK4": RK4, "KENRK4": KENRK4, "LSLDDRK4": LSLDDRK4}
-_LES = {"NOMODEL": NOMODEL, "NONE": NOMODEL, "VREMAN": VREMAN, "DSM": 2}
+_LES = {"NOMODEL": NOMODEL, "NONE": NOMODEL, "VREMAN": VREMAN, "DSM": 2, "MLP": 3}
 _AVG = {"NONE": 0, "XI1_AVG": 1, "XI2_AVG": 2, "XI3_AVG": 3, "LOCAL": 4, "GLOBAL": 5}
 _BCKIND = {"PERIODIC": 0, "INTERNALLY_PERIODIC": 1, "SPONGE": 2, "ADIABATIC_WALL": 3, "CONST_T_WALL": 4,
            "MOVING_ADIABATIC_WALL": 5, "INLET": 6}
@@ -234,6 +234,69 @@ class Options:
         return (self.c.Nz, self.c.Ny, self.c.Nx)
 
 
+def _fp(a):
+    return C.cast(C.c_void_p(a.data_ptr()), C.c_void_p)
+
+
+class MLPClosure:
+    """Learned SGS closure (no counterpart in the reference): a 9-64-64-64-2
+    GELU MLP from velocity-gradient invariants and the grid scale to C and
+    Pr_t, with FP32 training kernels and BF16 tensor-core inference. Arrays
+    are CUDA float32 torch tensors: x [n, 9] raw features, y [n, 2]."""
+
+    N_PARAMS = 9090
+
+    def __init__(self, seed=0, device=0):
+        h = C.c_void_p()
+        N.check(N.host_lib().mc3d_mlp_create(int(seed), device, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                N.host_lib().mc3d_mlp_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_normalization(self, mean, std, lo, hi, ymean, ystd):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (mean, std, lo, hi, ymean, ystd)]
+        ptrs = [a.ctypes.data_as(C.POINTER(C.c_float)) for a in arrs]
+        N.check(N.host_lib().mc3d_mlp_set_normalization(self._h, *ptrs))
+
+    def normalization(self):
+        out = np.zeros(4 * 9 + 4, dtype=np.float32)
+        N.check(N.host_lib().mc3d_mlp_get_normalization(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return dict(mean=out[0:9], std=out[9:18], lo=out[18:27], hi=out[27:36], ymean=out[36:38], ystd=out[38:40])
+
+    def train_step(self, x, y, lr=1e-3, stream=None):
+        """One Adam step on the MSE against normalised targets y; returns the loss."""
+        loss = C.c_double()
+        N.check(N.host_lib().mc3d_mlp_train_step(self._h, _fp(x), _fp(y), x.shape[0], lr, C.byref(loss), stream))
+        return loss.value
+
+    def forward(self, x, y, stream=None):
+        N.check(N.host_lib().mc3d_mlp_forward(self._h, _fp(x), _fp(y), x.shape[0], stream))
+
+    def infer_bf16(self, x, y, stream=None):
+        N.check(N.host_lib().mc3d_mlp_infer_bf16(self._h, _fp(x), _fp(y), x.shape[0], stream))
+
+    def params(self):
+        P = np.zeros(self.N_PARAMS, dtype=np.float32)
+        N.check(N.host_lib().mc3d_mlp_get_params(self._h, P.ctypes.data_as(C.POINTER(C.c_float))))
+        return P
+
+    def set_params(self, P):
+        P = np.ascontiguousarray(P, dtype=np.float32)
+        N.check(N.host_lib().mc3d_mlp_set_params(self._h, P.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def save(self, path):
+        N.check(N.host_lib().mc3d_mlp_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        N.check(N.host_lib().mc3d_mlp_load(self._h, str(path).encode()))
+
+
 class CurvilinearCSolver:
     """CurvilinearCSolver + its AbstractRK driver on one GPU
     (src/CurvilinearCSolver.hpp:25-379, src/AbstractRK.hpp:6-17)."""
@@ -263,6 +326,16 @@ class CurvilinearCSolver:
         p = (C.POINTER(C.c_double) * 10)(*[N.dptr(a) for a in arrs])
         N.check(N.host_lib().mc3d_solver_set_metrics(self._h, p))
 
+    def set_mlp(self, mlp: MLPClosure):
+        """The learned closure of a LESMODEL = MLP solver (kept alive by the solver object)."""
+        self._mlp = mlp
+        N.check(N.host_lib().mc3d_solver_set_mlp(self._h, mlp._h))
+
+    def mlp_fallbacks(self):
+        v = C.c_longlong()
+        N.check(N.host_lib().mc3d_solver_mlp_fallbacks(self._h, C.byref(v)))
+        return v.value
+
     def set_sponge(self, sigma):
         """Sponge strength field (SpongeBC::sigma); needed before the initial condition."""
         a = np.ascontiguousarray(sigma, dtype=np.float64)
@@ -288,6 +361,11 @@ class CurvilinearCSolver:
         out = [np.empty(self.shape) for _ in range(5)]
         N.check(N.host_lib().mc3d_solver_get_conserved(self._h, *[N.dptr(a) for a in out]))
         return out
+
+    def copy_conserved_device(self, dst):
+        """Device-to-device copy of rho1..rhoE1 into 5 CUDA float64 tensors."""
+        p = (C.c_void_p * 5)(*[t.data_ptr() for t in dst])
+        N.check(N.host_lib().mc3d_solver_copy_conserved_device(self._h, p))
 
     def conserved_device_ptrs(self):
         p = (C.c_void_p * 5)()

@@ -88,6 +88,23 @@ def host_lib():
             "mc3d_hit_randvec": (ip, [C.POINTER(C.c_int), C.POINTER(dp), C.c_longlong, C.POINTER(dp)]),
             "mc3d_cfl_max_noalloc": (ip, [vp] * 8 + [dp] * 3 + [ip] * 3 + [dp] * 3 + [vp, vp]),
             "mc3d_sponge_sigma": (ip, [C.POINTER(Config)] + [C.POINTER(dp)] * 4),
+            "mc3d_mlp_create": (ip, [C.c_ulonglong, ip, C.POINTER(vp)]),
+            "mc3d_mlp_destroy": (ip, [vp]),
+            "mc3d_mlp_set_normalization": (ip, [vp] + [C.POINTER(C.c_float)] * 6),
+            "mc3d_mlp_get_normalization": (ip, [vp, C.POINTER(C.c_float)]),
+            "mc3d_mlp_train_step": (ip, [vp, vp, vp, ip, C.c_float, C.POINTER(dp), vp]),
+            "mc3d_mlp_forward": (ip, [vp, vp, vp, ip, vp]),
+            "mc3d_mlp_infer_bf16": (ip, [vp, vp, vp, ip, vp]),
+            "mc3d_mlp_get_params": (ip, [vp, C.POINTER(C.c_float)]),
+            "mc3d_mlp_set_params": (ip, [vp, C.POINTER(C.c_float)]),
+            "mc3d_mlp_save": (ip, [vp, C.c_char_p]),
+            "mc3d_mlp_load": (ip, [vp, C.c_char_p]),
+            "mc3d_sgs_box_filter": (ip, [C.POINTER(vp), ip, ip, ip, ip, C.POINTER(vp), vp]),
+            "mc3d_sgs_training_pairs": (ip, [C.POINTER(vp), C.POINTER(vp), ip, ip, ip, C.POINTER(dp), dp, dp,
+                                             vp, vp, vp]),
+            "mc3d_solver_set_mlp": (ip, [vp, vp]),
+            "mc3d_solver_copy_conserved_device": (ip, [vp, C.POINTER(vp)]),
+            "mc3d_solver_mlp_fallbacks": (ip, [vp, C.POINTER(C.c_longlong)]),
             "mc3d_solver_set_sponge": (ip, [vp, C.POINTER(dp)]),
             "mc3d_solver_set_sponge_avg": (ip, [vp, C.POINTER(C.POINTER(dp))]),
         }

@@ -254,7 +254,8 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
         // [STATS], [LES]
         parse_enum(ini, "STATS.STATSAVGTYPE", {{"NONE", 0}, {"XI1_AVG", 1}, {"XI2_AVG", 2}, {"XI3_AVG", 3}, {"LOCAL", 4}, {"GLOBAL", 5}});
         c->les_model = parse_enum(ini, "LES.LESMODEL", {{"NOMODEL", MC3D_NOMODEL}, {"NONE", MC3D_NOMODEL},
-                                                        {"VREMAN", MC3D_VREMAN}, {"DSM", MC3D_DSM}});
+                                                        {"VREMAN", MC3D_VREMAN}, {"DSM", MC3D_DSM},
+                                                        {"MLP", MC3D_MLPSGS}});
         c->les_averaging = parse_enum(ini, "LES.LESAVERAGING",
                                       {{"NONE", MC3D_AVG_NONE}, {"XI1_AVG", MC3D_AVG_XI1}, {"XI2_AVG", MC3D_AVG_XI2},
                                        {"XI3_AVG", MC3D_AVG_XI3}, {"LOCAL", MC3D_AVG_LOCAL}, {"GLOBAL", MC3D_AVG_GLOBAL}});

@@ -1,5 +1,6 @@
 // Internal declarations shared by the host and device translation units.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -218,6 +219,36 @@ struct TimeState {
 };
 int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, int first_step,
                        cudaStream_t st);
+
+// ---- learned SGS closure (mlp.cu) --------------------------------------------
+constexpr int MLP_IN = 9, MLP_OUT = 2;
+constexpr int MLP_NPARAM = 9090;   // 9*64+64 + 2*(64*64+64) + 64*2+2
+constexpr int MLP_NHALF = 64 * 24 + 2 * 64 * 72 + 8 * 72;
+// input normalisation x_n = (x - mean) * inv_std, and the training range [lo, hi]
+struct MlpNorm {
+    float mean[MLP_IN], inv_std[MLP_IN], lo[MLP_IN], hi[MLP_IN];
+    float ymean[MLP_OUT], ystd[MLP_OUT];   // targets: y = out * ystd + ymean
+};
+struct MlpDev {
+    float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr;   // FP32 master, grads, Adam moments
+    __nv_bfloat16 *Hw = nullptr;                                     // packed bf16 weights
+    float *Bc = nullptr;                                             // compact biases [64|64|64|2]
+    MlpNorm norm{};
+    long long t = 0;                                                 // Adam step
+};
+int mlp_pack(const MlpDev &m, cudaStream_t st);
+int mlp_forward_fp32(const MlpDev &m, const float *x, int n, float *act, float *out, cudaStream_t st);
+int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, float *act, float *out, float *delta,
+                   double *loss, cudaStream_t st);
+int mlp_infer_bf16(const MlpDev &m, const float *x, int n, float *out, cudaStream_t st);
+const MlpDev *mlp_dev(mc3d_mlp m);
+// fused closure in the time step: d[12] the xi-derivatives of U, V, W, T
+template <typename R>
+int launch_sgs_mlp(const Grid3 &g, const R *rho, const R *T, const R *const d[12], const Metrics<R> &m, double dvol,
+                   double mu_ref, const MlpDev &mlp, R *mu_sgs, R *ksgs, int *flag, cudaStream_t st);
+int launch_box_filter(const Grid3 &gf, int f, const double *const q[5], double *const out[14], cudaStream_t st);
+int launch_training_pairs(const Grid3 &gc, const double *const coarse[14], const double *const grads[12],
+                          const double jd[3], double delta, double mu_ref, float *x, float *y, cudaStream_t st);
 
 // ---- boundary conditions (bc.cu) -------------------------------------------
 // face: 0 X0, 1 X1, 2 Y0, 3 Y1, 4 Z0, 5 Z1

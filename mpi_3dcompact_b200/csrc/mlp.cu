@@ -1,0 +1,301 @@
+// Learned SGS closure: a 9 -> 64 -> 64 -> 64 -> 2 MLP (GELU) mapping local
+// invariants of the resolved velocity-gradient tensor and the grid scale to
+// the Smagorinsky-form coefficient C (nu_t = C Delta^2 |S|) and the turbulent
+// Prandtl number. No counterpart in the reference: it stands in for
+// VremanSGS / DSMSGS (src/VremanSGS.hpp, src/DSMSGS.hpp) behind the same
+// solver path, with DSM kept as the fallback.
+//
+// Training (FP32, CUDA cores): mlp_forward stores pre- and post-activations,
+// mlp_backward the per-sample deltas and the MSE, mlp_wgrad reduces the weight
+// and bias gradients over the batch (split over the batch, one atomic add per
+// split), mlp_adam applies Adam with bias correction.
+// Inference (BF16 tensor cores, FP32 accumulate): mma.sync m16n8k16 tiles of
+// 16 points; a layer's accumulator fragments become the next layer's A
+// fragments in registers, so activations never leave the SM.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "mlp_common.cuh"
+
+namespace mc3d {
+
+// parameter offsets (floats) of the FP32 master copy
+constexpr int MLP_W1 = 0;                          // [64][9]
+constexpr int MLP_B1 = MLP_W1 + 64 * MLP_IN;       // [64]
+constexpr int MLP_W2 = MLP_B1 + 64;                // [64][64]
+constexpr int MLP_B2 = MLP_W2 + 64 * 64;
+constexpr int MLP_W3 = MLP_B2 + 64;
+constexpr int MLP_B3 = MLP_W3 + 64 * 64;
+constexpr int MLP_W4 = MLP_B3 + 64;                // [2][64]
+constexpr int MLP_B4 = MLP_W4 + MLP_OUT * 64;
+constexpr int MLP_NP = MLP_B4 + MLP_OUT;           // 9090
+static_assert(MLP_NP == MLP_NPARAM, "parameter count");
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// training kernels (thread per sample, parameters staged in shared memory)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) mlp_forward_kernel(const float *__restrict__ P, const float *__restrict__ x,
+                                                           int n, MlpNorm nrm, float *__restrict__ act,
+                                                           float *__restrict__ out) {
+    extern __shared__ float sp[];
+    for (int k = threadIdx.x; k < MLP_NP; k += blockDim.x) sp[k] = P[k];
+    __syncthreads();
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    float a0[MLP_IN];
+#pragma unroll
+    for (int k = 0; k < MLP_IN; k++) a0[k] = (x[(size_t)b * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k];
+    float h[64], z[64];
+    // layer 1
+#pragma unroll 4
+    for (int o = 0; o < 64; o++) {
+        float s = sp[MLP_B1 + o];
+#pragma unroll
+        for (int k = 0; k < MLP_IN; k++) s += sp[MLP_W1 + o * MLP_IN + k] * a0[k];
+        z[o] = s;
+    }
+    // act layout: [6][n][64]: z1, h1, z2, h2, z3, h3
+#pragma unroll 4
+    for (int o = 0; o < 64; o++) {
+        h[o] = gelu(z[o]);
+        if (act) {
+            act[(size_t)0 * n * 64 + (size_t)b * 64 + o] = z[o];
+            act[(size_t)1 * n * 64 + (size_t)b * 64 + o] = h[o];
+        }
+    }
+    for (int layer = 0; layer < 2; layer++) {
+        const int W = layer == 0 ? MLP_W2 : MLP_W3, B = layer == 0 ? MLP_B2 : MLP_B3;
+#pragma unroll 2
+        for (int o = 0; o < 64; o++) {
+            float s = sp[B + o];
+#pragma unroll
+            for (int k = 0; k < 64; k++) s += sp[W + o * 64 + k] * h[k];
+            z[o] = s;
+        }
+#pragma unroll 4
+        for (int o = 0; o < 64; o++) {
+            h[o] = gelu(z[o]);
+            if (act) {
+                act[(size_t)(2 + 2 * layer) * n * 64 + (size_t)b * 64 + o] = z[o];
+                act[(size_t)(3 + 2 * layer) * n * 64 + (size_t)b * 64 + o] = h[o];
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 0; o < MLP_OUT; o++) {
+        float s = sp[MLP_B4 + o];
+#pragma unroll
+        for (int k = 0; k < 64; k++) s += sp[MLP_W4 + o * 64 + k] * h[k];
+        out[(size_t)b * MLP_OUT + o] = s;
+    }
+}
+
+// deltas of every layer for MSE loss = (1/n) sum_b sum_o (out - y)^2; loss accumulated
+__global__ void __launch_bounds__(128) mlp_backward_kernel(const float *__restrict__ P, const float *__restrict__ act,
+                                                            const float *__restrict__ out, const float *__restrict__ y,
+                                                            int n, float *__restrict__ delta, double *loss) {
+    extern __shared__ float sp[];
+    for (int k = threadIdx.x; k < MLP_NP; k += blockDim.x) sp[k] = P[k];
+    __syncthreads();
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (b < n) {
+        float d4[MLP_OUT];
+#pragma unroll
+        for (int o = 0; o < MLP_OUT; o++) {
+            const float e = out[(size_t)b * MLP_OUT + o] - y[(size_t)b * MLP_OUT + o];
+            l += (double)e * e;
+            d4[o] = 2.0f * e / (float)n;
+            delta[(size_t)3 * n * 64 + (size_t)b * MLP_OUT + o] = d4[o];
+        }
+        float d[64], dn[64];
+        // delta3 = (W4^T d4) * gelu'(z3)
+#pragma unroll 4
+        for (int k = 0; k < 64; k++) {
+            float s = 0;
+#pragma unroll
+            for (int o = 0; o < MLP_OUT; o++) s += sp[MLP_W4 + o * 64 + k] * d4[o];
+            d[k] = s * gelu_grad(act[(size_t)4 * n * 64 + (size_t)b * 64 + k]);
+            delta[(size_t)2 * n * 64 + (size_t)b * 64 + k] = d[k];
+        }
+        for (int layer = 1; layer >= 0; layer--) {
+            // delta_{l} = (W_{l+1}^T delta_{l+1}) * gelu'(z_l); W_{l+1} = W3 (layer 1) or W2 (layer 0)
+            const int W = layer == 1 ? MLP_W3 : MLP_W2;
+            const size_t zoff = (size_t)(2 * layer) * n * 64;
+#pragma unroll 2
+            for (int k = 0; k < 64; k++) {
+                float s = 0;
+#pragma unroll
+                for (int o = 0; o < 64; o++) s += sp[W + o * 64 + k] * d[o];
+                dn[k] = s * gelu_grad(act[zoff + (size_t)b * 64 + k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 64; k++) {
+                d[k] = dn[k];
+                delta[(size_t)layer * n * 64 + (size_t)b * 64 + k] = d[k];
+            }
+        }
+    }
+    // block-reduce the loss
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l / (double)n);
+}
+
+// G[layer] += sum_b delta[b][o] * a_prev[b][i]; bias gradients in the extra column
+__global__ void mlp_wgrad_kernel(const float *__restrict__ x, MlpNorm nrm, const float *__restrict__ act,
+                                 const float *__restrict__ delta, int n, int layer, float *__restrict__ G) {
+    const int nin = layer == 0 ? MLP_IN : 64, nout = layer == 3 ? MLP_OUT : 64;
+    const int o = blockIdx.x;                  // output row
+    const int i = threadIdx.x;                 // input column, i == nin: bias
+    if (o >= nout || i > nin) return;
+    const int splits = gridDim.y;
+    const int b0 = (int)((long long)n * blockIdx.y / splits), b1 = (int)((long long)n * (blockIdx.y + 1) / splits);
+    const float *dl = layer == 3 ? delta + (size_t)3 * n * 64 : delta + (size_t)layer * n * 64;
+    const int dstride = layer == 3 ? MLP_OUT : 64;
+    const float *ap = layer == 0 ? nullptr : act + (size_t)(2 * layer - 1) * n * 64;   // h_{layer}
+    float s = 0;
+    for (int b = b0; b < b1; b++) {
+        const float dv = dl[(size_t)b * dstride + o];
+        float a;
+        if (i == nin) a = 1.0f;
+        else if (layer == 0) a = (x[(size_t)b * MLP_IN + i] - nrm.mean[i]) * nrm.inv_std[i];
+        else a = ap[(size_t)b * 64 + i];
+        s += dv * a;
+    }
+    const int W = layer == 0 ? MLP_W1 : layer == 1 ? MLP_W2 : layer == 2 ? MLP_W3 : MLP_W4;
+    const int B = layer == 0 ? MLP_B1 : layer == 1 ? MLP_B2 : layer == 2 ? MLP_B3 : MLP_B4;
+    atomicAdd(i == nin ? &G[B + o] : &G[W + o * nin + i], s);
+}
+
+__global__ void mlp_adam_kernel(float *P, float *G, float *M, float *V, float lr, float b1t, float b2t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= MLP_NP) return;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float g = G[k];
+    const float m = b1 * M[k] + (1.0f - b1) * g;
+    const float v = b2 * V[k] + (1.0f - b2) * g * g;
+    M[k] = m;
+    V[k] = v;
+    const float mh = m / (1.0f - b1t), vh = v / (1.0f - b2t);
+    P[k] -= lr * mh / (sqrtf(vh) + eps);
+    G[k] = 0.0f;
+}
+
+__global__ void mlp_pack_kernel(const float *__restrict__ P, __nv_bfloat16 *__restrict__ Hw, float *__restrict__ Bc) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < MLPH_N; k += gridDim.x * blockDim.x) {
+        float v = 0.0f;
+        if (k < MLPH_W2) {
+            const int o = k / MLPH_P1, c = k % MLPH_P1;
+            v = c < MLP_IN ? P[MLP_W1 + o * MLP_IN + c] : 0.0f;
+        } else if (k < MLPH_W4) {
+            const int w = k < MLPH_W3 ? MLP_W2 : MLP_W3, kk = k - (k < MLPH_W3 ? MLPH_W2 : MLPH_W3);
+            const int o = kk / MLPH_P, c = kk % MLPH_P;
+            v = c < 64 ? P[w + o * 64 + c] : 0.0f;
+        } else {
+            const int o = (k - MLPH_W4) / MLPH_P, c = (k - MLPH_W4) % MLPH_P;
+            v = (o < MLP_OUT && c < 64) ? P[MLP_W4 + o * 64 + c] : 0.0f;
+        }
+        Hw[k] = __float2bfloat16_rn(v);
+    }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 3 * 64 + MLP_OUT; k += gridDim.x * blockDim.x)
+        Bc[k] = k < 64 ? P[MLP_B1 + k] : k < 128 ? P[MLP_B2 + k - 64] : k < 192 ? P[MLP_B3 + k - 128] : P[MLP_B4 + k - 192];
+}
+
+}  // namespace
+
+namespace {
+
+// standalone inference: x [n][9] (raw features) -> out [n][2] (raw outputs)
+__global__ void __launch_bounds__(128) mlp_infer_kernel(const __nv_bfloat16 *__restrict__ Hw,
+                                                         const float *__restrict__ Bc, MlpNorm nrm,
+                                                         const float *__restrict__ x, int n, float *__restrict__ out) {
+    constexpr int XS = 24;   // bf16 row pitch of 48 bytes: the fragment loads hit distinct banks
+    __shared__ __align__(16) __nv_bfloat16 sW[MLPH_N];
+    __shared__ float bias[3 * 64 + MLP_OUT];
+    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * XS];
+    __shared__ float ys[4][64];
+    for (int k = threadIdx.x; k < MLPH_N; k += blockDim.x) sW[k] = Hw[k];
+    for (int k = threadIdx.x; k < 3 * 64 + MLP_OUT; k += blockDim.x) bias[k] = Bc[k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * 4 * 32;
+    for (long long base = ((long long)blockIdx.x * 4 + warp) * 32; base < n; base += stride) {
+        const long long p = base + lane;
+        __nv_bfloat16 *row = xs[warp] + lane * XS;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            float v = 0.0f;
+            if (k < MLP_IN && p < n) v = (x[p * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k];
+            row[k] = __float2bfloat16_rn(v);
+        }
+        __syncwarp();
+        mlp_tile16<XS>(xs[warp], 0, sW, bias, ys[warp], lane);
+        mlp_tile16<XS>(xs[warp], 16, sW, bias, ys[warp], lane);
+        __syncwarp();
+        if (p < n) {
+            out[p * 2 + 0] = ys[warp][lane * 2 + 0];
+            out[p * 2 + 1] = ys[warp][lane * 2 + 1];
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int mlp_pack(const MlpDev &m, cudaStream_t st) {
+    mlp_pack_kernel<<<16, 256, 0, st>>>(m.P, m.Hw, m.Bc);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+int mlp_forward_fp32(const MlpDev &m, const float *x, int n, float *act, float *out, cudaStream_t st) {
+    const size_t smem = MLP_NP * sizeof(float);
+    static bool configured = false;
+    if (!configured) {
+        MC3D_CUDA_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MC3D_CUDA_TRY(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    mlp_forward_kernel<<<(n + 127) / 128, 128, smem, st>>>(m.P, x, n, m.norm, act, out);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, float *act, float *out, float *delta,
+                   double *loss, cudaStream_t st) {
+    int rc;
+    if ((rc = mlp_forward_fp32(m, x, n, act, out, st))) return rc;
+    const size_t smem = MLP_NP * sizeof(float);
+    mlp_backward_kernel<<<(n + 127) / 128, 128, smem, st>>>(m.P, act, out, y, n, delta, loss);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    const int splits = std::max(1, std::min(128, n / 512));
+    for (int layer = 0; layer < 4; layer++) {
+        const int nout = layer == 3 ? MLP_OUT : 64, nin = layer == 0 ? MLP_IN : 64;
+        mlp_wgrad_kernel<<<dim3(nout, splits), nin + 1, 0, st>>>(x, m.norm, act, delta, n, layer, m.G);
+        MC3D_CUDA_TRY(cudaGetLastError());
+    }
+    m.t += 1;
+    const float b1t = (float)std::pow(0.9, (double)m.t), b2t = (float)std::pow(0.999, (double)m.t);
+    mlp_adam_kernel<<<(MLP_NP + 255) / 256, 256, 0, st>>>(m.P, m.G, m.M, m.V, lr, b1t, b2t);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return mlp_pack(m, st);
+}
+
+int mlp_infer_bf16(const MlpDev &m, const float *x, int n, float *out, cudaStream_t st) {
+    const int blocks = std::max(1, std::min((n + 127) / 128, 148 * 8));
+    mlp_infer_kernel<<<blocks, 128, 0, st>>>(m.Hw, m.Bc, m.norm, x, n, out);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+}  // namespace mc3d

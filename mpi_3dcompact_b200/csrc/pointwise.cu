@@ -317,7 +317,12 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
         if (fp.les >= 2) ld_np<R, NP>(mu_sgs_f, i, two, ms);
         if (fp.les == 3) {
             ld_np<R, NP>(ksgs_f, i, two, ks);
-            ld_np<R, NP>(taukk_f, i, two, tk);
+            if (taukk_f) {
+                ld_np<R, NP>(taukk_f, i, two, tk);
+            } else {
+#pragma unroll
+                for (int q = 0; q < NP; q++) tk[q] = R(0);
+            }
         }
         R out[15][NP];
 #pragma unroll

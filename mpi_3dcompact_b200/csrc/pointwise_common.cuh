@@ -31,6 +31,20 @@ struct P5w {
 };
 
 template <typename R>
+struct DerivPtrs12c {
+    const R *p[12];
+};
+struct CoarseOut {
+    double *p[14];
+};
+struct CoarseIn {
+    const double *p[14];
+};
+struct GradIn {
+    const double *p[12];
+};
+
+template <typename R>
 __device__ __forceinline__ R met(const Metrics<R> &m, int c, long long i) {
     return m.constant ? m.c[c] : m.m[c][i];
 }

@@ -1,0 +1,282 @@
+// Learned SGS closure in the time step, and the kernels that make its training
+// data from this solver's own DNS fields. No counterpart in the reference.
+//
+// Features of a point (dimensionless, from the resolved state and the grid):
+//   x0 log(1 + rho Delta^2 |S| / mu)       grid Reynolds number of the strain
+//   x1 W:W / (S:S + W:W)                  rotation fraction
+//   x2 tr(S^3) / (S:S)^(3/2)              strain shape
+//   x3 tr(S W W) / (S:S + W:W)^(3/2)      strain-rotation alignment
+//   x4 tr(S S W W) / (S:S + W:W)^2
+//   x5 tr(grad u) / (S:S + W:W)^(1/2)     dilatation
+//   x6 Delta |grad T| / T
+//   x7 Delta |S| / c                      grid-scale strain Mach number
+//   x8 log(rho)
+// with S, W the symmetric and antisymmetric parts of grad u, |S| = (2 S:S)^(1/2)
+// and Delta = (dxi deta dzeta / J)^(1/3) (the Vreman/DSM grid scale,
+// src/VremanSGS.hpp:49-52). Outputs: C (mu_t = rho C Delta^2 |S|) and Pr_t;
+// k_sgs = cp mu_t / Pr_t (the form of DSM's k_sgs in the flux, Core.cpp:636-639).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "mlp_common.cuh"
+
+namespace mc3d {
+
+__device__ __forceinline__ void mlp_features(const double gu[3][3], double rho, double T, const double gT[3],
+                                             double delta, double mu, double *x) {
+    double S[3][3], Wm[3][3];
+    double s2 = 0, w2 = 0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            S[a][b] = 0.5 * (gu[a][b] + gu[b][a]);
+            Wm[a][b] = 0.5 * (gu[a][b] - gu[b][a]);
+            s2 += S[a][b] * S[a][b];
+            w2 += Wm[a][b] * Wm[a][b];
+        }
+    double S2[3][3], W2[3][3];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            double p = 0, q = 0;
+            for (int k = 0; k < 3; k++) {
+                p += S[a][k] * S[k][b];
+                q += Wm[a][k] * Wm[k][b];
+            }
+            S2[a][b] = p;
+            W2[a][b] = q;
+        }
+    double trS3 = 0, trSW2 = 0, trS2W2 = 0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            trS3 += S2[a][b] * S[b][a];
+            trSW2 += S[a][b] * W2[b][a];
+            trS2W2 += S2[a][b] * W2[b][a];
+        }
+    const double eps = 1e-30, sw = s2 + w2;
+    const double smag = sqrt(2.0 * s2);
+    const double c = sqrt(GAMMA * R_GAS * T);
+    const double gTm = sqrt(gT[0] * gT[0] + gT[1] * gT[1] + gT[2] * gT[2]);
+    x[0] = log1p(rho * delta * delta * smag / mu);
+    x[1] = w2 / (sw + eps);
+    x[2] = trS3 / (pow(s2, 1.5) + eps);
+    x[3] = trSW2 / (pow(sw, 1.5) + eps);
+    x[4] = trS2W2 / (sw * sw + eps);
+    x[5] = (gu[0][0] + gu[1][1] + gu[2][2]) / (sqrt(sw) + eps);
+    x[6] = delta * gTm / T;
+    x[7] = delta * smag / c;
+    x[8] = log(rho);
+}
+
+namespace {
+
+template <typename R>
+__device__ __forceinline__ double metv(const Metrics<R> &m, int c, long long i) {
+    return (double)(m.constant ? m.c[c] : m.m[c][i]);
+}
+
+// Fused closure evaluation: features of every point, BF16 tensor-core MLP,
+// mu_sgs and k_sgs; points with a feature outside the training range set *flag.
+template <typename R>
+__global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f,
+                                                       DerivPtrs12c<R> dp, Metrics<R> m, double dvol, double mu_ref,
+                                                       const __nv_bfloat16 *__restrict__ Hw,
+                                                       const float *__restrict__ Bc, MlpNorm nrm, R *mu_sgs, R *ksgs,
+                                                       int *flag) {
+    constexpr int XS = 24;
+    __shared__ __align__(16) __nv_bfloat16 sW[MLP_NHALF];
+    __shared__ float bias[3 * 64 + MLP_OUT];
+    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * XS];
+    __shared__ float ys[4][64];
+    for (int k = threadIdx.x; k < MLP_NHALF; k += blockDim.x) sW[k] = Hw[k];
+    for (int k = threadIdx.x; k < 3 * 64 + MLP_OUT; k += blockDim.x) bias[k] = Bc[k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long n = g.n();
+    const long long stride = (long long)gridDim.x * 4 * 32;
+    for (long long base = ((long long)blockIdx.x * 4 + warp) * 32; base < n; base += stride) {
+        const long long i = base + lane;
+        const bool ok = i < n;
+        double rho = 1.0, scale = 0.0;
+        bool out_of_range = false;
+        __nv_bfloat16 *row = xs[warp] + lane * XS;
+        if (ok) {
+            double gu[3][3], gT[3];
+            for (int a = 0; a < 3; a++) {
+                const double d1 = (double)dp.p[3 * a][i], d2 = (double)dp.p[3 * a + 1][i], d3 = (double)dp.p[3 * a + 2][i];
+                for (int b = 0; b < 3; b++) gu[a][b] = metv(m, 1 + b, i) * d1 + metv(m, 4 + b, i) * d2 + metv(m, 7 + b, i) * d3;
+            }
+            {
+                const double d1 = (double)dp.p[9][i], d2 = (double)dp.p[10][i], d3 = (double)dp.p[11][i];
+                for (int b = 0; b < 3; b++) gT[b] = metv(m, 1 + b, i) * d1 + metv(m, 4 + b, i) * d2 + metv(m, 7 + b, i) * d3;
+            }
+            rho = (double)rho_f[i];
+            const double T = (double)T_f[i];
+            const double delta = pow(dvol / metv(m, 0, i), 1.0 / 3.0);
+            const double mu = mu_ref * pow(T, 0.76);
+            double x[MLP_IN];
+            mlp_features(gu, rho, T, gT, delta, mu, x);
+            double s2 = 0;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    const double sab = 0.5 * (gu[a][b] + gu[b][a]);
+                    s2 += sab * sab;
+                }
+            scale = rho * delta * delta * sqrt(2.0 * s2);   // mu_t / C
+#pragma unroll
+            for (int k = 0; k < MLP_IN; k++) {
+                if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;
+                row[k] = __float2bfloat16_rn(((float)x[k] - nrm.mean[k]) * nrm.inv_std[k]);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < MLP_IN; k++) row[k] = __float2bfloat16_rn(0.0f);
+        }
+#pragma unroll
+        for (int k = MLP_IN; k < 16; k++) row[k] = __float2bfloat16_rn(0.0f);
+        if (__any_sync(0xffffffffu, out_of_range) && lane == 0) atomicOr(flag, 1);
+        __syncwarp();
+        mlp_tile16<XS>(xs[warp], 0, sW, bias, ys[warp], lane);
+        mlp_tile16<XS>(xs[warp], 16, sW, bias, ys[warp], lane);
+        __syncwarp();
+        if (ok) {
+            const double C = fmax(0.0, (double)ys[warp][lane * 2 + 0] * nrm.ystd[0] + nrm.ymean[0]);
+            const double prt = fmin(10.0, fmax(0.1, (double)ys[warp][lane * 2 + 1] * nrm.ystd[1] + nrm.ymean[1]));
+            const double mt = C * scale;
+            mu_sgs[i] = (R)mt;
+            ksgs[i] = (R)(CP * mt / prt);
+        }
+        __syncwarp();
+    }
+}
+
+// ---- training data -----------------------------------------------------------
+// box filter of factor f of the DNS state (FP64, fine grid Nx*Ny*Nz) onto the
+// coarse grid: rho, rhoU_i, rhoU_i U_j (6), rho T, rhoU_i T (3): 14 fields
+__global__ void box_filter_kernel(Grid3 gf, int f, Q5c q, CoarseOut out) {
+    const Grid3 gc{gf.Nx / f, gf.Ny / f, gf.Nz / f};
+    const long long nc = gc.n();
+    const double w = 1.0 / ((double)f * f * f);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+        const long long ci = c % gc.Nx, cj = (c / gc.Nx) % gc.Ny, ck = c / ((long long)gc.Nx * gc.Ny);
+        double acc[14];
+        for (int k = 0; k < 14; k++) acc[k] = 0.0;
+        for (int dk = 0; dk < f; dk++)
+            for (int dj = 0; dj < f; dj++)
+                for (int di = 0; di < f; di++) {
+                    const long long i = (ci * f + di) + (long long)gf.Nx * ((cj * f + dj) + (long long)gf.Ny * (ck * f + dk));
+                    const double rho = q.p[0][i], ru = q.p[1][i], rv = q.p[2][i], rw = q.p[3][i];
+                    const double u = ru / rho, v = rv / rho, wv = rw / rho;
+                    const double p = (GAMMA - 1) * (q.p[4][i] - 0.5 * rho * (u * u + v * v + wv * wv));
+                    const double T = p / (rho * R_GAS);
+                    const double vals[14] = {rho, ru, rv, rw, ru * u, ru * v, ru * wv, rv * v, rv * wv, rw * wv,
+                                             rho * T, ru * T, rv * T, rw * T};
+                    for (int k = 0; k < 14; k++) acc[k] += vals[k];
+                }
+        for (int k = 0; k < 14; k++) out.p[k][c] = acc[k] * w;
+    }
+}
+
+// features and least-squares targets on the coarse grid. gd[3*var + dir]:
+// d/dxi_dir of u, v, w, T (Favre-filtered) with box metrics J_ii = jd[dir].
+// C = -tau^d_ij S^d_ij / (2 rho Delta^2 |S| S^d:S^d); kappa_t = -q_j dT_j / |dT|^2,
+// Pr_t = mu_t / kappa_t clipped to [0.1, 10] (0.9 where it is undefined).
+__global__ void training_pairs_kernel(Grid3 gc, CoarseIn c, GradIn gd, double jd0, double jd1, double jd2,
+                                      double delta, double mu_ref, float *__restrict__ x, float *__restrict__ y) {
+    const long long n = gc.n();
+    const double jd[3] = {jd0, jd1, jd2};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double rho = c.p[0][i];
+        const double ut[3] = {c.p[1][i] / rho, c.p[2][i] / rho, c.p[3][i] / rho};
+        const double T = c.p[10][i] / rho;
+        double gu[3][3], gT[3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) gu[a][b] = jd[b] * gd.p[3 * a + b][i];
+        for (int b = 0; b < 3; b++) gT[b] = jd[b] * gd.p[9 + b][i];
+        const double mu = mu_ref * pow(T, 0.76);
+        double f[MLP_IN];
+        mlp_features(gu, rho, T, gT, delta, mu, f);
+        // SGS stress and heat flux of the box filter
+        const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+        double tau[3][3];
+        for (int k = 0; k < 6; k++) {
+            const int a = ij[k][0], b = ij[k][1];
+            tau[a][b] = tau[b][a] = c.p[4 + k][i] - c.p[1 + a][i] * c.p[1 + b][i] / rho;
+        }
+        const double trt = (tau[0][0] + tau[1][1] + tau[2][2]) / 3.0;
+        double S[3][3], trs = 0;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) S[a][b] = 0.5 * (gu[a][b] + gu[b][a]);
+        trs = (S[0][0] + S[1][1] + S[2][2]) / 3.0;
+        double ts = 0, ss = 0, s2 = 0;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                const double sd = S[a][b] - (a == b ? trs : 0.0);
+                const double td = tau[a][b] - (a == b ? trt : 0.0);
+                ts += td * sd;
+                ss += sd * sd;
+                s2 += S[a][b] * S[a][b];
+            }
+        const double smag = sqrt(2.0 * s2);
+        const double denom = 2.0 * rho * delta * delta * smag * ss;
+        const double C = denom > 0 ? -ts / denom : 0.0;
+        double qd = 0, g2 = 0;
+        for (int b = 0; b < 3; b++) {
+            const double qb = c.p[11 + b][i] - c.p[1 + b][i] * c.p[10][i] / rho;
+            qd += qb * gT[b];
+            g2 += gT[b] * gT[b];
+        }
+        const double kappa = g2 > 0 ? -qd / g2 : 0.0;
+        const double mut = rho * C * delta * delta * smag;
+        double prt = 0.9;
+        if (kappa > 0 && mut > 0) prt = fmin(10.0, fmax(0.1, mut / kappa));
+        for (int k = 0; k < MLP_IN; k++) x[i * MLP_IN + k] = (float)f[k];
+        y[i * 2 + 0] = (float)C;
+        y[i * 2 + 1] = (float)prt;
+    }
+}
+
+}  // namespace
+
+template <typename R>
+int launch_sgs_mlp(const Grid3 &g, const R *rho, const R *T, const R *const d[12], const Metrics<R> &m, double dvol,
+                   double mu_ref, const MlpDev &mlp, R *mu_sgs, R *ksgs, int *flag, cudaStream_t st) {
+    DerivPtrs12c<R> dp;
+    for (int k = 0; k < 12; k++) dp.p[k] = d[k];
+    const int blocks = (int)std::min<long long>((g.n() + 127) / 128, 148 * 6);
+    sgs_mlp_kernel<R><<<blocks, 128, 0, st>>>(g, rho, T, dp, m, dvol, mu_ref, mlp.Hw, mlp.Bc, mlp.norm, mu_sgs, ksgs,
+                                              flag);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+template int launch_sgs_mlp<float>(const Grid3 &, const float *, const float *, const float *const[12],
+                                   const Metrics<float> &, double, double, const MlpDev &, float *, float *, int *,
+                                   cudaStream_t);
+template int launch_sgs_mlp<double>(const Grid3 &, const double *, const double *, const double *const[12],
+                                    const Metrics<double> &, double, double, const MlpDev &, double *, double *, int *,
+                                    cudaStream_t);
+
+int launch_box_filter(const Grid3 &gf, int f, const double *const q[5], double *const out[14], cudaStream_t st) {
+    Q5c qq;
+    CoarseOut o;
+    for (int v = 0; v < 5; v++) qq.p[v] = q[v];
+    for (int k = 0; k < 14; k++) o.p[k] = out[k];
+    const long long nc = (long long)(gf.Nx / f) * (gf.Ny / f) * (gf.Nz / f);
+    box_filter_kernel<<<(int)std::min<long long>((nc + 255) / 256, 148 * 16), 256, 0, st>>>(gf, f, qq, o);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+int launch_training_pairs(const Grid3 &gc, const double *const coarse[14], const double *const grads[12],
+                          const double jd[3], double delta, double mu_ref, float *x, float *y, cudaStream_t st) {
+    CoarseIn c;
+    GradIn gd;
+    for (int k = 0; k < 14; k++) c.p[k] = coarse[k];
+    for (int k = 0; k < 12; k++) gd.p[k] = grads[k];
+    training_pairs_kernel<<<(int)std::min<long long>((gc.n() + 255) / 256, 148 * 16), 256, 0, st>>>(
+        gc, c, gd, jd[0], jd[1], jd[2], delta, mu_ref, x, y);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+}  // namespace mc3d

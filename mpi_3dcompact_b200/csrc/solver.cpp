@@ -44,6 +44,10 @@ struct mc3d_solver_s {
     void *Tmu = nullptr;
     int wall_mask = 0;
     bool tmu_from_init = false;
+    // learned closure (LESMODEL = MLP): the network, its out-of-range flag and the DSM fallbacks
+    mc3d_mlp mlp = nullptr;
+    int *mlp_flag = nullptr, *mlp_flag_host = nullptr;
+    long long mlp_fallbacks = 0;
     double *met64[10] = {};
     void *metR[10] = {};
     bool const_met = true;
@@ -417,7 +421,7 @@ static int dsm_ksgs(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
 template <typename R>
 static int stage_rhs(mc3d_solver s, double *const *qP) {
     int rc;
-    const bool dsm = s->cfg.les_model == MC3D_DSM;
+    bool dsm = s->cfg.les_model == MC3D_DSM;
     // gradients of U, V, W, T in each direction: der[3*var + dir]; with DSM
     // the T gradient waits for the tau_kk correction of T
     for (int d = 0; d < 3; d++) {
@@ -451,7 +455,25 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
             mu_sgs = (const R *)res[0];
             fp.les = 2;
         }
-    } else if (dsm) {
+    } else if (s->cfg.les_model == MC3D_MLPSGS) {
+        // learned closure; a feature outside the training range sends the stage to DSM
+        MC3D_CUDA_TRY(cudaMemsetAsync(s->mlp_flag, 0, sizeof(int), s->stream));
+        s->launches++;
+        if ((rc = tic(s, KC_SGS, (14.0 + 2.0) * sizeof(R) * (double)s->g.n()))) return rc;
+        if ((rc = launch_sgs_mlp<R>(s->g, pr[0], pr[4], dd, m, s->dxi[0] * s->dxi[1] * s->dxi[2], s->cfg.mu_ref,
+                                    *mlp_dev(s->mlp), (R *)s->mu_sgs, (R *)s->ksgs, s->mlp_flag, s->stream)))
+            return rc;
+        if ((rc = toc(s))) return rc;
+        MC3D_CUDA_TRY(cudaMemcpyAsync(s->mlp_flag_host, s->mlp_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        if (*s->mlp_flag_host) {
+            s->mlp_fallbacks++;
+            dsm = true;
+        } else {
+            fp.les = 3;   // mu_sgs and k_sgs fields, no tau_kk
+        }
+    }
+    if (dsm) {
         if ((rc = dsm_mu_taukk<R>(s, qP, m))) return rc;
         for (int d = 0; d < 3; d++) {
             void *in[1] = {s->prim[4]}, *out[1] = {s->der[9 + d]};
@@ -468,7 +490,7 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
                    (s->const_met ? 0 : 10.0 * sizeof(R));
         if ((rc = tic(s, KC_FLUX, b * (double)s->g.n()))) return rc;
     }
-    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, mu_sgs, (const R *)s->ksgs, (const R *)s->taukk,
+    if ((rc = launch_flux<R>(s->g, pr, dd, m, fp, mu_sgs, (const R *)s->ksgs, dsm ? (const R *)s->taukk : nullptr,
                              (const R *)s->Tmu, F, s->stream)))
         return rc;
     if ((rc = toc(s))) return rc;
@@ -618,7 +640,7 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
             if ((rc = upload_line_op(dh, c.precision, s->dop[d]))) break;
             if ((rc = upload_line_op(fh, c.precision, s->fop[d]))) break;
             if ((rc = upload_line_op(vh, c.precision, s->vop[d]))) break;
-            if (c.les_model == MC3D_DSM) {
+            if (c.les_model == MC3D_DSM || c.les_model == MC3D_MLPSGS) {
                 // DSMTESTFILTER 1 -> Pade, 2 -> explicit (src/DSMSGS.hpp:57-67)
                 LineOpHost th = build_testfilter_op(c.dsm_test_filter == 1 ? MC3D_TESTFILTER_PADE : MC3D_TESTFILTER_EXP,
                                                     c.bc_type[d], N[d]);
@@ -644,7 +666,14 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
     for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
     if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, &s->mu_sgs, n * rb);
-    if (c.les_model == MC3D_DSM) {
+    if (c.les_model == MC3D_MLPSGS) {
+        if (!rc) rc = salloc(s, (void **)&s->mlp_flag, sizeof(int));
+        if (!rc) {
+            cudaError_t he = cudaMallocHost((void **)&s->mlp_flag_host, sizeof(int));
+            if (he != cudaSuccess) rc = fail(MC3D_ERR_OOM, "cudaMallocHost");
+        }
+    }
+    if (c.les_model == MC3D_DSM || c.les_model == MC3D_MLPSGS) {
         for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dA[i], n * rb);
         for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dB[i], n * rb);
         if (!rc) rc = salloc(s, &s->smag, n * rb);
@@ -685,6 +714,7 @@ int mc3d_solver_destroy(mc3d_solver s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (cudaEvent_t e : s->events) cudaEventDestroy(e);
     for (void *p : s->allocs) cudaFree(p);
+    if (s->mlp_flag_host) cudaFreeHost(s->mlp_flag_host);
     for (int d = 0; d < 3; d++) {
         free_line_op(s->dop[d]);
         free_line_op(s->fop[d]);
@@ -850,6 +880,19 @@ int mc3d_solver_set_initial_device(mc3d_solver s, const double *rho, const doubl
     return set_initial_impl(s, rho, U, V, W, p, true);
 }
 
+int mc3d_solver_set_mlp(mc3d_solver s, mc3d_mlp m) {
+    if (!s || !m) return fail(MC3D_ERR_ARG, "null argument");
+    if (s->cfg.les_model != MC3D_MLPSGS) return fail(MC3D_ERR_CONFIG, "LESMODEL is not MLP");
+    s->mlp = m;
+    return MC3D_OK;
+}
+
+int mc3d_solver_mlp_fallbacks(mc3d_solver s, long long *stages) {
+    if (!s || !stages) return fail(MC3D_ERR_ARG, "null argument");
+    *stages = s->mlp_fallbacks;
+    return MC3D_OK;
+}
+
 int mc3d_solver_set_sponge(mc3d_solver s, const double *sigma) {
     if (!s || !sigma) return fail(MC3D_ERR_ARG, "null argument");
     if (!s->have_sponge) return fail(MC3D_ERR_CONFIG, "no face is a SPONGE");
@@ -875,6 +918,7 @@ int mc3d_solver_set_sponge_avg(mc3d_solver s, const double *const avg[5]) {
 int mc3d_solver_step(mc3d_solver s, int nsteps) {
     if (!s) return fail(MC3D_ERR_ARG, "null solver");
     if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no initial condition");
+    if (s->cfg.les_model == MC3D_MLPSGS && !s->mlp) return fail(MC3D_ERR_CONFIG, "LESMODEL = MLP needs mc3d_solver_set_mlp");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
     for (int i = 0; i < nsteps; i++) {
         int rc = s->prec == MC3D_FP64 ? one_step<double>(s) : one_step<float>(s);
@@ -894,6 +938,16 @@ int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *
     TimeState t;
     MC3D_CUDA_TRY(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
     if (t.nonfinite) return fail(MC3D_ERR_NONFINITE, "the state became non-finite");
+    return MC3D_OK;
+}
+
+int mc3d_solver_copy_conserved_device(mc3d_solver s, double *const dst[5]) {
+    if (!s || !dst) return fail(MC3D_ERR_ARG, "null argument");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    size_t n = (size_t)s->g.n();
+    for (int v = 0; v < 5; v++)
+        if (dst[v]) MC3D_CUDA_TRY(cudaMemcpyAsync(dst[v], s->q1[v], n * 8, cudaMemcpyDeviceToDevice, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return MC3D_OK;
 }
 

@@ -1,0 +1,121 @@
+"""Training of the learned SGS closure from this solver's own DNS.
+
+No counterpart in the reference (its SGS models are VremanSGS and DSMSGS).
+Pipeline, all on the GPU:
+
+1. DNS of decaying HIT on a fine grid with ``CurvilinearCSolver``
+   (LESMODEL = NOMODEL), snapshots of the conserved state;
+2. box filter of factor f onto the coarse LES grid (``mc3d_sgs_box_filter``):
+   rho, rhoU_i, rhoU_iU_j, rhoT, rhoU_iT;
+3. Favre-filtered u, v, w, T and their compact xi-derivatives on the coarse
+   grid (the solver's own ``Pade6`` operators);
+4. features and least-squares targets per coarse point
+   (``mc3d_sgs_training_pairs``): C = -tau^d:S^d / (2 rho Delta^2 |S| S^d:S^d)
+   and Pr_t from the SGS heat flux;
+5. Adam on the MSE of normalised targets (``MLPClosure.train_step``); the
+   feature normalisation and the training range (outside which the solver
+   falls back to DSM) come from the training set.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _native as N
+from . import CurvilinearCSolver, MLPClosure, Options, Pade6, PERIODIC_SOLVE
+from .hit_ic import hit_initial_condition
+
+C_RANGE = (-0.2, 0.5)      # clip of the pointwise least-squares coefficient
+PRT_RANGE = (0.1, 10.0)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _vp_array(ts):
+    return (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+def training_pairs(q, n_fine, factor, box=2.0 * math.pi, mu_ref=1e-3):
+    """Features x [n, 9] and targets y [n, 2] (torch float32 on the GPU) from
+    a DNS state q (5 device FP64 tensors (N, N, N)) box-filtered by `factor`."""
+    torch = _torch()
+    nc = n_fine // factor
+    coarse = [torch.empty((nc, nc, nc), dtype=torch.float64, device="cuda") for _ in range(14)]
+    N.check(N.host_lib().mc3d_sgs_box_filter(_vp_array(q), n_fine, n_fine, n_fine, factor, _vp_array(coarse), None))
+    rho = coarse[0]
+    fav = [coarse[1] / rho, coarse[2] / rho, coarse[3] / rho, coarse[10] / rho]   # u, v, w, T
+    grads = [torch.empty_like(rho) for _ in range(12)]
+    ops = [Pade6((nc, nc, nc), PERIODIC_SOLVE, d) for d in range(3)]
+    for v in range(4):
+        for d in range(3):
+            ops[d].calc1stDerivField(fav[v].contiguous(), grads[3 * v + d])
+    n = nc ** 3
+    x = torch.empty((n, 9), dtype=torch.float32, device="cuda")
+    y = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    jd = (C.c_double * 3)(1.0 / box, 1.0 / box, 1.0 / box)
+    N.check(N.host_lib().mc3d_sgs_training_pairs(_vp_array(coarse), _vp_array(grads), nc, nc, nc, jd, box / nc,
+                                                 mu_ref, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), None))
+    torch.cuda.synchronize()
+    ok = torch.isfinite(x).all(dim=1) & torch.isfinite(y).all(dim=1)
+    x, y = x[ok], y[ok]
+    y[:, 0].clamp_(*C_RANGE)
+    y[:, 1].clamp_(*PRT_RANGE)
+    return x, y
+
+
+def dns_snapshots(n=128, seeds=(0,), steps=(20, 40), k0=4.0, mt=0.3, mu_ref=1e-3, precision=0):
+    """Conserved-state snapshots (device FP64 tensors (n, n, n)) of HIT DNS runs
+    with the given seeds, taken after each count of time steps in `steps`."""
+    torch = _torch()
+    out = []
+    for seed in seeds:
+        opt = Options(grid=n, fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=mu_ref,
+                      precision=precision)
+        s = CurvilinearCSolver(opt)
+        s.set_box_metrics(2.0 * math.pi)
+        s.set_initial_conditions(*hit_initial_condition(n, k0=k0, seed=seed, mt=mt))
+        done = 0
+        for target in steps:
+            s.step(target - done)
+            done = target
+            snap = [torch.empty((n, n, n), dtype=torch.float64, device="cuda") for _ in range(5)]
+            s.copy_conserved_device(snap)
+            out.append(snap)
+        del s
+    return out
+
+
+def fit_normalization(mlp: MLPClosure, x, y, margin=0.05):
+    """Feature/target statistics of the training set into the network; the
+    training range is the data range widened by `margin` of its width."""
+    xd = x.double()
+    mean = xd.mean(0).cpu().numpy()
+    std = xd.std(0).clamp_min(1e-6).cpu().numpy()
+    lo = xd.min(0).values.cpu().numpy()
+    hi = xd.max(0).values.cpu().numpy()
+    w = hi - lo
+    yd = y.double()
+    mlp.set_normalization(mean, std, lo - margin * w, hi + margin * w, yd.mean(0).cpu().numpy(),
+                          yd.std(0).clamp_min(1e-6).cpu().numpy())
+
+
+def train(mlp: MLPClosure, x, y, steps=2000, batch=65536, lr=1e-3, seed=0):
+    """Adam on minibatches of the normalised targets; returns the loss history."""
+    torch = _torch()
+    nrm = mlp.normalization()
+    ym = torch.tensor(nrm["ymean"], device="cuda")
+    ys = torch.tensor(nrm["ystd"], device="cuda")
+    yn = ((y - ym) / ys).contiguous()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    n = x.shape[0]
+    hist = []
+    for it in range(steps):
+        idx = torch.randint(0, n, (min(batch, n),), device="cuda", generator=g)
+        hist.append(mlp.train_step(x[idx].contiguous(), yn[idx].contiguous(), lr))
+    return hist

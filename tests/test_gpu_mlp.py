@@ -1,0 +1,189 @@
+"""GPU tests of the learned SGS closure (no counterpart in the reference):
+the FP32 forward and the Adam step against a numpy restatement of the
+network, the BF16 tensor-core inference against the FP32 forward, training
+progress, save/load, training pairs from a DNS of this solver, and the solver
+running LESMODEL = MLP with its DSM fallback.
+
+Tolerances: FP32 forward 1e-5 relative to the output scale (FP32 rounding of
+~200-term dot products); BF16 inference 3e-2 of the output scale (8-bit
+mantissas through four layers, FP32 accumulation)."""
+import math
+
+import numpy as np
+import pytest
+from scipy.special import erf
+
+import mpi_3dcompact_b200 as m
+
+pytestmark = pytest.mark.gpu
+
+OFF = dict(W1=0, B1=576, W2=640, B2=4736, W3=4800, B3=8896, W4=8960, B4=9088)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def np_forward(P, x, mean, std):
+    """The network as numpy (float64): returns pre-activations, activations, output."""
+    def lin(a, w, b, nout, nin):
+        return a @ P[w:w + nout * nin].reshape(nout, nin).T.astype(np.float64) + P[b:b + nout]
+    a0 = (x - mean) / std
+    z1 = lin(a0, OFF["W1"], OFF["B1"], 64, 9)
+    h1 = 0.5 * z1 * (1 + erf(z1 / math.sqrt(2)))
+    z2 = lin(h1, OFF["W2"], OFF["B2"], 64, 64)
+    h2 = 0.5 * z2 * (1 + erf(z2 / math.sqrt(2)))
+    z3 = lin(h2, OFF["W3"], OFF["B3"], 64, 64)
+    h3 = 0.5 * z3 * (1 + erf(z3 / math.sqrt(2)))
+    out = lin(h3, OFF["W4"], OFF["B4"], 2, 64)
+    return (a0, z1, h1, z2, h2, z3, h3), out
+
+
+def np_grad(P, x, y, mean, std):
+    """Gradient of mean_b sum_o (out - y)^2 with respect to every parameter."""
+    (a0, z1, h1, z2, h2, z3, h3), out = np_forward(P, x, mean, std)
+    n = x.shape[0]
+    G = np.zeros(P.shape, dtype=np.float64)
+
+    def dgelu(z):
+        return 0.5 * (1 + erf(z / math.sqrt(2))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    d4 = 2 * (out - y) / n
+    W4 = P[OFF["W4"]:OFF["W4"] + 128].reshape(2, 64).astype(np.float64)
+    W3 = P[OFF["W3"]:OFF["W3"] + 4096].reshape(64, 64).astype(np.float64)
+    W2 = P[OFF["W2"]:OFF["W2"] + 4096].reshape(64, 64).astype(np.float64)
+    d3 = (d4 @ W4) * dgelu(z3)
+    d2 = (d3 @ W3) * dgelu(z2)
+    d1 = (d2 @ W2) * dgelu(z1)
+    for d, a, w, b, no, ni in ((d1, a0, "W1", "B1", 64, 9), (d2, h1, "W2", "B2", 64, 64),
+                               (d3, h2, "W3", "B3", 64, 64), (d4, h3, "W4", "B4", 2, 64)):
+        G[OFF[w]:OFF[w] + no * ni] = (d.T @ a).reshape(-1)
+        G[OFF[b]:OFF[b] + no] = d.sum(0)
+    return G
+
+
+def _mlp_with_random_params(seed=1):
+    rng = np.random.default_rng(seed)
+    mlp = m.MLPClosure(seed=seed)
+    P = (rng.standard_normal(9090) * 0.2).astype(np.float32)
+    mlp.set_params(P)
+    mean = rng.standard_normal(9).astype(np.float32)
+    std = (0.5 + rng.random(9)).astype(np.float32)
+    mlp.set_normalization(mean, std, np.full(9, -1e30), np.full(9, 1e30), np.zeros(2), np.ones(2))
+    return mlp, P, mean, std, rng
+
+
+def test_forward_matches_numpy():
+    torch = _torch()
+    mlp, P, mean, std, rng = _mlp_with_random_params()
+    x = rng.standard_normal((1000, 9)).astype(np.float32)
+    xt = torch.tensor(x, device="cuda")
+    yt = torch.empty((1000, 2), dtype=torch.float32, device="cuda")
+    mlp.forward(xt, yt)
+    torch.cuda.synchronize()
+    _, ref = np_forward(P.astype(np.float64), x.astype(np.float64), mean.astype(np.float64), std.astype(np.float64))
+    scale = np.abs(ref).max()
+    assert np.abs(yt.cpu().numpy() - ref).max() <= 1e-5 * scale
+
+
+def test_bf16_inference_matches_fp32():
+    torch = _torch()
+    mlp, P, mean, std, rng = _mlp_with_random_params(2)
+    n = 10007                                    # not a multiple of 32: ragged last tile
+    x = torch.tensor(rng.standard_normal((n, 9)).astype(np.float32), device="cuda")
+    y32 = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    y16 = torch.empty_like(y32)
+    mlp.forward(x, y32)
+    mlp.infer_bf16(x, y16)
+    torch.cuda.synchronize()
+    scale = y32.abs().max().item()
+    err = (y16 - y32).abs().max().item()
+    assert err <= 3e-2 * scale, (err, scale)
+
+
+def test_adam_first_step_follows_the_gradient():
+    torch = _torch()
+    mlp, P, mean, std, rng = _mlp_with_random_params(3)
+    n = 2048
+    x = rng.standard_normal((n, 9)).astype(np.float32)
+    y = rng.standard_normal((n, 2)).astype(np.float32)
+    G = np_grad(P.astype(np.float64), x.astype(np.float64), y.astype(np.float64), mean.astype(np.float64),
+                std.astype(np.float64))
+    lr = 1e-4
+    loss = mlp.train_step(torch.tensor(x, device="cuda"), torch.tensor(y, device="cuda"), lr)
+    _, out = np_forward(P.astype(np.float64), x.astype(np.float64), mean.astype(np.float64), std.astype(np.float64))
+    assert abs(loss - np.mean(np.sum((out - y) ** 2, axis=1))) <= 1e-4 * loss
+    dP = mlp.params().astype(np.float64) - P.astype(np.float64)
+    big = np.abs(G) > 1e-3 * np.abs(G).max()
+    # the first Adam step is -lr * g / (|g| + eps): -lr * sign(g) where g is not tiny
+    assert np.mean(np.sign(dP[big]) == -np.sign(G[big])) > 0.995
+    assert np.allclose(np.abs(dP[big]), lr, rtol=2e-2)
+
+
+def test_training_reduces_loss_and_save_load(tmp_path):
+    torch = _torch()
+    rng = np.random.default_rng(4)
+    n = 20000
+    x = rng.standard_normal((n, 9)).astype(np.float32)
+    y = np.stack([np.sin(x[:, 0]) + 0.5 * x[:, 1] ** 2, np.cos(x[:, 2]) * x[:, 3]], axis=1).astype(np.float32)
+    mlp = m.MLPClosure(seed=5)
+    mlp.set_normalization(np.zeros(9), np.ones(9), np.full(9, -10.0), np.full(9, 10.0), np.zeros(2), np.ones(2))
+    xt, yt = torch.tensor(x, device="cuda"), torch.tensor(y, device="cuda")
+    losses = [mlp.train_step(xt[i * 4000:(i + 1) * 4000], yt[i * 4000:(i + 1) * 4000], 3e-3) for i in range(5)]
+    for it in range(400):
+        idx = torch.randint(0, n, (4096,), device="cuda")
+        losses.append(mlp.train_step(xt[idx].contiguous(), yt[idx].contiguous(), 3e-3))
+    assert losses[-1] < 0.1 * losses[0], (losses[0], losses[-1])
+    path = tmp_path / "closure.bin"
+    mlp.save(path)
+    other = m.MLPClosure(seed=99)
+    other.load(path)
+    assert np.array_equal(other.params(), mlp.params())
+    a, b = torch.empty((n, 2), device="cuda"), torch.empty((n, 2), device="cuda")
+    mlp.infer_bf16(xt, a)
+    other.infer_bf16(xt, b)
+    assert torch.equal(a, b)
+
+
+def _hit_les_solver(n, les, avg="GLOBAL", precision=m.FP32BULK):
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    opt = m.Options(grid=n, fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=1e-3, les=les,
+                    les_avg=avg, precision=precision)
+    s = m.CurvilinearCSolver(opt)
+    s.set_box_metrics(2.0 * math.pi)
+    s.set_initial_conditions(*hit_initial_condition(n, k0=4.0, seed=7, mt=0.3))
+    return s
+
+
+def test_training_pairs_and_les_with_fallback():
+    """Training pairs from a 64^3 DNS box-filtered to 16^3, a short training,
+    then 16^3 LES with the closure: finite, dissipative; a training range that
+    excludes every state sends every stage to DSM."""
+    from mpi_3dcompact_b200 import learned_sgs as L
+    snaps = L.dns_snapshots(n=64, seeds=(1,), steps=(10, 20))
+    xs, ys = zip(*[L.training_pairs(q, 64, 4) for q in snaps])
+    torch = _torch()
+    x, y = torch.cat(xs), torch.cat(ys)
+    assert x.shape[1] == 9 and x.shape[0] > 7000
+    assert torch.isfinite(x).all() and torch.isfinite(y).all()
+    assert y[:, 0].mean().item() > 0            # net forward energy transfer on average
+    mlp = m.MLPClosure(seed=6)
+    L.fit_normalization(mlp, x, y)
+    hist = L.train(mlp, x, y, steps=150, batch=4096, lr=1e-3)
+    assert hist[-1] < hist[0]
+    s = _hit_les_solver(16, "MLP")
+    s.set_mlp(mlp)
+    ke0, _ = s.integrals()
+    s.step(3)
+    ke1, _ = s.integrals()
+    assert 0 < ke1 < ke0
+    # a training range no state can lie in: every stage falls back to DSM
+    nrm = mlp.normalization()
+    mlp2 = m.MLPClosure(seed=6)
+    mlp2.set_params(mlp.params())
+    mlp2.set_normalization(nrm["mean"], nrm["std"], nrm["hi"] + 1.0, nrm["hi"] + 2.0, nrm["ymean"], nrm["ystd"])
+    s2 = _hit_les_solver(16, "MLP")
+    s2.set_mlp(mlp2)
+    s2.step(2)
+    assert s2.mlp_fallbacks() == 8
+    assert s.mlp_fallbacks() <= 12
