@@ -10,6 +10,12 @@ One "step" is one time step of the solver (LSLDDRK4 alternates 5- and
 6-stage halves; the metric counts the stages actually run). N > 1 runs
 independent replicas (one per rank, different seeds): the path has no
 exchange between GPUs. Rank 0 prints one JSON line.
+
+At N = 1 the line also carries "learned_sgs": a posteriori 128^3 LES of the
+same HIT (PADE6, RK4, COMPACT10 alpha_f = 0.49, FP32-bulk, 500 steps) with
+the learned closure shipped in mpi_3dcompact_b200/data (DSM with GLOBAL
+averaging as its fallback) against DSM and against no model: device time per
+step, fallback stages, kinetic-energy decay and the final energy spectrum.
 """
 from __future__ import annotations
 
@@ -35,6 +41,9 @@ SCHEME = dict(fd="PENTA10", filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4", les="
 WORKLOAD = ("decaying HIT 256^3 periodic box 2*pi, PENTA10 derivatives, COMPACT8 filter alpha_f=0.45 every step, "
             "LSLDDRK4, VREMAN SGS, CFL 0.5, Mt=0.3, Re_lambda~100, FP32-bulk (FP64 state, RK registers, dt/time)")
 CPU_SAMPLE_GRID = 64
+LES_GRID, LES_STEPS, LES_MU, LES_SEED = 128, 500, 2.5e-4, 5
+LES_SCHEME = dict(fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", les_avg="GLOBAL", cfl=0.5)
+MLP_WEIGHTS = os.path.join(ROOT, "mpi_3dcompact_b200", "data", "mlp_sgs_hit128.bin")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -179,6 +188,91 @@ def run_reference_arm(args):
     return 0
 
 
+def energy_spectrum(torch, q):
+    """Shell-summed kinetic energy spectrum E(k), k = 0..N/2, of a periodic
+    conserved state q (5 device tensors (N, N, N))."""
+    n = q[0].shape[0]
+    e = None
+    for c in range(1, 4):
+        uh = torch.fft.fftn(q[c] / q[0]) / n ** 3
+        p = 0.5 * (uh.real ** 2 + uh.imag ** 2)
+        e = p if e is None else e + p
+    k = torch.fft.fftfreq(n, d=1.0 / n, device=e.device, dtype=torch.float64)
+    kk = torch.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2)
+    shell = torch.round(kk).long().clamp_(max=n)
+    return torch.bincount(shell.reshape(-1), weights=e.reshape(-1), minlength=n + 1)[: n // 2 + 1].cpu().numpy()
+
+
+def learned_sgs_block(args, local):
+    """A posteriori LES with the learned closure against DSM and no model."""
+    import numpy as np
+    import torch
+
+    import mpi_3dcompact_b200 as m
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+
+    n, steps, chunk = LES_GRID, args.les_steps, 25
+    ic = hit_initial_condition(n, k0=K0, seed=LES_SEED, mt=MT)
+    out = {}
+    for les in ("MLP", "DSM", "NOMODEL"):
+        s = m.CurvilinearCSolver(m.Options(grid=n, mu_ref=LES_MU, les=les, precision=m.FP32BULK, **LES_SCHEME),
+                                 device=local)
+        s.set_box_metrics(2 * math.pi)
+        s.set_initial_conditions(*ic)
+        if les == "MLP":
+            mlp = m.MLPClosure(device=local)
+            mlp.load(MLP_WEIGHTS)
+            s.set_mlp(mlp)
+        stream = torch.cuda.ExternalStream(s.stream())
+        ke = [s.integrals()[0]]
+        ms = 0.0
+        done = 0
+        while done < steps:
+            k = min(chunk, steps - done)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.step(k)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            done += k
+            ke.append(s.integrals()[0])
+        q = [torch.empty((n, n, n), dtype=torch.float64, device=f"cuda:{local}") for _ in range(5)]
+        s.copy_conserved_device(q)
+        spec = energy_spectrum(torch, q)
+        out[les] = dict(ms=ms / steps, ke=np.array(ke), spec=spec, stages=s.info()["stages"],
+                        fallbacks=s.mlp_fallbacks() if les == "MLP" else None,
+                        finite=bool(all(torch.isfinite(t).all().item() for t in q)))
+        del s, q
+    mlp, dsm, nom = out["MLP"], out["DSM"], out["NOMODEL"]
+
+    def decay_diff(a):
+        da, dd = a["ke"][0] - a["ke"], dsm["ke"][0] - dsm["ke"]
+        return float(np.max(np.abs(da[1:] - dd[1:]) / np.abs(dd[1:])))
+
+    kmax = n // 3   # resolved band below the filter cut-off
+    band = slice(1, kmax + 1)
+
+    def spec_diff(a):
+        return float(np.linalg.norm(a["spec"][band] - dsm["spec"][band]) / np.linalg.norm(dsm["spec"][band]))
+
+    return {
+        "workload": f"decaying HIT {n}^3 LES, PADE6, RK4, COMPACT10 alpha_f=0.49 every step, CFL 0.5, Mt=0.3, "
+                    f"mu_ref={LES_MU}, FP32-bulk, {steps} steps from the seed-{LES_SEED} initial field",
+        "closure": "9-64-64-64-2 GELU MLP, BF16 tensor-core inference fused into the SGS pass; trained on 512^3 "
+                   "DNS box-filtered to 128^3 (mpi_3dcompact_b200/train_sgs.py)",
+        "ms_per_step": {"mlp": mlp["ms"], "dsm": dsm["ms"], "nomodel": nom["ms"]},
+        "mlp_speedup_over_dsm": dsm["ms"] / mlp["ms"],
+        "fallback_stages": mlp["fallbacks"], "stages": mlp["stages"],
+        "ke_decay_max_rel_diff_vs_dsm": {"mlp": decay_diff(mlp), "nomodel": decay_diff(nom)},
+        "ke_final": {"mlp": float(mlp["ke"][-1]), "dsm": float(dsm["ke"][-1]), "nomodel": float(nom["ke"][-1]),
+                     "initial": float(dsm["ke"][0])},
+        "spectrum_rel_l2_vs_dsm_k1_to_%d" % kmax: {"mlp": spec_diff(mlp), "nomodel": spec_diff(nom)},
+        "finite": {k: v["finite"] for k, v in out.items()},
+        "timing": "CUDA events on the solver stream over 25-step chunks, summed",
+    }
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -290,6 +384,10 @@ def run_ours(args):
                "d2h_bytes_per_step": int(5 * 8 * pts / args.steps + 32)}
         del out
 
+    les = None
+    if ws == 1 and not args.no_learned_sgs:
+        les = learned_sgs_block(args, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         rate, sample, kind, _ = cpu_reference_rate(CPU_SAMPLE_GRID, 2, 0)
@@ -321,7 +419,7 @@ def run_ours(args):
         "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
         "fp32_vs_fp64_rel_l2": err,
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk,
+        "clocks": clk, "learned_sgs": les,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -337,6 +435,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned-sgs", action="store_true")
+    ap.add_argument("--les-steps", type=int, default=LES_STEPS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -104,6 +104,12 @@ typedef struct mc3d_config {
      * (V, W) on X faces, (U, W) on Y faces, (U, V) on Z faces; the reference
      * sets them to zero in its constructor (src/CurvilinearCSolver.hpp:219-221) */
     double wall_velocity[6][2];
+    /* LESMODEL = MLP: a stage falls back to DSM when more than this fraction
+     * of its points has a feature outside the closure's training range; the
+     * features of the other out-of-range points are clamped to the range
+     * (LES.MLPFALLBACKFRAC, default 1e-3; 0 = any point). No counterpart in
+     * the reference. */
+    double mlp_fallback_frac;
 } mc3d_config;
 
 /* ---- configuration ---- */

@@ -184,7 +184,7 @@ class Options:
     def __init__(self, grid=(64, 64, 64), fd="PADE6", filter="COMPACT10", alphaF=0.45, mu_ref=1e-3, rk="RK4",
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
-                 dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None):
+                 dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -205,6 +205,7 @@ class Options:
         c.reference_quirks = int(bool(reference_quirks))
         c.dsm_test_filter = int(dsm_test_filter)
         c.dsm_use_taukk = int(bool(dsm_use_taukk))
+        c.mlp_fallback_frac = mlp_fallback_frac
         # BC kinds of the faces X0, X1, Y0, Y1, Z0, Z1 (names of src/Options.hpp:21-27);
         # default: PERIODIC on periodic directions, ADIABATIC_WALL otherwise
         kinds = bc_kind or [("PERIODIC" if bc[f // 2] == PERIODIC_SOLVE else "ADIABATIC_WALL") for f in range(6)]

@@ -24,7 +24,7 @@ CONST_DT, CONST_CFL = 0, 1
 PERIODIC_SOLVE, DIRICHLET_SOLVE = 0, 1
 CD2, PADE6, PENTA10 = 0, 1, 2
 COMPACT8, COMPACT10 = 0, 1
-NOMODEL, VREMAN, DSM = 0, 1, 2
+NOMODEL, VREMAN, DSM, MLPSGS = 0, 1, 2, 3
 AVG_NONE, AVG_XI1, AVG_XI2, AVG_XI3, AVG_LOCAL, AVG_GLOBAL = range(6)
 TVDRK3, RK4, KENRK4, LSLDDRK4 = 0, 1, 2, 3
 
@@ -46,7 +46,7 @@ class Config(C.Structure):
                 ("reference_quirks", C.c_int), ("dsm_test_filter", C.c_int), ("dsm_use_taukk", C.c_int),
                 ("sponge_kind", C.c_int), ("sponge_strength", C.c_double), ("sponge_rect_perc", C.c_double * 6),
                 ("sponge_cyl_orient", C.c_int), ("sponge_cyl_axis", C.c_double * 3), ("sponge_rmin", C.c_double),
-                ("wall_velocity", (C.c_double * 2) * 6)]
+                ("wall_velocity", (C.c_double * 2) * 6), ("mlp_fallback_frac", C.c_double)]
 
 
 _lib = None

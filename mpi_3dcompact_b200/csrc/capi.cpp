@@ -74,6 +74,7 @@ int mc3d_config_default(mc3d_config *c) {
     for (int d = 0; d < 3; d++) c->sponge_cyl_axis[d] = 0.0;
     c->sponge_rmin = 0.0;
     for (int f = 0; f < 6; f++) c->wall_velocity[f][0] = c->wall_velocity[f][1] = 0.0;
+    c->mlp_fallback_frac = 1e-3;
     return MC3D_OK;
 }
 
@@ -111,7 +112,7 @@ const char *KNOWN_KEYS[] = {
     "RESTART.SPONGEAVGFILENAME", "STATS.VELOCITYSTATS", "STATS.THERMOSTATS", "STATS.VELOCITYSTATSFROMRESTART",
     "STATS.THERMOSTATSFROMRESTART", "STATS.VELOCITYSTATSFILENAME", "STATS.THERMOSTATSFILENAME",
     "STATS.STATSAVGTYPE", "STATS.INTERVAL", "LES.LESMODEL", "LES.LESAVERAGING", "LES.DSMTESTFILTER",
-    "LES.DSMUSETAUKK", "LES.DSMCOEFFRANGE", "GPU.PRECISION", "GPU.REFERENCEQUIRKS"};
+    "LES.DSMUSETAUKK", "LES.DSMCOEFFRANGE", "LES.MLPFALLBACKFRAC", "GPU.PRECISION", "GPU.REFERENCEQUIRKS"};
 
 struct CfgError {
     std::string msg;
@@ -265,6 +266,11 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
             if (c->dsm_test_filter != 1 && c->dsm_test_filter != 2) throw CfgError{"DSMTESTFILTER must be 1 or 2"};
         }
         if (ini.has("LES.DSMUSETAUKK")) c->dsm_use_taukk = parse_bool("DSMUSETAUKK", ini.get("LES.DSMUSETAUKK"));
+        if (ini.has("LES.MLPFALLBACKFRAC")) {
+            c->mlp_fallback_frac = parse_double("MLPFALLBACKFRAC", ini.get("LES.MLPFALLBACKFRAC"));
+            if (!(c->mlp_fallback_frac >= 0.0 && c->mlp_fallback_frac <= 1.0))
+                throw CfgError{"MLPFALLBACKFRAC must lie in [0, 1]"};
+        }
         // [SPONGE]: read when a face is a sponge (src/Options.hpp:314-358)
         bool sponge = false;
         for (int f = 0; f < 6; f++) sponge = sponge || c->bc_kind[f] == MC3D_BC_SPONGE;

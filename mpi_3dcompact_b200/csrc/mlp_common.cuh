@@ -19,10 +19,23 @@ constexpr int MLPH_W4 = MLPH_W3 + 64 * MLPH_P;
 constexpr int MLPH_N = MLPH_W4 + 8 * MLPH_P;
 static_assert(MLPH_N == MLP_NHALF, "packed size");
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))): the
+// training kernels use tanhf, the tensor-core inference the hardware tanh.approx
+constexpr float GELU_K0 = 0.7978845608028654f, GELU_K1 = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+    return 0.5f * x * (1.0f + tanhf(GELU_K0 * (x + GELU_K1 * x * x * x)));
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-    // Phi(x) + x phi(x)
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+    const float t = tanhf(GELU_K0 * (x + GELU_K1 * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_K0 * (1.0f + 3.0f * GELU_K1 * x * x);
+}
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_fast(float x) {
+    return 0.5f * x * (1.0f + tanh_approx(GELU_K0 * (x + GELU_K1 * x * x * x)));
 }
 
 // ---------------------------------------------------------------------------
@@ -67,10 +80,10 @@ __device__ __forceinline__ void mlp_layer(const unsigned (&a)[KT][4], const __nv
                 mma_bf16(c[h], a[kt], b0, b1);
             }
         }
-        next[j][0] = pack_bf2(gelu(c[0][0]), gelu(c[0][1]));
-        next[j][1] = pack_bf2(gelu(c[0][2]), gelu(c[0][3]));
-        next[j][2] = pack_bf2(gelu(c[1][0]), gelu(c[1][1]));
-        next[j][3] = pack_bf2(gelu(c[1][2]), gelu(c[1][3]));
+        next[j][0] = pack_bf2(gelu_fast(c[0][0]), gelu_fast(c[0][1]));
+        next[j][1] = pack_bf2(gelu_fast(c[0][2]), gelu_fast(c[0][3]));
+        next[j][2] = pack_bf2(gelu_fast(c[1][0]), gelu_fast(c[1][1]));
+        next[j][3] = pack_bf2(gelu_fast(c[1][2]), gelu_fast(c[1][3]));
     }
 }
 
@@ -105,6 +118,52 @@ __device__ __forceinline__ void mlp_tile16(const __nv_bfloat16 *xs, int r0, cons
         ys[(r0 + g + 8) * 2 + 0] = c[2] + bias[192];
         ys[(r0 + g + 8) * 2 + 1] = c[3] + bias[193];
     }
+}
+
+// Features of one point (see sgs_mlp.cu), in FP32: the inference and the
+// training data both use this function.
+__device__ __forceinline__ void mlp_features(const float gu[3][3], float rho, float T, const float gT[3], float delta,
+                                             float mu, float *x) {
+    float S[3][3], Wm[3][3];
+    float s2 = 0.f, w2 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            S[a][b] = 0.5f * (gu[a][b] + gu[b][a]);
+            Wm[a][b] = 0.5f * (gu[a][b] - gu[b][a]);
+            s2 += S[a][b] * S[a][b];
+            w2 += Wm[a][b] * Wm[a][b];
+        }
+    float trS3 = 0.f, trSW2 = 0.f, trS2W2 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            float p = 0.f, q = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                p += S[a][k] * S[k][b];
+                q += Wm[a][k] * Wm[k][b];
+            }
+            // p = (S S)_ab, q = (W W)_ab
+            trS3 += p * S[b][a];
+            trSW2 += S[a][b] * q;
+            trS2W2 += p * q;
+        }
+    const float eps = 1e-30f, sw = s2 + w2;
+    const float smag = sqrtf(2.0f * s2);
+    const float c = sqrtf((float)(GAMMA * R_GAS) * T);
+    const float gTm = sqrtf(gT[0] * gT[0] + gT[1] * gT[1] + gT[2] * gT[2]);
+    x[0] = log1pf(rho * delta * delta * smag / mu);
+    x[1] = w2 / (sw + eps);
+    x[2] = trS3 / (s2 * sqrtf(s2) + eps);
+    x[3] = trSW2 / (sw * sqrtf(sw) + eps);
+    x[4] = trS2W2 / (sw * sw + eps);
+    x[5] = (gu[0][0] + gu[1][1] + gu[2][2]) / (sqrtf(sw) + eps);
+    x[6] = delta * gTm / T;
+    x[7] = delta * smag / c;
+    x[8] = logf(rho);
 }
 
 }  // namespace mc3d

@@ -24,59 +24,16 @@
 
 namespace mc3d {
 
-__device__ __forceinline__ void mlp_features(const double gu[3][3], double rho, double T, const double gT[3],
-                                             double delta, double mu, double *x) {
-    double S[3][3], Wm[3][3];
-    double s2 = 0, w2 = 0;
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++) {
-            S[a][b] = 0.5 * (gu[a][b] + gu[b][a]);
-            Wm[a][b] = 0.5 * (gu[a][b] - gu[b][a]);
-            s2 += S[a][b] * S[a][b];
-            w2 += Wm[a][b] * Wm[a][b];
-        }
-    double S2[3][3], W2[3][3];
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++) {
-            double p = 0, q = 0;
-            for (int k = 0; k < 3; k++) {
-                p += S[a][k] * S[k][b];
-                q += Wm[a][k] * Wm[k][b];
-            }
-            S2[a][b] = p;
-            W2[a][b] = q;
-        }
-    double trS3 = 0, trSW2 = 0, trS2W2 = 0;
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++) {
-            trS3 += S2[a][b] * S[b][a];
-            trSW2 += S[a][b] * W2[b][a];
-            trS2W2 += S2[a][b] * W2[b][a];
-        }
-    const double eps = 1e-30, sw = s2 + w2;
-    const double smag = sqrt(2.0 * s2);
-    const double c = sqrt(GAMMA * R_GAS * T);
-    const double gTm = sqrt(gT[0] * gT[0] + gT[1] * gT[1] + gT[2] * gT[2]);
-    x[0] = log1p(rho * delta * delta * smag / mu);
-    x[1] = w2 / (sw + eps);
-    x[2] = trS3 / (pow(s2, 1.5) + eps);
-    x[3] = trSW2 / (pow(sw, 1.5) + eps);
-    x[4] = trS2W2 / (sw * sw + eps);
-    x[5] = (gu[0][0] + gu[1][1] + gu[2][2]) / (sqrt(sw) + eps);
-    x[6] = delta * gTm / T;
-    x[7] = delta * smag / c;
-    x[8] = log(rho);
-}
-
 namespace {
 
 template <typename R>
-__device__ __forceinline__ double metv(const Metrics<R> &m, int c, long long i) {
-    return (double)(m.constant ? m.c[c] : m.m[c][i]);
+__device__ __forceinline__ float metf(const Metrics<R> &m, int c, long long i) {
+    return (float)(m.constant ? m.c[c] : m.m[c][i]);
 }
 
 // Fused closure evaluation: features of every point, BF16 tensor-core MLP,
-// mu_sgs and k_sgs; points with a feature outside the training range set *flag.
+// mu_sgs and k_sgs; *flag counts the points with a feature outside the training
+// range (those features are clamped to the range before the network).
 template <typename R>
 __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f,
                                                        DerivPtrs12c<R> dp, Metrics<R> m, double dvol, double mu_ref,
@@ -94,6 +51,7 @@ __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restri
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long n = g.n();
     const long long stride = (long long)gridDim.x * 4 * 32;
+    const float delta_c = m.constant ? cbrtf((float)(dvol / (double)m.c[0])) : 0.f;   // Delta of a uniform block
     for (long long base = ((long long)blockIdx.x * 4 + warp) * 32; base < n; base += stride) {
         const long long i = base + lane;
         const bool ok = i < n;
@@ -101,32 +59,40 @@ __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restri
         bool out_of_range = false;
         __nv_bfloat16 *row = xs[warp] + lane * XS;
         if (ok) {
-            double gu[3][3], gT[3];
+            float gu[3][3], gT[3];
+#pragma unroll
             for (int a = 0; a < 3; a++) {
-                const double d1 = (double)dp.p[3 * a][i], d2 = (double)dp.p[3 * a + 1][i], d3 = (double)dp.p[3 * a + 2][i];
-                for (int b = 0; b < 3; b++) gu[a][b] = metv(m, 1 + b, i) * d1 + metv(m, 4 + b, i) * d2 + metv(m, 7 + b, i) * d3;
+                const float d1 = (float)dp.p[3 * a][i], d2 = (float)dp.p[3 * a + 1][i], d3 = (float)dp.p[3 * a + 2][i];
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    gu[a][b] = metf(m, 1 + b, i) * d1 + metf(m, 4 + b, i) * d2 + metf(m, 7 + b, i) * d3;
             }
             {
-                const double d1 = (double)dp.p[9][i], d2 = (double)dp.p[10][i], d3 = (double)dp.p[11][i];
-                for (int b = 0; b < 3; b++) gT[b] = metv(m, 1 + b, i) * d1 + metv(m, 4 + b, i) * d2 + metv(m, 7 + b, i) * d3;
+                const float d1 = (float)dp.p[9][i], d2 = (float)dp.p[10][i], d3 = (float)dp.p[11][i];
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    gT[b] = metf(m, 1 + b, i) * d1 + metf(m, 4 + b, i) * d2 + metf(m, 7 + b, i) * d3;
             }
-            rho = (double)rho_f[i];
-            const double T = (double)T_f[i];
-            const double delta = pow(dvol / metv(m, 0, i), 1.0 / 3.0);
-            const double mu = mu_ref * pow(T, 0.76);
-            double x[MLP_IN];
-            mlp_features(gu, rho, T, gT, delta, mu, x);
-            double s2 = 0;
+            const float rhof = (float)rho_f[i], T = (float)T_f[i];
+            rho = rhof;
+            const float delta = m.constant ? delta_c : cbrtf((float)dvol / metf(m, 0, i));
+            const float mu = (float)mu_ref * __powf(T, 0.76f);
+            float x[MLP_IN];
+            mlp_features(gu, rhof, T, gT, delta, mu, x);
+            float s2 = 0.f;
+#pragma unroll
             for (int a = 0; a < 3; a++)
+#pragma unroll
                 for (int b = 0; b < 3; b++) {
-                    const double sab = 0.5 * (gu[a][b] + gu[b][a]);
+                    const float sab = 0.5f * (gu[a][b] + gu[b][a]);
                     s2 += sab * sab;
                 }
-            scale = rho * delta * delta * sqrt(2.0 * s2);   // mu_t / C
+            scale = (double)(rhof * delta * delta * sqrtf(2.0f * s2));   // mu_t / C
 #pragma unroll
             for (int k = 0; k < MLP_IN; k++) {
-                if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;
-                row[k] = __float2bfloat16_rn(((float)x[k] - nrm.mean[k]) * nrm.inv_std[k]);
+                if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;   // NaN counts as outside
+                const float xc = fminf(fmaxf(x[k], nrm.lo[k]), nrm.hi[k]);
+                row[k] = __float2bfloat16_rn((xc - nrm.mean[k]) * nrm.inv_std[k]);
             }
         } else {
 #pragma unroll
@@ -134,7 +100,8 @@ __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restri
         }
 #pragma unroll
         for (int k = MLP_IN; k < 16; k++) row[k] = __float2bfloat16_rn(0.0f);
-        if (__any_sync(0xffffffffu, out_of_range) && lane == 0) atomicOr(flag, 1);
+        const unsigned outside = __ballot_sync(0xffffffffu, out_of_range);
+        if (outside && lane == 0) atomicAdd(flag, __popc(outside));
         __syncwarp();
         mlp_tile16<XS>(xs[warp], 0, sW, bias, ys[warp], lane);
         mlp_tile16<XS>(xs[warp], 16, sW, bias, ys[warp], lane);
@@ -194,8 +161,12 @@ __global__ void training_pairs_kernel(Grid3 gc, CoarseIn c, GradIn gd, double jd
             for (int b = 0; b < 3; b++) gu[a][b] = jd[b] * gd.p[3 * a + b][i];
         for (int b = 0; b < 3; b++) gT[b] = jd[b] * gd.p[9 + b][i];
         const double mu = mu_ref * pow(T, 0.76);
-        double f[MLP_IN];
-        mlp_features(gu, rho, T, gT, delta, mu, f);
+        float guf[3][3], gTf[3], f[MLP_IN];
+        for (int a = 0; a < 3; a++) {
+            gTf[a] = (float)gT[a];
+            for (int b = 0; b < 3; b++) guf[a][b] = (float)gu[a][b];
+        }
+        mlp_features(guf, (float)rho, (float)T, gTf, (float)delta, (float)mu, f);
         // SGS stress and heat flux of the box filter
         const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
         double tau[3][3];

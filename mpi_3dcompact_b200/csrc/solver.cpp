@@ -456,7 +456,8 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
             fp.les = 2;
         }
     } else if (s->cfg.les_model == MC3D_MLPSGS) {
-        // learned closure; a feature outside the training range sends the stage to DSM
+        // learned closure; the stage goes to DSM when more than mlp_fallback_frac
+        // of the points have a feature outside the training range
         MC3D_CUDA_TRY(cudaMemsetAsync(s->mlp_flag, 0, sizeof(int), s->stream));
         s->launches++;
         if ((rc = tic(s, KC_SGS, (14.0 + 2.0) * sizeof(R) * (double)s->g.n()))) return rc;
@@ -466,7 +467,7 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
         if ((rc = toc(s))) return rc;
         MC3D_CUDA_TRY(cudaMemcpyAsync(s->mlp_flag_host, s->mlp_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
         MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
-        if (*s->mlp_flag_host) {
+        if ((double)*s->mlp_flag_host > s->cfg.mlp_fallback_frac * (double)s->g.n()) {
             s->mlp_fallbacks++;
             dsm = true;
         } else {
@@ -607,6 +608,8 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         return fail(MC3D_ERR_CONFIG, "DSMTESTFILTER must be 1 or 2");
     if (c.les_averaging < MC3D_AVG_NONE || c.les_averaging > MC3D_AVG_GLOBAL)
         return fail(MC3D_ERR_CONFIG, "unknown LESAVERAGING");
+    if (c.les_model == MC3D_MLPSGS && !(c.mlp_fallback_frac >= 0.0 && c.mlp_fallback_frac <= 1.0))
+        return fail(MC3D_ERR_CONFIG, "MLPFALLBACKFRAC must lie in [0, 1]");
     for (int f = 0; f < 6; f++)
         if (c.bc_kind[f] == MC3D_BC_INLET)
             return fail(MC3D_ERR_CONFIG, "INLET faces have no boundary treatment in the reference solver");

@@ -1,0 +1,62 @@
+"""Train the learned SGS closure from this solver's own HIT DNS and write the
+closure file the solver loads (``MLPClosure.load``).
+
+    python -m mpi_3dcompact_b200.train_sgs --dns 512 --factor 4 --seeds 0 \\
+        --snapshots 20,60,120,240,400 --steps 3000 --out mpi_3dcompact_b200/data/mlp_sgs_hit128.bin
+
+DNS: decaying HIT (PADE6, RK4, COMPACT10 alpha 0.49, Mt 0.3, k0 4) on dns^3
+points; box filter of `factor` gives the (dns/factor)^3 LES grid the closure
+is trained for (the grid scale enters its features). The snapshots span the
+decay (DNS step 400 is about LES step 100 at four times the time step), so
+that an LES of that length stays inside the training range. Adam, lr 1e-3,
+batch 65536.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--dns", type=int, default=512)
+    ap.add_argument("--factor", type=int, default=4)
+    ap.add_argument("--seeds", default="0")
+    ap.add_argument("--snapshots", default="20,60,120,240,400")
+    ap.add_argument("--mu-ref", type=float, default=2.5e-4)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+
+    import torch
+
+    from . import MLPClosure
+    from . import learned_sgs as L
+
+    t0 = time.time()
+    xs, ys = [], []
+    seeds = [int(s) for s in a.seeds.split(",")]
+    snaps = [int(s) for s in a.snapshots.split(",")]
+    for seed in seeds:
+        for q in L.dns_snapshots(n=a.dns, seeds=(seed,), steps=snaps, mu_ref=a.mu_ref):
+            x, y = L.training_pairs(q, a.dns, a.factor, mu_ref=a.mu_ref)
+            xs.append(x)
+            ys.append(y)
+            del q
+        torch.cuda.empty_cache()
+    x, y = torch.cat(xs), torch.cat(ys)
+    t1 = time.time()
+    mlp = MLPClosure(seed=0)
+    L.fit_normalization(mlp, x, y)
+    hist = L.train(mlp, x, y, steps=a.steps, batch=a.batch, lr=a.lr)
+    t2 = time.time()
+    mlp.save(a.out)
+    print(json.dumps({"samples": int(x.shape[0]), "loss_first": hist[0], "loss_last": hist[-1],
+                      "dns_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "out": a.out}))
+
+
+if __name__ == "__main__":
+    main()

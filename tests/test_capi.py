@@ -139,6 +139,16 @@ def test_ini_rejects_bad_values(tmp_path):
             m.Options.from_ini(_write(tmp_path, HIT_IN.replace(a, b)))
 
 
+def test_ini_mlp_closure_keys(tmp_path):
+    txt = HIT_IN.replace("LESMODEL = VREMAN", "LESMODEL = MLP")
+    c = m.Options.from_ini(_write(tmp_path, txt)).c
+    assert c.les_model == N.MLPSGS and c.mlp_fallback_frac == 1e-3
+    c = m.Options.from_ini(_write(tmp_path, txt.replace("[LES]", "[LES]\nMLPFALLBACKFRAC = 0.01"))).c
+    assert c.mlp_fallback_frac == 0.01
+    with pytest.raises(N.Mc3dError):
+        m.Options.from_ini(_write(tmp_path, txt.replace("[LES]", "[LES]\nMLPFALLBACKFRAC = 2")))
+
+
 def test_ini_lesmodel_none_alias(tmp_path):
     c = m.Options.from_ini(_write(tmp_path, HIT_IN.replace("LESMODEL = VREMAN", "LESMODEL = NONE"))).c
     assert c.les_model == N.NOMODEL

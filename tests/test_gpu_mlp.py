@@ -11,13 +11,18 @@ import math
 
 import numpy as np
 import pytest
-from scipy.special import erf
 
 import mpi_3dcompact_b200 as m
 
 pytestmark = pytest.mark.gpu
 
 OFF = dict(W1=0, B1=576, W2=640, B2=4736, W3=4800, B3=8896, W4=8960, B4=9088)
+K0, K1 = math.sqrt(2.0 / math.pi), 0.044715
+
+
+def gelu(z):
+    """GELU in its tanh form, as the closure uses it."""
+    return 0.5 * z * (1 + np.tanh(K0 * (z + K1 * z ** 3)))
 
 
 def _torch():
@@ -31,11 +36,11 @@ def np_forward(P, x, mean, std):
         return a @ P[w:w + nout * nin].reshape(nout, nin).T.astype(np.float64) + P[b:b + nout]
     a0 = (x - mean) / std
     z1 = lin(a0, OFF["W1"], OFF["B1"], 64, 9)
-    h1 = 0.5 * z1 * (1 + erf(z1 / math.sqrt(2)))
+    h1 = gelu(z1)
     z2 = lin(h1, OFF["W2"], OFF["B2"], 64, 64)
-    h2 = 0.5 * z2 * (1 + erf(z2 / math.sqrt(2)))
+    h2 = gelu(z2)
     z3 = lin(h2, OFF["W3"], OFF["B3"], 64, 64)
-    h3 = 0.5 * z3 * (1 + erf(z3 / math.sqrt(2)))
+    h3 = gelu(z3)
     out = lin(h3, OFF["W4"], OFF["B4"], 2, 64)
     return (a0, z1, h1, z2, h2, z3, h3), out
 
@@ -47,7 +52,8 @@ def np_grad(P, x, y, mean, std):
     G = np.zeros(P.shape, dtype=np.float64)
 
     def dgelu(z):
-        return 0.5 * (1 + erf(z / math.sqrt(2))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+        t = np.tanh(K0 * (z + K1 * z ** 3))
+        return 0.5 * (1 + t) + 0.5 * z * (1 - t * t) * K0 * (1 + 3 * K1 * z * z)
     d4 = 2 * (out - y) / n
     W4 = P[OFF["W4"]:OFF["W4"] + 128].reshape(2, 64).astype(np.float64)
     W3 = P[OFF["W3"]:OFF["W3"] + 4096].reshape(64, 64).astype(np.float64)
@@ -145,10 +151,10 @@ def test_training_reduces_loss_and_save_load(tmp_path):
     assert torch.equal(a, b)
 
 
-def _hit_les_solver(n, les, avg="GLOBAL", precision=m.FP32BULK):
+def _hit_les_solver(n, les, avg="GLOBAL", precision=m.FP32BULK, frac=1e-3):
     from mpi_3dcompact_b200.hit_ic import hit_initial_condition
     opt = m.Options(grid=n, fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=1e-3, les=les,
-                    les_avg=avg, precision=precision)
+                    les_avg=avg, precision=precision, mlp_fallback_frac=frac)
     s = m.CurvilinearCSolver(opt)
     s.set_box_metrics(2.0 * math.pi)
     s.set_initial_conditions(*hit_initial_condition(n, k0=4.0, seed=7, mt=0.3))
@@ -187,3 +193,11 @@ def test_training_pairs_and_les_with_fallback():
     s2.step(2)
     assert s2.mlp_fallbacks() == 8
     assert s.mlp_fallbacks() <= 12
+    # the same closure with a tolerance of every point: no fallback, the
+    # features are clamped to the range and the run stays finite
+    s3 = _hit_les_solver(16, "MLP", frac=1.0)
+    s3.set_mlp(mlp2)
+    s3.step(2)
+    assert s3.mlp_fallbacks() == 0
+    ke3, _ = s3.integrals()
+    assert math.isfinite(ke3) and 0 < ke3 < ke0
