@@ -110,6 +110,10 @@ typedef struct mc3d_config {
      * (LES.MLPFALLBACKFRAC, default 1e-3; 0 = any point). No counterpart in
      * the reference. */
     double mlp_fallback_frac;
+    /* BC.PERIODICDISP{X,Y,Z}_{X,Y,Z}: displacement of the X1 (Y1, Z1) face
+     * from the X0 (Y0, Z0) face, row = face pair, column = component; read
+     * for PERIODIC faces (src/Options.hpp:152-160), used by mc3d_solver_set_mesh */
+    double periodic_disp[3][3];
 } mc3d_config;
 
 /* ---- configuration ---- */
@@ -202,6 +206,16 @@ int mc3d_solver_set_metrics(mc3d_solver s, const double *const metrics[10]);
 /* The uniform periodic box x = L*xi (the HIT mesh,
  * tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156). */
 int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz);
+/* Metrics computed on the device, in FP64, from the mesh coordinates x, y, z
+ * (host, Nx*Ny*Nz each, x fastest): AbstractSingleBlockMesh::solveForJacobians
+ * (src/AbstractSingleBlockMesh.cpp:23-1308) with the solver's derivative
+ * schemes, TPB derivatives along periodic directions translated as
+ * handlePeriodicStuff does (:2019-2083, from cfg.periodic_disp), and with
+ * cfg.reference_quirks the two BW7 calls that pass their Nm2 ghost as Nm3
+ * (:273, :706). Replaces mc3d_solver_set_metrics. */
+int mc3d_solver_set_mesh(mc3d_solver s, const double *x, const double *y, const double *z);
+/* Copy the FP64 metrics J, J11..J33 the solver holds into 10 host arrays. */
+int mc3d_solver_get_metrics(mc3d_solver s, double *const metrics[10]);
 
 /* The learned closure a LESMODEL = MLP solver evaluates (kept by reference;
  * it must outlive the solver). */

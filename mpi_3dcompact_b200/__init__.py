@@ -184,7 +184,8 @@ class Options:
     def __init__(self, grid=(64, 64, 64), fd="PADE6", filter="COMPACT10", alphaF=0.45, mu_ref=1e-3, rk="RK4",
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
-                 dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3):
+                 dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3,
+                 periodic_disp=None):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -206,6 +207,10 @@ class Options:
         c.dsm_test_filter = int(dsm_test_filter)
         c.dsm_use_taukk = int(bool(dsm_use_taukk))
         c.mlp_fallback_frac = mlp_fallback_frac
+        # BC.PERIODICDISP{X,Y,Z}_{X,Y,Z} (row = face pair, column = component)
+        for d in range(3):
+            for e in range(3):
+                c.periodic_disp[d][e] = 0.0 if periodic_disp is None else float(periodic_disp[d][e])
         # BC kinds of the faces X0, X1, Y0, Y1, Z0, Z1 (names of src/Options.hpp:21-27);
         # default: PERIODIC on periodic directions, ADIABATIC_WALL otherwise
         kinds = bc_kind or [("PERIODIC" if bc[f // 2] == PERIODIC_SOLVE else "ADIABATIC_WALL") for f in range(6)]
@@ -326,6 +331,23 @@ class CurvilinearCSolver:
         self._met_keep = arrs
         p = (C.POINTER(C.c_double) * 10)(*[N.dptr(a) for a in arrs])
         N.check(N.host_lib().mc3d_solver_set_metrics(self._h, p))
+
+    def set_mesh(self, x, y, z):
+        """Metrics from the mesh coordinates (3 float64 arrays shaped (Nz, Ny,
+        Nx)), computed on the GPU as AbstractSingleBlockMesh::solveForJacobians
+        does (src/AbstractSingleBlockMesh.cpp:23-1308)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        for a in arrs:
+            if a.shape != self.shape:
+                raise ValueError(f"mesh arrays must be shaped {self.shape}")
+        N.check(N.host_lib().mc3d_solver_set_mesh(self._h, *[N.dptr(a) for a in arrs]))
+
+    def metrics(self):
+        """The FP64 metrics J, J11..J33 the solver holds (10 arrays (Nz, Ny, Nx))."""
+        out = [np.empty(self.shape) for _ in range(10)]
+        p = (C.POINTER(C.c_double) * 10)(*[N.dptr(a) for a in out])
+        N.check(N.host_lib().mc3d_solver_get_metrics(self._h, p))
+        return out
 
     def set_mlp(self, mlp: MLPClosure):
         """The learned closure of a LESMODEL = MLP solver (kept alive by the solver object)."""

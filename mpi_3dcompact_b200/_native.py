@@ -46,7 +46,8 @@ class Config(C.Structure):
                 ("reference_quirks", C.c_int), ("dsm_test_filter", C.c_int), ("dsm_use_taukk", C.c_int),
                 ("sponge_kind", C.c_int), ("sponge_strength", C.c_double), ("sponge_rect_perc", C.c_double * 6),
                 ("sponge_cyl_orient", C.c_int), ("sponge_cyl_axis", C.c_double * 3), ("sponge_rmin", C.c_double),
-                ("wall_velocity", (C.c_double * 2) * 6), ("mlp_fallback_frac", C.c_double)]
+                ("wall_velocity", (C.c_double * 2) * 6), ("mlp_fallback_frac", C.c_double),
+                ("periodic_disp", (C.c_double * 3) * 3)]
 
 
 _lib = None
@@ -73,6 +74,8 @@ def host_lib():
             "mc3d_solver_destroy": (ip, [vp]),
             "mc3d_solver_set_metrics": (ip, [vp, C.POINTER(C.POINTER(dp))]),
             "mc3d_solver_set_box_metrics": (ip, [vp, dp, dp, dp]),
+            "mc3d_solver_set_mesh": (ip, [vp, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
+            "mc3d_solver_get_metrics": (ip, [vp, C.POINTER(C.POINTER(dp))]),
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),
             "mc3d_solver_set_initial_device": (ip, [vp] + [vp] * 5),
             "mc3d_solver_step": (ip, [vp, ip]),

@@ -75,6 +75,8 @@ int mc3d_config_default(mc3d_config *c) {
     c->sponge_rmin = 0.0;
     for (int f = 0; f < 6; f++) c->wall_velocity[f][0] = c->wall_velocity[f][1] = 0.0;
     c->mlp_fallback_frac = 1e-3;
+    for (int d = 0; d < 3; d++)
+        for (int e = 0; e < 3; e++) c->periodic_disp[d][e] = 0.0;
     return MC3D_OK;
 }
 
@@ -243,6 +245,7 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
                 for (int e = 0; e < 3; e++) {
                     std::string k = std::string("BC.PERIODICDISP") + ax[d] + "_" + ax[e];
                     if (!ini.has(k)) throw CfgError{k + " not specified, NEEDS TO BE SPECIFED"};
+                    c->periodic_disp[d][e] = parse_double(k.c_str() + 3, ini.get(k));
                 }
             bool ip0 = p0 || k0 == MC3D_BC_INTERNALLY_PERIODIC, ip1 = p1 || k1 == MC3D_BC_INTERNALLY_PERIODIC;
             if (c->bc_type[d] == MC3D_PERIODIC_SOLVE) {

@@ -330,4 +330,29 @@ int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scrat
 int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cudaStream_t st);
 int launch_nonfinite_check(const Grid3 &g, const double *const q[5], int *flag, cudaStream_t st);
 
+// ---- grid metrics (metrics.cu) -----------------------------------------------
+// RHS of the reference's TPB derivative along `dir` (periodic lines whose
+// stencil reads ghost values): row n = (sum_k st[k] F[n+k-H]) / dh with F the
+// line values inside [0, N) and, outside, sum_t (X_t -+ T[t]) W_t at the wrapped
+// index (N-m before the start, m-1 after the end; W_t == nullptr: 1). CD2
+// (explicit_cd2) uses the reference's mirrored end rows. nm3_from_nm2: the
+// Nm3 ghost is the Nm2 one.
+struct TpbArgs {
+    int N, H, nterms, explicit_cd2, nm3_from_nm2;
+    double st[7];
+    double dh;
+    double T[3];
+    const double *X[3];
+    const double *W[3];
+};
+struct MetOut9 {
+    double *p[9];
+};
+int launch_tpb_rhs(const Grid3 &g, int dir, const double *f, const TpbArgs &a, double *rhs, cudaStream_t st);
+int launch_metric_mul(long long n, const double *a, const double *b, double *o, cudaStream_t st);
+int launch_metric_sub(long long n, const double *a, const double *b, double *o, cudaStream_t st);
+int launch_metric_dot3(long long n, const double *const xyz[3], const double *const abc[3], double *o,
+                       cudaStream_t st);
+int launch_metric_finish(long long n, const double *const jdet[3], double *const jij[9], double *J, cudaStream_t st);
+
 }  // namespace mc3d

@@ -784,6 +784,225 @@ int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz) 
     return upload_metrics(s, nullptr, c);
 }
 
+namespace mc3d {
+
+// Translation of each PERIODIC_SOLVE direction (handlePeriodicStuff,
+// src/AbstractSingleBlockMesh.cpp:2019-2083). The xi1 branch tests the Y faces
+// (:2034), so x takes PERIODICDISPX only when the Y faces are PERIODIC;
+// INTERNALLY_PERIODIC faces translate by zero; the reference leaves any other
+// combination unset, zero here.
+static void periodic_translations(const mc3d_config &c, double T[3][3]) {
+    for (int d = 0; d < 3; d++) {
+        for (int e = 0; e < 3; e++) T[d][e] = 0.0;
+        if (c.bc_type[d] != MC3D_PERIODIC_SOLVE) continue;
+        const int face = d == 0 ? 2 : 2 * d;
+        if (c.bc_kind[face] == MC3D_BC_PERIODIC && c.bc_kind[face + 1] == MC3D_BC_PERIODIC)
+            for (int e = 0; e < 3; e++) T[d][e] = c.periodic_disp[d][e];
+    }
+}
+
+// Operators of one metric direction: the derivative, and for periodic
+// directions the same left-hand side with an identity RHS stencil (the solve
+// of a TPB right-hand side built by tpb_rhs_kernel).
+struct MetricDir {
+    LineOpBuf deriv, solve;
+    bool periodic = false, cd2 = false;
+    int H = 0;
+    double st[7] = {0};
+    double dh = 1.0;
+};
+
+// One metric derivative along d, in -> out. On a periodic direction whose
+// translation or ghost quirk changes the ghosts, the reference's TPB
+// derivative: the RHS with ghosts sum_t (X_t -+ T_t) W_t at the wrapped indices
+// (tmp), then the periodic solve; otherwise the solver's plain derivative.
+static int metric_deriv(mc3d_solver s, int d, const MetricDir &md, const double *in, double *out, double *tmp,
+                        int nterms, const double *T, const double *const *X, const double *const *W, bool nm3_quirk) {
+    bool tpb = md.periodic && nm3_quirk;
+    for (int t = 0; t < nterms && md.periodic; t++) tpb = tpb || T[t] != 0.0;
+    SweepBatch<double> b{};
+    b.nf = 1;
+    RhsFinalArgs<double> rf{};
+    if (!tpb) {
+        b.in[0] = in;
+        b.out[0] = out;
+        return launch_sweep<double>(d, s->g, md.deriv.f64, b, EPI_STORE, rf, s->cfg.bc_type, false, s->stream);
+    }
+    TpbArgs a{};
+    a.N = d == 0 ? s->g.Nx : (d == 1 ? s->g.Ny : s->g.Nz);
+    a.H = md.H;
+    a.nterms = nterms;
+    a.explicit_cd2 = md.cd2 ? 1 : 0;
+    a.nm3_from_nm2 = nm3_quirk ? 1 : 0;
+    for (int k = 0; k < 7; k++) a.st[k] = md.st[k];
+    a.dh = md.dh;
+    for (int t = 0; t < nterms; t++) {
+        a.T[t] = T[t];
+        a.X[t] = X[t];
+        a.W[t] = W ? W[t] : nullptr;
+    }
+    if (md.cd2) return launch_tpb_rhs(s->g, d, in, a, out, s->stream);   // explicit: the RHS is the derivative
+    int rc = launch_tpb_rhs(s->g, d, in, a, tmp, s->stream);
+    if (rc) return rc;
+    b.in[0] = tmp;
+    b.out[0] = out;
+    return launch_sweep<double>(d, s->g, md.solve.f64, b, EPI_STORE, rf, s->cfg.bc_type, false, s->stream);
+}
+
+// solveForJacobians (src/AbstractSingleBlockMesh.cpp:23-1308) on the device.
+static int compute_metrics(mc3d_solver s, const double *hx, const double *hy, const double *hz,
+                           std::vector<std::vector<double>> &host) {
+    const long long n = s->g.n();
+    const size_t bytes = (size_t)n * sizeof(double);
+    const int Ns[3] = {s->g.Nx, s->g.Ny, s->g.Nz};
+    std::vector<void *> mine;
+    MetricDir md[3];
+    int rc = MC3D_OK;
+    auto dalloc = [&](size_t b) -> double * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, b) != cudaSuccess) return nullptr;
+        mine.push_back(p);
+        return (double *)p;
+    };
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(s->stream);
+        for (void *p : mine) cudaFree(p);
+        for (int d = 0; d < 3; d++) {
+            free_line_op(md[d].deriv);
+            free_line_op(md[d].solve);
+        }
+    };
+    // x, y, z; xE1j = dx/dxi_j, xE2j = dy/dxi_j; the nine cofactors; temporaries
+    double *X[3], *xE1[3], *xE2[3], *Jr[9], *t0, *t1, *t2, *tr, *Jf;
+    double **slots[] = {&X[0], &X[1], &X[2], &xE1[0], &xE1[1], &xE1[2], &xE2[0], &xE2[1], &xE2[2], &Jr[0], &Jr[1],
+                        &Jr[2], &Jr[3], &Jr[4], &Jr[5], &Jr[6], &Jr[7], &Jr[8], &t0, &t1, &t2, &tr, &Jf};
+    for (double **sl : slots)
+        if (!(*sl = dalloc(bytes))) {
+            cleanup();
+            return fail(MC3D_ERR_OOM, "device allocation for the metric computation failed");
+        }
+    const double *hs[3] = {hx, hy, hz};
+    for (int c = 0; c < 3; c++)
+        if (cudaMemcpyAsync(X[c], hs[c], bytes, cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+            cleanup();
+            return fail(MC3D_ERR_CUDA, "mesh upload failed");
+        }
+    try {
+        for (int d = 0; d < 3 && !rc; d++) {
+            LineOpHost h = build_deriv_op(s->cfg.fd_type[d], s->cfg.bc_type[d], Ns[d], s->dxi[d]);
+            if ((rc = upload_line_op(h, MC3D_FP64, md[d].deriv))) break;
+            md[d].periodic = s->cfg.bc_type[d] == MC3D_PERIODIC_SOLVE;
+            md[d].cd2 = s->cfg.fd_type[d] == MC3D_CD2;
+            md[d].H = h.H;
+            for (int k = 0; k <= 2 * h.H && k < 7; k++) md[d].st[k] = h.st[k];
+            md[d].dh = s->dxi[d];
+            if (md[d].periodic && !md[d].cd2) {
+                LineOpHost sv = h;
+                for (double &v : sv.st) v = 0.0;
+                sv.st[sv.H] = 1.0;
+                sv.deriv = false;
+                sv.inv_dh = 1.0;
+                rc = upload_line_op(sv, MC3D_FP64, md[d].solve);
+            }
+        }
+    } catch (const std::exception &e) {
+        cleanup();
+        return fail(MC3D_ERR_CONFIG, e.what());
+    }
+    if (rc) {
+        cleanup();
+        return fail(rc, "metric operator setup failed");
+    }
+    double T[3][3];
+    periodic_translations(s->cfg, T);
+    const bool q = s->cfg.reference_quirks != 0;
+    auto penta = [&](int d) { return s->cfg.fd_type[d] == MC3D_PENTA10; };
+#define MC3D_MTRY(x)      \
+    if ((rc = (x))) {     \
+        cleanup();        \
+        return rc;        \
+    }
+    // xE1j, xE2j (:39-303); d y / d xi3 of a BW7 scheme passes Nm2 as Nm3 (:273)
+    for (int j = 0; j < 3; j++) {
+        const double *xc[1] = {X[0]}, *yc[1] = {X[1]};
+        MC3D_MTRY(metric_deriv(s, j, md[j], X[0], xE1[j], tr, 1, &T[j][0], xc, nullptr, false));
+        MC3D_MTRY(metric_deriv(s, j, md[j], X[1], xE2[j], tr, 1, &T[j][1], yc, nullptr, q && j == 2 && penta(2)));
+    }
+    // cofactors from the off-diagonal derivatives of Va_j = xE1j y, Vb_j = xE1j z,
+    // Vc_j = xE2j z (:320-1023): J_ab = dV[j1]/dxi[k1] - dV[j2]/dxi[k2]
+    static const int tab[9][5] = {{2, 1, 2, 2, 1}, {1, 2, 1, 1, 2}, {0, 1, 2, 2, 1},
+                                  {2, 2, 0, 0, 2}, {1, 0, 2, 2, 0}, {0, 2, 0, 0, 2},
+                                  {2, 0, 1, 1, 0}, {1, 1, 0, 0, 1}, {0, 0, 1, 1, 0}};
+    auto dV = [&](int fam, int j, int k, double *out) -> int {
+        const double *w = fam == 2 ? xE2[j] : xE1[j];
+        const int c = fam == 0 ? 1 : 2;
+        int r = launch_metric_mul(n, w, X[c], t0, s->stream);
+        if (r) return r;
+        const double *xc[1] = {X[c]}, *wc[1] = {w};
+        // d Vc3 / d xi1 of a BW7 scheme passes Nm2 as Nm3 (:706)
+        return metric_deriv(s, k, md[k], t0, out, tr, 1, &T[k][c], xc, wc,
+                            q && fam == 2 && j == 2 && k == 0 && penta(0));
+    };
+    for (int ab = 0; ab < 9; ab++) {
+        MC3D_MTRY(dV(tab[ab][0], tab[ab][1], tab[ab][2], t1));
+        MC3D_MTRY(dV(tab[ab][0], tab[ab][3], tab[ab][4], t2));
+        MC3D_MTRY(launch_metric_sub(n, t1, t2, Jr[ab], s->stream));
+    }
+    // determinant: (1/3) sum_i d(x J_i1 + y J_i2 + z J_i3)/dxi_i (:1058-1296)
+    double *jd[3] = {xE1[0], xE1[1], xE1[2]};
+    for (int i = 0; i < 3; i++) {
+        const double *xyz[3] = {X[0], X[1], X[2]};
+        const double *abc[3] = {Jr[3 * i], Jr[3 * i + 1], Jr[3 * i + 2]};
+        MC3D_MTRY(launch_metric_dot3(n, xyz, abc, t0, s->stream));
+        MC3D_MTRY(metric_deriv(s, i, md[i], t0, jd[i], tr, 3, T[i], xyz, abc, false));
+    }
+    const double *jdc[3] = {jd[0], jd[1], jd[2]};
+    MC3D_MTRY(launch_metric_finish(n, jdc, Jr, Jf, s->stream));
+#undef MC3D_MTRY
+    host.assign(10, std::vector<double>((size_t)n));
+    const double *src[10] = {Jf, Jr[0], Jr[1], Jr[2], Jr[3], Jr[4], Jr[5], Jr[6], Jr[7], Jr[8]};
+    for (int c = 0; c < 10; c++)
+        if (cudaMemcpyAsync(host[c].data(), src[c], bytes, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess) {
+            cleanup();
+            return fail(MC3D_ERR_CUDA, "metric download failed");
+        }
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    cleanup();
+    if (e != cudaSuccess) return fail(MC3D_ERR_CUDA, cudaGetErrorString(e));
+    return MC3D_OK;
+}
+
+}  // namespace mc3d
+
+int mc3d_solver_set_mesh(mc3d_solver s, const double *x, const double *y, const double *z) {
+    if (!s || !x || !y || !z) return fail(MC3D_ERR_ARG, "null argument");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    std::vector<std::vector<double>> h;
+    int rc = mc3d::compute_metrics(s, x, y, z, h);
+    if (rc) return rc;
+    const double *p[10];
+    for (int c = 0; c < 10; c++) p[c] = h[c].data();
+    return upload_metrics(s, p, nullptr);
+}
+
+int mc3d_solver_get_metrics(mc3d_solver s, double *const metrics[10]) {
+    if (!s || !metrics) return fail(MC3D_ERR_ARG, "null argument");
+    for (int c = 0; c < 10; c++)
+        if (!metrics[c]) return fail(MC3D_ERR_ARG, "null metric field");
+    if (!s->have_metrics) return fail(MC3D_ERR_CONFIG, "no metrics set");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.n();
+    for (int c = 0; c < 10; c++) {
+        if (s->const_met) {
+            for (size_t i = 0; i < n; i++) metrics[c][i] = s->met_c[c];
+        } else {
+            MC3D_CUDA_TRY(cudaMemcpyAsync(metrics[c], s->met64[c], n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        }
+    }
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
+}
+
 static int set_initial_impl(mc3d_solver s, const double *rho, const double *U, const double *V, const double *W,
                             const double *p, bool device) {
     if (!s || !rho || !U || !V || !W || !p) return fail(MC3D_ERR_ARG, "null argument");

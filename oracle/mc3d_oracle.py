@@ -564,6 +564,9 @@ class Config:
     # periodic translation of each periodic direction's faces along its own axis
     # (BC.PERIODICDISP*), for the reference runs; None: the 2*pi HIT box
     periodic_box: tuple = None
+    # full BC.PERIODICDISP{X,Y,Z}_{X,Y,Z} table (row = face pair, column =
+    # component); None: periodic_box on the diagonal
+    periodic_disp: tuple = None
 
     def kinds(self):
         if self.bc_kind is not None:
@@ -1105,6 +1108,168 @@ def ogrid_mesh(N, r0=0.5, ratio=1.08, span=2.0):
     zz = span * np.arange(Nz) / Nz
     Z, Rr, TH = np.meshgrid(zz, r, th, indexing="ij")
     return Rr * np.cos(TH), Rr * np.sin(TH), Z
+
+
+# --------------------------------------------------------------------------
+# Grid metrics (src/AbstractSingleBlockMesh.cpp:23-1308, :2019-2083)
+# --------------------------------------------------------------------------
+def periodic_disp_table(cfg: Config):
+    """BC.PERIODICDISP* as the reference runs set them: cfg.periodic_disp, else
+    periodic_box (or 2*pi) on the diagonal of each PERIODIC face pair."""
+    kinds = cfg.kinds()
+    t = np.zeros((3, 3))
+    for d in range(3):
+        if kinds[2 * d] == "PERIODIC":
+            if cfg.periodic_disp is not None:
+                t[d] = cfg.periodic_disp[d]
+            else:
+                t[d, d] = (cfg.periodic_box[d] if cfg.periodic_box is not None else 2.0 * math.pi)
+    return t
+
+
+def periodic_translations(cfg: Config):
+    """handlePeriodicStuff (src/AbstractSingleBlockMesh.cpp:2019-2083): the
+    translation of each PERIODIC_SOLVE direction. The xi1 test reads the Y
+    faces (:2034), so an x-periodic block takes PERIODICDISPX only when its Y
+    faces are PERIODIC; INTERNALLY_PERIODIC faces translate by zero; any other
+    combination leaves the translation unset in the reference (zero here)."""
+    kinds = cfg.kinds()
+    disp = periodic_disp_table(cfg)
+    T = np.zeros((3, 3))
+    for d in range(3):
+        if cfg.bc[d] != PERIODIC:
+            continue
+        test = 2 if d == 0 else 2 * d       # the xi1 branch looks at Y0/Y1
+        if kinds[test] == "PERIODIC" and kinds[test + 1] == "PERIODIC":
+            T[d] = disp[d]
+        # INTERNALLY_PERIODIC and the unset case: zero
+    return T
+
+
+def _tpb_lines(phi, gm, gp, scheme, dh):
+    """calc1stDeriv_TPB of periodic lines (src/Pade6.cpp:220-249,359-363,
+    src/Penta10.cpp:175-207,263-269, src/CD2.cpp:144-150): the RHS stencil reads
+    the ghost values gm[..., m-1] = Nm_m (before index 0) and gp[..., m-1] =
+    Np_m (after index N-1) instead of the wrapped line values."""
+    n = phi.shape[-1]
+    if scheme == "CD2":
+        out = cd2_deriv_lines(phi, dh, PERIODIC)
+        a, c = -0.5, 0.5
+        out[..., 0] = (a * gm[..., 0] + c * phi[..., 1]) / dh
+        out[..., n - 1] = (a * phi[..., n - 2] + c * gp[..., 0]) / dh
+        return out
+    if scheme == "PADE6":
+        a_1d, b_1d = 14.0 / 9.0, 1.0 / 9.0
+        st = [-b_1d / 4.0, -a_1d / 2.0, 0.0, a_1d / 2.0, b_1d / 4.0]
+        H = 2
+    else:
+        a, b, c = 17.0 / 12.0, 101.0 / 150.0, 1.0 / 100.0
+        st = [-c / 6.0, -b / 4.0, -a / 2.0, 0.0, a / 2.0, b / 4.0, c / 6.0]
+        H = 3
+    ext = np.concatenate([gm[..., ::-1], phi, gp], axis=-1)     # [Nm_H..Nm_1, phi, Np_1..Np_H]
+    rhs = np.zeros(phi.shape)
+    for k, s in enumerate(st):
+        if s != 0.0:
+            rhs = rhs + s * ext[..., k:k + n]
+    rhs = rhs / dh
+    if scheme == "PADE6":
+        lo, dg, up = pade6_lhs(n, PERIODIC)
+        return cyclic(lo, dg, up, 1.0 / 3.0, 1.0 / 3.0, rhs)
+    lo2, lo, dg, up, up2 = penta10_lhs(n, PERIODIC)
+    beta, alpha = 1.0 / 20.0, 1.0 / 2.0
+    return cyclic_penta(lo2, lo, dg, up, up2, rhs, [beta, alpha, beta, beta, alpha, beta])
+
+
+def _deriv_tpb(cfg, dxi, f, d, ghost):
+    """One metric derivative along d: TPB with ghost(idx, sign) giving the
+    translated line values at wrapped indices (sign -1 before the start, +1
+    after the end) on PERIODIC_SOLVE directions, the plain derivative else."""
+    scheme = cfg.fd[d]
+    if cfg.bc[d] != PERIODIC:
+        return deriv(f, d, scheme, cfg.bc[d], dxi[d])
+    H = {"PADE6": 2, "PENTA10": 3, "CD2": 2}[scheme]
+    n = f.shape[_AXIS[d]]
+    lines = _to_lines(f, d)
+    gm = np.stack([ghost(n - m, -1) for m in range(1, H + 1)], axis=-1)   # Nm_1..Nm_H
+    gp = np.stack([ghost(m - 1, +1) for m in range(1, H + 1)], axis=-1)   # Np_1..Np_H
+    return np.ascontiguousarray(_from_lines(_tpb_lines(lines, gm, gp, scheme, dxi[d]), d))
+
+
+def solve_for_jacobians(cfg: Config, x, y, z, quirks=True):
+    """AbstractSingleBlockMesh::solveForJacobians (src/AbstractSingleBlockMesh.cpp:23-1308):
+    xE_ij = d(x, y)/dxi_j (:39-303), V products (:320-333), their off-diagonal
+    derivatives (:335-1008), cofactors J_ij (:1010-1023), determinant from
+    (1/3) sum_i d(x . J_i)/dxi_i (:1058-1296), J = 1/det and J_ij *= J
+    (:1298-1308). Periodic directions use the TPB derivatives with the ghost
+    values translated by handlePeriodicStuff. With `quirks`, two BW7 calls
+    pass their Nm2 ghost as the Nm3 ghost: d y/d xi3 (:273) and d Vc3/d xi1
+    (:706). Returns [J, J11, ..., J33]."""
+    dxi = [1.0 / n if b == PERIODIC else 1.0 / (n - 1.0) for n, b in zip(cfg.N, cfg.bc)]
+    T = periodic_translations(cfg)
+    X = [x, y, z]
+
+    def line_at(a, d, idx):
+        return np.take(_to_lines(a, d), idx, axis=-1)
+
+    def coord_ghost(c, d):
+        return lambda idx, sg: line_at(X[c], d, idx) + sg * T[d, c]
+
+    def deriv_of(f, d, ghost):
+        return _deriv_tpb(cfg, dxi, f, d, ghost)
+
+    # xE1j = dx/dxi_j, xE2j = dy/dxi_j
+    def nm3_as_nm2(g, d):
+        # the Nm3 ghost (index N-3, before the start) replaced by the Nm2 one
+        n = x.shape[_AXIS[d]]
+        return lambda idx, sg: g(n - 2, sg) if (sg < 0 and idx == n - 3) else g(idx, sg)
+
+    xE1 = [deriv_of(x, j, coord_ghost(0, j)) for j in range(3)]
+    xE2 = []
+    for j in range(3):
+        g = coord_ghost(1, j)
+        if quirks and j == 2 and cfg.fd[2] == "PENTA10":
+            g = nm3_as_nm2(g, 2)
+        xE2.append(deriv_of(y, j, g))
+
+    def vprod(w, c, j):
+        # V = w_j * X_c with ghosts (X_c +- T_c) * w_j
+        f = w[j] * X[c]
+
+        def ghost_for(k):
+            return lambda idx, sg: (line_at(X[c], k, idx) + sg * T[k, c]) * line_at(w[j], k, idx)
+        return f, ghost_for
+
+    Va = [vprod(xE1, 1, j) for j in range(3)]   # xE1j * y
+    Vb = [vprod(xE1, 2, j) for j in range(3)]   # xE1j * z
+    Vc = [vprod(xE2, 2, j) for j in range(3)]   # xE2j * z
+
+    def dV(V, j, k):
+        f, gf = V[j]
+        g = gf(k)
+        if quirks and V is Vc and j == 2 and k == 0 and cfg.fd[0] == "PENTA10":
+            g = nm3_as_nm2(g, 0)
+        return deriv_of(f, k, g)
+
+    # 0-based: dV?[j][k] = d V?_j / d xi_k
+    J11 = dV(Vc, 1, 2) - dV(Vc, 2, 1)
+    J12 = dV(Vb, 2, 1) - dV(Vb, 1, 2)
+    J13 = dV(Va, 1, 2) - dV(Va, 2, 1)
+    J21 = dV(Vc, 2, 0) - dV(Vc, 0, 2)
+    J22 = dV(Vb, 0, 2) - dV(Vb, 2, 0)
+    J23 = dV(Va, 2, 0) - dV(Va, 0, 2)
+    J31 = dV(Vc, 0, 1) - dV(Vc, 1, 0)
+    J32 = dV(Vb, 1, 0) - dV(Vb, 0, 1)
+    J33 = dV(Va, 0, 1) - dV(Va, 1, 0)
+    Jr = [[J11, J12, J13], [J21, J22, J23], [J31, J32, J33]]
+    jd = []
+    for i in range(3):
+        pre = x * Jr[i][0] + y * Jr[i][1] + z * Jr[i][2]
+
+        def ghost(idx, sg, i=i):
+            return sum((line_at(X[c], i, idx) + sg * T[i, c]) * line_at(Jr[i][c], i, idx) for c in range(3))
+        jd.append(deriv_of(pre, i, ghost))
+    J = 1.0 / ((1.0 / 3.0) * (jd[0] + jd[1] + jd[2]))
+    return [J] + [J * Jr[a][b] for a in range(3) for b in range(3)]
 
 
 def cube_metrics(N, L=2.0 * math.pi):

@@ -65,8 +65,10 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
         if kinds[2 * ax] == "PERIODIC":
             L = getattr(cfg, "periodic_box", None)
             b = L[ax] if L is not None else box
-            for c in "XYZ":
-                lines.append(f"PERIODICDISP{name}_{c} = {(b if c == name else 0.0)!r}")
+            full = getattr(cfg, "periodic_disp", None)
+            for ci, c in enumerate("XYZ"):
+                v = full[ax][ci] if full is not None else (b if c == name else 0.0)
+                lines.append(f"PERIODICDISP{name}_{c} = {float(v)!r}")
     sp = getattr(cfg, "sponge", None)
     if "SPONGE" in kinds and sp:
         lines += ["[SPONGE]", f"KIND = {sp.get('kind', 'RECTILINEAR')}", f"STRENGTH = {sp.get('strength', 1.0)!r}"]

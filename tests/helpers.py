@@ -17,6 +17,10 @@ def golden_steps():
     return np.load(os.path.join(HERE, "golden", "steps.npz"))
 
 
+def golden_metrics():
+    return np.load(os.path.join(HERE, "golden", "metrics.npz"))
+
+
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 

@@ -110,6 +110,8 @@ def test_ini_parses_hit_case(tmp_path):
     assert c.les_model == N.VREMAN and c.les_averaging == N.AVG_NONE
     assert c.mu_ref == 0.00033 and c.max_time_step == 200 and c.filter_step == 1
     assert c.precision == N.FP32BULK and c.reference_quirks == 1
+    disp = [[c.periodic_disp[d][e] for e in range(3)] for d in range(3)]
+    assert disp == [[6.2831853, 0.0, 0.0], [0.0, 6.2831853, 0.0], [0.0, 0.0, 6.2831853]]
 
 
 def test_ini_defaults(tmp_path):

@@ -85,6 +85,36 @@ def test_cube_metrics_match_reference_metrics():
         assert np.max(np.abs(a - b)) < 1e-13
 
 
+@pytest.mark.parametrize("name", list(G.METRIC_CASES))
+def test_oracle_metrics_match_reference_fixtures(name):
+    """solveForJacobians restated (TPB ghosts, translations, both BW7 ghost
+    quirks) against the reference's own metrics of the same mesh: the
+    restatement follows its arithmetic order, so it is bit-identical except for
+    the sign of underflowed off-diagonal terms."""
+    cfg, coords = G.metric_case(name)
+    got = O.solve_for_jacobians(cfg, *coords)
+    gold = H.golden_metrics()
+    for c in range(10):
+        ref = gold[f"{name}_met{c}"]
+        assert np.abs(got[c] - ref).max() <= 1e-300 + 1e-15 * np.abs(ref).max(), (name, c)
+
+
+def test_oracle_metrics_quirks_matter():
+    """The BW7 ghost quirks change the PENTA10 metrics (so the fixtures pin them)."""
+    cfg, coords = G.metric_case("wavy_penta10")
+    a = O.solve_for_jacobians(cfg, *coords, quirks=True)
+    b = O.solve_for_jacobians(cfg, *coords, quirks=False)
+    assert max(H.rel_max(x, y) for x, y in zip(a, b)) > 1e-6
+
+
+def test_oracle_metrics_of_the_cube_are_analytic():
+    cfg = O.Config(N=(12, 13, 14))
+    xi = [np.arange(n) / n for n in cfg.N]
+    z, y, x = np.meshgrid(2 * math.pi * xi[2], 2 * math.pi * xi[1], 2 * math.pi * xi[0], indexing="ij")
+    for a, b in zip(O.solve_for_jacobians(cfg, x, y, z), O.cube_metrics(cfg.N)):
+        assert np.abs(a - b).max() < 1e-13
+
+
 def test_oracle_live_reference_run():
     """Live check against the reference binary on a fresh configuration."""
     if not R.available():
