@@ -114,6 +114,14 @@ typedef struct mc3d_config {
      * from the X0 (Y0, Z0) face, row = face pair, column = component; read
      * for PERIODIC faces (src/Options.hpp:152-160), used by mc3d_solver_set_mesh */
     double periodic_disp[3][3];
+    int dump_step;           /* TIMESTEPPING.DUMPSTEP (default 1000, src/Options.hpp:237) */
+    /* [RESTART] (src/Options.hpp:186-193, :365-391): FROMRESTART,
+     * ONLYGRIDFROMRESTART, FILENAME; SPONGEAVGFROMRESTART, SPONGEAVGFILENAME.
+     * With either restart flag DOMAIN.N* come from the file's header
+     * (src/MPI_3DCompact.cpp:80-110); mc3d_solver_start applies them. */
+    int from_restart, only_grid_from_restart, sponge_avg_from_restart;
+    char restart_file[512];
+    char sponge_avg_file[512];
 } mc3d_config;
 
 /* ---- configuration ---- */
@@ -254,6 +262,47 @@ int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *
 int mc3d_solver_copy_conserved_device(mc3d_solver s, double *const dst[5]);
 /* Device pointers (FP64) of the five conserved fields. */
 int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]);
+
+/* ---- checkpoint files in the reference's formats ---- */
+/* SolutionDump (CurvilinearCSolver::dumpSolution, src/CurvilinearCSolver_Core.cpp:1333-1405):
+ * 5 FP64 header values (time step, time, Nx, Ny, Nz), then x, y, z, rho,
+ * rhoU, rhoV, rhoW, rhoE, Nx*Ny*Nz FP64 values each, x fastest. */
+int mc3d_dump_read_header(const char *path, int *time_step, double *time, int *Nx, int *Ny, int *Nz);
+/* fields[0..7] = x, y, z, rho, rhoU, rhoV, rhoW, rhoE (NULL entries are
+ * skipped); n = Nx*Ny*Nz must match the header. */
+int mc3d_dump_read_fields(const char *path, long long n, double *const fields[8]);
+int mc3d_dump_write(const char *path, int time_step, double time, int Nx, int Ny, int Nz,
+                    const double *const fields[8]);
+/* The solver's conserved state, time step and time as a SolutionDump. path
+ * NULL: "SolutionDump.<time step>" in the working directory. x, y, z NULL:
+ * the mesh of mc3d_solver_set_mesh / mc3d_solver_restart, or the box of
+ * mc3d_solver_set_box_metrics (x = L*xi). */
+int mc3d_solver_dump(mc3d_solver s, const char *path, const double *x, const double *y, const double *z);
+/* Restart from a SolutionDump (src/MPI_3DCompact.cpp:80-271): metrics from
+ * the file's mesh (as mc3d_solver_set_mesh); unless grid_only
+ * (RESTART.ONLYGRIDFROMRESTART) also the conserved state, turned into
+ * primitives by IdealGas::solveU/solvep (src/IdealGas.hpp:58-64) and set as
+ * the initial condition, with the file's time step and time (so the first
+ * step after it again leaves time unchanged, Core.cpp:221-228; the filter
+ * direction rotation and the LSLDDRK4 halves start over). */
+int mc3d_solver_restart(mc3d_solver s, const char *path, int grid_only);
+/* SpongeAvgDump (SpongeBC::dumpSpongeAvg, src/SpongeBC.cpp:363-424): the five
+ * sponge target fields, no header; path NULL: "SpongeAvgDump.<time step>". */
+int mc3d_solver_dump_sponge_avg(mc3d_solver s, const char *path);
+/* readSpongeAvgFromRestart (src/SpongeBC.cpp:426-480): the sponge target
+ * from such a file (after the initial condition, which sets it otherwise). */
+int mc3d_solver_read_sponge_avg(mc3d_solver s, const char *path);
+/* The reference's driver loop for a configuration (src/MPI_3DCompact.cpp
+ * with AbstractRK::executeSolverLoop and CurvilinearCSolver::postStep,
+ * src/CurvilinearCSolver.hpp:355-375): when cfg.from_restart /
+ * only_grid_from_restart / sponge_avg_from_restart are set, mc3d_solver_start
+ * reads those files first; mc3d_solver_run then steps until checkEnd
+ * (time >= MAXTIME, time step >= MAXTIMESTEP, or a file "killsolver" in dir,
+ * removed when found, src/CurvilinearCSolver_Core.cpp:1750-1824), writing
+ * SolutionDump.<step> (and SpongeAvgDump.<step> with sponges) into dir (NULL:
+ * working directory) every DUMPSTEP steps and at the end. */
+int mc3d_solver_start(mc3d_solver s);
+int mc3d_solver_run(mc3d_solver s, const char *dir);
 
 /* Time-step counter, time, last dt and total RK stages run (synchronises). */
 int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, long long *stages);

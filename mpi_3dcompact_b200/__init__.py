@@ -170,6 +170,29 @@ _BCKIND = {"PERIODIC": 0, "INTERNALLY_PERIODIC": 1, "SPONGE": 2, "ADIABATIC_WALL
            "MOVING_ADIABATIC_WALL": 5, "INLET": 6}
 
 
+def read_dump(path):
+    """A SolutionDump file: (header dict, [x, y, z, rho, rhoU, rhoV, rhoW,
+    rhoE]) with arrays shaped (Nz, Ny, Nx)."""
+    ts, t, nx, ny, nz = C.c_int(), C.c_double(), C.c_int(), C.c_int(), C.c_int()
+    lib = N.host_lib()
+    N.check(lib.mc3d_dump_read_header(str(path).encode(), C.byref(ts), C.byref(t), C.byref(nx), C.byref(ny),
+                                      C.byref(nz)))
+    shape = (nz.value, ny.value, nx.value)
+    out = [np.empty(shape) for _ in range(8)]
+    p = (C.POINTER(C.c_double) * 8)(*[N.dptr(a) for a in out])
+    N.check(lib.mc3d_dump_read_fields(str(path).encode(), nx.value * ny.value * nz.value, p))
+    return {"time_step": ts.value, "time": t.value, "N": (nx.value, ny.value, nz.value)}, out
+
+
+def write_dump(path, time_step, time, fields):
+    """Write a SolutionDump file from 8 arrays (x, y, z, rho, rhoU, rhoV, rhoW,
+    rhoE) shaped (Nz, Ny, Nx)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in fields]
+    nz, ny, nx = arrs[0].shape
+    p = (C.POINTER(C.c_double) * 8)(*[N.dptr(a) for a in arrs])
+    N.check(N.host_lib().mc3d_dump_write(str(path).encode(), int(time_step), float(time), nx, ny, nz, p))
+
+
 def sponge_sigma(opt, x, y, z):
     """SpongeBC sigma (src/SpongeBC.cpp:65-360) from mesh coordinates (host arrays)."""
     arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
@@ -185,7 +208,7 @@ class Options:
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
                  dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3,
-                 periodic_disp=None):
+                 periodic_disp=None, max_time_step=None, max_time=None, dump_step=None):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -207,6 +230,12 @@ class Options:
         c.dsm_test_filter = int(dsm_test_filter)
         c.dsm_use_taukk = int(bool(dsm_use_taukk))
         c.mlp_fallback_frac = mlp_fallback_frac
+        if max_time_step is not None:
+            c.max_time_step = int(max_time_step)
+        if max_time is not None:
+            c.max_time = float(max_time)
+        if dump_step is not None:
+            c.dump_step = int(dump_step)
         # BC.PERIODICDISP{X,Y,Z}_{X,Y,Z} (row = face pair, column = component)
         for d in range(3):
             for e in range(3):
@@ -341,6 +370,37 @@ class CurvilinearCSolver:
             if a.shape != self.shape:
                 raise ValueError(f"mesh arrays must be shaped {self.shape}")
         N.check(N.host_lib().mc3d_solver_set_mesh(self._h, *[N.dptr(a) for a in arrs]))
+
+    def dump(self, path=None, mesh=None):
+        """Write the state as the reference's SolutionDump file (path None:
+        SolutionDump.<time step> in the working directory); mesh (x, y, z)
+        None: the solver's own mesh or box."""
+        if mesh is None:
+            N.check(N.host_lib().mc3d_solver_dump(self._h, None if path is None else str(path).encode(),
+                                                  None, None, None))
+            return
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in mesh]
+        N.check(N.host_lib().mc3d_solver_dump(self._h, None if path is None else str(path).encode(),
+                                              *[N.dptr(a) for a in arrs]))
+
+    def restart(self, path, grid_only=False):
+        """Restart from a SolutionDump file (src/MPI_3DCompact.cpp:80-271)."""
+        N.check(N.host_lib().mc3d_solver_restart(self._h, str(path).encode(), int(bool(grid_only))))
+
+    def dump_sponge_avg(self, path=None):
+        N.check(N.host_lib().mc3d_solver_dump_sponge_avg(self._h, None if path is None else str(path).encode()))
+
+    def read_sponge_avg(self, path):
+        N.check(N.host_lib().mc3d_solver_read_sponge_avg(self._h, str(path).encode()))
+
+    def start(self):
+        """Apply the configuration's [RESTART] files (mc3d_solver_start)."""
+        N.check(N.host_lib().mc3d_solver_start(self._h))
+
+    def run(self, directory=None):
+        """Step until MAXTIMESTEP / MAXTIME / a killsolver file, dumping every
+        DUMPSTEP steps and at the end (mc3d_solver_run)."""
+        N.check(N.host_lib().mc3d_solver_run(self._h, None if directory is None else str(directory).encode()))
 
     def metrics(self):
         """The FP64 metrics J, J11..J33 the solver holds (10 arrays (Nz, Ny, Nx))."""

@@ -47,7 +47,9 @@ class Config(C.Structure):
                 ("sponge_kind", C.c_int), ("sponge_strength", C.c_double), ("sponge_rect_perc", C.c_double * 6),
                 ("sponge_cyl_orient", C.c_int), ("sponge_cyl_axis", C.c_double * 3), ("sponge_rmin", C.c_double),
                 ("wall_velocity", (C.c_double * 2) * 6), ("mlp_fallback_frac", C.c_double),
-                ("periodic_disp", (C.c_double * 3) * 3)]
+                ("periodic_disp", (C.c_double * 3) * 3), ("dump_step", C.c_int),
+                ("from_restart", C.c_int), ("only_grid_from_restart", C.c_int), ("sponge_avg_from_restart", C.c_int),
+                ("restart_file", C.c_char * 512), ("sponge_avg_file", C.c_char * 512)]
 
 
 _lib = None
@@ -76,6 +78,16 @@ def host_lib():
             "mc3d_solver_set_box_metrics": (ip, [vp, dp, dp, dp]),
             "mc3d_solver_set_mesh": (ip, [vp, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
             "mc3d_solver_get_metrics": (ip, [vp, C.POINTER(C.POINTER(dp))]),
+            "mc3d_dump_read_header": (ip, [C.c_char_p, C.POINTER(ip), C.POINTER(dp), C.POINTER(ip), C.POINTER(ip),
+                                           C.POINTER(ip)]),
+            "mc3d_dump_read_fields": (ip, [C.c_char_p, C.c_longlong, C.POINTER(C.POINTER(dp))]),
+            "mc3d_dump_write": (ip, [C.c_char_p, ip, dp, ip, ip, ip, C.POINTER(C.POINTER(dp))]),
+            "mc3d_solver_dump": (ip, [vp, C.c_char_p, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
+            "mc3d_solver_restart": (ip, [vp, C.c_char_p, ip]),
+            "mc3d_solver_dump_sponge_avg": (ip, [vp, C.c_char_p]),
+            "mc3d_solver_read_sponge_avg": (ip, [vp, C.c_char_p]),
+            "mc3d_solver_start": (ip, [vp]),
+            "mc3d_solver_run": (ip, [vp, C.c_char_p]),
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),
             "mc3d_solver_set_initial_device": (ip, [vp] + [vp] * 5),
             "mc3d_solver_step": (ip, [vp, ip]),

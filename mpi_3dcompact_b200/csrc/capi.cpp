@@ -77,6 +77,9 @@ int mc3d_config_default(mc3d_config *c) {
     c->mlp_fallback_frac = 1e-3;
     for (int d = 0; d < 3; d++)
         for (int e = 0; e < 3; e++) c->periodic_disp[d][e] = 0.0;
+    c->dump_step = 1000;   // src/Options.hpp:237
+    c->from_restart = c->only_grid_from_restart = c->sponge_avg_from_restart = 0;
+    c->restart_file[0] = c->sponge_avg_file[0] = '\0';
     return MC3D_OK;
 }
 
@@ -191,6 +194,8 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
             c->max_time_step = parse_int("MAXTIMESTEP", ini.get("TIMESTEPPING.MAXTIMESTEP"));
         if (ini.has("TIMESTEPPING.FILTERSTEP"))
             c->filter_step = parse_int("FILTERSTEP", ini.get("TIMESTEPPING.FILTERSTEP"));
+        if (ini.has("TIMESTEPPING.DUMPSTEP")) c->dump_step = parse_int("DUMPSTEP", ini.get("TIMESTEPPING.DUMPSTEP"));
+        if (c->dump_step <= 0) throw CfgError{"DUMPSTEP must be positive"};
         if (ini.has("TIMESTEPPING.SUBSTEPFILTERING"))
             c->substep_filtering = parse_bool("SUBSTEPFILTERING", ini.get("TIMESTEPPING.SUBSTEPFILTERING"));
         // [DOMAIN] (required unless restarting, Options.hpp:380-385)
@@ -203,12 +208,31 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
         if (!ini.has("RESTART.SPONGEAVGFROMRESTART"))
             throw CfgError{"spongeFromRestart not specified, NEEDS TO BE SPECIFED"};
         if (restart && gridrs) throw CfgError{"'only use grid from restart file' and 'from restart file' conflict"};
-        if (restart || gridrs) throw CfgError{"restart files are not read by this build"};
-        const char *dk[3] = {"DOMAIN.NX", "DOMAIN.NY", "DOMAIN.NZ"};
-        int *dn[3] = {&c->Nx, &c->Ny, &c->Nz};
-        for (int d = 0; d < 3; d++) {
-            if (!ini.has(dk[d])) throw CfgError{std::string(dk[d]) + " not specified, NEEDS TO BE SPECIFED"};
-            *dn[d] = parse_int(dk[d], ini.get(dk[d]));
+        c->from_restart = restart ? 1 : 0;
+        c->only_grid_from_restart = gridrs ? 1 : 0;
+        if (restart || gridrs) {
+            if (!ini.has("RESTART.FILENAME")) throw CfgError{"restart filename not specified, NEEDS TO BE SPECIFED"};
+            const std::string fn = ini.get("RESTART.FILENAME");
+            if (fn.size() >= sizeof(c->restart_file)) throw CfgError{"RESTART.FILENAME is too long"};
+            std::snprintf(c->restart_file, sizeof(c->restart_file), "%s", fn.c_str());
+            // grid sizes from the file's header (src/MPI_3DCompact.cpp:80-110)
+            if (read_solution_header(c->restart_file, nullptr, nullptr, &c->Nx, &c->Ny, &c->Nz))
+                throw CfgError{"ERROR: Couldn't open file " + fn};
+        } else {
+            const char *dk[3] = {"DOMAIN.NX", "DOMAIN.NY", "DOMAIN.NZ"};
+            int *dn[3] = {&c->Nx, &c->Ny, &c->Nz};
+            for (int d = 0; d < 3; d++) {
+                if (!ini.has(dk[d])) throw CfgError{std::string(dk[d]) + " not specified, NEEDS TO BE SPECIFED"};
+                *dn[d] = parse_int(dk[d], ini.get(dk[d]));
+            }
+        }
+        c->sponge_avg_from_restart = parse_bool("SPONGEAVGFROMRESTART", ini.get("RESTART.SPONGEAVGFROMRESTART")) ? 1 : 0;
+        if (c->sponge_avg_from_restart) {
+            if (!ini.has("RESTART.SPONGEAVGFILENAME"))
+                throw CfgError{"sponge_filename not specified, NEEDS TO BE SPECIFED"};
+            const std::string fn = ini.get("RESTART.SPONGEAVGFILENAME");
+            if (fn.size() >= sizeof(c->sponge_avg_file)) throw CfgError{"RESTART.SPONGEAVGFILENAME is too long"};
+            std::snprintf(c->sponge_avg_file, sizeof(c->sponge_avg_file), "%s", fn.c_str());
         }
         if (c->Nx <= 10 || c->Ny <= 10 || c->Nz <= 10)
             throw CfgError{"Number of grid points in any direction must be greater than 10!"};

@@ -349,6 +349,14 @@ struct MetOut9 {
     double *p[9];
 };
 int launch_tpb_rhs(const Grid3 &g, int dir, const double *f, const TpbArgs &a, double *rhs, cudaStream_t st);
+
+// ---- checkpoint files (checkpoint.cpp) ----------------------------------------
+int write_solution_dump(const char *path, int time_step, double time, int Nx, int Ny, int Nz,
+                        const double *const fields[8]);
+int read_solution_header(const char *path, int *time_step, double *time, int *Nx, int *Ny, int *Nz);
+int read_solution_fields(const char *path, long long n, double *const fields[8]);
+int write_sponge_avg(const char *path, long long n, const double *const fields[5]);
+int read_sponge_avg(const char *path, long long n, double *const fields[5]);
 int launch_metric_mul(long long n, const double *a, const double *b, double *o, cudaStream_t st);
 int launch_metric_sub(long long n, const double *a, const double *b, double *o, cudaStream_t st);
 int launch_metric_dot3(long long n, const double *const xyz[3], const double *const abc[3], double *o,

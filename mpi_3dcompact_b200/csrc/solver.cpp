@@ -53,6 +53,11 @@ struct mc3d_solver_s {
     bool const_met = true;
     double met_c[10] = {0};
     bool have_metrics = false;
+    // the mesh behind the metrics, for SolutionDump files: coordinates given to
+    // set_mesh / restart, or the box lengths of set_box_metrics
+    std::vector<double> mesh_xyz[3];
+    double box_L[3] = {0, 0, 0};
+    int mesh_kind = 0;   // 0 none, 1 coordinates, 2 box
     mc3d::TimeState *ts = nullptr;
     double *acc = nullptr;
     int host_time_step = 0;
@@ -781,7 +786,14 @@ int mc3d_solver_set_box_metrics(mc3d_solver s, double Lx, double Ly, double Lz) 
     if (!(Lx > 0 && Ly > 0 && Lz > 0)) return fail(MC3D_ERR_ARG, "box lengths must be positive");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
     double c[10] = {1.0 / (Lx * Ly * Lz), 1.0 / Lx, 0, 0, 0, 1.0 / Ly, 0, 0, 0, 1.0 / Lz};
-    return upload_metrics(s, nullptr, c);
+    int rc = upload_metrics(s, nullptr, c);
+    if (rc) return rc;
+    s->box_L[0] = Lx;
+    s->box_L[1] = Ly;
+    s->box_L[2] = Lz;
+    s->mesh_kind = 2;
+    for (auto &v : s->mesh_xyz) std::vector<double>().swap(v);
+    return MC3D_OK;
 }
 
 namespace mc3d {
@@ -982,7 +994,14 @@ int mc3d_solver_set_mesh(mc3d_solver s, const double *x, const double *y, const 
     if (rc) return rc;
     const double *p[10];
     for (int c = 0; c < 10; c++) p[c] = h[c].data();
-    return upload_metrics(s, p, nullptr);
+    rc = upload_metrics(s, p, nullptr);
+    if (rc) return rc;
+    const size_t n = (size_t)s->g.n();
+    s->mesh_xyz[0].assign(x, x + n);
+    s->mesh_xyz[1].assign(y, y + n);
+    s->mesh_xyz[2].assign(z, z + n);
+    s->mesh_kind = 1;
+    return MC3D_OK;
 }
 
 int mc3d_solver_get_metrics(mc3d_solver s, double *const metrics[10]) {
@@ -1176,6 +1195,187 @@ int mc3d_solver_copy_conserved_device(mc3d_solver s, double *const dst[5]) {
 int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]) {
     if (!s || !ptrs) return fail(MC3D_ERR_ARG, "null argument");
     for (int v = 0; v < 5; v++) ptrs[v] = s->q1[v];
+    return MC3D_OK;
+}
+
+// ---- checkpoints and the driver loop ------------------------------------------
+
+// The time origin of a (re)start: time step and time of the state, the counters
+// a fresh solver starts with (src/MPI_3DCompact.cpp:99-101 sets opt->timeStep
+// and opt->time, which the solver takes over in its constructor,
+// src/CurvilinearCSolver.hpp:147-148).
+static int set_time_origin(mc3d_solver s, int time_step, double time) {
+    s->cfg.time_step0 = time_step;
+    s->cfg.time0 = time;
+    s->host_time_step = time_step;
+    s->filter_time_step = 0;
+    s->lsldd_half = 1;
+    mc3d::TimeState t{};
+    t.time = time;
+    t.time_step = time_step;
+    t.dt = s->cfg.ts_type == MC3D_CONST_DT ? s->cfg.dt : 0.0;
+    MC3D_CUDA_TRY(cudaMemcpyAsync(s->ts, &t, sizeof(t), cudaMemcpyHostToDevice, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
+}
+
+int mc3d_solver_dump(mc3d_solver s, const char *path, const double *x, const double *y, const double *z) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no state to dump");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.n();
+    std::vector<double> q[5], box[3];
+    for (auto &v : q) v.resize(n);
+    int rc = mc3d_solver_get_conserved(s, q[0].data(), q[1].data(), q[2].data(), q[3].data(), q[4].data());
+    if (rc) return rc;
+    int ts;
+    double time;
+    if ((rc = mc3d_solver_info(s, &ts, &time, nullptr, nullptr))) return rc;
+    const double *xyz[3] = {x, y, z};
+    if (!x || !y || !z) {
+        if (s->mesh_kind == 1) {
+            for (int c = 0; c < 3; c++) xyz[c] = s->mesh_xyz[c].data();
+        } else if (s->mesh_kind == 2) {
+            // the box x = L*xi with Domain's xi (src/Domain.hpp:44-56)
+            const int N[3] = {s->g.Nx, s->g.Ny, s->g.Nz};
+            for (int c = 0; c < 3; c++) {
+                std::vector<double> xi(N[c]);
+                for (int i = 0; i < N[c]; i++)
+                    xi[i] = s->cfg.bc_type[c] == MC3D_PERIODIC_SOLVE ? (double)i * 1.0 / (double)N[c]
+                                                                     : ((double)i / ((double)N[c] - 1.0)) * 1.0;
+                box[c].resize(n);
+                for (int k = 0; k < s->g.Nz; k++)
+                    for (int j = 0; j < s->g.Ny; j++)
+                        for (int i = 0; i < s->g.Nx; i++) {
+                            const int ix[3] = {i, j, k};
+                            box[c][i + (size_t)s->g.Nx * (j + (size_t)s->g.Ny * k)] = s->box_L[c] * xi[ix[c]];
+                        }
+                xyz[c] = box[c].data();
+            }
+        } else {
+            return fail(MC3D_ERR_CONFIG, "no mesh: pass x, y, z (metrics were given directly)");
+        }
+    }
+    const std::string name = path ? std::string(path) : "SolutionDump." + std::to_string(ts);
+    const double *f[8] = {xyz[0], xyz[1], xyz[2], q[0].data(), q[1].data(), q[2].data(), q[3].data(), q[4].data()};
+    return write_solution_dump(name.c_str(), ts, time, s->g.Nx, s->g.Ny, s->g.Nz, f);
+}
+
+int mc3d_solver_restart(mc3d_solver s, const char *path, int grid_only) {
+    if (!s || !path) return fail(MC3D_ERR_ARG, "null argument");
+    int ts, Nx, Ny, Nz;
+    double time;
+    int rc = read_solution_header(path, &ts, &time, &Nx, &Ny, &Nz);
+    if (rc) return rc;
+    if (Nx != s->g.Nx || Ny != s->g.Ny || Nz != s->g.Nz)
+        return fail(MC3D_ERR_CONFIG, std::string("grid of ") + path + " differs from the solver's");
+    const long long n = s->g.n();
+    std::vector<double> f[8];
+    double *fp[8];
+    for (int k = 0; k < 8; k++) {
+        if (grid_only && k >= 3) {
+            fp[k] = nullptr;
+            continue;
+        }
+        f[k].resize((size_t)n);
+        fp[k] = f[k].data();
+    }
+    if ((rc = read_solution_fields(path, n, fp))) return rc;
+    // AlgebraicSingleBlockMesh::getMesh reads the grid of a restart (src/AlgebraicSingleBlockMesh.hpp:77-101)
+    if ((rc = mc3d_solver_set_mesh(s, fp[0], fp[1], fp[2]))) return rc;
+    if (s->have_sponge && !s->sigma_set) {
+        // SpongeBC builds its strength field from the mesh (src/SpongeBC.cpp:65-189)
+        std::vector<double> sig((size_t)n);
+        if ((rc = mc3d_sponge_sigma(&s->cfg, fp[0], fp[1], fp[2], sig.data()))) return rc;
+        if ((rc = mc3d_solver_set_sponge(s, sig.data()))) return rc;
+    }
+    if (grid_only) return MC3D_OK;
+    // src/MPI_3DCompact.cpp:248-262 with IdealGas::solveU / solvep (src/IdealGas.hpp:58-64)
+    const double gamma = 1.4;
+    std::vector<double> U((size_t)n), V((size_t)n), W((size_t)n), p((size_t)n);
+    for (long long i = 0; i < n; i++) {
+        const double rho = f[3][i];
+        U[i] = f[4][i] / rho;
+        V[i] = f[5][i] / rho;
+        W[i] = f[6][i] / rho;
+        p[i] = (gamma - 1) * (f[7][i] - 0.5 * rho * (U[i] * U[i] + V[i] * V[i] + W[i] * W[i]));
+    }
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    if ((rc = set_time_origin(s, ts, time))) return rc;
+    return mc3d_solver_set_initial(s, f[3].data(), U.data(), V.data(), W.data(), p.data());
+}
+
+int mc3d_solver_dump_sponge_avg(mc3d_solver s, const char *path) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    if (!s->have_sponge) return fail(MC3D_ERR_CONFIG, "no face is a SPONGE");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.n();
+    std::vector<double> a[5];
+    const double *ap[5];
+    for (int v = 0; v < 5; v++) {
+        a[v].resize(n);
+        MC3D_CUDA_TRY(cudaMemcpyAsync(a[v].data(), s->spg_avg[v], n * 8, cudaMemcpyDeviceToHost, s->stream));
+        ap[v] = a[v].data();
+    }
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    int ts;
+    int rc = mc3d_solver_info(s, &ts, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    const std::string name = path ? std::string(path) : "SpongeAvgDump." + std::to_string(ts);
+    return write_sponge_avg(name.c_str(), (long long)n, ap);
+}
+
+int mc3d_solver_read_sponge_avg(mc3d_solver s, const char *path) {
+    if (!s || !path) return fail(MC3D_ERR_ARG, "null argument");
+    const size_t n = (size_t)s->g.n();
+    std::vector<double> a[5];
+    double *ap[5];
+    for (int v = 0; v < 5; v++) {
+        a[v].resize(n);
+        ap[v] = a[v].data();
+    }
+    int rc = read_sponge_avg(path, (long long)n, ap);
+    if (rc) return rc;
+    const double *cp[5] = {ap[0], ap[1], ap[2], ap[3], ap[4]};
+    return mc3d_solver_set_sponge_avg(s, cp);
+}
+
+int mc3d_solver_start(mc3d_solver s) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    int rc = MC3D_OK;
+    if (s->cfg.from_restart || s->cfg.only_grid_from_restart)
+        rc = mc3d_solver_restart(s, s->cfg.restart_file, s->cfg.only_grid_from_restart);
+    if (!rc && s->cfg.sponge_avg_from_restart) rc = mc3d_solver_read_sponge_avg(s, s->cfg.sponge_avg_file);
+    return rc;
+}
+
+int mc3d_solver_run(mc3d_solver s, const char *dir) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    const std::string base = dir ? std::string(dir) + "/" : std::string();
+    auto dump = [&](int ts) -> int {
+        int rc = mc3d_solver_dump(s, (base + "SolutionDump." + std::to_string(ts)).c_str(), nullptr, nullptr, nullptr);
+        if (!rc && s->have_sponge)
+            rc = mc3d_solver_dump_sponge_avg(s, (base + "SpongeAvgDump." + std::to_string(ts)).c_str());
+        return rc;
+    };
+    bool end = false;
+    while (!end) {
+        int rc = mc3d_solver_step(s, 1);
+        if (rc) return rc;
+        int ts;
+        double time;
+        if ((rc = mc3d_solver_info(s, &ts, &time, nullptr, nullptr))) return rc;
+        // postStep (src/CurvilinearCSolver.hpp:367-369), then checkEnd (Core.cpp:1785-1824)
+        if (ts % s->cfg.dump_step == 0 && (rc = dump(ts))) return rc;
+        const std::string kill = base + "killsolver";
+        if (FILE *kf = std::fopen(kill.c_str(), "r")) {
+            std::fclose(kf);
+            std::remove(kill.c_str());
+            end = true;
+        }
+        if (time >= s->cfg.max_time || ts >= s->cfg.max_time_step) end = true;
+        if (end && (rc = dump(ts))) return rc;
+    }
     return MC3D_OK;
 }
 

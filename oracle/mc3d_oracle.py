@@ -1272,6 +1272,32 @@ def solve_for_jacobians(cfg: Config, x, y, z, quirks=True):
     return [J] + [J * Jr[a][b] for a in range(3) for b in range(3)]
 
 
+# --------------------------------------------------------------------------
+# Checkpoints (src/CurvilinearCSolver_Core.cpp:1333-1405, src/MPI_3DCompact.cpp:80-271)
+# --------------------------------------------------------------------------
+def parse_solution_dump(raw: bytes):
+    """A SolutionDump file as dumpSolution writes it: 5 FP64 header values
+    (time step, time, Nx, Ny, Nz) then x, y, z, rho, rhoU, rhoV, rhoW, rhoE,
+    Nx*Ny*Nz FP64 values each, x fastest. Returns (header, 8 fields (Nz, Ny, Nx))."""
+    a = np.frombuffer(raw, dtype=np.float64)
+    ts, t, nx, ny, nz = a[:5]
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    n = nx * ny * nz
+    if a.size != 5 + 8 * n:
+        raise ValueError("not a SolutionDump of its header's size")
+    fields = [a[5 + k * n:5 + (k + 1) * n].reshape(nz, ny, nx).copy() for k in range(8)]
+    return {"time_step": int(ts), "time": float(t), "N": (nx, ny, nz)}, fields
+
+
+def restart_primitives(q):
+    """src/MPI_3DCompact.cpp:248-262: rho, U, V, W, p of a restart from its
+    conserved fields through IdealGas::solveU / solvep (src/IdealGas.hpp:58-64)."""
+    rho, ru, rv, rw, re = q
+    U, V, W = ru / rho, rv / rho, rw / rho
+    p = (1.4 - 1) * (re - 0.5 * rho * (U * U + V * V + W * W))
+    return rho, U, V, W, p
+
+
 def cube_metrics(N, L=2.0 * math.pi):
     """Analytic metrics of the periodic cube x = L*xi (the HIT box of
     tests/hit/Samtaney_D4/AlgebraicSingleBlockMesh.hpp:154-156): J_ii = 1/L,
@@ -1283,11 +1309,12 @@ def cube_metrics(N, L=2.0 * math.pi):
     return [np.full(shp, 1.0 / L ** 3), d, z, z, z, d.copy(), z, z, z, d.copy()]
 
 
-def run(cfg: Config, ic, nsteps, metrics=None, sigma=None):
-    """Run `nsteps` time steps from primitive ICs (rho, U, V, W, p) and return
-    (conserved state rho1..rhoE1, state object)."""
+def run(cfg: Config, ic, nsteps, metrics=None, sigma=None, time=0.0, time_step=0):
+    """Run `nsteps` time steps from primitive ICs (rho, U, V, W, p), starting
+    at `time` / `time_step` (a restart), and return (conserved state
+    rho1..rhoE1, state object)."""
     o = Oracle(cfg, metrics if metrics is not None else cube_metrics(cfg.N), sigma=sigma)
-    o.init(*ic)
+    o.init(*ic, time=time, time_step=time_step)
     for _ in range(nsteps):
         o.step()
     return o.state.q1, o.state

@@ -17,11 +17,20 @@
  *        SOLVER.ALPHAF) or TESTPADE|TESTEXP (the DSM test filters
  *        CommN5PadeTestFilter / CommN5ExpTestFilter); dir = 0,1,2.
  *   metrics <mesh> <out.bin>               J, J11..J33 from solveForJacobians.
- * <mesh> is "cube:<L>" (x = L*xi, the HIT box) or "file:<path>" (x,y,z FP64).
+ *   restart <SolutionDump> <out.bin>       restart as src/MPI_3DCompact.cpp:80-271
+ *        does (time step, time, mesh and conserved state from the dump,
+ *        primitives through IdealGas::solveU/solvep), run to MAXTIMESTEP.
+ * <mesh> is "cube:<L>" (x = L*xi, the HIT box), "file:<path>" (x,y,z FP64)
+ * or "dump:<path>" (x,y,z after the 5-value header of a SolutionDump file,
+ * as AlgebraicSingleBlockMesh::getMesh reads a restart grid,
+ * src/AlgebraicSingleBlockMesh.hpp:77-101).
+ * Every "run"/"restart" also leaves the reference's own SolutionDump.<step>
+ * (written by CurvilinearCSolver::checkEnd at the last step).
  * All binary fields are FP64, x-fastest global order (i + Nx*(j + Ny*k)).
  */
 #include <mpi.h>
 #include <cmath>
+#include <new>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -49,6 +58,26 @@ using namespace std;
 #include "CommN5PadeTestFilter.hpp"
 #include "CommN5ExpTestFilter.hpp"
 
+// Every allocation of the reference starts zero-filled. Its C2Decomp::alloc*
+// arrays come from new[] and are not cleared, and solveForJacobians reads some
+// of that memory before writing it on meshes with a wall direction (restarts
+// of the same mesh gave different metrics until allocations were zeroed); the
+// GPU context zero-initialises its buffers, so the oracle runs do the same.
+void *operator new[](size_t n) {
+    void *p = calloc(n ? n : 1, 1);
+    if (!p) throw std::bad_alloc();
+    return p;
+}
+void *operator new(size_t n) {
+    void *p = calloc(n ? n : 1, 1);
+    if (!p) throw std::bad_alloc();
+    return p;
+}
+void operator delete[](void *p) noexcept { free(p); }
+void operator delete(void *p) noexcept { free(p); }
+void operator delete[](void *p, size_t) noexcept { free(p); }
+void operator delete(void *p, size_t) noexcept { free(p); }
+
 // wall-clock stamp at the end of every time step (postStep -> fullStepTemporalHook)
 static std::vector<double> g_step_stamps;
 
@@ -69,10 +98,11 @@ static void die(const string &m) {
     exit(2);
 }
 
-static vector<double> read_bin(const string &path, size_t n) {
+static vector<double> read_bin(const string &path, size_t n, size_t skip = 0) {
     vector<double> v(n);
     FILE *f = fopen(path.c_str(), "rb");
     if (!f) die("cannot open " + path);
+    if (skip && fseek(f, (long)(skip * sizeof(double)), SEEK_SET) != 0) die("seek " + path);
     if (fread(v.data(), sizeof(double), n, f) != n) die("short read " + path);
     fclose(f);
     return v;
@@ -100,6 +130,12 @@ class HarnessMesh : public AbstractSingleBlockMesh {
         Nz = d->gNz;
         allocateForMesh();
         getMesh();
+        // handlePeriodicStuff leaves a periodic direction's translation unset
+        // when its faces are neither both PERIODIC (as tested, the Y faces for
+        // x, src/AbstractSingleBlockMesh.cpp:2034) nor INTERNALLY_PERIODIC; the
+        // members are otherwise uninitialised, so they start from zero here
+        for (int c = 0; c < 3; c++)
+            periodicXTranslation[c] = periodicYTranslation[c] = periodicZTranslation[c] = 0.0;
         handlePeriodicStuff();
         solveForJacobians();
     }
@@ -109,9 +145,9 @@ class HarnessMesh : public AbstractSingleBlockMesh {
         bool cube = spec.compare(0, 5, "cube:") == 0;
         if (cube) {
             L = atof(spec.c_str() + 5);
-        } else if (spec.compare(0, 5, "file:") == 0) {
+        } else if (spec.compare(0, 5, "file:") == 0 || spec.compare(0, 5, "dump:") == 0) {
             size_t n = (size_t)Nx * Ny * Nz;
-            vector<double> all = read_bin(spec.substr(5), 3 * n);
+            vector<double> all = read_bin(spec.substr(5), 3 * n, spec[0] == 'd' ? 5 : 0);
             X.assign(all.begin(), all.begin() + n);
             Y.assign(all.begin() + n, all.begin() + 2 * n);
             Z.assign(all.begin() + 2 * n, all.end());
@@ -182,10 +218,17 @@ static void write_fields(const string &path, const vector<double *> &fields, int
     fclose(f);
 }
 
-static int mode_run(const string &mesh, const string &icpath, const string &out) {
+static int mode_run(const string &mesh, const string &icpath, const string &out, const string &restart = "") {
     Setup s = make_setup();
     int Nx = s.opt->Nx, Ny = s.opt->Ny, Nz = s.opt->Nz;
     size_t n = (size_t)Nx * Ny * Nz;
+    if (!restart.empty()) {
+        // src/MPI_3DCompact.cpp:80-110: time step, time and sizes from the header
+        vector<double> h = read_bin(restart, 5);
+        if ((int)h[2] != Nx || (int)h[3] != Ny || (int)h[4] != Nz) die("restart file sizes differ from DOMAIN");
+        s.opt->timeStep = (int)h[0];
+        s.opt->time = h[1];
+    }
     CurvilinearCSolver *cs = new CurvilinearCSolver(s.c2d, s.d, s.bc, s.ts, s.opt);
     // The reference allocates solver arrays with new[] and never clears them;
     // the momentum update accumulates into rho{U,V,W}k2 (Core.cpp:839,872,904),
@@ -201,17 +244,33 @@ static int mode_run(const string &mesh, const string &icpath, const string &out)
     else if (s.opt->rkType == Options::LSLDDRK4) rk = new LSLDDRK4(cs);
     else die("unknown RK type");
 
-    vector<double> ic = read_bin(icpath, 5 * n);
-    for (int k = 0; k < Nz; k++)
-        for (int j = 0; j < Ny; j++)
-            for (int i = 0; i < Nx; i++) {
-                size_t g = glob(i, j, k, Nx, Ny), ip = ymaj(i, j, k, Ny, Nz);
-                cs->rho0[ip] = ic[g];
-                cs->U0[ip] = ic[n + g];
-                cs->V0[ip] = ic[2 * n + g];
-                cs->W0[ip] = ic[3 * n + g];
-                cs->p0[ip] = ic[4 * n + g];
-            }
+    if (restart.empty()) {
+        vector<double> ic = read_bin(icpath, 5 * n);
+        for (int k = 0; k < Nz; k++)
+            for (int j = 0; j < Ny; j++)
+                for (int i = 0; i < Nx; i++) {
+                    size_t g = glob(i, j, k, Nx, Ny), ip = ymaj(i, j, k, Ny, Nz);
+                    cs->rho0[ip] = ic[g];
+                    cs->U0[ip] = ic[n + g];
+                    cs->V0[ip] = ic[2 * n + g];
+                    cs->W0[ip] = ic[3 * n + g];
+                    cs->p0[ip] = ic[4 * n + g];
+                }
+    } else {
+        // src/MPI_3DCompact.cpp:220-262: conserved fields after the header and
+        // the mesh, primitives through the solver's IdealGas
+        vector<double> q = read_bin(restart, 5 * n, 5 + 3 * n);
+        for (int k = 0; k < Nz; k++)
+            for (int j = 0; j < Ny; j++)
+                for (int i = 0; i < Nx; i++) {
+                    size_t g = glob(i, j, k, Nx, Ny), ip = ymaj(i, j, k, Ny, Nz);
+                    cs->rho0[ip] = q[g];
+                    cs->U0[ip] = cs->ig->solveU(q[g], q[n + g]);
+                    cs->V0[ip] = cs->ig->solveU(q[g], q[2 * n + g]);
+                    cs->W0[ip] = cs->ig->solveU(q[g], q[3 * n + g]);
+                    cs->p0[ip] = cs->ig->solvep(q[g], q[4 * n + g], cs->U0[ip], cs->V0[ip], cs->W0[ip]);
+                }
+    }
     cs->setInitialConditions();
 
     double t0 = MPI_Wtime();
@@ -293,12 +352,13 @@ static int mode_ops(const string &scheme, int dir, const string &in, const strin
 
 int main(int argc, char **argv) {
     MPI_Init(&argc, &argv);
-    if (argc < 2) die("usage: mc3d_ref run|ops|metrics ...");
+    if (argc < 2) die("usage: mc3d_ref run|ops|metrics|restart ...");
     string mode = argv[1];
     int rc = 2;
     if (mode == "run" && argc == 5) rc = mode_run(argv[2], argv[3], argv[4]);
     else if (mode == "ops" && argc == 6) rc = mode_ops(argv[2], atoi(argv[3]), argv[4], argv[5]);
     else if (mode == "metrics" && argc == 4) rc = mode_metrics(argv[2], argv[3]);
+    else if (mode == "restart" && argc == 4) rc = mode_run(string("dump:") + argv[2], "", argv[3], argv[2]);
     else die("bad arguments");
     MPI_Finalize();
     return rc;

@@ -7,6 +7,7 @@ Fields cross the process boundary as FP64 arrays shaped (Nz, Ny, Nx).
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import tempfile
 import time
@@ -117,26 +118,43 @@ def _read_fields(path, N, nf, header=8):
     return hdr, fields
 
 
-def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coords=None):
+def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coords=None, dump_to=None,
+               restart_from=None, sponge_dump_to=None):
     """Run the reference solver for `nsteps` time steps from primitive ICs
     (rho, U, V, W, p). `coords` = (x, y, z) selects a mesh from file. Returns
-    (conserved fields, header dict)."""
+    (conserved fields, header dict). `dump_to`: copy the SolutionDump.<step>
+    file the reference writes when it reaches its last step
+    (CurvilinearCSolver::checkEnd, src/CurvilinearCSolver_Core.cpp:1820-1823)
+    to this path. `restart_from`: start from a SolutionDump file instead of
+    `ic` (mesh, conserved state, time step and time from the file, as
+    src/MPI_3DCompact.cpp:80-271 restarts); nsteps then counts from its step.
+    `sponge_dump_to`: copy the SpongeAvgDump.<step> written with it."""
     if not available():
         raise RuntimeError("oracle/_ref/mc3d_ref is not built (make -C oracle)")
+    if restart_from is not None:
+        nsteps += int(np.fromfile(restart_from, dtype=np.float64, count=1)[0])   # MAXTIMESTEP is absolute
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "MPI_3DCompact.in"), "w") as f:
             f.write(ini_text(cfg, nsteps))
-        _write(os.path.join(d, "ic.bin"), ic)
-        if coords is not None:
-            _write(os.path.join(d, "mesh.bin"), coords)
-            mesh = "file:mesh.bin"
+        if restart_from is not None:
+            shutil.copy(restart_from, os.path.join(d, "restart.bin"))
+            cmd = [REF_BIN, "restart", "restart.bin", "out.bin"]
+        else:
+            _write(os.path.join(d, "ic.bin"), ic)
+            if coords is not None:
+                _write(os.path.join(d, "mesh.bin"), coords)
+                mesh = "file:mesh.bin"
+            cmd = [REF_BIN, "run", mesh, "ic.bin", "out.bin"]
         t0 = time.perf_counter()
-        r = subprocess.run([REF_BIN, "run", mesh, "ic.bin", "out.bin"], cwd=d,
-                           capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0
         if r.returncode != 0:
             raise RuntimeError("mc3d_ref failed: " + r.stderr[-2000:] + r.stdout[-2000:])
         hdr, fields = _read_fields(os.path.join(d, "out.bin"), cfg.N, 5)
+        if dump_to is not None:
+            shutil.copy(os.path.join(d, f"SolutionDump.{int(hdr[0])}"), dump_to)
+        if sponge_dump_to is not None:
+            shutil.copy(os.path.join(d, f"SpongeAvgDump.{int(hdr[0])}"), sponge_dump_to)
         st = os.path.join(d, "step_times.txt")
         step_s = [float(x) for x in open(st).read().split()] if os.path.exists(st) else []
     info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall,
