@@ -174,6 +174,10 @@ struct FluxParams {
 
 template <typename R>
 int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st);
+// primitives and the CFL wave-speed maximum (atomicMax into *umax, as launch_cfl)
+template <typename R>
+int launch_primitives_cfl(const Grid3 &g, const double *const q[5], R *const prim[5], const Metrics<R> &m,
+                          const double dxi[3], unsigned long long *umax, cudaStream_t st);
 
 // prim = rho, U, V, W, T of the stage state
 // les 3 (DSM): mu_sgs, k_sgs and tau_kk fields; T in prim[4] is the
@@ -196,10 +200,12 @@ struct RkStage {
     int nstages;
     double a, b;       // scheme coefficients of this stage
 };
-// prim (optional, may be null): also write rho, U, V, W, T of the new stage state
+// prim (optional, may be null): also write rho, U, V, W, T of the new stage
+// state, or with copy_final on the last stage the final state in R instead
 template <typename R>
 int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
-                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st);
+                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st,
+                     bool copy_final = false);
 
 template <typename R>
 int launch_to_real(const Grid3 &g, const double *const src[5], R *const dst[5], cudaStream_t st);

@@ -40,6 +40,57 @@ __global__ void primitives_kernel(Grid3 g, const double *__restrict__ r0, const 
         prims_of<R>(r0[i], r1[i], r2[i], r3[i], r4[i], P.p, i);
 }
 
+// Primitives of the stage-1 state together with the CFL wave-speed maximum of
+// calcDtFromCFL (src/CurvilinearCSolver_Core.cpp:189-212), which reads the same
+// state: max over points of J11 (|U| + c)/dxi + J22 (|V| + c)/deta + J33 (|W| + c)/dzeta.
+template <typename R>
+__global__ void primitives_cfl_kernel(Grid3 g, const double *__restrict__ r0, const double *__restrict__ r1,
+                                      const double *__restrict__ r2, const double *__restrict__ r3,
+                                      const double *__restrict__ r4, P5<R> P, Metrics<R> m, double i0, double i1,
+                                      double i2, unsigned long long *umax) {
+    __shared__ double red[32];
+    double best = 0.0;
+    bool bad = false;
+    const long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double rho = r0[i], q1 = r1[i], q2 = r2[i], q3 = r3[i], q4 = r4[i];
+        prims_of<R>(rho, q1, q2, q3, q4, P.p, i);
+        const double u = q1 / rho, v = q2 / rho, w = q3 / rho;
+        const double p = (GAMMA - 1) * (q4 - 0.5 * rho * (u * u + v * v + w * w));
+        const double c = sqrt(GAMMA * p / rho);
+        const double uc = (double)met(m, 1, i) * (fabs(u) + c) * i0 + (double)met(m, 5, i) * (fabs(v) + c) * i1 +
+                          (double)met(m, 9, i) * (fabs(w) + c) * i2;
+        if (!isfinite(uc)) bad = true;
+        else if (uc > best) best = uc;
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double b = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+        if (threadIdx.x == 0) atomicMax(umax, (unsigned long long)__double_as_longlong(b));
+    }
+    // a non-finite state poisons the maximum: dt becomes NaN and the host check reports it
+    if (bad) atomicMax(umax, 0x7ff8000000000000ull);
+}
+
+template <typename R>
+int launch_primitives_cfl(const Grid3 &g, const double *const q[5], R *const prim[5], const Metrics<R> &m,
+                          const double dxi[3], unsigned long long *umax, cudaStream_t st) {
+    P5<R> P;
+    for (int v = 0; v < 5; v++) P.p[v] = prim[v];
+    primitives_cfl_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], P, m,
+                                                                   1.0 / dxi[0], 1.0 / dxi[1], 1.0 / dxi[2], umax);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+template int launch_primitives_cfl<float>(const Grid3 &, const double *const[5], float *const[5],
+                                          const Metrics<float> &, const double[3], unsigned long long *, cudaStream_t);
+template int launch_primitives_cfl<double>(const Grid3 &, const double *const[5], double *const[5],
+                                           const Metrics<double> &, const double[3], unsigned long long *,
+                                           cudaStream_t);
+
 template <typename R>
 int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st) {
     P5<R> P;
@@ -487,8 +538,13 @@ __global__ void __launch_bounds__(256) rk_kernel(Grid3 g, RkStage rs, K5<R> k2, 
             if (wr_qk) st_pair<double>(qk.p[v], i, two, ok[v][0], ok[v][1]);
             if (wr_q2) st_pair<double>(q2.p[v], i, two, o2[v][0], o2[v][1]);
         }
+        // the final state in the working precision, for the filter that follows
+        if (last && want_prims == 2) {
+#pragma unroll
+            for (int v = 0; v < 5; v++) st_pair<R>(prim.p[v], i, two, (R)o2[v][0], (R)o2[v][1]);
+        }
         // primitives of the next stage state (updateNonConservedData, Core.cpp:1165-1177)
-        if (want_prims) {
+        if (!last && want_prims == 1) {
             double pr[5][2];
 #pragma unroll
             for (int p = 0; p < 2; p++) {
@@ -509,7 +565,8 @@ __global__ void __launch_bounds__(256) rk_kernel(Grid3 g, RkStage rs, K5<R> k2, 
 
 template <typename R>
 int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], double *const q1[5],
-                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st) {
+                     double *const qk[5], double *const q2[5], R *const prim[5], cudaStream_t st,
+                     bool copy_final) {
     K5<R> k;
     Q5 a, b, c;
     P5<R> P;
@@ -525,7 +582,8 @@ int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], do
     if (rs.scheme == MC3D_RK4) mode = first ? RKM_RK4_1 : (last ? RKM_RK4_LAST : RKM_RK4_MID);
     else if (rs.scheme == MC3D_TVDRK3) mode = first ? RKM_TVD_1 : (last ? RKM_TVD_3 : RKM_TVD_2);
     else mode = first ? RKM_2N_1 : (last ? RKM_2N_LAST : RKM_2N_MID);
-    const int grid = grid_for((g.n() + 1) / 2, 256), wp = prim != nullptr;
+    // 1: primitives of the next stage state; 2 (last stage): the final state in R
+    const int grid = grid_for((g.n() + 1) / 2, 256), wp = prim == nullptr ? 0 : (copy_final ? 2 : 1);
     switch (mode) {
         case RKM_RK4_1: rk_kernel<R, RKM_RK4_1><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
         case RKM_RK4_MID: rk_kernel<R, RKM_RK4_MID><<<grid, 256, 0, st>>>(g, rs, k, a, b, c, P, wp); break;
@@ -664,7 +722,7 @@ int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cud
     template int launch_vreman<R>(const Grid3 &, const R *const[5], const R *const[12], const Metrics<R> &,       \
                                   const FluxParams &, R *, cudaStream_t);                                         \
     template int launch_rk_update<R>(const Grid3 &, const RkStage &, const R *const[5], double *const[5],         \
-                                     double *const[5], double *const[5], R *const[5], cudaStream_t);              \
+                                     double *const[5], double *const[5], R *const[5], cudaStream_t, bool);        \
     template int launch_to_real<R>(const Grid3 &, const double *const[5], R *const[5], cudaStream_t);             \
     template int launch_cfl<R>(const Grid3 &, const double *const[5], const Metrics<R> &, const double[3],        \
                                unsigned long long *, cudaStream_t);

@@ -62,6 +62,7 @@ struct mc3d_solver_s {
     double *acc = nullptr;
     int host_time_step = 0;
     int filter_time_step = 0;
+    bool tc_fresh = false;   // tC holds the working-precision copy of the state the filter reads
     int lsldd_half = 1;
     long long stages = 0;
     long long launches = 0;
@@ -191,12 +192,16 @@ static int filter_state(mc3d_solver s, double *const in[5], double *const out[5]
     if (s->prec == MC3D_FP64) {
         for (int v = 0; v < 5; v++) src0[v] = in[v];
     } else {
-        R *dst[5];
-        for (int v = 0; v < 5; v++) dst[v] = (R *)s->tC[v];
-        s->launches++;
-        if ((rc = tic(s, KC_TOREAL, (8.0 + sizeof(R)) * 5 * (double)s->g.n()))) return rc;
-        if ((rc = launch_to_real<R>(s->g, in, dst, s->stream))) return rc;
-        if ((rc = toc(s))) return rc;
+        // the last RK stage of a filtered step already wrote the copy
+        if (!s->tc_fresh) {
+            R *dst[5];
+            for (int v = 0; v < 5; v++) dst[v] = (R *)s->tC[v];
+            s->launches++;
+            if ((rc = tic(s, KC_TOREAL, (8.0 + sizeof(R)) * 5 * (double)s->g.n()))) return rc;
+            if ((rc = launch_to_real<R>(s->g, in, dst, s->stream))) return rc;
+            if ((rc = toc(s))) return rc;
+        }
+        s->tc_fresh = false;
         for (int v = 0; v < 5; v++) src0[v] = s->tC[v];
     }
     if ((rc = sweep<R>(s, order[0], ops[order[0]], 5, src0, s->tA, EPI_STORE, nullptr, nullptr, true))) return rc;
@@ -534,15 +539,21 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
 template <typename R>
 static int one_step(mc3d_solver s) {
     int rc;
-    // preStep: calcDtFromCFL on the current state (Core.cpp:189-237)
+    // preStep: calcDtFromCFL on the current state (Core.cpp:189-237), fused into
+    // the primitives of stage 1, which read the same state
     Metrics<R> m = metrics_of<R>(s);
-    s->launches += 2;
-    if ((rc = tic(s, KC_CFL, 5.0 * 8 * (double)s->g.n()))) return rc;
-    if ((rc = launch_cfl<R>(s->g, s->q1, m, s->dxi, &s->ts->umax_bits, s->stream))) return rc;
-    int first = s->host_time_step == s->cfg.time_step0;
-    if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
-    if ((rc = toc(s))) return rc;
+    const int first = s->host_time_step == s->cfg.time_step0;
+    {
+        R *prim[5];
+        for (int v = 0; v < 5; v++) prim[v] = (R *)s->prim[v];
+        s->launches += 2;
+        if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 5.0 * sizeof(R)) * (double)s->g.n()))) return rc;
+        if ((rc = launch_primitives_cfl<R>(s->g, s->q1, prim, m, s->dxi, &s->ts->umax_bits, s->stream))) return rc;
+        if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
+        if ((rc = toc(s))) return rc;
+    }
     s->host_time_step++;
+    const bool filter_now = s->host_time_step % s->cfg.filter_step == 0;
 
     int scheme = s->cfg.rk_type;
     int ns = scheme == MC3D_RK4 ? 4 : scheme == MC3D_TVDRK3 ? 3 : scheme == MC3D_KENRK4 ? 5 : (s->lsldd_half == 1 ? 5 : 6);
@@ -550,8 +561,8 @@ static int one_step(mc3d_solver s) {
         // stage 1 works on q1 (filtered at the end of the previous step); later
         // stages on qk, whose primitives the RK update of the previous stage
         // already wrote unless a sub-step filter changed qk since
-        if (st == 1 || s->cfg.substep_filtering)
-            if ((rc = primitives<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
+        if (st > 1 && s->cfg.substep_filtering)
+            if ((rc = primitives<R>(s, s->qk))) return rc;
         if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
         if ((rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
         RkStage rs{};
@@ -575,6 +586,10 @@ static int one_step(mc3d_solver s) {
             pw[v] = (R *)s->prim[v];
         }
         bool fuse_prims = st < ns && !s->cfg.substep_filtering;
+        // last stage of a filtered step (FP32 path): the filter's working copy
+        const bool copy_final = st == ns && filter_now && s->prec != MC3D_FP64;
+        if (copy_final)
+            for (int v = 0; v < 5; v++) pw[v] = (R *)s->tC[v];
         s->launches++;
         {
             // reads k2 and the FP64 registers the scheme touches, writes the updated ones
@@ -582,11 +597,14 @@ static int one_step(mc3d_solver s) {
             if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
             else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
             else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
-            if (fuse_prims) b += 5.0 * sizeof(R);
+            if (fuse_prims || copy_final) b += 5.0 * sizeof(R);
             if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
         }
-        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, fuse_prims ? pw : nullptr, s->stream))) return rc;
+        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, (fuse_prims || copy_final) ? pw : nullptr,
+                                      s->stream, copy_final)))
+            return rc;
         if ((rc = toc(s))) return rc;
+        if (copy_final) s->tc_fresh = true;
         bool last = st == ns;
         if (last || s->cfg.substep_filtering)
             if ((rc = filter_conserved<R>(s, last))) return rc;

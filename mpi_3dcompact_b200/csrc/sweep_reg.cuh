@@ -185,8 +185,10 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
     }
 }
 
-template <int DIR, typename R, int KIND, int H, int L>
-__global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op, SweepBatch<R> b, int epi,
+// E: the caller's operation (EpiMode), compiled into the kernel so that each
+// instantiation carries one epilogue only.
+template <int DIR, typename R, int KIND, int H, int L, int E>
+__global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op, SweepBatch<R> b,
                                                         RhsFinalArgs<R> rf, int pass_y, int pass_z, int pass_x) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
@@ -538,35 +540,19 @@ __global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op
         }
         __syncwarp();
         const int tile0 = blockIdx.x * W;
-#define MC3D_REGX(E) reg_copy_out<R, E, L>(b, rf, f, tile0, N, nl, a, lane, tile)
-        switch (epi) {
-            case EPI_STORE: MC3D_REGX(EPI_STORE); break;
-            case EPI_STORE_NEG: MC3D_REGX(EPI_STORE_NEG); break;
-            case EPI_SUB: MC3D_REGX(EPI_SUB); break;
-            case EPI_STORE_F64: MC3D_REGX(EPI_STORE_F64); break;
-            case EPI_RHS_FINAL: MC3D_REGX(EPI_RHS_FINAL); break;
-        }
-#undef MC3D_REGX
+        reg_copy_out<R, E, L>(b, rf, f, tile0, N, nl, a, lane, tile);
     } else if (t.active) {
         const int off0 = (int)t.base + a * (int)t.stride;
-#define MC3D_REGS(E) reg_store_rows<R, E, L>(b, rf, f, off0, (int)t.stride, y)
-        switch (epi) {
-            case EPI_STORE: MC3D_REGS(EPI_STORE); break;
-            case EPI_STORE_NEG: MC3D_REGS(EPI_STORE_NEG); break;
-            case EPI_SUB: MC3D_REGS(EPI_SUB); break;
-            case EPI_STORE_F64: MC3D_REGS(EPI_STORE_F64); break;
-            case EPI_RHS_FINAL: MC3D_REGS(EPI_RHS_FINAL); break;
-        }
-#undef MC3D_REGS
+        reg_store_rows<R, E, L>(b, rf, f, off0, (int)t.stride, y);
     }
 }
 
-template <int DIR, typename R, int KIND, int H, int L>
-static int launch_reg_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
-                          const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
+template <int DIR, typename R, int KIND, int H, int L, int E>
+static int launch_reg_epi(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, const RhsFinalArgs<R> &rf,
+                          int px, int py, int pz, cudaStream_t st) {
     const int S = op.N / L;
     size_t smem = reg_smem_bytes(DIR, op.N, S, sizeof(R));
-    auto kern = sweep_reg_kernel<DIR, R, KIND, H, L>;
+    auto kern = sweep_reg_kernel<DIR, R, KIND, H, L, E>;
     static thread_local int configured_smem = -1;
     if ((int)smem > configured_smem) {
         MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -577,9 +563,26 @@ static int launch_reg_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBat
     else if (DIR == 1) tiles = ((g.Nx + W - 1) / W) * g.Nz;
     else tiles = (int)(((long long)g.Nx * g.Ny + W - 1) / W);
     dim3 grid(tiles, b.nf);
-    kern<<<grid, 32 * S, smem, st>>>(g, op, b, epi, rf, py, pz, px);
+    kern<<<grid, 32 * S, smem, st>>>(g, op, b, rf, py, pz, px);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
+}
+
+// Epilogues instantiated per operator family: derivatives (H <= 3) store,
+// negate, accumulate or assemble k2; filters (H >= 4) store in the working
+// precision or in FP64. Other combinations go to the shared-memory kernels.
+template <int DIR, typename R, int KIND, int H, int L>
+static int launch_reg_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
+                          const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
+    if (epi == EPI_STORE) return launch_reg_epi<DIR, R, KIND, H, L, EPI_STORE>(g, op, b, rf, px, py, pz, st);
+    if constexpr (H <= 3) {
+        if (epi == EPI_STORE_NEG) return launch_reg_epi<DIR, R, KIND, H, L, EPI_STORE_NEG>(g, op, b, rf, px, py, pz, st);
+        if (epi == EPI_SUB) return launch_reg_epi<DIR, R, KIND, H, L, EPI_SUB>(g, op, b, rf, px, py, pz, st);
+        if (epi == EPI_RHS_FINAL) return launch_reg_epi<DIR, R, KIND, H, L, EPI_RHS_FINAL>(g, op, b, rf, px, py, pz, st);
+    } else {
+        if (epi == EPI_STORE_F64) return launch_reg_epi<DIR, R, KIND, H, L, EPI_STORE_F64>(g, op, b, rf, px, py, pz, st);
+    }
+    return MC3D_ERR_CONFIG;
 }
 
 // Register-resident launch for direction DIR; returns MC3D_ERR_CONFIG (without
