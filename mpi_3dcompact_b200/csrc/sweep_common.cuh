@@ -73,7 +73,7 @@ __device__ __forceinline__ TileGeom tile_geom(const Grid3 &g, int tile, int lane
 }
 
 template <int DIR>
-__device__ __forceinline__ int tile_count(const Grid3 &g) {
+__host__ __device__ __forceinline__ int tile_count(const Grid3 &g) {
     if (DIR == 0) return (int)(((long long)g.Ny * g.Nz + W - 1) / W);
     if (DIR == 1) return ((g.Nx + W - 1) / W) * g.Nz;
     return (int)(((long long)g.Nx * g.Ny + W - 1) / W);
