@@ -11,7 +11,10 @@ One "step" is one time step of the solver (LSLDDRK4 alternates 5- and
 independent replicas (one per rank, different seeds): the path has no
 exchange between GPUs. Rank 0 prints one JSON line.
 
-At N = 1 the line also carries "learned_sgs": a posteriori 128^3 LES of the
+At N = 1 the line also carries "cylinder": the curvilinear O-grid configuration
+(512 x 256 x 64 around a cylinder, wall + cylindrical sponge, PADE6 with
+boundary closures, KENRK4, COMPACT10, DSM, FP32-bulk, metrics computed on the
+GPU from the mesh), and "learned_sgs": a posteriori 128^3 LES of the
 same HIT (PADE6, RK4, COMPACT10 alpha_f = 0.49, FP32-bulk, 500 steps) with
 the learned closure shipped in mpi_3dcompact_b200/data (DSM with GLOBAL
 averaging as its fallback) against DSM and against no model: device time per
@@ -203,6 +206,82 @@ def energy_spectrum(torch, q):
     return torch.bincount(shell.reshape(-1), weights=e.reshape(-1), minlength=n + 1)[: n // 2 + 1].cpu().numpy()
 
 
+def cylinder_block(args, local):
+    """The O-grid cylinder configuration: grid-point RK stages per second with
+    DSM (GLOBAL averaging), and whether the configuration's LOCAL averaging
+    stays finite."""
+    import numpy as np
+    import torch
+
+    import mpi_3dcompact_b200 as m
+
+    Nx, Ny, Nz = 512, 256, 64
+    r0, r1, span = 0.5, 30.0, 2.0
+    ratio = (r1 / r0) ** (1.0 / (Ny - 1))
+    th = 2 * math.pi * np.arange(Nx) / Nx
+    r = r0 * ratio ** np.arange(Ny)
+    zz = span * np.arange(Nz) / Nz
+    Z, Rr, TH = np.meshgrid(zz, r, th, indexing="ij")
+    x, y, z = Rr * np.cos(TH), -Rr * np.sin(TH), Z      # (theta clockwise, r, z): J > 0
+    rng = np.random.default_rng(3)
+    shp = (Nz, Ny, Nx)
+    ic = [np.ones(shp), 0.2 * (1 + 0.01 * rng.standard_normal(shp)), 0.002 * rng.standard_normal(shp),
+          0.002 * rng.standard_normal(shp), np.full(shp, 1 / 1.4)]
+
+    def make(avg):
+        opt = m.Options(grid=(Nx, Ny, Nz), fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="KENRK4",
+                        mu_ref=0.2 / 3900.0, les="DSM", les_avg=avg, dsm_test_filter=1, precision=m.FP32BULK,
+                        bc=(m.PERIODIC_SOLVE, m.DIRICHLET_SOLVE, m.PERIODIC_SOLVE),
+                        bc_kind=("INTERNALLY_PERIODIC", "INTERNALLY_PERIODIC", "ADIABATIC_WALL", "SPONGE",
+                                 "PERIODIC", "PERIODIC"),
+                        sponge={"kind": "CYLINDRICAL", "strength": 1.0, "orient": 2, "cyl_axis": [0.0, 0.0, 0.0],
+                                "rmin": 0.8 * r1},
+                        periodic_disp=((0, 0, 0), (0, 0, 0), (0, 0, span)), cfl=0.5)
+        s = m.CurvilinearCSolver(opt, device=local)
+        t0 = time.perf_counter()
+        s.set_mesh(x, y, z)
+        tm = time.perf_counter() - t0
+        s.set_sponge(m.sponge_sigma(opt, x, y, z))
+        s.set_initial_conditions(*ic)
+        return s, tm
+
+    s, metrics_s = make("GLOBAL")
+    s.step(3)
+    s.sync()
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st0 = s.info()["stages"]
+    e0.record(stream)
+    s.step(args.cyl_steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    stages = s.info()["stages"] - st0
+    del s
+    sl, _ = make("LOCAL")
+    local_steps = None
+    for k in range(1, 4):
+        sl.step(1)
+        try:
+            sl.info()
+        except Exception:
+            local_steps = k
+            break
+    del sl
+    return {
+        "workload": "O-grid cylinder 512 (theta, periodic) x 256 (r 0.5..30, geometric) x 64 (z periodic, span 2), "
+                    "M 0.2, Re_D 3900, adiabatic wall, cylindrical sponge r > 24, PADE6 + boundary closures, KENRK4, "
+                    "COMPACT10 alpha_f=0.49, DSM (DSMTESTFILTER=1), FP32-bulk, 1% seeded velocity perturbation",
+        "metric": UNIT, "value": Nx * Ny * Nz * stages / (ms * 1e-3), "ms_per_step": ms / args.cyl_steps,
+        "steps": args.cyl_steps, "averaging": "GLOBAL",
+        "metrics_on_gpu_s": metrics_s,
+        "local_averaging_nonfinite_after_steps": local_steps,
+        "note": "the configuration's LOCAL averaging divides by a locally filtered M_ij M_ij and goes non-finite "
+                "in the reference's own solver as well (128x64x32 O-grid, first step); radial ratio "
+                "(30/0.5)^(1/255) = %.4f so that r ends at 30" % ratio,
+    }
+
+
 def learned_sgs_block(args, local):
     """A posteriori LES with the learned closure against DSM and no model."""
     import numpy as np
@@ -362,7 +441,13 @@ def run_ours(args):
     if not args.no_e2e:
         se = m.CurvilinearCSolver(m.Options(grid=n, mu_ref=mu, precision=m.FP32BULK, **SCHEME), device=local)
         se.set_box_metrics(2 * math.pi)
-        host_ic = [np.ascontiguousarray(a) for a in ic]
+
+        def pinned():
+            return torch.empty(ic[0].shape, dtype=torch.float64, pin_memory=True).numpy()
+        host_ic = [pinned() for _ in range(5)]        # the initial condition in pinned host memory
+        for a, b in zip(host_ic, ic):
+            a[...] = b
+        out = [pinned() for _ in range(5)]
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
@@ -370,7 +455,7 @@ def run_ours(args):
         for _ in range(args.steps):
             se.step(1)
             se.info()                                # per-step device -> host read of time step / dt
-        out = se.conserved()                         # device -> host (FP64 conserved state)
+        se.conserved(out=out)                        # device -> host (FP64 conserved state)
         wall = time.perf_counter() - t0
         barrier()
         st_e = se.info()["stages"]
@@ -387,6 +472,9 @@ def run_ours(args):
     les = None
     if ws == 1 and not args.no_learned_sgs:
         les = learned_sgs_block(args, local)
+    cyl = None
+    if ws == 1 and not args.no_cylinder:
+        cyl = cylinder_block(args, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -419,7 +507,7 @@ def run_ours(args):
         "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
         "fp32_vs_fp64_rel_l2": err,
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk, "learned_sgs": les,
+        "clocks": clk, "cylinder": cyl, "learned_sgs": les,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -436,6 +524,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned-sgs", action="store_true")
+    ap.add_argument("--no-cylinder", action="store_true")
+    ap.add_argument("--cyl-steps", type=int, default=5)
     ap.add_argument("--les-steps", type=int, default=LES_STEPS)
     args = ap.parse_args()
     if args.warmup < 3:

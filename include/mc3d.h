@@ -122,6 +122,13 @@ typedef struct mc3d_config {
     int from_restart, only_grid_from_restart, sponge_avg_from_restart;
     char restart_file[512];
     char sponge_avg_file[512];
+    /* [STATS] (src/Options.hpp:194-201, :392-417): running statistics updated
+     * every stats_interval steps (default 5); stats_avg_type is STATSAVGTYPE
+     * (MC3D_AVG_*: only XI1/XI3 average, as Stats::doAveraging does) */
+    int velocity_stats, thermo_stats, stats_interval, stats_avg_type;
+    int velocity_stats_from_restart, thermo_stats_from_restart;
+    char velocity_stats_file[512];
+    char thermo_stats_file[512];
 } mc3d_config;
 
 /* ---- configuration ---- */
@@ -303,6 +310,25 @@ int mc3d_solver_read_sponge_avg(mc3d_solver s, const char *path);
  * working directory) every DUMPSTEP steps and at the end. */
 int mc3d_solver_start(mc3d_solver s);
 int mc3d_solver_run(mc3d_solver s, const char *dir);
+
+/* ---- running statistics (Stats, src/Stats.cpp:127-347) ---- */
+/* With cfg.velocity_stats / thermo_stats set, every mc3d_solver_step updates
+ * them after each stats_interval-th time step (postStep): time-weighted
+ * means, RMS and Reynolds stresses of U, V, W of the filtered state and of
+ * rho (the unfiltered rho2), p, T, with the XI1/XI3 index averaging of
+ * STATSAVGTYPE; FP64 on the device. Copies to host: velocity[9] = UAVG, VAVG,
+ * WAVG, URMS, VRMS, WRMS, UVREY, UWREY, VWREY; thermo[6] = RHOAVG, RHORMS,
+ * PAVG, PRMS, TAVG, TRMS (NULL arrays skipped); weights[2] = the two
+ * accumulated time weights. */
+int mc3d_solver_get_stats(mc3d_solver s, double *const velocity[9], double *const thermo[6], double weights[2]);
+/* VelocityStats / ThermoStats files (Stats::dumpStatsFields, src/Stats.cpp:3-125:
+ * the weight, then the fields, x fastest); NULL paths: "VelocityStats.<step>"
+ * and "ThermoStats.<step>" in the working directory. mc3d_solver_run writes
+ * them with each SolutionDump. */
+int mc3d_solver_dump_stats(mc3d_solver s, const char *velocity_path, const char *thermo_path);
+/* Statistics from such files (STATS.*STATSFROMRESTART, Stats.hpp:60-266);
+ * NULL paths are skipped; mc3d_solver_start reads the configured ones. */
+int mc3d_solver_read_stats(mc3d_solver s, const char *velocity_path, const char *thermo_path);
 
 /* Time-step counter, time, last dt and total RK stages run (synchronises). */
 int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, long long *stages);

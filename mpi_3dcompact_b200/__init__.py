@@ -208,7 +208,7 @@ class Options:
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
                  dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3,
-                 periodic_disp=None, max_time_step=None, max_time=None, dump_step=None):
+                 periodic_disp=None, max_time_step=None, max_time=None, dump_step=None, stats=None):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -236,6 +236,11 @@ class Options:
             c.max_time = float(max_time)
         if dump_step is not None:
             c.dump_step = int(dump_step)
+        if stats:   # {"velocity": bool, "thermo": bool, "avg": "NONE"|"XI1_AVG"|..., "interval": int}
+            c.velocity_stats = int(bool(stats.get("velocity", True)))
+            c.thermo_stats = int(bool(stats.get("thermo", True)))
+            c.stats_avg_type = _AVG[stats.get("avg", "NONE")]
+            c.stats_interval = int(stats.get("interval", 5))
         # BC.PERIODICDISP{X,Y,Z}_{X,Y,Z} (row = face pair, column = component)
         for d in range(3):
             for e in range(3):
@@ -402,6 +407,27 @@ class CurvilinearCSolver:
         DUMPSTEP steps and at the end (mc3d_solver_run)."""
         N.check(N.host_lib().mc3d_solver_run(self._h, None if directory is None else str(directory).encode()))
 
+    def stats(self):
+        """Running statistics (Stats): {"velocity": [UAVG, VAVG, WAVG, URMS, VRMS,
+        WRMS, UVREY, UWREY, VWREY] or None, "thermo": [RHOAVG, RHORMS, PAVG, PRMS,
+        TAVG, TRMS] or None, "weights": (velocity, thermo)}."""
+        c = self.opt.c
+        v = [np.empty(self.shape) for _ in range(9)] if c.velocity_stats else None
+        t = [np.empty(self.shape) for _ in range(6)] if c.thermo_stats else None
+        pv = (C.POINTER(C.c_double) * 9)(*[N.dptr(a) for a in v]) if v else None
+        pt = (C.POINTER(C.c_double) * 6)(*[N.dptr(a) for a in t]) if t else None
+        w = (C.c_double * 2)()
+        N.check(N.host_lib().mc3d_solver_get_stats(self._h, pv, pt, w))
+        return {"velocity": v, "thermo": t, "weights": (w[0], w[1])}
+
+    def dump_stats(self, velocity_path=None, thermo_path=None):
+        enc = (lambda p: None if p is None else str(p).encode())
+        N.check(N.host_lib().mc3d_solver_dump_stats(self._h, enc(velocity_path), enc(thermo_path)))
+
+    def read_stats(self, velocity_path=None, thermo_path=None):
+        enc = (lambda p: None if p is None else str(p).encode())
+        N.check(N.host_lib().mc3d_solver_read_stats(self._h, enc(velocity_path), enc(thermo_path)))
+
     def metrics(self):
         """The FP64 metrics J, J11..J33 the solver holds (10 arrays (Nz, Ny, Nx))."""
         out = [np.empty(self.shape) for _ in range(10)]
@@ -439,9 +465,14 @@ class CurvilinearCSolver:
     def step(self, n=1):
         N.check(N.host_lib().mc3d_solver_step(self._h, int(n)))
 
-    def conserved(self):
-        """Host copies of rho1, rhoU1, rhoV1, rhoW1, rhoE1."""
-        out = [np.empty(self.shape) for _ in range(5)]
+    def conserved(self, out=None):
+        """Host copies of rho1, rhoU1, rhoV1, rhoW1, rhoE1 (into `out`, five
+        C-contiguous float64 arrays of the grid's shape, e.g. pinned buffers)."""
+        if out is None:
+            out = [np.empty(self.shape) for _ in range(5)]
+        for a in out:
+            if a.shape != self.shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("conserved(out=...) needs C-contiguous float64 arrays of the grid's shape")
         N.check(N.host_lib().mc3d_solver_get_conserved(self._h, *[N.dptr(a) for a in out]))
         return out
 

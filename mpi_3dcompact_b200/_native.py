@@ -49,7 +49,11 @@ class Config(C.Structure):
                 ("wall_velocity", (C.c_double * 2) * 6), ("mlp_fallback_frac", C.c_double),
                 ("periodic_disp", (C.c_double * 3) * 3), ("dump_step", C.c_int),
                 ("from_restart", C.c_int), ("only_grid_from_restart", C.c_int), ("sponge_avg_from_restart", C.c_int),
-                ("restart_file", C.c_char * 512), ("sponge_avg_file", C.c_char * 512)]
+                ("restart_file", C.c_char * 512), ("sponge_avg_file", C.c_char * 512),
+                ("velocity_stats", C.c_int), ("thermo_stats", C.c_int), ("stats_interval", C.c_int),
+                ("stats_avg_type", C.c_int), ("velocity_stats_from_restart", C.c_int),
+                ("thermo_stats_from_restart", C.c_int), ("velocity_stats_file", C.c_char * 512),
+                ("thermo_stats_file", C.c_char * 512)]
 
 
 _lib = None
@@ -87,6 +91,9 @@ def host_lib():
             "mc3d_solver_dump_sponge_avg": (ip, [vp, C.c_char_p]),
             "mc3d_solver_read_sponge_avg": (ip, [vp, C.c_char_p]),
             "mc3d_solver_start": (ip, [vp]),
+            "mc3d_solver_get_stats": (ip, [vp, C.POINTER(C.POINTER(dp)), C.POINTER(C.POINTER(dp)), C.POINTER(dp)]),
+            "mc3d_solver_dump_stats": (ip, [vp, C.c_char_p, C.c_char_p]),
+            "mc3d_solver_read_stats": (ip, [vp, C.c_char_p, C.c_char_p]),
             "mc3d_solver_run": (ip, [vp, C.c_char_p]),
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),
             "mc3d_solver_set_initial_device": (ip, [vp] + [vp] * 5),

@@ -80,6 +80,11 @@ int mc3d_config_default(mc3d_config *c) {
     c->dump_step = 1000;   // src/Options.hpp:237
     c->from_restart = c->only_grid_from_restart = c->sponge_avg_from_restart = 0;
     c->restart_file[0] = c->sponge_avg_file[0] = '\0';
+    c->velocity_stats = c->thermo_stats = 0;
+    c->stats_interval = 5;   // src/Options.hpp:417
+    c->stats_avg_type = MC3D_AVG_NONE;
+    c->velocity_stats_from_restart = c->thermo_stats_from_restart = 0;
+    c->velocity_stats_file[0] = c->thermo_stats_file[0] = '\0';
     return MC3D_OK;
 }
 
@@ -280,7 +285,32 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
             }
         }
         // [STATS], [LES]
-        parse_enum(ini, "STATS.STATSAVGTYPE", {{"NONE", 0}, {"XI1_AVG", 1}, {"XI2_AVG", 2}, {"XI3_AVG", 3}, {"LOCAL", 4}, {"GLOBAL", 5}});
+        c->stats_avg_type = parse_enum(ini, "STATS.STATSAVGTYPE",
+                                       {{"NONE", MC3D_AVG_NONE}, {"XI1_AVG", MC3D_AVG_XI1}, {"XI2_AVG", MC3D_AVG_XI2},
+                                        {"XI3_AVG", MC3D_AVG_XI3}, {"LOCAL", MC3D_AVG_LOCAL}, {"GLOBAL", MC3D_AVG_GLOBAL}});
+        if (ini.has("STATS.VELOCITYSTATS")) c->velocity_stats = parse_bool("VELOCITYSTATS", ini.get("STATS.VELOCITYSTATS"));
+        if (ini.has("STATS.THERMOSTATS")) c->thermo_stats = parse_bool("THERMOSTATS", ini.get("STATS.THERMOSTATS"));
+        if (ini.has("STATS.INTERVAL")) c->stats_interval = parse_int("INTERVAL", ini.get("STATS.INTERVAL"));
+        if (c->stats_interval <= 0) throw CfgError{"STATS.INTERVAL must be positive"};
+        {
+            const char *flag[2] = {"STATS.VELOCITYSTATSFROMRESTART", "STATS.THERMOSTATSFROMRESTART"};
+            const char *file[2] = {"STATS.VELOCITYSTATSFILENAME", "STATS.THERMOSTATSFILENAME"};
+            const char *what[2] = {"velocityStatsFromRestart", "thermoStatsFromRestart"};
+            int on[2] = {c->velocity_stats, c->thermo_stats};
+            int *from[2] = {&c->velocity_stats_from_restart, &c->thermo_stats_from_restart};
+            char *dst[2] = {c->velocity_stats_file, c->thermo_stats_file};
+            for (int k = 0; k < 2; k++) {
+                if (!on[k]) continue;
+                if (!ini.has(flag[k])) throw CfgError{std::string(what[k]) + " not specified, NEEDS TO BE SPECIFED"};
+                *from[k] = parse_bool(flag[k], ini.get(flag[k])) ? 1 : 0;
+                if (*from[k]) {
+                    if (!ini.has(file[k])) throw CfgError{std::string(file[k]) + " not specified, NEEDS TO BE SPECIFED"};
+                    const std::string fn = ini.get(file[k]);
+                    if (fn.size() >= 512) throw CfgError{std::string(file[k]) + " is too long"};
+                    std::snprintf(dst[k], 512, "%s", fn.c_str());
+                }
+            }
+        }
         c->les_model = parse_enum(ini, "LES.LESMODEL", {{"NOMODEL", MC3D_NOMODEL}, {"NONE", MC3D_NOMODEL},
                                                         {"VREMAN", MC3D_VREMAN}, {"DSM", MC3D_DSM},
                                                         {"MLP", MC3D_MLPSGS}});

@@ -174,6 +174,9 @@ struct FluxParams {
 
 template <typename R>
 int launch_primitives(const Grid3 &g, const double *const q[5], R *const prim[5], cudaStream_t st);
+// conserved state of primitive fields rho, U, V, W, p (device); *bad |= 1 on a
+// non-finite value or rho <= 0
+int launch_init_conserved(long long n, const double *const prim[5], double *const q[5], int *bad, cudaStream_t st);
 // primitives and the CFL wave-speed maximum (atomicMax into *umax, as launch_cfl)
 template <typename R>
 int launch_primitives_cfl(const Grid3 &g, const double *const q[5], R *const prim[5], const Metrics<R> &m,
@@ -355,6 +358,20 @@ struct MetOut9 {
     double *p[9];
 };
 int launch_tpb_rhs(const Grid3 &g, int dir, const double *f, const TpbArgs &a, double *rhs, cudaStream_t st);
+
+// ---- running statistics (stats.cu) ------------------------------------------
+struct StatsIn {
+    const double *q[5];      // filtered conserved state (rho1 .. rhoE1)
+    const double *rho2;      // density before the filter
+};
+struct StatsOut {
+    double *p[9];
+};
+// One Stats::updateStatsFields with time increment dt and old weights ovw /
+// otw: v = UAVG, VAVG, WAVG, URMS, VRMS, WRMS, UVREY, UWREY, VWREY; t = RHOAVG,
+// RHORMS, PAVG, PRMS, TAVG, TRMS.
+int launch_stats_update(const Grid3 &g, const StatsIn &in, double *const v[9], double *const t[6], double dt,
+                        double ovw, double otw, int avg_type, int vel, int thermo, cudaStream_t st);
 
 // ---- checkpoint files (checkpoint.cpp) ----------------------------------------
 int write_solution_dump(const char *path, int time_step, double time, int Nx, int Ny, int Nz,

@@ -599,6 +599,35 @@ int launch_rk_update(const Grid3 &g, const RkStage &rs, const R *const k2[5], do
     return MC3D_OK;
 }
 
+// setInitialConditions without walls (src/CurvilinearCSolver_BC.cpp:31-59):
+// rhoU = rho U, ..., rhoE = p/(gamma-1) + (1/2) rho |U|^2, rounded as the host
+// restatement does; *bad is set where the state is non-finite or rho <= 0.
+__global__ void init_conserved_kernel(long long n, const double *__restrict__ rho, const double *__restrict__ U,
+                                      const double *__restrict__ V, const double *__restrict__ W,
+                                      const double *__restrict__ p, Q5 q, int *bad) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double r = rho[i], u = U[i], v = V[i], w = W[i], pp = p[i];
+        const double e = __dadd_rn(__ddiv_rn(pp, GAMMA - 1.0),
+                                   __dmul_rn(__dmul_rn(0.5, r), __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)),
+                                                                        __dmul_rn(w, w))));
+        q.p[0][i] = r;
+        q.p[1][i] = __dmul_rn(r, u);
+        q.p[2][i] = __dmul_rn(r, v);
+        q.p[3][i] = __dmul_rn(r, w);
+        q.p[4][i] = e;
+        if (!isfinite(e) || !(r > 0)) atomicOr(bad, 1);
+    }
+}
+
+int launch_init_conserved(long long n, const double *const prim[5], double *const q[5], int *bad, cudaStream_t st) {
+    Q5 o;
+    for (int v = 0; v < 5; v++) o.p[v] = q[v];
+    init_conserved_kernel<<<(int)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(
+        n, prim[0], prim[1], prim[2], prim[3], prim[4], o, bad);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
 template <typename R>
 __global__ void to_real_kernel(Grid3 g, Q5 src, K5<R> dst) {
     long long n = g.n();

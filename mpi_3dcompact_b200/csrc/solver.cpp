@@ -63,6 +63,10 @@ struct mc3d_solver_s {
     int host_time_step = 0;
     int filter_time_step = 0;
     bool tc_fresh = false;   // tC holds the working-precision copy of the state the filter reads
+    // running statistics (FP64): velocity (9) and thermodynamic (6) fields, their
+    // time weights and the time of the last update
+    double *stv[9] = {}, *stt[6] = {};
+    double st_vw = 0.0, st_tw = 0.0, st_prev = 0.0;
     int lsldd_half = 1;
     long long stages = 0;
     long long launches = 0;
@@ -692,6 +696,11 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
     for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
     if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, &s->mu_sgs, n * rb);
+    if (c.velocity_stats)
+        for (int k = 0; k < 9 && !rc; k++) rc = salloc(s, (void **)&s->stv[k], n * sizeof(double));
+    if (c.thermo_stats)
+        for (int k = 0; k < 6 && !rc; k++) rc = salloc(s, (void **)&s->stt[k], n * sizeof(double));
+    s->st_prev = c.time0;   // Stats takes the solver's time at construction (src/Stats.hpp:58)
     if (c.les_model == MC3D_MLPSGS) {
         if (!rc) rc = salloc(s, (void **)&s->mlp_flag, sizeof(int));
         if (!rc) {
@@ -1046,6 +1055,41 @@ static int set_initial_impl(mc3d_solver s, const double *rho, const double *U, c
     if (!s->have_metrics) return fail(MC3D_ERR_CONFIG, "set the metrics before the initial condition");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
     size_t n = (size_t)s->g.n();
+    if (!s->have_walls) {
+        // no wall treatment: the conserved state is formed on the device. Host
+        // primitives go through the (not yet used) q2 registers.
+        if (s->have_sponge && !s->sigma_set)
+            return fail(MC3D_ERR_CONFIG, "set the sponge strength before the initial condition");
+        const double *src[5] = {rho, U, V, W, p};
+        const double *dp[5];
+        for (int v = 0; v < 5; v++) {
+            if (device) {
+                dp[v] = src[v];
+            } else {
+                MC3D_CUDA_TRY(cudaMemcpyAsync(s->q2[v], src[v], n * 8, cudaMemcpyHostToDevice, s->stream));
+                dp[v] = s->q2[v];
+            }
+        }
+        int *bad = s->ts ? &s->ts->nonfinite : nullptr;
+        MC3D_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), s->stream));
+        int rc = launch_init_conserved((long long)n, dp, s->q1, bad, s->stream);
+        if (rc) return rc;
+        for (int v = 0; v < 5; v++) {
+            MC3D_CUDA_TRY(cudaMemsetAsync(s->k2[v], 0, n * (s->prec == MC3D_FP64 ? 8 : 4), s->stream));
+            // the sponge target starts as the initial state (src/CurvilinearCSolver_BC.cpp:325-341)
+            if (s->have_sponge)
+                MC3D_CUDA_TRY(cudaMemcpyAsync(s->spg_avg[v], s->q1[v], n * 8, cudaMemcpyDeviceToDevice, s->stream));
+        }
+        int hbad = 0;
+        MC3D_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        if (hbad) {
+            MC3D_CUDA_TRY(cudaMemset(bad, 0, sizeof(int)));
+            return fail(MC3D_ERR_NONFINITE, "non-finite or non-positive initial state");
+        }
+        s->initialized = true;
+        return MC3D_OK;
+    }
     // conserved state of setInitialConditions (src/CurvilinearCSolver_BC.cpp:31-59)
     std::vector<double> h[5];
     std::vector<double> hr(n), hu(n), hv(n), hw(n), hp(n);
@@ -1174,6 +1218,123 @@ int mc3d_solver_set_sponge_avg(mc3d_solver s, const double *const avg[5]) {
     return MC3D_OK;
 }
 
+// postStep's Stats::updateStatsFields (src/CurvilinearCSolver.hpp:362-364,
+// src/Stats.cpp:127-223): time weights from the device time, fields on device.
+static int stats_update(mc3d_solver s) {
+    mc3d::TimeState t;
+    MC3D_CUDA_TRY(cudaMemcpyAsync(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const double dt = t.time - s->st_prev;
+    if (dt != 0.0) {
+        mc3d::StatsIn in{};
+        for (int v = 0; v < 5; v++) in.q[v] = s->q1[v];
+        in.rho2 = s->q2[0];
+        double *v9[9], *t6[6];
+        for (int k = 0; k < 9; k++) v9[k] = s->stv[k];
+        for (int k = 0; k < 6; k++) t6[k] = s->stt[k];
+        int rc = mc3d::launch_stats_update(s->g, in, v9, t6, dt, s->st_vw, s->st_tw, s->cfg.stats_avg_type,
+                                           s->cfg.velocity_stats, s->cfg.thermo_stats, s->stream);
+        if (rc) return rc;
+        if (s->cfg.velocity_stats) s->st_vw += dt;
+        if (s->cfg.thermo_stats) s->st_tw += dt;
+    }
+    s->st_prev = t.time;
+    return MC3D_OK;
+}
+
+int mc3d_solver_get_stats(mc3d_solver s, double *const velocity[9], double *const thermo[6], double weights[2]) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    const size_t bytes = (size_t)s->g.n() * sizeof(double);
+    for (int k = 0; k < 9 && velocity; k++) {
+        if (!velocity[k]) continue;
+        if (!s->cfg.velocity_stats) return fail(MC3D_ERR_CONFIG, "VELOCITYSTATS is off");
+        MC3D_CUDA_TRY(cudaMemcpyAsync(velocity[k], s->stv[k], bytes, cudaMemcpyDeviceToHost, s->stream));
+    }
+    for (int k = 0; k < 6 && thermo; k++) {
+        if (!thermo[k]) continue;
+        if (!s->cfg.thermo_stats) return fail(MC3D_ERR_CONFIG, "THERMOSTATS is off");
+        MC3D_CUDA_TRY(cudaMemcpyAsync(thermo[k], s->stt[k], bytes, cudaMemcpyDeviceToHost, s->stream));
+    }
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (weights) {
+        weights[0] = s->st_vw;
+        weights[1] = s->st_tw;
+    }
+    return MC3D_OK;
+}
+
+// Stats::dumpStatsFields (src/Stats.cpp:3-125): the weight, then the fields
+static int write_stats_file(const std::string &path, double w, double *const *dev, int nf, size_t n,
+                            cudaStream_t st) {
+    std::vector<double> h(n);
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return fail(MC3D_ERR_ARG, "cannot write " + path);
+    bool ok = std::fwrite(&w, sizeof(double), 1, f) == 1;
+    for (int k = 0; k < nf && ok; k++) {
+        if (cudaMemcpyAsync(h.data(), dev[k], n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            std::fclose(f);
+            return fail(MC3D_ERR_CUDA, "stats download failed");
+        }
+        ok = std::fwrite(h.data(), sizeof(double), n, f) == n;
+    }
+    std::fclose(f);
+    return ok ? MC3D_OK : fail(MC3D_ERR_ARG, "write failed: " + path);
+}
+
+static int read_stats_file(const std::string &path, double &w, double *const *dev, int nf, size_t n,
+                           cudaStream_t st) {
+    std::vector<double> h(n);
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return fail(MC3D_ERR_ARG, "ERROR: Couldn't open file " + path);
+    bool ok = std::fread(&w, sizeof(double), 1, f) == 1;
+    for (int k = 0; k < nf && ok; k++) {
+        ok = std::fread(h.data(), sizeof(double), n, f) == n;
+        if (ok && (cudaMemcpyAsync(dev[k], h.data(), n * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                   cudaStreamSynchronize(st) != cudaSuccess)) {
+            std::fclose(f);
+            return fail(MC3D_ERR_CUDA, "stats upload failed");
+        }
+    }
+    std::fclose(f);
+    return ok ? MC3D_OK : fail(MC3D_ERR_ARG, "short file: " + path);
+}
+
+int mc3d_solver_dump_stats(mc3d_solver s, const char *velocity_path, const char *thermo_path) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    int ts;
+    int rc = mc3d_solver_info(s, &ts, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    const size_t n = (size_t)s->g.n();
+    if (s->cfg.velocity_stats) {
+        const std::string p = velocity_path ? velocity_path : "VelocityStats." + std::to_string(ts);
+        if ((rc = write_stats_file(p, s->st_vw, s->stv, 9, n, s->stream))) return rc;
+    }
+    if (s->cfg.thermo_stats) {
+        const std::string p = thermo_path ? thermo_path : "ThermoStats." + std::to_string(ts);
+        if ((rc = write_stats_file(p, s->st_tw, s->stt, 6, n, s->stream))) return rc;
+    }
+    return MC3D_OK;
+}
+
+int mc3d_solver_read_stats(mc3d_solver s, const char *velocity_path, const char *thermo_path) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.n();
+    int rc;
+    if (velocity_path) {
+        if (!s->cfg.velocity_stats) return fail(MC3D_ERR_CONFIG, "VELOCITYSTATS is off");
+        if ((rc = read_stats_file(velocity_path, s->st_vw, s->stv, 9, n, s->stream))) return rc;
+    }
+    if (thermo_path) {
+        if (!s->cfg.thermo_stats) return fail(MC3D_ERR_CONFIG, "THERMOSTATS is off");
+        if ((rc = read_stats_file(thermo_path, s->st_tw, s->stt, 6, n, s->stream))) return rc;
+    }
+    return MC3D_OK;
+}
+
 int mc3d_solver_step(mc3d_solver s, int nsteps) {
     if (!s) return fail(MC3D_ERR_ARG, "null solver");
     if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no initial condition");
@@ -1182,6 +1343,8 @@ int mc3d_solver_step(mc3d_solver s, int nsteps) {
     for (int i = 0; i < nsteps; i++) {
         int rc = s->prec == MC3D_FP64 ? one_step<double>(s) : one_step<float>(s);
         if (rc) return rc;
+        if ((s->cfg.velocity_stats || s->cfg.thermo_stats) && s->host_time_step % s->cfg.stats_interval == 0)
+            if ((rc = stats_update(s))) return rc;
     }
     return MC3D_OK;
 }
@@ -1225,6 +1388,7 @@ int mc3d_solver_conserved_device(mc3d_solver s, double *ptrs[5]) {
 static int set_time_origin(mc3d_solver s, int time_step, double time) {
     s->cfg.time_step0 = time_step;
     s->cfg.time0 = time;
+    s->st_prev = time;
     s->host_time_step = time_step;
     s->filter_time_step = 0;
     s->lsldd_half = 1;
@@ -1364,6 +1528,9 @@ int mc3d_solver_start(mc3d_solver s) {
     if (s->cfg.from_restart || s->cfg.only_grid_from_restart)
         rc = mc3d_solver_restart(s, s->cfg.restart_file, s->cfg.only_grid_from_restart);
     if (!rc && s->cfg.sponge_avg_from_restart) rc = mc3d_solver_read_sponge_avg(s, s->cfg.sponge_avg_file);
+    if (!rc && (s->cfg.velocity_stats_from_restart || s->cfg.thermo_stats_from_restart))
+        rc = mc3d_solver_read_stats(s, s->cfg.velocity_stats_from_restart ? s->cfg.velocity_stats_file : nullptr,
+                                    s->cfg.thermo_stats_from_restart ? s->cfg.thermo_stats_file : nullptr);
     return rc;
 }
 
@@ -1374,6 +1541,9 @@ int mc3d_solver_run(mc3d_solver s, const char *dir) {
         int rc = mc3d_solver_dump(s, (base + "SolutionDump." + std::to_string(ts)).c_str(), nullptr, nullptr, nullptr);
         if (!rc && s->have_sponge)
             rc = mc3d_solver_dump_sponge_avg(s, (base + "SpongeAvgDump." + std::to_string(ts)).c_str());
+        if (!rc && (s->cfg.velocity_stats || s->cfg.thermo_stats))
+            rc = mc3d_solver_dump_stats(s, (base + "VelocityStats." + std::to_string(ts)).c_str(),
+                                        (base + "ThermoStats." + std::to_string(ts)).c_str());
         return rc;
     };
     bool end = false;

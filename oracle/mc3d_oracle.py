@@ -567,6 +567,8 @@ class Config:
     # full BC.PERIODICDISP{X,Y,Z}_{X,Y,Z} table (row = face pair, column =
     # component); None: periodic_box on the diagonal
     periodic_disp: tuple = None
+    # [STATS]: dict(velocity=bool, thermo=bool, avg="NONE"|"XI1_AVG"|"XI2_AVG"|"XI3_AVG", interval=int)
+    stats: dict = None
 
     def kinds(self):
         if self.bc_kind is not None:
@@ -1008,6 +1010,7 @@ class Oracle:
         self.state = State(q1=q1, qk=[z.copy() for _ in range(5)], k2=[z.copy() for _ in range(5)],
                            q2=[z.copy() for _ in range(5)], time=time, time_step=time_step)
         self.start_step = time_step
+        self.stats = Stats(self.cfg.stats, rho0.shape, time) if self.cfg.stats else None
         T0 = p0 / (rho0 * R_GAS)
         self._prims = (U0, V0, W0, p0, T0, self.cfg.mu_ref * np.power(T0, 0.76), np.sqrt(GAMMA * p0 / rho0))
         if self.walls:
@@ -1029,6 +1032,14 @@ class Oracle:
         self._prims = primitives(src, self.cfg.mu_ref)
 
     def step(self):
+        """One time step then postStep's statistics update every STATS.INTERVAL
+        steps (src/CurvilinearCSolver.hpp:355-375)."""
+        self._advance()
+        st = self.state
+        if self.stats is not None and st.time_step % self.stats.interval == 0:
+            self.stats.update(st.time, st.q1, st.q2)
+
+    def _advance(self):
         """One time step (or the LSLDDRK4 two-step pair's half): src/RK4.hpp:127-178,
         src/TVDRK3.hpp, src/KenRK4.hpp:154-217, src/LSLDDRK4.hpp:324-459."""
         c, st = self.cfg, self.state
@@ -1307,6 +1318,104 @@ def cube_metrics(N, L=2.0 * math.pi):
     z = np.zeros(shp)
     d = np.full(shp, 1.0 / L)
     return [np.full(shp, 1.0 / L ** 3), d, z, z, z, d.copy(), z, z, z, d.copy()]
+
+
+class Stats:
+    """Running statistics of the solver (src/Stats.hpp:30-266, src/Stats.cpp:127-347):
+    time-weighted means, RMS and Reynolds stresses of U, V, W and means / RMS of
+    rho, p, T, updated every `interval` time steps in postStep
+    (src/CurvilinearCSolver.hpp:362-364). Velocity, p and T are those of the
+    filtered state; rho is rho2, the state before the filter (Stats.hpp:45)."""
+
+    def __init__(self, spec, shape, time):
+        self.spec = dict(spec)
+        self.velocity = self.spec.get("velocity", True)
+        self.thermo = self.spec.get("thermo", True)
+        self.avg = self.spec.get("avg", "NONE")
+        self.interval = self.spec.get("interval", 1)
+        self.prev_time = time                    # Stats.hpp:58
+        self.vw = 0.0
+        self.tw = 0.0
+        z = np.zeros(shape)
+        # UAVG, VAVG, WAVG, URMS, VRMS, WRMS, UVREY, UWREY, VWREY (the dump order)
+        self.v = [z.copy() for _ in range(9)]
+        # RHOAVG, RHORMS, PAVG, PRMS, TAVG, TRMS
+        self.t = [z.copy() for _ in range(6)]
+
+    def _average(self, phi):
+        """Stats::doAveraging (src/Stats.cpp:225-347): index means along xi1 or
+        xi3 summed term by term as phi/N; the XI2 branch averages the solver's
+        scratch array instead of phi (:268-296), which leaves phi unchanged;
+        other types do nothing."""
+        if self.avg == "XI1_AVG":
+            n = phi.shape[2]
+            acc = np.zeros(phi.shape[:2])
+            for i in range(n):
+                acc = acc + phi[:, :, i] / float(n)
+            return np.repeat(acc[:, :, None], n, axis=2)
+        if self.avg == "XI3_AVG":
+            n = phi.shape[0]
+            acc = np.zeros(phi.shape[1:])
+            for k in range(n):
+                acc = acc + phi[k] / float(n)
+            return np.repeat(acc[None], n, axis=0)
+        return phi
+
+    def update(self, time, q1, q2):
+        """Stats::updateStatsFields (src/Stats.cpp:127-223)."""
+        dt = time - self.prev_time
+        rho1, ru, rv, rw, re = q1
+        U, V, W = ru / rho1, rv / rho1, rw / rho1
+        p = (GAMMA - 1) * (re - 0.5 * rho1 * (U * U + V * V + W * W))
+        T = p / (rho1 * R_GAS)
+        if self.velocity and dt != 0.0:
+            ow, nw = self.vw, self.vw + dt
+            UA, VA, WA, UR, VR, WR, UV, UW, VW = self.v
+            UR = (ow * (UR * UR + UA * UA) + dt * U * U) / nw
+            VR = (ow * (VR * VR + VA * VA) + dt * V * V) / nw
+            WR = (ow * (WR * WR + WA * WA) + dt * W * W) / nw
+            UV = (ow * (UV + UA * VA) + dt * U * V) / nw
+            UW = (ow * (UW + UA * WA) + dt * U * W) / nw
+            VW = (ow * (VW + VA * WA) + dt * V * W) / nw
+            UA = (ow * UA + dt * U) / nw
+            VA = (ow * VA + dt * V) / nw
+            WA = (ow * WA + dt * W) / nw
+            UR, VR, WR, UV, UW, VW, UA, VA, WA = [self._average(a) for a in (UR, VR, WR, UV, UW, VW, UA, VA, WA)]
+            UR = np.sqrt(np.abs(UR - UA * UA))
+            VR = np.sqrt(np.abs(VR - VA * VA))
+            WR = np.sqrt(np.abs(WR - WA * WA))
+            UV = UV - UA * VA
+            UW = UW - UA * WA
+            VW = VW - VA * WA
+            self.v = [UA, VA, WA, UR, VR, WR, UV, UW, VW]
+            self.vw = nw
+        if self.thermo and dt != 0.0:
+            rho = q2[0]
+            ow, nw = self.tw, self.tw + dt
+            RA, RR, PA, PR, TA, TR = self.t
+            RR = (ow * (RR * RR + RA * RA) + dt * rho * rho) / nw
+            PR = (ow * (PR * PR + PA * PA) + dt * p * p) / nw
+            TR = (ow * (TR * TR + TA * TA) + dt * T * T) / nw
+            RA = (ow * RA + dt * rho) / nw
+            PA = (ow * PA + dt * p) / nw
+            TA = (ow * TA + dt * T) / nw
+            RR, PR, TR, RA, PA, TA = [self._average(a) for a in (RR, PR, TR, RA, PA, TA)]
+            RR = np.sqrt(np.abs(RR - RA * RA))
+            PR = np.sqrt(np.abs(PR - PA * PA))
+            TR = np.sqrt(np.abs(TR - TA * TA))
+            self.t = [RA, RR, PA, PR, TA, TR]
+            self.tw = nw
+        self.prev_time = time
+
+
+def parse_stats_file(raw: bytes, nfields, shape):
+    """VelocityStats / ThermoStats as Stats::dumpStatsFields writes them
+    (src/Stats.cpp:3-125): the weight, then the fields, x fastest."""
+    a = np.frombuffer(raw, dtype=np.float64)
+    n = int(np.prod(shape))
+    if a.size != 1 + nfields * n:
+        raise ValueError("not a stats file of this size")
+    return float(a[0]), [a[1 + k * n:1 + (k + 1) * n].reshape(shape).copy() for k in range(nfields)]
 
 
 def run(cfg: Config, ic, nsteps, metrics=None, sigma=None, time=0.0, time_step=0):

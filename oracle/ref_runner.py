@@ -54,9 +54,16 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
         "ONLYGRIDFROMRESTART = false",
         "SPONGEAVGFROMRESTART = false",
         "[STATS]",
-        "VELOCITYSTATS = false",
-        "THERMOSTATS = false",
-        "STATSAVGTYPE = NONE",
+    ]
+    st = getattr(cfg, "stats", None)
+    if st:
+        lines += [f"VELOCITYSTATS = {'true' if st.get('velocity', True) else 'false'}",
+                  f"THERMOSTATS = {'true' if st.get('thermo', True) else 'false'}",
+                  "VELOCITYSTATSFROMRESTART = false", "THERMOSTATSFROMRESTART = false",
+                  f"STATSAVGTYPE = {st.get('avg', 'NONE')}", f"INTERVAL = {st.get('interval', 1)}"]
+    else:
+        lines += ["VELOCITYSTATS = false", "THERMOSTATS = false", "STATSAVGTYPE = NONE"]
+    lines += [
         "[BC]",
     ]
     for ax, name in enumerate("XYZ"):
@@ -119,7 +126,7 @@ def _read_fields(path, N, nf, header=8):
 
 
 def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coords=None, dump_to=None,
-               restart_from=None, sponge_dump_to=None):
+               restart_from=None, sponge_dump_to=None, stats_to=None):
     """Run the reference solver for `nsteps` time steps from primitive ICs
     (rho, U, V, W, p). `coords` = (x, y, z) selects a mesh from file. Returns
     (conserved fields, header dict). `dump_to`: copy the SolutionDump.<step>
@@ -128,7 +135,9 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
     to this path. `restart_from`: start from a SolutionDump file instead of
     `ic` (mesh, conserved state, time step and time from the file, as
     src/MPI_3DCompact.cpp:80-271 restarts); nsteps then counts from its step.
-    `sponge_dump_to`: copy the SpongeAvgDump.<step> written with it."""
+    `sponge_dump_to`: copy the SpongeAvgDump.<step> written with it;
+    `stats_to`: (velocity, thermo) paths for the VelocityStats.<step> /
+    ThermoStats.<step> files written with it (cfg.stats enabled)."""
     if not available():
         raise RuntimeError("oracle/_ref/mc3d_ref is not built (make -C oracle)")
     if restart_from is not None:
@@ -155,6 +164,10 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
             shutil.copy(os.path.join(d, f"SolutionDump.{int(hdr[0])}"), dump_to)
         if sponge_dump_to is not None:
             shutil.copy(os.path.join(d, f"SpongeAvgDump.{int(hdr[0])}"), sponge_dump_to)
+        if stats_to is not None:
+            for name, dst in zip(("VelocityStats", "ThermoStats"), stats_to):
+                if dst is not None:
+                    shutil.copy(os.path.join(d, f"{name}.{int(hdr[0])}"), dst)
         st = os.path.join(d, "step_times.txt")
         step_s = [float(x) for x in open(st).read().split()] if os.path.exists(st) else []
     info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall,

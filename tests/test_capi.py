@@ -151,6 +151,17 @@ def test_ini_mlp_closure_keys(tmp_path):
         m.Options.from_ini(_write(tmp_path, txt.replace("[LES]", "[LES]\nMLPFALLBACKFRAC = 2")))
 
 
+def test_ini_stats_keys(tmp_path):
+    txt = HIT_IN.replace("VELOCITYSTATS = 0", "VELOCITYSTATS = 1\nVELOCITYSTATSFROMRESTART = TRUE\n"
+                         "VELOCITYSTATSFILENAME = VelocityStats.100")
+    c = m.Options.from_ini(_write(tmp_path, txt)).c
+    assert c.velocity_stats == 1 and c.thermo_stats == 0 and c.stats_interval == 1
+    assert c.stats_avg_type == N.AVG_XI3 and c.velocity_stats_from_restart == 1
+    assert c.velocity_stats_file.decode() == "VelocityStats.100"
+    with pytest.raises(N.Mc3dError):   # the restart flag is required once the stats are on
+        m.Options.from_ini(_write(tmp_path, HIT_IN.replace("VELOCITYSTATS = 0", "VELOCITYSTATS = 1")))
+
+
 def test_ini_lesmodel_none_alias(tmp_path):
     c = m.Options.from_ini(_write(tmp_path, HIT_IN.replace("LESMODEL = VREMAN", "LESMODEL = NONE"))).c
     assert c.les_model == N.NOMODEL

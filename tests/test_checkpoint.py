@@ -108,3 +108,50 @@ def test_ini_restart_keys(tmp_path):
     p.write_text(textwrap.dedent(bad))
     with pytest.raises(N.Mc3dError):
         m.Options.from_ini(p)
+
+
+def _moments(v, t):
+    """Means, mean squares and mean products of the stats fields: the
+    well-conditioned quantities behind RMS = sqrt(|<x^2> - <x>^2|)."""
+    m = [v[0], v[1], v[2], t[0], t[2], t[4]]
+    m += [v[3 + k] ** 2 + v[k] ** 2 for k in range(3)]
+    m += [t[2 * k + 1] ** 2 + t[2 * k] ** 2 for k in range(3)]
+    m += [v[6 + k] + v[a] * v[b] for k, (a, b) in enumerate(((0, 1), (0, 2), (1, 2)))]
+    return m
+
+
+def stats_errors(v, t, weights, name):
+    gold = np.load(G.os.path.join(G.HERE, "stats.npz"))
+    gv = [gold[f"{name}_v{k}"] for k in range(9)]
+    gt = [gold[f"{name}_t{k}"] for k in range(6)]
+    gw = gold[f"{name}_weights"]
+    e_w = float(np.max(np.abs(np.asarray(weights) - gw) / np.abs(gw)))
+    e_m = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(_moments(v, t), _moments(gv, gt)))
+    return e_w, e_m
+
+
+@pytest.mark.parametrize("name", list(G.STATS_CASES))
+def test_oracle_stats_match_reference(name):
+    """Stats::updateStatsFields restated against the reference's own stats
+    files: weights and moments to 1e-13."""
+    cfg, ic, n = G.stats_case(name)
+    o = O.Oracle(cfg, O.cube_metrics(cfg.N))
+    o.init(*ic)
+    for _ in range(n):
+        o.step()
+    e_w, e_m = stats_errors(o.stats.v, o.stats.t, [o.stats.vw, o.stats.tw], name)
+    assert e_w <= 1e-13 and e_m <= 1e-13, (e_w, e_m)
+
+
+def test_oracle_stats_xi2_leaves_fields_unaveraged():
+    """The reference's XI2 branch averages its scratch array, not the field."""
+    runs = []
+    for avg in ("XI2_AVG", "NONE"):
+        c, ic, n = G.stats_case("mixed_rk4_xi2")
+        c.stats = dict(avg=avg, interval=1)
+        o = O.Oracle(c, O.cube_metrics(c.N))
+        o.init(*ic)
+        for _ in range(n):
+            o.step()
+        runs.append(o.stats.v + o.stats.t)
+    assert all(np.array_equal(a, b) for a, b in zip(*runs))
