@@ -311,6 +311,16 @@ int mc3d_solver_read_sponge_avg(mc3d_solver s, const char *path);
 int mc3d_solver_start(mc3d_solver s);
 int mc3d_solver_run(mc3d_solver s, const char *dir);
 
+/* ---- diagnostic hooks of the reference drivers, as device reductions ---- */
+/* One turbdata.out line of the HIT driver (tests/hit/Samtaney_D4/MPI_3DCompact.cpp:370-555)
+ * for the current state: out = time, tau = sqrt(2 pi)/k0/u', Re_lambda, Mt,
+ * dissipation / mean rho, u', Kolmogorov length, rho', dilatation', vorticity',
+ * mean rho|u|^2 (the driver passes k0 = 8). */
+int mc3d_solver_turbdata(mc3d_solver s, double k0, double out[11]);
+/* The cylinder driver's surface data (src/MPI_3DCompact.cpp:408-485): p, U, V,
+ * W on the j = 0 face averaged over xi3, Nx values each (host arrays). */
+int mc3d_solver_wall_span_average(mc3d_solver s, double *p, double *U, double *V, double *W);
+
 /* ---- running statistics (Stats, src/Stats.cpp:127-347) ---- */
 /* With cfg.velocity_stats / thermo_stats set, every mc3d_solver_step updates
  * them after each stats_interval-th time step (postStep): time-weighted

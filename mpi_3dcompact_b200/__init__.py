@@ -420,6 +420,20 @@ class CurvilinearCSolver:
         N.check(N.host_lib().mc3d_solver_get_stats(self._h, pv, pt, w))
         return {"velocity": v, "thermo": t, "weights": (w[0], w[1])}
 
+    def turbdata(self, k0=8.0):
+        """One turbdata.out line of the HIT driver for the current state: time,
+        tau, Re_lambda, Mt, dissipation, u', Kolmogorov length, rho', dil',
+        vorticity', mean rho|u|^2."""
+        out = (C.c_double * 11)()
+        N.check(N.host_lib().mc3d_solver_turbdata(self._h, float(k0), out))
+        return list(out)
+
+    def wall_span_average(self):
+        """p, U, V, W on the j = 0 face averaged over xi3 (Nx values each)."""
+        out = [np.empty(self.shape[2]) for _ in range(4)]
+        N.check(N.host_lib().mc3d_solver_wall_span_average(self._h, *[N.dptr(a) for a in out]))
+        return out
+
     def dump_stats(self, velocity_path=None, thermo_path=None):
         enc = (lambda p: None if p is None else str(p).encode())
         N.check(N.host_lib().mc3d_solver_dump_stats(self._h, enc(velocity_path), enc(thermo_path)))

@@ -93,6 +93,8 @@ def host_lib():
             "mc3d_solver_start": (ip, [vp]),
             "mc3d_solver_get_stats": (ip, [vp, C.POINTER(C.POINTER(dp)), C.POINTER(C.POINTER(dp)), C.POINTER(dp)]),
             "mc3d_solver_dump_stats": (ip, [vp, C.c_char_p, C.c_char_p]),
+            "mc3d_solver_turbdata": (ip, [vp, dp, C.POINTER(dp)]),
+            "mc3d_solver_wall_span_average": (ip, [vp] + [C.POINTER(dp)] * 4),
             "mc3d_solver_read_stats": (ip, [vp, C.c_char_p, C.c_char_p]),
             "mc3d_solver_run": (ip, [vp, C.c_char_p]),
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),

@@ -373,6 +373,17 @@ struct StatsOut {
 int launch_stats_update(const Grid3 &g, const StatsIn &in, double *const v[9], double *const t[6], double dt,
                         double ovw, double otw, int avg_type, int vel, int thermo, cudaStream_t st);
 
+// ---- diagnostic hooks of the reference drivers (hooks.cu) --------------------
+constexpr int TURB_NSUM = 9;   // block sums of the HIT statistics, pass 1
+// pass 1: sums of rho, mu, dissipation, |u|^2/3, (u_x^2+v_y^2+w_z^2)/3, |u|^2,
+// c, u_x^2, rho |u|^2; pass 2: sums of (rho - mean_rho)^2, dil^2, |omega|^2.
+// partial[k * nblocks + block]
+template <typename R>
+int launch_turb_sums(const Grid3 &g, const R *const prim[5], const R *const d[12], const Metrics<R> &m,
+                     double mu_ref, int pass, double mean_rho, double *partial, int nblocks, cudaStream_t st);
+// out[4][Nx]: span averages of p, U, V, W on the j = 0 face
+int launch_wall_span_average(const Grid3 &g, const double *const q[5], double *out, cudaStream_t st);
+
 // ---- checkpoint files (checkpoint.cpp) ----------------------------------------
 int write_solution_dump(const char *path, int time_step, double time, int Nx, int Ny, int Nz,
                         const double *const fields[8]);

@@ -31,6 +31,11 @@ struct P5w {
 };
 
 template <typename R>
+struct P5c {
+    const R *p[5];
+};
+
+template <typename R>
 struct DerivPtrs12c {
     const R *p[12];
 };

@@ -67,6 +67,7 @@ struct mc3d_solver_s {
     // time weights and the time of the last update
     double *stv[9] = {}, *stt[6] = {};
     double st_vw = 0.0, st_tw = 0.0, st_prev = 0.0;
+    double *hook_scratch = nullptr;   // block partials of the diagnostic reductions
     int lsldd_half = 1;
     long long stages = 0;
     long long launches = 0;
@@ -1239,6 +1240,97 @@ static int stats_update(mc3d_solver s) {
         if (s->cfg.thermo_stats) s->st_tw += dt;
     }
     s->st_prev = t.time;
+    return MC3D_OK;
+}
+
+}  // extern "C"
+
+namespace mc3d {
+constexpr int HOOK_BLOCKS = 148 * 4;
+
+template <typename R>
+static int turbdata_impl(mc3d_solver s, double k0, double out[11]) {
+    int rc;
+    if (!s->hook_scratch && (rc = salloc(s, (void **)&s->hook_scratch, (size_t)TURB_NSUM * HOOK_BLOCKS * 8))) return rc;
+    // the driver's computeGradient of U, V, W of the current (filtered) state
+    if ((rc = primitives<R>(s, s->q1))) return rc;
+    for (int d = 0; d < 3; d++) {
+        void *o[3] = {s->der[0 + d], s->der[3 + d], s->der[6 + d]};
+        if ((rc = sweep<R>(s, d, s->dop[d], 3, s->prim + 1, o, EPI_STORE, nullptr, nullptr, false))) return rc;
+    }
+    const R *pr[5], *dd[12];
+    for (int v = 0; v < 5; v++) pr[v] = (const R *)s->prim[v];
+    for (int k = 0; k < 12; k++) dd[k] = (const R *)s->der[k];
+    Metrics<R> m = metrics_of<R>(s);
+    const double nall = (double)s->g.n();
+    std::vector<double> part((size_t)TURB_NSUM * HOOK_BLOCKS);
+    double sum1[TURB_NSUM] = {0}, sum2[3] = {0};
+    for (int pass = 1; pass <= 2; pass++) {
+        const double mean_rho = sum1[0] / nall;
+        if ((rc = launch_turb_sums<R>(s->g, pr, dd, m, s->cfg.mu_ref, pass, mean_rho, s->hook_scratch, HOOK_BLOCKS,
+                                      s->stream)))
+            return rc;
+        const int nk = pass == 1 ? TURB_NSUM : 3;
+        MC3D_CUDA_TRY(cudaMemcpyAsync(part.data(), s->hook_scratch, (size_t)nk * HOOK_BLOCKS * 8,
+                                      cudaMemcpyDeviceToHost, s->stream));
+        MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        for (int k = 0; k < nk; k++)
+            for (int b = 0; b < HOOK_BLOCKS; b++) (pass == 1 ? sum1 : sum2)[k] += part[(size_t)k * HOOK_BLOCKS + b];
+    }
+    TimeState t;
+    MC3D_CUDA_TRY(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+    // tests/hit/Samtaney_D4/MPI_3DCompact.cpp:522-555
+    const double meanRho = sum1[0] / nall, meanMu = sum1[1] / nall;
+    const double meanTurbDiss = (sum1[2] / nall) / meanRho;
+    const double uprime = std::sqrt(sum1[3] / nall), uiprime = std::sqrt(sum1[4] / nall);
+    const double urms = std::sqrt(sum1[5] / nall), meanSOS = sum1[6] / nall;
+    const double meanKE = sum1[8] / nall;
+    const double rhoprime = std::sqrt(sum2[0] / nall), dilprime = std::sqrt(sum2[1] / nall);
+    const double vortprime = std::sqrt(sum2[2] / nall);
+    const double meanNu = meanMu / meanRho;
+    const double taylorMicro = uprime / uiprime;
+    const double pi = 3.14159265358979323846;
+    out[0] = t.time;
+    out[1] = std::sqrt(2 * pi) / k0 / uprime;
+    out[2] = uprime * taylorMicro / meanNu;
+    out[3] = urms / meanSOS;
+    out[4] = meanTurbDiss;
+    out[5] = uprime;
+    out[6] = std::pow(std::pow(meanNu, 3.0) / meanTurbDiss, 0.25);
+    out[7] = rhoprime;
+    out[8] = dilprime;
+    out[9] = vortprime;
+    out[10] = meanKE;
+    return MC3D_OK;
+}
+}  // namespace mc3d
+
+extern "C" {
+
+int mc3d_solver_turbdata(mc3d_solver s, double k0, double out[11]) {
+    if (!s || !out) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no state");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    return s->prec == MC3D_FP64 ? mc3d::turbdata_impl<double>(s, k0, out) : mc3d::turbdata_impl<float>(s, k0, out);
+}
+
+int mc3d_solver_wall_span_average(mc3d_solver s, double *p, double *U, double *V, double *W) {
+    if (!s || !p || !U || !V || !W) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no state");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    int rc;
+    const size_t need = (size_t)4 * s->g.Nx;
+    double *buf = nullptr;
+    MC3D_CUDA_TRY(cudaMallocAsync((void **)&buf, need * 8, s->stream));
+    if ((rc = mc3d::launch_wall_span_average(s->g, s->q1, buf, s->stream))) {
+        cudaFreeAsync(buf, s->stream);
+        return rc;
+    }
+    double *dst[4] = {p, U, V, W};
+    for (int k = 0; k < 4; k++)
+        MC3D_CUDA_TRY(cudaMemcpyAsync(dst[k], buf + (size_t)k * s->g.Nx, s->g.Nx * 8, cudaMemcpyDeviceToHost, s->stream));
+    MC3D_CUDA_TRY(cudaFreeAsync(buf, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return MC3D_OK;
 }
 

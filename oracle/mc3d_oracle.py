@@ -1408,6 +1408,55 @@ class Stats:
         self.prev_time = time
 
 
+def hit_turbdata(o: "Oracle", k0=8.0):
+    """The HIT driver's turbdata.out line (tests/hit/Samtaney_D4/MPI_3DCompact.cpp:
+    370-555) for the oracle's current state: gradients of U, V, W of the filtered
+    state, Cartesian components through the metrics (:410-420), dissipation
+    2 mu S^d_ij du_i/dx_j (:430-450), block means (:480-495, :511-515) and the
+    11 output values (:522-552)."""
+    st = o.state
+    U, V, W, p, T, mu, sos = primitives(st.q1, o.cfg.mu_ref)
+    rho = st.q1[0]
+    d = [o.grad(f) for f in (U, V, W)]          # d[var][dir]
+    Jm = o.Jm
+    gu = [[Jm[0][b] * d[a][0] + Jm[1][b] * d[a][1] + Jm[2][b] * d[a][2] for b in range(3)] for a in range(3)]
+    dil = gu[0][0] + gu[1][1] + gu[2][2]
+    diss = 0.0
+    for a in range(3):
+        for b in range(3):
+            s = 0.5 * (gu[a][b] + gu[b][a]) - ((1.0 / 3.0) * dil if a == b else 0.0)
+            diss = diss + s * gu[a][b]
+    diss = diss * 2 * mu
+    uvar = U * U + V * V + W * W
+    mean = (lambda f: float(np.mean(f)))
+    meanRho, meanMu = mean(rho), mean(mu)
+    meanTurbDiss = mean(diss) / meanRho
+    uprime, uiprime = math.sqrt(mean(uvar / 3.0)), math.sqrt(mean((gu[0][0] ** 2 + gu[1][1] ** 2 + gu[2][2] ** 2) / 3.0))
+    urms, meanSOS = math.sqrt(mean(uvar)), mean(sos)
+    wx, wy, wz = gu[2][1] - gu[1][2], gu[0][2] - gu[2][0], gu[1][0] - gu[0][1]
+    rhoprime = math.sqrt(mean((rho - meanRho) ** 2))
+    dilprime = math.sqrt(mean(dil * dil))
+    vortprime = math.sqrt(mean(wx * wx + wy * wy + wz * wz))
+    meanNu = meanMu / meanRho
+    taylor = uprime / uiprime
+    return [st.time, math.sqrt(2 * math.pi) / k0 / uprime, uprime * taylor / meanNu, urms / meanSOS, meanTurbDiss,
+            uprime, (meanNu ** 3 / meanTurbDiss) ** 0.25, rhoprime, dilprime, vortprime, mean(rho * uvar)]
+
+
+def wall_span_average(q):
+    """The cylinder driver's surface averages (src/MPI_3DCompact.cpp:408-461):
+    p, U, V, W on the j = 0 face summed as x/Nz over xi3."""
+    U, V, W, p, T, mu, sos = primitives([a[:, 0, :] for a in q], 1.0)
+    nz = q[0].shape[0]
+    out = []
+    for f in (p, U, V, W):
+        acc = np.zeros(f.shape[1])
+        for k in range(nz):
+            acc = acc + f[k] / float(nz)
+        out.append(acc)
+    return out
+
+
 def parse_stats_file(raw: bytes, nfields, shape):
     """VelocityStats / ThermoStats as Stats::dumpStatsFields writes them
     (src/Stats.cpp:3-125): the weight, then the fields, x fastest."""

@@ -1,0 +1,56 @@
+"""GPU tests of the drivers' diagnostic hooks as device reductions: the HIT
+turbdata.out line against the oracle's restatement of the HIT driver's hook on
+the same state, and the cylinder driver's span-averaged wall values against
+the restatement applied to the solver's own state.
+
+Tolerances: 1e-10 relative for the turbdata values (means of products of
+derivatives summed in a different order than numpy's), 1e-14 for the wall
+averages (same summation order)."""
+import math
+
+import numpy as np
+import pytest
+
+import mpi_3dcompact_b200 as m
+from oracle import mc3d_oracle as O
+from tests import helpers as H
+from tests.golden import gen_golden as G
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["pade6_rk4_c10", "mixed_rk4_noncubic"])
+def test_turbdata_matches_restatement(name):
+    cfg, ic, n = H.oracle_config(name)
+    s = m.CurvilinearCSolver(m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF,
+                                       mu_ref=cfg.mu_ref, rk=cfg.rk, cfl=cfg.cfl, les=cfg.les, les_avg=cfg.les_avg))
+    s.set_box_metrics(2.0 * math.pi)
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    got = s.turbdata(8.0)
+    o = O.Oracle(cfg, O.cube_metrics(cfg.N))
+    o.init(*ic)
+    for _ in range(n):
+        o.step()
+    want = O.hit_turbdata(o, 8.0)
+    for k, (a, b) in enumerate(zip(got, want)):
+        assert abs(a - b) <= 1e-10 * abs(b) + 1e-300, (k, a, b)
+
+
+def test_wall_span_average_matches_restatement():
+    name = "ogrid_cyl_sponge_kenrk4"
+    cfg, ic, n, coords = G.wall_case(name)
+    opt = m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                    cfl=cfg.cfl, bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge,
+                    periodic_disp=O.periodic_disp_table(cfg))
+    s = m.CurvilinearCSolver(opt)
+    s.set_mesh(*coords)
+    s.set_sponge(m.sponge_sigma(opt, *coords))
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    got = s.wall_span_average()
+    want = O.wall_span_average(s.conserved())
+    for a, b in zip(got, want):
+        assert np.abs(a - b).max() <= 1e-14 * max(np.abs(b).max(), 1.0)
+    # a no-slip wall: the averaged wall velocity is zero
+    assert max(np.abs(a).max() for a in got[1:]) == 0.0

@@ -161,3 +161,14 @@ def test_oracle_boundary_cases_match_reference_fixtures(name):
     ts, t, dt = gold[f"{name}_info"]
     assert st.time_step == int(ts)
     assert abs(st.dt - dt) <= 1e-13 * abs(dt)
+
+
+def test_oracle_turbdata_of_the_initial_field():
+    """The HIT driver's statistics of the seeded initial field: Mt as scaled,
+    rho' = 0 and mean rho|u|^2 = Mt^2 c^2 with c = 1."""
+    cfg, ic, n = H.oracle_config("pade6_rk4_c10")
+    o = O.Oracle(cfg, O.cube_metrics(cfg.N))
+    o.init(*ic)
+    t = O.hit_turbdata(o, 8.0)
+    assert abs(t[3] - 0.3) < 1e-12 and t[7] < 1e-14
+    assert abs(t[10] - 0.09) < 1e-12
