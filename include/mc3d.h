@@ -129,6 +129,13 @@ typedef struct mc3d_config {
     int velocity_stats_from_restart, thermo_stats_from_restart;
     char velocity_stats_file[512];
     char thermo_stats_file[512];
+    /* SPONGE.AVGTIME (default 1), SPONGE.PINF (default 1/gamma), read with the
+     * sponge (src/Options.hpp:321-322); sponge_relax turns on the relaxation of
+     * the sponge target toward the state after every step
+     * (CurvilinearCSolver::updateSponge, src/CurvilinearCSolver_BC.cpp:843-928),
+     * which the reference leaves commented out in postStep (default 0). No key. */
+    double sponge_avg_time, sponge_p_inf;
+    int sponge_relax;
 } mc3d_config;
 
 /* ---- configuration ---- */

@@ -208,7 +208,8 @@ class Options:
                  ts_type="CONST_CFL", cfl=0.5, dt=-1.0, filter_step=1, substep_filtering=False, les="NOMODEL",
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
                  dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3,
-                 periodic_disp=None, max_time_step=None, max_time=None, dump_step=None, stats=None):
+                 periodic_disp=None, max_time_step=None, max_time=None, dump_step=None, stats=None,
+                 sponge_relax=None):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -259,6 +260,10 @@ class Options:
             for d, v in enumerate(sponge.get("cyl_axis", [0.0] * 3)):
                 c.sponge_cyl_axis[d] = v
             c.sponge_rmin = sponge.get("rmin", 0.0)
+        if sponge_relax:   # {"avg_time": float, "p_inf": float}: updateSponge after every step
+            c.sponge_relax = 1
+            c.sponge_avg_time = float(sponge_relax.get("avg_time", 1.0))
+            c.sponge_p_inf = float(sponge_relax.get("p_inf", 1.0 / 1.4))
         self.c = c
 
     @classmethod

@@ -53,7 +53,8 @@ class Config(C.Structure):
                 ("velocity_stats", C.c_int), ("thermo_stats", C.c_int), ("stats_interval", C.c_int),
                 ("stats_avg_type", C.c_int), ("velocity_stats_from_restart", C.c_int),
                 ("thermo_stats_from_restart", C.c_int), ("velocity_stats_file", C.c_char * 512),
-                ("thermo_stats_file", C.c_char * 512)]
+                ("thermo_stats_file", C.c_char * 512), ("sponge_avg_time", C.c_double),
+                ("sponge_p_inf", C.c_double), ("sponge_relax", C.c_int)]
 
 
 _lib = None

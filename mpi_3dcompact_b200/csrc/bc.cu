@@ -206,4 +206,39 @@ MC3D_BC_INST(float)
 MC3D_BC_INST(double)
 #undef MC3D_BC_INST
 
+// updateSponge (src/CurvilinearCSolver_BC.cpp:843-928): the sponge target
+// relaxes toward the state with eps = 1/(avgT/dt + 1), its energy blended
+// toward the back pressure with epsP = 0.005 (src/SpongeBC.cpp:37); then the
+// points of every SPONGE face take the target state.
+__global__ void sponge_relax_kernel(Grid3 g, Q5d q, Q5d avg, const TimeState *ts, double avg_t, double p_inf,
+                                    int sponge_faces) {
+    const double eps = 1.0 / (avg_t / ts->dt + 1.0);
+    const double eps_p = 0.005;
+    const long long n = g.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double a[5];
+        for (int v = 0; v < 5; v++) a[v] = avg.p[v][i] + eps * (q.p[v][i] - avg.p[v][i]);
+        a[4] = eps_p * a[4] + (1.0 - eps_p) * (p_inf / (GAMMA - 1.0) + 0.5 * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) / a[0]);
+        for (int v = 0; v < 5; v++) avg.p[v][i] = a[v];
+        const long long x = i % g.Nx, y = (i / g.Nx) % g.Ny, z = i / ((long long)g.Nx * g.Ny);
+        const bool on = ((sponge_faces & 1) && x == 0) || ((sponge_faces & 2) && x == g.Nx - 1) ||
+                        ((sponge_faces & 4) && y == 0) || ((sponge_faces & 8) && y == g.Ny - 1) ||
+                        ((sponge_faces & 16) && z == 0) || ((sponge_faces & 32) && z == g.Nz - 1);
+        if (on)
+            for (int v = 0; v < 5; v++) q.p[v][i] = a[v];
+    }
+}
+
+int launch_sponge_relax(const Grid3 &g, double *const q[5], double *const avg[5], const TimeState *ts, double avg_t,
+                        double p_inf, int sponge_faces, cudaStream_t st) {
+    Q5d qq, aa;
+    for (int v = 0; v < 5; v++) {
+        qq.p[v] = q[v];
+        aa.p[v] = avg[v];
+    }
+    sponge_relax_kernel<<<grid_for(g.n(), 256), 256, 0, st>>>(g, qq, aa, ts, avg_t, p_inf, sponge_faces);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
 }  // namespace mc3d

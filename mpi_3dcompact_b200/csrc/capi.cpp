@@ -82,6 +82,9 @@ int mc3d_config_default(mc3d_config *c) {
     c->restart_file[0] = c->sponge_avg_file[0] = '\0';
     c->velocity_stats = c->thermo_stats = 0;
     c->stats_interval = 5;   // src/Options.hpp:417
+    c->sponge_avg_time = 1.0;       // src/Options.hpp:321
+    c->sponge_p_inf = 1.0 / 1.4;    // src/Options.hpp:322
+    c->sponge_relax = 0;
     c->stats_avg_type = MC3D_AVG_NONE;
     c->velocity_stats_from_restart = c->thermo_stats_from_restart = 0;
     c->velocity_stats_file[0] = c->thermo_stats_file[0] = '\0';
@@ -335,6 +338,8 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
             c->sponge_kind = parse_enum(ini, "SPONGE.KIND", {{"RECTILINEAR", MC3D_SPONGE_RECTILINEAR},
                                                              {"CYLINDRICAL", MC3D_SPONGE_CYLINDRICAL}});
             if (ini.has("SPONGE.STRENGTH")) c->sponge_strength = parse_double("STRENGTH", ini.get("SPONGE.STRENGTH"));
+            if (ini.has("SPONGE.AVGTIME")) c->sponge_avg_time = parse_double("AVGTIME", ini.get("SPONGE.AVGTIME"));
+            if (ini.has("SPONGE.PINF")) c->sponge_p_inf = parse_double("PINF", ini.get("SPONGE.PINF"));
             const char *pk[6] = {"SPONGE.RECTX0PERC", "SPONGE.RECTX1PERC", "SPONGE.RECTY0PERC",
                                  "SPONGE.RECTY1PERC", "SPONGE.RECTZ0PERC", "SPONGE.RECTZ1PERC"};
             if (c->sponge_kind == MC3D_SPONGE_RECTILINEAR) {

@@ -125,7 +125,8 @@ __global__ void dsm_mu_taukk_kernel(Grid3 g, DsmMuTaukk<R> a) {
         a.taukk[i] = tk;
         // p of updateNonConservedData less tau_kk / 2, and the temperature of that pressure
         const double u = a.q[1][i] / rho, v = a.q[2][i] / rho, w = a.q[3][i] / rho;
-        const double p = (GAMMA - 1) * (a.q[4][i] - 0.5 * rho * (u * u + v * v + w * w));
+        double p = (GAMMA - 1) * (a.q[4][i] - 0.5 * rho * (u * u + v * v + w * w));
+        if (a.cons_mask && on_faces(g, i, a.cons_mask)) p = (double)a.rho_prim[i] * R_GAS * (double)a.T[i];
         const R pn = (R)p - (R)0.5 * tk;
         a.T[i] = pn / (rhoR * (R)R_GAS);
     }

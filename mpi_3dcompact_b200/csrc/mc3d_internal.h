@@ -170,6 +170,12 @@ struct FluxParams {
     int les;                 // 0 none, 1 Vreman inline, 2 mu_sgs field, 3 DSM fields
     double pr_t;
     int wall_mask;           // bit f: face f is a wall (mu there from the saved temperature)
+    // bit f: on face f the conserved state cons[] differs from the one the
+    // primitives were formed from (a sponge relaxation after the previous
+    // step); the convective terms there take rho, rhoU, rhoV, rhoW, rhoE from
+    // cons[] and p from the primitives, as preStepDerivatives reads them
+    int cons_mask;
+    const double *cons[5];
 };
 
 template <typename R>
@@ -296,6 +302,9 @@ struct DsmMuTaukk {
     R *mu_sgs, *taukk;
     R *T;                 // temperature of p - tau_kk / 2 (written in place)
     int use_taukk;
+    // on the faces in cons_mask p is that of the primitives (rho_prim R T), not of q
+    int cons_mask;
+    const R *rho_prim;
 };
 template <typename R>
 struct DsmPrepK {
@@ -372,6 +381,11 @@ struct StatsOut {
 // RHORMS, PAVG, PRMS, TAVG, TRMS.
 int launch_stats_update(const Grid3 &g, const StatsIn &in, double *const v[9], double *const t[6], double dt,
                         double ovw, double otw, int avg_type, int vel, int thermo, cudaStream_t st);
+
+// updateSponge: relax the sponge target toward q, then set the SPONGE faces
+// (bit f of sponge_faces: face X0, X1, Y0, Y1, Z0, Z1) to it
+int launch_sponge_relax(const Grid3 &g, double *const q[5], double *const avg[5], const TimeState *ts, double avg_t,
+                        double p_inf, int sponge_faces, cudaStream_t st);
 
 // ---- diagnostic hooks of the reference drivers (hooks.cu) --------------------
 constexpr int TURB_NSUM = 9;   // block sums of the HIT statistics, pass 1

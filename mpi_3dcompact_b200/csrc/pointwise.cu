@@ -216,7 +216,7 @@ enum MetForm { MET_FIELD = 0, MET_CONST = 1, MET_DIAG = 2 };
 template <typename R, int MET>
 __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, R Tm, const R (&dd)[12], const R (&mj)[10],
                                            R msgs, R ksgs, R tk, const Metrics<R> &m, const FluxParams &fp, R d1c,
-                                           R iJc, double dvol, R (&o)[15]) {
+                                           R iJc, double dvol, R (&o)[15], const double *qc = nullptr) {
     constexpr bool DIAG = MET == MET_DIAG;
     const R J = MET == MET_FIELD ? mj[0] : m.c[0];
     const R J11 = MET == MET_FIELD ? mj[1] : m.c[1], J12 = MET == MET_FIELD ? mj[2] : m.c[2],
@@ -230,6 +230,16 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, R Tm, cons
     R rhoU = rho * U, rhoV = rho * V, rhoW = rho * W;
     // with DSM, p (and T, mu) carry -tau_kk / 2 but rhoE is the state's (Core.cpp:573-584)
     R rhoE = (fp.les == 3 ? p + (R)0.5 * tk : p) / (R)(GAMMA - 1.0) + (R)0.5 * rho * (U * U + V * V + W * W);
+    if (qc) {
+        // the conserved state where it no longer matches the primitives; with
+        // DSM T there is the temperature of p - tau_kk/2 at the conserved rho
+        rho = (R)qc[0];
+        if (fp.les == 3) p = rho * (R)R_GAS * T;
+        rhoU = (R)qc[1];
+        rhoV = (R)qc[2];
+        rhoW = (R)qc[3];
+        rhoE = (R)qc[4];
+    }
     R mu = mu_of_T(Tm, fp.mu_ref);
     R Ucurv = DIAG ? J11 * U : J11 * U + J12 * V + J13 * W;
     R Vcurv = DIAG ? J22 * V : J21 * U + J22 * V + J23 * W;
@@ -327,16 +337,9 @@ __device__ __forceinline__ void flux_point(R rho, R U, R V, R W, R T, R Tm, cons
     o[14] = iJ * (f3 - g3);
 }
 
-// is linear index i on one of the faces in mask (bit f: 0 X0, 1 X1, 2 Y0, 3 Y1, 4 Z0, 5 Z1)
-__device__ __forceinline__ bool on_faces(const Grid3 &g, long long i, int mask) {
-    const long long ix = i % g.Nx, r = i / g.Nx, iy = r % g.Ny, iz = r / g.Ny;
-    return ((mask & 1) && ix == 0) || ((mask & 2) && ix == g.Nx - 1) || ((mask & 4) && iy == 0) ||
-           ((mask & 8) && iy == g.Ny - 1) || ((mask & 16) && iz == 0) || ((mask & 32) && iz == g.Nz - 1);
-}
-
 // NP consecutive points per thread (2 in FP32: paired 8-byte accesses), all
 // inputs of the iteration loaded before its 15 stores. WALL: mu on wall points
-// from Tmu.
+// from Tmu, and the conserved state on the faces of fp.cons_mask.
 template <typename R, int MET, int NP, bool WALL>
 __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restrict__ r0, const R *__restrict__ r1,
                                                       const R *__restrict__ r2, const R *__restrict__ r3,
@@ -383,10 +386,17 @@ __global__ void __launch_bounds__(256, 2) flux_kernel(Grid3 g, const R *__restri
             for (int k = 0; k < 12; k++) dq[k] = dd[k][q];
 #pragma unroll
             for (int c = 0; c < 10; c++) mq[c] = MET == MET_FIELD ? mj[c][q] : R(0);
+            // (q == 1 without `two` is the padding point past the grid's end)
+            const bool real = NP == 1 || two || q == 0;
             R Tm = T[q];
-            if (WALL && fp.les != 3 && on_faces(g, i + q, fp.wall_mask)) Tm = Tmu[i + q];
+            if (WALL && fp.les != 3 && real && on_faces(g, i + q, fp.wall_mask)) Tm = Tmu[i + q];
+            double qc[5];
+            const bool cons = WALL && fp.cons_mask && real && on_faces(g, i + q, fp.cons_mask);
+            if (cons)
+                for (int v = 0; v < 5; v++) qc[v] = fp.cons[v][i + q];
             flux_point<R, MET>(rho[q], U[q], V[q], Wv[q], T[q], Tm, dq, mq, fp.les >= 2 ? ms[q] : R(0),
-                               fp.les == 3 ? ks[q] : R(0), fp.les == 3 ? tk[q] : R(0), m, fp, d1c, iJc, dvol, oq);
+                               fp.les == 3 ? ks[q] : R(0), fp.les == 3 ? tk[q] : R(0), m, fp, d1c, iJc, dvol, oq,
+                               cons ? qc : nullptr);
 #pragma unroll
             for (int k = 0; k < 15; k++) out[k][q] = oq[k];
         }
@@ -409,7 +419,7 @@ int launch_flux(const Grid3 &g, const R *const q[5], const R *const d[12], const
     for (int c : {2, 3, 4, 6, 7, 8}) diag = diag && m.c[c] == R(0);
 #define MC3D_FLUX(MF, WL) \
     flux_kernel<R, MF, NP, WL><<<grid, 256, 0, st>>>(g, q[0], q[1], q[2], q[3], q[4], dp, m, p, mu_sgs, k_sgs, taukk, Tmu, op)
-    const bool wall = p.wall_mask != 0;
+    const bool wall = p.wall_mask != 0 || p.cons_mask != 0;
     if (!m.constant) {
         if (wall) MC3D_FLUX(MET_FIELD, true);
         else MC3D_FLUX(MET_FIELD, false);
@@ -434,7 +444,9 @@ __global__ void vreman_kernel(Grid3 g, const R *__restrict__ r0, DerivPtrs12 dp,
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         R gu[3][3];
         velocity_gradient<R>(m, i, d, gu);
-        mu_sgs[i] = vreman_mu<R>(gu, (R)r0[i], vreman_d1<R>(dvol, met(m, 0, i)));
+        // getSGSViscosity reads the conserved rho (Core.cpp:567)
+        const R rho = fp.cons_mask && on_faces(g, i, fp.cons_mask) ? (R)fp.cons[0][i] : (R)r0[i];
+        mu_sgs[i] = vreman_mu<R>(gu, rho, vreman_d1<R>(dvol, met(m, 0, i)));
     }
 }
 

@@ -54,4 +54,11 @@ __device__ __forceinline__ R met(const Metrics<R> &m, int c, long long i) {
     return m.constant ? m.c[c] : m.m[c][i];
 }
 
+// is linear index i on one of the faces in mask (bit f: 0 X0, 1 X1, 2 Y0, 3 Y1, 4 Z0, 5 Z1)
+__device__ __forceinline__ bool on_faces(const Grid3 &g, long long i, int mask) {
+    const long long ix = i % g.Nx, r = i / g.Nx, iy = r % g.Ny, iz = r / g.Ny;
+    return ((mask & 1) && ix == 0) || ((mask & 2) && ix == g.Nx - 1) || ((mask & 4) && iy == 0) ||
+           ((mask & 8) && iy == g.Ny - 1) || ((mask & 16) && iz == 0) || ((mask & 32) && iz == g.Nz - 1);
+}
+
 }  // namespace mc3d

@@ -63,6 +63,12 @@ struct mc3d_solver_s {
     int host_time_step = 0;
     int filter_time_step = 0;
     bool tc_fresh = false;   // tC holds the working-precision copy of the state the filter reads
+    // prim and the CFL maximum already hold the primitives of the next step:
+    // formed before a sponge relaxation changed rho1..rhoE1
+    bool prims_ready = false;
+    // faces whose conserved state the current stage takes in place of the
+    // primitives' (set for stage 1 after a sponge relaxation)
+    int cons_mask = 0;
     // running statistics (FP64): velocity (9) and thermodynamic (6) fields, their
     // time weights and the time of the last update
     double *stv[9] = {}, *stt[6] = {};
@@ -388,6 +394,8 @@ static int dsm_mu_taukk(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
     mt.taukk = (R *)s->taukk;
     mt.T = (R *)s->prim[4];
     mt.use_taukk = s->cfg.dsm_use_taukk;
+    mt.cons_mask = s->cons_mask;
+    mt.rho_prim = (const R *)s->prim[0];
     s->launches++;
     if ((rc = tic(s, KC_SGS, (5.0 * 8 + 8.0 * sizeof(R)) * n))) return rc;
     if ((rc = launch_dsm_mu_taukk<R>(s->g, mt, s->stream))) return rc;
@@ -453,6 +461,8 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
     fp.pr_t = 0.9;   // src/CurvilinearCSolver.hpp:232
     fp.les = 0;
     fp.wall_mask = s->wall_mask;
+    fp.cons_mask = s->cons_mask;
+    for (int v = 0; v < 5; v++) fp.cons[v] = qP[v];
     const R *dd[12];
     for (int i = 0; i < 12; i++) dd[i] = (const R *)s->der[i];
     const R *mu_sgs = (const R *)s->mu_sgs;
@@ -541,22 +551,41 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
     return MC3D_OK;
 }
 
+// bit f: face f is a SPONGE
+static int sponge_faces(mc3d_solver s) {
+    int faces = 0;
+    for (int f = 0; f < 6; f++)
+        if (s->cfg.bc_kind[f] == MC3D_BC_SPONGE) faces |= 1 << f;
+    return faces;
+}
+
+// primitives of rho1..rhoE1 (updateNonConservedData, Core.cpp:1165-1177) and
+// the CFL maximum over them, which calcDtFromCFL (Core.cpp:189-237) reads
+template <typename R>
+static int primitives_cfl(mc3d_solver s) {
+    R *prim[5];
+    for (int v = 0; v < 5; v++) prim[v] = (R *)s->prim[v];
+    s->launches++;
+    int rc;
+    if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 5.0 * sizeof(R)) * (double)s->g.n()))) return rc;
+    if ((rc = launch_primitives_cfl<R>(s->g, s->q1, prim, metrics_of<R>(s), s->dxi, &s->ts->umax_bits, s->stream)))
+        return rc;
+    return toc(s);
+}
+
 template <typename R>
 static int one_step(mc3d_solver s) {
     int rc;
-    // preStep: calcDtFromCFL on the current state (Core.cpp:189-237), fused into
-    // the primitives of stage 1, which read the same state
-    Metrics<R> m = metrics_of<R>(s);
+    // preStep: calcDtFromCFL on the current state, fused into the primitives of
+    // stage 1, which read the same state (unless a sponge relaxation after the
+    // previous step formed both already)
     const int first = s->host_time_step == s->cfg.time_step0;
-    {
-        R *prim[5];
-        for (int v = 0; v < 5; v++) prim[v] = (R *)s->prim[v];
-        s->launches += 2;
-        if ((rc = tic(s, KC_PRIM, (5.0 * 8 + 5.0 * sizeof(R)) * (double)s->g.n()))) return rc;
-        if ((rc = launch_primitives_cfl<R>(s->g, s->q1, prim, m, s->dxi, &s->ts->umax_bits, s->stream))) return rc;
-        if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
-        if ((rc = toc(s))) return rc;
-    }
+    if (!s->prims_ready)
+        if ((rc = primitives_cfl<R>(s))) return rc;
+    const int relaxed = s->prims_ready ? sponge_faces(s) : 0;
+    s->prims_ready = false;
+    s->launches++;
+    if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
     s->host_time_step++;
     const bool filter_now = s->host_time_step % s->cfg.filter_step == 0;
 
@@ -569,7 +598,10 @@ static int one_step(mc3d_solver s) {
         if (st > 1 && s->cfg.substep_filtering)
             if ((rc = primitives<R>(s, s->qk))) return rc;
         if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
-        if ((rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
+        s->cons_mask = st == 1 ? relaxed : 0;
+        rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk);
+        s->cons_mask = 0;
+        if (rc) return rc;
         RkStage rs{};
         rs.scheme = scheme;
         rs.stage = st;
@@ -1056,6 +1088,7 @@ static int set_initial_impl(mc3d_solver s, const double *rho, const double *U, c
     if (!s->have_metrics) return fail(MC3D_ERR_CONFIG, "set the metrics before the initial condition");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
     size_t n = (size_t)s->g.n();
+    s->prims_ready = false;
     if (!s->have_walls) {
         // no wall treatment: the conserved state is formed on the device. Host
         // primitives go through the (not yet used) q2 registers.
@@ -1435,8 +1468,22 @@ int mc3d_solver_step(mc3d_solver s, int nsteps) {
     for (int i = 0; i < nsteps; i++) {
         int rc = s->prec == MC3D_FP64 ? one_step<double>(s) : one_step<float>(s);
         if (rc) return rc;
+        // postStep (src/CurvilinearCSolver.hpp:355-375). The statistics read the
+        // primitives of the filtered state and rho2, neither of which the
+        // sponge relaxation changes, so they are updated first.
         if ((s->cfg.velocity_stats || s->cfg.thermo_stats) && s->host_time_step % s->cfg.stats_interval == 0)
             if ((rc = stats_update(s))) return rc;
+        if (s->cfg.sponge_relax && s->have_sponge) {
+            // updateSponge changes rho1..rhoE1 alone: the primitives, and with
+            // them the next step's CFL and stage-1 derivatives, stay those of
+            // the filtered state, so they are formed before the relaxation
+            if ((rc = s->prec == MC3D_FP64 ? primitives_cfl<double>(s) : primitives_cfl<float>(s))) return rc;
+            s->prims_ready = true;
+            s->launches++;
+            if ((rc = mc3d::launch_sponge_relax(s->g, s->q1, s->spg_avg, s->ts, s->cfg.sponge_avg_time,
+                                                s->cfg.sponge_p_inf, sponge_faces(s), s->stream)))
+                return rc;
+        }
     }
     return MC3D_OK;
 }

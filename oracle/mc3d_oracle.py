@@ -569,6 +569,9 @@ class Config:
     periodic_disp: tuple = None
     # [STATS]: dict(velocity=bool, thermo=bool, avg="NONE"|"XI1_AVG"|"XI2_AVG"|"XI3_AVG", interval=int)
     stats: dict = None
+    # updateSponge after every step (commented out in the reference's postStep):
+    # dict(avg_time=float, p_inf=float) or None
+    sponge_relax: dict = None
 
     def kinds(self):
         if self.bc_kind is not None:
@@ -1032,12 +1035,36 @@ class Oracle:
         self._prims = primitives(src, self.cfg.mu_ref)
 
     def step(self):
-        """One time step then postStep's statistics update every STATS.INTERVAL
-        steps (src/CurvilinearCSolver.hpp:355-375)."""
+        """One time step then postStep (src/CurvilinearCSolver.hpp:355-375): the
+        sponge relaxation when switched on and the statistics update every
+        STATS.INTERVAL steps. The statistics read the primitives of the
+        filtered state and rho2, which the relaxation leaves as they were, so
+        they are taken before it."""
         self._advance()
         st = self.state
         if self.stats is not None and st.time_step % self.stats.interval == 0:
             self.stats.update(st.time, st.q1, st.q2)
+        if self.cfg.sponge_relax and self.sponge_on:
+            self.update_sponge()
+
+    def update_sponge(self):
+        """CurvilinearCSolver::updateSponge (src/CurvilinearCSolver_BC.cpp:843-928):
+        the target relaxes toward rho1..rhoE1 with eps = 1/(avgT/dt + 1), its
+        energy is blended toward the back pressure (epsP = 0.005,
+        src/SpongeBC.cpp:37), and the SPONGE faces take the target state.
+        Only rho1..rhoE1 change: the primitives of the filtered state, which
+        the next step's CFL and first-stage derivatives read, stay as they were."""
+        st, sr = self.state, self.cfg.sponge_relax
+        eps = 1.0 / (sr.get("avg_time", 1.0) / st.dt + 1.0)
+        a = [self.spg_avg[v] + eps * (st.q1[v] - self.spg_avg[v]) for v in range(5)]
+        eps_p, p_inf = 0.005, sr.get("p_inf", 1.0 / 1.4)
+        a[4] = eps_p * a[4] + (1.0 - eps_p) * (p_inf / (GAMMA - 1.0) + 0.5 * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) / a[0])
+        self.spg_avg = a
+        for f in range(6):
+            if self.kinds[f] == "SPONGE":
+                sl = _face_slices(f, a[0].shape)[0]
+                for v in range(5):
+                    st.q1[v][sl] = a[v][sl]
 
     def _advance(self):
         """One time step (or the LSLDDRK4 two-step pair's half): src/RK4.hpp:127-178,

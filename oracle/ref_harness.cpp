@@ -80,10 +80,19 @@ void operator delete(void *p, size_t) noexcept { free(p); }
 
 // wall-clock stamp at the end of every time step (postStep -> fullStepTemporalHook)
 static std::vector<double> g_step_stamps;
+// MC3D_REF_UPDATE_SPONGE=1: call updateSponge where postStep has it commented
+// out (src/CurvilinearCSolver.hpp:355-359), i.e. right after this hook
+static bool update_sponge_on() {
+    const char *e = getenv("MC3D_REF_UPDATE_SPONGE");
+    return e && e[0] == '1';
+}
 
 // ---- solver hooks (the reference leaves their bodies to the driver) ----
 void CurvilinearCSolver::initialHook() {}
-void CurvilinearCSolver::fullStepTemporalHook() { g_step_stamps.push_back(MPI_Wtime()); }
+void CurvilinearCSolver::fullStepTemporalHook() {
+    g_step_stamps.push_back(MPI_Wtime());
+    if (update_sponge_on()) updateSponge();
+}
 void CurvilinearCSolver::subStepTemporalHook() {}
 void CurvilinearCSolver::preStepBoundaryHook() {}
 void CurvilinearCSolver::postStepBoundaryHook() {}

@@ -80,6 +80,10 @@ def ini_text(cfg, max_steps: int, kinds=None, box=6.283185307179586) -> str:
     sp = getattr(cfg, "sponge", None)
     if "SPONGE" in kinds and sp:
         lines += ["[SPONGE]", f"KIND = {sp.get('kind', 'RECTILINEAR')}", f"STRENGTH = {sp.get('strength', 1.0)!r}"]
+        relax = getattr(cfg, "sponge_relax", None)
+        if relax:
+            lines += [f"AVGTIME = {float(relax.get('avg_time', 1.0))!r}",
+                      f"PINF = {float(relax.get('p_inf', 1.0 / 1.4))!r}"]
         if sp.get("kind", "RECTILINEAR") == "RECTILINEAR":
             for f, key in enumerate(("X0", "X1", "Y0", "Y1", "Z0", "Z1")):
                 if kinds[f] == "SPONGE":
@@ -155,7 +159,9 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
                 mesh = "file:mesh.bin"
             cmd = [REF_BIN, "run", mesh, "ic.bin", "out.bin"]
         t0 = time.perf_counter()
-        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout)
+        env = dict(os.environ)
+        env["MC3D_REF_UPDATE_SPONGE"] = "1" if getattr(cfg, "sponge_relax", None) else "0"
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout, env=env)
         wall = time.perf_counter() - t0
         if r.returncode != 0:
             raise RuntimeError("mc3d_ref failed: " + r.stderr[-2000:] + r.stdout[-2000:])

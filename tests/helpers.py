@@ -17,6 +17,10 @@ def golden_steps():
     return np.load(os.path.join(HERE, "golden", "steps.npz"))
 
 
+def golden_relax():
+    return np.load(os.path.join(HERE, "golden", "sponge_relax.npz"))
+
+
 def golden_metrics():
     return np.load(os.path.join(HERE, "golden", "metrics.npz"))
 

@@ -54,3 +54,30 @@ def test_wall_span_average_matches_restatement():
         assert np.abs(a - b).max() <= 1e-14 * max(np.abs(b).max(), 1.0)
     # a no-slip wall: the averaged wall velocity is zero
     assert max(np.abs(a).max() for a in got[1:]) == 0.0
+
+
+@pytest.mark.parametrize("name", list(G.RELAX_CASES))
+def test_sponge_relaxation_matches_reference(name):
+    """updateSponge after every step (left commented out in the reference's
+    postStep, called by the fixture run): FP64 against the reference's state,
+    <= 1e-12 relative, and the relaxation changes the result."""
+    cfg, ic, n, coords, base = G.relax_case(name)
+    gold, relaxed = H.golden_steps(), H.golden_relax()
+    opt = m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                    ts_type=cfg.ts_type, cfl=cfg.cfl, dt=cfg.dt, filter_step=cfg.filter_step,
+                    substep_filtering=cfg.substep_filtering, les=cfg.les, les_avg=cfg.les_avg,
+                    dsm_test_filter=cfg.dsm_test_filter, bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge,
+                    sponge_relax=cfg.sponge_relax)
+    s = m.CurvilinearCSolver(opt)
+    s.set_metrics([gold[f"{base}_met{c}"] for c in range(10)])
+    s.set_sponge(m.sponge_sigma(opt, *coords))
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    got = s.conserved()
+    for i in range(5):
+        err = H.rel_max(got[i], relaxed[f"{name}_q{i}"])
+        assert err <= 1e-12, (i, err)
+    if base == name:
+        assert max(H.rel_max(got[i], gold[f"{name}_q{i}"]) for i in range(5)) > 1e-6
+    ts, t, dt = relaxed[f"{name}_info"]
+    assert s.info()["time_step"] == int(ts)

@@ -172,3 +172,30 @@ def test_oracle_turbdata_of_the_initial_field():
     t = O.hit_turbdata(o, 8.0)
     assert abs(t[3] - 0.3) < 1e-12 and t[7] < 1e-14
     assert abs(t[10] - 0.09) < 1e-12
+
+
+@pytest.mark.parametrize("name", list(G.RELAX_CASES))
+def test_oracle_sponge_relaxation_matches_reference_fixtures(name):
+    """updateSponge restatement against the reference run with the call made
+    after every step: <= 1e-12 relative; the SPONGE faces carry the relaxed
+    target and its pressure moves toward SPONGE.PINF."""
+    cfg, ic, n, coords, base = G.relax_case(name)
+    gold, relaxed = H.golden_steps(), H.golden_relax()
+    o = O.Oracle(cfg, [gold[f"{base}_met{c}"] for c in range(10)], sigma=O.sponge_sigma(cfg, *coords))
+    o.init(*ic)
+    for _ in range(n):
+        o.step()
+    for i in range(5):
+        err = H.rel_max(o.state.q1[i], relaxed[f"{name}_q{i}"])
+        assert err <= 1e-12, (i, err)
+    kinds = cfg.kinds()
+    faces = [f for f in range(6) if kinds[f] == "SPONGE"]
+    assert faces
+    for f in faces:
+        sl = O._face_slices(f, o.state.q1[0].shape)[0]
+        for v in range(5):
+            assert np.array_equal(o.state.q1[v][sl], o.spg_avg[v][sl])
+    a = o.spg_avg
+    p = (O.GAMMA - 1.0) * (a[4] - 0.5 * (a[1] ** 2 + a[2] ** 2 + a[3] ** 2) / a[0])
+    p_inf = cfg.sponge_relax["p_inf"]
+    assert abs(float(np.mean(p)) - p_inf) < abs(1.0 / 1.4 - p_inf)
