@@ -327,6 +327,10 @@ int mc3d_solver_turbdata(mc3d_solver s, double k0, double out[11]);
 /* The cylinder driver's surface data (src/MPI_3DCompact.cpp:408-485): p, U, V,
  * W on the j = 0 face averaged over xi3, Nx values each (host arrays). */
 int mc3d_solver_wall_span_average(mc3d_solver s, double *p, double *U, double *V, double *W);
+/* The cylinder driver's wake strip (src/MPI_3DCompact.cpp:488-527): V along
+ * xi3 at the grid point (i, j) (the driver takes i = 0, j = 143), Nz values
+ * (host array). MC3D_ERR_ARG when (i, j) lies outside the grid. */
+int mc3d_solver_wake_strip(mc3d_solver s, int i, int j, double *V);
 
 /* ---- running statistics (Stats, src/Stats.cpp:127-347) ---- */
 /* With cfg.velocity_stats / thermo_stats set, every mc3d_solver_step updates

@@ -17,6 +17,7 @@ Fields are CUDA torch tensors (or any object with .data_ptr()) shaped
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -191,6 +192,22 @@ def write_dump(path, time_step, time, fields):
     nz, ny, nx = arrs[0].shape
     p = (C.POINTER(C.c_double) * 8)(*[N.dptr(a) for a in arrs])
     N.check(N.host_lib().mc3d_dump_write(str(path).encode(), int(time_step), float(time), nx, ny, nz, p))
+
+
+def append_turbdata_line(path, values):
+    """Append one turbdata.out line: the values as the HIT driver's ofstream
+    with precision 17 prints them, each followed by a space
+    (tests/hit/Samtaney_D4/MPI_3DCompact.cpp:545-555)."""
+    with open(path, "a") as f:
+        f.write("".join(f"{float(v):.17g} " for v in values) + "\n")
+
+
+def append_record(path, time, values):
+    """Append time and the values as raw doubles (the cylinder driver's
+    cylinder{P,U,V,W}.dat and VWakeStrip.dat records, src/MPI_3DCompact.cpp:463-483, :518-524)."""
+    with open(path, "ab") as f:
+        f.write(np.float64(time).tobytes())
+        f.write(np.ascontiguousarray(values, dtype=np.float64).tobytes())
 
 
 def sponge_sigma(opt, x, y, z):
@@ -438,6 +455,31 @@ class CurvilinearCSolver:
         out = [np.empty(self.shape[2]) for _ in range(4)]
         N.check(N.host_lib().mc3d_solver_wall_span_average(self._h, *[N.dptr(a) for a in out]))
         return out
+
+    def wake_strip(self, i=0, j=143):
+        """V along xi3 at the grid point (i, j) (Nz values)."""
+        out = np.empty(self.shape[0])
+        N.check(N.host_lib().mc3d_solver_wake_strip(self._h, int(i), int(j), N.dptr(out)))
+        return out
+
+    def write_turbdata(self, path="turbdata.out", k0=8.0):
+        """Append the HIT driver's turbdata.out line for the current state
+        (tests/hit/Samtaney_D4/MPI_3DCompact.cpp:545-555)."""
+        append_turbdata_line(path, self.turbdata(k0))
+
+    def write_cylinder_data(self, directory=".", strip=(0, 143)):
+        """Append the cylinder driver's records for the current state
+        (src/MPI_3DCompact.cpp:463-527): time and the span-averaged wall p, U,
+        V, W to cylinderP/U/V/W.dat, time and the wake strip V to
+        VWakeStrip.dat; a strip point outside the grid gives the driver's
+        -100000 fill."""
+        t = self.info()["time"]
+        for name, a in zip("PUVW", self.wall_span_average()):
+            append_record(os.path.join(directory, f"cylinder{name}.dat"), t, a)
+        i, j = strip
+        nx, ny = self.shape[2], self.shape[1]
+        v = self.wake_strip(i, j) if 0 <= i < nx and 0 <= j < ny else np.full(self.shape[0], -100000.0)
+        append_record(os.path.join(directory, "VWakeStrip.dat"), t, v)
 
     def dump_stats(self, velocity_path=None, thermo_path=None):
         enc = (lambda p: None if p is None else str(p).encode())

@@ -1,7 +1,8 @@
 // Device reductions behind the reference drivers' diagnostic hooks:
 //   HIT turbulence statistics, one line of turbdata.out
 //     (tests/hit/Samtaney_D4/MPI_3DCompact.cpp:370-555, fullStepTemporalHook);
-//   span-averaged wall values of the cylinder (src/MPI_3DCompact.cpp:408-485).
+//   span-averaged wall values of the cylinder (src/MPI_3DCompact.cpp:408-485)
+//   and its wake strip, V along xi3 at one (xi1, xi2) point (:488-527).
 #include "mc3d_internal.h"
 #include "pointwise_common.cuh"
 
@@ -100,6 +101,14 @@ __global__ void wall_span_kernel(Grid3 g, Q5c q, double *out) {
     }
 }
 
+// V = rhoV / rho along xi3 at (i, j) (src/MPI_3DCompact.cpp:491-507)
+__global__ void wake_strip_kernel(Grid3 g, Q5c q, int i, int j, double *out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.Nz; k += gridDim.x * blockDim.x) {
+        const long long p = i + (long long)g.Nx * (j + (long long)g.Ny * k);
+        out[k] = q.p[2][p] / q.p[0][p];
+    }
+}
+
 }  // namespace
 
 template <typename R>
@@ -122,6 +131,14 @@ int launch_wall_span_average(const Grid3 &g, const double *const q[5], double *o
     Q5c qq;
     for (int v = 0; v < 5; v++) qq.p[v] = q[v];
     wall_span_kernel<<<(g.Nx + 127) / 128, 128, 0, st>>>(g, qq, out);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+int launch_wake_strip(const Grid3 &g, const double *const q[5], int i, int j, double *out, cudaStream_t st) {
+    Q5c qq;
+    for (int v = 0; v < 5; v++) qq.p[v] = q[v];
+    wake_strip_kernel<<<(g.Nz + 127) / 128, 128, 0, st>>>(g, qq, i, j, out);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }

@@ -397,6 +397,7 @@ int launch_turb_sums(const Grid3 &g, const R *const prim[5], const R *const d[12
                      double mu_ref, int pass, double mean_rho, double *partial, int nblocks, cudaStream_t st);
 // out[4][Nx]: span averages of p, U, V, W on the j = 0 face
 int launch_wall_span_average(const Grid3 &g, const double *const q[5], double *out, cudaStream_t st);
+int launch_wake_strip(const Grid3 &g, const double *const q[5], int i, int j, double *out, cudaStream_t st);
 
 // ---- checkpoint files (checkpoint.cpp) ----------------------------------------
 int write_solution_dump(const char *path, int time_step, double time, int Nx, int Ny, int Nz,

@@ -1367,6 +1367,24 @@ int mc3d_solver_wall_span_average(mc3d_solver s, double *p, double *U, double *V
     return MC3D_OK;
 }
 
+int mc3d_solver_wake_strip(mc3d_solver s, int i, int j, double *V) {
+    if (!s || !V) return fail(MC3D_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no state");
+    if (i < 0 || i >= s->g.Nx || j < 0 || j >= s->g.Ny) return fail(MC3D_ERR_ARG, "strip point outside the grid");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    int rc;
+    double *buf = nullptr;
+    MC3D_CUDA_TRY(cudaMallocAsync((void **)&buf, (size_t)s->g.Nz * 8, s->stream));
+    if ((rc = mc3d::launch_wake_strip(s->g, s->q1, i, j, buf, s->stream))) {
+        cudaFreeAsync(buf, s->stream);
+        return rc;
+    }
+    MC3D_CUDA_TRY(cudaMemcpyAsync(V, buf, (size_t)s->g.Nz * 8, cudaMemcpyDeviceToHost, s->stream));
+    MC3D_CUDA_TRY(cudaFreeAsync(buf, s->stream));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MC3D_OK;
+}
+
 int mc3d_solver_get_stats(mc3d_solver s, double *const velocity[9], double *const thermo[6], double weights[2]) {
     if (!s) return fail(MC3D_ERR_ARG, "null solver");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));

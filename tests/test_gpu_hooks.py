@@ -81,3 +81,35 @@ def test_sponge_relaxation_matches_reference(name):
         assert max(H.rel_max(got[i], gold[f"{name}_q{i}"]) for i in range(5)) > 1e-6
     ts, t, dt = relaxed[f"{name}_info"]
     assert s.info()["time_step"] == int(ts)
+
+
+def test_wake_strip_and_cylinder_records(tmp_path):
+    """The wake strip is V = rhoV / rho of the state along xi3 at (i, j); the
+    record files carry the time then the values; a strip point outside the
+    grid gives the driver's -100000 fill and the ABI call rejects it."""
+    name = "ogrid_cyl_sponge_kenrk4"
+    cfg, ic, n, coords = G.wall_case(name)
+    opt = m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                    cfl=cfg.cfl, bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge,
+                    periodic_disp=O.periodic_disp_table(cfg))
+    s = m.CurvilinearCSolver(opt)
+    s.set_mesh(*coords)
+    s.set_sponge(m.sponge_sigma(opt, *coords))
+    s.set_initial_conditions(*ic)
+    s.step(n)
+    q = s.conserved()
+    i, j = 3, 7
+    assert np.array_equal(s.wake_strip(i, j), q[2][:, j, i] / q[0][:, j, i])
+    with pytest.raises(Exception):
+        s.wake_strip(0, cfg.N[1])
+    s.write_cylinder_data(tmp_path, strip=(i, j))
+    s.write_cylinder_data(tmp_path)   # the driver's (0, 143): outside this 24 x 20 x 12 grid
+    t = s.info()["time"]
+    nx, nz = cfg.N[0], cfg.N[2]
+    for k, a in enumerate(s.wall_span_average()):
+        raw = np.fromfile(tmp_path / f"cylinder{'PUVW'[k]}.dat", dtype=np.float64)
+        assert raw.size == 2 * (1 + nx) and raw[0] == t and np.array_equal(raw[1:1 + nx], a)
+    raw = np.fromfile(tmp_path / "VWakeStrip.dat", dtype=np.float64)
+    assert raw.size == 2 * (1 + nz) and raw[0] == t
+    assert np.array_equal(raw[1:1 + nz], q[2][:, j, i] / q[0][:, j, i])
+    assert np.all(raw[2 + nz:] == -100000.0)
