@@ -187,81 +187,26 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
 
 // E: the caller's operation (EpiMode), compiled into the kernel so that each
 // instantiation carries one epilogue only.
-template <int DIR, typename R, int KIND, int H, int L, int E>
-__global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op, SweepBatch<R> b,
-                                                        RhsFinalArgs<R> rf, int pass_y, int pass_z, int pass_x) {
+// The solve of one tile once each lane holds rows a-H .. a+L+H-1 of its line
+// in v: Dirichlet boundary rows, pass 1, the forward chain and fold, pass 2,
+// the backward chain, fold and cyclic correction; y gets the solution rows
+// a .. a+L-1. sh: the chain-state area of the shared memory ([4][S][2][W]
+// states, [2][W] last values, [W][4] correction scalars). Every thread of the
+// CTA calls it (it synchronises the CTA).
+template <typename R, int KIND, int H, int L>
+__device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L + 2 * H], R (&y)[L], bool work,
+                                          int lane, int seg, int S, int a, R *sh) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
     constexpr int NB = L / UB;
-    constexpr int NV = L + 2 * H;
-    constexpr int P = W + 1;
     using V = RegVec<R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *sh = reinterpret_cast<R *>(smem_raw);
-    const int S = blockDim.x >> 5;
-    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
-    const int N = op.N, a = seg * L;
-    const int f = blockIdx.y;
+    const int N = op.N;
     R *fwdEnd = sh;                    // [S][2][W] local end states of pass 1
     R *fwdIn = fwdEnd + S * 2 * W;     // [S][2][W] incoming forward states
     R *bwdStart = fwdIn + S * 2 * W;   // [S][2][W] local start values of pass 2
     R *bwdNext = bwdStart + S * 2 * W; // [S][2][W] incoming backward states
     R *lastx = bwdNext + S * 2 * W;    // [2][W] x_{N-1}, x_{N-2}
     R *scorr = lastx + 2 * W;          // [W][4] cyclic correction scalars
-    R *tile = scorr + 4 * W;           // x lines: [N][W+1]
-
-    const TileGeom t = tile_geom<DIR>(g, blockIdx.x, lane);
-    bool pass = false;
-    if (DIR == 0) pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
-    if (DIR == 1) pass = (pass_x && (t.i == 0 || t.i == g.Nx - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
-    if (DIR == 2) pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_x && (t.i == 0 || t.i == g.Nx - 1));
-    const bool work = t.active && !pass;
-
-    // ---- load rows a-H .. a+L+H-1 of this lane's line (periodic wrap / zero) ----
-    R v[NV];
-    int nl = W;
-    if (DIR == 0) {
-        const long long rem = (long long)g.Ny * g.Nz - (long long)blockIdx.x * W;
-        nl = rem < W ? (int)rem : W;
-        const R *src = b.in[f] + (size_t)blockIdx.x * W * N;
-        for (int l = 0; l < nl; l++) {
-#pragma unroll
-            for (int i0 = 0; i0 < L; i0 += 32) cp_async_elem(&tile[(a + i0 + lane) * P + l], src + l * N + a + i0 + lane);
-        }
-        cp_async_wait_all();
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-            int n = a - H + k;
-            bool in = true;
-            if (k < H && n < 0) {
-                n += N;
-                in = PER;
-            }
-            if (k >= H + L && n >= N) {
-                n -= N;
-                in = PER;
-            }
-            v[k] = in ? tile[n * P + lane] : R(0);
-        }
-    } else {
-        const R *src = b.in[f] + (int)t.base;
-        const int stride = (int)t.stride;
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-            int n = a - H + k;
-            bool in = true;
-            if (k < H && n < 0) {
-                n += N;
-                in = PER;
-            }
-            if (k >= H + L && n >= N) {
-                n -= N;
-                in = PER;
-            }
-            v[k] = (t.active && in) ? src[n * stride] : R(0);
-        }
-    }
 
     // ---- Dirichlet boundary rows (first / last segment) ----
     R headr[H], tailr[H];
@@ -284,7 +229,6 @@ __global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op
 
     // ---- pass 1: RHS + local forward elimination (zero incoming state) ----
     // Pass-through and inactive lines keep their input in y.
-    R y[L];
     R y1 = 0, y2 = 0;   // y_{n-1}, y_{n-2}
 #pragma unroll
     for (int blk = 0; blk < NB; blk++) {
@@ -532,6 +476,78 @@ __global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op
         }
     }
 
+}
+
+template <int DIR, typename R, int KIND, int H, int L, int E>
+__global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op, SweepBatch<R> b,
+                                                        RhsFinalArgs<R> rf, int pass_y, int pass_z, int pass_x) {
+    constexpr bool PER = (KIND % 2) == 0;
+    constexpr int NV = L + 2 * H;
+    constexpr int P = W + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *sh = reinterpret_cast<R *>(smem_raw);
+    const int S = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+    const int N = op.N, a = seg * L;
+    const int f = blockIdx.y;
+    R *tile = sh + 8 * S * W + 6 * W;  // x lines: [N][W+1], after the chain states
+
+    const TileGeom t = tile_geom<DIR>(g, blockIdx.x, lane);
+    bool pass = false;
+    if (DIR == 0) pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
+    if (DIR == 1) pass = (pass_x && (t.i == 0 || t.i == g.Nx - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
+    if (DIR == 2) pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_x && (t.i == 0 || t.i == g.Nx - 1));
+    const bool work = t.active && !pass;
+
+    // ---- load rows a-H .. a+L+H-1 of this lane's line (periodic wrap / zero) ----
+    R v[NV];
+    int nl = W;
+    if (DIR == 0) {
+        const long long rem = (long long)g.Ny * g.Nz - (long long)blockIdx.x * W;
+        nl = rem < W ? (int)rem : W;
+        const R *src = b.in[f] + (size_t)blockIdx.x * W * N;
+        for (int l = 0; l < nl; l++) {
+#pragma unroll
+            for (int i0 = 0; i0 < L; i0 += 32) cp_async_elem(&tile[(a + i0 + lane) * P + l], src + l * N + a + i0 + lane);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            int n = a - H + k;
+            bool in = true;
+            if (k < H && n < 0) {
+                n += N;
+                in = PER;
+            }
+            if (k >= H + L && n >= N) {
+                n -= N;
+                in = PER;
+            }
+            v[k] = in ? tile[n * P + lane] : R(0);
+        }
+    } else {
+        const R *src = b.in[f] + (int)t.base;
+        const int stride = (int)t.stride;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            int n = a - H + k;
+            bool in = true;
+            if (k < H && n < 0) {
+                n += N;
+                in = PER;
+            }
+            if (k >= H + L && n >= N) {
+                n -= N;
+                in = PER;
+            }
+            v[k] = (t.active && in) ? src[n * stride] : R(0);
+        }
+    }
+
+    R y[L];
+    reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
+
     // ---- epilogue ----
     if (DIR == 0) {
         if (t.active) {
@@ -590,6 +606,10 @@ static int launch_reg_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBat
 template <int DIR, typename R>
 int launch_sweep_reg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
                      const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
+    if constexpr (DIR == 0 && sizeof(R) == 4) {
+        const int rc = launch_sweep_tma_x(g, op, b, epi, px, py, pz, st);
+        if (rc != MC3D_ERR_CONFIG) return rc;
+    }
 #define MC3D_RCASE(K, HH, LL)                                                  \
     if (op.kind == K && op.H == HH && op.L == LL)                              \
         return launch_reg_one<DIR, R, K, HH, LL>(g, op, b, epi, rf, px, py, pz, st);

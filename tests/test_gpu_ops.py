@@ -133,3 +133,36 @@ def test_segmented_lines_vs_oracle(n, bc, prec):
             torch.cuda.synchronize()
             err = H.rel_max(y.double().cpu().numpy(), ref)
             assert err <= TOL[prec], (op, n, d, bc, err)
+
+
+@pytest.mark.parametrize("prec", [m.FP64, m.FP32BULK])
+def test_register_kernel_pass_through_lines(prec):
+    """Filter lines on the faces of the other (Dirichlet) directions pass
+    through unchanged (Compact10Filter::filterField) in the register-resident
+    kernel: 64-point lines in every direction, against the oracle."""
+    torch = _torch()
+    from oracle import mc3d_oracle as O
+    rng = np.random.default_rng(11)
+    dt = torch.float64 if prec == m.FP64 else torch.float32
+    shape = (64, 64, 64)
+    f = rng.standard_normal(shape)
+    x = torch.tensor(f, dtype=dt, device="cuda")
+    for d in range(3):
+        bcs = [m.DIRICHLET_SOLVE] * 3
+        bcs[d] = m.PERIODIC_SOLVE
+        for op in ("COMPACT8", "COMPACT10", "TESTPADE"):
+            o = _make(op, d, bcs, shape, prec)
+            y = torch.empty_like(x)
+            o.filterField(x, y)
+            if op == "TESTPADE":
+                ref = O.test_filter(f, d, 1, tuple(bcs))
+            else:
+                ref = O.filt(f, d, op, G.OPS_ALPHA, tuple(bcs))
+            torch.cuda.synchronize()
+            out = y.double().cpu().numpy()
+            err = H.rel_max(out, ref)
+            assert err <= TOL[prec], (op, d, err)
+            # the face lines are the input, bit for bit
+            face = [slice(None)] * 3
+            face[2 - (d + 1) % 3] = 0
+            assert np.array_equal(out[tuple(face)], x.double().cpu().numpy()[tuple(face)]), (op, d)
