@@ -94,10 +94,14 @@ template <int DIR, typename R>
 int launch_sweep_reg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
                      const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st);
 
-// FP32 x-line solves staged through shared memory by TMA (sweep_tma.cuh);
+// FP32 x-line solves staged through shared memory by TMA (sweep_tma.cuh,
+// sweeps_tma.cu);
 // MC3D_ERR_CONFIG, without recording an error, when the case is not covered
 // (or MC3D_NO_TMA=1 is set).
 int launch_sweep_tma_x(const Grid3 &g, const LineOpDev<float> &op, const SweepBatch<float> &b, int epi, int px,
                        int py, int pz, cudaStream_t st);
+// the same for y (dir 1) and z (dir 2) lines
+int launch_sweep_tma_yz(int dir, const Grid3 &g, const LineOpDev<float> &op, const SweepBatch<float> &b, int epi,
+                        const RhsFinalArgs<float> &rf, int px, int py, int pz, cudaStream_t st);
 
 }  // namespace mc3d

@@ -606,8 +606,9 @@ static int launch_reg_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBat
 template <int DIR, typename R>
 int launch_sweep_reg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
                      const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
-    if constexpr (DIR == 0 && sizeof(R) == 4) {
-        const int rc = launch_sweep_tma_x(g, op, b, epi, px, py, pz, st);
+    if constexpr (sizeof(R) == 4) {
+        const int rc = DIR == 0 ? launch_sweep_tma_x(g, op, b, epi, px, py, pz, st)
+                                : launch_sweep_tma_yz(DIR, g, op, b, epi, rf, px, py, pz, st);
         if (rc != MC3D_ERR_CONFIG) return rc;
     }
 #define MC3D_RCASE(K, HH, LL)                                                  \

@@ -1,122 +1,7 @@
-// Register-resident line solves along x (kernels in sweep_reg.cuh and
-// sweep_tma.cuh) and the tensor maps of the TMA-staged path.
-#include <cstdlib>
-#include <map>
-#include <mutex>
-#include <tuple>
-
-#include "sweep_tma.cuh"
+// Register-resident line solves along x (kernel in sweep_reg.cuh).
+#include "sweep_reg.cuh"
 
 namespace mc3d {
-namespace {
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point, so the
-// library loads without libcuda on hosts that only build or test it
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            return (EncodeTiledFn) nullptr;
-        return reinterpret_cast<EncodeTiledFn>(p);
-    }();
-    return fn;
-}
-
-// Tensor map of a field viewed as [Ny*Nz lines][Nx] FP32, 32 x 32 boxes with
-// the 128-byte swizzle; cached per (address, Nx, lines) since a run reuses a
-// fixed set of field buffers.
-bool tensor_map_x(const void *p, int nx, long long lines, CUtensorMap *out) {
-    static std::mutex mu;
-    static std::map<std::tuple<const void *, int, long long>, CUtensorMap> cache;
-    std::lock_guard<std::mutex> lk(mu);
-    const auto key = std::make_tuple(p, nx, lines);
-    auto it = cache.find(key);
-    if (it != cache.end()) {
-        *out = it->second;
-        return true;
-    }
-    if (((uintptr_t)p & 15) != 0 || ((size_t)nx * 4) % 16 != 0) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)lines};
-    cuuint64_t strides[1] = {(cuuint64_t)nx * 4};
-    cuuint32_t box[2] = {(cuuint32_t)TMA_BOX, (cuuint32_t)W};
-    cuuint32_t estr[2] = {1, 1};
-    const EncodeTiledFn enc = encode_tiled();
-    if (!enc) return false;
-    CUtensorMap m;
-    if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(p), dims, strides, box, estr,
-                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return false;
-    if (cache.size() > 4096) cache.clear();
-    cache.emplace(key, m);
-    *out = m;
-    return true;
-}
-
-template <int KIND, int H, int L, int E>
-int launch_tma_epi(const Grid3 &g, const LineOpDev<float> &op, const TmaMapsX &maps, int nf, int py, int pz,
-                   cudaStream_t st) {
-    const int S = op.N / L;
-    const size_t smem = 1024 + (size_t)(op.N / TMA_BOX) * 4096 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
-    auto kern = sweep_tma_x_kernel<KIND, H, L, E>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
-    dim3 grid(tile_count<0>(g), nf);
-    kern<<<grid, 32 * S, smem, st>>>(g, op, maps, py, pz);
-    MC3D_CUDA_TRY(cudaGetLastError());
-    return MC3D_OK;
-}
-
-template <int KIND, int H>
-int launch_tma_kind(const Grid3 &g, const LineOpDev<float> &op, const TmaMapsX &maps, int nf, int epi, int py, int pz,
-                    cudaStream_t st) {
-    if (epi == EPI_STORE) return launch_tma_epi<KIND, H, 64, EPI_STORE>(g, op, maps, nf, py, pz, st);
-    if constexpr (H <= 3) {
-        if (epi == EPI_STORE_NEG) return launch_tma_epi<KIND, H, 64, EPI_STORE_NEG>(g, op, maps, nf, py, pz, st);
-    }
-    return MC3D_ERR_CONFIG;
-}
-
-}  // namespace
-
-int launch_sweep_tma_x(const Grid3 &g, const LineOpDev<float> &op, const SweepBatch<float> &b, int epi, int px,
-                       int py, int pz, cudaStream_t st) {
-    static const bool disabled = [] {
-        const char *e = std::getenv("MC3D_NO_TMA");
-        return e && e[0] == '1';
-    }();
-    if (disabled) return MC3D_ERR_CONFIG;
-    // stores and negated stores (the latter without pass-through lines) of
-    // lines up to 256 values in 64-row segments
-    if (!(epi == EPI_STORE || (epi == EPI_STORE_NEG && !px && !py && !pz))) return MC3D_ERR_CONFIG;
-    if (op.L != 64 || op.N % TMA_BOX != 0 || op.N > 256 || op.N != g.Nx) return MC3D_ERR_CONFIG;
-    if (b.nf < 1 || b.nf > TMA_MAXF) return MC3D_ERR_CONFIG;
-    const long long lines = (long long)g.Ny * g.Nz;
-    TmaMapsX maps;
-    for (int f = 0; f < b.nf; f++)
-        if (!tensor_map_x(b.in[f], g.Nx, lines, &maps.in[f]) || !tensor_map_x(b.out[f], g.Nx, lines, &maps.out[f]))
-            return MC3D_ERR_CONFIG;
-    if (op.kind == K_TRI_PER && op.H == 2) return launch_tma_kind<K_TRI_PER, 2>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_TRI_DIR && op.H == 2) return launch_tma_kind<K_TRI_DIR, 2>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_PEN_PER && op.H == 3) return launch_tma_kind<K_PEN_PER, 3>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_PEN_DIR && op.H == 3) return launch_tma_kind<K_PEN_DIR, 3>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_TRI_PER && op.H == 4) return launch_tma_kind<K_TRI_PER, 4>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_TRI_DIR && op.H == 4) return launch_tma_kind<K_TRI_DIR, 4>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_TRI_PER && op.H == 5) return launch_tma_kind<K_TRI_PER, 5>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_TRI_DIR && op.H == 5) return launch_tma_kind<K_TRI_DIR, 5>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_PEN_PER && op.H == 5) return launch_tma_kind<K_PEN_PER, 5>(g, op, maps, b.nf, epi, py, pz, st);
-    if (op.kind == K_PEN_DIR && op.H == 5) return launch_tma_kind<K_PEN_DIR, 5>(g, op, maps, b.nf, epi, py, pz, st);
-    return MC3D_ERR_CONFIG;
-}
-
 template int launch_sweep_reg<0, float>(const Grid3 &, const LineOpDev<float> &, const SweepBatch<float> &, int,
                                          const RhsFinalArgs<float> &, int, int, int, cudaStream_t);
 template int launch_sweep_reg<0, double>(const Grid3 &, const LineOpDev<double> &, const SweepBatch<double> &, int,
