@@ -70,7 +70,7 @@ struct RegVec<double> {
 // block of UB rows ahead of the block being stored, in program order before
 // those stores, so each block costs one memory round trip at most and the
 // loads overlap the previous block's stores.
-template <typename R, int E, int L>
+template <typename R, int E, int L, bool PREFETCH = true>
 __device__ __forceinline__ void reg_store_rows(const SweepBatch<R> &b, const RhsFinalArgs<R> &rf, int f, int off0,
                                                int stride, const R (&y)[L]) {
     constexpr int NB = L / UB;
@@ -84,8 +84,9 @@ __device__ __forceinline__ void reg_store_rows(const SweepBatch<R> &b, const Rhs
     const R *ax = b.aux[f];
     const R *jp = rf.J;
     // FP32: the next block's operands are fetched while this block is stored;
-    // FP64 (twice the registers per value): each block fetches its own.
-    constexpr bool AHEAD = sizeof(R) == 4;
+    // FP64 (twice the registers per value), or PREFETCH false: each block
+    // fetches its own.
+    constexpr bool AHEAD = PREFETCH && sizeof(R) == 4;
     R old[2][UB], aux[2][UB], jj[2][UB];
     auto fetch = [&](int blk, int slot) {
 #pragma unroll

@@ -87,6 +87,27 @@ int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBat
                       const RhsFinalArgs<float> &rf, const TmaMaps &maps, int px, int py, int pz, cudaStream_t st) {
     const int S = op.N / L;
     const size_t smem = 1024 + (size_t)op.N * 128 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
+    // plain and negated stores: persistent CTAs with the next tile's load in
+    // flight; the operations that read operands keep one CTA per tile (their
+    // operand buffers and the loop state exceed the register budget together)
+    if constexpr (E == EPI_STORE || E == EPI_STORE_NEG) {
+        auto kern = sweep_tma_yz_persist_kernel<DIR, KIND, H, L, E>;
+        static thread_local int configured_smem = -1;
+        static thread_local int ctas = 0;
+        if ((int)smem > configured_smem) {
+            MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured_smem = (int)smem;
+            int dev = 0, nsm = 0, per = 0;
+            MC3D_CUDA_TRY(cudaGetDevice(&dev));
+            MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * S, smem));
+            ctas = nsm * (per > 0 ? per : 1);
+        }
+        const int items = tile_count<DIR>(g) * b.nf;
+        kern<<<items < ctas ? items : ctas, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
+        MC3D_CUDA_TRY(cudaGetLastError());
+        return MC3D_OK;
+    }
     auto kern = sweep_tma_yz_kernel<DIR, KIND, H, L, E>;
     static thread_local int configured_smem = -1;
     if ((int)smem > configured_smem) {
@@ -116,16 +137,23 @@ int launch_tma_yz_kind(const Grid3 &g, const LineOpDev<float> &op, const SweepBa
 template <int KIND, int H, int L, int E>
 int launch_tma_epi(const Grid3 &g, const LineOpDev<float> &op, const TmaMaps &maps, int nf, int py, int pz,
                    cudaStream_t st) {
+    // input and output tiles, chain states; persistent CTAs, as many as fit
     const int S = op.N / L;
-    const size_t smem = 1024 + (size_t)(op.N / TMA_BOX) * 4096 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
-    auto kern = sweep_tma_x_kernel<KIND, H, L, E>;
+    const size_t smem = 1024 + 2 * (size_t)(op.N / TMA_BOX) * 4096 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
+    auto kern = sweep_tma_x_persist_kernel<KIND, H, L, E>;
     static thread_local int configured_smem = -1;
+    static thread_local int ctas = 0;
     if ((int)smem > configured_smem) {
         MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured_smem = (int)smem;
+        int dev = 0, nsm = 0, per = 0;
+        MC3D_CUDA_TRY(cudaGetDevice(&dev));
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * S, smem));
+        ctas = nsm * (per > 0 ? per : 1);
     }
-    dim3 grid(tile_count<0>(g), nf);
-    kern<<<grid, 32 * S, smem, st>>>(g, op, maps, py, pz);
+    const int items = tile_count<0>(g) * nf;
+    kern<<<items < ctas ? items : ctas, 32 * S, smem, st>>>(g, op, maps, nf, py, pz);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
