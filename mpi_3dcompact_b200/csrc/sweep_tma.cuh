@@ -18,11 +18,11 @@
 // (y lines) or of the flattened x-y index (z lines); one box of 32 points by
 // the N rows of the lines (a {32, N, 1} box of the 3-D field for y, a {32, N}
 // box of the [Nz][Nx*Ny] view for z) lands as N rows of 128 bytes with the
-// same swizzle, so the 32 lanes reading one row hit 32 banks. Results leave
-// with direct stores (one 128-byte row per warp instruction). Plain and
+// same swizzle, so the 32 lanes reading one row hit 32 banks. Plain and
 // negated stores run persistent CTAs that load the next tile during the
-// solve; the operations that read operands (accumulate, k2 assembly) run one
-// CTA per tile.
+// solve and store directly (one 128-byte row per warp instruction); the
+// operations that read operands (accumulate, k2 assembly) run one CTA per
+// tile, bring their operand tiles in by TMA during the solve and store by TMA.
 #pragma once
 #include <cuda.h>
 
@@ -36,6 +36,7 @@ constexpr int TMA_BOX = 32;   // box edge: 32 x-values (128 bytes, the swizzle s
 struct TmaMaps {
     CUtensorMap in[TMA_MAXF];
     CUtensorMap out[TMA_MAXF];
+    CUtensorMap aux[TMA_MAXF];   // partial RHS of the k2 assembly
 };
 
 // CTAs whose tile load did not complete within the wait limit
@@ -62,6 +63,12 @@ __device__ __forceinline__ unsigned swz_row(int n, int l) {
     return (unsigned)(n * 128) + (lane_part ^ (unsigned)((n & 7) << 4));
 }
 
+// y/z lines, operations that read operands (accumulate: the previous output;
+// k2 assembly: the partial RHS and, for momentum with the carry-over, the
+// previous k2): one CTA per tile. The input tile arrives by TMA; once every
+// lane holds its rows the same buffer receives the first operand tile while
+// the lanes solve, then (k2 assembly of momentum) the second; the results go
+// back into the buffer and leave by one TMA store.
 template <int DIR, int KIND, int H, int L, int E>
 __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<float> op, SweepBatch<float> b,
                                                            RhsFinalArgs<float> rf, const __grid_constant__ TmaMaps maps,
@@ -87,12 +94,10 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
         c0 = blockIdx.x * W;
     }
     const unsigned bar_a = smem_u32(&bar);
-
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // one box of `m` into the tile (thread 0)
+    auto load = [&](const CUtensorMap *m) {
+        const unsigned long long tm = reinterpret_cast<unsigned long long>(m);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(N * 128) : "memory");
-        const unsigned long long tm = reinterpret_cast<unsigned long long>(&maps.in[f]);
         if (DIR == 1)
             asm volatile(
                 "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
@@ -105,19 +110,29 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
                 "[%4];" ::"r"(smem_u32(tile)),
                 "l"(tm), "r"(c0), "r"(0), "r"(bar_a)
                 : "memory");
+    };
+    // bounded wait for the phase of the given parity; the CTA decides together
+    auto wait = [&](unsigned parity) -> bool {
+        unsigned done = 0;
+        for (int it = 0; it < (1 << 22) && !done; it++)
+            asm volatile(
+                "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(bar_a), "r"(parity)
+                : "memory");
+        if (__syncthreads_and(done != 0)) return true;
+        if (threadIdx.x == 0) atomicAdd(&g_tma_wait_timeouts, 1);
+        return false;
+    };
+    auto at = [&](int r) -> R & { return *reinterpret_cast<R *>(tile + swz_row(a + r, lane)); };
+
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        load(&maps.in[f]);
     }
     __syncthreads();
-    unsigned done = 0;
-    for (int it = 0; it < (1 << 22) && !done; it++)
-        asm volatile(
-            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\nselp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(bar_a)
-            : "memory");
-    if (!__syncthreads_and(done != 0)) {
-        if (threadIdx.x == 0) atomicAdd(&g_tma_wait_timeouts, 1);
-        return;
-    }
+    if (!wait(0)) return;
 
     const TileGeom t = tile_geom<DIR>(g, blockIdx.x, lane);
     bool pass;
@@ -141,13 +156,54 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
         }
         v[k] = in ? *reinterpret_cast<const R *>(tile + swz_row(n, lane)) : R(0);
     }
+    __syncthreads();   // every lane holds its rows: the tile takes the first operand
+    const bool mom = E == EPI_RHS_FINAL && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
+    if (threadIdx.x == 0) load(E == EPI_SUB ? &maps.out[f] : &maps.aux[f]);
 
     R y[L];
     reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
 
-    // operations that read operands (accumulate, k2 assembly): direct stores
-    // with the operands fetched a block of rows ahead
-    if (t.active) reg_store_rows<R, E, L>(b, rf, f, (int)t.base + a * (int)t.stride, (int)t.stride, y);
+    if (!wait(1)) return;
+    // accumulate: old - v; k2 assembly: tt = aux - v (src/CurvilinearCSolver_Core.cpp:790-947)
+#pragma unroll
+    for (int r = 0; r < L; r++) y[r] = at(r) - y[r];
+    if (E == EPI_RHS_FINAL) {
+        if (mom) {
+            __syncthreads();   // every lane has read the partial RHS
+            if (threadIdx.x == 0) load(&maps.out[f]);
+            if (!wait(0)) return;
+#pragma unroll
+            for (int r = 0; r < L; r++) y[r] = at(r) + y[r];
+        }
+        const R dt = (R)(*rf.dt);
+        if (!rf.J) {
+            const R dtJ = dt * rf.Jc;
+#pragma unroll
+            for (int r = 0; r < L; r++) y[r] = y[r] * dtJ;
+        } else if (t.active) {
+            const int off0 = (int)t.base + a * (int)t.stride, stride = (int)t.stride;
+#pragma unroll
+            for (int r = 0; r < L; r++) y[r] = y[r] * (dt * rf.J[off0 + r * stride]);
+        }
+    }
+    __syncthreads();   // every lane has read its operands
+#pragma unroll
+    for (int r = 0; r < L; r++) at(r) = y[r];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long tm = reinterpret_cast<unsigned long long>(&maps.out[f]);
+        if (DIR == 1)
+            asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
+                         "r"(c0), "r"(0), "r"(c2), "r"(smem_u32(tile))
+                         : "memory");
+        else
+            asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tm),
+                         "r"(c0), "r"(0), "r"(smem_u32(tile))
+                         : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
 }
 
 // Persistent form of the y/z kernel (plain and negated stores): each CTA

@@ -88,8 +88,8 @@ int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBat
     const int S = op.N / L;
     const size_t smem = 1024 + (size_t)op.N * 128 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
     // plain and negated stores: persistent CTAs with the next tile's load in
-    // flight; the operations that read operands keep one CTA per tile (their
-    // operand buffers and the loop state exceed the register budget together)
+    // flight; the operations that read operands: one CTA per tile, the
+    // operand tiles arriving by TMA during the solve
     if constexpr (E == EPI_STORE || E == EPI_STORE_NEG) {
         auto kern = sweep_tma_yz_persist_kernel<DIR, KIND, H, L, E>;
         static thread_local int configured_smem = -1;
@@ -107,17 +107,18 @@ int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBat
         kern<<<items < ctas ? items : ctas, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
         MC3D_CUDA_TRY(cudaGetLastError());
         return MC3D_OK;
+    } else {
+        auto kern = sweep_tma_yz_kernel<DIR, KIND, H, L, E>;
+        static thread_local int configured_smem = -1;
+        if ((int)smem > configured_smem) {
+            MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured_smem = (int)smem;
+        }
+        dim3 grid(tile_count<DIR>(g), b.nf);
+        kern<<<grid, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
+        MC3D_CUDA_TRY(cudaGetLastError());
+        return MC3D_OK;
     }
-    auto kern = sweep_tma_yz_kernel<DIR, KIND, H, L, E>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
-    dim3 grid(tile_count<DIR>(g), b.nf);
-    kern<<<grid, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
-    MC3D_CUDA_TRY(cudaGetLastError());
-    return MC3D_OK;
 }
 
 template <int DIR, int KIND, int H>
@@ -215,9 +216,11 @@ int launch_sweep_tma_yz(int dir, const Grid3 &g, const LineOpDev<float> &op, con
     if (op.L != 64 || op.N != n || n > 256) return MC3D_ERR_CONFIG;
     if (b.nf < 1 || b.nf > TMA_MAXF) return MC3D_ERR_CONFIG;
     TmaMaps maps;
-    for (int f = 0; f < b.nf; f++)
+    for (int f = 0; f < b.nf; f++) {
         if (!tensor_map_yz(dir, b.in[f], g, &maps.in[f]) || !tensor_map_yz(dir, b.out[f], g, &maps.out[f]))
             return MC3D_ERR_CONFIG;
+        if (epi == EPI_RHS_FINAL && !tensor_map_yz(dir, b.aux[f], g, &maps.aux[f])) return MC3D_ERR_CONFIG;
+    }
 #define MC3D_TCASE(K, HH)                                                                                    \
     if (op.kind == K && op.H == HH)                                                                          \
         return dir == 1 ? launch_tma_yz_kind<1, K, HH>(g, op, b, epi, rf, maps, px, py, pz, st)              \
