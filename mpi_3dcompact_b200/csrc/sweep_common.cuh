@@ -82,10 +82,15 @@ __host__ __device__ __forceinline__ int tile_count(const Grid3 &g) {
 // rows per register block of the line solves
 constexpr int UB = 8;
 
-// shared-memory bytes of the register-resident kernel: chain states,
-// correction scalars and, for x lines, the transposed tile
+// elements of the segment-chain area of the register-resident solve: the
+// local end states of both passes ([2][S][2][W]) and the last two values of
+// the last segment ([2][W])
+__host__ __device__ constexpr int reg_chain_elems(int S) { return 4 * S * W + 2 * W; }
+
+// shared-memory bytes of the register-resident kernel: chain states and, for
+// x lines, the transposed tile
 inline size_t reg_smem_bytes(int dir, int N, int S, size_t esize) {
-    return ((size_t)8 * S * W + 6 * W + (dir == 0 ? (size_t)N * (W + 1) : 0)) * esize;
+    return ((size_t)reg_chain_elems(S) + (dir == 0 ? (size_t)N * (W + 1) : 0)) * esize;
 }
 
 // Register-resident segmented line solve along DIR (sweep_reg.cuh); returns

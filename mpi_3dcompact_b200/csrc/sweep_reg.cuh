@@ -191,9 +191,10 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
 // The solve of one tile once each lane holds rows a-H .. a+L+H-1 of its line
 // in v: Dirichlet boundary rows, pass 1, the forward chain and fold, pass 2,
 // the backward chain, fold and cyclic correction; y gets the solution rows
-// a .. a+L-1. sh: the chain-state area of the shared memory ([4][S][2][W]
-// states, [2][W] last values, [W][4] correction scalars). Every thread of the
-// CTA calls it (it synchronises the CTA).
+// a .. a+L-1. sh: the chain-state area of the shared memory (reg_chain_elems:
+// the segments' local end states of both passes and the last segment's last
+// two values). Every thread of the CTA calls it (it synchronises the CTA
+// twice; each warp then chains the states it needs itself).
 template <typename R, int KIND, int H, int L>
 __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L + 2 * H], R (&y)[L], bool work,
                                           int lane, int seg, int S, int a, R *sh) {
@@ -203,11 +204,8 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
     using V = RegVec<R>;
     const int N = op.N;
     R *fwdEnd = sh;                    // [S][2][W] local end states of pass 1
-    R *fwdIn = fwdEnd + S * 2 * W;     // [S][2][W] incoming forward states
-    R *bwdStart = fwdIn + S * 2 * W;   // [S][2][W] local start values of pass 2
-    R *bwdNext = bwdStart + S * 2 * W; // [S][2][W] incoming backward states
-    R *lastx = bwdNext + S * 2 * W;    // [2][W] x_{N-1}, x_{N-2}
-    R *scorr = lastx + 2 * W;          // [W][4] cyclic correction scalars
+    R *bwdStart = fwdEnd + S * 2 * W;  // [S][2][W] local start values of pass 2
+    R *lastx = bwdStart + S * 2 * W;   // [2][W] x_{N-1}, x_{N-2}
 
     // ---- Dirichlet boundary rows (first / last segment) ----
     R headr[H], tailr[H];
@@ -278,29 +276,23 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
     fwdEnd[(seg * 2 + 1) * W + lane] = y2;
     __syncthreads();
 
-    // ---- chain the forward states: incoming (y_{a-1}, y_{a-2}) of every segment ----
-    if (seg == 0) {
-        R X1 = 0, X2 = 0;
-        fwdIn[lane] = 0;
-        fwdIn[W + lane] = 0;
-        for (int ws = 1; ws < S; ws++) {
-            const int e1 = ws * L - 1, e2 = e1 - 1;
-            R s1a, s1b, s2a, s2b;
-            V::ld2(op.sf2 + 2 * e1, s1a, s1b);
-            V::ld2(op.sf2 + 2 * e2, s2a, s2b);
-            R n1 = fwdEnd[((ws - 1) * 2 + 0) * W + lane] + s1a * X1 + s1b * X2;
-            R n2 = fwdEnd[((ws - 1) * 2 + 1) * W + lane] + s2a * X1 + s2b * X2;
-            X1 = work ? n1 : R(0);
-            X2 = work ? n2 : R(0);
-            fwdIn[(ws * 2 + 0) * W + lane] = X1;
-            fwdIn[(ws * 2 + 1) * W + lane] = X2;
-        }
+    // ---- chain the forward states up to this segment: its incoming (y_{a-1}, y_{a-2}) ----
+    // (each warp runs the chain of the segments before its own, so no further
+    // barrier is needed)
+    R F1 = 0, F2 = 0;
+    for (int ws = 1; ws <= seg; ws++) {
+        const int e1 = ws * L - 1, e2 = e1 - 1;
+        R s1a, s1b, s2a, s2b;
+        V::ld2(op.sf2 + 2 * e1, s1a, s1b);
+        V::ld2(op.sf2 + 2 * e2, s2a, s2b);
+        R n1 = fwdEnd[((ws - 1) * 2 + 0) * W + lane] + s1a * F1 + s1b * F2;
+        R n2 = fwdEnd[((ws - 1) * 2 + 1) * W + lane] + s2a * F1 + s2b * F2;
+        F1 = work ? n1 : R(0);
+        F2 = work ? n2 : R(0);
     }
-    __syncthreads();
 
     // ---- forward fold: propagate the incoming state through the first kf rows ----
     if (seg > 0) {
-        R F1 = fwdIn[(seg * 2 + 0) * W + lane], F2 = fwdIn[(seg * 2 + 1) * W + lane];
         const int kf = op.seg_kf;
 #pragma unroll
         for (int blk = 0; blk < NB; blk++) {
@@ -372,12 +364,14 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
     }
     __syncthreads();
 
-    // ---- chain the backward states; cyclic correction scalars ----
-    if (seg == 0) {
+    // ---- chain the backward states down to this segment (periodic lines: down
+    // to the first, for the cyclic correction scalars); every warp runs it ----
+    R G1 = 0, G2 = 0;   // incoming backward state of this segment
+    R c[4] = {R(0), R(0), R(0), R(0)};
+    {
         R Y1 = 0, Y2 = 0;
-        bwdNext[((S - 1) * 2 + 0) * W + lane] = 0;
-        bwdNext[((S - 1) * 2 + 1) * W + lane] = 0;
-        for (int ws = S - 2; ws >= 0; ws--) {
+        const int wlo = PER ? 0 : seg;
+        for (int ws = S - 2; ws >= wlo; ws--) {
             const int s0 = (ws + 1) * L;
             R b1a, b1b, b2a, b2b;
             V::ld2(op.sb2 + 2 * s0, b1a, b1b);
@@ -386,10 +380,11 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
             R n2 = bwdStart[((ws + 1) * 2 + 1) * W + lane] + b2a * Y1 + b2b * Y2;
             Y1 = work ? n1 : R(0);
             Y2 = work ? n2 : R(0);
-            bwdNext[(ws * 2 + 0) * W + lane] = Y1;
-            bwdNext[(ws * 2 + 1) * W + lane] = Y2;
+            if (ws == seg) {
+                G1 = Y1;
+                G2 = Y2;
+            }
         }
-        R c[4] = {R(0), R(0), R(0), R(0)};
         if (work && PER) {
             // final x_0, x_1 (first segment, folded) and x_{N-1}, x_{N-2} (last segment)
             R b0a, b0b, b1a, b1b;
@@ -413,14 +408,10 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                 c[3] = op.Hm[12] * r0 + op.Hm[13] * r1 + op.Hm[14] * r2 + op.Hm[15] * r3;
             }
         }
-#pragma unroll
-        for (int k = 0; k < 4; k++) scorr[lane * 4 + k] = c[k];
     }
-    __syncthreads();
 
     // ---- backward fold: propagate the incoming state up through the last kb rows ----
     if (seg < S - 1) {
-        R G1 = bwdNext[(seg * 2 + 0) * W + lane], G2 = bwdNext[(seg * 2 + 1) * W + lane];
         const int kb = op.seg_kb;
 #pragma unroll
         for (int blk = NB - 1; blk >= 0; blk--) {
@@ -455,8 +446,7 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
 
     // ---- cyclic correction (src/Utils.cpp:45 and :183-190) where its columns matter ----
     if (PER) {
-        const R c0 = scorr[lane * 4 + 0], c1 = scorr[lane * 4 + 1], c2 = scorr[lane * 4 + 2],
-                c3 = scorr[lane * 4 + 3];
+        const R c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
 #pragma unroll
         for (int blk = 0; blk < NB; blk++) {
             const int n0 = a + blk * UB;
@@ -491,7 +481,7 @@ __global__ void __launch_bounds__(512) sweep_reg_kernel(Grid3 g, LineOpDev<R> op
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int N = op.N, a = seg * L;
     const int f = blockIdx.y;
-    R *tile = sh + 8 * S * W + 6 * W;  // x lines: [N][W+1], after the chain states
+    R *tile = sh + reg_chain_elems(S);   // x lines: [N][W+1], after the chain states
 
     const TileGeom t = tile_geom<DIR>(g, blockIdx.x, lane);
     bool pass = false;

@@ -86,7 +86,7 @@ template <int DIR, int KIND, int H, int L, int E>
 int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBatch<float> &b,
                       const RhsFinalArgs<float> &rf, const TmaMaps &maps, int px, int py, int pz, cudaStream_t st) {
     const int S = op.N / L;
-    const size_t smem = 1024 + (size_t)op.N * 128 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
+    const size_t smem = 1024 + (size_t)op.N * 128 + (size_t)reg_chain_elems(S) * sizeof(float);
     // plain and negated stores: persistent CTAs with the next tile's load in
     // flight; the operations that read operands: one CTA per tile, the
     // operand tiles arriving by TMA during the solve
@@ -140,7 +140,7 @@ int launch_tma_epi(const Grid3 &g, const LineOpDev<float> &op, const TmaMaps &ma
                    cudaStream_t st) {
     // input and output tiles, chain states; persistent CTAs, as many as fit
     const int S = op.N / L;
-    const size_t smem = 1024 + 2 * (size_t)(op.N / TMA_BOX) * 4096 + ((size_t)8 * S * W + 6 * W) * sizeof(float);
+    const size_t smem = 1024 + 2 * (size_t)(op.N / TMA_BOX) * 4096 + (size_t)reg_chain_elems(S) * sizeof(float);
     auto kern = sweep_tma_x_persist_kernel<KIND, H, L, E>;
     static thread_local int configured_smem = -1;
     static thread_local int ctas = 0;
