@@ -372,6 +372,12 @@ int mc3d_solver_sync(mc3d_solver s);
 int mc3d_solver_set_timing(mc3d_solver s, int enable);
 const char *mc3d_solver_timing_report(mc3d_solver s);
 
+/* Number of line-solve CTAs on `device` whose TMA tile load did not arrive
+ * within the kernel's bounded wait (they skipped their tile: the results of
+ * that launch are invalid). mc3d_solver_info and mc3d_solver_get_conserved
+ * return MC3D_ERR_TIMEOUT when it is nonzero. */
+int mc3d_tma_wait_timeouts(int device, int *count);
+
 /* ---- allocation-free CFL reduction ----
  * No counterpart in the reference: an extra entry point for callers that must
  * not have the library allocate device memory (a host code that hands all GPU

@@ -194,6 +194,14 @@ def write_dump(path, time_step, time, fields):
     N.check(N.host_lib().mc3d_dump_write(str(path).encode(), int(time_step), float(time), nx, ny, nz, p))
 
 
+def tma_wait_timeouts(device=0):
+    """Line-solve CTAs on `device` whose TMA tile load gave up waiting (0 in a
+    healthy run)."""
+    n = C.c_int()
+    N.check(N.host_lib().mc3d_tma_wait_timeouts(int(device), C.byref(n)))
+    return n.value
+
+
 def append_turbdata_line(path, values):
     """Append one turbdata.out line: the values as the HIT driver's ofstream
     with precision 17 prints them, each followed by a space

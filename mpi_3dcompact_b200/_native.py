@@ -97,6 +97,7 @@ def host_lib():
             "mc3d_solver_turbdata": (ip, [vp, dp, C.POINTER(dp)]),
             "mc3d_solver_wall_span_average": (ip, [vp] + [C.POINTER(dp)] * 4),
             "mc3d_solver_wake_strip": (ip, [vp, C.c_int, C.c_int, C.POINTER(dp)]),
+            "mc3d_tma_wait_timeouts": (ip, [C.c_int, C.POINTER(C.c_int)]),
             "mc3d_solver_read_stats": (ip, [vp, C.c_char_p, C.c_char_p]),
             "mc3d_solver_run": (ip, [vp, C.c_char_p]),
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),

@@ -399,6 +399,10 @@ int launch_turb_sums(const Grid3 &g, const R *const prim[5], const R *const d[12
 int launch_wall_span_average(const Grid3 &g, const double *const q[5], double *out, cudaStream_t st);
 int launch_wake_strip(const Grid3 &g, const double *const q[5], int i, int j, double *out, cudaStream_t st);
 
+// CTAs of the TMA-staged line solves on the current device whose tile load
+// did not arrive within the wait limit (their results are invalid)
+int tma_wait_timeouts(int *count);
+
 // ---- checkpoint files (checkpoint.cpp) ----------------------------------------
 int write_solution_dump(const char *path, int time_step, double time, int Nx, int Ny, int Nz,
                         const double *const fields[8]);

@@ -551,6 +551,14 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
     return MC3D_OK;
 }
 
+// MC3D_ERR_TIMEOUT when a line-solve tile load gave up waiting on this device
+static int tma_timeouts_failed(mc3d_solver s) {
+    (void)s;
+    int n = 0;
+    if (int rc = tma_wait_timeouts(&n)) return rc;
+    return n ? fail(MC3D_ERR_TIMEOUT, "a line-solve tile load did not arrive within the wait limit") : MC3D_OK;
+}
+
 // bit f: face f is a SPONGE
 static int sponge_faces(mc3d_solver s) {
     int faces = 0;
@@ -1517,6 +1525,7 @@ int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *
     TimeState t;
     MC3D_CUDA_TRY(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
     if (t.nonfinite) return fail(MC3D_ERR_NONFINITE, "the state became non-finite");
+    if (int rc_tma = tma_timeouts_failed(s)) return rc_tma;
     return MC3D_OK;
 }
 
@@ -1735,6 +1744,7 @@ int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, lo
     if (dt) *dt = t.dt;
     if (stages) *stages = s->stages;
     if (t.nonfinite) return fail(MC3D_ERR_NONFINITE, "the state became non-finite");
+    if (int rc_tma = tma_timeouts_failed(s)) return rc_tma;
     return MC3D_OK;
 }
 

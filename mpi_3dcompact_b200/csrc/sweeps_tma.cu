@@ -239,4 +239,15 @@ int launch_sweep_tma_yz(int dir, const Grid3 &g, const LineOpDev<float> &op, con
     return MC3D_ERR_CONFIG;
 }
 
+int tma_wait_timeouts(int *count) {
+    MC3D_CUDA_TRY(cudaMemcpyFromSymbol(count, g_tma_wait_timeouts, sizeof(int)));
+    return MC3D_OK;
+}
+
 }  // namespace mc3d
+
+extern "C" int mc3d_tma_wait_timeouts(int device, int *count) {
+    if (!count) return mc3d::fail(MC3D_ERR_ARG, "null argument");
+    MC3D_CUDA_TRY(cudaSetDevice(device));
+    return mc3d::tma_wait_timeouts(count);
+}

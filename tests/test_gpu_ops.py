@@ -166,3 +166,30 @@ def test_register_kernel_pass_through_lines(prec):
             face = [slice(None)] * 3
             face[2 - (d + 1) % 3] = 0
             assert np.array_equal(out[tuple(face)], x.double().cpu().numpy()[tuple(face)]), (op, d)
+
+
+def test_tma_line_solves_complete_their_waits():
+    """The TMA-staged FP32 line solves (256-point lines: persistent x and y/z
+    kernels) finish without a bounded wait giving up, and agree with the
+    FP64 solve of the same field."""
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    shape = (256, 64, 256)
+    f = rng.standard_normal(shape)
+    x32 = torch.tensor(f, dtype=torch.float32, device="cuda")
+    x64 = torch.tensor(f, dtype=torch.float64, device="cuda")
+    bcs = [m.PERIODIC_SOLVE] * 3
+    for d in (0, 2):
+        for op in ("PENTA10", "COMPACT8"):
+            y32, y64 = torch.empty_like(x32), torch.empty_like(x64)
+            o32, o64 = _make(op, d, bcs, shape, m.FP32BULK), _make(op, d, bcs, shape, m.FP64)
+            if op.startswith("COMPACT"):
+                o32.filterField(x32, y32)
+                o64.filterField(x64, y64)
+            else:
+                o32.calc1stDerivField(x32, y32)
+                o64.calc1stDerivField(x64, y64)
+            torch.cuda.synchronize()
+            err = H.rel_max(y32.double().cpu().numpy(), y64.cpu().numpy())
+            assert err <= TOL[m.FP32BULK], (op, d, err)
+    assert m.tma_wait_timeouts(0) == 0
