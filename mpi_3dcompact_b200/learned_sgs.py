@@ -14,7 +14,13 @@ Pipeline, all on the GPU:
    and Pr_t from the SGS heat flux;
 5. Adam on the MSE of normalised targets (``MLPClosure.train_step``); the
    feature normalisation and the training range (outside which the solver
-   falls back to DSM) come from the training set.
+   falls back to DSM) come from the training set;
+6. a posteriori calibration of the coefficient: LES of decaying HIT on the
+   coarse grid from held-out seeds with the closure and with DSM, and the one
+   scale of C whose decayed kinetic energy stays closest to DSM's is folded
+   into the output normalisation (``calibrate_output_scale``). The pointwise
+   least-squares coefficients of the box-filtered DNS dissipate several times
+   more than the compact-filtered LES needs.
 """
 from __future__ import annotations
 
@@ -119,3 +125,65 @@ def train(mlp: MLPClosure, x, y, steps=2000, batch=65536, lr=1e-3, seed=0):
         idx = torch.randint(0, n, (min(batch, n),), device="cuda", generator=g)
         hist.append(mlp.train_step(x[idx].contiguous(), yn[idx].contiguous(), lr))
     return hist
+
+
+# LES of the calibration (the a posteriori configuration of the closure)
+LES_SCHEME = dict(fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", les_avg="GLOBAL", cfl=0.5)
+
+
+def scale_output(mlp: MLPClosure, s):
+    """Multiply the closure's coefficient C by s > 0 (C = max(0, out * ystd +
+    ymean) scales with ymean and ystd)."""
+    nrm = mlp.normalization()
+    ym, ys = nrm["ymean"].copy(), nrm["ystd"].copy()
+    ym[0] *= s
+    ys[0] *= s
+    mlp.set_normalization(nrm["mean"], nrm["std"], nrm["lo"], nrm["hi"], ym, ys)
+
+
+def decayed_energy(les, mlp=None, n=128, seed=1, steps=500, chunk=50, mu_ref=2.5e-4, k0=4.0, mt=0.3, frac=1.0):
+    """Kinetic energy every `chunk` steps of an FP32-bulk LES of decaying HIT
+    on n^3 (LES_SCHEME) with closure `les` ("MLP" uses `mlp` with fallback
+    fraction `frac`)."""
+    from . import FP32BULK
+    ic = hit_initial_condition(n, k0=k0, seed=seed, mt=mt)
+    kw = dict(grid=n, mu_ref=mu_ref, les=les, precision=FP32BULK, **LES_SCHEME)
+    if les == "MLP":
+        kw["mlp_fallback_frac"] = frac
+    s = CurvilinearCSolver(Options(**kw))
+    s.set_box_metrics(2.0 * math.pi)
+    s.set_initial_conditions(*ic)
+    if les == "MLP":
+        s.set_mlp(mlp)
+    ke = [s.integrals()[0]]
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        s.step(k)
+        done += k
+        ke.append(s.integrals()[0])
+    return np.array(ke)
+
+
+def decay_difference(ke, ke_ref):
+    """Largest relative difference of the decayed energy KE(0) - KE(t) over
+    the checkpoints."""
+    d, r = ke[0] - ke, ke_ref[0] - ke_ref
+    return float(np.max(np.abs(d[1:] - r[1:]) / np.abs(r[1:])))
+
+
+def calibrate_output_scale(mlp: MLPClosure, seeds=(1, 2), scales=(0.15, 0.2, 0.25, 0.3, 0.4, 0.55, 0.7, 1.0),
+                           **les_kw):
+    """A posteriori calibration: the scale of C (from `scales`) minimising the
+    largest decay difference to DSM over LES from `seeds` (no DSM fallback),
+    applied to `mlp`; returns (scale, {scale: [difference per seed]})."""
+    ref = {sd: decayed_energy("DSM", seed=sd, **les_kw) for sd in seeds}
+    nrm = mlp.normalization()
+    table = {}
+    for sc in scales:
+        scale_output(mlp, sc)
+        table[sc] = [decay_difference(decayed_energy("MLP", mlp, seed=sd, **les_kw), ref[sd]) for sd in seeds]
+        mlp.set_normalization(nrm["mean"], nrm["std"], nrm["lo"], nrm["hi"], nrm["ymean"], nrm["ystd"])
+    best = min(table, key=lambda k: max(table[k]))
+    scale_output(mlp, best)
+    return best, table

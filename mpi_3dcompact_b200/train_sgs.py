@@ -2,14 +2,20 @@
 closure file the solver loads (``MLPClosure.load``).
 
     python -m mpi_3dcompact_b200.train_sgs --dns 512 --factor 4 --seeds 0 \\
-        --snapshots 20,60,120,240,400 --steps 3000 --out mpi_3dcompact_b200/data/mlp_sgs_hit128.bin
+        --snapshots 20,60,120,240,400 --steps 3000 --calibrate-seeds 1,2 \\
+        --out mpi_3dcompact_b200/data/mlp_sgs_hit128.bin
+
+    python -m mpi_3dcompact_b200.train_sgs --init <trained file> --calibrate-seeds 1,2 --out <file>
+        (calibration of an already trained closure)
 
 DNS: decaying HIT (PADE6, RK4, COMPACT10 alpha 0.49, Mt 0.3, k0 4) on dns^3
 points; box filter of `factor` gives the (dns/factor)^3 LES grid the closure
 is trained for (the grid scale enters its features). The snapshots span the
 decay (DNS step 400 is about LES step 100 at four times the time step), so
 that an LES of that length stays inside the training range. Adam, lr 1e-3,
-batch 65536.
+batch 65536. Then the coefficient C is calibrated a posteriori: one scale,
+chosen on (dns/factor)^3 LES from the held-out calibration seeds so that the
+decayed kinetic energy stays closest to DSM's (learned_sgs.calibrate_output_scale).
 """
 from __future__ import annotations
 
@@ -29,6 +35,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", required=True)
+    ap.add_argument("--init", default=None, help="calibrate this trained closure instead of training one")
+    ap.add_argument("--calibrate-seeds", default="1,2", help="LES seeds of the calibration ('' to skip it)")
     a = ap.parse_args(argv)
 
     import torch
@@ -36,6 +44,15 @@ def main(argv=None):
     from . import MLPClosure
     from . import learned_sgs as L
 
+    if a.init:
+        mlp = MLPClosure(seed=0)
+        mlp.load(a.init)
+        best, table = L.calibrate_output_scale(mlp, seeds=[int(s) for s in a.calibrate_seeds.split(",")],
+                                               n=a.dns // a.factor, mu_ref=a.mu_ref)
+        mlp.save(a.out)
+        print(json.dumps({"calibration_scale": best, "decay_difference": {str(k): v for k, v in table.items()},
+                          "out": a.out}))
+        return
     t0 = time.time()
     xs, ys = [], []
     seeds = [int(s) for s in a.seeds.split(",")]
@@ -53,9 +70,15 @@ def main(argv=None):
     L.fit_normalization(mlp, x, y)
     hist = L.train(mlp, x, y, steps=a.steps, batch=a.batch, lr=a.lr)
     t2 = time.time()
+    best, table = None, None
+    if a.calibrate_seeds:
+        best, table = L.calibrate_output_scale(mlp, seeds=[int(s) for s in a.calibrate_seeds.split(",")],
+                                               n=a.dns // a.factor, mu_ref=a.mu_ref)
     mlp.save(a.out)
     print(json.dumps({"samples": int(x.shape[0]), "loss_first": hist[0], "loss_last": hist[-1],
-                      "dns_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "out": a.out}))
+                      "dns_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "calibration_scale": best,
+                      "decay_difference": None if table is None else {str(k): v for k, v in table.items()},
+                      "out": a.out}))
 
 
 if __name__ == "__main__":
