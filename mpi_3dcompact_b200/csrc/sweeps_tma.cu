@@ -87,10 +87,10 @@ int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBat
                       const RhsFinalArgs<float> &rf, const TmaMaps &maps, int px, int py, int pz, cudaStream_t st) {
     const int S = op.N / L;
     const size_t smem = 1024 + (size_t)op.N * 128 + (size_t)reg_chain_elems(S) * sizeof(float);
-    // plain and negated stores: persistent CTAs with the next tile's load in
+    // plain, negated and FP64 stores: persistent CTAs with the next tile's load in
     // flight; the operations that read operands: one CTA per tile, the
     // operand tiles arriving by TMA during the solve
-    if constexpr (E == EPI_STORE || E == EPI_STORE_NEG) {
+    if constexpr (E == EPI_STORE || E == EPI_STORE_NEG || E == EPI_STORE_F64) {
         auto kern = sweep_tma_yz_persist_kernel<DIR, KIND, H, L, E>;
         static thread_local int configured_smem = -1;
         static thread_local int ctas = 0;
@@ -125,6 +125,10 @@ template <int DIR, int KIND, int H>
 int launch_tma_yz_kind(const Grid3 &g, const LineOpDev<float> &op, const SweepBatch<float> &b, int epi,
                        const RhsFinalArgs<float> &rf, const TmaMaps &maps, int px, int py, int pz, cudaStream_t st) {
     if (epi == EPI_STORE) return launch_tma_yz_epi<DIR, KIND, H, 64, EPI_STORE>(g, op, b, rf, maps, px, py, pz, st);
+    if constexpr (H >= 4) {
+        if (epi == EPI_STORE_F64)
+            return launch_tma_yz_epi<DIR, KIND, H, 64, EPI_STORE_F64>(g, op, b, rf, maps, px, py, pz, st);
+    }
     if constexpr (H <= 3) {
         if (epi == EPI_STORE_NEG)
             return launch_tma_yz_epi<DIR, KIND, H, 64, EPI_STORE_NEG>(g, op, b, rf, maps, px, py, pz, st);
@@ -209,16 +213,20 @@ int launch_sweep_tma_yz(int dir, const Grid3 &g, const LineOpDev<float> &op, con
     }();
     if (disabled || (dir != 1 && dir != 2)) return MC3D_ERR_CONFIG;
     // the operations of the derivative and filter sweeps; pass-through lines
-    // only with plain stores
-    if (!(epi == EPI_STORE || epi == EPI_STORE_NEG || epi == EPI_SUB || epi == EPI_RHS_FINAL)) return MC3D_ERR_CONFIG;
-    if (epi != EPI_STORE && (px || py || pz)) return MC3D_ERR_CONFIG;
+    // only with the plain and FP64 stores of the filters
+    if (!(epi == EPI_STORE || epi == EPI_STORE_NEG || epi == EPI_SUB || epi == EPI_RHS_FINAL || epi == EPI_STORE_F64))
+        return MC3D_ERR_CONFIG;
+    if (epi != EPI_STORE && epi != EPI_STORE_F64 && (px || py || pz)) return MC3D_ERR_CONFIG;
     const int n = dir == 1 ? g.Ny : g.Nz;
     if (op.L != 64 || op.N != n || n > 256) return MC3D_ERR_CONFIG;
     if (b.nf < 1 || b.nf > TMA_MAXF) return MC3D_ERR_CONFIG;
     TmaMaps maps;
+    // input tiles for every operation; the output (TMA store and previous
+    // values) and partial-RHS tiles for the operations that read operands
+    const bool operands = epi == EPI_SUB || epi == EPI_RHS_FINAL;
     for (int f = 0; f < b.nf; f++) {
-        if (!tensor_map_yz(dir, b.in[f], g, &maps.in[f]) || !tensor_map_yz(dir, b.out[f], g, &maps.out[f]))
-            return MC3D_ERR_CONFIG;
+        if (!tensor_map_yz(dir, b.in[f], g, &maps.in[f])) return MC3D_ERR_CONFIG;
+        if (operands && !tensor_map_yz(dir, b.out[f], g, &maps.out[f])) return MC3D_ERR_CONFIG;
         if (epi == EPI_RHS_FINAL && !tensor_map_yz(dir, b.aux[f], g, &maps.aux[f])) return MC3D_ERR_CONFIG;
     }
 #define MC3D_TCASE(K, HH)                                                                                    \

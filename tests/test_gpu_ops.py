@@ -135,16 +135,17 @@ def test_segmented_lines_vs_oracle(n, bc, prec):
             assert err <= TOL[prec], (op, n, d, bc, err)
 
 
-@pytest.mark.parametrize("prec", [m.FP64, m.FP32BULK])
-def test_register_kernel_pass_through_lines(prec):
+@pytest.mark.parametrize("prec,n", [(m.FP64, 64), (m.FP32BULK, 64), (m.FP32BULK, 128)])
+def test_register_kernel_pass_through_lines(prec, n):
     """Filter lines on the faces of the other (Dirichlet) directions pass
     through unchanged (Compact10Filter::filterField) in the register-resident
-    kernel: 64-point lines in every direction, against the oracle."""
+    kernels (64-point lines) and the TMA-staged ones (128-point FP32 lines), in
+    every direction, against the oracle."""
     torch = _torch()
     from oracle import mc3d_oracle as O
     rng = np.random.default_rng(11)
     dt = torch.float64 if prec == m.FP64 else torch.float32
-    shape = (64, 64, 64)
+    shape = (n, n, n)
     f = rng.standard_normal(shape)
     x = torch.tensor(f, dtype=dt, device="cuda")
     for d in range(3):
