@@ -62,6 +62,23 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest x over the ranks (the slowest rank's time); x itself
+    without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(ws, points, stages, seconds):
+    """Whole-job grid-point RK stages per second: ws replicas of `points`
+    points each ran `stages` stages within `seconds` (the slowest rank)."""
+    return ws * float(points) * stages / seconds
+
+
 def lsldd_stages(first_step: int, nsteps: int) -> int:
     """Stages of LSLDDRK4 steps first_step..first_step+nsteps-1 (1-based): odd
     steps run the 5-stage half, even steps the 6-stage half."""
@@ -421,12 +438,9 @@ def run_ours(args):
     clocks.start()
     ms, stages, launches, rep = timed(s32, args.steps, args.warmup, True)
     clk = clocks.stop()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     pts = float(n) ** 3
-    value = ws * pts * stages / (ms * 1e-3)
+    value = job_rate(ws, pts, stages, ms * 1e-3)
     q32 = s32.conserved()
     del s32
 
@@ -466,11 +480,8 @@ def run_ours(args):
         barrier()
         st_e = se.info()["stages"]
         del se
-        if dist is not None:
-            t = torch.tensor([wall], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
-        e2e = {"value": ws * pts * st_e / wall, "unit": UNIT,
+        wall = max_over_ranks(wall, dist, "cuda")
+        e2e = {"value": job_rate(ws, pts, st_e, wall), "unit": UNIT,
                "h2d_bytes_per_step": int(5 * 8 * pts / args.steps),
                "d2h_bytes_per_step": int(5 * 8 * pts / args.steps + 32)}
         del out
