@@ -141,10 +141,12 @@ def scale_output(mlp: MLPClosure, s):
     mlp.set_normalization(nrm["mean"], nrm["std"], nrm["lo"], nrm["hi"], ym, ys)
 
 
-def decayed_energy(les, mlp=None, n=128, seed=1, steps=500, chunk=50, mu_ref=2.5e-4, k0=4.0, mt=0.3, frac=1.0):
+def decayed_energy(les, mlp=None, n=128, seed=1, steps=500, chunk=50, mu_ref=2.5e-4, k0=4.0, mt=0.3, frac=1.0,
+                   timing=None):
     """Kinetic energy every `chunk` steps of an FP32-bulk LES of decaying HIT
     on n^3 (LES_SCHEME) with closure `les` ("MLP" uses `mlp` with fallback
-    fraction `frac`)."""
+    fraction `frac`); `timing` (a dict) receives the device milliseconds of the
+    steps ("ms", CUDA events on the solver's stream) and the fallback count."""
     from . import FP32BULK
     ic = hit_initial_condition(n, k0=k0, seed=seed, mt=mt)
     kw = dict(grid=n, mu_ref=mu_ref, les=les, precision=FP32BULK, **LES_SCHEME)
@@ -155,13 +157,23 @@ def decayed_energy(les, mlp=None, n=128, seed=1, steps=500, chunk=50, mu_ref=2.5
     s.set_initial_conditions(*ic)
     if les == "MLP":
         s.set_mlp(mlp)
+    torch = _torch()
+    stream = torch.cuda.ExternalStream(s.stream())
     ke = [s.integrals()[0]]
-    done = 0
+    done, ms = 0, 0.0
     while done < steps:
         k = min(chunk, steps - done)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         s.step(k)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
         done += k
         ke.append(s.integrals()[0])
+    if timing is not None:
+        timing["ms"] = ms
+        timing["fallbacks"] = s.mlp_fallbacks() if les == "MLP" else None
     return np.array(ke)
 
 
