@@ -14,6 +14,7 @@ CurvilinearCSolver mirror).
     the oracle after two steps: 1e-12 (FP64), 1e-5 (FP32-bulk).
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -222,3 +223,27 @@ def test_fp32bulk_tma_line_solves_follow_fp64():
         err = np.linalg.norm(outs[1][i] - outs[0][i]) / np.linalg.norm(outs[0][i])
         assert err <= 1e-5, (i, err)
     assert m.tma_wait_timeouts(0) == 0
+
+
+def test_ten_steps_match_reference_solver():
+    """The bench's scheme for 10 time steps (55 LSLDDRK4 stages) on 64 x 24 x 16:
+    FP64 within 1e-12 relative of the reference solver per conserved field,
+    FP32-bulk within 1e-5 relative L2; same time step, time within the same
+    tolerances."""
+    cfg, ic, n = G.ten_step_case()
+    gold = np.load(os.path.join(G.HERE, "ten_steps.npz"))
+    for prec, tol in ((m.FP64, 1e-12), (m.FP32BULK, 1e-5)):
+        s = m.CurvilinearCSolver(m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF,
+                                           mu_ref=cfg.mu_ref, rk=cfg.rk, les=cfg.les, cfl=cfg.cfl, precision=prec))
+        s.set_box_metrics(2.0 * np.pi)
+        s.set_initial_conditions(*ic)
+        s.step(n)
+        q = s.conserved()
+        for i in range(5):
+            ref = gold[f"q{i}"]
+            err = H.rel_max(q[i], ref) if prec == m.FP64 else np.linalg.norm(q[i] - ref) / np.linalg.norm(ref)
+            assert err <= tol, (prec, i, err)
+        info = s.info()
+        assert info["time_step"] == int(gold["info"][0])
+        # FP32-bulk: dt from the CFL maximum over FP32 primitives
+        assert abs(info["time"] - gold["info"][1]) <= tol * gold["info"][1], (prec, info["time"])

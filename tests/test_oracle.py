@@ -199,3 +199,16 @@ def test_oracle_sponge_relaxation_matches_reference_fixtures(name):
     p = (O.GAMMA - 1.0) * (a[4] - 0.5 * (a[1] ** 2 + a[2] ** 2 + a[3] ** 2) / a[0])
     p_inf = cfg.sponge_relax["p_inf"]
     assert abs(float(np.mean(p)) - p_inf) < abs(1.0 / 1.4 - p_inf)
+
+
+def test_oracle_ten_steps_match_reference_fixture():
+    """The oracle restatement over 10 steps of the bench's scheme (64 x 24 x 16)
+    against the reference solver: <= 1e-12 relative per conserved field."""
+    import os
+    cfg, ic, n = G.ten_step_case()
+    gold = np.load(os.path.join(G.HERE, "ten_steps.npz"))
+    q, st = O.run(cfg, ic, n)
+    for i in range(5):
+        err = H.rel_max(q[i], gold[f"q{i}"])
+        assert err <= 1e-12, (i, err)
+    assert st.time_step == int(gold["info"][0])
