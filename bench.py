@@ -446,7 +446,7 @@ def run_ours(args):
 
     # ---- FP64 GPU path on the same input ----
     fp64 = None
-    err = None
+    err = err_max = ke_decay = None
     if not args.no_fp64:
         s64 = make(m.FP64)
         ms64, st64, _, _ = timed(s64, args.steps, args.warmup, False)
@@ -455,6 +455,12 @@ def run_ours(args):
         fp64 = pts * st64 / (ms64 * 1e-3)
         names = ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]
         err = {nm: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for nm, a, b in zip(names, q32, q64)}
+        err_max = {nm: float(np.abs(a - b).max() / np.abs(b).max()) for nm, a, b in zip(names, q32, q64)}
+
+        def kinetic(q):
+            return 0.5 * float(np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0]))
+        ke0 = 0.5 * float(np.sum(ic[0] * (ic[1] ** 2 + ic[2] ** 2 + ic[3] ** 2)))
+        ke_decay = (ke0 - kinetic(q32)) / (ke0 - kinetic(q64)) - 1.0
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
@@ -523,6 +529,8 @@ def run_ours(args):
                    "replicas" if ws > 1 else "single GPU"},
         "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
         "fp32_vs_fp64_rel_l2": err,
+        "fp32_vs_fp64_rel_max": err_max,
+        "fp32_vs_fp64_ke_decay_rel_diff": ke_decay,
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk, "cylinder": cyl, "learned_sgs": les,
     }
