@@ -161,6 +161,19 @@ def mu_for(ic):
     return up * lam / RE_LAMBDA
 
 
+def host_cpu():
+    """(CPU model name, logical cores) of this host."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return name, os.cpu_count()
+
+
 def cpu_reference_rate(grid, steps, warmup):
     """The reference's own C++ time step (oracle/_ref/mc3d_ref, one core) on a
     `grid`^3 sample of the same scheme; returns (pt-stages/s, sample text, kind)."""
@@ -205,7 +218,8 @@ def run_reference_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded HIT IC)",
         "config": {"workload": WORKLOAD.replace("FP32-bulk (FP64 state, RK registers, dt/time)", "FP64"),
                    "sample_grid": CPU_SAMPLE_GRID, "parallelism": "single rank"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+                         "cpu": "{}, 1 of {} logical cores used".format(*host_cpu())},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -502,7 +516,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         rate, sample, kind, _ = cpu_reference_rate(CPU_SAMPLE_GRID, 2, 0)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample}
+        model, ncores = host_cpu()
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+               "cpu": f"{model}, 1 of {ncores} logical cores used"}
 
     peak, peak_kind = hbm_peak()
     sw = rep.get("sweep_linesolve", {}) if rep else {}
