@@ -34,8 +34,12 @@ __device__ __forceinline__ float tanh_approx(float x) {
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// the same function in six instructions: u = x (K0 + K0 K1 x^2), h = x / 2,
+// gelu = h + h tanh(u)
 __device__ __forceinline__ float gelu_fast(float x) {
-    return 0.5f * x * (1.0f + tanh_approx(GELU_K0 * (x + GELU_K1 * x * x * x)));
+    const float u = x * fmaf(GELU_K0 * GELU_K1, x * x, GELU_K0);
+    const float h = 0.5f * x;
+    return fmaf(h, tanh_approx(u), h);
 }
 
 // ---------------------------------------------------------------------------
