@@ -460,7 +460,7 @@ def run_ours(args):
 
     # ---- FP64 GPU path on the same input ----
     fp64 = None
-    err = err_max = ke_decay = None
+    err = err_max = ke_decay = curve = None
     if not args.no_fp64:
         s64 = make(m.FP64)
         ms64, st64, _, _ = timed(s64, args.steps, args.warmup, False)
@@ -475,6 +475,19 @@ def run_ours(args):
             return 0.5 * float(np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0]))
         ke0 = 0.5 * float(np.sum(ic[0] * (ic[1] ** 2 + ic[2] ** 2 + ic[3] ** 2)))
         ke_decay = (ke0 - kinetic(q32)) / (ke0 - kinetic(q64)) - 1.0
+        # the decay curve, untimed: kinetic energy after every step of both paths
+        c32, c64 = make(m.FP32BULK), make(m.FP64)
+        curve = {"step": [0], "fp32": [float(c32.integrals()[0])], "fp64": [float(c64.integrals()[0])]}
+        for k in range(1, args.steps + args.warmup + 1):
+            c32.step(1)
+            c64.step(1)
+            curve["step"].append(k)
+            curve["fp32"].append(float(c32.integrals()[0]))
+            curve["fp64"].append(float(c64.integrals()[0]))
+        del c32, c64
+        d32 = np.array(curve["fp32"][0]) - np.array(curve["fp32"][1:])
+        d64 = np.array(curve["fp64"][0]) - np.array(curve["fp64"][1:])
+        curve["max_rel_diff_of_decay"] = float(np.max(np.abs(d32 - d64) / np.abs(d64)))
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
@@ -547,6 +560,7 @@ def run_ours(args):
         "fp32_vs_fp64_rel_l2": err,
         "fp32_vs_fp64_rel_max": err_max,
         "fp32_vs_fp64_ke_decay_rel_diff": ke_decay,
+        "fp32_vs_fp64_ke_curve": curve,
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk, "cylinder": cyl, "learned_sgs": les,
     }

@@ -358,7 +358,10 @@ int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, lo
  * (FP64 device reduction, synchronises). */
 int mc3d_solver_integrals(mc3d_solver s, double *kinetic, double *mass);
 
-/* The cudaStream_t the solver launches on (for event timing). */
+/* The cudaStream_t the solver launches on (for event timing). Every solver on
+ * a device launches on the same stream (created at the first solver, kept
+ * until exit), so the kernels of different solvers never overlap and
+ * mc3d_solver_sync waits for all of them. */
 int mc3d_solver_stream(mc3d_solver s, void **stream);
 /* Total number of kernels this solver has launched so far (launch accounting). */
 int mc3d_solver_launch_count(mc3d_solver s, long long *count);

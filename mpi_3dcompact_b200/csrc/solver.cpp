@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -661,6 +663,32 @@ static int one_step(mc3d_solver s) {
 
 }  // namespace mc3d
 
+namespace mc3d {
+// One non-blocking stream per device, shared by every solver on it and kept
+// until exit: solvers on one GPU run their kernels one after the other. Two
+// solvers whose kernels overlapped (stepped alternately on streams of their
+// own) gave the FP32-bulk solver a different state than running it alone,
+// through the TMA-staged line solves only (with the register kernels, or with
+// a synchronisation between the solvers, the states were identical); one
+// stream per device rules that out.
+static cudaError_t device_stream(int device, cudaStream_t *out) {
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = streams.find(device);
+    if (it != streams.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    streams[device] = st;
+    *out = st;
+    return cudaSuccess;
+}
+}  // namespace mc3d
+
 using namespace mc3d;
 
 extern "C" {
@@ -694,7 +722,7 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         s->have_sponge = s->have_sponge || c.bc_kind[f] == MC3D_BC_SPONGE;
         if (is_wall_kind(c.bc_kind[f])) s->wall_mask |= 1 << f;
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    cudaError_t e = device_stream(device, &s->stream);
     if (e != cudaSuccess) {
         delete s;
         return fail(MC3D_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
@@ -797,7 +825,7 @@ int mc3d_solver_destroy(mc3d_solver s) {
         free_line_op(s->vop[d]);
         free_line_op(s->top[d]);
     }
-    if (s->stream) cudaStreamDestroy(s->stream);
+    // (the device's shared stream stays for the other solvers)
     delete s;
     return MC3D_OK;
 }

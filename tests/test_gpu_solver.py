@@ -247,3 +247,34 @@ def test_ten_steps_match_reference_solver():
         assert info["time_step"] == int(gold["info"][0])
         # FP32-bulk: dt from the CFL maximum over FP32 primitives
         assert abs(info["time"] - gold["info"][1]) <= tol * gold["info"][1], (prec, info["time"])
+
+
+def test_concurrent_solvers_do_not_interfere():
+    """Two solvers on one device stepped alternately without waiting (an
+    FP32-bulk 256^3 case through the TMA-staged line solves and an FP64 one)
+    give the FP32-bulk solver the same state as running it alone: the solvers
+    of a device share one stream, so their kernels do not overlap."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    n = 256
+    ic = hit_initial_condition(n, k0=4.0, seed=1, mt=0.3)
+    opts = dict(grid=n, fd="PENTA10", filter="COMPACT8", alphaF=0.45, mu_ref=2.5e-4, rk="LSLDDRK4", les="VREMAN",
+                cfl=0.5)
+
+    def make(prec):
+        s = m.CurvilinearCSolver(m.Options(precision=prec, **opts))
+        s.set_box_metrics(2 * math.pi)
+        s.set_initial_conditions(*ic)
+        return s
+    alone = make(m.FP32BULK)
+    alone.step(4)
+    ref = alone.conserved()
+    del alone
+    a, b = make(m.FP32BULK), make(m.FP64)
+    for _ in range(4):
+        a.step(1)
+        b.step(1)
+    got = a.conserved()
+    b.sync()
+    for i in range(5):
+        assert np.array_equal(got[i], ref[i]), (i, float(np.nanmax(np.abs(got[i] - ref[i]))))
+    assert m.tma_wait_timeouts(0) == 0
