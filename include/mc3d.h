@@ -176,7 +176,12 @@ int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_typ
 
 /* calc1stDerivField / filterField on `nfields` device fields at once:
  * out[f] = op(in[f]). `stream` is a cudaStream_t (NULL = legacy default).
- * in[f] and out[f] may not alias. */
+ * in[f] and out[f] may not alias. FP32 lines of 128-256 points go through the
+ * TMA-staged kernels; while solvers on one device share one stream, calls
+ * here run on the caller's stream: two solvers whose kernels overlapped on
+ * separate streams once gave different FP32 results through these kernels
+ * (cause not found), so callers that overlap FP32 calls with other GPU work
+ * should serialise them or set MC3D_NO_TMA=1. */
 int mc3d_op_apply(mc3d_op op, const void *const *in, void *const *out, int nfields, void *stream);
 int mc3d_op_destroy(mc3d_op op);
 
