@@ -44,7 +44,11 @@ K0, MT, RE_LAMBDA = 4.0, 0.3, 100.0
 SCHEME = dict(fd="PENTA10", filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4", les="VREMAN", les_avg="NONE", cfl=0.5)
 WORKLOAD = ("decaying HIT 256^3 periodic box 2*pi, PENTA10 derivatives, COMPACT8 filter alpha_f=0.45 every step, "
             "LSLDDRK4, VREMAN SGS, CFL 0.5, Mt=0.3, Re_lambda~100, FP32-bulk (FP64 state, RK registers, dt/time)")
-CPU_SAMPLE_GRID = 64
+# the reference's CPU time step is timed on a 128^3 sample of the same scheme
+# (one core: the reference has no threading and no MPI runtime here)
+CPU_SAMPLE_GRID = 128
+# FP32-bulk against FP64 after the configuration's 200 steps (untimed)
+ERR_STEPS = 200
 LES_GRID, LES_STEPS, LES_MU, LES_SEED = 128, 500, 2.5e-4, 5
 # the learned closure's stage goes to DSM when more than this fraction of the
 # points has a feature outside the training range (features are clamped)
@@ -156,9 +160,21 @@ class ClockSampler:
 
 
 def mu_for(ic):
-    from mpi_3dcompact_b200.hit_ic import reynolds_lambda_mu
-    up, lam = reynolds_lambda_mu(ic)
+    up, lam = _hit_ic().reynolds_lambda_mu(ic)
     return up * lam / RE_LAMBDA
+
+
+def _hit_ic():
+    """The HIT initial-condition module, loaded from its file alone: the
+    reference arm must not import the package (nor map libmc3d.so)."""
+    import importlib.util
+    name = "mc3d_hit_ic_standalone"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "mpi_3dcompact_b200", "hit_ic.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
 
 
 def host_cpu():
@@ -174,20 +190,26 @@ def host_cpu():
     return name, os.cpu_count()
 
 
-def cpu_reference_rate(grid, steps, warmup):
+def cpu_reference_rate(grid, min_stages, warmup_steps):
     """The reference's own C++ time step (oracle/_ref/mc3d_ref, one core) on a
-    `grid`^3 sample of the same scheme; returns (pt-stages/s, sample text, kind)."""
-    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    `grid`^3 sample of the same scheme, timed over the fewest whole time steps
+    that run at least `min_stages` RK stages after `warmup_steps` untimed ones.
+    Returns (pt-stages/s, sample text, kind, timed seconds, timed steps,
+    timed stages). Imports nothing of the package: the initial condition comes
+    from hit_ic.py loaded on its own."""
     from oracle import mc3d_oracle as O
     from oracle import ref_runner as R
-    ic = hit_initial_condition(grid, k0=K0, seed=1, mt=MT)
+    ic = _hit_ic().hit_initial_condition(grid, k0=K0, seed=1, mt=MT)
     cfg = O.Config(N=(grid,) * 3, fd=(SCHEME["fd"],) * 3, filter=SCHEME["filter"], alphaF=SCHEME["alphaF"],
                    rk=SCHEME["rk"], les=SCHEME["les"], les_avg=SCHEME["les_avg"], cfl=SCHEME["cfl"],
                    mu_ref=mu_for(ic))
-    total = warmup + steps
+    steps = 1
+    while lsldd_stages(warmup_steps + 1, steps) < min_stages:
+        steps += 1
+    total = warmup_steps + steps
     if R.available():
         _, info = R.run_solver(cfg, ic, total)
-        st = info["step_s"][warmup:total]
+        st = info["step_s"][warmup_steps:total]
         kind = "reference"
     else:   # the numpy restatement when the reference binary is not built
         o = O.Oracle(cfg, O.cube_metrics(cfg.N))
@@ -196,28 +218,33 @@ def cpu_reference_rate(grid, steps, warmup):
         for i in range(total):
             t0 = time.perf_counter()
             o.step()
-            if i >= warmup:
+            if i >= warmup_steps:
                 st.append(time.perf_counter() - t0)
         kind = "port"
-    stages = lsldd_stages(warmup + 1, steps)
+    stages = lsldd_stages(warmup_steps + 1, steps)
     rate = grid ** 3 * stages / sum(st)
-    sample = (f"{grid}^3 box, same scheme, {steps} timed time steps ({stages} RK stages) after {warmup} warm-up, "
-              f"1 core")
-    return rate, sample, kind, sum(st)
+    sample = (f"{grid}^3 box, same scheme in FP64, {steps} timed time steps ({stages} RK stages) after "
+              f"{warmup_steps} warm-up time step(s), 1 core")
+    return rate, sample, kind, sum(st), steps, stages
 
 
 def run_reference_arm(args):
+    """The reference's CPU time step on the bench's scheme. Each of the K arm
+    steps is one RK stage of a 128^3 sample (the reference's 256^3 time step
+    takes minutes on one core); the stages run as whole LSLDDRK4 time steps."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    w = max(args.warmup, 1)
-    rate, sample, kind, secs = cpu_reference_rate(CPU_SAMPLE_GRID, args.steps, w)
+    w = max(1, round(args.warmup / 5.5))
+    rate, sample, kind, secs, tsteps, stages = cpu_reference_rate(CPU_SAMPLE_GRID, args.steps, w)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": w, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded HIT IC)",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / stages, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded HIT initial condition, "
+        "k0=4, Mt=0.3)",
         "config": {"workload": WORKLOAD.replace("FP32-bulk (FP64 state, RK registers, dt/time)", "FP64"),
-                   "sample_grid": CPU_SAMPLE_GRID, "parallelism": "single rank"},
+                   "grid": CPU_SAMPLE_GRID, "arm_step": "one RK stage (ms_per_step is per stage)",
+                   "time_steps_timed": tsteps, "stages_timed": stages, "parallelism": "single rank, one core"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
                          "cpu": "{}, 1 of {} logical cores used".format(*host_cpu())},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -389,6 +416,34 @@ def learned_sgs_block(args, local):
     }
 
 
+def fp32_vs_fp64(m, make, nsteps):
+    """FP32-bulk against the FP64 path from the same initial field after
+    `nsteps` time steps (untimed): per-field relative L2 and max differences of
+    the conserved state, the decay of the kinetic energy and its curve."""
+    import numpy as np
+    a, b = make(m.FP32BULK), make(m.FP64)
+    curve = {"step": [0], "fp32": [float(a.integrals()[0])], "fp64": [float(b.integrals()[0])]}
+    for k in range(1, nsteps + 1):
+        a.step(1)
+        b.step(1)
+        if k % 10 == 0 or k == nsteps:
+            curve["step"].append(k)
+            curve["fp32"].append(float(a.integrals()[0]))
+            curve["fp64"].append(float(b.integrals()[0]))
+    qa, qb = a.conserved(), b.conserved()
+    ta, tb = a.info()["time"], b.info()["time"]
+    del a, b
+    names = ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]
+    l2 = {nm: float(np.linalg.norm(x - y) / np.linalg.norm(y)) for nm, x, y in zip(names, qa, qb)}
+    mx = {nm: float(np.abs(x - y).max() / np.abs(y).max()) for nm, x, y in zip(names, qa, qb)}
+    d32 = curve["fp32"][0] - np.array(curve["fp32"][1:])
+    d64 = curve["fp64"][0] - np.array(curve["fp64"][1:])
+    return {"steps": nsteps, "rel_l2": l2, "rel_max": mx, "max_rel_l2": max(l2.values()),
+            "ke_decay_rel_diff_final": float(d32[-1] / d64[-1] - 1.0),
+            "ke_decay_max_rel_diff": float(np.max(np.abs(d32 - d64) / np.abs(d64))),
+            "time": {"fp32": ta, "fp64": tb}, "curve": curve}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -455,39 +510,17 @@ def run_ours(args):
     ms = max_over_ranks(ms, dist, "cuda")
     pts = float(n) ** 3
     value = job_rate(ws, pts, stages, ms * 1e-3)
-    q32 = s32.conserved()
     del s32
 
     # ---- FP64 GPU path on the same input ----
     fp64 = None
-    err = err_max = ke_decay = curve = None
+    cmp = None
     if not args.no_fp64:
         s64 = make(m.FP64)
         ms64, st64, _, _ = timed(s64, args.steps, args.warmup, False)
-        q64 = s64.conserved()
         del s64
         fp64 = pts * st64 / (ms64 * 1e-3)
-        names = ["rho", "rhoU", "rhoV", "rhoW", "rhoE"]
-        err = {nm: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for nm, a, b in zip(names, q32, q64)}
-        err_max = {nm: float(np.abs(a - b).max() / np.abs(b).max()) for nm, a, b in zip(names, q32, q64)}
-
-        def kinetic(q):
-            return 0.5 * float(np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0]))
-        ke0 = 0.5 * float(np.sum(ic[0] * (ic[1] ** 2 + ic[2] ** 2 + ic[3] ** 2)))
-        ke_decay = (ke0 - kinetic(q32)) / (ke0 - kinetic(q64)) - 1.0
-        # the decay curve, untimed: kinetic energy after every step of both paths
-        c32, c64 = make(m.FP32BULK), make(m.FP64)
-        curve = {"step": [0], "fp32": [float(c32.integrals()[0])], "fp64": [float(c64.integrals()[0])]}
-        for k in range(1, args.steps + args.warmup + 1):
-            c32.step(1)
-            c64.step(1)
-            curve["step"].append(k)
-            curve["fp32"].append(float(c32.integrals()[0]))
-            curve["fp64"].append(float(c64.integrals()[0]))
-        del c32, c64
-        d32 = np.array(curve["fp32"][0]) - np.array(curve["fp32"][1:])
-        d64 = np.array(curve["fp64"][0]) - np.array(curve["fp64"][1:])
-        curve["max_rel_diff_of_decay"] = float(np.max(np.abs(d32 - d64) / np.abs(d64)))
+        cmp = fp32_vs_fp64(m, make, args.err_steps)
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
@@ -528,7 +561,8 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        rate, sample, kind, _ = cpu_reference_rate(CPU_SAMPLE_GRID, 2, 0)
+        # one 5-stage time step of the reference at 128^3 (about half a minute)
+        rate, sample, kind, _, _, _ = cpu_reference_rate(CPU_SAMPLE_GRID, 5, 0)
         model, ncores = host_cpu()
         cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
                "cpu": f"{model}, 1 of {ncores} logical cores used"}
@@ -556,13 +590,13 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "grid": n, "stages_timed": stages,
                    "l2": "inputs larger than L2: 40 resident fields of 64-128 MB", "parallelism":
                    "replicas" if ws > 1 else "single GPU"},
-        "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
-        "fp32_vs_fp64_rel_l2": err,
-        "fp32_vs_fp64_rel_max": err_max,
-        "fp32_vs_fp64_ke_decay_rel_diff": ke_decay,
-        "fp32_vs_fp64_ke_curve": curve,
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk, "cylinder": cyl, "learned_sgs": les,
+        "clocks": clk, "fp32_vs_fp64_ke_curve": cmp.pop("curve") if cmp else None, "cylinder": cyl,
+        "learned_sgs": les,
+        # the FP32-bulk evidence last, where a truncated record still keeps it
+        "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
+        "fp64_over_cpu_reference": (fp64 / cpu["value"]) if (fp64 and cpu) else None,
+        "fp32_vs_fp64": cmp,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -582,6 +616,7 @@ def main():
     ap.add_argument("--no-cylinder", action="store_true")
     ap.add_argument("--cyl-steps", type=int, default=5)
     ap.add_argument("--les-steps", type=int, default=LES_STEPS)
+    ap.add_argument("--err-steps", type=int, default=ERR_STEPS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -177,11 +177,8 @@ int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_typ
 /* calc1stDerivField / filterField on `nfields` device fields at once:
  * out[f] = op(in[f]). `stream` is a cudaStream_t (NULL = legacy default).
  * in[f] and out[f] may not alias. FP32 lines of 128-256 points go through the
- * TMA-staged kernels; while solvers on one device share one stream, calls
- * here run on the caller's stream: two solvers whose kernels overlapped on
- * separate streams once gave different FP32 results through these kernels
- * (cause not found), so callers that overlap FP32 calls with other GPU work
- * should serialise them or set MC3D_NO_TMA=1. */
+ * TMA-staged kernels. Calls may overlap solver steps and other calls on other
+ * streams; each result is the same as when it runs alone. */
 int mc3d_op_apply(mc3d_op op, const void *const *in, void *const *out, int nfields, void *stream);
 int mc3d_op_destroy(mc3d_op op);
 
@@ -363,11 +360,18 @@ int mc3d_solver_info(mc3d_solver s, int *time_step, double *time, double *dt, lo
  * (FP64 device reduction, synchronises). */
 int mc3d_solver_integrals(mc3d_solver s, double *kinetic, double *mass);
 
-/* The cudaStream_t the solver launches on (for event timing). Every solver on
- * a device launches on the same stream (created at the first solver, kept
- * until exit), so the kernels of different solvers never overlap and
- * mc3d_solver_sync waits for all of them. */
+/* The cudaStream_t the solver launches on (for event timing). By default every
+ * solver on a device launches on one non-blocking stream of that device
+ * (created at the first solver, kept until exit); mc3d_solver_set_stream
+ * moves a solver to a stream of the caller's. */
 int mc3d_solver_stream(mc3d_solver s, void **stream);
+/* Binds the solver to `stream` (a cudaStream_t of the solver's device; NULL:
+ * the device's shared stream). Work already queued on the previous stream is
+ * completed first; every later call queues the solver's kernels on the new
+ * stream. Solvers on different streams run concurrently and independently:
+ * their kernels share no memory. Like the reference's one solver per MPI rank,
+ * a solver is driven from one host thread at a time. */
+int mc3d_solver_set_stream(mc3d_solver s, void *stream);
 /* Total number of kernels this solver has launched so far (launch accounting). */
 int mc3d_solver_launch_count(mc3d_solver s, long long *count);
 int mc3d_solver_sync(mc3d_solver s);

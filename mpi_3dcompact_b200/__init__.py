@@ -570,6 +570,11 @@ class CurvilinearCSolver:
         N.check(N.host_lib().mc3d_solver_stream(self._h, C.byref(s)))
         return s.value
 
+    def set_stream(self, stream=None):
+        """Queue this solver's kernels on `stream` (a cudaStream_t handle, e.g.
+        torch.cuda.Stream().cuda_stream; None: the device's shared stream)."""
+        N.check(N.host_lib().mc3d_solver_set_stream(self._h, C.c_void_p(stream) if stream else None))
+
     def launch_count(self):
         c = C.c_longlong()
         N.check(N.host_lib().mc3d_solver_launch_count(self._h, C.byref(c)))

@@ -108,6 +108,7 @@ def host_lib():
             "mc3d_solver_info": (ip, [vp, C.POINTER(ip), C.POINTER(dp), C.POINTER(dp), C.POINTER(C.c_longlong)]),
             "mc3d_solver_integrals": (ip, [vp, C.POINTER(dp), C.POINTER(dp)]),
             "mc3d_solver_stream": (ip, [vp, C.POINTER(vp)]),
+            "mc3d_solver_set_stream": (ip, [vp, vp]),
             "mc3d_solver_launch_count": (ip, [vp, C.POINTER(C.c_longlong)]),
             "mc3d_solver_sync": (ip, [vp]),
             "mc3d_solver_set_timing": (ip, [vp, ip]),

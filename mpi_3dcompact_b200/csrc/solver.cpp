@@ -664,13 +664,10 @@ static int one_step(mc3d_solver s) {
 }  // namespace mc3d
 
 namespace mc3d {
-// One non-blocking stream per device, shared by every solver on it and kept
-// until exit: solvers on one GPU run their kernels one after the other. Two
-// solvers whose kernels overlapped (stepped alternately on streams of their
-// own) gave the FP32-bulk solver a different state than running it alone,
-// through the TMA-staged line solves only (with the register kernels, or with
-// a synchronisation between the solvers, the states were identical); one
-// stream per device rules that out.
+// The default stream of the solvers on a device: one non-blocking stream per
+// device, created with the first solver and kept until exit, so solvers that
+// their caller does not place (mc3d_solver_set_stream) queue one after the
+// other and mc3d_solver_sync waits for all of them.
 static cudaError_t device_stream(int device, cudaStream_t *out) {
     static std::mutex mu;
     static std::map<int, cudaStream_t> streams;
@@ -1793,6 +1790,19 @@ int mc3d_solver_integrals(mc3d_solver s, double *kinetic, double *mass) {
 int mc3d_solver_stream(mc3d_solver s, void **stream) {
     if (!s || !stream) return fail(MC3D_ERR_ARG, "null argument");
     *stream = (void *)s->stream;
+    return MC3D_OK;
+}
+
+int mc3d_solver_set_stream(mc3d_solver s, void *stream) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (stream) {
+        s->stream = (cudaStream_t)stream;
+        return MC3D_OK;
+    }
+    cudaError_t e = device_stream(s->device, &s->stream);
+    if (e != cudaSuccess) return fail(MC3D_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     return MC3D_OK;
 }
 

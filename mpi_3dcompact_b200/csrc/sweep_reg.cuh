@@ -560,11 +560,8 @@ static int launch_reg_epi(const Grid3 &g, const LineOpDev<R> &op, const SweepBat
     const int S = op.N / L;
     size_t smem = reg_smem_bytes(DIR, op.N, S, sizeof(R));
     auto kern = sweep_reg_kernel<DIR, R, KIND, H, L, E>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
+    static KernelLaunchState ls;
+    if (int rc = open_kernel(kern, ls, smem, 0, nullptr)) return rc;
     int tiles;
     if (DIR == 0) tiles = (int)(((long long)g.Ny * g.Nz + W - 1) / W);
     else if (DIR == 1) tiles = ((g.Nx + W - 1) / W) * g.Nz;

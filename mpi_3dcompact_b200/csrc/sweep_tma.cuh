@@ -52,6 +52,17 @@ __device__ __forceinline__ unsigned swz_off(int l, int x) {
     return (unsigned)((x >> 5) * 4096) + (lane_part ^ (unsigned)(((x >> 2) & 7) << 4)) + (unsigned)((x & 3) << 2);
 }
 
+// A tile that the lanes have read with ordinary shared-memory loads (the
+// generic proxy) is refilled by a TMA load (the async proxy). The CTA barrier
+// alone orders the two only within the generic proxy: without a proxy fence
+// the bulk copy may land in the tile before every lane's earlier loads have
+// read it, and those lanes then solve with rows of the next tile. Each thread
+// fences its own reads, then the barrier hands that ordering to the thread
+// that issues the copy (the write-after-read form of the proxy rule of the
+// PTX memory model; the read-after-write form is the fence before each TMA
+// store).
+__device__ __forceinline__ void tile_reads_done() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 __device__ __forceinline__ float4 lds4(const unsigned char *tile, unsigned off) {
     return *reinterpret_cast<const float4 *>(tile + off);
 }
@@ -156,6 +167,7 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
         }
         v[k] = in ? *reinterpret_cast<const R *>(tile + swz_row(n, lane)) : R(0);
     }
+    tile_reads_done();
     __syncthreads();   // every lane holds its rows: the tile takes the first operand
     const bool mom = E == EPI_RHS_FINAL && rf.quirk && b.eq[f] >= 1 && b.eq[f] <= 3;
     if (threadIdx.x == 0) load(E == EPI_SUB ? &maps.out[f] : &maps.aux[f]);
@@ -169,6 +181,7 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
     for (int r = 0; r < L; r++) y[r] = at(r) - y[r];
     if (E == EPI_RHS_FINAL) {
         if (mom) {
+            tile_reads_done();
             __syncthreads();   // every lane has read the partial RHS
             if (threadIdx.x == 0) load(&maps.out[f]);
             if (!wait(0)) return;
@@ -290,6 +303,7 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
             }
             v[k] = in ? *reinterpret_cast<const R *>(tile + swz_row(n, lane)) : R(0);
         }
+        tile_reads_done();
         __syncthreads();   // every lane holds its rows: the buffer takes the next item
         if (threadIdx.x == 0 && w + (int)gridDim.x < nitems) issue(w + gridDim.x);
         R y[L];
@@ -400,6 +414,7 @@ __global__ void __launch_bounds__(512) sweep_tma_x_persist_kernel(Grid3 g, LineO
                 if (k < NV) v[k] = e2[j];
             }
         }
+        tile_reads_done();
         __syncthreads();   // every lane holds its rows: the input tile takes the next item
         if (threadIdx.x == 0) {
             if (w + (int)gridDim.x < nitems) issue(w + gridDim.x);

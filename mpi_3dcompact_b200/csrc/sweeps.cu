@@ -343,11 +343,8 @@ static int launch_one(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R
                       const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
     size_t smem = ((size_t)(op.N + H + UB) * SP + 4 * W) * sizeof(R);
     auto kern = sweep_kernel<DIR, R, KIND, H>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
+    static KernelLaunchState ls;
+    if (int rc = open_kernel(kern, ls, smem, 0, nullptr)) return rc;
     int tiles;
     if (DIR == 0) tiles = (int)(((long long)g.Ny * g.Nz + W - 1) / W);
     else if (DIR == 1) tiles = ((g.Nx + W - 1) / W) * g.Nz;
@@ -739,11 +736,8 @@ static int launch_seg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R
                       const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
     size_t smem = seg_smem_elems<S>(op.N, H, seg_pitch<DIR>()) * sizeof(R);
     auto kern = sweep_seg_kernel<DIR, R, KIND, H, S>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
+    static KernelLaunchState ls;
+    if (int rc = open_kernel(kern, ls, smem, 0, nullptr)) return rc;
     int tiles;
     if (DIR == 0) tiles = (int)(((long long)g.Ny * g.Nz + W - 1) / W);
     else if (DIR == 1) tiles = ((g.Nx + W - 1) / W) * g.Nz;

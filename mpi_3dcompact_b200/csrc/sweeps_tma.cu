@@ -28,15 +28,16 @@ EncodeTiledFn encode_tiled() {
 
 // FP32 tensor map (rank 2 or 3, innermost first; strides in bytes of the
 // outer dimensions) with the 128-byte swizzle; cached per (address, shape,
-// box) since a run reuses a fixed set of field buffers.
+// strides, box) since a run reuses a fixed set of field buffers.
 bool tensor_map(const void *p, int rank, const cuuint64_t *dims, const cuuint64_t *strides, const cuuint32_t *box,
                 CUtensorMap *out) {
+    using Key = std::tuple<const void *, int, cuuint64_t, cuuint64_t, cuuint64_t, cuuint64_t, cuuint64_t, cuuint32_t,
+                           cuuint32_t, cuuint32_t>;
     static std::mutex mu;
-    static std::map<std::tuple<const void *, int, cuuint64_t, cuuint64_t, cuuint64_t, cuuint32_t, cuuint32_t>,
-                    CUtensorMap>
-        cache;
+    static std::map<Key, CUtensorMap> cache;
     std::lock_guard<std::mutex> lk(mu);
-    const auto key = std::make_tuple(p, rank, dims[0], dims[1], rank > 2 ? dims[2] : 0, box[0], box[1]);
+    const Key key{p,          rank,   dims[0], dims[1], rank > 2 ? dims[2] : 0, strides[0], rank > 2 ? strides[1] : 0,
+                  box[0],     box[1], rank > 2 ? box[2] : 0};
     auto it = cache.find(key);
     if (it != cache.end()) {
         *out = it->second;
@@ -92,28 +93,17 @@ int launch_tma_yz_epi(const Grid3 &g, const LineOpDev<float> &op, const SweepBat
     // operand tiles arriving by TMA during the solve
     if constexpr (E == EPI_STORE || E == EPI_STORE_NEG || E == EPI_STORE_F64) {
         auto kern = sweep_tma_yz_persist_kernel<DIR, KIND, H, L, E>;
-        static thread_local int configured_smem = -1;
-        static thread_local int ctas = 0;
-        if ((int)smem > configured_smem) {
-            MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured_smem = (int)smem;
-            int dev = 0, nsm = 0, per = 0;
-            MC3D_CUDA_TRY(cudaGetDevice(&dev));
-            MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-            MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * S, smem));
-            ctas = nsm * (per > 0 ? per : 1);
-        }
+        static KernelLaunchState ls;
+        int ctas = 0;
+        if (int rc = open_kernel(kern, ls, smem, 32 * S, &ctas)) return rc;
         const int items = tile_count<DIR>(g) * b.nf;
         kern<<<items < ctas ? items : ctas, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
         MC3D_CUDA_TRY(cudaGetLastError());
         return MC3D_OK;
     } else {
         auto kern = sweep_tma_yz_kernel<DIR, KIND, H, L, E>;
-        static thread_local int configured_smem = -1;
-        if ((int)smem > configured_smem) {
-            MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured_smem = (int)smem;
-        }
+        static KernelLaunchState ls;
+        if (int rc = open_kernel(kern, ls, smem, 32 * S, nullptr)) return rc;
         dim3 grid(tile_count<DIR>(g), b.nf);
         kern<<<grid, 32 * S, smem, st>>>(g, op, b, rf, maps, px, py, pz);
         MC3D_CUDA_TRY(cudaGetLastError());
@@ -146,17 +136,9 @@ int launch_tma_epi(const Grid3 &g, const LineOpDev<float> &op, const TmaMaps &ma
     const int S = op.N / L;
     const size_t smem = 1024 + 2 * (size_t)(op.N / TMA_BOX) * 4096 + (size_t)reg_chain_elems(S) * sizeof(float);
     auto kern = sweep_tma_x_persist_kernel<KIND, H, L, E>;
-    static thread_local int configured_smem = -1;
-    static thread_local int ctas = 0;
-    if ((int)smem > configured_smem) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-        int dev = 0, nsm = 0, per = 0;
-        MC3D_CUDA_TRY(cudaGetDevice(&dev));
-        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * S, smem));
-        ctas = nsm * (per > 0 ? per : 1);
-    }
+    static KernelLaunchState ls;
+    int ctas = 0;
+    if (int rc = open_kernel(kern, ls, smem, 32 * S, &ctas)) return rc;
     const int items = tile_count<0>(g) * nf;
     kern<<<items < ctas ? items : ctas, 32 * S, smem, st>>>(g, op, maps, nf, py, pz);
     MC3D_CUDA_TRY(cudaGetLastError());

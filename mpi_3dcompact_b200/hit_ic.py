@@ -42,24 +42,47 @@ class _Gen:
         self.r, self.ix1, self.ix2, self.ix3 = r, ix1, ix2, ix3
 
     def vec(self, n: int) -> np.ndarray:
-        try:
-            from . import _native
-            lib = _native.host_lib()
-        except Exception:  # the host library is optional for small fields
-            lib = None
-        if lib is not None and n > 200000:
-            return _native.hit_randvec(lib, self, n)
-        out = np.empty(n)
-        r, ix1, ix2, ix3 = self.r, self.ix1, self.ix2, self.ix3
-        for m in range(n):
-            ix1 = (_IA1 * ix1 + _IC1) % _M1
-            ix2 = (_IA2 * ix2 + _IC2) % _M2
-            ix3 = (_IA3 * ix3 + _IC3) % _M3
-            j = (97 * ix3) // _M3 % 97
-            out[m] = r[j]
-            r[j] = min(1.0, max(0.0, (float(ix1) + float(ix2) * _RM2) * _RM1))
-        self.ix1, self.ix2, self.ix3 = ix1, ix2, ix3
+        """The next n values of randvec, vectorised: each of the three LCG
+        sequences is produced by doubling (x -> A x + C composed with itself),
+        and the shuffle table's output at step m is the table value written at
+        the last earlier step that drew the same slot (or the initial value),
+        found with one stable sort by slot. Bit-identical to the loop of
+        generate_init_hit.f90:54-81 (same integer arithmetic, same FP64
+        expression for the table values)."""
+        if n <= 0:
+            return np.empty(0)
+        ix1 = _lcg(self.ix1, _IA1, _IC1, _M1, n)
+        ix2 = _lcg(self.ix2, _IA2, _IC2, _M2, n)
+        ix3 = _lcg(self.ix3, _IA3, _IC3, _M3, n)
+        slot = ((97 * ix3) // _M3 % 97).astype(np.uint8)
+        val = np.clip((ix1.astype(np.float64) + ix2.astype(np.float64) * _RM2) * _RM1, 0.0, 1.0)
+        order = np.argsort(slot, kind="stable")
+        ss = slot[order]
+        prev = np.full(n, -1, dtype=np.int64)
+        same = ss[1:] == ss[:-1]
+        prev[order[1:][same]] = order[:-1][same]
+        table = np.array(self.r, dtype=np.float64)
+        out = np.where(prev >= 0, val[np.maximum(prev, 0)], table[slot])
+        last = np.ones(n, dtype=bool)
+        last[:-1] = ~same
+        table[ss[last]] = val[order[last]]
+        self.r = table.tolist()
+        self.ix1, self.ix2, self.ix3 = int(ix1[-1]), int(ix2[-1]), int(ix3[-1])
         return out
+
+
+def _lcg(x0: int, a: int, c: int, m: int, n: int) -> np.ndarray:
+    """x_1..x_n of x_{k+1} = (a x_k + c) mod m."""
+    out = np.empty(n, dtype=np.int64)
+    out[0] = (a * x0 + c) % m
+    A, Cc, filled = a, c, 1          # (A, Cc): the map x -> x_{k+filled}
+    while filled < n:
+        take = min(filled, n - filled)
+        out[filled:filled + take] = (A * out[:take] + Cc) % m
+        Cc = (A * Cc + Cc) % m
+        A = (A * A) % m
+        filled += take
+    return out
 
 
 def hit_velocity(n: int, k0: float = 4.0, seed: int = 1):

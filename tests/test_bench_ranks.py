@@ -63,3 +63,18 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = argparse.Namespace(gpus=2, steps=2, warmup=1)
     assert bench.run_reference_arm(args) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_maps_no_package_library():
+    """The reference arm builds its initial condition from hit_ic.py alone and
+    runs the reference's C++ (or the oracle port): its process never maps
+    libmc3d.so, and it imports nothing of the package."""
+    import subprocess
+    code = ("import sys; sys.path.insert(0, %r); import bench; r = bench.cpu_reference_rate(16, 5, 0); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('libmc3d' in maps, 'mpi_3dcompact_b200' in sys.modules, r[2], r[0] > 0)" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    mapped, imported, kind, positive = out.stdout.split()
+    assert mapped == "False" and imported == "False" and positive == "True", out.stdout
+    assert kind in ("reference", "port")

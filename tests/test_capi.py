@@ -176,10 +176,15 @@ def test_calc_neumann_matches_reference_formula():
 
 
 def test_hit_randvec_matches_restatement():
+    """The C generator (mc3d_hit_randvec) and the vectorised numpy restatement
+    give the same sequence, also across consecutive calls of different sizes."""
     from mpi_3dcompact_b200.hit_ic import _Gen
-    a = _Gen(7).vec(5000)
-    b = N.hit_randvec(N.host_lib(), _Gen(7), 5000)
-    assert np.array_equal(a, b)
+    ga, gb = _Gen(7), _Gen(7)
+    for n in (5000, 1, 300001, 97):
+        a = ga.vec(n)
+        b = N.hit_randvec(N.host_lib(), gb, n)
+        assert np.array_equal(a, b), n
+        assert (ga.ix1, ga.ix2, ga.ix3) == (gb.ix1, gb.ix2, gb.ix3) and ga.r == gb.r
 
 
 def test_null_arguments_are_errors_not_crashes():

@@ -249,32 +249,125 @@ def test_ten_steps_match_reference_solver():
         assert abs(info["time"] - gold["info"][1]) <= tol * gold["info"][1], (prec, info["time"])
 
 
-def test_concurrent_solvers_do_not_interfere():
-    """Two solvers on one device stepped alternately without waiting (an
-    FP32-bulk 256^3 case through the TMA-staged line solves and an FP64 one)
-    give the FP32-bulk solver the same state as running it alone: the solvers
-    of a device share one stream, so their kernels do not overlap."""
+def _hit_solver(n, prec, ic):
+    s = m.CurvilinearCSolver(m.Options(grid=n, fd="PENTA10", filter="COMPACT8", alphaF=0.45, mu_ref=2.5e-4,
+                                       rk="LSLDDRK4", les="VREMAN", cfl=0.5, precision=prec))
+    s.set_box_metrics(2 * math.pi)
+    s.set_initial_conditions(*ic)
+    return s
+
+
+def test_concurrent_solvers_on_own_streams_do_not_interfere():
+    """Two solvers on one device, each on a stream of its own (an FP32-bulk
+    256^3 case through the TMA-staged line solves and an FP64 one), stepped
+    alternately without waiting so that their kernels overlap: in each of
+    three trials the FP32-bulk state equals running it alone, bit for bit."""
+    import torch
     from mpi_3dcompact_b200.hit_ic import hit_initial_condition
     n = 256
     ic = hit_initial_condition(n, k0=4.0, seed=1, mt=0.3)
-    opts = dict(grid=n, fd="PENTA10", filter="COMPACT8", alphaF=0.45, mu_ref=2.5e-4, rk="LSLDDRK4", les="VREMAN",
-                cfl=0.5)
-
-    def make(prec):
-        s = m.CurvilinearCSolver(m.Options(precision=prec, **opts))
-        s.set_box_metrics(2 * math.pi)
-        s.set_initial_conditions(*ic)
-        return s
-    alone = make(m.FP32BULK)
+    alone = _hit_solver(n, m.FP32BULK, ic)
     alone.step(4)
     ref = alone.conserved()
     del alone
-    a, b = make(m.FP32BULK), make(m.FP64)
-    for _ in range(4):
-        a.step(1)
-        b.step(1)
-    got = a.conserved()
-    b.sync()
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    for trial in range(3):
+        a, b = _hit_solver(n, m.FP32BULK, ic), _hit_solver(n, m.FP64, ic)
+        a.set_stream(sa.cuda_stream)
+        b.set_stream(sb.cuda_stream)
+        for _ in range(4):
+            a.step(1)
+            b.step(1)
+        got = a.conserved()
+        b.sync()
+        for i in range(5):
+            assert np.array_equal(got[i], ref[i]), (trial, i, float(np.nanmax(np.abs(got[i] - ref[i]))))
+        del a, b
+    assert m.tma_wait_timeouts(0) == 0
+
+
+def test_operator_calls_on_default_stream_overlap_a_solver_step():
+    """Operator calls on the legacy default stream (mc3d_op_apply with a NULL
+    stream, as a reference-side adapter makes them: FP32 Penta10 along x, y
+    and z of five 256^3 fields, FP64 along x) queued while an FP32-bulk solver
+    steps on its own non-blocking stream: the operator results and the solver
+    state both equal their solo runs bit for bit."""
+    import torch
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    n = 256
+    ic = hit_initial_condition(n, k0=4.0, seed=2, mt=0.3)
+    alone = _hit_solver(n, m.FP32BULK, ic)
+    alone.step(2)
+    ref = alone.conserved()
+    del alone
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x32 = [torch.randn(n, n, n, device="cuda", generator=g) for _ in range(5)]
+    x64 = [torch.randn(n, n, n, device="cuda", generator=g, dtype=torch.float64) for _ in range(5)]
+    ops32 = [m.Penta10((n, n, n), m.PERIODIC_SOLVE, d, precision=m.FP32BULK) for d in range(3)]
+    op64 = m.Penta10((n, n, n), m.PERIODIC_SOLVE, 0)
+    y32 = [[torch.empty_like(x32[0]) for _ in range(5)] for _ in range(3)]
+    y64 = [torch.empty_like(x64[0]) for _ in range(5)]
+    for d in range(3):
+        ops32[d].calc1stDerivFields(x32, y32[d])
+    op64.calc1stDerivFields(x64, y64)
+    torch.cuda.synchronize()
+    solo32 = [[t.clone() for t in y32[d]] for d in range(3)]
+    solo64 = [t.clone() for t in y64]
+    s = _hit_solver(n, m.FP32BULK, ic)
+    own = torch.cuda.Stream()
+    s.set_stream(own.cuda_stream)
+    for _ in range(2):
+        for d in range(3):
+            for t in y32[d]:
+                t.zero_()
+        torch.cuda.synchronize()
+        s.step(1)                      # queued on the solver's stream
+        for d in range(3):             # queued on the legacy default stream meanwhile
+            ops32[d].calc1stDerivFields(x32, y32[d])
+            op64.calc1stDerivFields(x64, y64)
+        torch.cuda.synchronize()
+        for d in range(3):
+            for f in range(5):
+                assert torch.equal(y32[d][f], solo32[d][f]), (d, f)
+        for f in range(5):
+            assert torch.equal(y64[f], solo64[f]), f
+    got = s.conserved()
     for i in range(5):
         assert np.array_equal(got[i], ref[i]), (i, float(np.nanmax(np.abs(got[i] - ref[i]))))
+    assert m.tma_wait_timeouts(0) == 0
+
+
+def test_fp32_line_solves_stay_bit_stable_under_overlapping_sweeps():
+    """FP32 Penta10 derivatives of five 256^3 fields along x, y and z (the
+    TMA-staged persistent kernels) on one stream while FP64 x sweeps (the
+    register kernel, staging its tiles with per-element asynchronous copies)
+    run on another: ten rounds, every output equal to the solo result."""
+    import torch
+    n = 256
+    g = torch.Generator(device="cuda").manual_seed(9)
+    xa = [torch.randn(n, n, n, device="cuda", generator=g) for _ in range(5)]
+    xb = [torch.randn(n, n, n, device="cuda", generator=g, dtype=torch.float64) for _ in range(5)]
+    opa = [m.Penta10((n, n, n), m.PERIODIC_SOLVE, d, precision=m.FP32BULK) for d in range(3)]
+    opb = m.Penta10((n, n, n), m.PERIODIC_SOLVE, 0)
+    ya = [[torch.empty_like(xa[0]) for _ in range(5)] for _ in range(3)]
+    yb = [torch.empty_like(xb[0]) for _ in range(5)]
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    for d in range(3):
+        opa[d].calc1stDerivFields(xa, ya[d], stream=sa.cuda_stream)
+    torch.cuda.synchronize()
+    ref = [[t.clone() for t in ya[d]] for d in range(3)]
+    for rnd in range(10):
+        for d in range(3):
+            for t in ya[d]:
+                t.zero_()
+        torch.cuda.synchronize()
+        for _ in range(3):
+            opb.calc1stDerivFields(xb, yb, stream=sb.cuda_stream)
+        for d in range(3):
+            opa[d].calc1stDerivFields(xa, ya[d], stream=sa.cuda_stream)
+            opb.calc1stDerivFields(xb, yb, stream=sb.cuda_stream)
+        torch.cuda.synchronize()
+        for d in range(3):
+            for f in range(5):
+                assert torch.equal(ya[d][f], ref[d][f]), (rnd, d, f)
     assert m.tma_wait_timeouts(0) == 0
