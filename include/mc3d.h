@@ -201,6 +201,11 @@ int mc3d_mlp_set_normalization(mc3d_mlp m, const float *mean, const float *std, 
 int mc3d_mlp_get_normalization(mc3d_mlp m, float *out);
 /* one Adam step (lr) on MSE against normalised targets y; loss (host, may be NULL) */
 int mc3d_mlp_train_step(mc3d_mlp m, const float *x, const float *y, int n, float lr, double *loss, void *stream);
+/* the gradient that step would use, without the update: G (host, MLP_NPARAM =
+ * 9090 floats, in the parameter order of mc3d_mlp_get_params) = d loss / dP
+ * with loss = mean_b sum_o (out_bo - y_bo)^2, computed by the same FP32
+ * forward, backward and weight-gradient kernels; loss (host, may be NULL) */
+int mc3d_mlp_gradient(mc3d_mlp m, const float *x, const float *y, int n, float *G, double *loss, void *stream);
 /* FP32 forward on CUDA cores, and the BF16 tensor-core inference */
 int mc3d_mlp_forward(mc3d_mlp m, const float *x, float *y, int n, void *stream);
 int mc3d_mlp_infer_bf16(mc3d_mlp m, const float *x, float *y, int n, void *stream);
@@ -402,11 +407,18 @@ int mc3d_tma_wait_timeouts(int device, int *count);
  * 512 KiB device array inside the library, which every GPU that loads the
  * library holds until the process exits; fields larger than 16,777,216
  * points (256^3) are rejected with MC3D_ERR_ARG. The first call on a device
- * looks up that array's address (cudaGetSymbolAddress), so make the first
- * call on each device before any stream capture. All calls share the array:
- * calls that overlap on the GPU (different streams, no ordering) race; no
- * scratch value needs to start at zero, every slot a call reads is written by
- * the same call. Asynchronous on `stream`. */
+ * sets up: it looks up that array's address (cudaGetSymbolAddress) and loads
+ * the two kernels, and CUDA's on-demand module loading claims device memory
+ * for that (the array and the kernels' code). Make the first call on each
+ * device at start-up, before the caller's pool takes the device's memory and
+ * before any stream capture; every later call allocates and loads nothing.
+ * All calls share the array: calls that overlap on the GPU (different
+ * streams, no ordering) race; no scratch value needs to start at zero, every
+ * slot a call reads is written by the same call. A non-finite wave speed
+ * anywhere (a NaN or infinite state) makes *out_max NaN, on purpose: the
+ * reference's `UChar > lmax` loop (src/CurvilinearCSolver_Core.cpp:200-205)
+ * skips NaN points instead, so check the result before dividing by it.
+ * Asynchronous on `stream`. */
 int mc3d_cfl_max_noalloc(const double *rho, const double *rhoU, const double *rhoV, const double *rhoW,
                          const double *rhoE, const double *J11, const double *J22, const double *J33,
                          double J11c, double J22c, double J33c, int Nx, int Ny, int Nz, double dxi, double deta,

@@ -345,6 +345,15 @@ class MLPClosure:
         N.check(N.host_lib().mc3d_mlp_train_step(self._h, _fp(x), _fp(y), x.shape[0], lr, C.byref(loss), stream))
         return loss.value
 
+    def gradient(self, x, y, stream=None):
+        """d loss / dP of the MSE against normalised targets y (the gradient
+        train_step would use), without updating; returns (G, loss)."""
+        G = np.zeros(self.N_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        N.check(N.host_lib().mc3d_mlp_gradient(self._h, _fp(x), _fp(y), x.shape[0],
+                                               G.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss), stream))
+        return G, loss.value
+
     def forward(self, x, y, stream=None):
         N.check(N.host_lib().mc3d_mlp_forward(self._h, _fp(x), _fp(y), x.shape[0], stream))
 

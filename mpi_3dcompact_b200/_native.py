@@ -122,6 +122,7 @@ def host_lib():
             "mc3d_mlp_get_normalization": (ip, [vp, C.POINTER(C.c_float)]),
             "mc3d_mlp_train_step": (ip, [vp, vp, vp, ip, C.c_float, C.POINTER(dp), vp]),
             "mc3d_mlp_forward": (ip, [vp, vp, vp, ip, vp]),
+            "mc3d_mlp_gradient": (ip, [vp, vp, vp, ip, C.POINTER(C.c_float), C.POINTER(dp), vp]),
             "mc3d_mlp_infer_bf16": (ip, [vp, vp, vp, ip, vp]),
             "mc3d_mlp_get_params": (ip, [vp, C.POINTER(C.c_float)]),
             "mc3d_mlp_set_params": (ip, [vp, C.POINTER(C.c_float)]),

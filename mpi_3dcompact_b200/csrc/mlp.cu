@@ -260,19 +260,17 @@ int mlp_pack(const MlpDev &m, cudaStream_t st) {
 
 int mlp_forward_fp32(const MlpDev &m, const float *x, int n, float *act, float *out, cudaStream_t st) {
     const size_t smem = MLP_NP * sizeof(float);
-    static bool configured = false;
-    if (!configured) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
+    static KernelLaunchState fwd, bwd;
+    int rc;
+    if ((rc = open_kernel(mlp_forward_kernel, fwd, smem, 128, nullptr))) return rc;
+    if ((rc = open_kernel(mlp_backward_kernel, bwd, smem, 128, nullptr))) return rc;
     mlp_forward_kernel<<<(n + 127) / 128, 128, smem, st>>>(m.P, x, n, m.norm, act, out);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
 
-int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, float *act, float *out, float *delta,
-                   double *loss, cudaStream_t st) {
+int mlp_gradient(MlpDev &m, const float *x, const float *y, int n, float *act, float *out, float *delta,
+                 double *loss, cudaStream_t st) {
     int rc;
     if ((rc = mlp_forward_fp32(m, x, n, act, out, st))) return rc;
     const size_t smem = MLP_NP * sizeof(float);
@@ -284,6 +282,13 @@ int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, f
         mlp_wgrad_kernel<<<dim3(nout, splits), nin + 1, 0, st>>>(x, m.norm, act, delta, n, layer, m.G);
         MC3D_CUDA_TRY(cudaGetLastError());
     }
+    return MC3D_OK;
+}
+
+int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, float *act, float *out, float *delta,
+                   double *loss, cudaStream_t st) {
+    int rc;
+    if ((rc = mlp_gradient(m, x, y, n, act, out, delta, loss, st))) return rc;
     m.t += 1;
     const float b1t = (float)std::pow(0.9, (double)m.t), b2t = (float)std::pow(0.999, (double)m.t);
     mlp_adam_kernel<<<(MLP_NP + 255) / 256, 256, 0, st>>>(m.P, m.G, m.M, m.V, lr, b1t, b2t);

@@ -152,6 +152,23 @@ int mc3d_mlp_train_step(mc3d_mlp m, const float *x, const float *y, int n, float
     return MC3D_OK;
 }
 
+int mc3d_mlp_gradient(mc3d_mlp m, const float *x, const float *y, int n, float *G, double *loss, void *stream) {
+    if (!m || !x || !y || !G || n <= 0) return fail(MC3D_ERR_ARG, "bad argument");
+    MC3D_CUDA_TRY(cudaSetDevice(m->device));
+    int rc = mlp_alloc_ws(m, n);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    MC3D_CUDA_TRY(cudaMemsetAsync(m->loss, 0, sizeof(double), st));
+    MC3D_CUDA_TRY(cudaMemsetAsync(m->dev.G, 0, MLP_NPARAM * sizeof(float), st));
+    if ((rc = mlp_gradient(m->dev, x, y, n, m->act, m->out, m->delta, m->loss, st))) return rc;
+    MC3D_CUDA_TRY(cudaMemcpyAsync(G, m->dev.G, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (loss) MC3D_CUDA_TRY(cudaMemcpyAsync(loss, m->loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    // the training step expects a zero gradient buffer
+    MC3D_CUDA_TRY(cudaMemsetAsync(m->dev.G, 0, MLP_NPARAM * sizeof(float), st));
+    MC3D_CUDA_TRY(cudaStreamSynchronize(st));
+    return MC3D_OK;
+}
+
 int mc3d_mlp_forward(mc3d_mlp m, const float *x, float *y, int n, void *stream) {
     if (!m || !x || !y || n <= 0) return fail(MC3D_ERR_ARG, "bad argument");
     MC3D_CUDA_TRY(cudaSetDevice(m->device));

@@ -80,8 +80,11 @@ __global__ void __launch_bounds__(1024) na_cfl_final(const double *partials, int
     if (threadIdx.x == 0) *out = v;
 }
 
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
+// Device address of the scratch array on the current device, looked up once
+// per device with that device current. CUDA loads a library's modules and
+// kernels on first use, and loading claims device memory (this file's module
+// holds the 512 KiB array); so the first call here also loads both kernels,
+// and every later call on the device neither loads nor allocates anything.
 int na_scratch(double **out) {
     int dev = 0;
     MC3D_CUDA_TRY(cudaGetDevice(&dev));
@@ -92,6 +95,11 @@ int na_scratch(double **out) {
         cudaError_t e = cudaGetSymbolAddress((void **)&p, g_cfl_partials);
         if (e != cudaSuccess)
             return mc3d::fail(MC3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, na_cfl_partials);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, na_cfl_final);
+        if (e != cudaSuccess)
+            return mc3d::fail(MC3D_ERR_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e));
         g_na_addr[dev] = p;
     }
     *out = g_na_addr[dev];

@@ -1,52 +1,11 @@
 // Device helpers shared by the line-solve kernels (sweeps.cu, sweeps_reg_*.cu).
 #pragma once
-#include <atomic>
 #include <cstdint>
 
 #include "mc3d_internal.h"
 
 namespace mc3d {
 
-// Launch settings of one kernel instantiation, kept per device because the
-// dynamic shared-memory attribute is set per device and the persistent CTA
-// count follows the device's SM count: the size the kernel has been opened
-// for (0: not yet) and the CTA count for that size, indexed by device ordinal.
-constexpr int MAX_DEVICES = 64;
-struct KernelLaunchState {
-    std::atomic<int> smem[MAX_DEVICES];
-    std::atomic<int> ctas[MAX_DEVICES];
-};
-
-// Opens `kern` for `smem` bytes of dynamic shared memory on the current
-// device (once per device and size) and, when ctas is given, returns the
-// number of CTAs of `threads` threads that fill the device.
-template <typename K>
-inline int open_kernel(K kern, KernelLaunchState &st, size_t smem, int threads, int *ctas) {
-    int dev = 0;
-    MC3D_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= MAX_DEVICES) return fail(MC3D_ERR_ARG, "device index out of range");
-    if ((int)smem > st.smem[dev].load()) {
-        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (ctas) {
-            int nsm = 0, per = 0;
-            MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-            MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem));
-            st.ctas[dev].store(nsm * (per > 0 ? per : 1));
-        }
-        st.smem[dev].store((int)smem);
-    }
-    if (ctas) {
-        *ctas = st.ctas[dev].load();
-        if (*ctas <= 0) {   // another thread opened the kernel without a CTA count
-            int nsm = 0, per = 0;
-            MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-            MC3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem));
-            *ctas = nsm * (per > 0 ? per : 1);
-            st.ctas[dev].store(*ctas);
-        }
-    }
-    return MC3D_OK;
-}
 
 constexpr int W = 32;       // lines per tile
 constexpr int SP = W + 1;   // shared-memory row pitch (elements)

@@ -36,13 +36,39 @@ def test_noalloc_cfl_matches_solver_dt_twice():
     s.set_initial_conditions(*hit_initial_condition(n, k0=4.0, seed=8, mt=0.3))
     stream = s.stream()
     out = torch.zeros(1, dtype=torch.float64, device="cuda")
-    for _ in range(2):
+    for call in range(2):
         s.sync()
+        free_before = torch.cuda.mem_get_info()[0]
         _noalloc_max(s, s.conserved_device_ptrs(), n, out, stream)   # ordered before the step on the same stream
+        s.sync()
+        if call == 1:
+            # after the set-up of the first call nothing more is claimed on the device
+            assert torch.cuda.mem_get_info()[0] == free_before
         s.step(1)
         dt = s.info()["dt"]
         got = cfl / out.item()
         assert abs(got - dt) <= 1e-12 * dt, (got, dt)
+
+
+def test_noalloc_cfl_reports_a_non_finite_state_as_nan():
+    """One NaN density makes the maximum NaN (the reference's loop would skip
+    that point), so a caller sees the broken state instead of a finite dt."""
+    import torch
+    n = 16
+    q = [torch.ones(n, n, n, dtype=torch.float64, device="cuda") for _ in range(5)]
+    q[4].fill_(2.5)
+    q[0][3, 4, 5] = float("nan")
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    lib = N.host_lib()
+    N.check(lib.mc3d_cfl_max_noalloc(*[C.c_void_p(t.data_ptr()) for t in q], None, None, None, 1.0, 1.0, 1.0,
+                                     n, n, n, 1.0 / n, 1.0 / n, 1.0 / n, C.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert math.isnan(out.item())
+    q[0][3, 4, 5] = 1.0
+    N.check(lib.mc3d_cfl_max_noalloc(*[C.c_void_p(t.data_ptr()) for t in q], None, None, None, 1.0, 1.0, 1.0,
+                                     n, n, n, 1.0 / n, 1.0 / n, 1.0 / n, C.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert math.isfinite(out.item()) and out.item() > 0
 
 
 def test_noalloc_rejects_fields_beyond_its_limit():
