@@ -277,18 +277,11 @@ def cylinder_block(args, local):
 
     import mpi_3dcompact_b200 as m
 
+    from mpi_3dcompact_b200.meshes import cylinder_flow_ic, cylinder_ogrid
     Nx, Ny, Nz = 512, 256, 64
-    r0, r1, span = 0.5, 30.0, 2.0
-    ratio = (r1 / r0) ** (1.0 / (Ny - 1))
-    th = 2 * math.pi * np.arange(Nx) / Nx
-    r = r0 * ratio ** np.arange(Ny)
-    zz = span * np.arange(Nz) / Nz
-    Z, Rr, TH = np.meshgrid(zz, r, th, indexing="ij")
-    x, y, z = Rr * np.cos(TH), -Rr * np.sin(TH), Z      # (theta clockwise, r, z): J > 0
-    rng = np.random.default_rng(3)
-    shp = (Nz, Ny, Nx)
-    ic = [np.ones(shp), 0.2 * (1 + 0.01 * rng.standard_normal(shp)), 0.002 * rng.standard_normal(shp),
-          0.002 * rng.standard_normal(shp), np.full(shp, 1 / 1.4)]
+    r1, span = 30.0, 2.0
+    x, y, z, ratio = cylinder_ogrid(Nx, Ny, Nz, 0.5, r1, span)   # (theta clockwise, r, z): J > 0
+    ic = cylinder_flow_ic((Nz, Ny, Nx), 0.2, 0.01, 3)
 
     def make(avg):
         opt = m.Options(grid=(Nx, Ny, Nz), fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="KENRK4",
