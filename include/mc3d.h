@@ -180,6 +180,23 @@ int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_typ
  * TMA-staged kernels. Calls may overlap solver steps and other calls on other
  * streams; each result is the same as when it runs alone. */
 int mc3d_op_apply(mc3d_op op, const void *const *in, void *const *out, int nfields, void *stream);
+
+/* calc1stDerivField_TPB (src/AbstractDerivatives.hpp:45 for Pade6 and CD2,
+ * :47 for Penta10; src/Pade6.cpp:48-107, src/Penta10.cpp:175-207,
+ * src/CD2.cpp:48-151) of a periodic derivative operator: the line's values
+ * beyond its ends come from caller-supplied ghost planes instead of wrapping
+ * around (the reference uses it for translated periodic meshes), then the
+ * periodic system is solved. *per_side = 2 (Pade6, CD2: Nm2 Nm1 | Np1 Np2)
+ * or 3 (Penta10: Nm3 Nm2 Nm1 | Np1 Np2 Np3). ghosts[f * 2 * per_side + m] are
+ * device planes of the op's precision, in the reference's argument order
+ * (Nm_{per_side} .. Nm1, Np1 .. Np_{per_side}); Nm_m holds the value at index
+ * -m of each line, Np_m the value at N - 1 + m. A plane has one value per line
+ * along dir, x fastest over the other two directions: dir 0: [k*Ny + j],
+ * dir 1: [k*Nx + i], dir 2: [j*Nx + i] (the reference's y-pencil planes are
+ * [i*Nz + k]). The first call allocates the operator's one-field scratch. */
+int mc3d_op_tpb_ghosts(mc3d_op op, int *per_side);
+int mc3d_op_apply_tpb(mc3d_op op, const void *const *in, void *const *out, int nfields,
+                      const void *const *ghosts, void *stream);
 int mc3d_op_destroy(mc3d_op op);
 
 /* AbstractDerivatives::calcNeumann (src/Pade6.cpp:395-397, src/CD2.cpp:183):
@@ -275,6 +292,39 @@ int mc3d_solver_set_initial_device(mc3d_solver s, const double *rho, const doubl
  * e.g. src/RK4.hpp:127-178). For LSLDDRK4 the 5- and 6-stage halves alternate,
  * one half per step. Asynchronous on the solver's stream. */
 int mc3d_solver_step(mc3d_solver s, int nsteps);
+
+/* ---- the same time step driven stage by stage ----
+ * The virtuals of AbstractCSolver that AbstractRK::executeSolverLoop calls
+ * (src/AbstractCSolver.hpp:82-87, e.g. the loop of src/RK4.hpp:127-178 and
+ * src/LSLDDRK4.hpp:324-459), and AbstractRK::updateConservedData
+ * (src/AbstractRK.hpp:15), so a GPU-backed RK object and solver drop in
+ * behind the reference's loop. Called in the reference's order, they give the
+ * state mc3d_solver_step gives, bit for bit; a call out of order returns
+ * MC3D_ERR_CONFIG and changes nothing. All asynchronous on the solver's stream.
+ *   preStep        calcDtFromCFL (src/CurvilinearCSolver.hpp:310-318)
+ *   preSubStep     preStepBCHandling + preStepDerivatives of stage rkStep and
+ *                  the first two directions of the flux divergence
+ *                  (src/CurvilinearCSolver.hpp:320-327)
+ *   solveEqnSet    solveContinuity .. solveEnergy: the third direction of the
+ *                  divergence with the k2 assembly (Core.cpp:790-947)
+ *   postSubStep    postStepBCHandling (src/CurvilinearCSolver_BC.cpp:702-842)
+ *   rk_update      updateConservedData of `scheme` (MC3D_RK4 ..), stage
+ *                  rkStep; dual_step: LSLDDRK4's rkDualStepStep (1: the
+ *                  5-stage half, 2: the 6-stage half), ignored otherwise
+ *   updateData     filterConservedData when rkLast (or SUBSTEPFILTERING) and
+ *                  updateNonConservedData (src/CurvilinearCSolver.hpp:346-353)
+ *   postStep       statistics and the optional sponge relaxation
+ *                  (src/CurvilinearCSolver.hpp:355-375)
+ * mc3d_solver_stage_count: the stages of the current time step (or of the
+ * next one between steps): RK4 4, TVDRK3 3, KENRK4 5, LSLDDRK4 5 or 6. */
+int mc3d_solver_pre_step(mc3d_solver s);
+int mc3d_solver_stage_count(mc3d_solver s, int *stages);
+int mc3d_solver_pre_substep(mc3d_solver s, int rk_step);
+int mc3d_solver_solve_eqn_set(mc3d_solver s);
+int mc3d_solver_post_substep(mc3d_solver s);
+int mc3d_rk_update(mc3d_solver s, int scheme, int rk_step, int dual_step);
+int mc3d_solver_update_data(mc3d_solver s, int rk_last);
+int mc3d_solver_post_step(mc3d_solver s);
 
 /* Copy the conserved state rho1, rhoU1, rhoV1, rhoW1, rhoE1 (FP64) to host. */
 int mc3d_solver_get_conserved(mc3d_solver s, double *rho, double *rhoU, double *rhoV, double *rhoW,
@@ -394,6 +444,39 @@ const char *mc3d_solver_timing_report(mc3d_solver s);
  * that launch are invalid). mc3d_solver_info and mc3d_solver_get_conserved
  * return MC3D_ERR_TIMEOUT when it is nonzero. */
 int mc3d_tma_wait_timeouts(int device, int *count);
+
+/* ---- SGS models on their own (AbstractSGS, src/AbstractSGS.hpp:10-42) ----
+ * A GPU VremanSGS / DSMSGS (src/VremanSGS.hpp:13-41, src/DSMSGS.hpp:20-118)
+ * that a caller drives with its own gradients: model MC3D_VREMAN | MC3D_DSM,
+ * LESAVERAGING (MC3D_AVG_*), DSMTESTFILTER (1 Pade, 2 explicit), DSMUSETAUKK,
+ * the block, the BC types of the three directions (periodic / Dirichlet
+ * test-filter and averaging closures), the computational spacings
+ * dxi[3] = Domain::dx, dy, dz and the metric Jacobian J (a device field of the
+ * object's precision, or NULL with the constant Jc; Vreman's filter width is
+ * (dx dy dz / J)^(1/3)). Fields are device arrays, x fastest: gradients and
+ * outputs in the object's precision (double for MC3D_FP64, float for
+ * MC3D_FP32BULK), the conserved rho..rhoE always FP64 (calcKSGS reads rho ..
+ * rhoW only; q[4] may be NULL there). gradU[3*a + b] = d u_a / d x_b and
+ * gradT[b] = d T / d x_b are physical gradients (preStepDerivatives'
+ * J^T-transformed ones, Core.cpp:548-561, :596-600). As in the reference,
+ * each model implements only its own virtuals and the others do nothing:
+ * Vreman getSGSViscosity (mu_sgs, averaged with Compact10(-0.49) filters
+ * when LOCAL); DSM calcMuSGSTaukk (mu_sgs and, with taukk non-NULL, tau_kk)
+ * and calcKSGS (k_sgs; it reuses the filtered fields of the preceding
+ * calcMuSGSTaukk, so call it after that one on the same state), averaged per
+ * doAveraging (src/AbstractSGS.cpp:13-160). The object holds its work
+ * fields (DSM: 49 fields of the block). */
+typedef struct mc3d_sgs_s *mc3d_sgs;
+int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, int Nx, int Ny, int Nz,
+                    const int bc_types[3], const double dxi[3], const void *J, double Jc, int precision,
+                    int device, mc3d_sgs *out);
+int mc3d_sgs_destroy(mc3d_sgs sgs);
+int mc3d_sgs_get_viscosity(mc3d_sgs sgs, const void *const gradU[9], const double *const q[5], void *mu_sgs,
+                           void *stream);
+int mc3d_sgs_calc_mu_taukk(mc3d_sgs sgs, const void *const gradU[9], const double *const q[5], void *mu_sgs,
+                           void *taukk, void *stream);
+int mc3d_sgs_calc_ksgs(mc3d_sgs sgs, const void *const gradT[3], const double *const q[5], const void *T,
+                       void *k_sgs, void *stream);
 
 /* ---- allocation-free CFL reduction ----
  * No counterpart in the reference: an extra entry point for callers that must

@@ -90,6 +90,27 @@ class _Derivative(_Operator):
         """Batched form: one launch for several fields."""
         self._apply(ins, outs, stream)
 
+    def calc1stDerivField_TPB(self, dataIn, dataOut, *ghosts, stream=None):
+        """AbstractDerivatives::calc1stDerivField_TPB (src/AbstractDerivatives.hpp:45,
+        :47): ghost planes Nm2, Nm1, Np1, Np2 (Pade6, CD2) or Nm3 .. Np3
+        (Penta10), each shaped like the field without its `direction` axis."""
+        w = C.c_int()
+        N.check(N.host_lib().mc3d_op_tpb_ghosts(self._h, C.byref(w)))
+        if len(ghosts) != 2 * w.value:
+            raise ValueError(f"{type(self).__name__} takes {2 * w.value} ghost planes")
+        for t in [dataIn, dataOut]:
+            if tuple(t.shape) != self.shape or not t.is_contiguous():
+                raise ValueError("fields must be contiguous and of the operator's shape")
+        pshape = tuple(n for a, n in enumerate(self.shape) if a != 2 - self.direction)
+        for gpl in ghosts:
+            if tuple(gpl.shape) != pshape or not gpl.is_contiguous():
+                raise ValueError(f"ghost planes must be contiguous of shape {pshape}")
+        a = (C.c_void_p * 1)(dataIn.data_ptr())
+        b = (C.c_void_p * 1)(dataOut.data_ptr())
+        g = (C.c_void_p * len(ghosts))(*[t.data_ptr() for t in ghosts])
+        st = C.c_void_p(stream) if stream is not None else None
+        N.check(N.host_lib().mc3d_op_apply_tpb(self._h, a, b, 1, g, st))
+
     def calcNeumann(self, f):
         return calc_neumann(self._fd, f)
 

@@ -76,6 +76,8 @@ def host_lib():
             "mc3d_filter_create": (ip, [ip, dp, ip, C.POINTER(C.c_int), ip, ip, ip, ip, ip, C.POINTER(vp)]),
             "mc3d_op_apply": (ip, [vp, C.POINTER(vp), C.POINTER(vp), ip, vp]),
             "mc3d_op_destroy": (ip, [vp]),
+            "mc3d_op_tpb_ghosts": (ip, [vp, C.POINTER(ip)]),
+            "mc3d_op_apply_tpb": (ip, [vp, C.POINTER(vp), C.POINTER(vp), ip, C.POINTER(vp), vp]),
             "mc3d_calc_neumann": (dp, [ip, C.POINTER(dp)]),
             "mc3d_solver_create": (ip, [C.POINTER(Config), ip, C.POINTER(vp)]),
             "mc3d_solver_destroy": (ip, [vp]),
@@ -103,6 +105,14 @@ def host_lib():
             "mc3d_solver_set_initial": (ip, [vp] + [C.POINTER(dp)] * 5),
             "mc3d_solver_set_initial_device": (ip, [vp] + [vp] * 5),
             "mc3d_solver_step": (ip, [vp, ip]),
+            "mc3d_solver_pre_step": (ip, [vp]),
+            "mc3d_solver_stage_count": (ip, [vp, C.POINTER(ip)]),
+            "mc3d_solver_pre_substep": (ip, [vp, ip]),
+            "mc3d_solver_solve_eqn_set": (ip, [vp]),
+            "mc3d_solver_post_substep": (ip, [vp]),
+            "mc3d_rk_update": (ip, [vp, ip, ip, ip]),
+            "mc3d_solver_update_data": (ip, [vp, ip]),
+            "mc3d_solver_post_step": (ip, [vp]),
             "mc3d_solver_get_conserved": (ip, [vp] + [C.POINTER(dp)] * 5),
             "mc3d_solver_conserved_device": (ip, [vp, C.POINTER(vp)]),
             "mc3d_solver_info": (ip, [vp, C.POINTER(ip), C.POINTER(dp), C.POINTER(dp), C.POINTER(C.c_longlong)]),
@@ -135,6 +145,12 @@ def host_lib():
             "mc3d_solver_copy_conserved_device": (ip, [vp, C.POINTER(vp)]),
             "mc3d_solver_mlp_fallbacks": (ip, [vp, C.POINTER(C.c_longlong)]),
             "mc3d_solver_set_sponge": (ip, [vp, C.POINTER(dp)]),
+            "mc3d_sgs_create": (ip, [ip, ip, ip, ip, ip, ip, ip, C.POINTER(ip), C.POINTER(dp), vp, dp, ip, ip,
+                                     C.POINTER(vp)]),
+            "mc3d_sgs_destroy": (ip, [vp]),
+            "mc3d_sgs_get_viscosity": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp]),
+            "mc3d_sgs_calc_mu_taukk": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp, vp]),
+            "mc3d_sgs_calc_ksgs": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp, vp]),
             "mc3d_solver_set_sponge_avg": (ip, [vp, C.POINTER(C.POINTER(dp))]),
         }
         for name, (res, args) in sigs.items():

@@ -32,6 +32,14 @@ struct mc3d_op_s {
     bool filter = false;
     int precision = MC3D_FP64;
     int device = 0;
+    // TPB form of a periodic derivative: the scheme, the same left-hand side
+    // with an identity right-hand-side stencil, and one field of scratch for
+    // the right-hand side (both made at the first TPB call)
+    int fd_type = -1;
+    double dh = 1.0;
+    LineOpBuf tpb_solve;
+    bool tpb_ready = false;
+    void *tpb_rhs = nullptr;
 };
 
 extern "C" {
@@ -401,6 +409,8 @@ extern "C" int mc3d_deriv_create(int fd_type, int bc_type, int dir, int Nx, int 
     o->bc_types[dir] = bc_type;
     o->precision = precision;
     o->device = device;
+    o->fd_type = fd_type;
+    o->dh = dh;
     int N[3] = {Nx, Ny, Nz};
     try {
         o->host = build_deriv_op(fd_type, bc_type, N[dir], dh);
@@ -471,8 +481,85 @@ extern "C" int mc3d_op_destroy(mc3d_op o) {
     if (!o) return MC3D_OK;
     cudaSetDevice(o->device);
     free_line_op(o->buf);
+    free_line_op(o->tpb_solve);
+    if (o->tpb_rhs) cudaFree(o->tpb_rhs);
     delete o;
     return MC3D_OK;
+}
+
+// ghost planes per side of the TPB form: the BW5 signature (Pade6, CD2) takes
+// Nm2, Nm1, Np1, Np2; the BW7 one (Penta10) Nm3 .. Np3
+static int tpb_width(const mc3d_op o) { return o->fd_type == MC3D_PENTA10 ? 3 : 2; }
+
+extern "C" int mc3d_op_tpb_ghosts(mc3d_op o, int *per_side) {
+    if (!o || !per_side) return fail(MC3D_ERR_ARG, "null argument");
+    if (o->filter || o->fd_type < 0) return fail(MC3D_ERR_CONFIG, "TPB is a form of the derivative operators only");
+    *per_side = tpb_width(o);
+    return MC3D_OK;
+}
+
+template <typename R>
+static int op_apply_tpb_t(mc3d_op o, const void *const *in, void *const *out, int nf, const void *const *ghosts,
+                          cudaStream_t st) {
+    const int G = tpb_width(o);
+    TpbPlanes<R> gp{};
+    gp.G = G;
+    gp.H = o->host.H;
+    gp.explicit_cd2 = o->fd_type == MC3D_CD2;
+    for (int k = 0; k < 7; k++) gp.st[k] = k <= 2 * o->host.H ? o->host.st[k] : 0.0;
+    const LineOpBuf &sb = o->tpb_solve;
+    const LineOpDev<R> &sd = std::is_same<R, float>::value ? *(const LineOpDev<R> *)&sb.f32
+                                                           : *(const LineOpDev<R> *)&sb.f64;
+    RhsFinalArgs<R> rf{};
+    for (int f = 0; f < nf; f++) {
+        if (!in[f] || !out[f]) return fail(MC3D_ERR_ARG, "null field pointer");
+        if (in[f] == out[f]) return fail(MC3D_ERR_ARG, "in and out alias");
+        for (int m = 0; m < 2 * G; m++) {
+            gp.p[m] = (const R *)ghosts[(size_t)f * 2 * G + m];
+            if (!gp.p[m]) return fail(MC3D_ERR_ARG, "null ghost plane");
+        }
+        int rc;
+        if (gp.explicit_cd2)   // explicit: the right-hand side is the derivative
+            rc = launch_tpb_planes_rhs<R>(o->g, o->dir, (const R *)in[f], gp, o->dh, (R *)out[f], st);
+        else {
+            rc = launch_tpb_planes_rhs<R>(o->g, o->dir, (const R *)in[f], gp, o->dh, (R *)o->tpb_rhs, st);
+            if (!rc) {
+                SweepBatch<R> b{};
+                b.nf = 1;
+                b.in[0] = (const R *)o->tpb_rhs;
+                b.out[0] = (R *)out[f];
+                rc = launch_sweep<R>(o->dir, o->g, sd, b, EPI_STORE, rf, o->bc_types, false, st);
+            }
+        }
+        if (rc) return rc;
+    }
+    return MC3D_OK;
+}
+
+extern "C" int mc3d_op_apply_tpb(mc3d_op o, const void *const *in, void *const *out, int nfields,
+                                 const void *const *ghosts, void *stream) {
+    if (!o || !in || !out || !ghosts) return fail(MC3D_ERR_ARG, "null argument");
+    if (o->filter || o->fd_type < 0) return fail(MC3D_ERR_CONFIG, "TPB is a form of the derivative operators only");
+    if (o->bc_types[o->dir] != MC3D_PERIODIC_SOLVE)
+        return fail(MC3D_ERR_CONFIG, "CANT USE calc1stDeriv_TPB for non-periodic boundary conditions!!");
+    if (nfields <= 0) return MC3D_OK;
+    MC3D_CUDA_TRY(cudaSetDevice(o->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!o->tpb_ready) {
+        if (o->fd_type != MC3D_CD2) {
+            LineOpHost sv = o->host;
+            for (double &v : sv.st) v = 0.0;
+            sv.st[sv.H] = 1.0;
+            sv.deriv = false;
+            sv.inv_dh = 1.0;
+            if (int rc = upload_line_op(sv, o->precision, o->tpb_solve)) return rc;
+            const size_t bytes = (size_t)o->g.n() * (o->precision == MC3D_FP64 ? 8 : 4);
+            MC3D_CUDA_TRY(cudaMalloc(&o->tpb_rhs, bytes));
+        }
+        o->tpb_ready = true;
+    }
+    return o->precision == MC3D_FP64 ? op_apply_tpb_t<double>(o, in, out, nfields, ghosts, st)
+                                     : op_apply_tpb_t<float>(o, in, out, nfields, ghosts, st);
 }
 
 extern "C" double mc3d_calc_neumann(int fd_type, const double *f) {

@@ -413,6 +413,19 @@ struct MetOut9 {
 };
 int launch_tpb_rhs(const Grid3 &g, int dir, const double *f, const TpbArgs &a, double *rhs, cudaStream_t st);
 
+// TPB right-hand side from caller-supplied ghost planes (tpb.cu): G planes per
+// side (p[0..G-1] = Nm_G..Nm_1, p[G..2G-1] = Np_1..Np_G), interior stencil
+// st[0..2H] (explicit_cd2: the reference's CD2 end rows)
+template <typename R>
+struct TpbPlanes {
+    const R *p[6];
+    int G, H, explicit_cd2;
+    double st[7];
+};
+template <typename R>
+int launch_tpb_planes_rhs(const Grid3 &g, int dir, const R *f, const TpbPlanes<R> &gp, double dh, R *rhs,
+                          cudaStream_t st);
+
 // ---- running statistics (stats.cu) ------------------------------------------
 struct StatsIn {
     const double *q[5];      // filtered conserved state (rho1 .. rhoE1)

@@ -77,6 +77,12 @@ struct mc3d_solver_s {
     double st_vw = 0.0, st_tw = 0.0, st_prev = 0.0;
     double *hook_scratch = nullptr;   // block partials of the diagnostic reductions
     int lsldd_half = 1;
+    // stage-level driving (mc3d_solver_pre_step .. mc3d_solver_post_step): the
+    // last call made in the current time step, its stage, the step's stage
+    // count, whether it filters, and the sponge faces relaxed before it
+    int phase = 0;
+    int cur_stage = 0, cur_ns = 0, cur_relaxed = 0;
+    bool cur_filter_now = false;
     long long stages = 0;
     long long launches = 0;
     bool initialized = false;
@@ -442,7 +448,9 @@ static int dsm_ksgs(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
     return toc(s);
 }
 
-// RHS of one stage; s->prim holds rho, U, V, W, T of the stage state qP.
+// preStepDerivatives and the first two divergence sweeps of one stage
+// (Core.cpp:468-787, the RHS up to the last direction); s->prim holds rho, U,
+// V, W, T of the stage state qP.
 template <typename R>
 static int stage_rhs(mc3d_solver s, double *const *qP) {
     int rc;
@@ -540,17 +548,28 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
             return rc;
         if ((rc = toc(s))) return rc;
     }
-    if ((rc = sweep<R>(s, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->rhs, nullptr, false))) return rc;
-    if (s->have_walls || s->have_sponge) {
-        // wall faces need the wall-normal derivative of the mass flux alone
-        for (int d = 0; d < 3; d++) {
-            if (!is_wall_kind(s->cfg.bc_kind[2 * d]) && !is_wall_kind(s->cfg.bc_kind[2 * d + 1])) continue;
-            void *in[1] = {s->flux[5 * d]}, *out[1] = {s->tB[d]};
-            if ((rc = sweep<R>(s, d, s->dop[d], 1, in, out, EPI_STORE, nullptr, nullptr, false))) return rc;
-        }
-        if ((rc = face_poststep<R>(s))) return rc;
-    }
     return MC3D_OK;
+}
+
+// solveContinuity .. solveEnergy (Core.cpp:790-947): the third divergence
+// sweep assembles k2 = dt J (partial RHS - dH/dxi3) in its epilogue
+template <typename R>
+static int stage_solve(mc3d_solver s) {
+    return sweep<R>(s, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->rhs, nullptr, false);
+}
+
+// postStepBCHandling (src/CurvilinearCSolver_BC.cpp:702-842) on k2
+template <typename R>
+static int stage_post(mc3d_solver s) {
+    if (!s->have_walls && !s->have_sponge) return MC3D_OK;
+    int rc;
+    // wall faces need the wall-normal derivative of the mass flux alone
+    for (int d = 0; d < 3; d++) {
+        if (!is_wall_kind(s->cfg.bc_kind[2 * d]) && !is_wall_kind(s->cfg.bc_kind[2 * d + 1])) continue;
+        void *in[1] = {s->flux[5 * d]}, *out[1] = {s->tB[d]};
+        if ((rc = sweep<R>(s, d, s->dop[d], 1, in, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+    }
+    return face_poststep<R>(s);
 }
 
 // MC3D_ERR_TIMEOUT when a line-solve tile load gave up waiting on this device
@@ -583,82 +602,128 @@ static int primitives_cfl(mc3d_solver s) {
     return toc(s);
 }
 
+static int stages_of(mc3d_solver s) {
+    const int scheme = s->cfg.rk_type;
+    return scheme == MC3D_RK4 ? 4 : scheme == MC3D_TVDRK3 ? 3 : scheme == MC3D_KENRK4 ? 5 : (s->lsldd_half == 1 ? 5 : 6);
+}
+
+// preStep (src/CurvilinearCSolver.hpp:310-318): calcDtFromCFL on the current
+// state, fused into the primitives of stage 1, which read the same state
+// (unless a sponge relaxation after the previous step formed both already)
 template <typename R>
-static int one_step(mc3d_solver s) {
+static int step_begin(mc3d_solver s) {
     int rc;
-    // preStep: calcDtFromCFL on the current state, fused into the primitives of
-    // stage 1, which read the same state (unless a sponge relaxation after the
-    // previous step formed both already)
     const int first = s->host_time_step == s->cfg.time_step0;
     if (!s->prims_ready)
         if ((rc = primitives_cfl<R>(s))) return rc;
-    const int relaxed = s->prims_ready ? sponge_faces(s) : 0;
+    s->cur_relaxed = s->prims_ready ? sponge_faces(s) : 0;
     s->prims_ready = false;
     s->launches++;
     if ((rc = launch_finalize_dt(s->ts, s->cfg.ts_type, s->cfg.cfl, s->cfg.dt, first, s->stream))) return rc;
     s->host_time_step++;
-    const bool filter_now = s->host_time_step % s->cfg.filter_step == 0;
-
-    int scheme = s->cfg.rk_type;
-    int ns = scheme == MC3D_RK4 ? 4 : scheme == MC3D_TVDRK3 ? 3 : scheme == MC3D_KENRK4 ? 5 : (s->lsldd_half == 1 ? 5 : 6);
-    for (int st = 1; st <= ns; st++) {
-        // stage 1 works on q1 (filtered at the end of the previous step); later
-        // stages on qk, whose primitives the RK update of the previous stage
-        // already wrote unless a sub-step filter changed qk since
-        if (st > 1 && s->cfg.substep_filtering)
-            if ((rc = primitives<R>(s, s->qk))) return rc;
-        if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
-        s->cons_mask = st == 1 ? relaxed : 0;
-        rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk);
-        s->cons_mask = 0;
-        if (rc) return rc;
-        RkStage rs{};
-        rs.scheme = scheme;
-        rs.stage = st;
-        rs.nstages = ns;
-        if (scheme == MC3D_RK4) {
-            rs.a = RK4_A[st - 1];
-            rs.b = st < 4 ? RK4_B[st - 1] : 0.0;
-        } else if (scheme == MC3D_KENRK4) {
-            rs.a = KEN_A[st - 1];
-            rs.b = KEN_B[st - 1];
-        } else if (scheme == MC3D_LSLDDRK4) {
-            rs.a = s->lsldd_half == 1 ? LS_A1[st - 1] : LS_A2[st - 1];
-            rs.b = s->lsldd_half == 1 ? LS_B1[st - 1] : LS_B2[st - 1];
-        }
-        const R *k2[5];
-        R *pw[5];
-        for (int v = 0; v < 5; v++) {
-            k2[v] = (const R *)s->k2[v];
-            pw[v] = (R *)s->prim[v];
-        }
-        bool fuse_prims = st < ns && !s->cfg.substep_filtering;
-        // last stage of a filtered step (FP32 path): the filter's working copy
-        const bool copy_final = st == ns && filter_now && s->prec != MC3D_FP64;
-        if (copy_final)
-            for (int v = 0; v < 5; v++) pw[v] = (R *)s->tC[v];
-        s->launches++;
-        {
-            // reads k2 and the FP64 registers the scheme touches, writes the updated ones
-            double b = 5.0 * sizeof(R);
-            if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
-            else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
-            else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
-            if (fuse_prims || copy_final) b += 5.0 * sizeof(R);
-            if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
-        }
-        if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, (fuse_prims || copy_final) ? pw : nullptr,
-                                      s->stream, copy_final)))
-            return rc;
-        if ((rc = toc(s))) return rc;
-        if (copy_final) s->tc_fresh = true;
-        bool last = st == ns;
-        if (last || s->cfg.substep_filtering)
-            if ((rc = filter_conserved<R>(s, last))) return rc;
-        s->stages++;
-    }
-    if (scheme == MC3D_LSLDDRK4) s->lsldd_half = s->lsldd_half == 1 ? 2 : 1;
+    s->cur_filter_now = s->host_time_step % s->cfg.filter_step == 0;
+    s->cur_ns = stages_of(s);
+    s->cur_stage = 0;
     return MC3D_OK;
+}
+
+// preSubStep (src/CurvilinearCSolver.hpp:320-327) of stage st: stage 1 works
+// on q1 (filtered at the end of the previous step); later stages on qk, whose
+// primitives the RK update of the previous stage already wrote unless a
+// sub-step filter changed qk since. preStepBCHandling, then
+// preStepDerivatives with the first two divergence sweeps.
+template <typename R>
+static int stage_begin(mc3d_solver s, int st) {
+    int rc;
+    if (st > 1 && s->cfg.substep_filtering)
+        if ((rc = primitives<R>(s, s->qk))) return rc;
+    if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
+    s->cons_mask = st == 1 ? s->cur_relaxed : 0;
+    rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk);
+    s->cons_mask = 0;
+    return rc;
+}
+
+// updateConservedData of the scheme's stage st (RK4.hpp:47-125,
+// TVDRK3.hpp:50-133, KenRK4.hpp:53-152, LSLDDRK4.hpp:93-320); except after a
+// step's last stage or with sub-step filtering, the same pass writes the
+// primitives of the next stage's state (updateNonConservedData)
+template <typename R>
+static int stage_rk(mc3d_solver s, int st) {
+    int rc;
+    const int scheme = s->cfg.rk_type, ns = s->cur_ns;
+    RkStage rs{};
+    rs.scheme = scheme;
+    rs.stage = st;
+    rs.nstages = ns;
+    if (scheme == MC3D_RK4) {
+        rs.a = RK4_A[st - 1];
+        rs.b = st < 4 ? RK4_B[st - 1] : 0.0;
+    } else if (scheme == MC3D_KENRK4) {
+        rs.a = KEN_A[st - 1];
+        rs.b = KEN_B[st - 1];
+    } else if (scheme == MC3D_LSLDDRK4) {
+        rs.a = s->lsldd_half == 1 ? LS_A1[st - 1] : LS_A2[st - 1];
+        rs.b = s->lsldd_half == 1 ? LS_B1[st - 1] : LS_B2[st - 1];
+    }
+    const R *k2[5];
+    R *pw[5];
+    for (int v = 0; v < 5; v++) {
+        k2[v] = (const R *)s->k2[v];
+        pw[v] = (R *)s->prim[v];
+    }
+    const bool fuse_prims = st < ns && !s->cfg.substep_filtering;
+    // last stage of a filtered step (FP32 path): the filter's working copy
+    const bool copy_final = st == ns && s->cur_filter_now && s->prec != MC3D_FP64;
+    if (copy_final)
+        for (int v = 0; v < 5; v++) pw[v] = (R *)s->tC[v];
+    s->launches++;
+    {
+        // reads k2 and the FP64 registers the scheme touches, writes the updated ones
+        double b = 5.0 * sizeof(R);
+        if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
+        else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
+        else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
+        if (fuse_prims || copy_final) b += 5.0 * sizeof(R);
+        if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
+    }
+    if ((rc = launch_rk_update<R>(s->g, rs, k2, s->q1, s->qk, s->q2, (fuse_prims || copy_final) ? pw : nullptr,
+                                  s->stream, copy_final)))
+        return rc;
+    if ((rc = toc(s))) return rc;
+    if (copy_final) s->tc_fresh = true;
+    return MC3D_OK;
+}
+
+// updateData (src/CurvilinearCSolver.hpp:346-353): filterConservedData after
+// the last stage (or every stage with sub-step filtering); the primitives of
+// the next state come from the RK update or from the next stage / step
+template <typename R>
+static int stage_end(mc3d_solver s, int st) {
+    int rc;
+    const bool last = st == s->cur_ns;
+    if (last || s->cfg.substep_filtering)
+        if ((rc = filter_conserved<R>(s, last))) return rc;
+    s->stages++;
+    return MC3D_OK;
+}
+
+// postStep (src/CurvilinearCSolver.hpp:355-375): LSLDDRK4 alternates its
+// halves; statistics; the optional sponge relaxation.
+static int step_end(mc3d_solver s);
+
+template <typename R>
+static int one_step(mc3d_solver s) {
+    int rc;
+    if ((rc = step_begin<R>(s))) return rc;
+    for (int st = 1; st <= s->cur_ns; st++) {
+        if ((rc = stage_begin<R>(s, st))) return rc;
+        if ((rc = stage_solve<R>(s))) return rc;
+        if ((rc = stage_post<R>(s))) return rc;
+        if ((rc = stage_rk<R>(s, st))) return rc;
+        if ((rc = stage_end<R>(s, st))) return rc;
+    }
+    return step_end(s);
 }
 
 }  // namespace mc3d
@@ -1312,6 +1377,28 @@ static int stats_update(mc3d_solver s) {
 }  // extern "C"
 
 namespace mc3d {
+
+// postStep (src/CurvilinearCSolver.hpp:355-375). The statistics read the
+// primitives of the filtered state and rho2, neither of which the sponge
+// relaxation changes, so they are updated first.
+static int step_end(mc3d_solver s) {
+    int rc;
+    if (s->cfg.rk_type == MC3D_LSLDDRK4) s->lsldd_half = s->lsldd_half == 1 ? 2 : 1;
+    if ((s->cfg.velocity_stats || s->cfg.thermo_stats) && s->host_time_step % s->cfg.stats_interval == 0)
+        if ((rc = ::stats_update(s))) return rc;
+    if (s->cfg.sponge_relax && s->have_sponge) {
+        // updateSponge changes rho1..rhoE1 alone: the primitives, and with
+        // them the next step's CFL and stage-1 derivatives, stay those of the
+        // filtered state, so they are formed before the relaxation
+        if ((rc = s->prec == MC3D_FP64 ? primitives_cfl<double>(s) : primitives_cfl<float>(s))) return rc;
+        s->prims_ready = true;
+        s->launches++;
+        if ((rc = launch_sponge_relax(s->g, s->q1, s->spg_avg, s->ts, s->cfg.sponge_avg_time, s->cfg.sponge_p_inf,
+                                      sponge_faces(s), s->stream)))
+            return rc;
+    }
+    return MC3D_OK;
+}
 constexpr int HOOK_BLOCKS = 148 * 4;
 
 template <typename R>
@@ -1516,26 +1603,102 @@ int mc3d_solver_step(mc3d_solver s, int nsteps) {
     if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no initial condition");
     if (s->cfg.les_model == MC3D_MLPSGS && !s->mlp) return fail(MC3D_ERR_CONFIG, "LESMODEL = MLP needs mc3d_solver_set_mlp");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    if (s->phase != 0) return fail(MC3D_ERR_CONFIG, "a time step driven stage by stage is in progress");
     for (int i = 0; i < nsteps; i++) {
         int rc = s->prec == MC3D_FP64 ? one_step<double>(s) : one_step<float>(s);
         if (rc) return rc;
-        // postStep (src/CurvilinearCSolver.hpp:355-375). The statistics read the
-        // primitives of the filtered state and rho2, neither of which the
-        // sponge relaxation changes, so they are updated first.
-        if ((s->cfg.velocity_stats || s->cfg.thermo_stats) && s->host_time_step % s->cfg.stats_interval == 0)
-            if ((rc = stats_update(s))) return rc;
-        if (s->cfg.sponge_relax && s->have_sponge) {
-            // updateSponge changes rho1..rhoE1 alone: the primitives, and with
-            // them the next step's CFL and stage-1 derivatives, stay those of
-            // the filtered state, so they are formed before the relaxation
-            if ((rc = s->prec == MC3D_FP64 ? primitives_cfl<double>(s) : primitives_cfl<float>(s))) return rc;
-            s->prims_ready = true;
-            s->launches++;
-            if ((rc = mc3d::launch_sponge_relax(s->g, s->q1, s->spg_avg, s->ts, s->cfg.sponge_avg_time,
-                                                s->cfg.sponge_p_inf, sponge_faces(s), s->stream)))
-                return rc;
-        }
     }
+    return MC3D_OK;
+}
+
+// ---- stage-level driving: the calls AbstractRK::executeSolverLoop makes ----
+// Phases of a time step: 0 between steps, 1 ready for a stage's preSubStep,
+// 2 preSubStep done, 3 solveEqnSet done, 4 postSubStep done, 5 RK update done,
+// 6 last stage done (postStep next).
+static int stage_ready(mc3d_solver s, int phase, const char *what) {
+    if (!s) return fail(MC3D_ERR_ARG, "null solver");
+    if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no initial condition");
+    if (s->cfg.les_model == MC3D_MLPSGS && !s->mlp) return fail(MC3D_ERR_CONFIG, "LESMODEL = MLP needs mc3d_solver_set_mlp");
+    if (s->phase != phase)
+        return fail(MC3D_ERR_CONFIG, std::string(what) + " out of order (the reference's RK loop order is preStep, "
+                                     "then per stage preSubStep, solveEqnSet, postSubStep, updateConservedData, "
+                                     "updateData, then postStep)");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    return MC3D_OK;
+}
+
+int mc3d_solver_pre_step(mc3d_solver s) {
+    if (int rc = stage_ready(s, 0, "preStep")) return rc;
+    int rc = s->prec == MC3D_FP64 ? step_begin<double>(s) : step_begin<float>(s);
+    if (rc) return rc;
+    s->phase = 1;
+    return MC3D_OK;
+}
+
+int mc3d_solver_stage_count(mc3d_solver s, int *stages) {
+    if (!s || !stages) return fail(MC3D_ERR_ARG, "null argument");
+    *stages = s->phase == 0 ? stages_of(s) : s->cur_ns;
+    return MC3D_OK;
+}
+
+int mc3d_solver_pre_substep(mc3d_solver s, int rk_step) {
+    if (int rc = stage_ready(s, 1, "preSubStep")) return rc;
+    if (rk_step != s->cur_stage + 1 || rk_step > s->cur_ns)
+        return fail(MC3D_ERR_CONFIG, "preSubStep: rkStep " + std::to_string(rk_step) + " where stage " +
+                                         std::to_string(s->cur_stage + 1) + " of " + std::to_string(s->cur_ns) +
+                                         " is next");
+    int rc = s->prec == MC3D_FP64 ? stage_begin<double>(s, rk_step) : stage_begin<float>(s, rk_step);
+    if (rc) return rc;
+    s->cur_stage = rk_step;
+    s->phase = 2;
+    return MC3D_OK;
+}
+
+int mc3d_solver_solve_eqn_set(mc3d_solver s) {
+    if (int rc = stage_ready(s, 2, "solveEqnSet")) return rc;
+    int rc = s->prec == MC3D_FP64 ? stage_solve<double>(s) : stage_solve<float>(s);
+    if (rc) return rc;
+    s->phase = 3;
+    return MC3D_OK;
+}
+
+int mc3d_solver_post_substep(mc3d_solver s) {
+    if (int rc = stage_ready(s, 3, "postSubStep")) return rc;
+    int rc = s->prec == MC3D_FP64 ? stage_post<double>(s) : stage_post<float>(s);
+    if (rc) return rc;
+    s->phase = 4;
+    return MC3D_OK;
+}
+
+int mc3d_rk_update(mc3d_solver s, int scheme, int rk_step, int dual_step) {
+    if (int rc = stage_ready(s, 4, "updateConservedData")) return rc;
+    if (scheme != s->cfg.rk_type)
+        return fail(MC3D_ERR_CONFIG, "updateConservedData: the RK scheme differs from the solver's RKTYPE");
+    if (rk_step != s->cur_stage) return fail(MC3D_ERR_CONFIG, "updateConservedData: rkStep is not the current stage");
+    if (scheme == MC3D_LSLDDRK4 && dual_step != s->lsldd_half)
+        return fail(MC3D_ERR_CONFIG, "updateConservedData: LSLDDRK4 dual step " + std::to_string(dual_step) +
+                                         " where " + std::to_string(s->lsldd_half) + " is current");
+    int rc = s->prec == MC3D_FP64 ? stage_rk<double>(s, rk_step) : stage_rk<float>(s, rk_step);
+    if (rc) return rc;
+    s->phase = 5;
+    return MC3D_OK;
+}
+
+int mc3d_solver_update_data(mc3d_solver s, int rk_last) {
+    if (int rc = stage_ready(s, 5, "updateData")) return rc;
+    if ((rk_last != 0) != (s->cur_stage == s->cur_ns))
+        return fail(MC3D_ERR_CONFIG, "updateData: rkLast disagrees with the scheme's stage count");
+    int rc = s->prec == MC3D_FP64 ? stage_end<double>(s, s->cur_stage) : stage_end<float>(s, s->cur_stage);
+    if (rc) return rc;
+    s->phase = rk_last ? 6 : 1;
+    return MC3D_OK;
+}
+
+int mc3d_solver_post_step(mc3d_solver s) {
+    if (int rc = stage_ready(s, 6, "postStep")) return rc;
+    int rc = step_end(s);
+    if (rc) return rc;
+    s->phase = 0;
     return MC3D_OK;
 }
 
@@ -1854,6 +2017,219 @@ const char *mc3d_solver_timing_report(mc3d_solver s) {
     o += "}";
     s->report = o;
     return s->report.c_str();
+}
+
+}  // extern "C"
+
+// ---- SGS models on their own: the AbstractSGS drop-in ----
+// The object keeps an internal solver record that holds only what the SGS
+// kernels read: the model settings, the test-filter and averaging operators,
+// the work fields, and metrics whose J_ij factors are the identity (so the
+// kernels take the caller's physical gradients as they are) and whose J is
+// the caller's.
+struct mc3d_sgs_s {
+    mc3d_solver rec = nullptr;
+    cudaStream_t home = nullptr;   // the record's own stream, restored after each call
+    void *taukk_own = nullptr;
+};
+
+extern "C" {
+
+int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, int Nx, int Ny, int Nz,
+                    const int bc_types[3], const double dxi[3], const void *J, double Jc, int precision, int device,
+                    mc3d_sgs *out) {
+    if (!out || !bc_types || !dxi) return fail(MC3D_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (model != MC3D_VREMAN && model != MC3D_DSM) return fail(MC3D_ERR_CONFIG, "model must be VREMAN or DSM");
+    if (averaging < MC3D_AVG_NONE || averaging > MC3D_AVG_GLOBAL) return fail(MC3D_ERR_CONFIG, "unknown LESAVERAGING");
+    if (model == MC3D_DSM && test_filter != 1 && test_filter != 2)
+        return fail(MC3D_ERR_CONFIG, "DSMTESTFILTER must be 1 or 2");
+    if (precision != MC3D_FP64 && precision != MC3D_FP32BULK) return fail(MC3D_ERR_CONFIG, "bad precision");
+    if (Nx <= 10 || Ny <= 10 || Nz <= 10)
+        return fail(MC3D_ERR_CONFIG, "Number of grid points in any direction must be greater than 10");
+    for (int d = 0; d < 3; d++)
+        if (!(dxi[d] > 0)) return fail(MC3D_ERR_ARG, "dxi must be positive");
+    if (!J && !(Jc != 0.0)) return fail(MC3D_ERR_ARG, "J: a field or a nonzero constant");
+    MC3D_CUDA_TRY(cudaSetDevice(device));
+    mc3d_sgs o = new mc3d_sgs_s();
+    mc3d_solver s = new mc3d_solver_s();
+    o->rec = s;
+    mc3d_config_default(&s->cfg);
+    s->cfg.Nx = Nx;
+    s->cfg.Ny = Ny;
+    s->cfg.Nz = Nz;
+    s->cfg.les_model = model;
+    s->cfg.les_averaging = averaging;
+    s->cfg.dsm_test_filter = test_filter;
+    s->cfg.dsm_use_taukk = use_taukk != 0;
+    s->cfg.precision = precision;
+    for (int d = 0; d < 3; d++) s->cfg.bc_type[d] = bc_types[d];
+    s->device = device;
+    s->prec = precision;
+    s->g = Grid3{Nx, Ny, Nz};
+    for (int d = 0; d < 3; d++) s->dxi[d] = dxi[d];
+    int rc = MC3D_OK;
+    cudaError_t e = device_stream(device, &s->stream);
+    if (e != cudaSuccess) rc = fail(MC3D_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    o->home = s->stream;
+    const int N[3] = {Nx, Ny, Nz};
+    try {
+        for (int d = 0; d < 3 && !rc; d++) {
+            if (model == MC3D_VREMAN) {
+                // VremanSGS averages with Compact10 filters of alpha -0.49 (src/VremanSGS.hpp:38-40)
+                rc = upload_line_op(build_filter_op(MC3D_COMPACT10, -0.49, bc_types[d], N[d]), precision, s->vop[d]);
+            } else {
+                // DSMTESTFILTER 1 -> Pade, 2 -> explicit (src/DSMSGS.hpp:57-67)
+                rc = upload_line_op(build_testfilter_op(test_filter == 1 ? MC3D_TESTFILTER_PADE : MC3D_TESTFILTER_EXP,
+                                                        bc_types[d], N[d]),
+                                    precision, s->top[d]);
+            }
+        }
+    } catch (const std::exception &ex) {
+        rc = fail(MC3D_ERR_CONFIG, ex.what());
+    }
+    const size_t n = (size_t)s->g.n(), rb = precision == MC3D_FP64 ? 8 : 4;
+    for (int v = 0; v < 5 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
+    if (!rc) rc = salloc(s, (void **)&s->avg_scratch, AVG_SCRATCH * sizeof(double));
+    if (model == MC3D_VREMAN && !rc) rc = salloc(s, &s->tA[0], n * rb);
+    if (model == MC3D_DSM) {
+        for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dA[i], n * rb);
+        for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dB[i], n * rb);
+        if (!rc) rc = salloc(s, &s->smag, n * rb);
+        if (!rc) rc = salloc(s, &o->taukk_own, n * rb);
+    }
+    // metrics: J_ij = identity, J from the caller
+    s->const_met = J == nullptr;
+    for (int c = 0; c < 10; c++) s->met_c[c] = 0.0;
+    s->met_c[0] = J ? 1.0 : Jc;
+    s->met_c[1] = s->met_c[5] = s->met_c[9] = 1.0;
+    if (J && !rc) {
+        void *ones = nullptr, *zeros = nullptr;
+        rc = salloc(s, &zeros, n * rb);
+        if (!rc) rc = salloc(s, &ones, n * rb);
+        if (!rc) {
+            std::vector<char> h(n * rb);
+            if (precision == MC3D_FP64) std::fill((double *)h.data(), (double *)h.data() + n, 1.0);
+            else std::fill((float *)h.data(), (float *)h.data() + n, 1.0f);
+            e = cudaMemcpy(ones, h.data(), n * rb, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) rc = fail(MC3D_ERR_CUDA, cudaGetErrorString(e));
+        }
+        for (int c = 1; c < 10 && !rc; c++) s->metR[c] = (c == 1 || c == 5 || c == 9) ? ones : zeros;
+        s->metR[0] = const_cast<void *>(J);
+    }
+    if (!rc) {
+        e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) rc = fail(MC3D_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc) {
+        mc3d_sgs_destroy(o);
+        return rc;
+    }
+    *out = o;
+    return MC3D_OK;
+}
+
+int mc3d_sgs_destroy(mc3d_sgs o) {
+    if (!o) return MC3D_OK;
+    if (o->rec) {
+        o->rec->stream = o->home;
+        mc3d_solver_destroy(o->rec);
+    }
+    delete o;
+    return MC3D_OK;
+}
+
+}  // extern "C"
+
+template <typename R>
+static int sgs_viscosity_t(mc3d_sgs o, const void *const gradU[9], const double *const q[5], void *mu_sgs) {
+    mc3d_solver s = o->rec;
+    int rc;
+    R *pr[5];
+    for (int v = 0; v < 5; v++) pr[v] = (R *)s->prim[v];
+    if ((rc = launch_to_real<R>(s->g, q, pr, s->stream))) return rc;
+    const R *dd[12];
+    for (int i = 0; i < 12; i++) dd[i] = (const R *)gradU[i < 9 ? i : 0];
+    FluxParams fp{};
+    for (int d = 0; d < 3; d++) fp.dxi[d] = s->dxi[d];
+    const R *prc[5] = {pr[0], pr[1], pr[2], pr[3], pr[4]};
+    if ((rc = launch_vreman<R>(s->g, prc, dd, metrics_of<R>(s), fp, (R *)mu_sgs, s->stream))) return rc;
+    void *a[1] = {mu_sgs}, *t1[1] = {s->tA[0]}, *res[1];
+    if ((rc = sgs_average<R>(s, 1, a, t1, s->vop, res))) return rc;
+    if (res[0] != mu_sgs)
+        MC3D_CUDA_TRY(cudaMemcpyAsync(mu_sgs, res[0], (size_t)s->g.n() * sizeof(R), cudaMemcpyDeviceToDevice,
+                                      s->stream));
+    return MC3D_OK;
+}
+
+template <typename R>
+static int sgs_mu_taukk_t(mc3d_sgs o, const void *const gradU[9], const double *const q[5], void *mu_sgs,
+                          void *taukk) {
+    mc3d_solver s = o->rec;
+    for (int i = 0; i < 9; i++) s->der[i] = const_cast<void *>(gradU[i]);
+    s->mu_sgs = mu_sgs;
+    s->taukk = taukk ? taukk : o->taukk_own;
+    s->cons_mask = 0;
+    // (the kernel also forms the temperature of p - tau_kk / 2, which the
+    // solver uses; here it lands in a work field)
+    return dsm_mu_taukk<R>(s, const_cast<double *const *>(q), metrics_of<R>(s));
+}
+
+template <typename R>
+static int sgs_ksgs_t(mc3d_sgs o, const void *const gradT[3], const double *const q[5], const void *T, void *k_sgs) {
+    mc3d_solver s = o->rec;
+    for (int i = 0; i < 3; i++) s->der[9 + i] = const_cast<void *>(gradT[i]);
+    void *keep = s->prim[4];
+    s->prim[4] = const_cast<void *>(T);
+    s->ksgs = k_sgs;
+    int rc = dsm_ksgs<R>(s, const_cast<double *const *>(q), metrics_of<R>(s));
+    s->prim[4] = keep;
+    return rc;
+}
+
+extern "C" {
+
+static int sgs_call(mc3d_sgs o, void *stream) {
+    if (!o) return fail(MC3D_ERR_ARG, "null argument");
+    MC3D_CUDA_TRY(cudaSetDevice(o->rec->device));
+    o->rec->stream = (cudaStream_t)stream;
+    return MC3D_OK;
+}
+
+int mc3d_sgs_get_viscosity(mc3d_sgs o, const void *const gradU[9], const double *const q[5], void *mu_sgs,
+                           void *stream) {
+    if (int rc = sgs_call(o, stream)) return rc;
+    if (!gradU || !q || !mu_sgs) return fail(MC3D_ERR_ARG, "null argument");
+    int rc = MC3D_OK;
+    if (o->rec->cfg.les_model == MC3D_VREMAN)
+        rc = o->rec->prec == MC3D_FP64 ? sgs_viscosity_t<double>(o, gradU, q, mu_sgs)
+                                       : sgs_viscosity_t<float>(o, gradU, q, mu_sgs);
+    o->rec->stream = o->home;
+    return rc;
+}
+
+int mc3d_sgs_calc_mu_taukk(mc3d_sgs o, const void *const gradU[9], const double *const q[5], void *mu_sgs,
+                           void *taukk, void *stream) {
+    if (int rc = sgs_call(o, stream)) return rc;
+    if (!gradU || !q || !mu_sgs) return fail(MC3D_ERR_ARG, "null argument");
+    int rc = MC3D_OK;
+    if (o->rec->cfg.les_model == MC3D_DSM)
+        rc = o->rec->prec == MC3D_FP64 ? sgs_mu_taukk_t<double>(o, gradU, q, mu_sgs, taukk)
+                                       : sgs_mu_taukk_t<float>(o, gradU, q, mu_sgs, taukk);
+    o->rec->stream = o->home;
+    return rc;
+}
+
+int mc3d_sgs_calc_ksgs(mc3d_sgs o, const void *const gradT[3], const double *const q[5], const void *T,
+                       void *k_sgs, void *stream) {
+    if (int rc = sgs_call(o, stream)) return rc;
+    if (!gradT || !q || !T || !k_sgs) return fail(MC3D_ERR_ARG, "null argument");
+    int rc = MC3D_OK;
+    if (o->rec->cfg.les_model == MC3D_DSM)
+        rc = o->rec->prec == MC3D_FP64 ? sgs_ksgs_t<double>(o, gradT, q, T, k_sgs)
+                                       : sgs_ksgs_t<float>(o, gradT, q, T, k_sgs);
+    o->rec->stream = o->home;
+    return rc;
 }
 
 int mc3d_solver_sync(mc3d_solver s) {

@@ -371,3 +371,67 @@ def test_fp32_line_solves_stay_bit_stable_under_overlapping_sweeps():
             for f in range(5):
                 assert torch.equal(ya[d][f], ref[d][f]), (rnd, d, f)
     assert m.tma_wait_timeouts(0) == 0
+
+
+def test_stage_by_stage_calls_equal_the_step():
+    """The stage-level calls in the reference's RK loop order (preStep, then
+    per stage preSubStep, solveEqnSet, postSubStep, updateConservedData,
+    updateData, then postStep) give mc3d_solver_step's state bit for bit, over
+    both LSLDDRK4 halves; a call out of order is refused and changes nothing."""
+    import ctypes as C
+    from mpi_3dcompact_b200 import _native as N
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    lib = N.host_lib()
+    n = 32
+    ic = hit_initial_condition(n, k0=4.0, seed=12, mt=0.3)
+    a, b = _hit_solver(n, m.FP32BULK, ic), _hit_solver(n, m.FP32BULK, ic)
+    a.step(3)
+    h = b._h
+    assert lib.mc3d_solver_pre_substep(h, 1) == 1          # before preStep: refused
+    for step in range(3):
+        N.check(lib.mc3d_solver_pre_step(h))
+        ns = C.c_int()
+        N.check(lib.mc3d_solver_stage_count(h, C.byref(ns)))
+        assert ns.value == (5 if step % 2 == 0 else 6)
+        for st in range(1, ns.value + 1):
+            N.check(lib.mc3d_solver_pre_substep(h, st))
+            N.check(lib.mc3d_solver_solve_eqn_set(h))
+            N.check(lib.mc3d_solver_post_substep(h))
+            assert lib.mc3d_rk_update(h, m.LSLDDRK4, st, 2 if step % 2 == 0 else 1) == 1   # wrong half
+            N.check(lib.mc3d_rk_update(h, m.LSLDDRK4, st, 1 if step % 2 == 0 else 2))
+            N.check(lib.mc3d_solver_update_data(h, int(st == ns.value)))
+        N.check(lib.mc3d_solver_post_step(h))
+    qa, qb = a.conserved(), b.conserved()
+    for i in range(5):
+        assert np.array_equal(qa[i], qb[i]), i
+    assert a.info() == b.info()
+
+
+@pytest.mark.parametrize("prec,tol", [(m.FP64, 1e-13), (m.FP32BULK, 3e-6)])
+@pytest.mark.parametrize("scheme", ["PADE6", "PENTA10", "CD2"])
+def test_tpb_derivative_matches_oracle(scheme, prec, tol):
+    """calc1stDerivField_TPB with caller ghost planes (mc3d_op_apply_tpb) along
+    each direction against the oracle's restatement of the reference's TPB rows
+    (pinned through the metric fixtures)."""
+    import torch
+    cls = {"PADE6": m.Pade6, "PENTA10": m.Penta10, "CD2": m.CD2}[scheme]
+    rng = np.random.default_rng(3)
+    shape = (20, 24, 32)          # (Nz, Ny, Nx)
+    f = rng.standard_normal(shape)
+    dt = torch.float64 if prec == m.FP64 else torch.float32
+    G = 3 if scheme == "PENTA10" else 2
+    for d in range(3):
+        ax = 2 - d
+        nline = shape[ax]
+        pshape = tuple(s for a, s in enumerate(shape) if a != ax)
+        ghosts = [rng.standard_normal(pshape) for _ in range(2 * G)]   # Nm_G .. Nm_1, Np_1 .. Np_G
+        op = cls(shape, m.PERIODIC_SOLVE, d, precision=prec)
+        x = torch.tensor(f, dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        op.calc1stDerivField_TPB(x, y, *[torch.tensor(g, dtype=dt, device="cuda") for g in ghosts])
+        lines = np.moveaxis(f, ax, -1)
+        gm = np.stack([ghosts[G - mm] for mm in range(1, G + 1)], axis=-1)
+        gp = np.stack([ghosts[G + mm - 1] for mm in range(1, G + 1)], axis=-1)
+        ref = np.moveaxis(O._tpb_lines(lines, gm, gp, scheme, 1.0 / nline), -1, ax)
+        err = H.rel_max(y.double().cpu().numpy(), ref)
+        assert err <= tol, (scheme, d, err)
