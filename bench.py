@@ -409,6 +409,91 @@ def learned_sgs_block(args, local):
     }
 
 
+HBM_GRID, HBM_K0 = 1024, 8.0
+HBM_WORKLOAD = ("HBM-sizing: decaying HIT 1024^3 periodic box 2*pi, PENTA10, COMPACT8 alpha_f=0.45 every step, "
+                "LSLDDRK4, learned SGS closure (MLP, stages past the fallback fraction counted: no DSM fallback "
+                "with lean storage), FP32-bulk with FP64 state and 2N register, GPU.STORAGE=LEAN, k0=8, Mt=0.3, "
+                "Re_lambda~100, CFL 0.5")
+
+
+def hbm_sizing_run(args, local):
+    """the 1024^3 block held on one GPU by lean storage. The
+    initial field is made on the device (the reference generator's sequence,
+    cuFFT), moved to host memory to free the device for the solver, and
+    uploaded by set_initial_conditions. Device time of `steps` steps after
+    `warmup`, CUDA events on the solver stream; resident bytes from
+    cudaMemGetInfo around the solver's creation."""
+    import numpy as np
+    import torch
+
+    import mpi_3dcompact_b200 as m
+    from mpi_3dcompact_b200.hit_ic import hit_velocity_device
+
+    n = args.hbm_grid
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    u = hit_velocity_device(n, k0=HBM_K0, seed=1, device=dev)
+    scale = MT / math.sqrt(float(sum((c * c).mean() for c in u)))
+    # Taylor microscale of the scaled field (spectral d/dx of u on the 2*pi box)
+    k = torch.fft.rfftfreq(n, d=1.0 / n, device=dev).to(torch.float64)
+    du = torch.fft.irfft(1j * k * torch.fft.rfft(u[0] * scale, dim=2), n=n, dim=2)
+    up = scale * math.sqrt(float(sum((c * c).mean() for c in u)) / 3.0)
+    lam = math.sqrt(float(((u[0] * scale) ** 2).mean()) / float((du * du).mean()))
+    del du
+    mu = up * lam / RE_LAMBDA
+    host = [np.ones((n, n, n))]
+    for c in u:
+        host.append((c * scale).cpu().numpy())
+    host.append(np.full((n, n, n), 1.0 / 1.4))
+    del u, c
+    torch.cuda.empty_cache()
+    ic_s = time.perf_counter() - t0
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    s = m.CurvilinearCSolver(m.Options(grid=n, fd="PENTA10", filter="COMPACT8", alphaF=0.45, rk="LSLDDRK4",
+                                       les="MLP", mlp_fallback_frac=LES_MLP_FALLBACK, mu_ref=mu, cfl=0.5,
+                                       precision=m.FP32BULK, storage="LEAN"), device=local)
+    s.set_box_metrics(2 * math.pi)
+    mlp = m.MLPClosure(device=local)
+    mlp.load(MLP_WEIGHTS)
+    s.set_mlp(mlp)
+    torch.cuda.synchronize(dev)
+    resident = free0 - torch.cuda.mem_get_info(dev)[0]
+    s.set_initial_conditions(*host)
+    del host
+    s.step(args.warmup)
+    s.sync()
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st0 = s.info()["stages"]
+    fb0 = s.mlp_fallbacks()
+    s.set_timing(True)
+    e0.record(stream)
+    s.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    rep = s.timing_report()
+    s.set_timing(False)
+    stages = s.info()["stages"] - st0
+    ke, mass = s.integrals()
+    peak, peak_kind = hbm_peak()
+    sw = rep.get("sweep_linesolve", {})
+    roof = None
+    if sw:
+        achieved = sw["bytes"] / sw["launches"] / (sw["ms"] * 1e-3 / sw["launches"]) / 1e9
+        roof = {"bound": "hbm", "kernel": "sweep_linesolve", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "kernel_share": sw["ms"] / sum(v["ms"] for v in rep.values())}
+    total_bytes = sum(v["bytes"] for v in rep.values())
+    return {"workload": HBM_WORKLOAD, "grid": n, "metric": UNIT, "value": float(n) ** 3 * stages / (ms * 1e-3),
+            "ms_per_step": ms / args.steps, "steps": args.steps, "warmup": args.warmup, "stages_timed": stages,
+            "resident_device_bytes": int(resident), "resident_fp32_field_equivalents": resident / (4.0 * n ** 3),
+            "algorithmic_bytes_per_pt_stage": total_bytes / (float(n) ** 3 * stages),
+            "all_kernels_gbs": total_bytes / (sum(v["ms"] for v in rep.values()) * 1e-3) / 1e9,
+            "mlp_out_of_range_stages": s.mlp_fallbacks() - fb0, "mu_ref": mu, "initial_field_s": ic_s,
+            "finite": bool(math.isfinite(ke) and math.isfinite(mass)), "roofline": roof, "kernels": rep}
+
+
 def fp32_vs_fp64(m, make, nsteps):
     """FP32-bulk against the FP64 path from the same initial field after
     `nsteps` time steps (untimed): per-field relative L2 and max differences of
@@ -610,11 +695,27 @@ def main():
     ap.add_argument("--cyl-steps", type=int, default=5)
     ap.add_argument("--les-steps", type=int, default=LES_STEPS)
     ap.add_argument("--err-steps", type=int, default=ERR_STEPS)
+    ap.add_argument("--workload", choices=["hit256", "hbm1024"], default="hit256",
+                    help="hbm1024: the 1024^3 HBM-sizing configuration with lean storage")
+    ap.add_argument("--hbm-grid", type=int, default=HBM_GRID)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "hbm1024":
+        import torch
+        ws, rank, local = dist_env()
+        torch.cuda.set_device(local)
+        res = hbm_sizing_run(args, local)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": 1,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic (seeded HIT initial condition, k0=8, Mt=0.3)",
+                              "config": {"workload": res["workload"], "grid": res["grid"]},
+                              "roofline": res["roofline"], "hbm_sizing": res}), flush=True)
+        return 0
     return run_ours(args)
 
 

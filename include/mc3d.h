@@ -136,6 +136,20 @@ typedef struct mc3d_config {
      * which the reference leaves commented out in postStep (default 0). No key. */
     double sponge_avg_time, sponge_p_inf;
     int sponge_relax;
+    /* GPU.STORAGE = FULL | LEAN (default FULL; no key in the reference). LEAN
+     * holds the periodic-box time step in 19 work fields of the working
+     * precision and 10 FP64 fields of the block instead of about 60 (a 1024^3
+     * block on one 180 GB GPU): the 2N schemes update the stage state in
+     * place, k2 accumulates the flux divergence (with the momentum carry-over
+     * when REFERENCEQUIRKS is on), and everything along xi1 and xi2 runs in
+     * slabs of xi3-planes, so only the xi3-gradients and xi3-fluxes are full
+     * fields. For periodic blocks with constant metrics, LESMODEL NOMODEL,
+     * VREMAN (no averaging) or MLP (no DSM fallback: stages past
+     * MLPFALLBACKFRAC are counted and keep the clamped network), no
+     * sub-step filtering and no statistics. GPU.LEANSLAB (lean_slab):
+     * xi3-planes per slab (0: about 2^26 points). */
+    int lean_storage;
+    int lean_slab;
 } mc3d_config;
 
 /* ---- configuration ---- */

@@ -255,7 +255,7 @@ class Options:
                  les_avg="NONE", precision=FP64, reference_quirks=True, bc=(PERIODIC_SOLVE,) * 3,
                  dsm_test_filter=1, dsm_use_taukk=True, bc_kind=None, sponge=None, mlp_fallback_frac=1e-3,
                  periodic_disp=None, max_time_step=None, max_time=None, dump_step=None, stats=None,
-                 sponge_relax=None):
+                 sponge_relax=None, storage="FULL", lean_slab=0):
         c = N.Config()
         N.check(N.host_lib().mc3d_config_default(C.byref(c)))
         c.Nx, c.Ny, c.Nz = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
@@ -277,6 +277,8 @@ class Options:
         c.dsm_test_filter = int(dsm_test_filter)
         c.dsm_use_taukk = int(bool(dsm_use_taukk))
         c.mlp_fallback_frac = mlp_fallback_frac
+        c.lean_storage = {"FULL": 0, "LEAN": 1}[storage]
+        c.lean_slab = int(lean_slab)
         if max_time_step is not None:
             c.max_time_step = int(max_time_step)
         if max_time is not None:

@@ -54,7 +54,8 @@ class Config(C.Structure):
                 ("stats_avg_type", C.c_int), ("velocity_stats_from_restart", C.c_int),
                 ("thermo_stats_from_restart", C.c_int), ("velocity_stats_file", C.c_char * 512),
                 ("thermo_stats_file", C.c_char * 512), ("sponge_avg_time", C.c_double),
-                ("sponge_p_inf", C.c_double), ("sponge_relax", C.c_int)]
+                ("sponge_p_inf", C.c_double), ("sponge_relax", C.c_int), ("lean_storage", C.c_int),
+                ("lean_slab", C.c_int)]
 
 
 _lib = None

@@ -93,6 +93,8 @@ int mc3d_config_default(mc3d_config *c) {
     c->sponge_avg_time = 1.0;       // src/Options.hpp:321
     c->sponge_p_inf = 1.0 / 1.4;    // src/Options.hpp:322
     c->sponge_relax = 0;
+    c->lean_storage = 0;
+    c->lean_slab = 0;
     c->stats_avg_type = MC3D_AVG_NONE;
     c->velocity_stats_from_restart = c->thermo_stats_from_restart = 0;
     c->velocity_stats_file[0] = c->thermo_stats_file[0] = '\0';
@@ -133,7 +135,8 @@ const char *KNOWN_KEYS[] = {
     "RESTART.SPONGEAVGFILENAME", "STATS.VELOCITYSTATS", "STATS.THERMOSTATS", "STATS.VELOCITYSTATSFROMRESTART",
     "STATS.THERMOSTATSFROMRESTART", "STATS.VELOCITYSTATSFILENAME", "STATS.THERMOSTATSFILENAME",
     "STATS.STATSAVGTYPE", "STATS.INTERVAL", "LES.LESMODEL", "LES.LESAVERAGING", "LES.DSMTESTFILTER",
-    "LES.DSMUSETAUKK", "LES.DSMCOEFFRANGE", "LES.MLPFALLBACKFRAC", "GPU.PRECISION", "GPU.REFERENCEQUIRKS"};
+    "LES.DSMUSETAUKK", "LES.DSMCOEFFRANGE", "LES.MLPFALLBACKFRAC", "GPU.PRECISION", "GPU.REFERENCEQUIRKS",
+    "GPU.STORAGE", "GPU.LEANSLAB"};
 
 struct CfgError {
     std::string msg;
@@ -373,6 +376,8 @@ extern "C" int mc3d_config_from_ini(const char *path, mc3d_config *c) {
         // [GPU]
         if (ini.has("GPU.PRECISION"))
             c->precision = parse_enum(ini, "GPU.PRECISION", {{"FP64", MC3D_FP64}, {"FP32BULK", MC3D_FP32BULK}});
+        if (ini.has("GPU.STORAGE")) c->lean_storage = parse_enum(ini, "GPU.STORAGE", {{"FULL", 0}, {"LEAN", 1}});
+        if (ini.has("GPU.LEANSLAB")) c->lean_slab = std::stoi(ini.get("GPU.LEANSLAB"));
         if (ini.has("GPU.REFERENCEQUIRKS"))
             c->reference_quirks = parse_bool("REFERENCEQUIRKS", ini.get("GPU.REFERENCEQUIRKS"));
     } catch (const CfgError &e) {

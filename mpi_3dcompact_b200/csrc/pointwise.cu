@@ -645,7 +645,8 @@ __global__ void to_real_kernel(Grid3 g, Q5 src, K5<R> dst) {
     long long n = g.n();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) const_cast<R *>(dst.p[v])[i] = (R)src.p[v][i];
+        for (int v = 0; v < 5; v++)
+            if (dst.p[v]) const_cast<R *>(dst.p[v])[i] = (R)src.p[v][i];
     }
 }
 

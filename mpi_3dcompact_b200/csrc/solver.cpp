@@ -77,6 +77,10 @@ struct mc3d_solver_s {
     double st_vw = 0.0, st_tw = 0.0, st_prev = 0.0;
     double *hook_scratch = nullptr;   // block partials of the diagnostic reductions
     int lsldd_half = 1;
+    // GPU.STORAGE = LEAN: work arrays along xi1 / xi2 hold one slab of slab_nz
+    // xi3-planes; q2 is qk for the 2N schemes; k2 accumulates the divergence
+    bool lean = false;
+    int slab_nz = 0;
     // stage-level driving (mc3d_solver_pre_step .. mc3d_solver_post_step): the
     // last call made in the current time step, its stage, the step's stage
     // count, whether it filters, and the sponge faces relaxed before it
@@ -169,8 +173,20 @@ template <>
 const LineOpDev<double> &opdev<double>(const LineOpBuf &b) { return b.f64; }
 
 template <typename R>
+static int sweep_on(mc3d_solver s, const Grid3 &g, int dir, const LineOpBuf &op, int nf, const void *const *in,
+                    void *const *out, int epi, const void *const *aux, double *const *out64, bool filter, bool quirk);
+
+template <typename R>
 static int sweep(mc3d_solver s, int dir, const LineOpBuf &op, int nf, const void *const *in, void *const *out,
                  int epi, const void *const *aux, double *const *out64, bool filter) {
+    return sweep_on<R>(s, s->g, dir, op, nf, in, out, epi, aux, out64, filter, s->cfg.reference_quirks != 0);
+}
+
+// one batched line solve along dir over the block (or slab) g; `quirk` turns
+// on the momentum k2 carry-over of the k2-assembly epilogue
+template <typename R>
+static int sweep_on(mc3d_solver s, const Grid3 &g, int dir, const LineOpBuf &op, int nf, const void *const *in,
+                    void *const *out, int epi, const void *const *aux, double *const *out64, bool filter, bool quirk) {
     SweepBatch<R> b{};
     b.nf = nf;
     for (int f = 0; f < nf; f++) {
@@ -184,18 +200,18 @@ static int sweep(mc3d_solver s, int dir, const LineOpBuf &op, int nf, const void
     rf.dt = &s->ts->dt;
     rf.J = s->const_met ? nullptr : (const R *)s->metR[0];
     rf.Jc = (R)s->met_c[0];
-    rf.quirk = s->cfg.reference_quirks;
+    rf.quirk = quirk;
     s->launches++;
     // algorithmic bytes: every field read once and written once, plus the
     // epilogue's extra operands (partial RHS, previous k2, FP64 store)
     double per = 2.0 * sizeof(R);
     if (epi == EPI_SUB) per = 3.0 * sizeof(R);
     if (epi == EPI_STORE_F64) per = sizeof(R) + 8.0;
-    double bytes = per * nf * (double)s->g.n();
-    if (epi == EPI_RHS_FINAL) bytes = (3.0 * nf + (s->cfg.reference_quirks ? 3.0 : 0.0)) * sizeof(R) * (double)s->g.n();
+    double bytes = per * nf * (double)g.n();
+    if (epi == EPI_RHS_FINAL) bytes = (3.0 * nf + (quirk ? 3.0 : 0.0)) * sizeof(R) * (double)g.n();
     int rc = tic(s, KC_SWEEP, bytes);
     if (rc) return rc;
-    rc = launch_sweep<R>(dir, s->g, opdev<R>(op), b, epi, rf, s->cfg.bc_type, filter, s->stream);
+    rc = launch_sweep<R>(dir, g, opdev<R>(op), b, epi, rf, s->cfg.bc_type, filter, s->stream);
     if (rc) return rc;
     return toc(s);
 }
@@ -233,6 +249,40 @@ static int filter_state(mc3d_solver s, double *const in[5], double *const out[5]
     return sweep<R>(s, order[2], ops[order[2]], 5, s->tB, nullptr, EPI_STORE_F64, nullptr, out, true);
 }
 
+// filterConservedData with LEAN storage: one conserved field at a time through
+// two full work fields (the xi3-flux fields, free once k2 is assembled)
+template <typename R>
+static int filter_state_lean(mc3d_solver s, double *const in[5], double *const out[5], const int order[3]) {
+    int rc;
+    void *t0 = s->tA[0], *t1 = s->tB[0];
+    for (int v = 0; v < 5; v++) {
+        void *a[1], *b[1] = {t1};
+        if (s->prec == MC3D_FP64) {
+            a[0] = in[v];
+        } else {
+            const double *src[5] = {in[v], in[v], in[v], in[v], in[v]};
+            R *dst[5] = {(R *)t0, nullptr, nullptr, nullptr, nullptr};
+            s->launches++;
+            if ((rc = tic(s, KC_TOREAL, (8.0 + sizeof(R)) * (double)s->g.n()))) return rc;
+            if ((rc = launch_to_real<R>(s->g, src, dst, s->stream))) return rc;
+            if ((rc = toc(s))) return rc;
+            a[0] = t0;
+        }
+        if ((rc = sweep<R>(s, order[0], s->fop[order[0]], 1, a, b, EPI_STORE, nullptr, nullptr, true))) return rc;
+        void *c[1] = {t0};
+        if ((rc = sweep<R>(s, order[1], s->fop[order[1]], 1, b, c, EPI_STORE, nullptr, nullptr, true))) return rc;
+        if (s->prec == MC3D_FP64) {
+            void *o[1] = {out[v]};
+            if ((rc = sweep<R>(s, order[2], s->fop[order[2]], 1, c, o, EPI_STORE, nullptr, nullptr, true))) return rc;
+        } else {
+            double *o64[1] = {out[v]};
+            if ((rc = sweep<R>(s, order[2], s->fop[order[2]], 1, c, nullptr, EPI_STORE_F64, nullptr, o64, true)))
+                return rc;
+        }
+    }
+    return MC3D_OK;
+}
+
 template <typename R>
 static int filter_conserved(mc3d_solver s, bool last) {
     double **in = last ? s->q2 : s->qk;
@@ -244,6 +294,7 @@ static int filter_conserved(mc3d_solver s, bool last) {
         if (r == 1) { order[0] = 1; order[1] = 2; order[2] = 0; }
         else if (r == 2) { order[0] = 2; order[1] = 0; order[2] = 1; }
         else { order[0] = 0; order[1] = 1; order[2] = 2; }
+        if (s->lean) return filter_state_lean<R>(s, in, out, order);
         return filter_state<R>(s, in, out, s->fop, order);
     }
     if (last) {
@@ -551,10 +602,103 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
     return MC3D_OK;
 }
 
+// preStepDerivatives and the first two divergence sweeps with LEAN storage.
+// The xi3-derivatives of U, V, W, T are formed over the whole block; then,
+// slab by slab of xi3-planes, the xi1- and xi2-derivatives, the SGS closure,
+// the 15 fluxes (the xi3-fluxes into their full fields) and the xi1- and
+// xi2-divergences, accumulated straight into k2. With the momentum carry-over
+// (Core.cpp:839,872,904) the momentum k2 starts from its previous value, so
+// k2 ends as (k2_prev + RHS) dt J there and RHS dt J elsewhere, as in
+// solveXMomentum etc.
+template <typename R>
+static int stage_rhs_lean(mc3d_solver s, double *const *qP) {
+    if (!s->const_met) return fail(MC3D_ERR_CONFIG, "GPU.STORAGE = LEAN needs constant metrics (a uniform box)");
+    int rc;
+    const Grid3 G = s->g;
+    const size_t plane = (size_t)G.Nx * G.Ny;
+    {
+        void *out[4] = {s->der[2], s->der[5], s->der[8], s->der[11]};
+        if ((rc = sweep<R>(s, 2, s->dop[2], 4, s->prim + 1, out, EPI_STORE, nullptr, nullptr, false))) return rc;
+    }
+    const Metrics<R> m = metrics_of<R>(s);
+    FluxParams fp{};
+    fp.mu_ref = s->cfg.mu_ref;
+    for (int i = 0; i < 3; i++) fp.dxi[i] = s->dxi[i];
+    fp.pr_t = 0.9;   // src/CurvilinearCSolver.hpp:232
+    const bool mlp = s->cfg.les_model == MC3D_MLPSGS;
+    fp.les = s->cfg.les_model == MC3D_VREMAN ? 1 : (mlp ? 3 : 0);
+    if (mlp) MC3D_CUDA_TRY(cudaMemsetAsync(s->mlp_flag, 0, sizeof(int), s->stream));
+    const bool quirk = s->cfg.reference_quirks != 0;
+    for (int k0 = 0; k0 < G.Nz; k0 += s->slab_nz) {
+        const int nz = std::min(s->slab_nz, G.Nz - k0);
+        const Grid3 gs{G.Nx, G.Ny, nz};
+        const size_t off = (size_t)k0 * plane;
+        void *pr[5], *k2s[5];
+        for (int v = 0; v < 5; v++) {
+            pr[v] = (R *)s->prim[v] + off;
+            k2s[v] = (R *)s->k2[v] + off;
+            fp.cons[v] = qP[v] + off;
+        }
+        for (int d = 0; d < 2; d++) {
+            void *out[4] = {s->der[0 + d], s->der[3 + d], s->der[6 + d], s->der[9 + d]};
+            if ((rc = sweep_on<R>(s, gs, d, s->dop[d], 4, pr + 1, out, EPI_STORE, nullptr, nullptr, false, quirk)))
+                return rc;
+        }
+        const R *dd[12], *prc[5];
+        for (int var = 0; var < 4; var++) {
+            dd[3 * var + 0] = (const R *)s->der[3 * var + 0];
+            dd[3 * var + 1] = (const R *)s->der[3 * var + 1];
+            dd[3 * var + 2] = (const R *)s->der[3 * var + 2] + off;
+        }
+        for (int v = 0; v < 5; v++) prc[v] = (const R *)pr[v];
+        if (mlp) {
+            s->launches++;
+            if ((rc = tic(s, KC_SGS, (14.0 + 2.0) * sizeof(R) * (double)gs.n()))) return rc;
+            if ((rc = launch_sgs_mlp<R>(gs, prc[0], prc[4], dd, m, s->dxi[0] * s->dxi[1] * s->dxi[2], s->cfg.mu_ref,
+                                        *mlp_dev(s->mlp), (R *)s->mu_sgs, (R *)s->ksgs, s->mlp_flag, s->stream)))
+                return rc;
+            if ((rc = toc(s))) return rc;
+        }
+        R *F[15];
+        for (int i = 0; i < 10; i++) F[i] = (R *)s->flux[i];
+        for (int i = 10; i < 15; i++) F[i] = (R *)s->flux[i] + off;
+        s->launches++;
+        {
+            const double b = (5.0 + 12.0 + 15.0) * sizeof(R) + (mlp ? 2.0 * sizeof(R) : 0.0);
+            if ((rc = tic(s, KC_FLUX, b * (double)gs.n()))) return rc;
+        }
+        if ((rc = launch_flux<R>(gs, prc, dd, m, fp, (const R *)s->mu_sgs, (const R *)s->ksgs, nullptr, nullptr, F,
+                                 s->stream)))
+            return rc;
+        if ((rc = toc(s))) return rc;
+        void *fx[5] = {F[0], F[1], F[2], F[3], F[4]}, *fy[5] = {F[5], F[6], F[7], F[8], F[9]};
+        if (quirk) {
+            void *ince[2] = {fx[0], fx[4]}, *outce[2] = {k2s[0], k2s[4]};
+            if ((rc = sweep_on<R>(s, gs, 0, s->dop[0], 2, ince, outce, EPI_STORE_NEG, nullptr, nullptr, false, quirk)))
+                return rc;
+            if ((rc = sweep_on<R>(s, gs, 0, s->dop[0], 3, fx + 1, k2s + 1, EPI_SUB, nullptr, nullptr, false, quirk)))
+                return rc;
+        } else if ((rc = sweep_on<R>(s, gs, 0, s->dop[0], 5, fx, k2s, EPI_STORE_NEG, nullptr, nullptr, false, quirk))) {
+            return rc;
+        }
+        if ((rc = sweep_on<R>(s, gs, 1, s->dop[1], 5, fy, k2s, EPI_SUB, nullptr, nullptr, false, quirk))) return rc;
+    }
+    if (mlp) {
+        // no DSM fallback with LEAN storage: such stages are counted
+        MC3D_CUDA_TRY(cudaMemcpyAsync(s->mlp_flag_host, s->mlp_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        if ((double)*s->mlp_flag_host > s->cfg.mlp_fallback_frac * (double)s->g.n()) s->mlp_fallbacks++;
+    }
+    return MC3D_OK;
+}
+
 // solveContinuity .. solveEnergy (Core.cpp:790-947): the third divergence
-// sweep assembles k2 = dt J (partial RHS - dH/dxi3) in its epilogue
+// sweep assembles k2 = dt J (partial RHS - dH/dxi3) in its epilogue (LEAN:
+// k2 holds the partial RHS itself, and the assembly runs in place)
 template <typename R>
 static int stage_solve(mc3d_solver s) {
+    if (s->lean)
+        return sweep_on<R>(s, s->g, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->k2, nullptr, false, false);
     return sweep<R>(s, 2, s->dop[2], 5, s->flux + 10, s->k2, EPI_RHS_FINAL, s->rhs, nullptr, false);
 }
 
@@ -639,7 +783,7 @@ static int stage_begin(mc3d_solver s, int st) {
         if ((rc = primitives<R>(s, s->qk))) return rc;
     if ((rc = wall_prestep<R>(s, st == 1 ? s->q1 : s->qk))) return rc;
     s->cons_mask = st == 1 ? s->cur_relaxed : 0;
-    rc = stage_rhs<R>(s, st == 1 ? s->q1 : s->qk);
+    rc = s->lean ? stage_rhs_lean<R>(s, st == 1 ? s->q1 : s->qk) : stage_rhs<R>(s, st == 1 ? s->q1 : s->qk);
     s->cons_mask = 0;
     return rc;
 }
@@ -674,7 +818,7 @@ static int stage_rk(mc3d_solver s, int st) {
     }
     const bool fuse_prims = st < ns && !s->cfg.substep_filtering;
     // last stage of a filtered step (FP32 path): the filter's working copy
-    const bool copy_final = st == ns && s->cur_filter_now && s->prec != MC3D_FP64;
+    const bool copy_final = !s->lean && st == ns && s->cur_filter_now && s->prec != MC3D_FP64;
     if (copy_final)
         for (int v = 0; v < 5; v++) pw[v] = (R *)s->tC[v];
     s->launches++;
@@ -772,6 +916,19 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         if (c.bc_kind[f] == MC3D_BC_INLET)
             return fail(MC3D_ERR_CONFIG, "INLET faces have no boundary treatment in the reference solver");
     if (c.filter_step < 1) return fail(MC3D_ERR_CONFIG, "FILTERSTEP must be >= 1");
+    if (c.lean_storage) {
+        for (int d = 0; d < 3; d++)
+            if (c.bc_type[d] != MC3D_PERIODIC_SOLVE)
+                return fail(MC3D_ERR_CONFIG, "GPU.STORAGE = LEAN needs periodic directions");
+        for (int f = 0; f < 6; f++)
+            if (is_wall_kind(c.bc_kind[f]) || c.bc_kind[f] == MC3D_BC_SPONGE)
+                return fail(MC3D_ERR_CONFIG, "GPU.STORAGE = LEAN has no walls or sponges");
+        if (c.les_model == MC3D_DSM || (c.les_model == MC3D_VREMAN && c.les_averaging != MC3D_AVG_NONE))
+            return fail(MC3D_ERR_CONFIG, "GPU.STORAGE = LEAN takes NOMODEL, VREMAN without averaging or MLP");
+        if (c.substep_filtering || c.velocity_stats || c.thermo_stats || c.sponge_relax)
+            return fail(MC3D_ERR_CONFIG, "GPU.STORAGE = LEAN has no sub-step filtering, statistics or relaxation");
+        if (c.lean_slab < 0) return fail(MC3D_ERR_CONFIG, "GPU.LEANSLAB must be >= 0");
+    }
     MC3D_CUDA_TRY(cudaSetDevice(device));
     mc3d_solver s = new mc3d_solver_s();
     s->cfg = c;
@@ -813,7 +970,43 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
     }
     size_t n = (size_t)s->g.n();
     size_t rb = c.precision == MC3D_FP64 ? sizeof(double) : sizeof(float);
-    for (int v = 0; v < 5 && !rc; v++) {
+    s->lean = c.lean_storage != 0;
+    if (s->lean) {
+        const long long plane = (long long)c.Nx * c.Ny;
+        s->slab_nz = c.lean_slab > 0 ? std::min(c.lean_slab, c.Nz)
+                                     : (int)std::max(1LL, std::min((long long)c.Nz, (1LL << 26) / plane));
+        const size_t ns = (size_t)plane * s->slab_nz;
+        const bool two_n = c.rk_type == MC3D_KENRK4 || c.rk_type == MC3D_LSLDDRK4;
+        for (int v = 0; v < 5 && !rc; v++) {
+            rc = rc ? rc : salloc(s, (void **)&s->q1[v], n * sizeof(double));
+            rc = rc ? rc : salloc(s, (void **)&s->qk[v], n * sizeof(double));
+            if (two_n) s->q2[v] = s->qk[v];   // the 2N schemes write the final state over the stage state
+            else rc = rc ? rc : salloc(s, (void **)&s->q2[v], n * sizeof(double));
+            rc = rc ? rc : salloc(s, &s->k2[v], n * rb);
+            rc = rc ? rc : salloc(s, &s->prim[v], n * rb);
+        }
+        for (int var = 0; var < 4 && !rc; var++) {
+            rc = salloc(s, &s->der[3 * var + 0], ns * rb);
+            if (!rc) rc = salloc(s, &s->der[3 * var + 1], ns * rb);
+            if (!rc) rc = salloc(s, &s->der[3 * var + 2], n * rb);
+        }
+        for (int i = 0; i < 15 && !rc; i++) rc = salloc(s, &s->flux[i], (i < 10 ? ns : n) * rb);
+        if (!rc) {
+            // the filter's two work fields are the xi3-flux fields
+            s->tA[0] = s->flux[10];
+            s->tB[0] = s->flux[11];
+        }
+        if (c.les_model == MC3D_MLPSGS) {
+            if (!rc) rc = salloc(s, &s->mu_sgs, ns * rb);
+            if (!rc) rc = salloc(s, &s->ksgs, ns * rb);
+            if (!rc) rc = salloc(s, (void **)&s->mlp_flag, sizeof(int));
+            if (!rc) {
+                cudaError_t he = cudaMallocHost((void **)&s->mlp_flag_host, sizeof(int));
+                if (he != cudaSuccess) rc = fail(MC3D_ERR_OOM, "cudaMallocHost");
+            }
+        }
+    }
+    for (int v = 0; v < 5 && !rc && !s->lean; v++) {
         rc = rc ? rc : salloc(s, (void **)&s->q1[v], n * sizeof(double));
         rc = rc ? rc : salloc(s, (void **)&s->qk[v], n * sizeof(double));
         rc = rc ? rc : salloc(s, (void **)&s->q2[v], n * sizeof(double));
@@ -823,23 +1016,23 @@ int mc3d_solver_create(const mc3d_config *cfg, int device, mc3d_solver *out) {
         rc = rc ? rc : salloc(s, &s->tB[v], n * rb);
         if (!rc && c.precision != MC3D_FP64) rc = salloc(s, &s->tC[v], n * rb);
     }
-    for (int v = 0; v < 5 && !rc; v++) rc = salloc(s, &s->prim[v], n * rb);
-    for (int v = 0; v < 12 && !rc; v++) rc = salloc(s, &s->der[v], n * rb);
-    for (int v = 0; v < 15 && !rc; v++) rc = salloc(s, &s->flux[v], n * rb);
-    if (!rc && c.les_model != MC3D_NOMODEL) rc = salloc(s, &s->mu_sgs, n * rb);
+    for (int v = 0; v < 5 && !rc && !s->lean; v++) rc = salloc(s, &s->prim[v], n * rb);
+    for (int v = 0; v < 12 && !rc && !s->lean; v++) rc = salloc(s, &s->der[v], n * rb);
+    for (int v = 0; v < 15 && !rc && !s->lean; v++) rc = salloc(s, &s->flux[v], n * rb);
+    if (!rc && !s->lean && c.les_model != MC3D_NOMODEL) rc = salloc(s, &s->mu_sgs, n * rb);
     if (c.velocity_stats)
         for (int k = 0; k < 9 && !rc; k++) rc = salloc(s, (void **)&s->stv[k], n * sizeof(double));
     if (c.thermo_stats)
         for (int k = 0; k < 6 && !rc; k++) rc = salloc(s, (void **)&s->stt[k], n * sizeof(double));
     s->st_prev = c.time0;   // Stats takes the solver's time at construction (src/Stats.hpp:58)
-    if (c.les_model == MC3D_MLPSGS) {
+    if (c.les_model == MC3D_MLPSGS && !s->lean) {
         if (!rc) rc = salloc(s, (void **)&s->mlp_flag, sizeof(int));
         if (!rc) {
             cudaError_t he = cudaMallocHost((void **)&s->mlp_flag_host, sizeof(int));
             if (he != cudaSuccess) rc = fail(MC3D_ERR_OOM, "cudaMallocHost");
         }
     }
-    if (c.les_model == MC3D_DSM || c.les_model == MC3D_MLPSGS) {
+    if ((c.les_model == MC3D_DSM || c.les_model == MC3D_MLPSGS) && !s->lean) {
         for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dA[i], n * rb);
         for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dB[i], n * rb);
         if (!rc) rc = salloc(s, &s->smag, n * rb);
@@ -1463,6 +1656,7 @@ extern "C" {
 int mc3d_solver_turbdata(mc3d_solver s, double k0, double out[11]) {
     if (!s || !out) return fail(MC3D_ERR_ARG, "null argument");
     if (!s->initialized) return fail(MC3D_ERR_CONFIG, "no state");
+    if (s->lean) return fail(MC3D_ERR_CONFIG, "turbdata needs the full-field gradients of GPU.STORAGE = FULL");
     MC3D_CUDA_TRY(cudaSetDevice(s->device));
     return s->prec == MC3D_FP64 ? mc3d::turbdata_impl<double>(s, k0, out) : mc3d::turbdata_impl<float>(s, k0, out);
 }

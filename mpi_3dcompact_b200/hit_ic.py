@@ -137,6 +137,103 @@ def hit_velocity(n: int, k0: float = 4.0, seed: int = 1):
     return out
 
 
+def _lcg_torch(torch, x0: int, a: int, c: int, m: int, n: int, device):
+    """x_1..x_n of x_{k+1} = (a x_k + c) mod m on `device` (as _lcg)."""
+    out = torch.empty(n, dtype=torch.int64, device=device)
+    out[0] = (a * x0 + c) % m
+    A, Cc, filled = a, c, 1
+    while filled < n:
+        take = min(filled, n - filled)
+        out[filled:filled + take] = (A * out[:take] + Cc) % m
+        Cc = (A * Cc + Cc) % m
+        A = (A * A) % m
+        filled += take
+    return out
+
+
+def _vec_torch(torch, g: _Gen, n: int, device):
+    """_Gen.vec on `device`: the same sequence, state updated the same way."""
+    ix1 = _lcg_torch(torch, g.ix1, _IA1, _IC1, _M1, n, device)
+    ix2 = _lcg_torch(torch, g.ix2, _IA2, _IC2, _M2, n, device)
+    ix3 = _lcg_torch(torch, g.ix3, _IA3, _IC3, _M3, n, device)
+    slot = (97 * ix3) // _M3 % 97
+    val = torch.clamp((ix1.double() + ix2.double() * _RM2) * _RM1, 0.0, 1.0)
+    last_state = (int(ix1[-1].item()), int(ix2[-1].item()), int(ix3[-1].item()))
+    del ix1, ix2, ix3
+    ss, order = torch.sort(slot, stable=True)
+    same = ss[1:] == ss[:-1]
+    prev = torch.full((n,), -1, dtype=torch.int64, device=device)
+    prev[order[1:][same]] = order[:-1][same]
+    table = torch.tensor(g.r, dtype=torch.float64, device=device)
+    out = torch.where(prev >= 0, val[prev.clamp(min=0)], table[slot])
+    last = torch.ones(n, dtype=torch.bool, device=device)
+    last[:-1] = ~same
+    table[ss[last]] = val[order[last]]
+    g.r = table.cpu().tolist()
+    g.ix1, g.ix2, g.ix3 = last_state
+    return out
+
+
+def hit_velocity_device(n: int, k0: float = 4.0, seed: int = 1, device="cuda"):
+    """hit_velocity on a torch device (the same generator sequence, spectrum,
+    solenoidal construction and symmetries; cuFFT for the c2r transform, so
+    the field differs from the numpy one by FFT rounding only). Returns three
+    float64 device tensors (n, n, n); peak device memory about 6 complex
+    half-spectra (n * n * (n/2 + 1) * 16 bytes each)."""
+    import torch
+    if n % 2:
+        raise ValueError("n must be even (generate_init_hit.f90:150-153)")
+    kx_max = n // 2 + 1
+    shape_f = (n, n, kx_max)
+    g = _Gen(seed)
+    cnt = kx_max * n * n
+    phis = [2.0 * math.pi * (_vec_torch(torch, g, cnt, device).reshape(shape_f) - 0.5) for _ in range(3)]
+    kmin = 1e-4
+    i = torch.arange(kx_max, dtype=torch.float64, device=device)
+    j = torch.arange(n, device=device)
+    half = torch.where(j + 1 > kx_max, -(n - j).double(), j.double())
+    kx = i[None, None, :]
+    ky = half[None, :, None]
+    kz = half[:, None, None]
+    kxyz = torch.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    kxy = torch.sqrt(kx ** 2 + ky ** 2) + 0.0 * kz
+    eq = (kxyz / k0) ** 4 * torch.exp(-2.0 * (kxyz / k0) ** 2)
+    amp = torch.where(kxyz > kmin, torch.sqrt(eq / (2.0 * math.pi * torch.clamp(kxyz, min=kmin) ** 2)),
+                      torch.zeros((), dtype=torch.float64, device=device))
+    del eq
+    a = amp * torch.exp(1j * phis[0]) * torch.cos(phis[2])
+    b = amp * torch.exp(1j * phis[1]) * torch.sin(phis[2])
+    del phis, amp
+    safe = torch.clamp(kxyz * kxy, min=1e-300)
+    out = []
+    for comp in range(3):
+        if comp == 0:
+            uk = torch.where(kxy > kmin, (a * kxyz * ky + b * kx * kz) / safe, (a + b) / math.sqrt(2.0))
+        elif comp == 1:
+            uk = torch.where(kxy > kmin, (b * ky * kz - a * kxyz * kx) / safe, (b - a) / math.sqrt(2.0))
+        else:
+            uk = -b * kxy / torch.clamp(kxyz, min=kmin)
+        uk = torch.where(kxyz > kmin, uk, torch.zeros((), dtype=uk.dtype, device=device))
+        # Hermitian symmetry on the kx = 0 plane (:338-348); every source lies
+        # outside the targets of its loop, so each loop is one assignment
+        p0 = uk[:, :, 0]
+        kk = torch.arange(1, n, device=device)
+        jj = torch.arange(kx_max, n, device=device)
+        p0[kk[:, None], jj[None, :]] = torch.conj(p0[(n - kk)[:, None], (n - jj)[None, :]])
+        kk2 = torch.arange(kx_max, n, device=device)
+        p0[kk2, 0] = torch.conj(p0[n - kk2, 0])
+        p0[0, jj] = torch.conj(p0[0, n - jj])
+        uk[:, :, 0] = p0
+        uk[:, :, kx_max - 1] = 0.0
+        uk[:, kx_max - 1, :] = 0.0
+        uk[kx_max - 1, :, :] = 0.0
+        uk[0, 0, 0] = 0.0
+        u = torch.fft.irfftn(uk, s=(n, n, n), dim=(0, 1, 2)) * float(n) ** 3
+        del uk
+        out.append(u.contiguous())
+    return out
+
+
 def hit_initial_condition(n: int, k0: float = 4.0, seed: int = 1, mt: float = 0.3, gamma: float = 1.4):
     """Primitive ICs (rho, U, V, W, p) with rho = 1, p = 1/gamma (c = 1) and the
     velocity scaled so that sqrt(<|u|^2>)/c = mt."""

@@ -239,3 +239,20 @@ def test_reference_ogrid_dsm_local_nonfinite_at_128x64x32():
         assert info["time_step"] == steps
         assert all(np.isfinite(a).all() for a in q) == finite, N
     assert np.isfinite(q[0]).all() and not any(np.isfinite(a).all() for a in q[1:])
+
+
+def test_device_hit_generator_matches_numpy():
+    """hit_velocity_device (the generator used for the 1024^3 block) draws the
+    same LCG sequence as the numpy restatement, bit for bit, and gives the same
+    field to FFT rounding (run here on the CPU device)."""
+    import torch
+    from mpi_3dcompact_b200 import hit_ic as HI
+    g1, g2 = HI._Gen(5), HI._Gen(5)
+    for n in (100003, 7):
+        a = HI._vec_torch(torch, g1, n, "cpu").numpy()
+        assert np.array_equal(a, g2.vec(n))
+        assert (g1.ix1, g1.ix2, g1.ix3) == (g2.ix1, g2.ix2, g2.ix3) and g1.r == g2.r
+    ref = HI.hit_velocity(16, 4.0, 3)
+    got = HI.hit_velocity_device(16, 4.0, 3, device="cpu")
+    for g, r in zip(got, ref):
+        assert np.abs(g.numpy() - r).max() <= 1e-14 * np.abs(r).max()
