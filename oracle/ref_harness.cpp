@@ -88,6 +88,12 @@ static bool update_sponge_on() {
 }
 
 // ---- solver hooks (the reference leaves their bodies to the driver) ----
+// Built with MC3D_REF_DRIVER_HOOKS, the harness links the hooks of one of the
+// reference's own drivers instead (tests/hit/Samtaney_D4/MPI_3DCompact.cpp or
+// src/MPI_3DCompact.cpp, compiled with their main renamed), which append to
+// turbdata.out / cylinder{P,U,V,W}.dat / VWakeStrip.dat in the run directory;
+// the step stamps are then not recorded.
+#ifndef MC3D_REF_DRIVER_HOOKS
 void CurvilinearCSolver::initialHook() {}
 void CurvilinearCSolver::fullStepTemporalHook() {
     g_step_stamps.push_back(MPI_Wtime());
@@ -101,6 +107,7 @@ double CurvilinearCSolver::xmomRHSSource(int) { return 0.0; }
 double CurvilinearCSolver::ymomRHSSource(int) { return 0.0; }
 double CurvilinearCSolver::zmomRHSSource(int) { return 0.0; }
 double CurvilinearCSolver::engyRHSSource(int) { return 0.0; }
+#endif
 
 static void die(const string &m) {
     fprintf(stderr, "mc3d_ref: %s\n", m.c_str());

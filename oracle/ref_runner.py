@@ -16,6 +16,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "mc3d_ref")
+# the harness with the hooks of the reference's HIT driver
+# (tests/hit/Samtaney_D4/MPI_3DCompact.cpp) or cylinder driver (src/MPI_3DCompact.cpp)
+HOOK_BINS = {"hit": os.path.join(HERE, "_ref", "mc3d_ref_hit"), "cyl": os.path.join(HERE, "_ref", "mc3d_ref_cyl")}
+HOOK_FILES = {"hit": ("turbdata.out",), "cyl": ("cylinderP.dat", "cylinderU.dat", "cylinderV.dat", "cylinderW.dat",
+                                                 "VWakeStrip.dat")}
 
 _BC = {0: "PERIODIC_SOLVE", 1: "DIRICHLET_SOLVE"}
 
@@ -130,7 +135,7 @@ def _read_fields(path, N, nf, header=8):
 
 
 def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coords=None, dump_to=None,
-               restart_from=None, sponge_dump_to=None, stats_to=None):
+               restart_from=None, sponge_dump_to=None, stats_to=None, hooks=None):
     """Run the reference solver for `nsteps` time steps from primitive ICs
     (rho, U, V, W, p). `coords` = (x, y, z) selects a mesh from file. Returns
     (conserved fields, header dict). `dump_to`: copy the SolutionDump.<step>
@@ -141,9 +146,12 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
     src/MPI_3DCompact.cpp:80-271 restarts); nsteps then counts from its step.
     `sponge_dump_to`: copy the SpongeAvgDump.<step> written with it;
     `stats_to`: (velocity, thermo) paths for the VelocityStats.<step> /
-    ThermoStats.<step> files written with it (cfg.stats enabled)."""
-    if not available():
-        raise RuntimeError("oracle/_ref/mc3d_ref is not built (make -C oracle)")
+    ThermoStats.<step> files written with it (cfg.stats enabled);
+    `hooks`: "hit" or "cyl" runs the harness with that reference driver's
+    hooks and returns the files they wrote in info["hooks"] (name -> bytes)."""
+    binary = REF_BIN if hooks is None else HOOK_BINS[hooks]
+    if not (os.path.isfile(binary) and os.access(binary, os.X_OK)):
+        raise RuntimeError(f"{binary} is not built (make -C oracle all hooks)")
     if restart_from is not None:
         nsteps += int(np.fromfile(restart_from, dtype=np.float64, count=1)[0])   # MAXTIMESTEP is absolute
     with tempfile.TemporaryDirectory() as d:
@@ -151,13 +159,13 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
             f.write(ini_text(cfg, nsteps))
         if restart_from is not None:
             shutil.copy(restart_from, os.path.join(d, "restart.bin"))
-            cmd = [REF_BIN, "restart", "restart.bin", "out.bin"]
+            cmd = [binary, "restart", "restart.bin", "out.bin"]
         else:
             _write(os.path.join(d, "ic.bin"), ic)
             if coords is not None:
                 _write(os.path.join(d, "mesh.bin"), coords)
                 mesh = "file:mesh.bin"
-            cmd = [REF_BIN, "run", mesh, "ic.bin", "out.bin"]
+            cmd = [binary, "run", mesh, "ic.bin", "out.bin"]
         t0 = time.perf_counter()
         env = dict(os.environ)
         env["MC3D_REF_UPDATE_SPONGE"] = "1" if getattr(cfg, "sponge_relax", None) else "0"
@@ -176,8 +184,12 @@ def run_solver(cfg, ic, nsteps, mesh="cube:6.283185307179586", timeout=3600, coo
                     shutil.copy(os.path.join(d, f"{name}.{int(hdr[0])}"), dst)
         st = os.path.join(d, "step_times.txt")
         step_s = [float(x) for x in open(st).read().split()] if os.path.exists(st) else []
+        hook_out = {}
+        for name in HOOK_FILES.get(hooks, ()):
+            fp = os.path.join(d, name)
+            hook_out[name] = open(fp, "rb").read() if os.path.exists(fp) else b""
     info = {"time_step": int(hdr[0]), "time": hdr[1], "dt": hdr[5], "solver_wall_s": hdr[6], "wall_s": wall,
-            "step_s": step_s}
+            "step_s": step_s, "hooks": hook_out}
     return fields, info
 
 

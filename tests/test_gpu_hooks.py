@@ -1,12 +1,19 @@
-"""GPU tests of the drivers' diagnostic hooks as device reductions: the HIT
-turbdata.out line against the oracle's restatement of the HIT driver's hook on
-the same state, and the cylinder driver's span-averaged wall values against
-the restatement applied to the solver's own state.
+"""GPU tests of the drivers' diagnostic hooks as device reductions.
 
-Tolerances: 1e-10 relative for the turbdata values (means of products of
-derivatives summed in a different order than numpy's), 1e-14 for the wall
-averages (same summation order)."""
+* Against the reference's own hook code (tests/golden/hooks.npz, written by
+  the harness built with the hooks of tests/hit/Samtaney_D4/MPI_3DCompact.cpp
+  and src/MPI_3DCompact.cpp): the HIT turbdata.out lines after steps 25 and 50
+  of a 24^3 run, and the cylinder's span-averaged wall p, U, V, W after step 50
+  and the V strip at (i, j) = (0, 143) after each of 50 steps on a
+  16 x 150 x 12 O-grid whose metrics the GPU computes from the mesh.
+  Tolerances: 1e-10 relative for turbdata (sums of products of derivatives in
+  another order), 1e-9 of the record's largest value for the cylinder records
+  (the GPU metrics differ from the reference's by rounding, 1e-13, and 50
+  steps of a wall-bounded flow carry that).
+* Against the oracle's restatement on the same state: the HIT line (1e-10)
+  and the wall averages (1e-14, same summation order)."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -35,6 +42,50 @@ def test_turbdata_matches_restatement(name):
     want = O.hit_turbdata(o, 8.0)
     for k, (a, b) in enumerate(zip(got, want)):
         assert abs(a - b) <= 1e-10 * abs(b) + 1e-300, (k, a, b)
+
+
+def test_turbdata_matches_reference_hook():
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    grid, kw, n, seed = G.HOOK_HIT
+    gold = np.load(os.path.join(G.HERE, "hooks.npz"))["hit_turbdata"]
+    s = m.CurvilinearCSolver(m.Options(grid=grid, **kw))
+    s.set_box_metrics(2.0 * math.pi)
+    s.set_initial_conditions(*hit_initial_condition(grid[0], k0=4.0, seed=seed, mt=0.3))
+    lines = []
+    for step in range(1, n + 1):
+        s.step(1)
+        if step % 25 == 0:           # the driver writes a line every 25 steps
+            lines.append(s.turbdata(8.0))
+    assert len(lines) == len(gold) == 2
+    for got, want in zip(lines, gold):
+        for k, (a, b) in enumerate(zip(got, want)):
+            assert abs(a - b) <= 1e-10 * abs(b) + 1e-300, (k, a, b)
+
+
+def test_cylinder_hooks_match_reference_hooks():
+    cfg, ic, n, coords = G.hook_cyl_case()
+    gold = np.load(os.path.join(G.HERE, "hooks.npz"))
+    opt = m.Options(grid=cfg.N, fd=cfg.fd, filter=cfg.filter, alphaF=cfg.alphaF, mu_ref=cfg.mu_ref, rk=cfg.rk,
+                    cfl=cfg.cfl, bc=cfg.bc, bc_kind=cfg.kinds(), sponge=cfg.sponge,
+                    periodic_disp=O.periodic_disp_table(cfg))
+    s = m.CurvilinearCSolver(opt)
+    s.set_mesh(*coords)
+    s.set_sponge(m.sponge_sigma(opt, *coords))
+    s.set_initial_conditions(*ic)
+    strip_gold = gold["cyl_VWakeStrip"]
+    assert strip_gold.shape[0] == n
+    for step in range(1, n + 1):
+        s.step(1)
+        t = s.info()["time"]
+        row = strip_gold[step - 1]
+        assert abs(t - row[0]) <= 1e-12 * max(abs(row[0]), 1e-30), (step, t, row[0])
+        got = s.wake_strip(0, 143)
+        assert np.abs(got - row[1:]).max() <= 1e-9 * np.abs(row[1:]).max(), step
+    avgs = s.wall_span_average()
+    for name, got in zip(("cylinderP", "cylinderU", "cylinderV", "cylinderW"), avgs):
+        row = gold[f"cyl_{name}"][-1]
+        assert abs(s.info()["time"] - row[0]) <= 1e-12 * row[0]
+        assert np.abs(got - row[1:]).max() <= 1e-9 * max(np.abs(row[1:]).max(), 1e-300), name
 
 
 def test_wall_span_average_matches_restatement():

@@ -2,6 +2,7 @@
 by the reference solver itself (tests/golden/gen_golden.py), operator
 known-answer tests, and a live comparison with oracle/_ref when it is built."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -256,3 +257,22 @@ def test_device_hit_generator_matches_numpy():
     got = HI.hit_velocity_device(16, 4.0, 3, device="cpu")
     for g, r in zip(got, ref):
         assert np.abs(g.numpy() - r).max() <= 1e-14 * np.abs(r).max()
+
+
+def test_oracle_turbdata_matches_reference_hook():
+    """The oracle's restatement of the HIT driver's turbdata hook against the
+    reference's own hook output (tests/golden/hooks.npz) on the same run."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    grid, kw, n, seed = G.HOOK_HIT
+    gold = np.load(os.path.join(G.HERE, "hooks.npz"))["hit_turbdata"]
+    cfg = O.Config(N=grid, **kw)
+    o = O.Oracle(cfg, O.cube_metrics(cfg.N))
+    o.init(*hit_initial_condition(grid[0], k0=4.0, seed=seed, mt=0.3))
+    rows = []
+    for step in range(1, n + 1):
+        o.step()
+        if step % 25 == 0:
+            rows.append(O.hit_turbdata(o, 8.0))
+    for got, want in zip(rows, gold):
+        for k, (a, b) in enumerate(zip(got, want)):
+            assert abs(a - b) <= 1e-11 * abs(b) + 1e-300, (k, a, b)
