@@ -237,7 +237,9 @@ int mc3d_mlp_train_step(mc3d_mlp m, const float *x, const float *y, int n, float
  * with loss = mean_b sum_o (out_bo - y_bo)^2, computed by the same FP32
  * forward, backward and weight-gradient kernels; loss (host, may be NULL) */
 int mc3d_mlp_gradient(mc3d_mlp m, const float *x, const float *y, int n, float *G, double *loss, void *stream);
-/* FP32 forward on CUDA cores, and the BF16 tensor-core inference */
+/* FP32 forward on CUDA cores, and the BF16 tensor-core inference (tcgen05
+ * MMAs on tiles of 128 points, FP32 accumulators in tensor memory, the kernel
+ * of the closure in the time step) */
 int mc3d_mlp_forward(mc3d_mlp m, const float *x, float *y, int n, void *stream);
 int mc3d_mlp_infer_bf16(mc3d_mlp m, const float *x, float *y, int n, void *stream);
 int mc3d_mlp_get_params(mc3d_mlp m, float *P);          /* host, 9090 floats */
@@ -453,10 +455,11 @@ int mc3d_solver_sync(mc3d_solver s);
 int mc3d_solver_set_timing(mc3d_solver s, int enable);
 const char *mc3d_solver_timing_report(mc3d_solver s);
 
-/* Number of line-solve CTAs on `device` whose TMA tile load did not arrive
- * within the kernel's bounded wait (they skipped their tile: the results of
- * that launch are invalid). mc3d_solver_info and mc3d_solver_get_conserved
- * return MC3D_ERR_TIMEOUT when it is nonzero. */
+/* Number of bounded waits on `device` that gave up: line-solve CTAs whose TMA
+ * tile load did not arrive (they skipped their tile) plus learned-closure
+ * warpgroups whose tensor-core MMAs did not complete (they stopped); the
+ * results of those launches are invalid. mc3d_solver_info and
+ * mc3d_solver_get_conserved return MC3D_ERR_TIMEOUT when it is nonzero. */
 int mc3d_tma_wait_timeouts(int device, int *count);
 
 /* ---- SGS models on their own (AbstractSGS, src/AbstractSGS.hpp:10-42) ----

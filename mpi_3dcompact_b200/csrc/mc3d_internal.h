@@ -250,6 +250,11 @@ struct RkStage {
     int stage;         // 1-based
     int nstages;
     double a, b;       // scheme coefficients of this stage
+    // last stage: leave out writes nothing reads after the step; bit 0 the
+    // 2N register (the next step starts from q1, written by the filter or the
+    // final-state copy), bit 1 the FP64 final state when the filter takes its
+    // working-precision copy and no statistics read it
+    int skip_last;
 };
 // prim (optional, may be null): also write rho, U, V, W, T of the new stage
 // state, or with copy_final on the last stage the final state in R instead
@@ -280,7 +285,7 @@ int launch_finalize_dt(TimeState *ts, int ts_type, double cfl, double dt_const, 
 // ---- learned SGS closure (mlp.cu) --------------------------------------------
 constexpr int MLP_IN = 9, MLP_OUT = 2;
 constexpr int MLP_NPARAM = 9090;   // 9*64+64 + 2*(64*64+64) + 64*2+2
-constexpr int MLP_NHALF = 64 * 24 + 2 * 64 * 72 + 8 * 72;
+constexpr int MLPT_BYTES = 29696;  // weight image of the tensor-core inference (mlp_common.cuh)
 // input normalisation x_n = (x - mean) * inv_std, and the training range [lo, hi]
 struct MlpNorm {
     float mean[MLP_IN], inv_std[MLP_IN], lo[MLP_IN], hi[MLP_IN];
@@ -288,8 +293,7 @@ struct MlpNorm {
 };
 struct MlpDev {
     float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr;   // FP32 master, grads, Adam moments
-    __nv_bfloat16 *Hw = nullptr;                                     // packed bf16 weights
-    float *Bc = nullptr;                                             // compact biases [64|64|64|2]
+    unsigned char *Tw = nullptr;   // BF16 weight image of the tensor-core inference (MLPT_BYTES)
     MlpNorm norm{};
     long long t = 0;                                                 // Adam step
 };
@@ -300,7 +304,10 @@ int mlp_gradient(MlpDev &m, const float *x, const float *y, int n, float *act, f
                  double *loss, cudaStream_t st);
 int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, float *act, float *out, float *delta,
                    double *loss, cudaStream_t st);
+// tensor-core inference of raw features x [n][9] -> raw outputs [n][2] (sgs_mlp.cu)
 int mlp_infer_bf16(const MlpDev &m, const float *x, int n, float *out, cudaStream_t st);
+// MMA completions that did not arrive within the wait limit (tensor-core inference)
+int mlp_wait_timeouts(int *count);
 const MlpDev *mlp_dev(mc3d_mlp m);
 // fused closure in the time step: d[12] the xi-derivatives of U, V, W, T
 template <typename R>

@@ -9,9 +9,9 @@
 // mlp_backward the per-sample deltas and the MSE, mlp_wgrad reduces the weight
 // and bias gradients over the batch (split over the batch, one atomic add per
 // split), mlp_adam applies Adam with bias correction.
-// Inference (BF16 tensor cores, FP32 accumulate): mma.sync m16n8k16 tiles of
-// 16 points; a layer's accumulator fragments become the next layer's A
-// fragments in registers, so activations never leave the SM.
+// Inference (BF16 tensor cores, FP32 accumulate in tensor memory) runs on
+// tcgen05 MMAs over tiles of 128 points (mlp_tc.cuh, kernels in sgs_mlp.cu);
+// mlp_pack writes its weight image after every change of the parameters.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -188,62 +188,54 @@ __global__ void mlp_adam_kernel(float *P, float *G, float *M, float *V, float lr
     G[k] = 0.0f;
 }
 
-__global__ void mlp_pack_kernel(const float *__restrict__ P, __nv_bfloat16 *__restrict__ Hw, float *__restrict__ Bc) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < MLPH_N; k += gridDim.x * blockDim.x) {
-        float v = 0.0f;
-        if (k < MLPH_W2) {
-            const int o = k / MLPH_P1, c = k % MLPH_P1;
-            v = c < MLP_IN ? P[MLP_W1 + o * MLP_IN + c] : 0.0f;
-        } else if (k < MLPH_W4) {
-            const int w = k < MLPH_W3 ? MLP_W2 : MLP_W3, kk = k - (k < MLPH_W3 ? MLPH_W2 : MLPH_W3);
-            const int o = kk / MLPH_P, c = kk % MLPH_P;
-            v = c < 64 ? P[w + o * 64 + c] : 0.0f;
-        } else {
-            const int o = (k - MLPH_W4) / MLPH_P, c = (k - MLPH_W4) % MLPH_P;
-            v = (o < MLP_OUT && c < 64) ? P[MLP_W4 + o * 64 + c] : 0.0f;
-        }
-        Hw[k] = __float2bfloat16_rn(v);
-    }
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 3 * 64 + MLP_OUT; k += gridDim.x * blockDim.x)
-        Bc[k] = k < 64 ? P[MLP_B1 + k] : k < 128 ? P[MLP_B2 + k - 64] : k < 192 ? P[MLP_B3 + k - 128] : P[MLP_B4 + k - 192];
+// The weight image of the tensor-core inference (layout in mlp_common.cuh),
+// written over a zeroed buffer: one thread per element of the eight blocks.
+// A bias b is carried as the BF16 pair (b_hi, b_lo), b_hi = bf16(b) and
+// b_lo = bf16(b - b_hi), against two constant-one input columns.
+__device__ __forceinline__ void bias_pair(float b, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(b);
+    lo = __float2bfloat16_rn(b - __bfloat162float(hi));
 }
 
-}  // namespace
-
-namespace {
-
-// standalone inference: x [n][9] (raw features) -> out [n][2] (raw outputs)
-__global__ void __launch_bounds__(128) mlp_infer_kernel(const __nv_bfloat16 *__restrict__ Hw,
-                                                         const float *__restrict__ Bc, MlpNorm nrm,
-                                                         const float *__restrict__ x, int n, float *__restrict__ out) {
-    constexpr int XS = 24;   // bf16 row pitch of 48 bytes: the fragment loads hit distinct banks
-    __shared__ __align__(16) __nv_bfloat16 sW[MLPH_N];
-    __shared__ float bias[3 * 64 + MLP_OUT];
-    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * XS];
-    __shared__ float ys[4][64];
-    for (int k = threadIdx.x; k < MLPH_N; k += blockDim.x) sW[k] = Hw[k];
-    for (int k = threadIdx.x; k < 3 * 64 + MLP_OUT; k += blockDim.x) bias[k] = Bc[k];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * 4 * 32;
-    for (long long base = ((long long)blockIdx.x * 4 + warp) * 32; base < n; base += stride) {
-        const long long p = base + lane;
-        __nv_bfloat16 *row = xs[warp] + lane * XS;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            float v = 0.0f;
-            if (k < MLP_IN && p < n) v = (x[p * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k];
-            row[k] = __float2bfloat16_rn(v);
+__global__ void mlp_pack_kernel(const float *__restrict__ P, unsigned char *__restrict__ img) {
+    // element counts of W1 [64][16], W2, W3 [64][64], W4 [16][64], B2, B3 [64][16], B4 [16][16], Ac [128][16]
+    constexpr int n1 = 64 * 16, n2 = 64 * 64, n4 = 16 * 64, nb = 64 * 16, nb4 = 16 * 16, nac = 128 * 16;
+    constexpr int total = n1 + 2 * n2 + n4 + 2 * nb + nb4 + nac;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        int k = e, off;
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (k < n1) {   // W1 and the layer-1 bias
+            const int o = k / 16, c = k % 16;
+            __nv_bfloat16 hi, lo;
+            bias_pair(P[MLP_B1 + o], hi, lo);
+            if (c < MLP_IN) v = __float2bfloat16_rn(P[MLP_W1 + o * MLP_IN + c]);
+            else if (c == MLP_IN) v = hi;
+            else if (c == MLP_IN + 1) v = lo;
+            off = MLPT_W1 + tc_off16(o, c);
+        } else if ((k -= n1) < 2 * n2) {   // W2, W3
+            const int w = k < n2 ? MLP_W2 : MLP_W3, kk = k % n2, o = kk / 64, c = kk % 64;
+            v = __float2bfloat16_rn(P[w + o * 64 + c]);
+            off = (k < n2 ? MLPT_W2 : MLPT_W3) + tc_off64(o, c);
+        } else if ((k -= 2 * n2) < n4) {   // W4, rows past the outputs zero
+            const int o = k / 64, c = k % 64;
+            if (o < MLP_OUT) v = __float2bfloat16_rn(P[MLP_W4 + o * 64 + c]);
+            off = MLPT_W4 + tc_off64(o, c);
+        } else if ((k -= n4) < 2 * nb + nb4) {   // bias blocks of layers 2, 3, 4
+            const int blk = k < nb ? 0 : k < 2 * nb ? 1 : 2, kk = k - blk * nb, o = kk / 16, c = kk % 16;
+            const int nout = blk == 2 ? MLP_OUT : 64;
+            if (o < nout && c < 2) {
+                __nv_bfloat16 hi, lo;
+                bias_pair(P[(blk == 0 ? MLP_B2 : blk == 1 ? MLP_B3 : MLP_B4) + o], hi, lo);
+                v = c == 0 ? hi : lo;
+            }
+            off = (blk == 0 ? MLPT_B2 : blk == 1 ? MLPT_B3 : MLPT_B4) + tc_off16(o, c);
+        } else {   // the constant-one columns of the bias MMAs
+            k -= 2 * nb + nb4;
+            const int r = k / 16, c = k % 16;
+            if (c < 2) v = __float2bfloat16_rn(1.0f);
+            off = MLPT_AC + tc_off16(r, c);
         }
-        __syncwarp();
-        mlp_tile16<XS>(xs[warp], 0, sW, bias, ys[warp], lane);
-        mlp_tile16<XS>(xs[warp], 16, sW, bias, ys[warp], lane);
-        __syncwarp();
-        if (p < n) {
-            out[p * 2 + 0] = ys[warp][lane * 2 + 0];
-            out[p * 2 + 1] = ys[warp][lane * 2 + 1];
-        }
-        __syncwarp();
+        *reinterpret_cast<__nv_bfloat16 *>(img + off) = v;
     }
 }
 
@@ -253,7 +245,8 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const __nv_bfloat16 *__r
 // host side
 // ---------------------------------------------------------------------------
 int mlp_pack(const MlpDev &m, cudaStream_t st) {
-    mlp_pack_kernel<<<16, 256, 0, st>>>(m.P, m.Hw, m.Bc);
+    MC3D_CUDA_TRY(cudaMemsetAsync(m.Tw, 0, MLPT_BYTES, st));
+    mlp_pack_kernel<<<16, 256, 0, st>>>(m.P, m.Tw);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -294,13 +287,6 @@ int mlp_train_step(MlpDev &m, const float *x, const float *y, int n, float lr, f
     mlp_adam_kernel<<<(MLP_NP + 255) / 256, 256, 0, st>>>(m.P, m.G, m.M, m.V, lr, b1t, b2t);
     MC3D_CUDA_TRY(cudaGetLastError());
     return mlp_pack(m, st);
-}
-
-int mlp_infer_bf16(const MlpDev &m, const float *x, int n, float *out, cudaStream_t st) {
-    const int blocks = std::max(1, std::min((n + 127) / 128, 148 * 8));
-    mlp_infer_kernel<<<blocks, 128, 0, st>>>(m.Hw, m.Bc, m.norm, x, n, out);
-    MC3D_CUDA_TRY(cudaGetLastError());
-    return MC3D_OK;
 }
 
 }  // namespace mc3d

@@ -76,8 +76,7 @@ int mc3d_mlp_create(unsigned long long seed, int device, mc3d_mlp *out) {
         if (e == cudaSuccess) e = cudaMalloc(b, MLP_NPARAM * sizeof(float));
         if (e == cudaSuccess) e = cudaMemset(*b, 0, MLP_NPARAM * sizeof(float));
     }
-    if (e == cudaSuccess) e = cudaMalloc(&m->dev.Hw, MLP_NHALF * sizeof(__nv_bfloat16));
-    if (e == cudaSuccess) e = cudaMalloc(&m->dev.Bc, (3 * 64 + MLP_OUT) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->dev.Tw, MLPT_BYTES);
     if (e == cudaSuccess) e = cudaMalloc(&m->loss, sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(m->dev.P, P.data(), MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -97,8 +96,8 @@ int mc3d_mlp_create(unsigned long long seed, int device, mc3d_mlp *out) {
 int mc3d_mlp_destroy(mc3d_mlp m) {
     if (!m) return MC3D_OK;
     cudaSetDevice(m->device);
-    for (void *p : {(void *)m->dev.P, (void *)m->dev.G, (void *)m->dev.M, (void *)m->dev.V, (void *)m->dev.Hw,
-                    (void *)m->dev.Bc, (void *)m->act, (void *)m->out, (void *)m->delta, (void *)m->loss})
+    for (void *p : {(void *)m->dev.P, (void *)m->dev.G, (void *)m->dev.M, (void *)m->dev.V, (void *)m->dev.Tw,
+                    (void *)m->act, (void *)m->out, (void *)m->delta, (void *)m->loss})
         if (p) cudaFree(p);
     delete m;
     return MC3D_OK;

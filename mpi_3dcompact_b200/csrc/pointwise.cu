@@ -544,11 +544,13 @@ __global__ void __launch_bounds__(256) rk_kernel(Grid3 g, RkStage rs, K5<R> k2, 
                 }
             }
         }
+        const bool put_q1 = wr_q1 && !(last && (rs.skip_last & 1));
+        const bool put_q2 = wr_q2 && !(last && (rs.skip_last & 2));
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            if (wr_q1) st_pair<double>(q1.p[v], i, two, o1[v][0], o1[v][1]);
+            if (put_q1) st_pair<double>(q1.p[v], i, two, o1[v][0], o1[v][1]);
             if (wr_qk) st_pair<double>(qk.p[v], i, two, ok[v][0], ok[v][1]);
-            if (wr_q2) st_pair<double>(q2.p[v], i, two, o2[v][0], o2[v][1]);
+            if (put_q2) st_pair<double>(q2.p[v], i, two, o2[v][0], o2[v][1]);
         }
         // the final state in the working precision, for the filter that follows
         if (last && want_prims == 2) {

@@ -20,7 +20,7 @@
 #include <algorithm>
 #include <cmath>
 
-#include "mlp_common.cuh"
+#include "mlp_tc.cuh"
 
 namespace mc3d {
 
@@ -31,33 +31,35 @@ __device__ __forceinline__ float metf(const Metrics<R> &m, int c, long long i) {
     return (float)(m.constant ? m.c[c] : m.m[c][i]);
 }
 
-// Fused closure evaluation: features of every point, BF16 tensor-core MLP,
-// mu_sgs and k_sgs; *flag counts the points with a feature outside the training
-// range (those features are clamped to the range before the network).
+// Warpgroups per CTA of the tensor-core kernels: 256 threads and 63.5 KB of
+// shared memory per CTA (the weight image and two activation tiles), so three
+// CTAs share an SM and hold 3 x 128 of its 512 TMEM columns.
+constexpr int TC_NWG = 2;
+constexpr size_t TC_SMEM = 1024 + MLPT_BYTES + TC_NWG * MLPT_TILE + 16 * TC_NWG;
+
+// Fused closure evaluation: features of every point, the network on the
+// tensor cores, mu_sgs and k_sgs; *flag counts the points with a feature
+// outside the training range (those features are clamped to the range before
+// the network). Persistent CTAs; each warpgroup walks tiles of 128 points,
+// thread r of the warpgroup owning point r of the tile.
 template <typename R>
-__global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f,
-                                                       DerivPtrs12c<R> dp, Metrics<R> m, double dvol, double mu_ref,
-                                                       const __nv_bfloat16 *__restrict__ Hw,
-                                                       const float *__restrict__ Bc, MlpNorm nrm, R *mu_sgs, R *ksgs,
-                                                       int *flag) {
-    constexpr int XS = 24;
-    __shared__ __align__(16) __nv_bfloat16 sW[MLP_NHALF];
-    __shared__ float bias[3 * 64 + MLP_OUT];
-    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * XS];
-    __shared__ float ys[4][64];
-    for (int k = threadIdx.x; k < MLP_NHALF; k += blockDim.x) sW[k] = Hw[k];
-    for (int k = threadIdx.x; k < 3 * 64 + MLP_OUT; k += blockDim.x) bias[k] = Bc[k];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long n = g.n();
-    const long long stride = (long long)gridDim.x * 4 * 32;
+__global__ void __launch_bounds__(TC_NWG * 128, 3)
+    sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f, DerivPtrs12c<R> dp,
+                   Metrics<R> m, double dvol, double mu_ref, const uint4 *__restrict__ img, MlpNorm nrm, R *mu_sgs,
+                   R *ksgs, int *flag) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const TcCta c = tc_setup<TC_NWG>(smem_raw, img);
+    const int wg = threadIdx.x >> 7, r = threadIdx.x & 127, lane = threadIdx.x & 31;
+    unsigned char *tile = c.img + MLPT_BYTES + wg * MLPT_TILE;
+    unsigned phase = 0;
+    const long long n = g.n(), ntiles = (n + 127) / 128;
     const float delta_c = m.constant ? cbrtf((float)(dvol / (double)m.c[0])) : 0.f;   // Delta of a uniform block
-    for (long long base = ((long long)blockIdx.x * 4 + warp) * 32; base < n; base += stride) {
-        const long long i = base + lane;
+    for (long long t = (long long)blockIdx.x * TC_NWG + wg; t < ntiles; t += (long long)gridDim.x * TC_NWG) {
+        const long long i = t * 128 + r;
         const bool ok = i < n;
-        double rho = 1.0, scale = 0.0;
+        double scale = 0.0;
         bool out_of_range = false;
-        __nv_bfloat16 *row = xs[warp] + lane * XS;
+        float xn[MLP_IN];
         if (ok) {
             float gu[3][3], gT[3];
 #pragma unroll
@@ -74,7 +76,6 @@ __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restri
                     gT[b] = metf(m, 1 + b, i) * d1 + metf(m, 4 + b, i) * d2 + metf(m, 7 + b, i) * d3;
             }
             const float rhof = (float)rho_f[i], T = (float)T_f[i];
-            rho = rhof;
             const float delta = m.constant ? delta_c : cbrtf((float)dvol / metf(m, 0, i));
             const float mu = (float)mu_ref * __powf(T, 0.76f);
             float x[MLP_IN];
@@ -92,29 +93,80 @@ __global__ void __launch_bounds__(128) sgs_mlp_kernel(Grid3 g, const R *__restri
             for (int k = 0; k < MLP_IN; k++) {
                 if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;   // NaN counts as outside
                 const float xc = fminf(fmaxf(x[k], nrm.lo[k]), nrm.hi[k]);
-                row[k] = __float2bfloat16_rn((xc - nrm.mean[k]) * nrm.inv_std[k]);
+                xn[k] = (xc - nrm.mean[k]) * nrm.inv_std[k];
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < MLP_IN; k++) row[k] = __float2bfloat16_rn(0.0f);
+            for (int k = 0; k < MLP_IN; k++) xn[k] = 0.0f;
         }
-#pragma unroll
-        for (int k = MLP_IN; k < 16; k++) row[k] = __float2bfloat16_rn(0.0f);
         const unsigned outside = __ballot_sync(0xffffffffu, out_of_range);
         if (outside && lane == 0) atomicAdd(flag, __popc(outside));
-        __syncwarp();
-        mlp_tile16<XS>(xs[warp], 0, sW, bias, ys[warp], lane);
-        mlp_tile16<XS>(xs[warp], 16, sW, bias, ys[warp], lane);
-        __syncwarp();
+        tc_put_input(tile, r, xn);
+        float o0, o1;
+        if (!tc_forward(c, wg, r, phase, o0, o1)) break;
         if (ok) {
-            const double C = fmax(0.0, (double)ys[warp][lane * 2 + 0] * nrm.ystd[0] + nrm.ymean[0]);
-            const double prt = fmin(10.0, fmax(0.1, (double)ys[warp][lane * 2 + 1] * nrm.ystd[1] + nrm.ymean[1]));
+            const double C = fmax(0.0, (double)o0 * nrm.ystd[0] + nrm.ymean[0]);
+            const double prt = fmin(10.0, fmax(0.1, (double)o1 * nrm.ystd[1] + nrm.ymean[1]));
             const double mt = C * scale;
             mu_sgs[i] = (R)mt;
             ksgs[i] = (R)(CP * mt / prt);
         }
-        __syncwarp();
     }
+    tc_teardown<TC_NWG>(c);
+}
+
+// standalone inference: x [n][9] (raw features, normalised without clamping)
+// -> out [n][2] (raw outputs)
+__global__ void __launch_bounds__(TC_NWG * 128, 3)
+    mlp_infer_kernel(const uint4 *__restrict__ img, MlpNorm nrm, const float *__restrict__ x, int n,
+                     float *__restrict__ out) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const TcCta c = tc_setup<TC_NWG>(smem_raw, img);
+    const int wg = threadIdx.x >> 7, r = threadIdx.x & 127;
+    unsigned char *tile = c.img + MLPT_BYTES + wg * MLPT_TILE;
+    unsigned phase = 0;
+    const long long ntiles = ((long long)n + 127) / 128;
+    for (long long t = (long long)blockIdx.x * TC_NWG + wg; t < ntiles; t += (long long)gridDim.x * TC_NWG) {
+        const long long p = t * 128 + r;
+        float xn[MLP_IN];
+#pragma unroll
+        for (int k = 0; k < MLP_IN; k++) xn[k] = p < n ? (x[p * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k] : 0.0f;
+        tc_put_input(tile, r, xn);
+        float o0, o1;
+        if (!tc_forward(c, wg, r, phase, o0, o1)) break;
+        if (p < n) {
+            out[p * 2 + 0] = o0;
+            out[p * 2 + 1] = o1;
+        }
+    }
+    tc_teardown<TC_NWG>(c);
+}
+
+// grid of the persistent tensor-core kernels: as many CTAs as fit on the SMs
+// together (shared memory, registers, threads, TMEM columns; counted here from
+// the kernel's attributes, with the largest shared-memory carveout requested),
+// and no more than there are tile pairs
+template <typename K>
+int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
+    if (int rc = open_kernel(kern, st, TC_SMEM, TC_NWG * 128, nullptr)) return rc;
+    MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+    int dev = 0, nsm = 0, smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
+    MC3D_CUDA_TRY(cudaGetDevice(&dev));
+    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    cudaFuncAttributes fa{};
+    MC3D_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    const int threads = TC_NWG * 128;
+    int per = std::min(smem_sm / (int)(TC_SMEM + resv), thr_sm / threads);
+    if (fa.numRegs > 0) per = std::min(per, regs_sm / (fa.numRegs * threads));
+    per = std::max(1, std::min(per, 512 / (TC_NWG * MLPT_NCOL)));
+    const long long need = (n + 128LL * TC_NWG - 1) / (128LL * TC_NWG);
+    *blocks = (int)std::max(1LL, std::min<long long>(need, (long long)nsm * per));
+    return MC3D_OK;
 }
 
 // ---- training data -----------------------------------------------------------
@@ -214,9 +266,12 @@ int launch_sgs_mlp(const Grid3 &g, const R *rho, const R *T, const R *const d[12
                    double mu_ref, const MlpDev &mlp, R *mu_sgs, R *ksgs, int *flag, cudaStream_t st) {
     DerivPtrs12c<R> dp;
     for (int k = 0; k < 12; k++) dp.p[k] = d[k];
-    const int blocks = (int)std::min<long long>((g.n() + 127) / 128, 148 * 6);
-    sgs_mlp_kernel<R><<<blocks, 128, 0, st>>>(g, rho, T, dp, m, dvol, mu_ref, mlp.Hw, mlp.Bc, mlp.norm, mu_sgs, ksgs,
-                                              flag);
+    static KernelLaunchState ks;
+    int blocks = 0;
+    if (int rc = tc_grid(sgs_mlp_kernel<R>, ks, g.n(), &blocks)) return rc;
+    sgs_mlp_kernel<R><<<blocks, TC_NWG * 128, TC_SMEM, st>>>(g, rho, T, dp, m, dvol, mu_ref,
+                                                              reinterpret_cast<const uint4 *>(mlp.Tw), mlp.norm,
+                                                              mu_sgs, ksgs, flag);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
@@ -226,6 +281,21 @@ template int launch_sgs_mlp<float>(const Grid3 &, const float *, const float *, 
 template int launch_sgs_mlp<double>(const Grid3 &, const double *, const double *, const double *const[12],
                                     const Metrics<double> &, double, double, const MlpDev &, double *, double *, int *,
                                     cudaStream_t);
+
+int mlp_infer_bf16(const MlpDev &m, const float *x, int n, float *out, cudaStream_t st) {
+    if (n <= 0) return MC3D_OK;
+    static KernelLaunchState ks;
+    int blocks = 0;
+    if (int rc = tc_grid(mlp_infer_kernel, ks, n, &blocks)) return rc;
+    mlp_infer_kernel<<<blocks, TC_NWG * 128, TC_SMEM, st>>>(reinterpret_cast<const uint4 *>(m.Tw), m.norm, x, n, out);
+    MC3D_CUDA_TRY(cudaGetLastError());
+    return MC3D_OK;
+}
+
+int mlp_wait_timeouts(int *count) {
+    MC3D_CUDA_TRY(cudaMemcpyFromSymbol(count, g_mlp_wait_timeouts, sizeof(int)));
+    return MC3D_OK;
+}
 
 int launch_box_filter(const Grid3 &gf, int f, const double *const q[5], double *const out[14], cudaStream_t st) {
     Q5c qq;

@@ -716,12 +716,16 @@ static int stage_post(mc3d_solver s) {
     return face_poststep<R>(s);
 }
 
-// MC3D_ERR_TIMEOUT when a line-solve tile load gave up waiting on this device
+// MC3D_ERR_TIMEOUT when a line-solve tile load or a tensor-core MMA of the
+// learned closure gave up waiting on this device
 static int tma_timeouts_failed(mc3d_solver s) {
     (void)s;
-    int n = 0;
+    int n = 0, nm = 0;
     if (int rc = tma_wait_timeouts(&n)) return rc;
-    return n ? fail(MC3D_ERR_TIMEOUT, "a line-solve tile load did not arrive within the wait limit") : MC3D_OK;
+    if (n) return fail(MC3D_ERR_TIMEOUT, "a line-solve tile load did not arrive within the wait limit");
+    if (int rc = mlp_wait_timeouts(&nm)) return rc;
+    return nm ? fail(MC3D_ERR_TIMEOUT, "a tensor-core MMA of the learned closure did not complete within the wait limit")
+              : MC3D_OK;
 }
 
 // bit f: face f is a SPONGE
@@ -821,6 +825,12 @@ static int stage_rk(mc3d_solver s, int st) {
     const bool copy_final = !s->lean && st == ns && s->cur_filter_now && s->prec != MC3D_FP64;
     if (copy_final)
         for (int v = 0; v < 5; v++) pw[v] = (R *)s->tC[v];
+    // after the last stage the step continues from q1 (filter_conserved), so
+    // the 2N register is dead there, and so is the FP64 final state q2 when
+    // the filter reads its working copy and no statistics read q2
+    const bool two_n = scheme == MC3D_KENRK4 || scheme == MC3D_LSLDDRK4;
+    const bool stats = s->cfg.velocity_stats || s->cfg.thermo_stats;
+    rs.skip_last = (two_n ? 1 : 0) | (copy_final && !stats ? 2 : 0);
     s->launches++;
     {
         // reads k2 and the FP64 registers the scheme touches, writes the updated ones
@@ -828,6 +838,7 @@ static int stage_rk(mc3d_solver s, int st) {
         if (scheme == MC3D_RK4) b += st == 1 ? 5.0 * 8 * 3 : (st < 4 ? 5.0 * 8 * 4 : 5.0 * 8 * 2);
         else if (scheme == MC3D_TVDRK3) b += st == 1 ? 5.0 * 8 * 2 : 5.0 * 8 * 3;
         else b += st == 1 ? 5.0 * 8 * 3 : 5.0 * 8 * 4;
+        if (st == ns) b -= 5.0 * 8 * ((rs.skip_last & 1) + ((rs.skip_last >> 1) & 1));
         if (fuse_prims || copy_final) b += 5.0 * sizeof(R);
         if ((rc = tic(s, KC_RK, b * (double)s->g.n()))) return rc;
     }

@@ -239,5 +239,9 @@ int tma_wait_timeouts(int *count) {
 extern "C" int mc3d_tma_wait_timeouts(int device, int *count) {
     if (!count) return mc3d::fail(MC3D_ERR_ARG, "null argument");
     MC3D_CUDA_TRY(cudaSetDevice(device));
-    return mc3d::tma_wait_timeouts(count);
+    int a = 0, b = 0;
+    if (int rc = mc3d::tma_wait_timeouts(&a)) return rc;
+    if (int rc = mc3d::mlp_wait_timeouts(&b)) return rc;
+    *count = a + b;
+    return MC3D_OK;
 }
