@@ -51,8 +51,9 @@ CPU_SAMPLE_GRID = 128
 ERR_STEPS = 200
 LES_GRID, LES_STEPS, LES_MU, LES_SEED = 128, 500, 2.5e-4, 5
 # the learned closure's stage goes to DSM when more than this fraction of the
-# points has a feature outside the training range (features are clamped)
-LES_MLP_FALLBACK = 0.1
+# points has a feature outside the training range (features are clamped): the
+# library's default LES.MLPFALLBACKFRAC
+LES_MLP_FALLBACK = 1e-3
 LES_SCHEME = dict(fd="PADE6", filter="COMPACT10", alphaF=0.49, rk="RK4", les_avg="GLOBAL", cfl=0.5)
 MLP_WEIGHTS = os.path.join(ROOT, "mpi_3dcompact_b200", "data", "mlp_sgs_hit128.bin")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -349,7 +350,7 @@ def learned_sgs_block(args, local):
     ic = hit_initial_condition(n, k0=K0, seed=LES_SEED, mt=MT)
     out = {}
     for les in ("MLP", "DSM", "NOMODEL"):
-        kw = dict(mlp_fallback_frac=LES_MLP_FALLBACK) if les == "MLP" else {}
+        kw = dict(mlp_fallback_frac=args.les_fallback) if les == "MLP" else {}
         s = m.CurvilinearCSolver(m.Options(grid=n, mu_ref=LES_MU, les=les, precision=m.FP32BULK, **LES_SCHEME, **kw),
                                  device=local)
         s.set_box_metrics(2 * math.pi)
@@ -394,12 +395,12 @@ def learned_sgs_block(args, local):
     return {
         "workload": f"decaying HIT {n}^3 LES, PADE6, RK4, COMPACT10 alpha_f=0.49 every step, CFL 0.5, Mt=0.3, "
                     f"mu_ref={LES_MU}, FP32-bulk, {steps} steps from the seed-{LES_SEED} initial field",
-        "closure": "9-64-64-64-2 GELU MLP, BF16 tensor-core inference fused into the SGS pass; trained on 512^3 "
-                   "DNS box-filtered to 128^3, coefficient calibrated a posteriori on LES seeds 1 and 2 "
-                   "(mpi_3dcompact_b200/train_sgs.py)",
+        "closure": "9-64-64-64-2 GELU MLP, BF16 tcgen05 tensor-core inference (TMEM accumulators, GELU in packed "
+                   "BF16) fused into the SGS pass; trained on 8 seeds of 512^3 DNS box-filtered to 128^3, coefficient "
+                   "calibrated a posteriori on LES seeds 1 and 2 (mpi_3dcompact_b200/train_sgs.py)",
         "ms_per_step": {"mlp": mlp["ms"], "dsm": dsm["ms"], "nomodel": nom["ms"]},
         "mlp_speedup_over_dsm": dsm["ms"] / mlp["ms"],
-        "fallback_frac": LES_MLP_FALLBACK, "fallback_stages": mlp["fallbacks"], "stages": mlp["stages"],
+        "fallback_frac": args.les_fallback, "fallback_stages": mlp["fallbacks"], "stages": mlp["stages"],
         "ke_decay_max_rel_diff_vs_dsm": {"mlp": decay_diff(mlp), "nomodel": decay_diff(nom)},
         "ke_final": {"mlp": float(mlp["ke"][-1]), "dsm": float(dsm["ke"][-1]), "nomodel": float(nom["ke"][-1]),
                      "initial": float(dsm["ke"][0])},
@@ -694,6 +695,8 @@ def main():
     ap.add_argument("--no-cylinder", action="store_true")
     ap.add_argument("--cyl-steps", type=int, default=5)
     ap.add_argument("--les-steps", type=int, default=LES_STEPS)
+    ap.add_argument("--les-fallback", type=float, default=LES_MLP_FALLBACK,
+                    help="fallback fraction of the learned closure in the 128^3 LES")
     ap.add_argument("--err-steps", type=int, default=ERR_STEPS)
     ap.add_argument("--workload", choices=["hit256", "hbm1024"], default="hit256",
                     help="hbm1024: the 1024^3 HBM-sizing configuration with lean storage")

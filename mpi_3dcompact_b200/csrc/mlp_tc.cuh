@@ -6,8 +6,9 @@
 //                         + Ac[128 x 16] B_l'[16 x N_l]        (the bias, one MMA)
 // BF16 operands in shared memory, FP32 accumulators in tensor memory (TMEM
 // lane = point, column = output). The accumulator of a layer is read back by
-// the warpgroup's own threads (tcgen05.ld, thread = point), put through the
-// GELU in registers and written as BF16 into the operand tile of the next
+// the warpgroup's own threads (tcgen05.ld, thread = point), rounded to BF16
+// pairs, put through the GELU in packed BF16 arithmetic in registers and
+// written into the operand tile of the next
 // layer, whose MMAs one thread then issues; tcgen05.commit on an mbarrier
 // signals their completion. The biases ride on the tensor cores: layer 1's
 // input carries two constant-one columns against the rows (b_hi, b_lo) of W1
@@ -167,8 +168,8 @@ __device__ __forceinline__ void tc_put_input(unsigned char *tile, int r, const f
     *reinterpret_cast<uint4 *>(tc_row_chunk(tile, r, 1)) = c1;
 }
 
-// accumulator columns [c0, c0 + 32) of this thread's row -> GELU -> BF16
-// chunks c0/8 .. c0/8 + 3 of the row
+// accumulator columns [c0, c0 + 32) of this thread's row -> BF16 pairs ->
+// GELU -> chunks c0/8 .. c0/8 + 3 of the row
 __device__ __forceinline__ void tc_gelu_half(unsigned taddr, unsigned char *tile, int r, int c0) {
     unsigned v[32];
     tc_ld32(taddr + (unsigned)c0, v);
@@ -176,10 +177,10 @@ __device__ __forceinline__ void tc_gelu_half(unsigned taddr, unsigned char *tile
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         uint4 o;
-        o.x = pack_bf2(gelu_fast(__uint_as_float(v[8 * q + 0])), gelu_fast(__uint_as_float(v[8 * q + 1])));
-        o.y = pack_bf2(gelu_fast(__uint_as_float(v[8 * q + 2])), gelu_fast(__uint_as_float(v[8 * q + 3])));
-        o.z = pack_bf2(gelu_fast(__uint_as_float(v[8 * q + 4])), gelu_fast(__uint_as_float(v[8 * q + 5])));
-        o.w = pack_bf2(gelu_fast(__uint_as_float(v[8 * q + 6])), gelu_fast(__uint_as_float(v[8 * q + 7])));
+        o.x = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 0]), __uint_as_float(v[8 * q + 1])));
+        o.y = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 2]), __uint_as_float(v[8 * q + 3])));
+        o.z = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 4]), __uint_as_float(v[8 * q + 5])));
+        o.w = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 6]), __uint_as_float(v[8 * q + 7])));
         *reinterpret_cast<uint4 *>(tc_row_chunk(tile, r, c0 / 8 + q)) = o;
     }
 }

@@ -15,10 +15,11 @@
 // bulk-copy instructions per CTA.
 //
 // y and z lines: the tile's 32 lines are 32 consecutive points of the x index
-// (y lines) or of the flattened x-y index (z lines); one box of 32 points by
-// the N rows of the lines (a {32, N, 1} box of the 3-D field for y, a {32, N}
-// box of the [Nz][Nx*Ny] view for z) lands as N rows of 128 bytes with the
-// same swizzle, so the 32 lanes reading one row hit 32 banks. Plain and
+// (y lines) or of the flattened x-y index (z lines); boxes of 32 points by up
+// to 256 rows of the lines ({32, rows, 1} boxes of the 3-D field for y,
+// {32, rows} boxes of the [Nz][Nx*Ny] view for z; lines of 512 or 1024 take
+// two or four) land as N rows of 128 bytes with the same swizzle, so the 32
+// lanes reading one row hit 32 banks. Plain and
 // negated stores run persistent CTAs that load the next tile during the
 // solve and store directly (one 128-byte row per warp instruction); the
 // operations that read operands (accumulate, k2 assembly) run one CTA per
@@ -32,6 +33,7 @@ namespace mc3d {
 
 constexpr int TMA_MAXF = 8;   // fields per launch
 constexpr int TMA_BOX = 32;   // box edge: 32 x-values (128 bytes, the swizzle span) by 32 lines
+constexpr int TMA_ROWS = 256; // rows per box of a y/z tile (the largest box extent); longer lines take several
 
 struct TmaMaps {
     CUtensorMap in[TMA_MAXF];
@@ -105,22 +107,24 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
         c0 = blockIdx.x * W;
     }
     const unsigned bar_a = smem_u32(&bar);
-    // one box of `m` into the tile (thread 0)
+    // the tile's boxes of `m` (thread 0)
     auto load = [&](const CUtensorMap *m) {
         const unsigned long long tm = reinterpret_cast<unsigned long long>(m);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(N * 128) : "memory");
-        if (DIR == 1)
-            asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
-                "%4}], [%5];" ::"r"(smem_u32(tile)),
-                "l"(tm), "r"(c0), "r"(0), "r"(c2), "r"(bar_a)
-                : "memory");
-        else
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                "[%4];" ::"r"(smem_u32(tile)),
-                "l"(tm), "r"(c0), "r"(0), "r"(bar_a)
-                : "memory");
+        for (int r0 = 0; r0 < N; r0 += TMA_ROWS) {
+            if (DIR == 1)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3, %4}], [%5];" ::"r"(smem_u32(tile + r0 * 128)),
+                    "l"(tm), "r"(c0), "r"(r0), "r"(c2), "r"(bar_a)
+                    : "memory");
+            else
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3}], [%4];" ::"r"(smem_u32(tile + r0 * 128)),
+                    "l"(tm), "r"(c0), "r"(r0), "r"(bar_a)
+                    : "memory");
+        }
     };
     // bounded wait for the phase of the given parity; the CTA decides together
     auto wait = [&](unsigned parity) -> bool {
@@ -206,14 +210,17 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_kernel(Grid3 g, LineOpDev<fl
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned long long tm = reinterpret_cast<unsigned long long>(&maps.out[f]);
-        if (DIR == 1)
-            asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
-                         "r"(c0), "r"(0), "r"(c2), "r"(smem_u32(tile))
-                         : "memory");
-        else
-            asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tm),
-                         "r"(c0), "r"(0), "r"(smem_u32(tile))
-                         : "memory");
+        for (int r0 = 0; r0 < N; r0 += TMA_ROWS) {
+            if (DIR == 1)
+                asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::
+                                 "l"(tm),
+                             "r"(c0), "r"(r0), "r"(c2), "r"(smem_u32(tile + r0 * 128))
+                             : "memory");
+            else
+                asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tm),
+                             "r"(c0), "r"(r0), "r"(smem_u32(tile + r0 * 128))
+                             : "memory");
+        }
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
@@ -249,18 +256,20 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
         const int f = w / ntiles, tl = w - f * ntiles;
         const unsigned long long tm = reinterpret_cast<unsigned long long>(&maps.in[f]);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(N * 128) : "memory");
-        if (DIR == 1)
-            asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
-                "%4}], [%5];" ::"r"(smem_u32(tile)),
-                "l"(tm), "r"((tl % tx) * W), "r"(0), "r"(tl / tx), "r"(bar_a)
-                : "memory");
-        else
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                "[%4];" ::"r"(smem_u32(tile)),
-                "l"(tm), "r"(tl * W), "r"(0), "r"(bar_a)
-                : "memory");
+        for (int r0 = 0; r0 < N; r0 += TMA_ROWS) {
+            if (DIR == 1)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3, %4}], [%5];" ::"r"(smem_u32(tile + r0 * 128)),
+                    "l"(tm), "r"((tl % tx) * W), "r"(r0), "r"(tl / tx), "r"(bar_a)
+                    : "memory");
+            else
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3}], [%4];" ::"r"(smem_u32(tile + r0 * 128)),
+                    "l"(tm), "r"(tl * W), "r"(r0), "r"(bar_a)
+                    : "memory");
+        }
     };
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");

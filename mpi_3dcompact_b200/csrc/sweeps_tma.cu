@@ -1,4 +1,5 @@
 // TMA-staged line solves (kernels in sweep_tma.cuh): tensor maps and launches.
+#include <algorithm>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -68,18 +69,18 @@ bool tensor_map_x(const void *p, int nx, long long lines, CUtensorMap *out) {
     return tensor_map(p, 2, dims, strides, box, out);
 }
 
-// y lines: the [Nz][Ny][Nx] field with {32, Ny, 1} boxes; z lines: the
-// [Nz][Nx*Ny] view with {32, Nz} boxes
+// y lines: the [Nz][Ny][Nx] field with {32, min(Ny, 256), 1} boxes; z lines:
+// the [Nz][Nx*Ny] view with {32, min(Nz, 256)} boxes
 bool tensor_map_yz(int dir, const void *p, const Grid3 &g, CUtensorMap *out) {
     if (dir == 1) {
         const cuuint64_t dims[3] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz};
         const cuuint64_t strides[2] = {(cuuint64_t)g.Nx * 4, (cuuint64_t)g.Nx * g.Ny * 4};
-        const cuuint32_t box[3] = {(cuuint32_t)W, (cuuint32_t)g.Ny, 1};
+        const cuuint32_t box[3] = {(cuuint32_t)W, (cuuint32_t)std::min(g.Ny, TMA_ROWS), 1};
         return tensor_map(p, 3, dims, strides, box, out);
     }
     const cuuint64_t dims[2] = {(cuuint64_t)g.Nx * g.Ny, (cuuint64_t)g.Nz};
     const cuuint64_t strides[1] = {(cuuint64_t)g.Nx * g.Ny * 4};
-    const cuuint32_t box[2] = {(cuuint32_t)W, (cuuint32_t)g.Nz};
+    const cuuint32_t box[2] = {(cuuint32_t)W, (cuuint32_t)std::min(g.Nz, TMA_ROWS)};
     return tensor_map(p, 2, dims, strides, box, out);
 }
 
@@ -199,8 +200,9 @@ int launch_sweep_tma_yz(int dir, const Grid3 &g, const LineOpDev<float> &op, con
     if (!(epi == EPI_STORE || epi == EPI_STORE_NEG || epi == EPI_SUB || epi == EPI_RHS_FINAL || epi == EPI_STORE_F64))
         return MC3D_ERR_CONFIG;
     if (epi != EPI_STORE && epi != EPI_STORE_F64 && (px || py || pz)) return MC3D_ERR_CONFIG;
+    // lines up to 256 rows in one box, up to 1024 in boxes of 256 rows
     const int n = dir == 1 ? g.Ny : g.Nz;
-    if (op.L != 64 || op.N != n || n > 256) return MC3D_ERR_CONFIG;
+    if (op.L != 64 || op.N != n || n > 4 * TMA_ROWS || (n > TMA_ROWS && n % TMA_ROWS != 0)) return MC3D_ERR_CONFIG;
     if (b.nf < 1 || b.nf > TMA_MAXF) return MC3D_ERR_CONFIG;
     TmaMaps maps;
     // input tiles for every operation; the output (TMA store and previous

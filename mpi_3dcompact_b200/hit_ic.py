@@ -245,6 +245,21 @@ def hit_initial_condition(n: int, k0: float = 4.0, seed: int = 1, mt: float = 0.
     return [rho, u * s, v * s, w * s, p]
 
 
+def hit_initial_condition_device(n: int, k0: float = 4.0, seed: int = 1, mt: float = 0.3, gamma: float = 1.4,
+                                 device="cuda"):
+    """hit_initial_condition with the velocity drawn by hit_velocity_device,
+    returned as host numpy arrays (the solver takes host initial conditions);
+    for large n, where the numpy transform takes minutes."""
+    import torch
+    u, v, w = hit_velocity_device(n, k0, seed, device)
+    urms = math.sqrt(float((u * u + v * v + w * w).mean().item()))
+    s = mt / urms if urms > 0 else 0.0
+    vel = [(a * s).cpu().numpy() for a in (u, v, w)]
+    del u, v, w
+    torch.cuda.empty_cache()
+    return [np.ones((n, n, n)), vel[0], vel[1], vel[2], np.full((n, n, n), 1.0 / gamma)]
+
+
 def reynolds_lambda_mu(ic, L=2.0 * math.pi):
     """mu_ref giving Re_lambda for a target (helper for the HIT configurations):
     returns (u', lambda) where u' = rms of one component and lambda the Taylor

@@ -31,10 +31,11 @@ import numpy as np
 
 from . import _native as N
 from . import CurvilinearCSolver, MLPClosure, Options, Pade6, PERIODIC_SOLVE
-from .hit_ic import hit_initial_condition
+from .hit_ic import hit_initial_condition, hit_initial_condition_device
 
 C_RANGE = (-0.2, 0.5)      # clip of the pointwise least-squares coefficient
 PRT_RANGE = (0.1, 10.0)
+DEFAULT_FALLBACK_FRAC = 1e-3   # the library's LES.MLPFALLBACKFRAC default
 
 
 def _torch():
@@ -76,7 +77,8 @@ def training_pairs(q, n_fine, factor, box=2.0 * math.pi, mu_ref=1e-3):
 
 def dns_snapshots(n=128, seeds=(0,), steps=(20, 40), k0=4.0, mt=0.3, mu_ref=1e-3, precision=0):
     """Conserved-state snapshots (device FP64 tensors (n, n, n)) of HIT DNS runs
-    with the given seeds, taken after each count of time steps in `steps`."""
+    with the given seeds, taken after each count of time steps in `steps`
+    (initial fields from the device generator from 256^3 up)."""
     torch = _torch()
     out = []
     for seed in seeds:
@@ -84,7 +86,8 @@ def dns_snapshots(n=128, seeds=(0,), steps=(20, 40), k0=4.0, mt=0.3, mu_ref=1e-3
                       precision=precision)
         s = CurvilinearCSolver(opt)
         s.set_box_metrics(2.0 * math.pi)
-        s.set_initial_conditions(*hit_initial_condition(n, k0=k0, seed=seed, mt=mt))
+        gen = hit_initial_condition_device if n >= 256 else hit_initial_condition
+        s.set_initial_conditions(*gen(n, k0=k0, seed=seed, mt=mt))
         done = 0
         for target in steps:
             s.step(target - done)

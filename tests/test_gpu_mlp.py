@@ -92,10 +92,13 @@ def test_forward_matches_numpy():
     assert np.abs(yt.cpu().numpy() - ref).max() <= 1e-5 * scale
 
 
-def test_bf16_inference_matches_fp32():
+@pytest.mark.parametrize("n", [5, 10007, 300000])
+def test_bf16_inference_matches_fp32(n):
+    """The tcgen05 inference (tiles of 128 points, two per CTA) against the FP32
+    forward: one partial tile, a ragged last tile, and more tiles than the
+    persistent CTAs take in one round."""
     torch = _torch()
     mlp, P, mean, std, rng = _mlp_with_random_params(2)
-    n = 10007                                    # not a multiple of 32: ragged last tile
     x = torch.tensor(rng.standard_normal((n, 9)).astype(np.float32), device="cuda")
     y32 = torch.empty((n, 2), dtype=torch.float32, device="cuda")
     y16 = torch.empty_like(y32)

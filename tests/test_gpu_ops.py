@@ -101,10 +101,11 @@ def test_operator_errors_are_reported():
 
 @pytest.mark.parametrize("prec", [m.FP64, m.FP32BULK])
 @pytest.mark.parametrize("bc", [m.PERIODIC_SOLVE, m.DIRICHLET_SOLVE])
-@pytest.mark.parametrize("n", [64, 128, 192, 256])
+@pytest.mark.parametrize("n", [64, 128, 192, 256, 512, 1024])
 def test_segmented_lines_vs_oracle(n, bc, prec):
-    """Lines long enough for the segmented solve (2 to 8 segments per line;
-    FP32 lines of 128-256 points through the TMA-staged kernels, the other
+    """Lines long enough for the segmented solve (2 to 16 segments per line;
+    FP32 lines of 128-256 points through the TMA-staged kernels, y and z lines
+    of 512 and 1024 points through them in boxes of 256 rows, the other
     dimensions not multiples of the 32-line tile), every operator kind, every
     direction, against the oracle."""
     torch = _torch()
