@@ -313,7 +313,19 @@ def cylinder_block(args, local):
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     stages = s.info()["stages"] - st0
+    # per-class algorithmic bytes and device time of two more steps, for the
+    # HBM roofline of the configuration (every kernel class together)
+    s.set_timing(True)
+    s.step(2)
+    rep = s.timing_report()
+    s.set_timing(False)
     del s
+    peak, peak_kind = hbm_peak()
+    tot_b = sum(v["bytes"] for v in rep.values())
+    tot_ms = sum(v["ms"] for v in rep.values())
+    roof = {"bound": "hbm", "kernels": "all kernel classes of the step", "achieved": tot_b / (tot_ms * 1e-3) / 1e9,
+            "peak": peak, "unit": "GB/s", "frac": tot_b / (tot_ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_pt_stage": tot_b / (float(Nx * Ny * Nz) * (stages / args.cyl_steps) * 2)}
     sl, _ = make("LOCAL")
     local_steps = None
     for k in range(1, 4):
@@ -331,6 +343,7 @@ def cylinder_block(args, local):
         "metric": UNIT, "value": Nx * Ny * Nz * stages / (ms * 1e-3), "ms_per_step": ms / args.cyl_steps,
         "steps": args.cyl_steps, "averaging": "GLOBAL",
         "metrics_on_gpu_s": metrics_s,
+        "roofline": roof, "kernels": rep,
         "local_averaging_nonfinite_after_steps": local_steps,
         "note": "the configuration's LOCAL averaging divides by a locally filtered M_ij M_ij and goes non-finite "
                 "in the reference's own solver as well (128x64x32 O-grid, first step); radial ratio "

@@ -191,9 +191,10 @@ int mc3d_filter_create(int filter_type, double alphaF, int dir, const int bc_typ
 /* calc1stDerivField / filterField on `nfields` device fields at once:
  * out[f] = op(in[f]). `stream` is a cudaStream_t (NULL = legacy default).
  * in[f] and out[f] may not alias. FP32 lines of 128-256 points (y and z lines
- * also of 512 and 1024) go through the TMA-staged kernels. Lines up to 1024
- * points, except FP64 x lines above 768 (their 32-line tile does not fit in
- * shared memory): MC3D_ERR_CONFIG. Calls may overlap solver steps and other
+ * also of 512 and 1024) go through the TMA-staged kernels. Lines of up to
+ * 1024 points in FP32 and 512 in FP64 run in every direction; longer FP64
+ * lines run while the shared-memory tile of the 32 lines fits, and give
+ * MC3D_ERR_CONFIG beyond (1024 points). Calls may overlap solver steps and other
  * calls on other streams; each result is the same as when it runs alone. */
 int mc3d_op_apply(mc3d_op op, const void *const *in, void *const *out, int nfields, void *stream);
 

@@ -93,7 +93,12 @@ __device__ int g_mlp_wait_timeouts;
 // Per-CTA state: shared-memory base of the weight image (the activation
 // tiles follow it, TC_SLOTS per warpgroup), TMEM base, and per slot the
 // mbarrier of its MMAs; per warpgroup an abort word.
-constexpr int TC_SLOTS = 2;   // tiles in flight per warpgroup
+// Tiles in flight per warpgroup. Two (the MMAs of one tile overlapping the
+// activation work of the other) need 128 TMEM columns and 32 KB of tiles per
+// warpgroup, which leaves 16 warps per SM: 242 us per 128^3 pass against
+// 212 us with one tile and 24 warps per SM, whose other warpgroups hide the
+// MMA latency instead.
+constexpr int TC_SLOTS = 1;
 struct TcCta {
     unsigned char *img;
     unsigned tmem;
@@ -209,11 +214,11 @@ __device__ __forceinline__ void tc_issue(const TcCta &c, int sl, unsigned tile_s
     tc_commit((unsigned)__cvta_generic_to_shared(&c.bar[sl]));
 }
 
-// The network over tiles of 128 points, two tiles in flight per warpgroup:
-// while the MMAs of one tile's layer run, the warpgroup reads back, activates
-// and stores the other tile's previous layer. Thread r of warpgroup wg owns
-// point r of both tiles. Tile pairs p = pair0, pair0 + pstride, ...: tiles 2p
-// and 2p + 1 of ntiles. P provides
+// The network over tiles of 128 points, TC_SLOTS tiles in flight per
+// warpgroup (with two, the MMAs of one tile's layer run while the warpgroup
+// reads back, activates and stores the other tile's previous layer). Thread r
+// of warpgroup wg owns point r of each tile. Groups of TC_SLOTS tiles
+// p = pair0, pair0 + pstride, ...: tiles TC_SLOTS p + q of ntiles. P provides
 //   feature(i, xn, aux): the normalised layer-1 inputs of point i (any i,
 //                        called by every thread of the warp) and a value kept
 //                        for emit;
@@ -226,12 +231,15 @@ __device__ __forceinline__ void tc_issue(const TcCta &c, int sl, unsigned tile_s
 template <class P>
 __device__ __forceinline__ void tc_run(const TcCta &c, int wg, int r, long long ntiles, long long pair0,
                                        long long pstride, P &pol) {
-    unsigned char *tile[2];
-    unsigned tile_s[2], trow[2], bar[2], ph[2] = {0u, 0u};
-    bool pend[2] = {false, false};
+    constexpr int SL = TC_SLOTS;
+    unsigned char *tile[SL];
+    unsigned tile_s[SL], trow[SL], bar[SL], ph[SL];
+    bool pend[SL];
     const bool leader = r == 0;
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < SL; q++) {
+        ph[q] = 0u;
+        pend[q] = false;
         const int sl = wg * TC_SLOTS + q;
         tile[q] = c.img + MLPT_BYTES + sl * MLPT_TILE;
         tile_s[q] = (unsigned)__cvta_generic_to_shared(tile[q]);
@@ -262,12 +270,12 @@ __device__ __forceinline__ void tc_run(const TcCta &c, int wg, int r, long long 
         }
         tc_fence_after();
     };
-    float aux[2];
+    float aux[SL];
     bool stopped = false;
-    for (long long p = pair0; 2 * p < ntiles && !stopped; p += pstride) {
-        const long long i0 = 2 * p * 128 + r;
+    for (long long p = pair0; SL * p < ntiles && !stopped; p += pstride) {
+        const long long i0 = SL * p * 128 + r;
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
+        for (int q = 0; q < SL; q++) {
             float xn[MLP_IN];
             pol.feature(i0 + q * 128, xn, aux[q]);
             tc_put_input(tile[q], r, xn);
@@ -276,14 +284,14 @@ __device__ __forceinline__ void tc_run(const TcCta &c, int wg, int r, long long 
 #pragma unroll
         for (int layer = 2; layer <= 4; layer++)
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
+            for (int q = 0; q < SL; q++) {
                 wait(q);
                 tc_gelu_half(trow[q], tile[q], r, 0);
                 tc_gelu_half(trow[q], tile[q], r, 32);
                 stopped |= !sync_issue(q, layer);
             }
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
+        for (int q = 0; q < SL; q++) {
             wait(q);
             unsigned a, b;
             tc_ld2(trow[q], a, b);
@@ -297,7 +305,7 @@ __device__ __forceinline__ void tc_run(const TcCta &c, int wg, int r, long long 
     if (leader) {
         atomicAdd(&g_mlp_wait_timeouts, 1);
 #pragma unroll
-        for (int q = 0; q < 2; q++)
+        for (int q = 0; q < SL; q++)
             if (pend[q]) tc_mbar_wait(bar[q], ph[q]);
     }
 }

@@ -31,9 +31,9 @@ __device__ __forceinline__ float metf(const Metrics<R> &m, int c, long long i) {
     return (float)(m.constant ? m.c[c] : m.m[c][i]);
 }
 
-// Warpgroups per CTA of the tensor-core kernels: 256 threads and 94 KB of
-// shared memory per CTA (the weight image and four activation tiles, two per
-// warpgroup), so two CTAs share an SM and hold its 512 TMEM columns.
+// Warpgroups per CTA of the tensor-core kernels: 256 threads and 63.5 KB of
+// shared memory per CTA (the weight image and one activation tile per
+// warpgroup), so three CTAs share an SM and hold 384 of its 512 TMEM columns.
 constexpr int TC_NWG = 2;
 constexpr size_t TC_SMEM = 1024 + MLPT_BYTES + TC_NWG * TC_SLOTS * MLPT_TILE + 16 * TC_NWG * TC_SLOTS;
 
@@ -110,10 +110,10 @@ struct SgsPoints {
     }
 };
 
-// Persistent CTAs; warpgroup wg of CTA b takes the tile pairs b * TC_NWG + wg,
+// Persistent CTAs; warpgroup wg of CTA b takes the tile groups b * TC_NWG + wg,
 // stepping by gridDim.x * TC_NWG.
 template <typename R>
-__global__ void __launch_bounds__(TC_NWG * 128, 2)
+__global__ void __launch_bounds__(TC_NWG * 128, 3)
     sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f,
                    const __grid_constant__ DerivPtrs12c<R> dp, const __grid_constant__ Metrics<R> m, double dvol,
                    double mu_ref, const uint4 *__restrict__ img, const __grid_constant__ MlpNorm nrm, R *mu_sgs,
@@ -148,7 +148,7 @@ struct RawPoints {
     }
 };
 
-__global__ void __launch_bounds__(TC_NWG * 128, 2)
+__global__ void __launch_bounds__(TC_NWG * 128, 3)
     mlp_infer_kernel(const uint4 *__restrict__ img, const __grid_constant__ MlpNorm nrm, const float *__restrict__ x,
                      int n, float *__restrict__ out) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(TC_NWG * 128, 2)
 // grid of the persistent tensor-core kernels: as many CTAs as fit on the SMs
 // together (shared memory, registers, threads, TMEM columns; counted here from
 // the kernel's attributes, with the largest shared-memory carveout requested),
-// and no more than there are tile pairs per warpgroup
+// and no more than there are tile groups per warpgroup
 template <typename K>
 int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
     if (int rc = open_kernel(kern, st, TC_SMEM, TC_NWG * 128, nullptr)) return rc;
@@ -182,7 +182,7 @@ int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
     int per = std::min(smem_sm / (int)(TC_SMEM + resv), thr_sm / threads);
     if (fa.numRegs > 0) per = std::min(per, regs_sm / (fa.numRegs * threads));
     per = std::max(1, std::min(per, 512 / (TC_NWG * TC_SLOTS * MLPT_NCOL)));
-    const long long need = (n + 256LL * TC_NWG - 1) / (256LL * TC_NWG);
+    const long long need = (n + 128LL * TC_SLOTS * TC_NWG - 1) / (128LL * TC_SLOTS * TC_NWG);
     *blocks = (int)std::max(1LL, std::min<long long>(need, (long long)nsm * per));
     return MC3D_OK;
 }

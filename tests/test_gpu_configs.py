@@ -23,6 +23,9 @@ where it was never built).
   well-conditioned states both measures are ~1e-14 and the bound is 1e-12;
   on the 32^3 states with the Pade test filter the reference's momentum moves
   by 1e-8..1e-7 after one step.
+* DSM without averaging (NONE): the reference reads averaged work arrays it
+  never wrote and is NaN everywhere after one step; the GPU computes the
+  pointwise coefficient and follows the oracle's restatement.
 * O-grid cylinder with DSM LOCAL: on 64 x 32 x 16 the GPU follows the
   reference for one step under the same rule (metrics from the reference); on
   128 x 64 x 32 both go non-finite within the first two steps (the
@@ -99,6 +102,40 @@ def test_dsm_local_averaging_matches_reference(n, tf, steps):
         assert err <= max(1e-12, 5 * gap), (i, err, gap)
     if n == 16:
         assert gap < 1e-12   # well conditioned: the plain FP64 bound applies
+
+
+@pytest.mark.parametrize("tf", [1, 2])
+def test_dsm_without_averaging_follows_the_restatement(tf):
+    """DSM with LESAVERAGING = NONE. The reference's doAveraging leaves its
+    output unwritten for NONE (src/AbstractSGS.cpp:160-162), and DSMSGS
+    averages into separate work arrays (src/DSMSGS.hpp:306-316), so the
+    reference divides arrays it never wrote: in the harness (zero-filled
+    allocations) 0/0, NaN everywhere after one step (tests/test_oracle.py).
+    Here NONE means no averaging, the pointwise coefficient, as the oracle's
+    restatement has it: the GPU state after one step is finite and within
+    max(1e-12, 5 x the restatement's own one-ulp sensitivity) of it."""
+    n = 16
+    ic = hit_initial_condition(n, k0=4.0, seed=3, mt=0.3)
+    cfg = O.Config(N=(n,) * 3, fd=("PADE6",) * 3, filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=0.005,
+                   les="DSM", les_avg="NONE", dsm_test_filter=tf)
+    qr, _ = R.run_solver(cfg, ic, 1)
+    assert all(np.isnan(a).all() for a in qr)
+    qo, _ = O.run(cfg, ic, 1)
+    assert all(np.isfinite(a).all() for a in qo)
+    rng = np.random.default_rng(1)
+    icp = [np.nextafter(a, np.where(rng.random(a.shape) < 0.5, -np.inf, np.inf)) if i in (1, 2, 3) else a
+           for i, a in enumerate(ic)]
+    qp, _ = O.run(cfg, icp, 1)
+    sens = max(H.rel_max(qp[i], qo[i]) for i in range(5))
+    s = m.CurvilinearCSolver(_opts(cfg))
+    s.set_box_metrics(2 * math.pi)
+    s.set_initial_conditions(*ic)
+    s.step(1)
+    q = s.conserved()
+    for i in range(5):
+        assert np.isfinite(q[i]).all()
+        err = H.rel_max(q[i], qo[i])
+        assert err <= max(1e-12, 5 * sens), (i, err, sens)
 
 
 def _ogrid_cfg(Nx, Ny, Nz):

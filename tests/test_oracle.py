@@ -242,6 +242,26 @@ def test_reference_ogrid_dsm_local_nonfinite_at_128x64x32():
     assert np.isfinite(q[0]).all() and not any(np.isfinite(a).all() for a in q[1:])
 
 
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref/mc3d_ref not built")
+@pytest.mark.parametrize("tf", [1, 2])
+def test_reference_dsm_without_averaging_is_nonfinite(tf):
+    """The reference's own solver with DSM and LESAVERAGING = NONE (either test
+    filter) on a 16^3 HIT state: every value of every conserved field is NaN
+    after one time step. doAveraging does nothing for NONE
+    (src/AbstractSGS.cpp:160-162) while DSMSGS reads the averages from separate
+    work arrays (src/DSMSGS.hpp:306-316), which nothing wrote: with the
+    harness's zero-filled allocations the coefficient is 0/0. The GPU path
+    takes NONE as no averaging (tests/test_gpu_configs.py)."""
+    from mpi_3dcompact_b200.hit_ic import hit_initial_condition
+    n = 16
+    ic = hit_initial_condition(n, k0=4.0, seed=3, mt=0.3)
+    cfg = O.Config(N=(n,) * 3, fd=("PADE6",) * 3, filter="COMPACT10", alphaF=0.49, rk="RK4", mu_ref=0.005,
+                   les="DSM", les_avg="NONE", dsm_test_filter=tf)
+    q, info = R.run_solver(cfg, ic, 1)
+    assert info["time_step"] == 1
+    assert all(np.isnan(a).all() for a in q)
+
+
 def test_device_hit_generator_matches_numpy():
     """hit_velocity_device (the generator used for the 1024^3 block) draws the
     same LCG sequence as the numpy restatement, bit for bit, and gives the same
