@@ -90,20 +90,13 @@ __device__ __forceinline__ bool tc_mbar_wait(unsigned bar, unsigned parity) {
 // CTAs whose MMA completion did not arrive within the wait limit
 __device__ int g_mlp_wait_timeouts;
 
-// Per-CTA state: shared-memory base of the weight image (the activation
-// tiles follow it, TC_SLOTS per warpgroup), TMEM base, and per slot the
-// mbarrier of its MMAs; per warpgroup an abort word.
-// Tiles in flight per warpgroup. Two (the MMAs of one tile overlapping the
-// activation work of the other) need 128 TMEM columns and 32 KB of tiles per
-// warpgroup, which leaves 16 warps per SM: 242 us per 128^3 pass against
-// 212 us with one tile and 24 warps per SM, whose other warpgroups hide the
-// MMA latency instead.
-constexpr int TC_SLOTS = 1;
+// Per-CTA state: shared-memory base of the weight image, TMEM base, and per
+// warpgroup the activation tile, the mbarrier, its phase and a status word.
 struct TcCta {
-    unsigned char *img;
+    unsigned char *img;   // MLPT_BYTES, then NWG activation tiles
     unsigned tmem;
     unsigned long long *bar;
-    int *abort;
+    int *status;
 };
 
 // Carve the dynamic shared memory, copy the weight image, allocate TMEM
@@ -113,24 +106,25 @@ __device__ __forceinline__ TcCta tc_setup(unsigned char *smem_raw, const uint4 *
     TcCta c;
     const unsigned base = (unsigned)__cvta_generic_to_shared(smem_raw);
     c.img = smem_raw + ((1024u - (base & 1023u)) & 1023u);
-    unsigned char *tail = c.img + MLPT_BYTES + NWG * TC_SLOTS * MLPT_TILE;
+    unsigned char *tail = c.img + MLPT_BYTES + NWG * MLPT_TILE;
     c.bar = reinterpret_cast<unsigned long long *>(tail);
-    c.abort = reinterpret_cast<int *>(tail + 8 * NWG * TC_SLOTS);
-    unsigned *tslot = reinterpret_cast<unsigned *>(tail + 8 * NWG * TC_SLOTS + 4 * NWG);
+    c.status = reinterpret_cast<int *>(tail + 8 * NWG);
+    unsigned *tslot = reinterpret_cast<unsigned *>(tail + 12 * NWG);
     uint4 *dst = reinterpret_cast<uint4 *>(c.img);
     for (int k = threadIdx.x; k < MLPT_BYTES / 16; k += blockDim.x) dst[k] = image[k];
     if (threadIdx.x < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          (unsigned)__cvta_generic_to_shared(tslot)),
-                     "r"(NWG * TC_SLOTS * MLPT_NCOL)
+                     "r"(NWG * MLPT_NCOL)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        for (int w = 0; w < NWG * TC_SLOTS; w++)
+        for (int w = 0; w < NWG; w++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&c.bar[w]))
                          : "memory");
-        for (int w = 0; w < NWG; w++) c.abort[w] = 0;
+            c.status[w] = 1;
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_proxy_fence();
@@ -141,16 +135,15 @@ __device__ __forceinline__ TcCta tc_setup(unsigned char *smem_raw, const uint4 *
     return c;
 }
 
-// Every thread of the CTA, after its warpgroup's last wait: warp 0 frees the
-// TMEM columns.
+// Every thread of the CTA: wait for the last MMAs of warpgroups that gave up
+// (bounded), then warp 0 frees the TMEM columns.
 template <int NWG>
 __device__ __forceinline__ void tc_teardown(const TcCta &c) {
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (threadIdx.x < 32)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem),
-                     "r"(NWG * TC_SLOTS * MLPT_NCOL)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem), "r"(NWG * MLPT_NCOL)
                      : "memory");
 }
 
@@ -192,12 +185,12 @@ __device__ __forceinline__ void tc_gelu_half(unsigned taddr, unsigned char *tile
     }
 }
 
-// One thread: the MMAs of `layer` on the tile of slot `sl` (activation tile at
-// shared address tile_s, accumulator at TMEM column sl * 64), then the commit
-// that arrives on the slot's mbarrier when they are done.
-__device__ __forceinline__ void tc_issue(const TcCta &c, int sl, unsigned tile_s, int layer) {
+// Issue (one thread) the MMAs of a layer and wait for them; the status word
+// tells the warpgroup whether they completed within the wait limit.
+__device__ __forceinline__ void tc_layer_issue(const TcCta &c, int wg, unsigned tile_s, int layer, unsigned &phase) {
     const unsigned img = (unsigned)__cvta_generic_to_shared(c.img);
-    const unsigned d = c.tmem + (unsigned)(sl * MLPT_NCOL);
+    const unsigned d = c.tmem + (unsigned)(wg * MLPT_NCOL);
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&c.bar[wg]);
     tc_fence_after();
     if (layer == 1) {
         tc_mma(d, tc_desc(tile_s, 128, 1024), tc_desc(img + MLPT_W1, 128, 256), tc_idesc(64), 0u);
@@ -211,103 +204,53 @@ __device__ __forceinline__ void tc_issue(const TcCta &c, int sl, unsigned tile_s
                    kk > 0 ? 1u : 0u);
         tc_mma(d, tc_desc(img + MLPT_AC, 128, 256), tc_desc(img + b, 128, 256), id, 1u);
     }
-    tc_commit((unsigned)__cvta_generic_to_shared(&c.bar[sl]));
+    tc_commit(bar);
+    const bool ok = tc_mbar_wait(bar, phase);
+    if (!ok) {
+        atomicAdd(&g_mlp_wait_timeouts, 1);
+        tc_mbar_wait(bar, phase);   // once more, for the copies still in flight
+    }
+    c.status[wg] = ok ? 1 : 0;
 }
 
-// The network over tiles of 128 points, TC_SLOTS tiles in flight per
-// warpgroup (with two, the MMAs of one tile's layer run while the warpgroup
-// reads back, activates and stores the other tile's previous layer). Thread r
-// of warpgroup wg owns point r of each tile. Groups of TC_SLOTS tiles
-// p = pair0, pair0 + pstride, ...: tiles TC_SLOTS p + q of ntiles. P provides
-//   feature(i, xn, aux): the normalised layer-1 inputs of point i (any i,
-//                        called by every thread of the warp) and a value kept
-//                        for emit;
-//   emit(i, o0, o1, aux): the raw outputs of point i (called for every i; the
-//                        policy skips points past the end).
-// Every thread waits on the slot's mbarrier itself (bounded); a wait that
-// gives up raises the warpgroup's abort word, which every thread reads after
-// the next warpgroup barrier, so the warpgroup stops together and the issuing
-// thread drains the MMAs still in flight (bounded) before the TMEM is freed.
-template <class P>
-__device__ __forceinline__ void tc_run(const TcCta &c, int wg, int r, long long ntiles, long long pair0,
-                                       long long pstride, P &pol) {
-    constexpr int SL = TC_SLOTS;
-    unsigned char *tile[SL];
-    unsigned tile_s[SL], trow[SL], bar[SL], ph[SL];
-    bool pend[SL];
+// The network on the warpgroup's tile whose layer-1 inputs the 128 threads
+// have written (row r = this thread's point). Returns false, uniformly over
+// the warpgroup, when an MMA did not complete in time; otherwise the two raw
+// outputs of row r. One tile per warpgroup and three CTAs of two warpgroups
+// per SM; the issuing thread alone waits on the mbarrier while the others
+// wait at the warpgroup barrier. Measured alternatives on the 128^3 pass (212
+// us here): every thread polling the mbarrier, 227 us (the polling takes
+// issue slots); two tiles in flight per warpgroup, the MMAs of one under the
+// activation work of the other, 242 us (128 TMEM columns and 32 KB of tiles
+// per warpgroup leave 16 warps per SM instead of 24).
+__device__ __forceinline__ bool tc_forward(const TcCta &c, int wg, int r, unsigned &phase, float &o0, float &o1) {
+    unsigned char *tile = c.img + MLPT_BYTES + wg * MLPT_TILE;
+    const unsigned tile_s = (unsigned)__cvta_generic_to_shared(tile);
+    const unsigned trow = c.tmem + ((unsigned)(r & ~31) << 16) + (unsigned)(wg * MLPT_NCOL);
     const bool leader = r == 0;
-#pragma unroll
-    for (int q = 0; q < SL; q++) {
-        ph[q] = 0u;
-        pend[q] = false;
-        const int sl = wg * TC_SLOTS + q;
-        tile[q] = c.img + MLPT_BYTES + sl * MLPT_TILE;
-        tile_s[q] = (unsigned)__cvta_generic_to_shared(tile[q]);
-        trow[q] = c.tmem + ((unsigned)(r & ~31) << 16) + (unsigned)(sl * MLPT_NCOL);
-        bar[q] = (unsigned)__cvta_generic_to_shared(&c.bar[sl]);
-    }
-    // the tile of slot q is in the operand buffer: barrier, then issue
-    // (false, and nothing issued, once the warpgroup has aborted)
-    auto sync_issue = [&](int q, int layer) -> bool {
+#pragma unroll 1
+    for (int layer = 1; layer <= 4; layer++) {
+        if (layer > 1) {
+            tc_gelu_half(trow, tile, r, 0);
+            tc_gelu_half(trow, tile, r, 32);
+        }
         tc_proxy_fence();
         tc_fence_before();
         wg_bar(wg);
+        if (leader) tc_layer_issue(c, wg, tile_s, layer, phase);
+        phase ^= 1u;
+        wg_bar(wg);
         tc_fence_after();
-        if (c.abort[wg]) return false;
-        if (leader) tc_issue(c, wg * TC_SLOTS + q, tile_s[q], layer);
-        pend[q] = true;
-        return true;
-    };
-    // (a wait that gives up keeps its parity and the slot pending, for the
-    // drain; after an abort the waits are skipped)
-    auto wait = [&](int q) {
-        if (!pend[q] || c.abort[wg]) return;
-        if (tc_mbar_wait(bar[q], ph[q])) {
-            pend[q] = false;
-            ph[q] ^= 1u;
-        } else {
-            c.abort[wg] = 1;
-        }
-        tc_fence_after();
-    };
-    float aux[SL];
-    bool stopped = false;
-    for (long long p = pair0; SL * p < ntiles && !stopped; p += pstride) {
-        const long long i0 = SL * p * 128 + r;
-#pragma unroll
-        for (int q = 0; q < SL; q++) {
-            float xn[MLP_IN];
-            pol.feature(i0 + q * 128, xn, aux[q]);
-            tc_put_input(tile[q], r, xn);
-            stopped |= !sync_issue(q, 1);
-        }
-#pragma unroll
-        for (int layer = 2; layer <= 4; layer++)
-#pragma unroll
-            for (int q = 0; q < SL; q++) {
-                wait(q);
-                tc_gelu_half(trow[q], tile[q], r, 0);
-                tc_gelu_half(trow[q], tile[q], r, 32);
-                stopped |= !sync_issue(q, layer);
-            }
-#pragma unroll
-        for (int q = 0; q < SL; q++) {
-            wait(q);
-            unsigned a, b;
-            tc_ld2(trow[q], a, b);
-            tc_wait_ld();
-            tc_fence_before();
-            if (!stopped) pol.emit(i0 + q * 128, __uint_as_float(a), __uint_as_float(b), aux[q]);
-        }
+        if (!c.status[wg]) return false;
     }
-    wg_bar(wg);   // a wait of the last pair that gave up
-    if (!c.abort[wg]) return;
-    if (leader) {
-        atomicAdd(&g_mlp_wait_timeouts, 1);
-#pragma unroll
-        for (int q = 0; q < SL; q++)
-            if (pend[q]) tc_mbar_wait(bar[q], ph[q]);
-    }
+    unsigned a, b;
+    tc_ld2(trow, a, b);
+    tc_wait_ld();
+    tc_fence_before();
+    o0 = __uint_as_float(a);
+    o1 = __uint_as_float(b);
+    return true;
 }
+
 
 }  // namespace mc3d

@@ -32,33 +32,35 @@ __device__ __forceinline__ float metf(const Metrics<R> &m, int c, long long i) {
 }
 
 // Warpgroups per CTA of the tensor-core kernels: 256 threads and 63.5 KB of
-// shared memory per CTA (the weight image and one activation tile per
-// warpgroup), so three CTAs share an SM and hold 384 of its 512 TMEM columns.
+// shared memory per CTA (the weight image and two activation tiles), so three
+// CTAs share an SM and hold 3 x 128 of its 512 TMEM columns.
 constexpr int TC_NWG = 2;
-constexpr size_t TC_SMEM = 1024 + MLPT_BYTES + TC_NWG * TC_SLOTS * MLPT_TILE + 16 * TC_NWG * TC_SLOTS;
+constexpr size_t TC_SMEM = 1024 + MLPT_BYTES + TC_NWG * MLPT_TILE + 16 * TC_NWG;
 
 // Fused closure evaluation: features of every point, the network on the
 // tensor cores, mu_sgs and k_sgs; *flag counts the points with a feature
 // outside the training range (those features are clamped to the range before
-// the network).
+// the network). Persistent CTAs; each warpgroup walks tiles of 128 points,
+// thread r of the warpgroup owning point r of the tile.
 template <typename R>
-struct SgsPoints {
-    Grid3 g;
-    const R *__restrict__ rho_f;
-    const R *__restrict__ T_f;
-    const DerivPtrs12c<R> &dp;
-    const Metrics<R> &m;
-    double dvol, mu_ref;
-    const MlpNorm &nrm;
-    R *mu_sgs, *ksgs;
-    int *flag;
-    float delta_c;   // Delta of a uniform block
-    long long n;
-
-    __device__ __forceinline__ void feature(long long i, float (&xn)[MLP_IN], float &scale) {
+__global__ void __launch_bounds__(TC_NWG * 128, 3)
+    sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f, DerivPtrs12c<R> dp,
+                   Metrics<R> m, double dvol, double mu_ref, const uint4 *__restrict__ img, MlpNorm nrm, R *mu_sgs,
+                   R *ksgs, int *flag) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const TcCta c = tc_setup<TC_NWG>(smem_raw, img);
+    const int wg = threadIdx.x >> 7, r = threadIdx.x & 127, lane = threadIdx.x & 31;
+    unsigned char *tile = c.img + MLPT_BYTES + wg * MLPT_TILE;
+    unsigned phase = 0;
+    const long long n = g.n(), ntiles = (n + 127) / 128;
+    const float delta_c = m.constant ? cbrtf((float)(dvol / (double)m.c[0])) : 0.f;   // Delta of a uniform block
+    for (long long t = (long long)blockIdx.x * TC_NWG + wg; t < ntiles; t += (long long)gridDim.x * TC_NWG) {
+        const long long i = t * 128 + r;
+        const bool ok = i < n;
+        double scale = 0.0;
         bool out_of_range = false;
-        scale = 0.0f;
-        if (i < n) {
+        float xn[MLP_IN];
+        if (ok) {
             float gu[3][3], gT[3];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
@@ -86,7 +88,7 @@ struct SgsPoints {
                     const float sab = 0.5f * (gu[a][b] + gu[b][a]);
                     s2 += sab * sab;
                 }
-            scale = rhof * delta * delta * sqrtf(2.0f * s2);   // mu_t / C
+            scale = (double)(rhof * delta * delta * sqrtf(2.0f * s2));   // mu_t / C
 #pragma unroll
             for (int k = 0; k < MLP_IN; k++) {
                 if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;   // NaN counts as outside
@@ -98,72 +100,52 @@ struct SgsPoints {
             for (int k = 0; k < MLP_IN; k++) xn[k] = 0.0f;
         }
         const unsigned outside = __ballot_sync(0xffffffffu, out_of_range);
-        if (outside && (threadIdx.x & 31) == 0) atomicAdd(flag, __popc(outside));
+        if (outside && lane == 0) atomicAdd(flag, __popc(outside));
+        tc_put_input(tile, r, xn);
+        float o0, o1;
+        if (!tc_forward(c, wg, r, phase, o0, o1)) break;
+        if (ok) {
+            const double C = fmax(0.0, (double)o0 * nrm.ystd[0] + nrm.ymean[0]);
+            const double prt = fmin(10.0, fmax(0.1, (double)o1 * nrm.ystd[1] + nrm.ymean[1]));
+            const double mt = C * scale;
+            mu_sgs[i] = (R)mt;
+            ksgs[i] = (R)(CP * mt / prt);
+        }
     }
-    __device__ __forceinline__ void emit(long long i, float o0, float o1, float scale) {
-        if (i >= n) return;
-        const double C = fmax(0.0, (double)o0 * nrm.ystd[0] + nrm.ymean[0]);
-        const double prt = fmin(10.0, fmax(0.1, (double)o1 * nrm.ystd[1] + nrm.ymean[1]));
-        const double mt = C * (double)scale;
-        mu_sgs[i] = (R)mt;
-        ksgs[i] = (R)(CP * mt / prt);
-    }
-};
-
-// Persistent CTAs; warpgroup wg of CTA b takes the tile groups b * TC_NWG + wg,
-// stepping by gridDim.x * TC_NWG.
-template <typename R>
-__global__ void __launch_bounds__(TC_NWG * 128, 3)
-    sgs_mlp_kernel(Grid3 g, const R *__restrict__ rho_f, const R *__restrict__ T_f,
-                   const __grid_constant__ DerivPtrs12c<R> dp, const __grid_constant__ Metrics<R> m, double dvol,
-                   double mu_ref, const uint4 *__restrict__ img, const __grid_constant__ MlpNorm nrm, R *mu_sgs,
-                   R *ksgs, int *flag) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    const TcCta c = tc_setup<TC_NWG>(smem_raw, img);
-    const int wg = threadIdx.x >> 7, r = threadIdx.x & 127;
-    SgsPoints<R> pol{g,      rho_f, T_f,  dp,   m,
-                     dvol,   mu_ref, nrm, mu_sgs, ksgs,
-                     flag,   m.constant ? cbrtf((float)(dvol / (double)m.c[0])) : 0.f, g.n()};
-    const long long ntiles = (g.n() + 127) / 128;
-    tc_run(c, wg, r, ntiles, (long long)blockIdx.x * TC_NWG + wg, (long long)gridDim.x * TC_NWG, pol);
     tc_teardown<TC_NWG>(c);
 }
 
 // standalone inference: x [n][9] (raw features, normalised without clamping)
 // -> out [n][2] (raw outputs)
-struct RawPoints {
-    const MlpNorm &nrm;
-    const float *__restrict__ x;
-    float *__restrict__ out;
-    long long n;
-    __device__ __forceinline__ void feature(long long p, float (&xn)[MLP_IN], float &aux) {
-        aux = 0.0f;
-#pragma unroll
-        for (int k = 0; k < MLP_IN; k++) xn[k] = p < n ? (x[p * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k] : 0.0f;
-    }
-    __device__ __forceinline__ void emit(long long p, float o0, float o1, float) {
-        if (p >= n) return;
-        out[p * 2 + 0] = o0;
-        out[p * 2 + 1] = o1;
-    }
-};
-
 __global__ void __launch_bounds__(TC_NWG * 128, 3)
-    mlp_infer_kernel(const uint4 *__restrict__ img, const __grid_constant__ MlpNorm nrm, const float *__restrict__ x,
-                     int n, float *__restrict__ out) {
+    mlp_infer_kernel(const uint4 *__restrict__ img, MlpNorm nrm, const float *__restrict__ x, int n,
+                     float *__restrict__ out) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const TcCta c = tc_setup<TC_NWG>(smem_raw, img);
     const int wg = threadIdx.x >> 7, r = threadIdx.x & 127;
-    RawPoints pol{nrm, x, out, (long long)n};
+    unsigned char *tile = c.img + MLPT_BYTES + wg * MLPT_TILE;
+    unsigned phase = 0;
     const long long ntiles = ((long long)n + 127) / 128;
-    tc_run(c, wg, r, ntiles, (long long)blockIdx.x * TC_NWG + wg, (long long)gridDim.x * TC_NWG, pol);
+    for (long long t = (long long)blockIdx.x * TC_NWG + wg; t < ntiles; t += (long long)gridDim.x * TC_NWG) {
+        const long long p = t * 128 + r;
+        float xn[MLP_IN];
+#pragma unroll
+        for (int k = 0; k < MLP_IN; k++) xn[k] = p < n ? (x[p * MLP_IN + k] - nrm.mean[k]) * nrm.inv_std[k] : 0.0f;
+        tc_put_input(tile, r, xn);
+        float o0, o1;
+        if (!tc_forward(c, wg, r, phase, o0, o1)) break;
+        if (p < n) {
+            out[p * 2 + 0] = o0;
+            out[p * 2 + 1] = o1;
+        }
+    }
     tc_teardown<TC_NWG>(c);
 }
 
 // grid of the persistent tensor-core kernels: as many CTAs as fit on the SMs
 // together (shared memory, registers, threads, TMEM columns; counted here from
 // the kernel's attributes, with the largest shared-memory carveout requested),
-// and no more than there are tile groups per warpgroup
+// and no more than there are tile pairs
 template <typename K>
 int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
     if (int rc = open_kernel(kern, st, TC_SMEM, TC_NWG * 128, nullptr)) return rc;
@@ -181,8 +163,8 @@ int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
     const int threads = TC_NWG * 128;
     int per = std::min(smem_sm / (int)(TC_SMEM + resv), thr_sm / threads);
     if (fa.numRegs > 0) per = std::min(per, regs_sm / (fa.numRegs * threads));
-    per = std::max(1, std::min(per, 512 / (TC_NWG * TC_SLOTS * MLPT_NCOL)));
-    const long long need = (n + 128LL * TC_SLOTS * TC_NWG - 1) / (128LL * TC_SLOTS * TC_NWG);
+    per = std::max(1, std::min(per, 512 / (TC_NWG * MLPT_NCOL)));
+    const long long need = (n + 128LL * TC_NWG - 1) / (128LL * TC_NWG);
     *blocks = (int)std::max(1LL, std::min<long long>(need, (long long)nsm * per));
     return MC3D_OK;
 }
