@@ -75,9 +75,11 @@ __device__ __forceinline__ unsigned gelu_bf16x2(unsigned x) {
 }
 
 // Features of one point (see sgs_mlp.cu), in FP32: the inference and the
-// training data both use this function.
-__device__ __forceinline__ void mlp_features(const float gu[3][3], float rho, float T, const float gT[3], float delta,
-                                             float mu, float *x) {
+// training data both use this function. Quotients by the hardware reciprocal
+// (__fdividef, 2 ulp), logarithm and square roots as the library rounds them;
+// returns |S| = (2 S:S)^(1/2).
+__device__ __forceinline__ float mlp_features(const float gu[3][3], float rho, float T, const float gT[3], float delta,
+                                              float mu, float *x) {
     float S[3][3], Wm[3][3];
     float s2 = 0.f, w2 = 0.f;
 #pragma unroll
@@ -106,18 +108,20 @@ __device__ __forceinline__ void mlp_features(const float gu[3][3], float rho, fl
             trS2W2 += p * q;
         }
     const float eps = 1e-30f, sw = s2 + w2;
-    const float smag = sqrtf(2.0f * s2);
+    const float rs = sqrtf(s2), rsw = sqrtf(sw);
+    const float smag = 1.41421356f * rs;
     const float c = sqrtf((float)(GAMMA * R_GAS) * T);
     const float gTm = sqrtf(gT[0] * gT[0] + gT[1] * gT[1] + gT[2] * gT[2]);
-    x[0] = log1pf(rho * delta * delta * smag / mu);
-    x[1] = w2 / (sw + eps);
-    x[2] = trS3 / (s2 * sqrtf(s2) + eps);
-    x[3] = trSW2 / (sw * sqrtf(sw) + eps);
-    x[4] = trS2W2 / (sw * sw + eps);
-    x[5] = (gu[0][0] + gu[1][1] + gu[2][2]) / (sqrtf(sw) + eps);
-    x[6] = delta * gTm / T;
-    x[7] = delta * smag / c;
+    x[0] = log1pf(__fdividef(rho * delta * delta * smag, mu));
+    x[1] = __fdividef(w2, sw + eps);
+    x[2] = __fdividef(trS3, s2 * rs + eps);
+    x[3] = __fdividef(trSW2, sw * rsw + eps);
+    x[4] = __fdividef(trS2W2, sw * sw + eps);
+    x[5] = __fdividef(gu[0][0] + gu[1][1] + gu[2][2], rsw + eps);
+    x[6] = __fdividef(delta * gTm, T);
+    x[7] = __fdividef(delta * smag, c);
     x[8] = logf(rho);
+    return smag;
 }
 
 }  // namespace mc3d

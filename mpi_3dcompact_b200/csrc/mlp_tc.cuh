@@ -8,9 +8,8 @@
 // lane = point, column = output). The accumulator of a layer is read back by
 // the warpgroup's own threads (tcgen05.ld, thread = point), rounded to BF16
 // pairs, put through the GELU in packed BF16 arithmetic in registers and
-// written into the operand tile of the next
-// layer, whose MMAs one thread then issues; tcgen05.commit on an mbarrier
-// signals their completion. The biases ride on the tensor cores: layer 1's
+// written into the operand tile of the next layer, whose MMAs one thread then
+// issues; tcgen05.commit on an mbarrier signals their completion. The biases ride on the tensor cores: layer 1's
 // input carries two constant-one columns against the rows (b_hi, b_lo) of W1
 // (b = b_hi + b_lo to 16 bits), the other layers add Ac B_l with the same two
 // columns. Operands use the K-major layout without swizzle: 8-row core

@@ -33,7 +33,9 @@ __device__ __forceinline__ float metf(const Metrics<R> &m, int c, long long i) {
 
 // Warpgroups per CTA of the tensor-core kernels: 256 threads and 63.5 KB of
 // shared memory per CTA (the weight image and two activation tiles), so three
-// CTAs share an SM and hold 3 x 128 of its 512 TMEM columns.
+// CTAs share an SM and hold 3 x 128 of its 512 TMEM columns. (Four warpgroups
+// per CTA at 64 registers, two CTAs and 32 warps per SM, took 220 us per
+// 128^3 pass against 212 us: more instructions at the lower register count.)
 constexpr int TC_NWG = 2;
 constexpr size_t TC_SMEM = 1024 + MLPT_BYTES + TC_NWG * MLPT_TILE + 16 * TC_NWG;
 
@@ -57,7 +59,7 @@ __global__ void __launch_bounds__(TC_NWG * 128, 3)
     for (long long t = (long long)blockIdx.x * TC_NWG + wg; t < ntiles; t += (long long)gridDim.x * TC_NWG) {
         const long long i = t * 128 + r;
         const bool ok = i < n;
-        double scale = 0.0;
+        float scale = 0.0f;
         bool out_of_range = false;
         float xn[MLP_IN];
         if (ok) {
@@ -79,16 +81,8 @@ __global__ void __launch_bounds__(TC_NWG * 128, 3)
             const float delta = m.constant ? delta_c : cbrtf((float)dvol / metf(m, 0, i));
             const float mu = (float)mu_ref * __powf(T, 0.76f);
             float x[MLP_IN];
-            mlp_features(gu, rhof, T, gT, delta, mu, x);
-            float s2 = 0.f;
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int b = 0; b < 3; b++) {
-                    const float sab = 0.5f * (gu[a][b] + gu[b][a]);
-                    s2 += sab * sab;
-                }
-            scale = (double)(rhof * delta * delta * sqrtf(2.0f * s2));   // mu_t / C
+            const float smag = mlp_features(gu, rhof, T, gT, delta, mu, x);
+            scale = rhof * delta * delta * smag;   // mu_t / C
 #pragma unroll
             for (int k = 0; k < MLP_IN; k++) {
                 if (!(x[k] >= nrm.lo[k] && x[k] <= nrm.hi[k])) out_of_range = true;   // NaN counts as outside
@@ -105,11 +99,11 @@ __global__ void __launch_bounds__(TC_NWG * 128, 3)
         float o0, o1;
         if (!tc_forward(c, wg, r, phase, o0, o1)) break;
         if (ok) {
-            const double C = fmax(0.0, (double)o0 * nrm.ystd[0] + nrm.ymean[0]);
-            const double prt = fmin(10.0, fmax(0.1, (double)o1 * nrm.ystd[1] + nrm.ymean[1]));
-            const double mt = C * scale;
+            const float C = fmaxf(0.0f, o0 * nrm.ystd[0] + nrm.ymean[0]);
+            const float prt = fminf(10.0f, fmaxf(0.1f, o1 * nrm.ystd[1] + nrm.ymean[1]));
+            const float mt = C * scale;
             mu_sgs[i] = (R)mt;
-            ksgs[i] = (R)(CP * mt / prt);
+            ksgs[i] = (R)__fdividef((float)CP * mt, prt);
         }
     }
     tc_teardown<TC_NWG>(c);
