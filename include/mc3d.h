@@ -485,7 +485,16 @@ int mc3d_tma_wait_timeouts(int device, int *count);
  * and calcKSGS (k_sgs; it reuses the filtered fields of the preceding
  * calcMuSGSTaukk, so call it after that one on the same state), averaged per
  * doAveraging (src/AbstractSGS.cpp:13-160). The object holds its work
- * fields (DSM: 49 fields of the block). */
+ * fields (DSM: 49 fields of the block).
+ * MC3D_MLPSGS (the learned closure; averaging, test_filter and use_taukk are
+ * ignored) takes its network and mu_ref from mc3d_sgs_set_mlp and works as a
+ * DSM-shaped pair: calcMuSGSTaukk keeps gradU and the mu_sgs destination and
+ * zeroes tau_kk (when given), then calcKSGS evaluates the closure (features
+ * of gradU, gradT, rho = q[0] and T; the tcgen05 network) into mu_sgs and
+ * k_sgs. Features outside the closure's training range are clamped; their
+ * points are counted (mc3d_sgs_mlp_out_of_range, the last calcKSGS). There
+ * is no fallback here: a caller that wants DSM for such states runs a DSM
+ * object. */
 typedef struct mc3d_sgs_s *mc3d_sgs;
 int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, int Nx, int Ny, int Nz,
                     const int bc_types[3], const double dxi[3], const void *J, double Jc, int precision,
@@ -497,6 +506,10 @@ int mc3d_sgs_calc_mu_taukk(mc3d_sgs sgs, const void *const gradU[9], const doubl
                            void *taukk, void *stream);
 int mc3d_sgs_calc_ksgs(mc3d_sgs sgs, const void *const gradT[3], const double *const q[5], const void *T,
                        void *k_sgs, void *stream);
+int mc3d_sgs_set_mlp(mc3d_sgs sgs, mc3d_mlp mlp, double mu_ref);
+/* points of the last learned-closure calcKSGS with a feature outside the
+ * training range (synchronises the device) */
+int mc3d_sgs_mlp_out_of_range(mc3d_sgs sgs, long long *points);
 
 /* ---- allocation-free CFL reduction ----
  * No counterpart in the reference: an extra entry point for callers that must

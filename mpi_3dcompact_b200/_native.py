@@ -152,6 +152,8 @@ def host_lib():
             "mc3d_sgs_get_viscosity": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp]),
             "mc3d_sgs_calc_mu_taukk": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp, vp]),
             "mc3d_sgs_calc_ksgs": (ip, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp, vp]),
+            "mc3d_sgs_set_mlp": (ip, [vp, vp, dp]),
+            "mc3d_sgs_mlp_out_of_range": (ip, [vp, C.POINTER(C.c_longlong)]),
             "mc3d_solver_set_sponge_avg": (ip, [vp, C.POINTER(C.POINTER(dp))]),
         }
         for name, (res, args) in sigs.items():

@@ -353,6 +353,17 @@ struct GpuDSMSGS : GpuSGS {
               int prec = MC3D_FP64, int dev = 0, void *st = nullptr)
         : GpuSGS(MC3D_DSM, averaging, test_filter, use_taukk, dom, bc, J, Jc, prec, dev, st) {}
 };
+// The learned closure behind the same interface, driven as DSM is
+// (calcMuSGSTaukk, then calcKSGS, which fills mu_sgs and k_sgs; tau_kk is
+// zero). `net` is a loaded closure (mc3d_mlp_create + mc3d_mlp_load), owned by
+// the caller; mu_ref is Options::mu_ref.
+struct GpuMlpSGS : GpuSGS {
+    GpuMlpSGS(mc3d_mlp net, double mu_ref, Domain *dom, BC *bc, const void *J, double Jc, int prec = MC3D_FP64,
+              int dev = 0, void *st = nullptr)
+        : GpuSGS(MC3D_MLPSGS, MC3D_AVG_NONE, 1, false, dom, bc, J, Jc, prec, dev, st) {
+        check(mc3d_sgs_set_mlp(sgs, net, mu_ref), "mc3d_sgs_set_mlp");
+    }
+};
 
 }  // namespace mc3d_adapters
 

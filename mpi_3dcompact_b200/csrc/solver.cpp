@@ -2245,7 +2245,8 @@ int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, in
                     mc3d_sgs *out) {
     if (!out || !bc_types || !dxi) return fail(MC3D_ERR_ARG, "null argument");
     *out = nullptr;
-    if (model != MC3D_VREMAN && model != MC3D_DSM) return fail(MC3D_ERR_CONFIG, "model must be VREMAN or DSM");
+    if (model != MC3D_VREMAN && model != MC3D_DSM && model != MC3D_MLPSGS)
+        return fail(MC3D_ERR_CONFIG, "model must be VREMAN, DSM or MLP");
     if (averaging < MC3D_AVG_NONE || averaging > MC3D_AVG_GLOBAL) return fail(MC3D_ERR_CONFIG, "unknown LESAVERAGING");
     if (model == MC3D_DSM && test_filter != 1 && test_filter != 2)
         return fail(MC3D_ERR_CONFIG, "DSMTESTFILTER must be 1 or 2");
@@ -2279,7 +2280,7 @@ int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, in
     o->home = s->stream;
     const int N[3] = {Nx, Ny, Nz};
     try {
-        for (int d = 0; d < 3 && !rc; d++) {
+        for (int d = 0; d < 3 && !rc && model != MC3D_MLPSGS; d++) {
             if (model == MC3D_VREMAN) {
                 // VremanSGS averages with Compact10 filters of alpha -0.49 (src/VremanSGS.hpp:38-40)
                 rc = upload_line_op(build_filter_op(MC3D_COMPACT10, -0.49, bc_types[d], N[d]), precision, s->vop[d]);
@@ -2302,6 +2303,11 @@ int mc3d_sgs_create(int model, int averaging, int test_filter, int use_taukk, in
         for (int i = 0; i < 24 && !rc; i++) rc = salloc(s, &s->dB[i], n * rb);
         if (!rc) rc = salloc(s, &s->smag, n * rb);
         if (!rc) rc = salloc(s, &o->taukk_own, n * rb);
+    }
+    if (model == MC3D_MLPSGS) {
+        if (!rc) rc = salloc(s, (void **)&s->mlp_flag, sizeof(int));
+        if (!rc && cudaMallocHost((void **)&s->mlp_flag_host, sizeof(int)) != cudaSuccess)
+            rc = fail(MC3D_ERR_OOM, "cudaMallocHost");
     }
     // metrics: J_ij = identity, J from the caller
     s->const_met = J == nullptr;
@@ -2392,7 +2398,56 @@ static int sgs_ksgs_t(mc3d_sgs o, const void *const gradT[3], const double *cons
     return rc;
 }
 
+// the learned closure on the caller's gradients: calcMuSGSTaukk keeps the
+// velocity gradients and the mu_sgs destination (tau_kk is zero), calcKSGS
+// runs the fused closure kernel for both outputs
+template <typename R>
+static int sgs_mlp_mu_t(mc3d_sgs o, const void *const gradU[9], void *mu_sgs, void *taukk) {
+    mc3d_solver s = o->rec;
+    for (int i = 0; i < 9; i++) s->der[i] = const_cast<void *>(gradU[i]);
+    s->mu_sgs = mu_sgs;
+    if (taukk) MC3D_CUDA_TRY(cudaMemsetAsync(taukk, 0, (size_t)s->g.n() * sizeof(R), s->stream));
+    return MC3D_OK;
+}
+
+template <typename R>
+static int sgs_mlp_k_t(mc3d_sgs o, const void *const gradT[3], const double *const q[5], const void *T, void *k_sgs) {
+    mc3d_solver s = o->rec;
+    if (!s->mlp) return fail(MC3D_ERR_CONFIG, "no closure attached (mc3d_sgs_set_mlp)");
+    if (!s->mu_sgs) return fail(MC3D_ERR_CONFIG, "calcKSGS of the learned closure needs calcMuSGSTaukk first");
+    int rc;
+    const double *src[5] = {q[0], nullptr, nullptr, nullptr, nullptr};
+    R *dst[5] = {(R *)s->prim[0], nullptr, nullptr, nullptr, nullptr};
+    if ((rc = launch_to_real<R>(s->g, src, dst, s->stream))) return rc;
+    const R *dd[12];
+    for (int i = 0; i < 9; i++) dd[i] = (const R *)s->der[i];
+    for (int i = 0; i < 3; i++) dd[9 + i] = (const R *)gradT[i];
+    MC3D_CUDA_TRY(cudaMemsetAsync(s->mlp_flag, 0, sizeof(int), s->stream));
+    return launch_sgs_mlp<R>(s->g, (const R *)s->prim[0], (const R *)T, dd, metrics_of<R>(s),
+                             s->dxi[0] * s->dxi[1] * s->dxi[2], s->cfg.mu_ref, *mlp_dev(s->mlp), (R *)s->mu_sgs,
+                             (R *)k_sgs, s->mlp_flag, s->stream);
+}
+
 extern "C" {
+
+int mc3d_sgs_set_mlp(mc3d_sgs o, mc3d_mlp mlp, double mu_ref) {
+    if (!o || !mlp) return fail(MC3D_ERR_ARG, "null argument");
+    if (o->rec->cfg.les_model != MC3D_MLPSGS) return fail(MC3D_ERR_CONFIG, "the SGS object's model is not MLP");
+    if (!(mu_ref > 0)) return fail(MC3D_ERR_ARG, "mu_ref must be positive");
+    o->rec->mlp = mlp;
+    o->rec->cfg.mu_ref = mu_ref;
+    return MC3D_OK;
+}
+
+int mc3d_sgs_mlp_out_of_range(mc3d_sgs o, long long *points) {
+    if (!o || !points) return fail(MC3D_ERR_ARG, "null argument");
+    mc3d_solver s = o->rec;
+    if (s->cfg.les_model != MC3D_MLPSGS) return fail(MC3D_ERR_CONFIG, "the SGS object's model is not MLP");
+    MC3D_CUDA_TRY(cudaSetDevice(s->device));
+    MC3D_CUDA_TRY(cudaMemcpy(s->mlp_flag_host, s->mlp_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    *points = *s->mlp_flag_host;
+    return MC3D_OK;
+}
 
 static int sgs_call(mc3d_sgs o, void *stream) {
     if (!o) return fail(MC3D_ERR_ARG, "null argument");
@@ -2421,6 +2476,9 @@ int mc3d_sgs_calc_mu_taukk(mc3d_sgs o, const void *const gradU[9], const double 
     if (o->rec->cfg.les_model == MC3D_DSM)
         rc = o->rec->prec == MC3D_FP64 ? sgs_mu_taukk_t<double>(o, gradU, q, mu_sgs, taukk)
                                        : sgs_mu_taukk_t<float>(o, gradU, q, mu_sgs, taukk);
+    if (o->rec->cfg.les_model == MC3D_MLPSGS)
+        rc = o->rec->prec == MC3D_FP64 ? sgs_mlp_mu_t<double>(o, gradU, mu_sgs, taukk)
+                                       : sgs_mlp_mu_t<float>(o, gradU, mu_sgs, taukk);
     o->rec->stream = o->home;
     return rc;
 }
@@ -2433,6 +2491,9 @@ int mc3d_sgs_calc_ksgs(mc3d_sgs o, const void *const gradT[3], const double *con
     if (o->rec->cfg.les_model == MC3D_DSM)
         rc = o->rec->prec == MC3D_FP64 ? sgs_ksgs_t<double>(o, gradT, q, T, k_sgs)
                                        : sgs_ksgs_t<float>(o, gradT, q, T, k_sgs);
+    if (o->rec->cfg.les_model == MC3D_MLPSGS)
+        rc = o->rec->prec == MC3D_FP64 ? sgs_mlp_k_t<double>(o, gradT, q, T, k_sgs)
+                                       : sgs_mlp_k_t<float>(o, gradT, q, T, k_sgs);
     o->rec->stream = o->home;
     return rc;
 }

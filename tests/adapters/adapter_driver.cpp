@@ -17,8 +17,10 @@
  *                 (MAXTIMESTEP), on the 2*pi box; writes the conserved state
  *                 (x fastest, after a header: time step, time) and prints the
  *                 largest difference from mc3d_solver_step on the same input
- *   sgs <in.bin> <out.bin>      GpuVremanSGS or GpuDSMSGS (LES.LESMODEL) via
- *                 AbstractSGS*: in = gradU (9), rho..rhoE (5), T, gradT (3);
+ *   sgs <in.bin> <out.bin> [closure.bin]   GpuVremanSGS or GpuDSMSGS
+ *                 (LES.LESMODEL), or with a closure file GpuMlpSGS (the
+ *                 learned closure, SOLVER.MU_REF), via AbstractSGS*:
+ *                 in = gradU (9), rho..rhoE (5), T, gradT (3);
  *                 out = mu_sgs, taukk, k_sgs (FP64, x fastest)
  */
 #include <mpi.h>
@@ -291,7 +293,7 @@ static int mode_solver(const string &icpath, const string &outpath) {
 }
 
 // ---- SGS through AbstractSGS ----------------------------------------------
-static int mode_sgs(const string &inpath, const string &outpath) {
+static int mode_sgs(const string &inpath, const string &outpath, const char *closure) {
     Setup s = make_setup();
     const int Nx = s.opt->Nx, Ny = s.opt->Ny, Nz = s.opt->Nz;
     const size_t n = (size_t)Nx * Ny * Nz;
@@ -311,10 +313,16 @@ static int mode_sgs(const string &inpath, const string &outpath) {
                     : a == Options::LOCAL   ? MC3D_AVG_LOCAL
                                             : MC3D_AVG_GLOBAL;
     AbstractSGS *sgs;
-    if (s.opt->lesModel == Options::VREMAN)
+    mc3d_mlp net = nullptr;
+    if (closure) {
+        if (mc3d_mlp_create(0, 0, &net) != MC3D_OK || mc3d_mlp_load(net, closure) != MC3D_OK)
+            die(string("closure: ") + mc3d_last_error());
+        sgs = new GpuMlpSGS(net, s.opt->mu_ref, s.d, s.bc, nullptr, Jc);
+    } else if (s.opt->lesModel == Options::VREMAN) {
         sgs = new GpuVremanSGS(avg, s.d, s.bc, nullptr, Jc);
-    else
+    } else {
         sgs = new GpuDSMSGS(avg, s.opt->testFilterType, s.opt->useTaukk, s.d, s.bc, nullptr, Jc);
+    }
     double *gu[3][3];
     for (int a2 = 0; a2 < 3; a2++)
         for (int b = 0; b < 3; b++) gu[a2][b] = f[3 * a2 + b]->p;
@@ -333,19 +341,20 @@ static int mode_sgs(const string &inpath, const string &outpath) {
     fclose(fo);
     printf("sgs ok\n");
     delete sgs;
+    if (net) mc3d_mlp_destroy(net);
     for (Dev *d : f) delete d;
     return 0;
 }
 
 int main(int argc, char **argv) {
     MPI_Init(&argc, &argv);
-    if (argc < 2) die("usage: adapter_driver ops <seed> | solver <ic> <out> | sgs <in> <out>");
+    if (argc < 2) die("usage: adapter_driver ops <seed> | solver <ic> <out> | sgs <in> <out> [closure]");
     const string mode = argv[1];
     int rc = 2;
     try {
         if (mode == "ops" && argc == 3) rc = mode_ops(atoi(argv[2]));
         else if (mode == "solver" && argc == 4) rc = mode_solver(argv[2], argv[3]);
-        else if (mode == "sgs" && argc == 4) rc = mode_sgs(argv[2], argv[3]);
+        else if (mode == "sgs" && (argc == 4 || argc == 5)) rc = mode_sgs(argv[2], argv[3], argc == 5 ? argv[4] : nullptr);
         else die("bad arguments");
     } catch (const std::exception &e) {
         die(e.what());
