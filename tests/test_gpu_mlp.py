@@ -8,6 +8,7 @@ Tolerances: FP32 forward 1e-5 relative to the output scale (FP32 rounding of
 ~200-term dot products); BF16 inference 3e-2 of the output scale (8-bit
 mantissas through four layers, FP32 accumulation)."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -253,3 +254,58 @@ def test_shipped_closure_gains_over_no_model():
     assert d_mlp < 0.02 and d_mlp < d_none, (d_mlp, d_none)
     assert tm["MLP"]["fallbacks"] == 0
     assert tm["MLP"]["ms"] < tm["DSM"]["ms"], tm
+
+
+def test_sgs_object_with_the_closure_reports_misuse_and_range():
+    """The standalone SGS object with the learned closure (mc3d_sgs_create with
+    the MLP model): calcKSGS before a closure is attached or before
+    calcMuSGSTaukk is refused, mc3d_sgs_set_mlp on a DSM object is refused,
+    and mc3d_sgs_mlp_out_of_range counts every point of a state whose
+    velocity gradients are far outside the training range."""
+    import ctypes as C
+    torch = _torch()
+    from mpi_3dcompact_b200 import _native as N
+    lib = N.host_lib()
+    n = 16
+    bcs = (C.c_int * 3)(m.PERIODIC_SOLVE, m.PERIODIC_SOLVE, m.PERIODIC_SOLVE)
+    dxi = (C.c_double * 3)(1.0 / n, 1.0 / n, 1.0 / n)
+
+    def create(model):
+        h = C.c_void_p()
+        N.check(lib.mc3d_sgs_create(model, N.AVG_GLOBAL, 1, 1, n, n, n, bcs, dxi, None, 1.0 / (2 * math.pi) ** 3,
+                                    m.FP32BULK, 0, C.byref(h)))
+        return h
+    net = m.MLPClosure()
+    net.load(os.path.join(os.path.dirname(m.__file__), "data", "mlp_sgs_hit128.bin"))
+    dsm = create(N.DSM)
+    with pytest.raises(m.Mc3dError):
+        N.check(lib.mc3d_sgs_set_mlp(dsm, net._h, 1e-3))
+    N.check(lib.mc3d_sgs_destroy(dsm))
+    o = create(N.MLPSGS)
+    rng = np.random.default_rng(3)
+    f32 = [torch.tensor(rng.standard_normal((n, n, n)).astype(np.float32) * 1e4, device="cuda") for _ in range(12)]
+    rho = torch.ones((n, n, n), dtype=torch.float64, device="cuda")
+    q = [rho] + [torch.zeros_like(rho) for _ in range(4)]
+    T = torch.ones((n, n, n), dtype=torch.float32, device="cuda")
+    mu, ks = torch.empty_like(T), torch.empty_like(T)
+
+    def vp(ts):
+        return (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+    with pytest.raises(m.Mc3dError):   # no closure attached
+        N.check(lib.mc3d_sgs_calc_ksgs(o, vp(f32[9:]), vp(q), C.c_void_p(T.data_ptr()),
+                                       C.c_void_p(ks.data_ptr()), None))
+    N.check(lib.mc3d_sgs_set_mlp(o, net._h, 1e-3))
+    fresh = create(N.MLPSGS)
+    N.check(lib.mc3d_sgs_set_mlp(fresh, net._h, 1e-3))
+    with pytest.raises(m.Mc3dError):   # calcKSGS before calcMuSGSTaukk
+        N.check(lib.mc3d_sgs_calc_ksgs(fresh, vp(f32[9:]), vp(q), C.c_void_p(T.data_ptr()),
+                                       C.c_void_p(ks.data_ptr()), None))
+    N.check(lib.mc3d_sgs_destroy(fresh))
+    N.check(lib.mc3d_sgs_calc_mu_taukk(o, vp(f32[:9]), vp(q), C.c_void_p(mu.data_ptr()), None, None))
+    N.check(lib.mc3d_sgs_calc_ksgs(o, vp(f32[9:]), vp(q), C.c_void_p(T.data_ptr()), C.c_void_p(ks.data_ptr()),
+                                   None))
+    count = C.c_longlong()
+    N.check(lib.mc3d_sgs_mlp_out_of_range(o, C.byref(count)))
+    assert count.value == n ** 3
+    assert torch.isfinite(mu).all() and torch.isfinite(ks).all()
+    N.check(lib.mc3d_sgs_destroy(o))
