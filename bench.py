@@ -685,7 +685,12 @@ def run_ours(args):
         "roofline": roof, "kernels": rep, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk, "fp32_vs_fp64_ke_curve": cmp.pop("curve") if cmp else None, "cylinder": cyl,
         "learned_sgs": les,
-        # the FP32-bulk evidence last, where a truncated record still keeps it
+        # the compact results last, where a truncated record still keeps them
+        "learned_vs_dsm": None if not les else {
+            "mlp_ms_per_step": les["ms_per_step"]["mlp"], "dsm_ms_per_step": les["ms_per_step"]["dsm"],
+            "speedup": les["mlp_speedup_over_dsm"], "fallback_frac": les["fallback_frac"],
+            "fallback_stages": les["fallback_stages"],
+            "ke_decay_max_rel_diff": les["ke_decay_max_rel_diff_vs_dsm"]["mlp"]},
         "fp64_value": fp64, "fp32_over_fp64": (value / ws / fp64) if fp64 else None,
         "fp64_over_cpu_reference": (fp64 / cpu["value"]) if (fp64 and cpu) else None,
         "fp32_vs_fp64": cmp,
