@@ -143,23 +143,29 @@ __global__ void __launch_bounds__(TC_NWG * 128, 3)
 template <typename K>
 int tc_grid(K kern, KernelLaunchState &st, long long n, int *blocks) {
     if (int rc = open_kernel(kern, st, TC_SMEM, TC_NWG * 128, nullptr)) return rc;
-    MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared));
-    int dev = 0, nsm = 0, smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
+    int dev = 0;
     MC3D_CUDA_TRY(cudaGetDevice(&dev));
-    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
-    MC3D_CUDA_TRY(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
-    cudaFuncAttributes fa{};
-    MC3D_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
-    const int threads = TC_NWG * 128;
-    int per = std::min(smem_sm / (int)(TC_SMEM + resv), thr_sm / threads);
-    if (fa.numRegs > 0) per = std::min(per, regs_sm / (fa.numRegs * threads));
-    per = std::max(1, std::min(per, 512 / (TC_NWG * MLPT_NCOL)));
+    int ctas = st.ctas[dev].load();
+    if (ctas <= 0) {   // first launch on this device: the CTAs that fit, counted once
+        MC3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared));
+        int nsm = 0, smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+        MC3D_CUDA_TRY(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+        cudaFuncAttributes fa{};
+        MC3D_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+        const int threads = TC_NWG * 128;
+        int per = std::min(smem_sm / (int)(TC_SMEM + resv), thr_sm / threads);
+        if (fa.numRegs > 0) per = std::min(per, regs_sm / (fa.numRegs * threads));
+        per = std::max(1, std::min(per, 512 / (TC_NWG * MLPT_NCOL)));
+        ctas = nsm * per;
+        st.ctas[dev].store(ctas);
+    }
     const long long need = (n + 128LL * TC_NWG - 1) / (128LL * TC_NWG);
-    *blocks = (int)std::max(1LL, std::min<long long>(need, (long long)nsm * per));
+    *blocks = (int)std::max(1LL, std::min<long long>(need, (long long)ctas));
     return MC3D_OK;
 }
 
