@@ -550,8 +550,19 @@ void segment(LineOpHost &h, int precision) {
 // Offsets (in elements) of the arrays inside one operator's device buffer.
 struct Layout {
     size_t arr = 0, head = 0, tail = 0, seg = 0;
-    size_t pf = 0, pb = 0, pz = 0, sf2 = 0, sb2 = 0, hp = 0, tp = 0;
+    size_t pf = 0, pb = 0, pz = 0, sf2 = 0, sb2 = 0, hp = 0, tp = 0, pbs = 0;
 };
+
+// Is the interior stencil of h antisymmetric with a zero centre (the first
+// derivatives), so that a row's RHS is sum_k st[H+k] (phi[n+k] - phi[n-k])?
+bool antisymmetric(const LineOpHost &h) {
+    if (h.H < 1 || h.H > 3 || h.st[h.H] != 0.0) return false;
+    for (int k = 1; k <= h.H; k++)
+        if (h.st[h.H + k] != -h.st[h.H - k]) return false;
+    for (int k = 2 * h.H + 1; k < 11; k++)
+        if (h.st[k] != 0.0) return false;
+    return true;
+}
 
 template <typename R>
 void fill_dev(const LineOpHost &h, const char *base, const Layout &lo, LineOpDev<R> &d) {
@@ -569,6 +580,16 @@ void fill_dev(const LineOpHost &h, const char *base, const Layout &lo, LineOpDev
     for (int i = 0; i < 4; i++) d.sc[i] = (R)h.sc[i];
     for (int i = 0; i < 16; i++) d.Hm[i] = (R)h.Hm[i];
     for (int i = 0; i < 6; i++) d.cp[i] = (R)h.cp[i];
+    d.asym = antisymmetric(h) ? 1 : 0;
+    for (int k = 0; k < 3; k++) d.sta[k] = d.asym && k < h.H ? (R)(h.st[h.H + 1 + k] * h.inv_dh) : R(0);
+    {
+        // stationary backward factors: tri (c, rw) = stat_c[2], stat_c[1]; penta (C, f, rD) = stat_c[3], stat_c[4], stat_c[2]
+        const bool tri = h.kind == K_TRI_PER || h.kind == K_TRI_DIR;
+        const double C = tri ? h.stat_c[2] : h.stat_c[3], f = tri ? 0.0 : h.stat_c[4], rD = tri ? h.stat_c[1] : h.stat_c[2];
+        d.stat_b[0] = (R)(C * rD);
+        d.stat_b[1] = (R)(f * rD);
+        d.stat_b[2] = (R)rD;
+    }
     const R *p = (const R *)base;
     size_t n = h.N;
     size_t na = h.arr.size() / n;
@@ -598,6 +619,7 @@ void fill_dev(const LineOpHost &h, const char *base, const Layout &lo, LineOpDev
     d.pz = h.L && h.kind == K_PEN_PER ? p + lo.pz : nullptr;
     d.sf2 = h.L ? p + lo.sf2 : nullptr;
     d.sb2 = h.L ? p + lo.sb2 : nullptr;
+    d.pbs = h.L ? p + lo.pbs : nullptr;
     const bool dir = h.kind == K_TRI_DIR || h.kind == K_PEN_DIR;
     d.hp = h.L && dir ? p + lo.hp : nullptr;
     d.tp = h.L && dir ? p + lo.tp : nullptr;
@@ -642,6 +664,15 @@ std::vector<R> flatten(const LineOpHost &h, Layout &lo) {
                 put(A(4, i));
                 put(A(2, i));
             }
+            put(0.0);
+        }
+        align4();
+        lo.pbs = v.size();
+        for (int i = 0; i < n; i++) {
+            const double C = tri ? A(2, i) : A(3, i), f = tri ? 0.0 : A(4, i), rD = tri ? A(1, i) : A(2, i);
+            put(C * rD);
+            put(f * rD);
+            put(rD);
             put(0.0);
         }
         if (h.kind == K_PEN_PER) {

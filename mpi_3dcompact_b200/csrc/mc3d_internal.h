@@ -146,6 +146,15 @@ struct LineOpDev {
     //   phi[0..BWMAX-1], tail right-aligned on phi[N-BWMAX..N-1])
     int L;
     const R *pf, *pb, *pz, *sf2, *sb2, *hp, *tp;
+    // FP32 derivative form of the register-resident solve (H <= 3): asym is 1
+    // when the interior stencil is antisymmetric with a zero centre, sta[k-1]
+    // = st[H+k] / dh; the backward factors pre-multiplied by the reciprocal
+    // pivot, stat_b = (C rD, f rD, rD) of the stationary rows and
+    //   pbs [N][4]  (C_n rD_n, f_n rD_n, rD_n, 0) | tri (c_n rw_n, 0, rw_n, 0)
+    int asym;
+    R sta[3];
+    R stat_b[3];
+    const R *pbs;
 };
 constexpr int MC3D_BWMAX = 11;   // widest boundary row (11-point filter closures)
 

@@ -195,12 +195,21 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
 // the segments' local end states of both passes and the last segment's last
 // two values). Every thread of the CTA calls it (it synchronises the CTA
 // twice; each warp then chains the states it needs itself).
-template <typename R, int KIND, int H, int L>
+template <typename R, int KIND, int H, int L, bool FASTOK = true>
 __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L + 2 * H], R (&y)[L], bool work,
                                           int lane, int seg, int S, int a, R *sh) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
     constexpr int NB = L / UB;
+    // FP32 first derivatives (H <= 3; the launchers send only antisymmetric
+    // stencils and no pass-through lines here): RHS from the differences
+    // phi[n+k] - phi[n-k] with 1/dh in the coefficients; pass 1 keeps each
+    // eliminated row times its pivot reciprocal rD_n (the multiply off the
+    // recurrence's path) and the backward factors come pre-multiplied by it,
+    // so pass 2 is two FMAs a row with one on its path; every lane's line is
+    // solved (lanes past the block's last line hold zeros and are not stored).
+    constexpr bool FAST = FASTOK && sizeof(R) == 4 && H <= 3;
+    if constexpr (FAST) work = true;
     using V = RegVec<R>;
     const int N = op.N;
     R *fwdEnd = sh;                    // [S][2][W] local end states of pass 1
@@ -236,20 +245,29 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
 #pragma unroll
         for (int u = 0; u < UB; u++) {
             const int r = blk * UB + u;
-            R acc = op.st[0] * v[r];
+            if constexpr (FAST) {
+                R acc = op.sta[0] * (v[r + H + 1] - v[r + H - 1]);
 #pragma unroll
-            for (int k = 1; k < 2 * H + 1; k++) acc += op.st[k] * v[r + k];
-            rhs[u] = acc * op.inv_dh;
+                for (int k = 2; k <= H; k++) acc += op.sta[k - 1] * (v[r + H + k] - v[r + H - k]);
+                rhs[u] = acc;
+            } else {
+                R acc = op.st[0] * v[r];
+#pragma unroll
+                for (int k = 1; k < 2 * H + 1; k++) acc += op.st[k] * v[r + k];
+                rhs[u] = acc * op.inv_dh;
+            }
         }
         const bool stat = n0 >= op.stat_lo && n0 + UB <= op.stat_hi && (PER || (n0 >= H && n0 + UB <= N - H));
         if (stat) {
             const R m1 = op.stat_c[0], m2 = op.stat_c[1];
+            const R rDs = FAST ? op.stat_b[2] : R(1);
 #pragma unroll
             for (int u = 0; u < UB; u++) {
                 R x = TRI ? rhs[u] - m1 * y1 : rhs[u] - m2 * y2 - m1 * y1;
                 y2 = y1;
                 y1 = x;
-                y[blk * UB + u] = work ? x : v[H + blk * UB + u];
+                if constexpr (FAST) y[blk * UB + u] = rDs * x;
+                else y[blk * UB + u] = work ? x : v[H + blk * UB + u];
             }
         } else {
 #pragma unroll
@@ -268,7 +286,8 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                 R x = TRI ? rr - m1 * y1 : rr - m2 * y2 - m1 * y1;
                 y2 = y1;
                 y1 = x;
-                y[blk * UB + u] = work ? x : v[H + blk * UB + u];
+                if constexpr (FAST) y[blk * UB + u] = ldc(op.pbs + 4 * n + 2) * x;
+                else y[blk * UB + u] = work ? x : v[H + blk * UB + u];
             }
         }
     }
@@ -301,10 +320,12 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                 const bool stat = n0 >= op.stat_lo && n0 + UB <= op.stat_hi;
                 if (stat) {
                     const R m1 = op.stat_c[0], m2 = op.stat_c[1];
+                    const R rDs = FAST ? op.stat_b[2] : R(1);
 #pragma unroll
                     for (int u = 0; u < UB; u++) {
                         R F = TRI ? -(m1 * F1) : -(m2 * F2) - m1 * F1;
-                        y[blk * UB + u] += F;
+                        if constexpr (FAST) y[blk * UB + u] += rDs * F;
+                        else y[blk * UB + u] += F;
                         F2 = F1;
                         F1 = F;
                     }
@@ -314,7 +335,8 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                         R m1, m2;
                         V::ld2(op.pf + 2 * (n0 + u), m1, m2);
                         R F = TRI ? -(m1 * F1) : -(m2 * F2) - m1 * F1;
-                        y[blk * UB + u] += F;
+                        if constexpr (FAST) y[blk * UB + u] += ldc(op.pbs + 4 * (n0 + u) + 2) * F;
+                        else y[blk * UB + u] += F;
                         F2 = F1;
                         F1 = F;
                     }
@@ -331,27 +353,51 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
             const int n0 = a + blk * UB;
             const bool stat = n0 >= op.stat_lo && n0 + UB <= op.stat_hi;
             if (stat) {
-                const R C = TRI ? op.stat_c[2] : op.stat_c[3];
-                const R fv = TRI ? R(0) : op.stat_c[4];
-                const R rD = TRI ? op.stat_c[1] : op.stat_c[2];
+                if constexpr (FAST) {
+                    const R Cs = op.stat_b[0], fs = op.stat_b[1];
 #pragma unroll
-                for (int u = UB - 1; u >= 0; u--) {
-                    const int r = blk * UB + u;
-                    R x = TRI ? (y[r] - C * x1) * rD : (y[r] - fv * x2 - C * x1) * rD;
-                    x2 = x1;
-                    x1 = x;
-                    if (work) y[r] = x;
+                    for (int u = UB - 1; u >= 0; u--) {
+                        const int r = blk * UB + u;
+                        R t = y[r];
+                        if (!TRI) t -= fs * x2;
+                        const R x = t - Cs * x1;
+                        x2 = x1;
+                        x1 = x;
+                        y[r] = x;
+                    }
+                } else {
+                    const R C = TRI ? op.stat_c[2] : op.stat_c[3];
+                    const R fv = TRI ? R(0) : op.stat_c[4];
+                    const R rD = TRI ? op.stat_c[1] : op.stat_c[2];
+#pragma unroll
+                    for (int u = UB - 1; u >= 0; u--) {
+                        const int r = blk * UB + u;
+                        R x = TRI ? (y[r] - C * x1) * rD : (y[r] - fv * x2 - C * x1) * rD;
+                        x2 = x1;
+                        x1 = x;
+                        if (work) y[r] = x;
+                    }
                 }
             } else {
 #pragma unroll
                 for (int u = UB - 1; u >= 0; u--) {
                     const int r = blk * UB + u;
                     R C, fv, rD, pad;
-                    V::ld4(op.pb + 4 * (n0 + u), C, fv, rD, pad);
-                    R x = TRI ? (y[r] - C * x1) * rD : (y[r] - fv * x2 - C * x1) * rD;
-                    x2 = x1;
-                    x1 = x;
-                    if (work) y[r] = x;
+                    if constexpr (FAST) {
+                        V::ld4(op.pbs + 4 * (n0 + u), C, fv, rD, pad);
+                        R t = y[r];
+                        if (!TRI) t -= fv * x2;
+                        const R x = t - C * x1;
+                        x2 = x1;
+                        x1 = x;
+                        y[r] = x;
+                    } else {
+                        V::ld4(op.pb + 4 * (n0 + u), C, fv, rD, pad);
+                        R x = TRI ? (y[r] - C * x1) * rD : (y[r] - fv * x2 - C * x1) * rD;
+                        x2 = x1;
+                        x1 = x;
+                        if (work) y[r] = x;
+                    }
                 }
             }
         }
@@ -419,12 +465,14 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                 const int n0 = a + blk * UB;
                 const bool stat = n0 >= op.stat_lo && n0 + UB <= op.stat_hi;
                 if (stat) {
-                    const R C = TRI ? op.stat_c[2] : op.stat_c[3];
-                    const R fv = TRI ? R(0) : op.stat_c[4];
+                    const R C = FAST ? op.stat_b[0] : (TRI ? op.stat_c[2] : op.stat_c[3]);
+                    const R fv = FAST ? op.stat_b[1] : (TRI ? R(0) : op.stat_c[4]);
                     const R rD = TRI ? op.stat_c[1] : op.stat_c[2];
 #pragma unroll
                     for (int u = UB - 1; u >= 0; u--) {
-                        R G = TRI ? (R(0) - C * G1) * rD : (R(0) - fv * G2 - C * G1) * rD;
+                        R G;
+                        if constexpr (FAST) G = TRI ? -(C * G1) : -(fv * G2) - C * G1;
+                        else G = TRI ? (R(0) - C * G1) * rD : (R(0) - fv * G2 - C * G1) * rD;
                         y[blk * UB + u] += G;
                         G2 = G1;
                         G1 = G;
@@ -432,9 +480,14 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                 } else {
 #pragma unroll
                     for (int u = UB - 1; u >= 0; u--) {
-                        R C, fv, rD, pad;
-                        V::ld4(op.pb + 4 * (n0 + u), C, fv, rD, pad);
-                        R G = TRI ? (R(0) - C * G1) * rD : (R(0) - fv * G2 - C * G1) * rD;
+                        R C, fv, rD, pad, G;
+                        if constexpr (FAST) {
+                            V::ld4(op.pbs + 4 * (n0 + u), C, fv, rD, pad);
+                            G = TRI ? -(C * G1) : -(fv * G2) - C * G1;
+                        } else {
+                            V::ld4(op.pb + 4 * (n0 + u), C, fv, rD, pad);
+                            G = TRI ? (R(0) - C * G1) * rD : (R(0) - fv * G2 - C * G1) * rD;
+                        }
                         y[blk * UB + u] += G;
                         G2 = G1;
                         G1 = G;
@@ -459,8 +512,16 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
                     } else {
                         R z0, z1, z2, z3;
                         V::ld4(op.pz + 4 * n, z0, z1, z2, z3);
-                        R sum = z0 * c0 + z1 * c1 + z2 * c2 + z3 * c3;
-                        y[blk * UB + u] -= sum;
+                        if constexpr (FAST) {
+                            // four FMAs into the row
+                            R t = y[blk * UB + u] - z0 * c0;
+                            t -= z1 * c1;
+                            t -= z2 * c2;
+                            y[blk * UB + u] = t - z3 * c3;
+                        } else {
+                            R sum = z0 * c0 + z1 * c1 + z2 * c2 + z3 * c3;
+                            y[blk * UB + u] -= sum;
+                        }
                     }
                 }
             }
@@ -595,6 +656,10 @@ template <int DIR, typename R>
 int launch_sweep_reg(const Grid3 &g, const LineOpDev<R> &op, const SweepBatch<R> &b, int epi,
                      const RhsFinalArgs<R> &rf, int px, int py, int pz, cudaStream_t st) {
     if constexpr (sizeof(R) == 4) {
+        // the FP32 solve of H <= 3 takes antisymmetric stencils and no
+        // pass-through lines (reg_solve); anything else goes to the
+        // shared-memory kernels
+        if (op.H <= 3 && (px || py || pz || !op.asym)) return MC3D_ERR_CONFIG;
         const int rc = DIR == 0 ? launch_sweep_tma_x(g, op, b, epi, px, py, pz, st)
                                 : launch_sweep_tma_yz(DIR, g, op, b, epi, rf, px, py, pz, st);
         if (rc != MC3D_ERR_CONFIG) return rc;

@@ -293,9 +293,11 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
         phase ^= 1u;
         const int f = w / ntiles, tl = w - f * ntiles;
         const TileGeom t = tile_geom<DIR>(g, tl, lane);
-        bool pass;
-        if (DIR == 1) pass = (pass_x && (t.i == 0 || t.i == g.Nx - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
-        else pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_x && (t.i == 0 || t.i == g.Nx - 1));
+        bool pass = false;   // (no pass-through lines with the derivatives, H <= 3)
+        if (H > 3) {
+            if (DIR == 1) pass = (pass_x && (t.i == 0 || t.i == g.Nx - 1)) || (pass_z && (t.k == 0 || t.k == g.Nz - 1));
+            else pass = (pass_y && (t.j == 0 || t.j == g.Ny - 1)) || (pass_x && (t.i == 0 || t.i == g.Nx - 1));
+        }
         const bool work = t.active && !pass;
         R v[NV];
 #pragma unroll
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
         __syncthreads();   // every lane holds its rows: the buffer takes the next item
         if (threadIdx.x == 0 && w + (int)gridDim.x < nitems) issue(w + gridDim.x);
         R y[L];
-        reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
+        reg_solve<R, KIND, H, L, DIR != 2>(op, v, y, work, lane, seg, S, a, sh);
         if (t.active) reg_store_rows<R, E, L>(b, rf, f, (int)t.base + a * (int)t.stride, (int)t.stride, y);
     }
 }
