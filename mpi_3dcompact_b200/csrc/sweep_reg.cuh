@@ -195,20 +195,23 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
 // the segments' local end states of both passes and the last segment's last
 // two values). Every thread of the CTA calls it (it synchronises the CTA
 // twice; each warp then chains the states it needs itself).
-template <typename R, int KIND, int H, int L, bool FASTOK = true>
+// NEG (the FP32 derivative form only): solve for the negated right-hand
+// side, so that a negated store needs no negation of its own.
+template <typename R, int KIND, int H, int L, bool NEG = false>
 __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L + 2 * H], R (&y)[L], bool work,
                                           int lane, int seg, int S, int a, R *sh) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
     constexpr int NB = L / UB;
     // FP32 first derivatives (H <= 3; the launchers send only antisymmetric
-    // stencils and no pass-through lines here): RHS from the differences
-    // phi[n+k] - phi[n-k] with 1/dh in the coefficients; pass 1 keeps each
+    // stencils and no pass-through lines here): RHS as the 2H products of the
+    // stencil without its zero centre, 1/dh in the coefficients; pass 1 keeps each
     // eliminated row times its pivot reciprocal rD_n (the multiply off the
     // recurrence's path) and the backward factors come pre-multiplied by it,
     // so pass 2 is two FMAs a row with one on its path; every lane's line is
     // solved (lanes past the block's last line hold zeros and are not stored).
-    constexpr bool FAST = FASTOK && sizeof(R) == 4 && H <= 3;
+    constexpr bool FAST = sizeof(R) == 4 && H <= 3;
+    static_assert(FAST || !NEG, "a negated right-hand side only in the FP32 derivative form");
     if constexpr (FAST) work = true;
     using V = RegVec<R>;
     const int N = op.N;
@@ -230,8 +233,8 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
 #pragma unroll
                 for (int k = 0; k < MC3D_BWMAX; k++) ts += ldc(op.tp + r * MC3D_BWMAX + k) * v[H + L - MC3D_BWMAX + k];
             }
-            headr[r] = hs * op.inv_dh;
-            tailr[r] = ts * op.inv_dh;
+            headr[r] = hs * (NEG ? -op.inv_dh : op.inv_dh);
+            tailr[r] = ts * (NEG ? -op.inv_dh : op.inv_dh);
         }
     }
 
@@ -246,9 +249,12 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
         for (int u = 0; u < UB; u++) {
             const int r = blk * UB + u;
             if constexpr (FAST) {
-                R acc = op.sta[0] * (v[r + H + 1] - v[r + H - 1]);
+                // 2H products, the zero centre skipped; the row's lowest value first
+                R acc = (NEG ? op.sta[H - 1] : -op.sta[H - 1]) * v[r];
 #pragma unroll
-                for (int k = 2; k <= H; k++) acc += op.sta[k - 1] * (v[r + H + k] - v[r + H - k]);
+                for (int k = H - 1; k >= 1; k--) acc += (NEG ? op.sta[k - 1] : -op.sta[k - 1]) * v[r + H - k];
+#pragma unroll
+                for (int k = 1; k <= H; k++) acc += (NEG ? -op.sta[k - 1] : op.sta[k - 1]) * v[r + H + k];
                 rhs[u] = acc;
             } else {
                 R acc = op.st[0] * v[r];

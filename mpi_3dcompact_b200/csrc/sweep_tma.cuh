@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
         __syncthreads();   // every lane holds its rows: the buffer takes the next item
         if (threadIdx.x == 0 && w + (int)gridDim.x < nitems) issue(w + gridDim.x);
         R y[L];
-        reg_solve<R, KIND, H, L, DIR != 2>(op, v, y, work, lane, seg, S, a, sh);
+        reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
         if (t.active) reg_store_rows<R, E, L>(b, rf, f, (int)t.base + a * (int)t.stride, (int)t.stride, y);
     }
 }
@@ -432,16 +432,18 @@ __global__ void __launch_bounds__(512) sweep_tma_x_persist_kernel(Grid3 g, LineO
             asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // previous store has read tout
         }
         R y[L];
-        reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
+        // (negated store: the solve itself yields -y)
+        static_assert(E != EPI_STORE_NEG || H <= 3, "negated x stores are derivative sweeps");
+        reg_solve<R, KIND, H, L, E == EPI_STORE_NEG>(op, v, y, work, lane, seg, S, a, sh);
         // (pass-through lines: y holds their input)
         if (t.active) {
 #pragma unroll
             for (int q = 0; q < L / 4; q++) {
                 float4 o4;
-                o4.x = E == EPI_STORE_NEG ? -y[4 * q + 0] : y[4 * q + 0];
-                o4.y = E == EPI_STORE_NEG ? -y[4 * q + 1] : y[4 * q + 1];
-                o4.z = E == EPI_STORE_NEG ? -y[4 * q + 2] : y[4 * q + 2];
-                o4.w = E == EPI_STORE_NEG ? -y[4 * q + 3] : y[4 * q + 3];
+                o4.x = y[4 * q + 0];
+                o4.y = y[4 * q + 1];
+                o4.z = y[4 * q + 2];
+                o4.w = y[4 * q + 3];
                 *reinterpret_cast<float4 *>(tout + swz_off(lane, a + 4 * q)) = o4;
             }
         }
