@@ -212,13 +212,13 @@ __global__ void mlp_pack_kernel(const float *__restrict__ P, unsigned char *__re
             else if (c == MLP_IN) v = hi;
             else if (c == MLP_IN + 1) v = lo;
             off = MLPT_W1 + tc_off16(o, c);
-        } else if ((k -= n1) < 2 * n2) {   // W2, W3
+        } else if ((k -= n1) < 2 * n2) {   // W2, W3, halved: their inputs are twice GELU (gelu2_bf16x2)
             const int w = k < n2 ? MLP_W2 : MLP_W3, kk = k % n2, o = kk / 64, c = kk % 64;
-            v = __float2bfloat16_rn(P[w + o * 64 + c]);
+            v = __float2bfloat16_rn(0.5f * P[w + o * 64 + c]);
             off = (k < n2 ? MLPT_W2 : MLPT_W3) + tc_off64(o, c);
-        } else if ((k -= 2 * n2) < n4) {   // W4, rows past the outputs zero
+        } else if ((k -= 2 * n2) < n4) {   // W4, halved likewise; rows past the outputs zero
             const int o = k / 64, c = k % 64;
-            if (o < MLP_OUT) v = __float2bfloat16_rn(P[MLP_W4 + o * 64 + c]);
+            if (o < MLP_OUT) v = __float2bfloat16_rn(0.5f * P[MLP_W4 + o * 64 + c]);
             off = MLPT_W4 + tc_off64(o, c);
         } else if ((k -= n4) < 2 * nb + nb4) {   // bias blocks of layers 2, 3, 4
             const int blk = k < nb ? 0 : k < 2 * nb ? 1 : 2, kk = k - blk * nb, o = kk / 16, c = kk % 16;

@@ -38,7 +38,7 @@ __host__ __device__ constexpr unsigned tc_idesc(int n) {
 }
 
 // GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))): the
-// training kernels use tanhf in FP32, the tensor-core inference gelu_bf16x2
+// training kernels use tanhf in FP32, the tensor-core inference gelu2_bf16x2
 constexpr float GELU_K0 = 0.7978845608028654f, GELU_K1 = 0.044715f;
 __device__ __forceinline__ float gelu(float x) {
     return 0.5f * x * (1.0f + tanhf(GELU_K0 * (x + GELU_K1 * x * x * x)));
@@ -53,25 +53,26 @@ __device__ __forceinline__ unsigned pack_bf2(float lo, float hi) {
     return *reinterpret_cast<unsigned *>(&v);
 }
 
-// The same GELU on a BF16 pair in seven packed instructions, as the
+// Twice the same GELU on a BF16 pair in five packed instructions (six with
+// the conversion of the FP32 accumulator pair), as the
 // tensor-core inference uses it (its operands are BF16 anyway): u = x (K0 +
-// K0 K1 x^2), h = x / 2, gelu = h + h tanh(u), every step rounded to BF16 and
-// tanh by the hardware's tanh.approx.bf16x2. Against GELU in FP32 rounded once
-// to BF16 this moves the shipped network's outputs by at most 0.6% of their
-// range on standard-normal inputs (numpy emulation with exact tanh).
-__device__ __forceinline__ unsigned gelu_bf16x2(unsigned x) {
-    const unsigned k01 = pack_bf2(GELU_K0 * GELU_K1, GELU_K0 * GELU_K1), k0 = pack_bf2(GELU_K0, GELU_K0),
-                   half = pack_bf2(0.5f, 0.5f);
+// K0 K1 x^2), 2 gelu = x + x tanh(u), every step rounded to BF16 and tanh by
+// the hardware's tanh.approx.bf16x2; the factor 1/2 sits in the next layer's
+// weights (mlp_pack halves them, exactly), so the products are those of
+// h = x / 2, gelu = h + h tanh(u) bit for bit. Against GELU in FP32 rounded
+// once to BF16 this moves the shipped network's outputs by at most 0.6% of
+// their range on standard-normal inputs (numpy emulation with exact tanh).
+__device__ __forceinline__ unsigned gelu2_bf16x2(unsigned x) {
+    const unsigned k01 = pack_bf2(GELU_K0 * GELU_K1, GELU_K0 * GELU_K1), k0 = pack_bf2(GELU_K0, GELU_K0);
     unsigned y;
-    asm("{\n.reg .b32 x2, t, u, th, h;\n"
+    asm("{\n.reg .b32 x2, t, u, th;\n"
         "mul.rn.bf16x2 x2, %1, %1;\n"
         "fma.rn.bf16x2 t, x2, %2, %3;\n"
         "mul.rn.bf16x2 u, %1, t;\n"
         "tanh.approx.bf16x2 th, u;\n"
-        "mul.rn.bf16x2 h, %1, %4;\n"
-        "fma.rn.bf16x2 %0, h, th, h;\n}"
+        "fma.rn.bf16x2 %0, %1, th, %1;\n}"
         : "=r"(y)
-        : "r"(x), "r"(k01), "r"(k0), "r"(half));
+        : "r"(x), "r"(k01), "r"(k0));
     return y;
 }
 

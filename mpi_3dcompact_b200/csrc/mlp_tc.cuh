@@ -176,10 +176,10 @@ __device__ __forceinline__ void tc_gelu_half(unsigned taddr, unsigned char *tile
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         uint4 o;
-        o.x = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 0]), __uint_as_float(v[8 * q + 1])));
-        o.y = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 2]), __uint_as_float(v[8 * q + 3])));
-        o.z = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 4]), __uint_as_float(v[8 * q + 5])));
-        o.w = gelu_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 6]), __uint_as_float(v[8 * q + 7])));
+        o.x = gelu2_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 0]), __uint_as_float(v[8 * q + 1])));
+        o.y = gelu2_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 2]), __uint_as_float(v[8 * q + 3])));
+        o.z = gelu2_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 4]), __uint_as_float(v[8 * q + 5])));
+        o.w = gelu2_bf16x2(pack_bf2(__uint_as_float(v[8 * q + 6]), __uint_as_float(v[8 * q + 7])));
         *reinterpret_cast<uint4 *>(tc_row_chunk(tile, r, c0 / 8 + q)) = o;
     }
 }
