@@ -61,13 +61,13 @@ __device__ __forceinline__ TileGeom tile_geom(const Grid3 &g, int tile, int lane
         t.k = k;
         t.j = 0;
     } else {
-        // (a plane of the block holds fewer than 2^31 points)
-        const int L = tile * W + lane, nl = g.Nx * g.Ny;
+        long long L = (long long)tile * W + lane;
+        long long nl = (long long)g.Nx * g.Ny;
         t.active = L < nl;
         t.base = L;
-        t.stride = nl;
-        t.i = L % g.Nx;
-        t.j = L / g.Nx;
+        t.stride = (long long)g.Nx * g.Ny;
+        t.i = (int)(L % g.Nx);
+        t.j = (int)(L / g.Nx);
         t.k = 0;
     }
     return t;
