@@ -197,9 +197,16 @@ __device__ __forceinline__ void reg_copy_out(const SweepBatch<R> &b, const RhsFi
 // twice; each warp then chains the states it needs itself).
 // NEG (the FP32 derivative form only): solve for the negated right-hand
 // side, so that a negated store needs no negation of its own.
-template <typename R, int KIND, int H, int L, bool NEG = false>
+// hook(0) runs in every thread just before the barrier that ends pass 1 and
+// hook(1) just after it: v is dead from there on, so a caller that loaded v
+// from a shared-memory tile can hand the tile to its next load there instead
+// of spending a barrier of its own.
+struct NoFwdHook {
+    __device__ __forceinline__ void operator()(int) const {}
+};
+template <typename R, int KIND, int H, int L, bool NEG = false, typename FwdHook = NoFwdHook>
 __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L + 2 * H], R (&y)[L], bool work,
-                                          int lane, int seg, int S, int a, R *sh) {
+                                          int lane, int seg, int S, int a, R *sh, const FwdHook &hook = FwdHook()) {
     constexpr bool PER = (KIND % 2) == 0;
     constexpr bool TRI = KIND == K_TRI_PER || KIND == K_TRI_DIR;
     constexpr int NB = L / UB;
@@ -299,7 +306,9 @@ __device__ __forceinline__ void reg_solve(const LineOpDev<R> &op, const R (&v)[L
     }
     fwdEnd[(seg * 2 + 0) * W + lane] = y1;
     fwdEnd[(seg * 2 + 1) * W + lane] = y2;
+    hook(0);
     __syncthreads();
+    hook(1);
 
     // ---- chain the forward states up to this segment: its incoming (y_{a-1}, y_{a-2}) ----
     // (each warp runs the chain of the segments before its own, so no further

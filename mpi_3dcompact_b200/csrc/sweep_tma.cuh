@@ -314,11 +314,13 @@ __global__ void __launch_bounds__(512) sweep_tma_yz_persist_kernel(Grid3 g, Line
             }
             v[k] = in ? *reinterpret_cast<const R *>(tile + swz_row(n, lane)) : R(0);
         }
-        tile_reads_done();
-        __syncthreads();   // every lane holds its rows: the buffer takes the next item
-        if (threadIdx.x == 0 && w + (int)gridDim.x < nitems) issue(w + gridDim.x);
+        // the buffer takes the next item at the barrier that ends pass 1
+        auto refill = [&](int ph) {
+            if (ph == 0) tile_reads_done();
+            else if (threadIdx.x == 0 && w + (int)gridDim.x < nitems) issue(w + gridDim.x);
+        };
         R y[L];
-        reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh);
+        reg_solve<R, KIND, H, L>(op, v, y, work, lane, seg, S, a, sh, refill);
         if (t.active) reg_store_rows<R, E, L>(b, rf, f, (int)t.base + a * (int)t.stride, (int)t.stride, y);
     }
 }
@@ -425,16 +427,21 @@ __global__ void __launch_bounds__(512) sweep_tma_x_persist_kernel(Grid3 g, LineO
                 if (k < NV) v[k] = e2[j];
             }
         }
-        tile_reads_done();
-        __syncthreads();   // every lane holds its rows: the input tile takes the next item
-        if (threadIdx.x == 0) {
-            if (w + (int)gridDim.x < nitems) issue(w + gridDim.x);
-            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // previous store has read tout
-        }
+        // the input tile takes the next item at the barrier that ends pass 1;
+        // the output tile is written after the solve's second barrier, which
+        // the issuing thread reaches only once the previous store has read it
+        auto refill = [&](int ph) {
+            if (ph == 0) {
+                tile_reads_done();
+            } else if (threadIdx.x == 0) {
+                if (w + (int)gridDim.x < nitems) issue(w + gridDim.x);
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // previous store has read tout
+            }
+        };
         R y[L];
         // (negated store: the solve itself yields -y)
         static_assert(E != EPI_STORE_NEG || H <= 3, "negated x stores are derivative sweeps");
-        reg_solve<R, KIND, H, L, E == EPI_STORE_NEG>(op, v, y, work, lane, seg, S, a, sh);
+        reg_solve<R, KIND, H, L, E == EPI_STORE_NEG>(op, v, y, work, lane, seg, S, a, sh, refill);
         // (pass-through lines: y holds their input)
         if (t.active) {
 #pragma unroll
