@@ -130,6 +130,10 @@ __global__ void sponge_source_kernel(Grid3 g, const double *__restrict__ sigma, 
     const long long n = g.n();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double s = sigma[i];
+        // outside the sponge (sigma = 0) a finite state adds a zero: the state,
+        // the target and the right-hand side there are not read (a cylindrical
+        // sponge covers a few of the radial lines)
+        if (s == 0.0) continue;
         const R Jv = J ? J[i] : Jc;
 #pragma unroll
         for (int e = 0; e < 5; e++) rhs.p[e][i] += (R)(s * (avg.p[e][i] - q.p[e][i])) / Jv;

@@ -40,6 +40,7 @@ struct mc3d_solver_s {
     // sponge: strength and target state (FP64); walls present
     double *sigma = nullptr, *spg_avg[5] = {};
     bool have_sponge = false, have_walls = false, sigma_set = false;
+    long long sponge_pts = 0;   // points with a nonzero sponge strength
     // walls: temperature that mu at wall points follows (set_initial fills it
     // with the initial temperature for the first stage; later stages save it
     // before the wall treatment)
@@ -593,7 +594,9 @@ static int stage_rhs(mc3d_solver s, double *const *qP) {
             ac[v] = s->spg_avg[v];
         }
         s->launches++;
-        if ((rc = tic(s, KC_BC, (8.0 + 10.0 * 8 + 10.0 * sizeof(R)) * (double)s->g.n()))) return rc;
+        // sigma everywhere; state, target, right-hand side (and J) where sigma is nonzero
+        const double per_pt = 10.0 * 8 + 10.0 * sizeof(R) + (s->const_met ? 0.0 : sizeof(R));
+        if ((rc = tic(s, KC_BC, 8.0 * (double)s->g.n() + per_pt * (double)s->sponge_pts))) return rc;
         if ((rc = launch_sponge_source<R>(s->g, s->sigma, ac, qc, s->const_met ? nullptr : (const R *)s->metR[0],
                                           (R)s->met_c[0], rh, s->stream)))
             return rc;
@@ -1539,6 +1542,8 @@ int mc3d_solver_set_sponge(mc3d_solver s, const double *sigma) {
     MC3D_CUDA_TRY(cudaMemcpyAsync(s->sigma, sigma, (size_t)s->g.n() * 8, cudaMemcpyHostToDevice, s->stream));
     MC3D_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->sigma_set = true;
+    s->sponge_pts = 0;
+    for (long long i = 0; i < s->g.n(); i++) s->sponge_pts += sigma[i] != 0.0;
     return MC3D_OK;
 }
 
