@@ -120,8 +120,9 @@ __global__ void dsm_mu_taukk_kernel(Grid3 g, DsmMuTaukk<R> a) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double rho = a.q[0][i];
         const R rhoR = (R)rho, Smag = a.smag[i];
-        a.mu_sgs[i] = rhoR * Smag * a.avg[2][i] / a.avg[3][i];
-        const R tk = a.use_taukk ? (R)2.0 * rhoR * Smag * Smag * a.avg[0][i] / a.avg[1][i] : R(0);
+        const long long ia = a.avg_scalar ? 0 : i;
+        a.mu_sgs[i] = rhoR * Smag * a.avg[2][ia] / a.avg[3][ia];
+        const R tk = a.use_taukk ? (R)2.0 * rhoR * Smag * Smag * a.avg[0][ia] / a.avg[1][ia] : R(0);
         a.taukk[i] = tk;
         // p of updateNonConservedData less tau_kk / 2, and the temperature of that pressure
         const double u = a.q[1][i] / rho, v = a.q[2][i] / rho, w = a.q[3][i] / rho;
@@ -175,10 +176,12 @@ __global__ void dsm_finish_k_kernel(Grid3 g, DsmFinishK<R> a) {
 
 template <typename R>
 __global__ void dsm_ksgs_kernel(Grid3 g, const double *__restrict__ rho, const R *__restrict__ smag,
-                                const R *__restrict__ nini, const R *__restrict__ niki, R *__restrict__ ksgs) {
+                                const R *__restrict__ nini, const R *__restrict__ niki, R *__restrict__ ksgs,
+                                int avg_scalar) {
     const long long n = g.n();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const R c_over_prt = niki[i] / nini[i];
+        const long long ia = avg_scalar ? 0 : i;
+        const R c_over_prt = niki[ia] / nini[ia];
         ksgs[i] = -(R)CP * c_over_prt * (R)rho[i] * smag[i];
     }
 }
@@ -232,9 +235,9 @@ __global__ void __launch_bounds__(256) global_sum_kernel(Grid3 g, AvgBatch<R> b,
     }
 }
 
-// out[f][i] = (sum of the partials of field f) / n, the block mean
+// out[f][i] = (sum of the partials of field f) / n, the block mean, for i < nfill
 template <typename R>
-__global__ void fill_mean_kernel(Grid3 g, AvgBatch<R> b, const double *partial, int nparts) {
+__global__ void fill_mean_kernel(Grid3 g, AvgBatch<R> b, const double *partial, int nparts, long long nfill) {
     const int f = blockIdx.y;
     __shared__ double mean;
     if (threadIdx.x == 0) {
@@ -244,8 +247,7 @@ __global__ void fill_mean_kernel(Grid3 g, AvgBatch<R> b, const double *partial, 
     }
     __syncthreads();
     const R m = (R)mean;
-    const long long n = g.n();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nfill; i += (long long)gridDim.x * blockDim.x)
         b.out[f][i] = m;
 }
 
@@ -283,15 +285,15 @@ int launch_dsm_finish_k(const Grid3 &g, const DsmFinishK<R> &a, cudaStream_t st)
 }
 template <typename R>
 int launch_dsm_ksgs(const Grid3 &g, const double *rho, const R *smag, const R *nini, const R *niki, R *ksgs,
-                    cudaStream_t st) {
-    dsm_ksgs_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rho, smag, nini, niki, ksgs);
+                    int avg_scalar, cudaStream_t st) {
+    dsm_ksgs_kernel<R><<<grid_for(g.n(), 256), 256, 0, st>>>(g, rho, smag, nini, niki, ksgs, avg_scalar);
     MC3D_CUDA_TRY(cudaGetLastError());
     return MC3D_OK;
 }
 
 template <typename R>
 int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scratch, size_t scratch_doubles,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool mean_only) {
     if (b.nf <= 0) return MC3D_OK;
     if (b.nf > 8) return fail(MC3D_ERR_ARG, "at most 8 fields per average");
     if (mode == MC3D_AVG_XI1 || mode == MC3D_AVG_XI2 || mode == MC3D_AVG_XI3) {
@@ -310,7 +312,9 @@ int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scrat
         if (parts < 1) return fail(MC3D_ERR_ARG, "averaging scratch too small");
         global_sum_kernel<R><<<dim3(parts, b.nf), 256, 0, st>>>(g, b, scratch);
         MC3D_CUDA_TRY(cudaGetLastError());
-        fill_mean_kernel<R><<<dim3(grid_for(g.n(), 256), b.nf), 256, 0, st>>>(g, b, scratch, parts);
+        // (mean_only: one block per field writes element 0)
+        fill_mean_kernel<R><<<dim3(mean_only ? 1 : grid_for(g.n(), 256), b.nf), 256, 0, st>>>(
+            g, b, scratch, parts, mean_only ? 1LL : g.n());
         MC3D_CUDA_TRY(cudaGetLastError());
         return MC3D_OK;
     }
@@ -324,8 +328,8 @@ int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scrat
     template int launch_dsm_prep_k<R>(const Grid3 &, const DsmPrepK<R> &, const Metrics<R> &, cudaStream_t);     \
     template int launch_dsm_finish_k<R>(const Grid3 &, const DsmFinishK<R> &, cudaStream_t);                    \
     template int launch_dsm_ksgs<R>(const Grid3 &, const double *, const R *, const R *, const R *, R *,          \
-                                    cudaStream_t);                                                              \
-    template int launch_average<R>(const Grid3 &, int, const AvgBatch<R> &, double *, size_t, cudaStream_t);
+                                    int, cudaStream_t);                                                                   \
+    template int launch_average<R>(const Grid3 &, int, const AvgBatch<R> &, double *, size_t, cudaStream_t, bool);
 MC3D_DSM_INST(float)
 MC3D_DSM_INST(double)
 #undef MC3D_DSM_INST

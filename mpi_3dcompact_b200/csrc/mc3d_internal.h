@@ -360,6 +360,7 @@ struct DsmMuTaukk {
     const double *q[5];
     const R *smag;
     const R *avg[4];      // averaged Lkk, C_I denominator, L_ij M_ij, M_ij M_ij
+    int avg_scalar;       // 1: avg[k][0] holds the value of every point (the GLOBAL mean)
     R *mu_sgs, *taukk;
     R *T;                 // temperature of p - tau_kk / 2 (written in place)
     int use_taukk;
@@ -399,12 +400,13 @@ template <typename R>
 int launch_dsm_finish_k(const Grid3 &g, const DsmFinishK<R> &a, cudaStream_t st);
 template <typename R>
 int launch_dsm_ksgs(const Grid3 &g, const double *rho, const R *smag, const R *nini, const R *niki, R *ksgs,
-                    cudaStream_t st);
+                    int avg_scalar, cudaStream_t st);
 // XI1/XI2/XI3 line means or the GLOBAL block mean of up to 8 fields (in may equal out);
 // scratch holds the FP64 partial sums of GLOBAL
 template <typename R>
+// mean_only (GLOBAL): write the mean into element 0 of each output only
 int launch_average(const Grid3 &g, int mode, const AvgBatch<R> &b, double *scratch, size_t scratch_doubles,
-                   cudaStream_t st);
+                   cudaStream_t st, bool mean_only = false);
 
 int launch_integrals(const Grid3 &g, const double *const q[5], double *acc2, cudaStream_t st);
 int launch_nonfinite_check(const Grid3 &g, const double *const q[5], int *flag, cudaStream_t st);

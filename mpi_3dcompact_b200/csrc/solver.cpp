@@ -396,9 +396,14 @@ static int test_filter3(mc3d_solver s, int nf, void *const *in, void *const *tmp
 // in t); XI1/XI2/XI3/GLOBAL average in place; NONE leaves them. Returns the
 // arrays that hold the result in res[].
 template <typename R>
-static int sgs_average(mc3d_solver s, int nf, void *const *f, void *const *t, const LineOpBuf *ops, void **res) {
+// scalar (optional): the caller reads element 0 of each result for every
+// point, so GLOBAL averaging writes the mean there only (*scalar = 1)
+static int sgs_average(mc3d_solver s, int nf, void *const *f, void *const *t, const LineOpBuf *ops, void **res,
+                       int *scalar = nullptr) {
     int rc;
     const int mode = s->cfg.les_averaging;
+    const bool mean_only = scalar && mode == MC3D_AVG_GLOBAL;
+    if (scalar) *scalar = mean_only ? 1 : 0;
     for (int i = 0; i < nf; i++) res[i] = f[i];
     if (mode == MC3D_AVG_NONE) return MC3D_OK;
     if (mode == MC3D_AVG_LOCAL) {
@@ -415,8 +420,8 @@ static int sgs_average(mc3d_solver s, int nf, void *const *f, void *const *t, co
         b.out[i] = (R *)f[i];
     }
     s->launches += mode == MC3D_AVG_GLOBAL ? 2 : 1;
-    if ((rc = tic(s, KC_SGS, 2.0 * nf * sizeof(R) * (double)s->g.n()))) return rc;
-    if ((rc = launch_average<R>(s->g, mode, b, s->avg_scratch, AVG_SCRATCH, s->stream))) return rc;
+    if ((rc = tic(s, KC_SGS, (mean_only ? 1.0 : 2.0) * nf * sizeof(R) * (double)s->g.n()))) return rc;
+    if ((rc = launch_average<R>(s->g, mode, b, s->avg_scratch, AVG_SCRATCH, s->stream, mean_only))) return rc;
     return toc(s);
 }
 
@@ -445,11 +450,13 @@ static int dsm_mu_taukk(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
     if ((rc = launch_dsm_finish_mu<R>(s->g, fm, s->stream))) return rc;
     if ((rc = toc(s))) return rc;
     void *avg[4];
-    if ((rc = sgs_average<R>(s, 4, s->dA, s->dA + 4, s->top, avg))) return rc;
+    int avg_scalar = 0;
+    if ((rc = sgs_average<R>(s, 4, s->dA, s->dA + 4, s->top, avg, &avg_scalar))) return rc;
     DsmMuTaukk<R> mt{};
     for (int v = 0; v < 5; v++) mt.q[v] = qP[v];
     mt.smag = (const R *)s->smag;
     for (int i = 0; i < 4; i++) mt.avg[i] = (const R *)avg[i];
+    mt.avg_scalar = avg_scalar;
     mt.mu_sgs = (R *)s->mu_sgs;
     mt.taukk = (R *)s->taukk;
     mt.T = (R *)s->prim[4];
@@ -457,7 +464,7 @@ static int dsm_mu_taukk(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
     mt.cons_mask = s->cons_mask;
     mt.rho_prim = (const R *)s->prim[0];
     s->launches++;
-    if ((rc = tic(s, KC_SGS, (5.0 * 8 + 8.0 * sizeof(R)) * n))) return rc;
+    if ((rc = tic(s, KC_SGS, (5.0 * 8 + (avg_scalar ? 4.0 : 8.0) * sizeof(R)) * n))) return rc;
     if ((rc = launch_dsm_mu_taukk<R>(s->g, mt, s->stream))) return rc;
     return toc(s);
 }
@@ -491,11 +498,12 @@ static int dsm_ksgs(mc3d_solver s, double *const *qP, const Metrics<R> &m) {
     if ((rc = launch_dsm_finish_k<R>(s->g, fk, s->stream))) return rc;
     if ((rc = toc(s))) return rc;
     void *avg[2];
-    if ((rc = sgs_average<R>(s, 2, s->dA, s->dA + 2, s->top, avg))) return rc;
+    int avg_scalar = 0;
+    if ((rc = sgs_average<R>(s, 2, s->dA, s->dA + 2, s->top, avg, &avg_scalar))) return rc;
     s->launches++;
-    if ((rc = tic(s, KC_SGS, (8.0 + 4.0 * sizeof(R)) * n))) return rc;
+    if ((rc = tic(s, KC_SGS, (8.0 + (avg_scalar ? 2.0 : 4.0) * sizeof(R)) * n))) return rc;
     if ((rc = launch_dsm_ksgs<R>(s->g, qP[0], (const R *)s->smag, (const R *)avg[0], (const R *)avg[1],
-                                 (R *)s->ksgs, s->stream)))
+                                 (R *)s->ksgs, avg_scalar, s->stream)))
         return rc;
     return toc(s);
 }
